@@ -1,0 +1,410 @@
+#!/usr/bin/env python
+"""Benchmark of the dense-MAC pressure projection (Maelstrom.jl's FlipBasin project!).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mpp|reference]
+
+One step = one projection (project!: volume and gamma, rhs, clearair, the pressure
+solve to 1e-6 relative residual, the gradient update with valid flags) of the 256^3
+basin with a Rankine vortex (Gamma = 225 m^2/s, core 2.5 m), FP32 face velocities
+uniform[-1, 1) m/s from seed 1001, synthetic. Each step restores the input velocities
+and starts the solve from P = 0, so every step does the same work.
+
+`value` is the mixed-precision (FP16-stored V-cycle, FP32 compute, FP64 reductions and
+coarsest solve), graph-captured projection rate; the plain FP32 form's rate is in
+`fp32_plain`. `e2e` is the same projection through the public API with the inputs in
+pinned host memory: every step copies u, v, w, types, phi, P to the device and reads
+u, v, w, fu, fv, fw, P back. Multi-GPU runs are independent replicas (the projection of
+one basin does not shard): `value` sums the ranks' rates, timed as the slowest rank.
+
+`--impl reference` times the CPU restatement of the reference's projection (the
+oracle; the reference itself is Julia on Vulkan and cannot run here) on the host's
+cores, on the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "maelstrom.jl_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "256³ projections/s to 1e-6 resid: mixed+graph vs plain FP32; % HBM peak"
+UNIT = "projections/s"
+WORKLOAD = "whirl256"
+TOL = 1e-6
+MAXITER = 200
+DT = 1.0 / 48
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload_config(precision, graph):
+    return {"workload": "whirl256: 256^3 cylindrical basin (wall r=0.45 N dx, water 0.6 deep, dx=0.05 m), "
+                        "Rankine vortex Gamma=225 m^2/s core 2.5 m + uniform[-1,1) m/s faces, seed 1001",
+            "cells": 256 ** 3, "tol": TOL, "precision": precision, "graph": graph,
+            "l2": "inputs larger than L2 (each CG iteration streams ~1 GB through 126 MB of L2); no flush",
+            "parallelism": "replicas"}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel_key):
+    """DRAM bytes per launch of the dominant kernel, from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, "profiles", "ncu_whirl256_kernels.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch\[" + re.escape(kernel_key) + r"\]\s*=\s*([0-9.eE+]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init():
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_mpp(args):
+    import numpy as np
+    import torch
+
+    import mpp
+    from mpp import scene
+
+    world, rank, local = dist_init()
+    dev = torch.device("cuda", local)
+    basin = scene.config_basin(WORKLOAD)
+    g = basin.grid
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    types, phi = T(basin.types), T(basin.phi)
+    u0, v0, w0 = T(basin.u), T(basin.v), T(basin.w)
+    u, v, w = u0.clone(), v0.clone(), w0.clone()
+    fu, fv, fw = (torch.zeros(a.numel(), dtype=torch.uint8, device=dev) for a in (u0, v0, w0))
+    P = torch.zeros(g.ncells, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def make(precision, graph):
+        return mpp.Projector(g, tol=TOL, maxiter=MAXITER, precision=precision, graph=graph)
+
+    def timed(proj, steps, warmup, sampler=None):
+        vol0 = proj.volume(phi)
+        launches, its, last = 0, [], None
+
+        def step():
+            nonlocal launches, last
+            u.copy_(u0)
+            v.copy_(v0)
+            w.copy_(w0)
+            P.zero_()
+            last = proj.project(u, v, w, fu, fv, fw, P, types, phi, vol0, DT)
+            return last
+
+        for _ in range(warmup):
+            step()
+        barrier(world)
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            r = step()
+            launches += r.kernel_launches
+            its.append(r.iterations)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        clocks = sampler.stop() if sampler else None
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
+        return ms, launches, its, last, clocks
+
+    # headline: mixed precision + graph
+    prec = args.precision
+    proj = make(prec, True)
+    sampler = ClockSampler(local) if rank == 0 else None
+    ms, launches, its, res, clocks = timed(proj, args.steps, args.warmup, sampler)
+    P_mixed = P.detach().cpu().numpy().copy()
+    value = world * args.steps / (ms / 1e3)
+
+    # plain FP32 (the reference's arithmetic, host-driven loop)
+    proj32 = make("fp32", False)
+    ms32, launches32, its32, res32, _ = timed(proj32, args.steps, args.warmup)
+    P_fp32 = P.detach().cpu().numpy().copy()
+    value32 = world * args.steps / (ms32 / 1e3)
+    del proj32
+
+    # FP64 oracle on the GPU: every result's pressure error
+    proj64 = make("fp64", True)
+    proj64.set(tol=1e-12, maxiter=400)
+    _, _, _, res64, _ = timed(proj64, 1, 0)
+    P64 = proj64.solution_f64()
+    del proj64
+    nrm = float(np.linalg.norm(P64))
+    err_mixed = float(np.linalg.norm(P_mixed - P64) / nrm)
+    err_fp32 = float(np.linalg.norm(P_fp32 - P64) / nrm)
+
+    # e2e: the public call with host buffers, copies inside the timed region
+    pin = lambda t: t.detach().cpu().pin_memory()
+    h_in = {"u": pin(u0), "v": pin(v0), "w": pin(w0), "types": pin(types), "phi": pin(phi),
+            "P": pin(torch.zeros_like(P))}
+    h_out = {k: torch.empty(t.numel(), dtype=t.dtype).pin_memory() for k, t in
+             (("u", u0), ("v", v0), ("w", w0), ("fu", fu), ("fv", fv), ("fw", fw), ("P", P))}
+    d_types, d_phi = torch.empty_like(types), torch.empty_like(phi)
+    h2d = sum(t.numel() * t.element_size() for t in h_in.values())
+    d2h = sum(t.numel() * t.element_size() for t in h_out.values())
+    vol0 = proj.volume(phi)
+    e2e_steps = max(1, min(args.steps, 50))
+
+    def e2e_step():
+        u.copy_(h_in["u"], non_blocking=True)
+        v.copy_(h_in["v"], non_blocking=True)
+        w.copy_(h_in["w"], non_blocking=True)
+        d_types.copy_(h_in["types"], non_blocking=True)
+        d_phi.copy_(h_in["phi"], non_blocking=True)
+        P.copy_(h_in["P"], non_blocking=True)
+        r = proj.project(u, v, w, fu, fv, fw, P, d_types, d_phi, vol0, DT)
+        for k, t in (("u", u), ("v", v), ("w", w), ("fu", fu), ("fv", fv), ("fw", fw), ("P", P)):
+            h_out[k].copy_(t, non_blocking=True)
+        return r
+
+    for _ in range(min(args.warmup, 2)):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_e2e = max_over_ranks(f0.elapsed_time(f1), world)
+    e2e_value = world * e2e_steps / (ms_e2e / 1e3)
+
+    # live per-kernel timing (CUDA events on the launching stream), one profiled projection
+    proj.profile(True)
+    for _ in range(2):
+        u.copy_(u0); v.copy_(v0); w.copy_(w0); P.zero_()
+        rprof = proj.project(u, v, w, fu, fv, fw, P, types, phi, vol0, DT)
+    prof = proj.profile_read()
+    proj.profile(False)
+    hbm, peak_src = peaks()
+    dom = max(prof, key=lambda e: e["ms"])
+    per_launch_bytes = dom["bytes"] / dom["launches"]
+    per_launch_ms = dom["ms"] / dom["launches"]
+    achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
+    key = f"{dom['name']}@{dom['level']}"
+    traffic = ncu_traffic(key)
+    # bytes per CG iteration (every kernel inside the loop) over the loop's time
+    loop = [e for e in prof if e["name"] in ("start", "rbgs", "residual", "restrict", "coarsest", "prolong", "dot",
+                                             "search", "advance")]
+    nit = max(1, 2 * rprof.iterations)
+    it_bytes = sum(e["bytes"] for e in loop) / nit
+    it_ms = sum(e["ms"] for e in loop) / nit
+    total_prof_ms = sum(e["ms"] for e in prof)
+
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset exists)",
+        "config": workload_config(prec, True),
+        "iterations": its[-1], "true_rel_residual": res.true_rel_residual, "fp64_rel_error": err_mixed,
+        "cells_per_s": value * g.ncells,
+        "fp32_plain": {"value": round(value32, 3), "unit": UNIT, "ms_per_step": round(ms32 / args.steps, 4),
+                       "iterations": its32[-1], "true_rel_residual": res32.true_rel_residual,
+                       "fp64_rel_error": err_fp32, "graph": False, "gpu_launches": launches32},
+        "mixed_over_fp32": round(value / value32, 3),
+        "fp64_oracle": {"iterations": res64.iterations, "true_rel_residual": res64.true_rel_residual},
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps},
+        "roofline": {"bound": "hbm", "kernel": key, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"
+                     if peak_src == "measured" else "fallback 6.65 TB/s",
+                     "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes,
+                     "launch_ms": round(per_launch_ms, 5),
+                     "share_of_profiled_time": round(dom["ms"] / total_prof_ms, 4)},
+        "iteration_roofline": {"bytes_per_iteration": it_bytes, "ms_per_iteration": round(it_ms, 4),
+                               "achieved": round(it_bytes / (it_ms / 1e3) / 1e9, 1), "peak": hbm,
+                               "frac": round(it_bytes / (it_ms / 1e3) / 1e9 / hbm, 4)},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(basin, max_seconds=args.cpu_seconds)
+    if rank == 0:
+        if args.profile_out:
+            with open(args.profile_out, "w") as f:
+                json.dump({"projection_profile": prof, "iterations": rprof.iterations}, f, indent=1)
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def cpu_baseline(basin, max_seconds=30.0):
+    """The oracle (the reference's FP32 projection restated in C + OpenMP) on this host."""
+    import oracle
+
+    threads = oracle.num_threads()
+    vol0 = oracle.volume(basin.grid, basin.phi)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        oracle.project(basin, volume0=vol0, dt=DT, tol=TOL, maxiter=MAXITER)
+        n += 1
+        el = time.perf_counter() - t0
+        if el * (n + 1) / n > max_seconds:
+            break
+    return {"value": round(n / el, 4), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} full whirl256 projection(s) (256^3, tol 1e-6) by the C/OpenMP oracle, {el:.1f} s"}
+
+
+def run_reference(args):
+    """The reference arm: the oracle's projection on the host cores (rank 0 only)."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    import oracle
+    from mpp import scene
+
+    basin = scene.config_basin(WORKLOAD)
+    threads = oracle.num_threads()
+    vol0 = oracle.volume(basin.grid, basin.phi)
+    run = lambda: oracle.project(basin, volume0=vol0, dt=DT, tol=TOL, maxiter=MAXITER)
+    t0 = time.perf_counter()
+    run()  # one warm-up projection whatever W is: each takes seconds on the CPU
+    first = time.perf_counter() - t0
+    budget = args.reference_seconds
+    steps = max(1, min(args.steps, int(budget / max(first, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        info = run()["info"]
+    el = time.perf_counter() - t0
+    value = steps / el
+    out = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "steps_timed": steps, "warmup": 1, "ms_per_step": round(1e3 * el / steps, 2), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset exists)",
+           "impl": "reference", "config": workload_config("fp32", False), "iterations": info.iterations,
+           "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
+                            "sample": f"{steps} full whirl256 projection(s) timed (of {args.steps} asked, within "
+                                      f"{budget:.0f} s) after 1 warm-up, C/OpenMP restatement of src/flip.jl"
+                                      f":1144-1156 (the Julia/Vulkan reference cannot run here)"},
+           "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="mpp", choices=["mpp", "reference"])
+    ap.add_argument("--precision", default="fp16", choices=["fp16", "bf16", "fp32"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--cpu-seconds", type=float, default=25.0)
+    ap.add_argument("--reference-seconds", type=float, default=150.0)
+    ap.add_argument("--profile-out", default=None)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "mpp":
+        ap.error("--warmup must be at least 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_mpp(args)
+
+
+if __name__ == "__main__":
+    main()

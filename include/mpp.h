@@ -1,0 +1,181 @@
+/*
+ * libmpp — the dense-MAC pressure projection of Maelstrom.jl's FlipBasin, as
+ * hand-written CUDA kernels for sm_100a behind a plain C ABI.
+ *
+ * The Julia package reaches it with `ccall`: every array is the FlipBasin's own
+ * device array, passed as a raw pointer, with the same bytes (Julia column-major,
+ * i fastest, 0-based linear index i + nx*(j + ny*k)):
+ *   u: (nx+1, ny, nz) float   v: (nx, ny+1, nz) float   w: (nx, ny, nz+1) float
+ *   fu, fv, fw: uint8 of the same face shapes
+ *   P, phi: (nx, ny, nz) float        types: (nx, ny, nz) uint8 (SOLID 0, LIQUID 1, AIR 2)
+ *
+ * The library owns its workspace (the CG vectors, the multigrid levels, partial sums,
+ * the CUDA graph) inside an opaque context, one per basin. All work is queued on
+ * the caller's stream; calls that return an mpp_result synchronise that stream once,
+ * at the end. A context is not thread-safe; distinct contexts are independent.
+ *
+ * Return codes: MPP_OK and the solver statuses are >= 0, API/CUDA errors < 0.
+ */
+#ifndef MAELSTROM_MPP_H
+#define MAELSTROM_MPP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* CUDA stream handle (cudaStream_t); NULL is the legacy default stream. */
+typedef struct CUstream_st* mpp_stream;
+
+typedef struct mpp_ctx mpp_ctx;
+
+/* Solver statuses (mpp_result.status, and the return value of the solve calls). */
+enum {
+    MPP_OK = 0,            /* converged to tol */
+    MPP_NOT_CONVERGED = 1, /* maxiter reached ("pressure solve did not converge", src/flip.jl:1109) */
+    MPP_NONFINITE = 2,     /* a NaN/Inf in a norm or step ("Nonfinite pressure ...", src/sflip.jl:1873-1892) */
+    MPP_INDEFINITE = 3,    /* p.Ap <= 0 or z.r <= 0 ("Pressure CG requires a positive ...", src/sflip.jl:1880-1896) */
+    MPP_BREAKDOWN = 4,     /* FGMRES Arnoldi breakdown (src/fgmres.jl:77) */
+};
+
+/* API errors. */
+enum {
+    MPP_ERR_INVALID = -1, /* bad argument, size or grid */
+    MPP_ERR_CUDA = -2,    /* a CUDA runtime call failed (mpp_last_error() has the text) */
+    MPP_ERR_NOMEM = -3,   /* workspace allocation failed */
+};
+
+/* Arithmetic of the solve. */
+enum {
+    MPP_PREC_FP32 = 0,       /* the reference's: FP32 values, standard PCG */
+    MPP_PREC_MIXED_FP16 = 1, /* V-cycle stored in FP16, computed in FP32; flexible CG; FP64 reductions and coarsest solve */
+    MPP_PREC_MIXED_BF16 = 2, /* as above with BF16 storage */
+    MPP_PREC_FP64 = 3,       /* everything in FP64: the accuracy oracle, on the GPU */
+};
+
+/* FlipGrid (src/flip.jl:39-46): origin of the low corner, cell size, cells per axis, the
+ * cylinder's radius and floor height (cells whose centre lies outside the cylinder or
+ * under the floor are solid), and the multigrid's level count. */
+typedef struct {
+    float lo[3];
+    float dx;
+    int32_t n[3];
+    float radius;
+    float floor_z;
+    int32_t levels;
+} mpp_grid;
+
+/* Solver knobs: pressure!(s; tol, maxiter, sweeps) (src/flip.jl:1082) and vcycle!'s
+ * `coarse` (src/flip.jl:992), plus this library's own. */
+typedef struct {
+    float tol;              /* relative residual target (reference default 1e-4) */
+    int32_t maxiter;        /* CG iterations (reference default 60) */
+    int32_t sweeps;         /* red-black sweeps down and up per level (default 2) */
+    int32_t coarse;         /* sweeps of the coarsest solve, each way (default 40) */
+    int32_t precision;      /* MPP_PREC_* */
+    int32_t graph;          /* 1: the whole projection is one CUDA graph launch with a
+                               device-side convergence test (no host round trips) */
+    int32_t fallback;       /* 1: FGMRES when CG fails or misses tol on the true residual */
+    int32_t restart;        /* FGMRES restart length (default 8, src/fgmres.jl:26) */
+    int32_t fallback_maxiter; /* FGMRES iterations (default 240) */
+    int32_t cg_maxiter_with_fallback; /* CG iterations before the fallback (default 80, src/fgmres.jl:99) */
+} mpp_opts;
+
+typedef struct {
+    int32_t iterations;          /* CG iterations (what pressure! returns) */
+    int32_t status;              /* MPP_OK, MPP_NOT_CONVERGED, ... */
+    int32_t fallback_used;       /* 1 if FGMRES ran */
+    int32_t fallback_iterations; /* its iterations */
+    double rel_residual;         /* last recursive residual / |b| */
+    double true_rel_residual;    /* |b - A P| / |b|, recomputed at exit */
+    double bnorm;                /* |b| */
+    double volume;               /* liquid volume at entry (m^3), volume(s) */
+    float gamma;                 /* the volume-control divergence put into the rhs */
+    int64_t kernel_launches;     /* kernels this call ran on the device */
+} mpp_result;
+
+/* Defaults: tol 1e-4, maxiter 60, sweeps 2, coarse 40, FP32, no graph, no fallback. */
+void mpp_opts_default(mpp_opts* opts);
+
+/* FlipGrid's level rule (src/flip.jl:53-61): the fewest levels (>= 2) whose coarsest
+ * grid has at most 1024 cells; -1 if n is not a multiple of the level's 2^(levels-1). */
+int32_t mpp_levels_for(const int32_t n[3]);
+
+/* Create a context for one basin: allocates the workspace on the current device.
+ * Replaces the workspace half of FlipBasin(...) (src/flip.jl:189-224): levels, b, r,
+ * z, d, q, diag, rv, partials. */
+int mpp_ctx_create(mpp_ctx** out, const mpp_grid* grid, const mpp_opts* opts);
+int mpp_ctx_destroy(mpp_ctx* ctx);
+/* Change the knobs of an existing context (precision changes need a new context). */
+int mpp_ctx_set_opts(mpp_ctx* ctx, const mpp_opts* opts);
+/* Device bytes the context holds. */
+size_t mpp_ctx_bytes(const mpp_ctx* ctx);
+
+/* volume(s) (src/flip.jl:293): liquid volume in m^3 from the level set. */
+int mpp_volume(mpp_ctx* ctx, const float* phi, double* volume, mpp_stream stream);
+
+/* project!(s, dt; recover) (src/flip.jl:1144-1156): gamma from the volume loss, the
+ * rhs, clearair, pressure!, and the gradient update with the valid-face flags.
+ * In: u, v, w (after forces!/solidify!), types, phi, P (warm start), volume0.
+ * Out: u, v, w, fu, fv, fw, P; `res` (may be NULL). Returns the solve status or an error. */
+int mpp_project(mpp_ctx* ctx, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv, uint8_t* fw,
+                float* P, const uint8_t* types, const float* phi, float volume0, double dt,
+                double recover, mpp_result* res, mpp_stream stream);
+
+/* pressure!(s) (src/flip.jl:1082-1111) for a given right-hand side b: P in = warm start,
+ * P out = pressure. Returns the solve status or an error. */
+int mpp_pressure(mpp_ctx* ctx, float* P, const float* b, const uint8_t* types, const float* phi,
+                 mpp_result* res, mpp_stream stream);
+
+/* ---- single passes, for tests and for callers that split project! ---- */
+/* rhs_kernel! (src/flip.jl:817-822): b = -dx div u + dx^2 gamma on LIQUID, else 0. */
+int mpp_rhs(mpp_ctx* ctx, float* b, const float* u, const float* v, const float* w,
+            const uint8_t* types, float gamma, mpp_stream stream);
+/* diag_kernel! (src/flip.jl:824-836). */
+int mpp_diag(mpp_ctx* ctx, float* diag, const uint8_t* types, const float* phi, mpp_stream stream);
+/* vcycle!(s, z, r) (src/flip.jl:992-1014): z = M^-1 r for this types/phi. */
+int mpp_vcycle(mpp_ctx* ctx, float* z, const float* r, const uint8_t* types, const float* phi,
+               mpp_stream stream);
+/* y = A x (residual_kernel!'s operator, src/flip.jl:859-863). */
+int mpp_apply(mpp_ctx* ctx, float* y, const float* x, const uint8_t* types, const float* phi,
+              mpp_stream stream);
+/* project_kernel! for the three face sets (src/flip.jl:1113-1130). */
+int mpp_gradient(mpp_ctx* ctx, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv, uint8_t* fw,
+                 const float* P, const uint8_t* types, const float* phi, mpp_stream stream);
+
+/* FP64 pressure of the last mpp_pressure/mpp_project on an MPP_PREC_FP64 context. */
+int mpp_solution_f64(mpp_ctx* ctx, double* out_host);
+
+/* ---- per-kernel timing (the reference has none: bakeflip only logs @elapsed per
+ * frame, src/flip.jl:1992-2010) ----
+ * With profiling on, solves run their CG loop from the host (no graph) and bracket
+ * every kernel with CUDA events on the caller's stream. Each entry sums one kernel
+ * family at one level: launches, device milliseconds, and the algorithmic bytes the
+ * launches had to move (the array elements each pass reads or writes once, over the
+ * level's active tiles; dense passes over every cell). */
+typedef struct {
+    char name[24];
+    int32_t level;    /* multigrid level (0 = fine), -1 for whole-grid passes */
+    int32_t reserved;
+    int64_t launches;
+    double ms;
+    double bytes;
+    int64_t cells;    /* cells the last launch covered (active tiles x 512, or the grid) */
+} mpp_prof_entry;
+
+/* Turn profiling on (1) or off (0); turning it on clears the accumulators. */
+int mpp_profile_enable(mpp_ctx* ctx, int on);
+/* Copy up to `max` entries; returns how many exist (may exceed max). */
+int mpp_profile_read(mpp_ctx* ctx, mpp_prof_entry* out, int max);
+
+/* Text of the last error on this thread. */
+const char* mpp_last_error(void);
+/* Library version string. */
+const char* mpp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1028 @@
+// libmpp: host side. The context (workspace of one basin), the launch sequence of a
+// projection, its CUDA graph (one launch per projection: the CG loop is a conditional
+// WHILE node whose condition the kernels set on the device), and the C ABI of
+// include/mpp.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "mpp.h"
+#include "mpp_kernels.cuh"
+
+using namespace mpp;
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+void set_err(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+#define CK(call)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            set_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return MPP_ERR_CUDA;                                                             \
+        }                                                                                    \
+    } while (0)
+
+constexpr int MAXLEV = 16;
+constexpr int NCOUNTERS = 8;
+enum { CNT_VOLUME, CNT_SETUP, CNT_DOT, CNT_SEARCH, CNT_ADVANCE, CNT_TRUE };
+
+int vsize(int prec) { return prec == MPP_PREC_FP64 ? 8 : 4; }
+int msize(int prec) {
+    return prec == MPP_PREC_FP64 ? 8 : (prec == MPP_PREC_MIXED_FP16 || prec == MPP_PREC_MIXED_BF16) ? 2 : 4;
+}
+
+struct LevelBuf {
+    int n[3];
+    int H, GH, GJ, GK, ntiles;
+    bool split;
+    uint8_t* code;
+    void* dg;
+    void* x;
+    void* b;
+    void* r;
+    uint8_t* types;
+    uint8_t* tflag;
+    uint32_t* tiles;
+    int* count;
+};
+
+// Kernel families, for the profiler.
+enum { F_VOLUME, F_SETUP, F_LEVEL, F_TILES, F_START, F_RBGS, F_RESID, F_RESTRICT, F_COARSEST, F_PROLONG, F_DOT,
+       F_SEARCH, F_ADVANCE, F_TRUE, F_GRADIENT, F_CONVERT, NFAM };
+const char* const FAM_NAMES[NFAM] = {"volume",   "setup",    "coarsen", "tilelists", "start",         "rbgs",
+                                     "residual", "restrict", "coarsest", "prolong",  "dot",           "search",
+                                     "advance",  "true_residual", "gradient", "convert"};
+struct ProfRec {
+    int fam, level;
+    cudaEvent_t a, b;
+};
+struct ProfAcc {
+    int64_t n;
+    double ms, bytes;
+    int64_t cells;
+};
+
+}  // namespace
+
+struct mpp_ctx {
+    mpp_grid grid;
+    mpp_opts opts;
+    int prec;
+    int L;
+    int dev, nsm;
+    LevelBuf lv[MAXLEV];
+    // fine-level CG vectors (row-split, type V)
+    void *diag, *bvec, *r, *d, *q;
+    void* Pd;  // FP64 solution (natural), FP64 contexts only
+    uint8_t* tflag_all;
+    size_t tflag_bytes;
+    Scalars* sc;
+    Scalars* sc_host;  // pinned
+    double* partials;
+    unsigned* counters;
+    std::vector<void*> allocs;
+    size_t bytes;
+    int64_t launches;
+    // graph cache
+    cudaGraphExec_t gexec;
+    cudaGraph_t graph;
+    cudaStream_t cap;  // stream the graph is captured on (never the caller's)
+    const void* gkey[10];
+    int gkind;
+    int g_prologue, g_body, g_epilogue;  // kernel counts in the graph's parts
+    // profiler
+    int prof_on;
+    std::vector<ProfRec> pending;
+    std::vector<cudaEvent_t> evfree, evall;
+    ProfAcc prof[NFAM][MAXLEV + 1];
+    int active[MAXLEV];
+};
+
+namespace {
+
+int alloc(mpp_ctx* c, void** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        set_err("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        return MPP_ERR_NOMEM;
+    }
+    e = cudaMemset(*p, 0, bytes);
+    if (e != cudaSuccess) {
+        set_err("cudaMemset failed: %s", cudaGetErrorString(e));
+        return MPP_ERR_CUDA;
+    }
+    c->allocs.push_back(*p);
+    c->bytes += bytes;
+    return MPP_OK;
+}
+
+template <class M>
+Lev<M> view(const mpp_ctx* c, int l) {
+    const LevelBuf& b = c->lv[l];
+    Lev<M> v;
+    v.n1 = b.n[0]; v.n2 = b.n[1]; v.n3 = b.n[2];
+    v.H = b.H; v.GH = b.GH; v.GJ = b.GJ; v.GK = b.GK;
+    v.code = b.code;
+    v.dg = (M*)b.dg; v.x = (M*)b.x; v.b = (M*)b.b; v.r = (M*)b.r;
+    v.types = b.types; v.tflag = b.tflag; v.tiles = b.tiles; v.count = b.count;
+    return v;
+}
+
+int grid_cells(const mpp_ctx* c, int64_t n) {
+    int64_t g = (n + TPB - 1) / TPB;
+    int64_t cap = (int64_t)c->nsm * MAXBLOCKS_PER_SM;
+    return (int)(g < cap ? (g > 0 ? g : 1) : cap);
+}
+int grid_tiles(const mpp_ctx* c, int l) {
+    int g = c->lv[l].ntiles;
+    int cap = c->nsm * MAXBLOCKS_PER_SM;
+    return g < cap ? (g > 0 ? g : 1) : cap;
+}
+
+Geo geo_of(const mpp_grid& g) {
+    Geo o;
+    for (int a = 0; a < 3; a++) { o.lo[a] = g.lo[a]; o.n[a] = g.n[a]; }
+    o.dx = g.dx;
+    o.radius = g.radius;
+    o.floor_z = g.floor_z;
+    return o;
+}
+
+cudaEvent_t prof_event(mpp_ctx* c) {
+    if (!c->evfree.empty()) {
+        cudaEvent_t e = c->evfree.back();
+        c->evfree.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    c->evall.push_back(e);
+    return e;
+}
+
+// Algorithmic bytes of one launch of a kernel family: each array element the pass must
+// read or write, counted once, over the cells it covers (m, v: the V-cycle's and the CG
+// vectors' element sizes; p: the solution's).
+void prof_size(const mpp_ctx* c, int fam, int level, double& bytes, int64_t& cells) {
+    const double m = msize(c->prec), v = vsize(c->prec), p = c->prec == MPP_PREC_FP64 ? 8 : 4;
+    const bool sep = m != v;
+    const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+    const int64_t tile_cells = 2 * TH * TY * TZ;
+    auto lcells = [&](int l) { return (int64_t)c->lv[l].n[0] * c->lv[l].n[1] * c->lv[l].n[2]; };
+    auto act = [&](int l) { return (int64_t)c->active[l] * tile_cells; };
+    double bpc = 0;
+    switch (fam) {
+        case F_VOLUME: cells = N; bpc = 4; break;
+        case F_SETUP: cells = N; bpc = 1 + 12 + 4 + 8 + 1 + 3 * v + (sep ? 2 * m : 0); break;
+        case F_LEVEL: cells = lcells(level); bpc = 8 + 1 + 1 + m; break;
+        case F_TILES: {
+            cells = 0;
+            for (int l = 0; l < c->L - 1; l++) cells += c->lv[l].ntiles;
+            bpc = 1 + 4;
+            break;
+        }
+        case F_START: cells = act(level); bpc = 1 + 2 * m; break;
+        case F_RBGS: cells = act(level); bpc = 0.5 + 2 * m; break;
+        case F_RESID: cells = act(level); bpc = 1 + 4 * m; break;
+        case F_RESTRICT: cells = act(level); bpc = 8 * (1 + m) + 1 + m; break;
+        case F_COARSEST: cells = lcells(level); bpc = 8 * (1 + m) + 1 + m; break;
+        case F_PROLONG: cells = act(level); bpc = 1 + 2 * m + (1 + m) / 8; break;
+        case F_DOT: cells = act(level); bpc = 1 + m + v + (sep ? v : 0); break;
+        case F_SEARCH: cells = act(level); bpc = 1 + m + 3 * v; break;
+        case F_ADVANCE: cells = act(level); bpc = 1 + m + 5 * v + 2 * p + (sep ? m : 0); break;
+        case F_TRUE: cells = act(level); bpc = 1 + 2 * v + p; break;
+        case F_GRADIENT: cells = N; bpc = 1 + 4 + 4 + 24 + 3; break;
+        case F_CONVERT: cells = N; bpc = 12; break;
+        default: cells = 0; bpc = 0;
+    }
+    bytes = bpc * (double)cells;
+}
+
+// Fold the finished launches' event pairs into the accumulators (after a sync).
+void prof_collect(mpp_ctx* c) {
+    if (c->pending.empty()) return;
+    for (int l = 0; l < c->L - 1; l++) cudaMemcpy(&c->active[l], c->lv[l].count, sizeof(int), cudaMemcpyDeviceToHost);
+    for (const ProfRec& r : c->pending) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        ProfAcc& a = c->prof[r.fam][r.level < 0 ? MAXLEV : r.level];
+        double bytes;
+        int64_t cells;
+        prof_size(c, r.fam, r.level, bytes, cells);
+        a.n += 1;
+        a.ms += ms;
+        a.bytes += bytes;
+        a.cells = cells;
+        c->evfree.push_back(r.a);
+        c->evfree.push_back(r.b);
+    }
+    c->pending.clear();
+}
+
+// ---- launch sequences (the same code records the graph and runs the host loop) ----
+// Every launch goes through beg()/end(): with profiling on they bracket it with CUDA
+// events on the launching stream, tagged with its kernel family and level.
+template <class Pr>
+struct Run {
+    using V = typename Pr::V;
+    using M = typename Pr::M;
+    mpp_ctx* c;
+    cudaStream_t s;
+    int nk = 0;  // kernels launched
+    cudaEvent_t ev0 = nullptr;
+    int fam = 0, lvl = 0;
+
+    unsigned* cnt(int i) { return c->counters + i; }
+
+    void beg(int f, int l) {
+        nk++;
+        if (!c->prof_on) return;
+        fam = f;
+        lvl = l;
+        ev0 = prof_event(c);
+        cudaEventRecord(ev0, s);
+    }
+    void end() {
+        if (!c->prof_on) return;
+        cudaEvent_t ev1 = prof_event(c);
+        cudaEventRecord(ev1, s);
+        c->pending.push_back(ProfRec{fam, lvl, ev0, ev1});
+    }
+
+    // volume(s) and gamma (src/flip.jl:1146-1147)
+    void volume(const float* phi) {
+        const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+        beg(F_VOLUME, -1);
+        k_volume<<<grid_cells(c, N), TPB, 0, s>>>(geo_of(c->grid), phi, c->sc, c->partials, cnt(CNT_VOLUME));
+        end();
+    }
+
+    // The fine set-up pass, the coarse levels and the tile lists.
+    void setup(const SetupIn<V>& in, cudaGraphConditionalHandle cond, int use_cond) {
+        cudaMemsetAsync(c->tflag_all, 0, c->tflag_bytes, s);
+        const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+        beg(F_SETUP, -1);
+        k_setup<Pr><<<grid_cells(c, N), TPB, 0, s>>>(in, view<M>(c, 0), (V*)c->diag, (V*)c->bvec, (V*)c->r, c->sc,
+                                                      c->partials, cnt(CNT_SETUP), cond, use_cond);
+        end();
+        for (int l = 1; l < c->L; l++) {
+            const LevelBuf& f = c->lv[l - 1];
+            const uint8_t* tf = l == 1 ? in.types : f.types;
+            const int64_t Nl = (int64_t)c->lv[l].n[0] * c->lv[l].n[1] * c->lv[l].n[2];
+            beg(F_LEVEL, l);
+            k_level<Pr><<<grid_cells(c, Nl), TPB, 0, s>>>(tf, f.n[0], f.n[1], f.n[2], view<M>(c, l),
+                                                           c->lv[l].split ? 1 : 0);
+            end();
+        }
+        TileTab tab;
+        memset(&tab, 0, sizeof(tab));
+        tab.nlev = c->L - 1;
+        for (int l = 0; l < c->L - 1; l++) {
+            tab.ntiles[l] = c->lv[l].ntiles;
+            tab.flags[l] = c->lv[l].tflag;
+            tab.tiles[l] = c->lv[l].tiles;
+            tab.count[l] = c->lv[l].count;
+        }
+        beg(F_TILES, -1);
+        k_tilelists<<<tab.nlev, 1024, 0, s>>>(tab);
+        end();
+    }
+
+    void smooth(int l, const std::vector<int>& colours) {
+        for (int col : colours) {
+            beg(F_RBGS, l);
+            k_rbgs<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l), col);
+            end();
+        }
+    }
+
+    // vcycle! (src/flip.jl:992-1014): z = M^-1 r from zero.
+    void vcycle() {
+        const int L = c->L, sw = c->opts.sweeps;
+        std::vector<int> down, up;
+        for (int q = 0; q < sw; q++) { down.push_back(0); down.push_back(1); }
+        down.erase(down.begin());  // the start kernel is the first colour's first sweep
+        for (int q = 0; q < sw; q++) { up.push_back(1); up.push_back(0); }
+        for (int l = 0; l < L - 1; l++) {
+            beg(F_START, l);
+            k_start<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l));
+            end();
+            smooth(l, down);
+            beg(F_RESID, l);
+            k_residual<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l));
+            end();
+            if (l + 1 < L - 1) {
+                beg(F_RESTRICT, l + 1);
+                k_restrict<Pr><<<grid_tiles(c, l + 1), TPB, 0, s>>>(view<M>(c, l), view<M>(c, l + 1));
+                end();
+            }
+        }
+        beg(F_COARSEST, L - 1);
+        k_coarsest<Pr><<<1, 1024, 0, s>>>(view<M>(c, L - 2), view<M>(c, L - 1), c->opts.coarse);
+        end();
+        for (int l = L - 2; l >= 0; l--) {
+            beg(F_PROLONG, l);
+            k_prolong<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l), view<M>(c, l + 1), l + 1 == L - 1 ? 1 : 0);
+            end();
+            smooth(l, up);
+        }
+    }
+
+    // One CG iteration, rotated so a loop of them is pressure!'s loop (src/flip.jl:1095-1108):
+    // z = M^-1 r, rho/beta, q = A p and alpha, then the step and the exit test.
+    void body(V* P, cudaGraphConditionalHandle cond, int use_cond) {
+        vcycle();
+        beg(F_DOT, 0);
+        k_dot<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->r, (const V*)c->q, c->sc, c->partials,
+                                                    cnt(CNT_DOT));
+        end();
+        beg(F_SEARCH, 0);
+        k_search<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q, c->sc,
+                                                       c->partials, cnt(CNT_SEARCH));
+        end();
+        beg(F_ADVANCE, 0);
+        k_advance<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (V*)c->d, (const V*)c->q, (V*)c->r, P, c->sc,
+                                                        c->partials, cnt(CNT_ADVANCE), cond, use_cond);
+        end();
+    }
+
+    void true_residual(const V* P) {
+        beg(F_TRUE, 0);
+        k_true_residual<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->bvec, (const V*)c->diag, P,
+                                                              nullptr, c->sc, c->partials, cnt(CNT_TRUE));
+        end();
+    }
+
+    void gradient(float* u, float* v, float* w, uint8_t* fu, uint8_t* fv, uint8_t* fw, const float* P,
+                  const uint8_t* types, const float* phi) {
+        const int64_t N = (int64_t)(c->grid.n[0] + 1) * (c->grid.n[1] + 1) * (c->grid.n[2] + 1);
+        beg(F_GRADIENT, -1);
+        k_gradient<<<grid_cells(c, N), TPB, 0, s>>>(c->grid.n[0], c->grid.n[1], c->grid.n[2], u, v, w, fu, fv, fw, P,
+                                                    types, phi, c->grid.dx);
+        end();
+    }
+
+    void widen(const float* P) {
+        const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+        beg(F_CONVERT, -1);
+        k_widen<<<grid_cells(c, N), TPB, 0, s>>>((double*)c->Pd, P, N);
+        end();
+    }
+    void narrow(float* P) {
+        const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+        beg(F_CONVERT, -1);
+        k_narrow<<<grid_cells(c, N), TPB, 0, s>>>(P, (const double*)c->Pd, N);
+        end();
+    }
+};
+
+int write_params(mpp_ctx* c, float volume0, double dt, double recover, int project, float gamma, cudaStream_t s) {
+    Params& p = c->sc_host->p;
+    p.volume0 = volume0;
+    p.tol = c->opts.tol;
+    p.dt = dt;
+    p.recover = recover;
+    p.maxiter = c->opts.maxiter;
+    p.project = project;
+    p.gamma = gamma;
+    CK(cudaMemcpyAsync(&c->sc->p, &c->sc_host->p, sizeof(Params), cudaMemcpyHostToDevice, s));
+    return MPP_OK;
+}
+
+int read_state(mpp_ctx* c, cudaStream_t s) {
+    CK(cudaMemcpyAsync(&c->sc_host->s, &c->sc->s, sizeof(State), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return MPP_OK;
+}
+
+// Leaf nodes of a graph (nodes nothing depends on).
+int graph_leaves(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves) {
+    size_t n = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    CK(cudaGraphGetNodes(g, nodes.data(), &n));
+    leaves.clear();
+    for (auto nd : nodes) {
+        size_t m = 0;
+        CK(cudaGraphNodeGetDependentNodes(nd, nullptr, &m));
+        if (m == 0) leaves.push_back(nd);
+    }
+    return MPP_OK;
+}
+
+struct Call {
+    // project (kind 1) or pressure (kind 0)
+    int kind;
+    float *u, *v, *w;
+    uint8_t *fu, *fv, *fw;
+    float* P;
+    const float* bnat;
+    const uint8_t* types;
+    const float* phi;
+};
+
+template <class Pr>
+SetupIn<typename Pr::V> setup_in(mpp_ctx* c, const Call& k) {
+    using V = typename Pr::V;
+    SetupIn<V> in;
+    in.u = k.kind == 1 ? k.u : nullptr;
+    in.v = k.kind == 1 ? k.v : nullptr;
+    in.w = k.kind == 1 ? k.w : nullptr;
+    in.bnat = k.kind == 1 ? nullptr : k.bnat;
+    in.P = std::is_same<V, double>::value ? (V*)c->Pd : (V*)k.P;
+    in.types = k.types;
+    in.phi = k.phi;
+    in.dx = c->grid.dx;
+    in.clear_P = k.kind == 1;
+    in.residual = 1;
+    return in;
+}
+
+// The prologue and epilogue of a solve, recorded on stream s.
+template <class Pr>
+void record_prologue(Run<Pr>& run, const Call& k, cudaGraphConditionalHandle cond, int use_cond) {
+    if (k.kind == 1) run.volume(k.phi);
+    if (std::is_same<typename Pr::V, double>::value) run.widen(k.P);
+    run.setup(setup_in<Pr>(run.c, k), cond, use_cond);
+}
+
+template <class Pr>
+void record_epilogue(Run<Pr>& run, const Call& k) {
+    using V = typename Pr::V;
+    mpp_ctx* c = run.c;
+    V* P = std::is_same<V, double>::value ? (V*)c->Pd : (V*)k.P;
+    run.true_residual(P);
+    if (std::is_same<V, double>::value) run.narrow(k.P);
+    if (k.kind == 1) run.gradient(k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.types, k.phi);
+}
+
+template <class Pr>
+int build_graph(mpp_ctx* c, const Call& k) {
+    using V = typename Pr::V;
+    cudaStream_t s = c->cap;
+    if (c->gexec) {
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+    }
+    if (c->graph) {
+        cudaGraphDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    c->graph = g;
+    cudaGraphConditionalHandle cond;
+    CK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+    Run<Pr> pro{c, s};
+    CK(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    record_prologue<Pr>(pro, k, cond, 1);
+    CK(cudaStreamEndCapture(s, &g));
+    std::vector<cudaGraphNode_t> leaves;
+    if (int e = graph_leaves(g, leaves)) return e;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CK(cudaGraphAddNode(&cnode, g, leaves.data(), leaves.size(), &cp));
+    cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+    Run<Pr> bod{c, s};
+    CK(cudaStreamBeginCaptureToGraph(s, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    V* P = std::is_same<V, double>::value ? (V*)c->Pd : (V*)k.P;
+    bod.body(P, cond, 1);
+    CK(cudaStreamEndCapture(s, &bodyg));
+    Run<Pr> epi{c, s};
+    CK(cudaStreamBeginCaptureToGraph(s, g, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
+    record_epilogue<Pr>(epi, k);
+    CK(cudaStreamEndCapture(s, &g));
+    CK(cudaGraphInstantiate(&c->gexec, g, 0));
+    c->g_prologue = pro.nk;
+    c->g_body = bod.nk;
+    c->g_epilogue = epi.nk;
+    const void* key[10] = {k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.bnat, k.types, k.phi};
+    memcpy(c->gkey, key, sizeof(key));
+    c->gkind = k.kind;
+    return MPP_OK;
+}
+
+template <class Pr>
+int solve(mpp_ctx* c, const Call& k, cudaStream_t s) {
+    using V = typename Pr::V;
+    int64_t launched = 0;
+    if (c->opts.graph && !c->prof_on) {
+        const void* key[10] = {k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.bnat, k.types, k.phi};
+        if (!c->gexec || c->gkind != k.kind || memcmp(key, c->gkey, sizeof(key)) != 0) {
+            if (int e = build_graph<Pr>(c, k)) return e;
+        }
+        CK(cudaGraphLaunch(c->gexec, s));
+        if (int e = read_state(c, s)) return e;
+        launched = c->g_prologue + (int64_t)c->g_body * c->sc_host->s.it + c->g_epilogue;
+    } else {
+        Run<Pr> run{c, s};
+        record_prologue<Pr>(run, k, 0, 0);
+        if (int e = read_state(c, s)) return e;
+        V* P = std::is_same<V, double>::value ? (V*)c->Pd : (V*)k.P;
+        while (!c->sc_host->s.done) {
+            run.body(P, 0, 0);
+            if (int e = read_state(c, s)) return e;
+        }
+        record_epilogue<Pr>(run, k);
+        if (int e = read_state(c, s)) return e;
+        launched = run.nk;
+        prof_collect(c);
+    }
+    CK(cudaGetLastError());
+    c->launches += launched;
+    return MPP_OK;
+}
+
+template <class F>
+int dispatch(int prec, F&& f) {
+    switch (prec) {
+        case MPP_PREC_FP32: return f(PrecFP32{});
+        case MPP_PREC_MIXED_FP16: return f(PrecFP16{});
+        case MPP_PREC_MIXED_BF16: return f(PrecBF16{});
+        case MPP_PREC_FP64: return f(PrecFP64{});
+    }
+    set_err("unknown precision %d", prec);
+    return MPP_ERR_INVALID;
+}
+
+void fill_result(mpp_ctx* c, mpp_result* res, int64_t launches) {
+    if (!res) return;
+    const State& S = c->sc_host->s;
+    memset(res, 0, sizeof(*res));
+    res->iterations = S.it;
+    res->status = S.status;
+    res->bnorm = S.bnorm;
+    res->rel_residual = S.bnorm > 0 ? S.rnorm / S.bnorm : 0.0;
+    res->true_rel_residual = S.bnorm > 0 ? sqrt(S.true_rr) / S.bnorm : 0.0;
+    res->volume = S.vol;
+    res->gamma = S.gamma;
+    res->kernel_launches = launches;
+}
+
+int check_ctx(mpp_ctx* c) {
+    if (!c) {
+        set_err("null context");
+        return MPP_ERR_INVALID;
+    }
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev != c->dev) {
+        set_err("context belongs to device %d, current device is %d", c->dev, dev);
+        return MPP_ERR_INVALID;
+    }
+    return MPP_OK;
+}
+
+// Operator-only set-up shared by the single-pass entry points.
+template <class Pr>
+int operator_setup(mpp_ctx* c, Run<Pr>& run, const uint8_t* types, const float* phi, const float* u,
+                   const float* v, const float* w, float gamma) {
+    SetupIn<typename Pr::V> in;
+    memset(&in, 0, sizeof(in));
+    in.u = u;
+    in.v = v;
+    in.w = w;
+    in.types = types;
+    in.phi = phi;
+    in.dx = c->grid.dx;
+    in.clear_P = 0;
+    in.residual = 0;
+    if (int e = write_params(c, 1.f, 1.0, 1.0, 0, gamma, run.s)) return e;
+    run.setup(in, 0, 0);
+    return MPP_OK;
+}
+
+Lev<float> fine_layout(mpp_ctx* c) { return view<float>(c, 0); }
+
+}  // namespace
+
+// ======================================================================= C ABI
+
+extern "C" {
+
+void mpp_opts_default(mpp_opts* o) {
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->tol = 1e-4f;
+    o->maxiter = 60;
+    o->sweeps = 2;
+    o->coarse = 40;
+    o->precision = MPP_PREC_FP32;
+    o->graph = 0;
+    o->fallback = 0;
+    o->restart = 8;
+    o->fallback_maxiter = 240;
+    o->cg_maxiter_with_fallback = 80;
+}
+
+int32_t mpp_levels_for(const int32_t n[3]) {
+    if (!n || n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return -1;
+    for (int levels = 2; levels < MAXLEV; levels++) {
+        const int m = 1 << (levels - 1);
+        if (n[0] % m || n[1] % m || n[2] % m) return -1;
+        if ((int64_t)(n[0] / m) * (n[1] / m) * (n[2] / m) <= 1024) return levels;
+    }
+    return -1;
+}
+
+const char* mpp_last_error(void) { return g_err; }
+const char* mpp_version(void) { return "libmpp 0.1 (sm_100a)"; }
+
+int mpp_ctx_destroy(mpp_ctx* c) {
+    if (!c) return MPP_OK;
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    for (void* p : c->allocs) cudaFree(p);
+    if (c->sc_host) cudaFreeHost(c->sc_host);
+    if (c->cap) cudaStreamDestroy(c->cap);
+    for (cudaEvent_t e : c->evall) cudaEventDestroy(e);
+    delete c;
+    return MPP_OK;
+}
+
+static int validate(const mpp_grid* g, const mpp_opts* o) {
+    if (!g || !o) {
+        set_err("null grid or options");
+        return MPP_ERR_INVALID;
+    }
+    if (g->levels < 2 || g->levels >= MAXLEV) {
+        set_err("levels must be in [2, %d), got %d", MAXLEV, g->levels);
+        return MPP_ERR_INVALID;
+    }
+    const int m = 1 << (g->levels - 1);
+    for (int a = 0; a < 3; a++)
+        if (g->n[a] <= 0 || g->n[a] % m) {
+            set_err("grid side %d = %d is not a positive multiple of 2^(levels-1) = %d", a, g->n[a], m);
+            return MPP_ERR_INVALID;
+        }
+    if ((int64_t)(g->n[0] / m) * (g->n[1] / m) * (g->n[2] / m) > 1024) {
+        set_err("the coarsest level has more than 1024 cells; use more levels");
+        return MPP_ERR_INVALID;
+    }
+    if (!(g->dx > 0.f)) {
+        set_err("dx must be positive");
+        return MPP_ERR_INVALID;
+    }
+    if (o->sweeps < 1 || o->sweeps > 16 || o->coarse < 0 || o->maxiter < 0 || !(o->tol >= 0.f)) {
+        set_err("bad solver options");
+        return MPP_ERR_INVALID;
+    }
+    if (o->precision < 0 || o->precision > 3) {
+        set_err("unknown precision %d", o->precision);
+        return MPP_ERR_INVALID;
+    }
+    return MPP_OK;
+}
+
+int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
+    if (!out) {
+        set_err("null output");
+        return MPP_ERR_INVALID;
+    }
+    *out = nullptr;
+    if (int e = validate(g, o)) return e;
+    mpp_ctx* c = new mpp_ctx();
+    memset(c->lv, 0, sizeof(c->lv));
+    c->grid = *g;
+    c->opts = *o;
+    c->prec = o->precision;
+    c->L = g->levels;
+    c->diag = c->bvec = c->r = c->d = c->q = c->Pd = nullptr;
+    c->gexec = nullptr;
+    c->graph = nullptr;
+    c->bytes = 0;
+    c->launches = 0;
+    c->sc_host = nullptr;
+    c->cap = nullptr;
+    c->prof_on = 0;
+    memset(c->prof, 0, sizeof(c->prof));
+    memset(c->active, 0, sizeof(c->active));
+    auto fail = [&](int e) {
+        mpp_ctx_destroy(c);
+        return e;
+    };
+    cudaError_t ce = cudaGetDevice(&c->dev);
+    if (ce != cudaSuccess) {
+        set_err("cudaGetDevice: %s", cudaGetErrorString(ce));
+        return fail(MPP_ERR_CUDA);
+    }
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
+    const size_t vs = vsize(c->prec), ms = msize(c->prec);
+    const bool alias = vs == ms;  // FP32 and FP64: the V-cycle's fine arrays alias the CG's
+    const int64_t N = (int64_t)g->n[0] * g->n[1] * g->n[2];
+    int e;
+    // level geometry
+    size_t tflag_total = 0;
+    for (int l = 0; l < c->L; l++) {
+        LevelBuf& b = c->lv[l];
+        for (int a = 0; a < 3; a++) b.n[a] = g->n[a] >> l;
+        b.split = l < c->L - 1;
+        if (b.split) {
+            b.H = b.n[0] / 2;
+            b.GH = (b.H + TH - 1) / TH;
+            b.GJ = (b.n[1] + TY - 1) / TY;
+            b.GK = (b.n[2] + TZ - 1) / TZ;
+            b.ntiles = b.GH * b.GJ * b.GK;
+            tflag_total += (size_t)b.ntiles;
+        }
+    }
+    c->tflag_bytes = tflag_total;
+    if ((e = alloc(c, (void**)&c->tflag_all, tflag_total))) return fail(e);
+    size_t off = 0;
+    for (int l = 0; l < c->L; l++) {
+        LevelBuf& b = c->lv[l];
+        const int64_t Nl = (int64_t)b.n[0] * b.n[1] * b.n[2];
+        if (l > 0 && (e = alloc(c, (void**)&b.types, Nl))) return fail(e);
+        if (b.split) {
+            b.tflag = c->tflag_all + off;
+            off += b.ntiles;
+            if ((e = alloc(c, (void**)&b.tiles, sizeof(uint32_t) * b.ntiles))) return fail(e);
+            if ((e = alloc(c, (void**)&b.count, sizeof(int)))) return fail(e);
+            if ((e = alloc(c, (void**)&b.code, Nl))) return fail(e);
+            if ((e = alloc(c, &b.x, ms * Nl))) return fail(e);
+            if ((e = alloc(c, &b.r, ms * Nl))) return fail(e);
+            if (l > 0 || !alias) {
+                if ((e = alloc(c, &b.dg, ms * Nl))) return fail(e);
+                if ((e = alloc(c, &b.b, ms * Nl))) return fail(e);
+            }
+        } else {
+            if ((e = alloc(c, &b.x, ms * Nl))) return fail(e);
+        }
+    }
+    if ((e = alloc(c, &c->diag, vs * N))) return fail(e);
+    if ((e = alloc(c, &c->bvec, vs * N))) return fail(e);
+    if ((e = alloc(c, &c->r, vs * N))) return fail(e);
+    if ((e = alloc(c, &c->d, vs * N))) return fail(e);
+    if ((e = alloc(c, &c->q, vs * N))) return fail(e);
+    if (alias) {
+        c->lv[0].dg = c->diag;
+        c->lv[0].b = c->r;
+    }
+    if (c->prec == MPP_PREC_FP64 && (e = alloc(c, &c->Pd, sizeof(double) * N))) return fail(e);
+    if ((e = alloc(c, (void**)&c->sc, sizeof(Scalars)))) return fail(e);
+    if ((e = alloc(c, (void**)&c->partials, sizeof(double) * MAXK * (size_t)c->nsm * MAXBLOCKS_PER_SM))) return fail(e);
+    if ((e = alloc(c, (void**)&c->counters, sizeof(unsigned) * NCOUNTERS))) return fail(e);
+    ce = cudaMallocHost((void**)&c->sc_host, sizeof(Scalars));
+    if (ce != cudaSuccess) {
+        set_err("cudaMallocHost: %s", cudaGetErrorString(ce));
+        return fail(MPP_ERR_NOMEM);
+    }
+    memset(c->sc_host, 0, sizeof(Scalars));
+    ce = cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) {
+        set_err("cudaStreamCreate: %s", cudaGetErrorString(ce));
+        return fail(MPP_ERR_CUDA);
+    }
+    *out = c;
+    return MPP_OK;
+}
+
+int mpp_ctx_set_opts(mpp_ctx* c, const mpp_opts* o) {
+    if (int e = check_ctx(c)) return e;
+    if (int e = validate(&c->grid, o)) return e;
+    if (o->precision != c->prec) {
+        set_err("precision is fixed at context creation");
+        return MPP_ERR_INVALID;
+    }
+    if (o->sweeps != c->opts.sweeps || o->coarse != c->opts.coarse || o->graph != c->opts.graph) {
+        if (c->gexec) cudaGraphExecDestroy(c->gexec);
+        if (c->graph) cudaGraphDestroy(c->graph);
+        c->gexec = nullptr;
+        c->graph = nullptr;
+    }
+    c->opts = *o;
+    return MPP_OK;
+}
+
+size_t mpp_ctx_bytes(const mpp_ctx* c) { return c ? c->bytes : 0; }
+
+int mpp_profile_enable(mpp_ctx* c, int on) {
+    if (int e = check_ctx(c)) return e;
+    c->prof_on = on ? 1 : 0;
+    if (on) memset(c->prof, 0, sizeof(c->prof));
+    return MPP_OK;
+}
+
+int mpp_profile_read(mpp_ctx* c, mpp_prof_entry* out, int max) {
+    if (int e = check_ctx(c)) return e;
+    int n = 0;
+    for (int f = 0; f < NFAM; f++)
+        for (int l = 0; l <= MAXLEV; l++) {
+            const ProfAcc& a = c->prof[f][l];
+            if (a.n == 0) continue;
+            if (out && n < max) {
+                mpp_prof_entry& e = out[n];
+                memset(&e, 0, sizeof(e));
+                snprintf(e.name, sizeof(e.name), "%s", FAM_NAMES[f]);
+                e.level = l == MAXLEV ? -1 : l;
+                e.launches = a.n;
+                e.ms = a.ms;
+                e.bytes = a.bytes;
+                e.cells = a.cells;
+            }
+            n++;
+        }
+    return n;
+}
+
+int mpp_volume(mpp_ctx* c, const float* phi, double* vol, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!phi || !vol) {
+        set_err("null argument");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (int e = write_params(c, 1.f, 1.0, 1.0, 0, 0.f, s)) return e;
+    Run<PrecFP32> run{c, s};
+    run.volume(phi);
+    if (int e = read_state(c, s)) return e;
+    CK(cudaGetLastError());
+    c->launches += run.nk;
+    *vol = c->sc_host->s.vol;
+    return MPP_OK;
+}
+
+int mpp_project(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv, uint8_t* fw, float* P,
+                const uint8_t* types, const float* phi, float volume0, double dt, double recover, mpp_result* res,
+                mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!u || !v || !w || !fu || !fv || !fw || !P || !types || !phi) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    if (!(dt > 0.0) || !(recover > 0.0) || !(volume0 != 0.f)) {
+        set_err("dt and recover must be positive and volume0 nonzero");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (int e = write_params(c, volume0, dt, recover, 1, 0.f, s)) return e;
+    Call k{1, u, v, w, fu, fv, fw, P, nullptr, types, phi};
+    const int64_t before = c->launches;
+    int e = dispatch(c->prec, [&](auto pr) { return solve<decltype(pr)>(c, k, s); });
+    if (e < 0) return e;
+    fill_result(c, res, c->launches - before);
+    return c->sc_host->s.status;
+}
+
+int mpp_pressure(mpp_ctx* c, float* P, const float* b, const uint8_t* types, const float* phi, mpp_result* res,
+                 mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!P || !b || !types || !phi) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (int e = write_params(c, 1.f, 1.0, 1.0, 0, 0.f, s)) return e;
+    Call k{0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, P, b, types, phi};
+    const int64_t before = c->launches;
+    int e = dispatch(c->prec, [&](auto pr) { return solve<decltype(pr)>(c, k, s); });
+    if (e < 0) return e;
+    fill_result(c, res, c->launches - before);
+    return c->sc_host->s.status;
+}
+
+int mpp_rhs(mpp_ctx* c, float* b, const float* u, const float* v, const float* w, const uint8_t* types, float gamma,
+            mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!b || !u || !v || !w || !types) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    // The rhs does not read phi; the set-up pass then skips the ghost-fluid terms.
+    return dispatch(c->prec, [&](auto pr) -> int {
+        using Pr = decltype(pr);
+        using V = typename Pr::V;
+        Run<Pr> run{c, s};
+        SetupIn<V> in;
+        memset(&in, 0, sizeof(in));
+        in.u = u; in.v = v; in.w = w; in.types = types; in.phi = nullptr; in.dx = c->grid.dx;
+        if (int e = write_params(c, 1.f, 1.0, 1.0, 0, gamma, s)) return e;
+        run.setup(in, 0, 0);
+        const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+        k_from_split<float, V><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), b, (const V*)c->bvec);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s));
+        c->launches += run.nk + 1;
+        return MPP_OK;
+    });
+}
+
+int mpp_diag(mpp_ctx* c, float* diag, const uint8_t* types, const float* phi, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!diag || !types || !phi) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    return dispatch(c->prec, [&](auto pr) -> int {
+        using Pr = decltype(pr);
+        using V = typename Pr::V;
+        Run<Pr> run{c, s};
+        if (int e = operator_setup<Pr>(c, run, types, phi, nullptr, nullptr, nullptr, 0.f)) return e;
+        const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+        k_from_split<float, V><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), diag, (const V*)c->diag);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s));
+        c->launches += run.nk + 1;
+        return MPP_OK;
+    });
+}
+
+int mpp_vcycle(mpp_ctx* c, float* z, const float* r, const uint8_t* types, const float* phi, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!z || !r || !types || !phi) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    return dispatch(c->prec, [&](auto pr) -> int {
+        using Pr = decltype(pr);
+        using M = typename Pr::M;
+        Run<Pr> run{c, s};
+        if (int e = operator_setup<Pr>(c, run, types, phi, nullptr, nullptr, nullptr, 0.f)) return e;
+        const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+        const size_t ms = msize(c->prec);
+        CK(cudaMemsetAsync(c->lv[0].x, 0, ms * N, s));
+        k_to_split<M, float><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), (M*)c->lv[0].b, r);
+        run.vcycle();
+        k_from_split<float, M><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), z, (const M*)c->lv[0].x);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s));
+        c->launches += run.nk + 2;
+        return MPP_OK;
+    });
+}
+
+int mpp_apply(mpp_ctx* c, float* y, const float* x, const uint8_t* types, const float* phi, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!y || !x || !types || !phi) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    return dispatch(c->prec, [&](auto pr) -> int {
+        using Pr = decltype(pr);
+        using V = typename Pr::V;
+        using M = typename Pr::M;
+        Run<Pr> run{c, s};
+        if (int e = operator_setup<Pr>(c, run, types, phi, nullptr, nullptr, nullptr, 0.f)) return e;
+        const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+        const size_t vs = vsize(c->prec);
+        CK(cudaMemsetAsync(c->q, 0, vs * N, s));
+        k_to_split<V, float><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), (V*)c->d, x);
+        k_apply<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q);
+        k_from_split<float, V><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), y, (const V*)c->q);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s));
+        c->launches += run.nk + 3;
+        return MPP_OK;
+    });
+}
+
+int mpp_gradient(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv, uint8_t* fw, const float* P,
+                 const uint8_t* types, const float* phi, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!u || !v || !w || !fu || !fv || !fw || !P || !types || !phi) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    Run<PrecFP32> run{c, s};
+    run.gradient(u, v, w, fu, fv, fw, P, types, phi);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    c->launches += run.nk;
+    return MPP_OK;
+}
+
+int mpp_solution_f64(mpp_ctx* c, double* out) {
+    if (int e = check_ctx(c)) return e;
+    if (c->prec != MPP_PREC_FP64 || !c->Pd || !out) {
+        set_err("no FP64 solution on this context");
+        return MPP_ERR_INVALID;
+    }
+    const size_t N = (size_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+    CK(cudaMemcpy(out, c->Pd, sizeof(double) * N, cudaMemcpyDeviceToHost));
+    return MPP_OK;
+}
+
+}  // extern "C"

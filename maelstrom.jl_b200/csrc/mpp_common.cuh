@@ -1,0 +1,210 @@
+// Shared device definitions of libmpp: cell classes, the internal layout, precision
+// bundles, conversions and deterministic block reductions.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+namespace mpp {
+
+// Cell classes, as the reference's SOLID/LIQUID/AIR (src/flip.jl:24-26).
+constexpr uint8_t SOLID = 0, LIQUID = 1, AIR = 2;
+
+// Per-cell stencil code (internal): bit m (m = 0..5 for +x,-x,+y,-y,+z,-z, the order of
+// `neighbour`, src/flip.jl:84-92) is set when that neighbour is LIQUID; SELF when the
+// cell itself is. A cell whose code lacks SELF is never updated and never read.
+constexpr uint8_t SELF = 1u << 6;
+
+// Tiles: 16 (h) x 4 (j) x 4 (k) slots of 2 cells each (one per colour), so a tile is a
+// 32 x 4 x 4 block of cells; 256 threads, one slot each.
+constexpr int TH = 16, TY = 4, TZ = 4, TPB = 256;
+
+// Grid-wide sums: at most MAXK values per block, at most MAXBLOCKS_PER_SM blocks per SM
+// (the partial-sum buffer holds MAXK * MAXBLOCKS_PER_SM * SMs doubles).
+constexpr int MAXK = 4, MAXBLOCKS_PER_SM = 8;
+
+// Precision bundles. V: the CG vectors and the fine operator; M: the V-cycle's storage;
+// C: stencil arithmetic; CC: the coarsest solve.
+struct PrecFP32 {
+    using V = float; using M = float; using C = float; using CC = float;
+    static constexpr bool flexible = false;  // standard PCG, beta = rho_new / rho
+    static constexpr bool f32_scalars = true;  // scalars rounded to Float32 like the reference
+    static constexpr bool scaled = false;      // coarse levels hold the reference's values
+};
+struct PrecFP16 {
+    using V = float; using M = __half; using C = float; using CC = double;
+    static constexpr bool flexible = true;  // Polak-Ribiere flexible PCG
+    static constexpr bool f32_scalars = false;
+    // 16-bit storage: level l holds 4^-l times the reference's b and x (restriction
+    // without its factor 4, prolongation with it; exact power-of-two scalings), and the
+    // fine residual handed to the V-cycle is scaled by a power of two, so values stay
+    // in FP16's range as the residual falls. CG is invariant to both.
+    static constexpr bool scaled = true;
+};
+struct PrecBF16 {
+    using V = float; using M = __nv_bfloat16; using C = float; using CC = double;
+    static constexpr bool flexible = true;
+    static constexpr bool f32_scalars = false;
+    static constexpr bool scaled = true;
+};
+struct PrecFP64 {
+    using V = double; using M = double; using C = double; using CC = double;
+    static constexpr bool flexible = false;
+    static constexpr bool f32_scalars = false;
+    static constexpr bool scaled = false;
+};
+
+template <class C, class T>
+__device__ __forceinline__ C ld(const T* p) {
+    if constexpr (std::is_same<T, __half>::value) return (C)__half2float(*p);
+    else if constexpr (std::is_same<T, __nv_bfloat16>::value) return (C)__bfloat162float(*p);
+    else return (C)(*p);
+}
+template <class T, class C>
+__device__ __forceinline__ void st(T* p, C v) {
+    if constexpr (std::is_same<T, __half>::value) *p = __float2half_rn((float)v);
+    else if constexpr (std::is_same<T, __nv_bfloat16>::value) *p = __float2bfloat16_rn((float)v);
+    else *p = (T)v;
+}
+
+// theta (src/flip.jl:113): the free surface's fraction of the way from a liquid cell
+// centre to an air one, clamp(phi_i / (phi_i - phi_j), 0.01, 1) in Julia's clamp order.
+template <class C>
+__device__ __forceinline__ C theta(C pi, C pj) {
+    C t = pi / (pi - pj);
+    return t > (C)1 ? (C)1 : (t < (C)0.01f ? (C)0.01f : t);
+}
+
+// One multigrid level as the kernels see it. Levels other than the coarsest are stored
+// row-split: each x-row of n1 cells holds its colour-0 cells (in i order) and then its
+// colour-1 cells, so cell (i,j,k) sits at row(j,k) + colour*H + i/2 with
+// colour = (i+j+k+1) & 1 (the reference's 1-based (i+j+k) % 2) and H = n1/2. A
+// red-black half-sweep then reads and writes only contiguous runs of its own colour.
+// The coarsest level is stored in natural order (i + n1*(j + n2*k)).
+template <class M>
+struct Lev {
+    int n1, n2, n3, H;
+    int GH, GJ, GK;  // tile grid
+    uint8_t* code;   // split
+    M* dg;           // diagonal used by the smoother (split)
+    M* x;            // correction
+    M* b;            // right-hand side
+    M* r;            // residual
+    uint8_t* types;  // natural order (coarse levels)
+    uint8_t* tflag;  // per-tile "has liquid" flags
+    uint32_t* tiles; // active tile list
+    int* count;      // its length (device)
+
+    __device__ __forceinline__ int64_t row(int j, int k) const { return ((int64_t)k * n2 + j) * n1; }
+    __device__ __forceinline__ int64_t pos(int i, int j, int k) const {
+        return row(j, k) + (int64_t)(((i + j + k + 1) & 1) * H + (i >> 1));
+    }
+    __device__ __forceinline__ int64_t nat(int i, int j, int k) const {
+        return (int64_t)i + (int64_t)n1 * ((int64_t)j + (int64_t)n2 * k);
+    }
+    __device__ __forceinline__ int tile_of(int i, int j, int k) const {
+        return (i >> 1) / TH + GH * (j / TY + GJ * (k / TZ));
+    }
+};
+
+// A thread's slot in a tile: column h (both colours), row j, plane k.
+struct Slot {
+    int h, j, k;
+    bool in;
+};
+template <class M>
+__device__ __forceinline__ Slot slot_of(const Lev<M>& L, uint32_t tile) {
+    int th = (int)(tile % (uint32_t)L.GH);
+    int tj = (int)((tile / (uint32_t)L.GH) % (uint32_t)L.GJ);
+    int tk = (int)(tile / ((uint32_t)L.GH * (uint32_t)L.GJ));
+    Slot s;
+    s.h = th * TH + (threadIdx.x & 15);
+    s.j = tj * TY + ((threadIdx.x >> 4) & 3);
+    s.k = tk * TZ + (threadIdx.x >> 6);
+    s.in = s.h < L.H && s.j < L.n2 && s.k < L.n3;
+    return s;
+}
+
+// Cell i of colour c in slot (h, j, k).
+__device__ __forceinline__ int cell_i(int h, int c, int j, int k) { return 2 * h + ((c + j + k + 1) & 1); }
+
+// Sum of x over the LIQUID neighbours of a row-split cell, in the reference's order
+// (liquidsum, src/flip.jl:852-857: s = 0, then +x,-x,+y,-y,+z,-z). `o` is the start of
+// the other colour's half of the cell's row; sy/sz the row and plane strides.
+template <class C, class T>
+__device__ __forceinline__ C nbsum(const T* __restrict__ x, uint8_t code, int64_t o, int i, int h, int64_t sy,
+                                   int64_t sz) {
+    C s = (C)0;
+    if (code & 1) s += ld<C>(x + o + ((i + 1) >> 1));
+    if (code & 2) s += ld<C>(x + o + ((i - 1) >> 1));
+    if (code & 4) s += ld<C>(x + o + sy + h);
+    if (code & 8) s += ld<C>(x + o - sy + h);
+    if (code & 16) s += ld<C>(x + o + sz + h);
+    if (code & 32) s += ld<C>(x + o - sz + h);
+    return s;
+}
+
+// ---- deterministic reductions ----
+// Block sums of K doubles (256 threads); the result is valid in thread 0.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K]) {
+    __shared__ double ws[K][TPB / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+        double a = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if (lane == 0) ws[q][w] = a;
+    }
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+            double a = lane < TPB / 32 ? ws[q][lane] : 0.0;
+#pragma unroll
+            for (int o = 4; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+            v[q] = a;
+        }
+    }
+    __syncthreads();
+}
+
+// Each block stores its K partial sums; the last block to finish adds all partials in
+// block order (fixed, so the result does not depend on scheduling), resets the counter
+// and returns true with the totals in thread 0's v.
+template <int K>
+__device__ __forceinline__ bool grid_sum(double (&v)[K], double* partials, unsigned* counter) {
+    static_assert(K <= MAXK, "partial-sum buffer holds MAXK values per block");
+    block_sum<K>(v);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < K; q++) partials[(size_t)blockIdx.x * K + q] = v[q];
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double s[K];
+#pragma unroll
+    for (int q = 0; q < K; q++) s[q] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < K; q++) s[q] += __ldcg(partials + (size_t)b * K + q);
+    }
+    block_sum<K>(s);
+    if (threadIdx.x == 0) {
+        *counter = 0u;
+#pragma unroll
+        for (int q = 0; q < K; q++) v[q] = s[q];
+    }
+    return true;
+}
+
+}  // namespace mpp

@@ -1,0 +1,281 @@
+"""Maelstrom's dense-MAC pressure projection on B200: the host side of libmpp.
+
+This mirrors the reference's interface for the path (src/flip.jl:809-1156):
+
+* :class:`FlipBasin` holds the arrays ``project!`` reads and writes, as CUDA tensors
+  with the reference's shapes and bytes (column-major, i fastest, flattened);
+* :func:`project` is ``project!(s, dt; recover, sweeps)`` and :func:`pressure` is
+  ``pressure!(s; tol, maxiter, sweeps)``: same argument meaning, same return value
+  (``pressure`` returns the iteration count and ``project`` pushes it to
+  ``s.iterations``), same error behaviour (a non-converged solve warns
+  "pressure solve did not converge"; a nonfinite or indefinite one raises with the
+  reference's message prefixes);
+* :class:`Projector` is the context the work runs in (libmpp's ``mpp_ctx``).
+
+All compute runs in libmpp.so's CUDA kernels; this module only passes device
+pointers. It raises if the library is not built or no GPU is present.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import warnings
+
+import numpy as np
+
+from . import _lib
+from ._lib import MppError, Result, check
+from . import scene
+
+__all__ = ["Projector", "FlipBasin", "project", "pressure", "MppError", "scene", "load"]
+
+
+def load():
+    return _lib.load()
+
+
+def _ptr(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _require(t, dtype, n, name):
+    import torch
+
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous() or t.numel() != n:
+        raise ValueError(f"{name} must be contiguous with {n} elements, got {t.numel()}")
+
+
+def _stream_ptr(stream):
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def grid_struct(g) -> _lib.Grid:
+    return _lib.Grid((ctypes.c_float * 3)(*g.lo), g.dx, (ctypes.c_int32 * 3)(*g.n), g.radius, g.floor, g.levels)
+
+
+class Projector:
+    """One basin's solver context (``mpp_ctx``): workspace, levels and CUDA graph.
+
+    ``precision`` is "fp32" (the reference's arithmetic), "fp16"/"mixed" or "bf16"
+    (V-cycle stored in 16 bits, flexible CG, FP64 reductions and coarsest solve) or
+    "fp64" (the FP64 oracle on the GPU). ``graph=True`` runs each call as one CUDA
+    graph launch whose CG loop is a device-side WHILE node.
+    """
+
+    def __init__(self, grid, *, tol=1e-4, maxiter=60, sweeps=2, coarse=40, precision="fp32", graph=False,
+                 fallback=False, restart=8, fallback_maxiter=240, cg_maxiter_with_fallback=80):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("libmpp needs a CUDA device")
+        self.lib = _lib.load()
+        self.grid = grid
+        self.opts = _lib.Opts()
+        self.lib.mpp_opts_default(ctypes.byref(self.opts))
+        self.set(tol=tol, maxiter=maxiter, sweeps=sweeps, coarse=coarse, graph=graph, fallback=fallback,
+                 restart=restart, fallback_maxiter=fallback_maxiter,
+                 cg_maxiter_with_fallback=cg_maxiter_with_fallback, _apply=False)
+        self.opts.precision = _lib.PREC[precision]
+        self.precision = precision
+        self._g = grid_struct(grid)
+        self._ctx = ctypes.c_void_p()
+        check(self.lib.mpp_ctx_create(ctypes.byref(self._ctx), ctypes.byref(self._g), ctypes.byref(self.opts)))
+
+    def set(self, _apply=True, **kw):
+        for k, v in kw.items():
+            setattr(self.opts, k, int(v) if k != "tol" else float(v))
+        if _apply:
+            check(self.lib.mpp_ctx_set_opts(self._ctx, ctypes.byref(self.opts)))
+
+    def close(self):
+        if getattr(self, "_ctx", None) and self._ctx.value:
+            self.lib.mpp_ctx_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nbytes(self) -> int:
+        return int(self.lib.mpp_ctx_bytes(self._ctx))
+
+    # ---- whole operations ----
+    def project(self, u, v, w, fu, fv, fw, P, types, phi, volume0, dt, recover=0.5, stream=None) -> Result:
+        import torch
+
+        g = self.grid
+        N = g.ncells
+        for t, name, axis in ((u, "u", 0), (v, "v", 1), (w, "w", 2)):
+            _require(t, torch.float32, int(np.prod(g.face_shape(axis))), name)
+        for t, name, axis in ((fu, "fu", 0), (fv, "fv", 1), (fw, "fw", 2)):
+            _require(t, torch.uint8, int(np.prod(g.face_shape(axis))), name)
+        _require(P, torch.float32, N, "P")
+        _require(types, torch.uint8, N, "types")
+        _require(phi, torch.float32, N, "phi")
+        res = Result()
+        check(self.lib.mpp_project(self._ctx, _ptr(u), _ptr(v), _ptr(w), _ptr(fu), _ptr(fv), _ptr(fw), _ptr(P),
+                                   _ptr(types), _ptr(phi), float(volume0), float(dt), float(recover),
+                                   ctypes.byref(res), _stream_ptr(stream)))
+        return res
+
+    def pressure(self, P, b, types, phi, stream=None) -> Result:
+        import torch
+
+        N = self.grid.ncells
+        _require(P, torch.float32, N, "P")
+        _require(b, torch.float32, N, "b")
+        _require(types, torch.uint8, N, "types")
+        _require(phi, torch.float32, N, "phi")
+        res = Result()
+        check(self.lib.mpp_pressure(self._ctx, _ptr(P), _ptr(b), _ptr(types), _ptr(phi), ctypes.byref(res),
+                                    _stream_ptr(stream)))
+        return res
+
+    def volume(self, phi, stream=None) -> float:
+        import torch
+
+        _require(phi, torch.float32, self.grid.ncells, "phi")
+        out = ctypes.c_double()
+        check(self.lib.mpp_volume(self._ctx, _ptr(phi), ctypes.byref(out), _stream_ptr(stream)))
+        return out.value
+
+    # ---- single passes ----
+    def rhs(self, u, v, w, types, gamma=0.0, stream=None):
+        import torch
+
+        b = torch.empty(self.grid.ncells, dtype=torch.float32, device=u.device)
+        check(self.lib.mpp_rhs(self._ctx, _ptr(b), _ptr(u), _ptr(v), _ptr(w), _ptr(types), float(gamma),
+                               _stream_ptr(stream)))
+        return b
+
+    def diag(self, types, phi, stream=None):
+        import torch
+
+        d = torch.empty(self.grid.ncells, dtype=torch.float32, device=types.device)
+        check(self.lib.mpp_diag(self._ctx, _ptr(d), _ptr(types), _ptr(phi), _stream_ptr(stream)))
+        return d
+
+    def vcycle(self, r, types, phi, stream=None):
+        import torch
+
+        z = torch.empty(self.grid.ncells, dtype=torch.float32, device=r.device)
+        check(self.lib.mpp_vcycle(self._ctx, _ptr(z), _ptr(r), _ptr(types), _ptr(phi), _stream_ptr(stream)))
+        return z
+
+    def apply(self, x, types, phi, stream=None):
+        import torch
+
+        y = torch.empty(self.grid.ncells, dtype=torch.float32, device=x.device)
+        check(self.lib.mpp_apply(self._ctx, _ptr(y), _ptr(x), _ptr(types), _ptr(phi), _stream_ptr(stream)))
+        return y
+
+    def gradient(self, u, v, w, fu, fv, fw, P, types, phi, stream=None):
+        check(self.lib.mpp_gradient(self._ctx, _ptr(u), _ptr(v), _ptr(w), _ptr(fu), _ptr(fv), _ptr(fw), _ptr(P),
+                                    _ptr(types), _ptr(phi), _stream_ptr(stream)))
+
+    # ---- per-kernel timing ----
+    def profile(self, on: bool = True):
+        """Bracket every kernel with CUDA events (solves then run their loop from the host)."""
+        check(self.lib.mpp_profile_enable(self._ctx, 1 if on else 0))
+
+    def profile_read(self) -> list:
+        """[{name, level, launches, ms, bytes, cells}] summed since profiling was turned on."""
+        n = check(self.lib.mpp_profile_read(self._ctx, None, 0))
+        arr = (_lib.ProfEntry * max(n, 1))()
+        check(self.lib.mpp_profile_read(self._ctx, ctypes.cast(arr, ctypes.c_void_p), n))
+        out = []
+        for e in arr[:n]:
+            out.append(dict(name=e.name.decode(), level=e.level, launches=e.launches, ms=e.ms, bytes=e.bytes,
+                            cells=e.cells))
+        return out
+
+    def solution_f64(self) -> np.ndarray:
+        out = np.empty(self.grid.ncells, dtype=np.float64)
+        check(self.lib.mpp_solution_f64(self._ctx, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+
+@dataclasses.dataclass
+class FlipBasin:
+    """The part of the reference's ``FlipBasin`` (src/flip.jl:161-224) the projection
+    touches, on the GPU: face velocities and valid flags, pressure (kept as the next
+    solve's warm start), cell classes, level set, the start volume and the iteration
+    log."""
+
+    grid: object
+    u: object
+    v: object
+    w: object
+    fu: object
+    fv: object
+    fw: object
+    P: object
+    types: object
+    phi: object
+    volume0: float
+    iterations: list
+    projector: Projector | None = None
+
+    @classmethod
+    def from_scene(cls, basin: "scene.Basin", device="cuda", **projector_kw) -> "FlipBasin":
+        import torch
+
+        dev = torch.device(device)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        g = basin.grid
+        s = cls(grid=g, u=t(basin.u), v=t(basin.v), w=t(basin.w),
+                fu=torch.zeros(basin.u.size, dtype=torch.uint8, device=dev),
+                fv=torch.zeros(basin.v.size, dtype=torch.uint8, device=dev),
+                fw=torch.zeros(basin.w.size, dtype=torch.uint8, device=dev),
+                P=torch.zeros(g.ncells, dtype=torch.float32, device=dev), types=t(basin.types), phi=t(basin.phi),
+                volume0=0.0, iterations=[])
+        s.projector = Projector(g, **projector_kw)
+        s.volume0 = s.projector.volume(s.phi)  # initialize!: s.volume0 = volume(s) (src/flip.jl:346)
+        return s
+
+
+def _raise_or_warn(res: Result, bnorm_ok=True):
+    if res.status == _lib.NOT_CONVERGED:
+        warnings.warn(f"pressure solve did not converge: residual = {res.rel_residual:.3e}, "
+                      f"iterations = {res.iterations}", RuntimeWarning, stacklevel=3)
+    elif res.status == _lib.NONFINITE:
+        raise RuntimeError("Nonfinite pressure residual")
+    elif res.status == _lib.INDEFINITE:
+        raise RuntimeError("Pressure CG requires a positive operator and preconditioner")
+    elif res.status == _lib.BREAKDOWN:
+        raise RuntimeError("Pressure Arnoldi breakdown")
+
+
+def project(s: FlipBasin, dt, recover=0.5, sweeps=None) -> FlipBasin:
+    """``project!(s, dt; recover = 0.5, sweeps = 2)`` (src/flip.jl:1144-1156)."""
+    p = s.projector
+    if sweeps is not None and sweeps != p.opts.sweeps:
+        p.set(sweeps=sweeps)
+    res = p.project(s.u, s.v, s.w, s.fu, s.fv, s.fw, s.P, s.types, s.phi, s.volume0, dt, recover)
+    s.iterations.append(res.iterations)
+    s.last = res
+    _raise_or_warn(res)
+    return s
+
+
+def pressure(s: FlipBasin, b, tol=None, maxiter=None, sweeps=None) -> int:
+    """``pressure!(s; tol = 1e-4, maxiter = 60, sweeps = 2) -> iterations``
+    (src/flip.jl:1082-1111), for the right-hand side ``b``."""
+    p = s.projector
+    kw = {k: v for k, v in (("tol", tol), ("maxiter", maxiter), ("sweeps", sweeps)) if v is not None}
+    if kw:
+        p.set(**kw)
+    res = p.pressure(s.P, b, s.types, s.phi)
+    s.last = res
+    _raise_or_warn(res)
+    return res.iterations

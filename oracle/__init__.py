@@ -1,0 +1,178 @@
+"""ctypes front of the CPU oracle (oracle.c). TEST INFRASTRUCTURE ONLY.
+
+Only the tests, the smoke check and the benchmark's CPU-baseline leg import this
+module; it is the checker, never the product. It restates src/flip.jl:809-1156 of
+the reference on the CPU (see oracle.h); parity with the reference itself is
+unpinned because the reference (Julia on Vulkan) cannot run here.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_float * 3), ("dx", ctypes.c_float), ("n", ctypes.c_int32 * 3),
+                ("radius", ctypes.c_float), ("floor_z", ctypes.c_float), ("levels", ctypes.c_int32)]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("converged", ctypes.c_int32), ("rnorm", ctypes.c_double),
+                ("bnorm", ctypes.c_double), ("volume", ctypes.c_double), ("gamma", ctypes.c_float)]
+
+
+def build() -> str:
+    """Compile liboracle.so with its Makefile (gcc + OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.c_void_p
+        G = ctypes.POINTER(Grid)
+        I = ctypes.POINTER(Info)
+        f, d, i32 = ctypes.c_float, ctypes.c_double, ctypes.c_int
+        sig = {
+            "orc_volume_f32": (d, [G, P]), "orc_volume_f64": (d, [G, P]),
+            "orc_rhs_f32": (None, [G, P, P, P, P, P, f]), "orc_rhs_f64": (None, [G, P, P, P, P, P, d]),
+            "orc_diag_f32": (None, [G, P, P, P]), "orc_diag_f64": (None, [G, P, P, P]),
+            "orc_coarsen": (None, [P, P, P]),
+            "orc_vcycle_f32": (None, [G, P, P, P, P, i32, i32]),
+            "orc_vcycle_f64": (None, [G, P, P, P, P, i32, i32]),
+            "orc_apply_f32": (None, [G, P, P, P, P]), "orc_apply_f64": (None, [G, P, P, P, P]),
+            "orc_gradient_f32": (None, [G, P, P, P, P, P, P, P, P, P]),
+            "orc_gradient_f64": (None, [G, P, P, P, P, P, P, P, P, P]),
+            "orc_pressure_f32": (i32, [G, P, P, P, P, f, i32, i32, i32, I]),
+            "orc_pressure_f64": (i32, [G, P, P, P, P, d, i32, i32, i32, I]),
+            "orc_project_f32": (i32, [G, P, P, P, P, P, P, P, P, P, f, d, d, f, i32, i32, i32, I]),
+            "orc_project_f64": (i32, [G, P, P, P, P, P, P, P, P, P, d, d, d, d, i32, i32, i32, I]),
+            "orc_num_threads": (i32, []), "orc_set_num_threads": (None, [i32]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(_lib, name)
+            fn.restype = res
+            fn.argtypes = args
+    return _lib
+
+
+def _grid(g) -> Grid:
+    return Grid((ctypes.c_float * 3)(*g.lo), g.dx, (ctypes.c_int32 * 3)(*g.n), g.radius, g.floor, g.levels)
+
+
+def _p(a: np.ndarray):
+    assert a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _ft(prec):
+    return np.float32 if prec == 32 else np.float64
+
+
+def volume(grid, phi, prec=32) -> float:
+    phi = np.ascontiguousarray(phi, dtype=_ft(prec))
+    return \
+        getattr(lib(), f"orc_volume_f{prec}")(ctypes.byref(_grid(grid)), _p(phi))
+
+
+def rhs(grid, u, v, w, types, gamma, prec=32):
+    t = _ft(prec)
+    b = np.zeros(grid.ncells, dtype=t)
+    u, v, w = (np.ascontiguousarray(a, dtype=t) for a in (u, v, w))
+    getattr(lib(), f"orc_rhs_f{prec}")(ctypes.byref(_grid(grid)), _p(b), _p(u), _p(v), _p(w),
+                                       _p(np.ascontiguousarray(types, dtype=np.uint8)), gamma)
+    return b
+
+
+def diag(grid, types, phi, prec=32):
+    t = _ft(prec)
+    d = np.zeros(grid.ncells, dtype=t)
+    getattr(lib(), f"orc_diag_f{prec}")(ctypes.byref(_grid(grid)), _p(d),
+                                        _p(np.ascontiguousarray(types, dtype=np.uint8)),
+                                        _p(np.ascontiguousarray(phi, dtype=t)))
+    return d
+
+
+def coarsen(nf, tf):
+    nf = (ctypes.c_int32 * 3)(*nf)
+    tc = np.zeros(len(tf) // 8, dtype=np.uint8)
+    lib().orc_coarsen(nf, _p(tc), _p(np.ascontiguousarray(tf, dtype=np.uint8)))
+    return tc
+
+
+def vcycle(grid, r, types, diag_, sweeps=2, coarse=40, prec=32):
+    t = _ft(prec)
+    z = np.zeros(grid.ncells, dtype=t)
+    getattr(lib(), f"orc_vcycle_f{prec}")(ctypes.byref(_grid(grid)), _p(z), _p(np.ascontiguousarray(r, dtype=t)),
+                                          _p(np.ascontiguousarray(types, dtype=np.uint8)),
+                                          _p(np.ascontiguousarray(diag_, dtype=t)), sweeps, coarse)
+    return z
+
+
+def apply(grid, x, types, diag_, prec=32):
+    t = _ft(prec)
+    y = np.zeros(grid.ncells, dtype=t)
+    getattr(lib(), f"orc_apply_f{prec}")(ctypes.byref(_grid(grid)), _p(y), _p(np.ascontiguousarray(x, dtype=t)),
+                                         _p(np.ascontiguousarray(types, dtype=np.uint8)),
+                                         _p(np.ascontiguousarray(diag_, dtype=t)))
+    return y
+
+
+def pressure(grid, P, b, types, phi, tol=1e-4, maxiter=60, sweeps=2, coarse=40, prec=32):
+    """pressure! on copies: returns (P, info)."""
+    t = _ft(prec)
+    P = np.array(P, dtype=t, copy=True)
+    info = Info()
+    getattr(lib(), f"orc_pressure_f{prec}")(ctypes.byref(_grid(grid)), _p(P), _p(np.ascontiguousarray(b, dtype=t)),
+                                            _p(np.ascontiguousarray(types, dtype=np.uint8)),
+                                            _p(np.ascontiguousarray(phi, dtype=t)), tol, maxiter, sweeps, coarse,
+                                            ctypes.byref(info))
+    return P, info
+
+
+def gradient(grid, u, v, w, P, types, phi, prec=32):
+    t = _ft(prec)
+    u, v, w = (np.array(a, dtype=t, copy=True) for a in (u, v, w))
+    fu, fv, fw = (np.zeros(a.size, dtype=np.uint8) for a in (u, v, w))
+    getattr(lib(), f"orc_gradient_f{prec}")(ctypes.byref(_grid(grid)), _p(u), _p(v), _p(w), _p(fu), _p(fv), _p(fw),
+                                            _p(np.ascontiguousarray(P, dtype=t)),
+                                            _p(np.ascontiguousarray(types, dtype=np.uint8)),
+                                            _p(np.ascontiguousarray(phi, dtype=t)))
+    return u, v, w, fu, fv, fw
+
+
+def project(basin, P=None, *, volume0=None, dt=1.0 / 48, recover=0.5, tol=1e-4, maxiter=60, sweeps=2, coarse=40,
+            prec=32):
+    """project! on copies of a scene.Basin: returns dict(u, v, w, fu, fv, fw, P, info)."""
+    g = basin.grid
+    t = _ft(prec)
+    u, v, w = (np.array(a, dtype=t, copy=True) for a in (basin.u, basin.v, basin.w))
+    fu, fv, fw = (np.zeros(a.size, dtype=np.uint8) for a in (u, v, w))
+    P = np.zeros(g.ncells, dtype=t) if P is None else np.array(P, dtype=t, copy=True)
+    phi = np.ascontiguousarray(basin.phi, dtype=t)
+    if volume0 is None:
+        volume0 = volume(g, basin.phi)
+    info = Info()
+    getattr(lib(), f"orc_project_f{prec}")(ctypes.byref(_grid(g)), _p(u), _p(v), _p(w), _p(fu), _p(fv), _p(fw),
+                                           _p(P), _p(np.ascontiguousarray(basin.types, dtype=np.uint8)), _p(phi),
+                                           volume0, dt, recover, tol, maxiter, sweeps, coarse, ctypes.byref(info))
+    return dict(u=u, v=v, w=w, fu=fu, fv=fv, fw=fw, P=P, info=info)
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def set_num_threads(n: int) -> None:
+    lib().orc_set_num_threads(n)

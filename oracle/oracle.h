@@ -1,0 +1,102 @@
+/*
+ * CPU oracle for the dense-MAC pressure projection of Maelstrom.jl's FlipBasin.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the checker: the parity tests, the
+ * smoke check and the CPU-baseline leg of the benchmark call it. Nothing in the
+ * product path (libmpp.so, the `mpp` Python package) links, loads or calls it.
+ *
+ * It is a plain C restatement of the reference's projection, src/flip.jl:809-1156
+ * (rhs, diagonal, residual, red-black Gauss-Seidel, coarsening, restriction,
+ * prolongation, the single-workgroup coarsest solve, the V-cycle, the fused CG
+ * passes, the PCG driver, the gradient update, clearair and project!), with the
+ * reductions of src/flip.jl:230-293 restated as per-group FP32 tree sums.
+ * Each function names the reference lines it follows.
+ *
+ * PARITY UNPINNED: the reference is Julia on a Vulkan device (through the
+ * un-vendored Mantle 0.1) and cannot run on this machine, and its own test suite
+ * (test/runtests.jl:48-57) holds no golden vectors for this path. The oracle is
+ * pinned instead by analytic known-answer problems (tests/test_oracle_kat.py) and by
+ * algebraic properties (operator symmetry, V-cycle symmetry, exact solves).
+ *
+ * Arrays are the reference's, byte for byte: Julia column-major with i fastest,
+ * 0-based here: cell (i,j,k) at i + nx*(j + ny*k); u is (nx+1,ny,nz), v is
+ * (nx,ny+1,nz), w is (nx,ny,nz+1); types are UInt8 SOLID=0, LIQUID=1, AIR=2.
+ *
+ * Every entry point exists twice: *_f32 is the reference arithmetic (Float32 values,
+ * Float32 group partials); *_f64 is the same algorithm in double precision, used as
+ * the FP64 accuracy oracle.
+ */
+#ifndef MAELSTROM_ORACLE_H
+#define MAELSTROM_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* FlipGrid (src/flip.jl:39-46): origin, spacing, cells, cylinder radius, floor, levels. */
+typedef struct {
+    float lo[3];
+    float dx;
+    int32_t n[3];
+    float radius;
+    float floor_z;
+    int32_t levels;
+} orc_grid;
+
+typedef struct {
+    int32_t iterations;    /* value pressure! returns (src/flip.jl:1082-1111) */
+    int32_t converged;     /* 1 unless maxiter ran out */
+    double rnorm;          /* last recursive residual norm */
+    double bnorm;          /* norm of the right-hand side */
+    double volume;         /* volume(s) at entry of project! (m^3) */
+    float gamma;           /* the volume-control divergence used in the rhs */
+} orc_info;
+
+/* ---- single passes (for unit tests) ---- */
+double orc_volume_f32(const orc_grid* g, const float* phi);
+double orc_volume_f64(const orc_grid* g, const double* phi);
+void orc_rhs_f32(const orc_grid* g, float* b, const float* u, const float* v, const float* w,
+                 const uint8_t* types, float gamma);
+void orc_rhs_f64(const orc_grid* g, double* b, const double* u, const double* v, const double* w,
+                 const uint8_t* types, double gamma);
+void orc_diag_f32(const orc_grid* g, float* diag, const uint8_t* types, const float* phi);
+void orc_diag_f64(const orc_grid* g, double* diag, const uint8_t* types, const double* phi);
+void orc_coarsen(const int32_t nf[3], uint8_t* tc, const uint8_t* tf);
+/* z = M^-1 r, one V-cycle (src/flip.jl:992-1014). level_types[l] for l=1..L-1 are the
+ * coarsened types (level 0 is `types`). */
+void orc_vcycle_f32(const orc_grid* g, float* z, const float* r, const uint8_t* types,
+                    const float* diag, int sweeps, int coarse);
+void orc_vcycle_f64(const orc_grid* g, double* z, const double* r, const uint8_t* types,
+                    const double* diag, int sweeps, int coarse);
+/* y = A x on LIQUID cells, 0 elsewhere (the operator inside residual_kernel!). */
+void orc_apply_f32(const orc_grid* g, float* y, const float* x, const uint8_t* types, const float* diag);
+void orc_apply_f64(const orc_grid* g, double* y, const double* x, const uint8_t* types, const double* diag);
+void orc_gradient_f32(const orc_grid* g, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv,
+                      uint8_t* fw, const float* P, const uint8_t* types, const float* phi);
+void orc_gradient_f64(const orc_grid* g, double* u, double* v, double* w, uint8_t* fu, uint8_t* fv,
+                      uint8_t* fw, const double* P, const uint8_t* types, const double* phi);
+
+/* ---- the solve and the whole projection ---- */
+/* pressure! (src/flip.jl:1082-1111): P is the warm start in, the pressure out; b the rhs. */
+int orc_pressure_f32(const orc_grid* g, float* P, const float* b, const uint8_t* types,
+                     const float* phi, float tol, int maxiter, int sweeps, int coarse, orc_info* info);
+int orc_pressure_f64(const orc_grid* g, double* P, const double* b, const uint8_t* types,
+                     const double* phi, double tol, int maxiter, int sweeps, int coarse, orc_info* info);
+/* project! (src/flip.jl:1144-1156). */
+int orc_project_f32(const orc_grid* g, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv,
+                    uint8_t* fw, float* P, const uint8_t* types, const float* phi, float volume0,
+                    double dt, double recover, float tol, int maxiter, int sweeps, int coarse,
+                    orc_info* info);
+int orc_project_f64(const orc_grid* g, double* u, double* v, double* w, uint8_t* fu, uint8_t* fv,
+                    uint8_t* fw, double* P, const uint8_t* types, const double* phi, double volume0,
+                    double dt, double recover, double tol, int maxiter, int sweeps, int coarse,
+                    orc_info* info);
+
+int orc_num_threads(void);
+void orc_set_num_threads(int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
