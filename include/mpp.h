@@ -148,6 +148,17 @@ int mpp_gradient(mpp_ctx* ctx, float* u, float* v, float* w, uint8_t* fu, uint8_
 /* FP64 pressure of the last mpp_pressure/mpp_project on an MPP_PREC_FP64 context. */
 int mpp_solution_f64(mpp_ctx* ctx, double* out_host);
 
+/* The liquid volume without allocating anything (no counterpart in the reference; it is
+ * volume(s), src/flip.jl:293, for callers that cannot allocate device memory when they
+ * want it, such as a monitoring or render callback under a fixed memory budget, where
+ * creating a context, which allocates the solver's whole workspace, is not an option).
+ * Its scratch is a static device array of 33,024 bytes that every GPU loading this
+ * library holds until exit; it handles grids of at most 16,777,216 cells (256^3) and
+ * returns MPP_ERR_INVALID beyond. All calls share that array: calls overlapping on the
+ * GPU race. The first call on a device sets up its address there, so make it before any
+ * stream capture. Synchronises `stream`; `volume` is a host pointer. */
+int mpp_volume_noalloc(const mpp_grid* grid, const float* phi, double* volume, mpp_stream stream);
+
 /* ---- per-kernel timing (the reference has none: bakeflip only logs @elapsed per
  * frame, src/flip.jl:1992-2010) ----
  * With profiling on, solves run their CG loop from the host (no graph) and bracket

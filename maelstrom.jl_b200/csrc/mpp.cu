@@ -1026,3 +1026,97 @@ int mpp_solution_f64(mpp_ctx* c, double* out) {
 }
 
 }  // extern "C"
+
+// ============================================== liquid volume without any allocation
+//
+// mpp_volume needs a context, and creating one allocates the whole solver workspace.
+// Some callers cannot allocate device memory at the moment they want the volume: a
+// render or monitoring callback with a fixed memory budget, code running while another
+// library owns the allocator, or a health check between steps that must not disturb the
+// memory the solver holds. mpp_volume_noalloc serves them: it runs the same volume
+// reduction with its scratch (per-block partial sums and the completion counter) in the
+// static device array below, which every GPU that loads this library holds until exit.
+//
+// Each block sums a fixed run of NOALLOC_BLOCK_CELLS cells, so the scratch bounds the
+// grid: at most NOALLOC_MAX_BLOCKS * NOALLOC_BLOCK_CELLS = 16,777,216 cells (256^3).
+// Every call shares the array, so calls that overlap on the GPU (on different streams
+// at once) race and give wrong results; calls in sequence are fine. The first call on a
+// device looks the array's address up once for that device (cudaGetSymbolAddress), so
+// that first call should come before any stream capture.
+namespace {
+
+constexpr int NOALLOC_BLOCK_CELLS = 4096;  // cells per block: 256 threads x 16
+constexpr int NOALLOC_MAX_BLOCKS = 4096;
+constexpr int64_t NOALLOC_MAX_CELLS = (int64_t)NOALLOC_BLOCK_CELLS * NOALLOC_MAX_BLOCKS;
+constexpr int NOALLOC_HEADER = 256;  // completion counter (offset 0) and the result (offset 8)
+constexpr size_t NOALLOC_SCRATCH_BYTES = NOALLOC_HEADER + sizeof(double) * NOALLOC_MAX_BLOCKS;  // 33,024
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// volume_kernel! + volume (src/flip.jl:261-279, 293), as k_volume, with the scratch laid
+// out in `scratch`: [counter u32 | result f64 | pad][partials f64 x blocks].
+__global__ void __launch_bounds__(TPB) k_volume_noalloc(Geo g, const float* __restrict__ phi, unsigned char* scratch) {
+    unsigned* counter = reinterpret_cast<unsigned*>(scratch);
+    double* result = reinterpret_cast<double*>(scratch + 8);
+    double* partials = reinterpret_cast<double*>(scratch + NOALLOC_HEADER);
+    const int64_t N = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    const int64_t lo = (int64_t)blockIdx.x * NOALLOC_BLOCK_CELLS;
+    const int64_t hi = lo + NOALLOC_BLOCK_CELLS < N ? lo + NOALLOC_BLOCK_CELLS : N;
+    double acc[1] = {0.0};
+    for (int64_t idx = lo + threadIdx.x; idx < hi; idx += TPB) {
+        const int i = (int)(idx % g.n[0]);
+        const int j = (int)((idx / g.n[0]) % g.n[1]);
+        const int k = (int)(idx / ((int64_t)g.n[0] * g.n[1]));
+        if (!issolidcell(g, i, j, k)) {
+            float x = 0.5f - phi[idx] / g.dx;
+            acc[0] += (double)(x > 1.f ? 1.f : (x < 0.f ? 0.f : x));
+        }
+    }
+    if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0)
+        *result = (double)((float)acc[0] * (g.dx * g.dx * g.dx));
+}
+
+// The array's device address, looked up once per device.
+constexpr int NOALLOC_MAX_DEVICES = 64;
+unsigned char* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+}  // namespace
+
+extern "C" int mpp_volume_noalloc(const mpp_grid* grid, const float* phi, double* volume, mpp_stream stream) {
+    if (!grid || !phi || !volume) {
+        set_err("null argument");
+        return MPP_ERR_INVALID;
+    }
+    if (grid->n[0] <= 0 || grid->n[1] <= 0 || grid->n[2] <= 0 || !(grid->dx > 0.f)) {
+        set_err("grid sides and dx must be positive");
+        return MPP_ERR_INVALID;
+    }
+    const int64_t N = (int64_t)grid->n[0] * grid->n[1] * grid->n[2];
+    if (N > NOALLOC_MAX_CELLS) {
+        set_err("mpp_volume_noalloc handles at most %lld cells (its static scratch holds %d block sums of %d cells); "
+                "this grid has %lld: use mpp_volume with a context",
+                (long long)NOALLOC_MAX_CELLS, NOALLOC_MAX_BLOCKS, NOALLOC_BLOCK_CELLS, (long long)N);
+        return MPP_ERR_INVALID;
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        set_err("device %d is beyond the %d devices mpp_volume_noalloc keeps addresses for", dev, NOALLOC_MAX_DEVICES);
+        return MPP_ERR_INVALID;
+    }
+    if (!g_noalloc_ptr[dev]) {
+        void* ptr = nullptr;
+        CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(ptr);
+    }
+    unsigned char* scratch = g_noalloc_ptr[dev];
+    cudaStream_t s = (cudaStream_t)stream;
+    // The counter must start at zero; an interrupted earlier call could have left it set.
+    CK(cudaMemsetAsync(scratch, 0, NOALLOC_HEADER, s));
+    const int blocks = (int)((N + NOALLOC_BLOCK_CELLS - 1) / NOALLOC_BLOCK_CELLS);
+    k_volume_noalloc<<<blocks, TPB, 0, s>>>(geo_of(*grid), phi, scratch);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(volume, scratch + 8, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return MPP_OK;
+}

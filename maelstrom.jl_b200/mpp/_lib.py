@@ -57,6 +57,7 @@ SIGNATURES = {
     "mpp_ctx_set_opts": (ctypes.c_int, [P, _O]),
     "mpp_ctx_bytes": (SZ, [P]),
     "mpp_volume": (ctypes.c_int, [P, P, ctypes.POINTER(F64), P]),
+    "mpp_volume_noalloc": (ctypes.c_int, [_G, P, ctypes.POINTER(F64), P]),
     "mpp_project": (ctypes.c_int, [P, P, P, P, P, P, P, P, P, P, F32, F64, F64, _R, P]),
     "mpp_pressure": (ctypes.c_int, [P, P, P, P, P, _R, P]),
     "mpp_rhs": (ctypes.c_int, [P, P, P, P, P, P, F32, P]),
