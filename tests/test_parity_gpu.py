@@ -186,6 +186,36 @@ def test_mixed_converges(cuda, basins, prec):
     assert err <= 1e-4
 
 
+@pytest.mark.parametrize("name", ["box16", "box32", "box32_gamma", "box16x16x32"])
+@pytest.mark.parametrize("prec,tol,bound", [("fp64", 1e-12, 1e-9), ("fp32", 1e-6, 1e-4), ("fp16", 1e-6, 1e-4),
+                                            ("bf16", 1e-6, 1e-4)])
+def test_golden_exact_solution(cuda, name, prec, tol, bound):
+    """Every form against the direct solve of the reference's equations (tests/golden)."""
+    import os
+    import sys
+
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, gold)
+    import make_golden
+
+    kw, gamma = make_golden.CASES[name]
+    basin = scene.box_basin(**kw)
+    fx = np.load(os.path.join(gold, f"{name}.npz"))
+    p = _projector(basin.grid, tol=tol, maxiter=300, precision=prec, graph=True)
+    P = _t(np.zeros(basin.grid.ncells, np.float32), cuda)
+    res = p.pressure(P, _t(fx["b"].astype(np.float32), cuda), _t(basin.types, cuda), _t(basin.phi, cuda))
+    assert res.status == 0, res.as_dict()
+    got = p.solution_f64() if prec == "fp64" else _np(P).astype(np.float64)
+    # FP64 solves the FP32-rounded rhs: compare against the exact solution of that rhs
+    exact = fx["P"]
+    if prec == "fp64":
+        b32 = fx["b"].astype(np.float32).astype(np.float64)
+        P32, _ = oracle.pressure(basin.grid, np.zeros(basin.grid.ncells), b32, basin.types, basin.phi, tol=1e-13,
+                                 maxiter=400, prec=64)
+        exact = P32
+    assert np.linalg.norm(got - exact) / np.linalg.norm(exact) <= bound
+
+
 def test_not_converged_warns(cuda, basins):
     import mpp
 
