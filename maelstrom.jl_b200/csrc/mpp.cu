@@ -11,7 +11,9 @@
 #include <vector>
 
 #include "mpp.h"
-#include "mpp_kernels.cuh"
+#include <cudaTypedefs.h>
+
+#include "mpp_tma.cuh"
 
 using namespace mpp;
 
@@ -38,6 +40,8 @@ void set_err(const char* fmt, ...) {
 constexpr int MAXLEV = 16;
 constexpr int NCOUNTERS = 8;
 enum { CNT_VOLUME, CNT_SETUP, CNT_DOT, CNT_SEARCH, CNT_ADVANCE, CNT_TRUE };
+// Smoother forms: 8-wide vector loads (default), the TMA pipeline, the per-column form.
+enum { RBGS_V8 = 0, RBGS_TMA = 1, RBGS_COLUMN = 2 };
 
 int vsize(int prec) { return prec == MPP_PREC_FP64 ? 8 : 4; }
 int msize(int prec) {
@@ -54,16 +58,17 @@ struct LevelBuf {
     void* b;
     void* r;
     uint8_t* types;
+    uint8_t* dc;
     uint8_t* tflag;
     uint32_t* tiles;
     int* count;
 };
 
 // Kernel families, for the profiler.
-enum { F_VOLUME, F_SETUP, F_LEVEL, F_TILES, F_START, F_RBGS, F_RESID, F_RESTRICT, F_COARSEST, F_PROLONG, F_DOT,
+enum { F_VOLUME, F_SETUP, F_LEVEL, F_TILES, F_START, F_RBGS, F_RESID, F_RESTRICT, F_BOTTOM, F_PROLONG, F_DOT,
        F_SEARCH, F_ADVANCE, F_TRUE, F_GRADIENT, F_CONVERT, NFAM };
 const char* const FAM_NAMES[NFAM] = {"volume",   "setup",    "coarsen", "tilelists", "start",         "rbgs",
-                                     "residual", "restrict", "coarsest", "prolong",  "dot",           "search",
+                                     "residual", "restrict", "bottom",   "prolong",  "dot",           "search",
                                      "advance",  "true_residual", "gradient", "convert"};
 struct ProfRec {
     int fam, level;
@@ -103,6 +108,16 @@ struct mpp_ctx {
     const void* gkey[10];
     int gkind;
     int g_prologue, g_body, g_epilogue;  // kernel counts in the graph's parts
+    // levels lb .. L-1 are solved in one CTA's shared memory (k_bottom)
+    int lb;
+    BotArgs bot;
+    size_t bot_smem, restrict_smem;
+    void* botb;  // level lb's right-hand side (natural order, stencil precision)
+    // TMA tensor maps of the row-split levels the smoother streams with cp.async.bulk.tensor
+    TmaLev tma[MAXLEV];
+    bool tma_ok[MAXLEV];
+    int tma_blocks;  // persistent grid of k_rbgs_tma
+    int rbgs_mode;   // which smoother form runs on row-split levels (MPP_RBGS: v8, tma, column)
     // profiler
     int prof_on;
     std::vector<ProfRec> pending;
@@ -112,6 +127,17 @@ struct mpp_ctx {
 };
 
 namespace {
+
+int alloc(mpp_ctx* c, void** p, size_t bytes);
+
+// An array read at neighbour offsets past its ends (see mpp_stream.cuh): `guard` zeroed
+// elements on each side; *p points at element 0.
+int alloc_guarded(mpp_ctx* c, void** p, size_t es, size_t n, size_t guard) {
+    void* base = nullptr;
+    if (int e = alloc(c, &base, es * (n + 2 * guard))) return e;
+    *p = static_cast<char*>(base) + es * guard;
+    return MPP_OK;
+}
 
 int alloc(mpp_ctx* c, void** p, size_t bytes) {
     if (bytes == 0) bytes = 16;
@@ -138,7 +164,7 @@ Lev<M> view(const mpp_ctx* c, int l) {
     v.H = b.H; v.GH = b.GH; v.GJ = b.GJ; v.GK = b.GK;
     v.code = b.code;
     v.dg = (M*)b.dg; v.x = (M*)b.x; v.b = (M*)b.b; v.r = (M*)b.r;
-    v.types = b.types; v.tflag = b.tflag; v.tiles = b.tiles; v.count = b.count;
+    v.types = b.types; v.dc = b.dc; v.tflag = b.tflag; v.tiles = b.tiles; v.count = b.count;
     return v;
 }
 
@@ -147,7 +173,14 @@ int grid_cells(const mpp_ctx* c, int64_t n) {
     int64_t cap = (int64_t)c->nsm * MAXBLOCKS_PER_SM;
     return (int)(g < cap ? (g > 0 ? g : 1) : cap);
 }
+// Column kernels: TILES_PER_BLOCK tiles per block per step of their grid-stride loop.
 int grid_tiles(const mpp_ctx* c, int l) {
+    int g = (c->lv[l].ntiles + TILES_PER_BLOCK - 1) / TILES_PER_BLOCK;
+    int cap = c->nsm * MAXBLOCKS_PER_SM;
+    return g < cap ? (g > 0 ? g : 1) : cap;
+}
+// Block-per-tile kernels (the restriction).
+int grid_tiles1(const mpp_ctx* c, int l) {
     int g = c->lv[l].ntiles;
     int cap = c->nsm * MAXBLOCKS_PER_SM;
     return g < cap ? (g > 0 ? g : 1) : cap;
@@ -191,7 +224,7 @@ void prof_size(const mpp_ctx* c, int fam, int level, double& bytes, int64_t& cel
         case F_LEVEL: cells = lcells(level); bpc = 8 + 1 + 1 + m; break;
         case F_TILES: {
             cells = 0;
-            for (int l = 0; l < c->L - 1; l++) cells += c->lv[l].ntiles;
+            for (int l = 0; l < c->lb; l++) cells += c->lv[l].ntiles;
             bpc = 1 + 4;
             break;
         }
@@ -199,7 +232,12 @@ void prof_size(const mpp_ctx* c, int fam, int level, double& bytes, int64_t& cel
         case F_RBGS: cells = act(level); bpc = 0.5 + 2 * m; break;
         case F_RESID: cells = act(level); bpc = 1 + 4 * m; break;
         case F_RESTRICT: cells = act(level); bpc = 8 * (1 + m) + 1 + m; break;
-        case F_COARSEST: cells = lcells(level); bpc = 8 * (1 + m) + 1 + m; break;
+        case F_BOTTOM: {  // the restriction into level lb reads the level above; the rest is on chip
+            cells = 0;
+            for (int l = c->lb; l < c->L; l++) cells += lcells(l);
+            bpc = (8.0 * (1 + m) * lcells(c->lb) + m * lcells(c->lb) + cells) / (double)cells;
+            break;
+        }
         case F_PROLONG: cells = act(level); bpc = 1 + 2 * m + (1 + m) / 8; break;
         case F_DOT: cells = act(level); bpc = 1 + m + v + (sep ? v : 0); break;
         case F_SEARCH: cells = act(level); bpc = 1 + m + 3 * v; break;
@@ -215,7 +253,7 @@ void prof_size(const mpp_ctx* c, int fam, int level, double& bytes, int64_t& cel
 // Fold the finished launches' event pairs into the accumulators (after a sync).
 void prof_collect(mpp_ctx* c) {
     if (c->pending.empty()) return;
-    for (int l = 0; l < c->L - 1; l++) cudaMemcpy(&c->active[l], c->lv[l].count, sizeof(int), cudaMemcpyDeviceToHost);
+    for (int l = 0; l < c->lb; l++) cudaMemcpy(&c->active[l], c->lv[l].count, sizeof(int), cudaMemcpyDeviceToHost);
     for (const ProfRec& r : c->pending) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, r.a, r.b);
@@ -290,9 +328,11 @@ struct Run {
         }
         TileTab tab;
         memset(&tab, 0, sizeof(tab));
-        tab.nlev = c->L - 1;
-        for (int l = 0; l < c->L - 1; l++) {
+        tab.nlev = c->lb;
+        for (int l = 0; l < c->lb; l++) {
             tab.ntiles[l] = c->lv[l].ntiles;
+            tab.GH[l] = c->lv[l].GH;
+            tab.GJ[l] = c->lv[l].GJ;
             tab.flags[l] = c->lv[l].tflag;
             tab.tiles[l] = c->lv[l].tiles;
             tab.count[l] = c->lv[l].count;
@@ -305,19 +345,31 @@ struct Run {
     void smooth(int l, const std::vector<int>& colours) {
         for (int col : colours) {
             beg(F_RBGS, l);
-            k_rbgs<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l), col);
+            if (c->rbgs_mode == RBGS_TMA && c->tma_ok[l]) {
+                const int g = c->lv[l].ntiles < c->tma_blocks ? c->lv[l].ntiles : c->tma_blocks;
+                k_rbgs_tma<Pr><<<g > 0 ? g : 1, TPB, TmaGeom<M>::SMEM, s>>>(view<M>(c, l), col, c->tma[l],
+                                                                           &c->sc->s.fault);
+            } else if (c->rbgs_mode != RBGS_COLUMN && c->lv[l].H % V8 == 0) {
+                const int wpb = TPB / 32, cap = c->nsm * MAXBLOCKS_PER_SM;
+                int g = (c->lv[l].ntiles + wpb - 1) / wpb;
+                g = g < cap ? (g > 0 ? g : 1) : cap;
+                k_rbgs_v8<Pr><<<g, TPB, 0, s>>>(view<M>(c, l), col);
+            } else {
+                k_rbgs<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l), col);
+            }
             end();
         }
     }
 
     // vcycle! (src/flip.jl:992-1014): z = M^-1 r from zero.
     void vcycle() {
-        const int L = c->L, sw = c->opts.sweeps;
+        const int sw = c->opts.sweeps;
         std::vector<int> down, up;
         for (int q = 0; q < sw; q++) { down.push_back(0); down.push_back(1); }
         down.erase(down.begin());  // the start kernel is the first colour's first sweep
         for (int q = 0; q < sw; q++) { up.push_back(1); up.push_back(0); }
-        for (int l = 0; l < L - 1; l++) {
+        const int lb = c->lb;
+        for (int l = 0; l < lb; l++) {
             beg(F_START, l);
             k_start<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l));
             end();
@@ -325,18 +377,28 @@ struct Run {
             beg(F_RESID, l);
             k_residual<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l));
             end();
-            if (l + 1 < L - 1) {
+            if (l + 1 < lb) {
                 beg(F_RESTRICT, l + 1);
-                k_restrict<Pr><<<grid_tiles(c, l + 1), TPB, 0, s>>>(view<M>(c, l), view<M>(c, l + 1));
+                k_restrict<Pr><<<grid_tiles1(c, l + 1), TPB, c->restrict_smem, s>>>(view<M>(c, l), view<M>(c, l + 1));
                 end();
             }
         }
-        beg(F_COARSEST, L - 1);
-        k_coarsest<Pr><<<1, 1024, 0, s>>>(view<M>(c, L - 2), view<M>(c, L - 1), c->opts.coarse);
+        BotArgs ba = c->bot;
+        ba.sweeps = sw;
+        ba.coarse = c->opts.coarse;
+        {
+            const int64_t Nb = (int64_t)c->lv[lb].n[0] * c->lv[lb].n[1] * c->lv[lb].n[2];
+            beg(F_RESTRICT, lb);
+            k_restrict_bottom<Pr><<<grid_cells(c, Nb), TPB, 0, s>>>(view<M>(c, lb - 1), view<M>(c, lb),
+                                                                    (typename Pr::C*)c->botb);
+            end();
+        }
+        beg(F_BOTTOM, lb);
+        k_bottom<Pr><<<1, 1024, c->bot_smem, s>>>((const typename Pr::C*)c->botb, (M*)c->lv[lb].x, ba);
         end();
-        for (int l = L - 2; l >= 0; l--) {
+        for (int l = lb - 1; l >= 0; l--) {
             beg(F_PROLONG, l);
-            k_prolong<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l), view<M>(c, l + 1), l + 1 == L - 1 ? 1 : 0);
+            k_prolong<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l), view<M>(c, l + 1), l + 1 == lb ? 1 : 0);
             end();
             smooth(l, up);
         }
@@ -524,6 +586,7 @@ template <class Pr>
 int solve(mpp_ctx* c, const Call& k, cudaStream_t s) {
     using V = typename Pr::V;
     int64_t launched = 0;
+    CK(cudaMemsetAsync(&c->sc->s.fault, 0, sizeof(int), s));
     if (c->opts.graph && !c->prof_on) {
         const void* key[10] = {k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.bnat, k.types, k.phi};
         if (!c->gexec || c->gkind != k.kind || memcmp(key, c->gkey, sizeof(key)) != 0) {
@@ -548,6 +611,10 @@ int solve(mpp_ctx* c, const Call& k, cudaStream_t s) {
     }
     CK(cudaGetLastError());
     c->launches += launched;
+    if (c->sc_host->s.fault) {
+        set_err("a bounded device wait (TMA pipeline) gave up; results are not valid");
+        return MPP_ERR_CUDA;
+    }
     return MPP_OK;
 }
 
@@ -611,6 +678,69 @@ int operator_setup(mpp_ctx* c, Run<Pr>& run, const uint8_t* types, const float* 
 }
 
 Lev<float> fine_layout(mpp_ctx* c) { return view<float>(c, 0); }
+
+// ---- TMA tensor maps (cuTensorMapEncodeTiled through the runtime's driver entry point) ----
+PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// A row-split level array as 4-D (h, colour, j, k), h innermost; box {bx, 1, by, bz}.
+bool encode_level(CUtensorMap* m, CUtensorMapDataType dt, void* base, size_t es, const LevelBuf& b, int bx, int by,
+                  int bz) {
+    auto enc = tma_encoder();
+    if (!enc || !base) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)b.H, 2, (cuuint64_t)b.n[1], (cuuint64_t)b.n[2]};
+    const cuuint64_t strides[3] = {(cuuint64_t)b.H * es, (cuuint64_t)b.n[0] * es,
+                                   (cuuint64_t)b.n[0] * (cuuint64_t)b.n[1] * es};
+    const cuuint32_t box[4] = {(cuuint32_t)bx, 1, (cuuint32_t)by, (cuuint32_t)bz};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(m, dt, 4, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor maps for every row-split level whose rows are whole tiles (h extent a multiple of
+// 16, so every box start is 16-byte aligned) and whose j and k extents hold a halo box.
+// Levels without them, or with MPP_NO_TMA set in the environment, use k_rbgs.
+int build_tma(mpp_ctx* c) {
+    const size_t ms = msize(c->prec);
+    const CUtensorMapDataType dt = c->prec == MPP_PREC_FP64        ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                   : c->prec == MPP_PREC_MIXED_FP16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                   : c->prec == MPP_PREC_MIXED_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                                    : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const int pad = 16 / (int)ms;
+    const bool off = getenv("MPP_NO_TMA") != nullptr;
+    const char* mode = getenv("MPP_RBGS");
+    c->rbgs_mode = !mode ? RBGS_V8 : (!strcmp(mode, "tma") ? RBGS_TMA : (!strcmp(mode, "column") ? RBGS_COLUMN : RBGS_V8));
+    for (int l = 0; l < MAXLEV; l++) c->tma_ok[l] = false;
+    for (int l = 0; l < c->lb; l++) {
+        const LevelBuf& b = c->lv[l];
+        if (off || b.H % TH != 0 || b.n[1] < TY + 4 || b.n[2] < TZ + 4) continue;
+        TmaLev& t = c->tma[l];
+        c->tma_ok[l] = encode_level(&t.xh, dt, b.x, ms, b, TH + 2 * pad, TY + 2, TZ + 2) &&
+                       encode_level(&t.b, dt, b.b, ms, b, TH, TY, TZ) &&
+                       encode_level(&t.dg, dt, b.dg, ms, b, TH, TY, TZ) &&
+                       encode_level(&t.code, CU_TENSOR_MAP_DATA_TYPE_UINT8, b.code, 1, b, TH, TY, TZ);
+    }
+    return dispatch(c->prec, [&](auto pr) -> int {
+        using Pr = decltype(pr);
+        using M = typename Pr::M;
+        CK(cudaFuncSetAttribute(k_rbgs_tma<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, TmaGeom<M>::SMEM));
+        int nb = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_rbgs_tma<Pr>, TPB, TmaGeom<M>::SMEM));
+        c->tma_blocks = (nb > 0 ? nb : 1) * c->nsm;
+        return MPP_OK;
+    });
+}
 
 }  // namespace
 
@@ -731,10 +861,19 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
     int e;
     // level geometry
     size_t tflag_total = 0;
+    // the first level small enough for the one-CTA bottom solve
+    c->lb = c->L - 1;
+    for (int l = 1; l < c->L; l++) {
+        const int64_t Nl = (int64_t)(g->n[0] >> l) * (g->n[1] >> l) * (g->n[2] >> l);
+        if (Nl <= BOTTOM_CELLS) {
+            c->lb = l;
+            break;
+        }
+    }
     for (int l = 0; l < c->L; l++) {
         LevelBuf& b = c->lv[l];
         for (int a = 0; a < 3; a++) b.n[a] = g->n[a] >> l;
-        b.split = l < c->L - 1;
+        b.split = l < c->lb;
         if (b.split) {
             b.H = b.n[0] / 2;
             b.GH = (b.H + TH - 1) / TH;
@@ -757,25 +896,76 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
             if ((e = alloc(c, (void**)&b.tiles, sizeof(uint32_t) * b.ntiles))) return fail(e);
             if ((e = alloc(c, (void**)&b.count, sizeof(int)))) return fail(e);
             if ((e = alloc(c, (void**)&b.code, Nl))) return fail(e);
-            if ((e = alloc(c, &b.x, ms * Nl))) return fail(e);
+            if ((e = alloc_guarded(c, &b.x, ms, Nl, guard_of(b.n[0], b.n[1])))) return fail(e);
             if ((e = alloc(c, &b.r, ms * Nl))) return fail(e);
             if (l > 0 || !alias) {
                 if ((e = alloc(c, &b.dg, ms * Nl))) return fail(e);
                 if ((e = alloc(c, &b.b, ms * Nl))) return fail(e);
             }
-        } else {
+        } else {  // a level of the one-CTA bottom solve: natural order
             if ((e = alloc(c, &b.x, ms * Nl))) return fail(e);
+            if ((e = alloc(c, (void**)&b.code, Nl))) return fail(e);
+            if ((e = alloc(c, (void**)&b.dc, Nl))) return fail(e);
         }
+    }
+    {
+        const LevelBuf& b = c->lv[c->lb];
+        const size_t cs = c->prec == MPP_PREC_FP64 ? 8 : 4;
+        if ((e = alloc(c, &c->botb, cs * (size_t)b.n[0] * b.n[1] * b.n[2]))) return fail(e);
+    }
+    {  // the bottom solve's shared-memory layout: levels lb .. L-1 in natural order
+        const size_t cs = c->prec == MPP_PREC_FP64 ? 8 : 4;   // stencil arithmetic (C)
+        const size_t ccs = c->prec == MPP_PREC_FP32 ? 4 : 8;  // coarsest (CC)
+        size_t o = 0;
+        auto take = [&](size_t bytes) {
+            const size_t at = o;
+            o += (bytes + 15) & ~(size_t)15;
+            return (int)at;
+        };
+        BotArgs& ba = c->bot;
+        memset(&ba, 0, sizeof(ba));
+        ba.nl = c->L - c->lb;
+        if (ba.nl > BOTTOM_MAXLEV) {
+            set_err("%d levels below %d cells; at most %d are supported", ba.nl, BOTTOM_CELLS, BOTTOM_MAXLEV);
+            return fail(MPP_ERR_INVALID);
+        }
+        for (int q = 0; q < ba.nl; q++) {
+            const LevelBuf& b = c->lv[c->lb + q];
+            const size_t Nl = (size_t)b.n[0] * b.n[1] * b.n[2];
+            const bool coarsest = q == ba.nl - 1;
+            BotLev& B = ba.lv[q];
+            B.n1 = b.n[0];
+            B.n2 = b.n[1];
+            B.n3 = b.n[2];
+            B.code = b.code;
+            B.dc = b.dc;
+            B.ox = take((coarsest ? ccs : cs) * Nl);
+            B.ob = take((coarsest ? ccs : cs) * Nl);
+            B.orr = coarsest ? 0 : take(cs * Nl);
+            B.ocode = take(Nl);
+            B.odc = take(Nl);
+        }
+        c->bot_smem = o;
+        c->restrict_smem = (size_t)RX * RY * RZ * cs;
+        const int ea = dispatch(c->prec, [&](auto pr) -> int {
+            using Pr = decltype(pr);
+            CK(cudaFuncSetAttribute(k_bottom<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->bot_smem));
+            CK(cudaFuncSetAttribute(k_restrict<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)c->restrict_smem));
+            return MPP_OK;
+        });
+        if (ea) return fail(ea);
     }
     if ((e = alloc(c, &c->diag, vs * N))) return fail(e);
     if ((e = alloc(c, &c->bvec, vs * N))) return fail(e);
     if ((e = alloc(c, &c->r, vs * N))) return fail(e);
-    if ((e = alloc(c, &c->d, vs * N))) return fail(e);
+    if ((e = alloc_guarded(c, &c->d, vs, N, guard_of(g->n[0], g->n[1])))) return fail(e);
     if ((e = alloc(c, &c->q, vs * N))) return fail(e);
     if (alias) {
         c->lv[0].dg = c->diag;
         c->lv[0].b = c->r;
     }
+    if ((e = build_tma(c))) return fail(e);
     if (c->prec == MPP_PREC_FP64 && (e = alloc(c, &c->Pd, sizeof(double) * N))) return fail(e);
     if ((e = alloc(c, (void**)&c->sc, sizeof(Scalars)))) return fail(e);
     if ((e = alloc(c, (void**)&c->partials, sizeof(double) * MAXK * (size_t)c->nsm * MAXBLOCKS_PER_SM))) return fail(e);

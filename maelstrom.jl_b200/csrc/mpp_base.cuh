@@ -1,0 +1,416 @@
+// The projection's whole-grid kernels (sm_100a): parameters and device state, volume,
+// the fine set-up pass, coarsening, the gradient update, layout conversions. Every kernel
+// names the reference kernel(s) of
+// src/flip.jl it computes; the per-cell arithmetic follows the reference's operation
+// order, and the library is built with -fmad=false, so the FP32 form rounds exactly as
+// the reference's Float32 code does. Reductions are FP64 and deterministic (mpp_common).
+#pragma once
+
+#include "mpp_common.cuh"
+
+namespace mpp {
+
+// ---- per-call parameters and the device-resident solver state ----
+struct Params {
+    float volume0;   // s.volume0
+    float tol;       // relative tolerance
+    double dt;       // time step (project!)
+    double recover;  // volume recovery time (project!)
+    int maxiter;
+    int project;     // 1: gamma from the volume loss; 0: no volume term
+    float gamma;     // (unused when project = 1)
+    int pad;
+};
+
+struct State {
+    double vol;      // volume(s), m^3
+    double bnorm, target, rnorm, rho, alpha, beta, pq, true_rr;
+    double nliq;     // LIQUID cells
+    double rscale;   // power of two the next V-cycle input is scaled by (16-bit forms)
+    float gamma;
+    int status;      // MPP_* status
+    int it;          // CG iterations done
+    int done;        // 1 once the loop must stop
+    int fault;       // a bounded device wait gave up (the host reports an error)
+    int pad;
+};
+
+struct Scalars {
+    Params p;
+    State s;
+};
+
+enum { ST_OK = 0, ST_NOT_CONVERGED = 1, ST_NONFINITE = 2, ST_INDEFINITE = 3, ST_BREAKDOWN = 4 };
+
+__device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
+
+// Scalars as the reference keeps them: Float32 (f32_scalars) or FP64.
+template <class Pr>
+__device__ __forceinline__ double rs(double x) {
+    if constexpr (Pr::f32_scalars) return (double)(float)x;
+    else return x;
+}
+template <class Pr>
+__device__ __forceinline__ double sq(double x) {
+    if constexpr (Pr::f32_scalars) return (double)sqrtf((float)x);
+    else return sqrt(x);
+}
+template <class Pr>
+__device__ __forceinline__ double dv(double a, double b) {
+    if constexpr (Pr::f32_scalars) return (double)((float)a / (float)b);
+    else return a / b;
+}
+
+// The power of two the next V-cycle input is scaled by in the 16-bit forms: it brings
+// the residual's typical entry, |r| / sqrt(liquid cells), to about 1/4, far from both
+// ends of FP16's range. (The V-cycle is linear and CG is invariant to a scalar on the
+// preconditioner, so the scale changes no iterate.)
+__device__ __forceinline__ double next_rscale(double rnorm, double nliq) {
+    if (!(rnorm > 0.0) || !isfinite(rnorm) || !(nliq > 0.0)) return 1.0;
+    double e = rint(log2(0.25 * sqrt(nliq) / rnorm));
+    e = e > 60.0 ? 60.0 : (e < -60.0 ? -60.0 : e);
+    return exp2(e);
+}
+
+__device__ __forceinline__ void set_cond(cudaGraphConditionalHandle h, int use, int go) {
+    if (use) cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// ---- geometry (FlipGrid, src/flip.jl:39-66) ----
+struct Geo {
+    float lo[3];
+    float dx;
+    int n[3];
+    float radius, floor_z;
+};
+// issolidcell: the cell centre lies outside the cylinder or under the floor (Float32).
+__device__ __forceinline__ bool issolidcell(const Geo& g, int i, int j, int k) {
+    float px = g.lo[0] + ((float)i + 0.5f) * g.dx;
+    float py = g.lo[1] + ((float)j + 0.5f) * g.dx;
+    float pz = g.lo[2] + ((float)k + 0.5f) * g.dx;
+    return px * px + py * py > g.radius * g.radius || pz < g.floor_z;
+}
+
+__device__ __forceinline__ uint8_t typeat(const uint8_t* __restrict__ t, int n1, int n2, int n3, int i, int j,
+                                          int k) {
+    return (i >= 0 && i < n1 && j >= 0 && j < n2 && k >= 0 && k < n3)
+               ? t[(int64_t)i + (int64_t)n1 * ((int64_t)j + (int64_t)n2 * k)]
+               : SOLID;
+}
+
+// volume_kernel! + volume + the gamma of project! (src/flip.jl:261-279, 293, 1146-1147):
+// liquid volume sum clamp(0.5 - phi/dx, 0, 1) dx^3 over cells whose centre is not solid,
+// then gamma = clamp(loss / recover, -0.01/dt, 0.01/dt) with loss the relative volume loss.
+__global__ void __launch_bounds__(TPB) k_volume(Geo g, const float* __restrict__ phi, Scalars* sc,
+                                                double* partials, unsigned* counter) {
+    const int64_t N = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    double acc[1] = {0.0};
+    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
+        int i = (int)(idx % g.n[0]);
+        int j = (int)((idx / g.n[0]) % g.n[1]);
+        int k = (int)(idx / ((int64_t)g.n[0] * g.n[1]));
+        if (!issolidcell(g, i, j, k)) {
+            float x = 0.5f - phi[idx] / g.dx;
+            acc[0] += (double)(x > 1.f ? 1.f : (x < 0.f ? 0.f : x));
+        }
+    }
+    if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
+        float vol = (float)acc[0] * (g.dx * g.dx * g.dx);
+        sc->s.vol = (double)vol;
+        if (sc->p.project) {
+            float loss = (sc->p.volume0 - vol) / sc->p.volume0;
+            double lo = -0.01 / sc->p.dt, hi = 0.01 / sc->p.dt, x = (double)loss / sc->p.recover;
+            sc->s.gamma = (float)(x > hi ? hi : (x < lo ? lo : x));
+        } else {
+            sc->s.gamma = sc->p.gamma;
+        }
+    }
+}
+
+// Inputs of the fine-level set-up pass.
+template <class V>
+struct SetupIn {
+    const float* u;  // faces, or null when b is given
+    const float* v;
+    const float* w;
+    const float* bnat;  // given rhs (natural), or null
+    V* P;               // pressure (natural): warm start in
+    const uint8_t* types;
+    const float* phi;   // null: no ghost-fluid terms (rhs-only passes)
+    float dx;
+    int clear_P;   // clearair (src/flip.jl:1132-1135)
+    int residual;  // 1: r = b - A P and the norms; 0: operator only
+};
+
+// The fine level's set-up, one pass over every cell (natural order):
+//   diag_kernel! (src/flip.jl:824-836) -> diag (and the smoother's copy),
+//   rhs_kernel!  (src/flip.jl:817-822) -> b (unless b is given),
+//   clearair_kernel! (src/flip.jl:1132-1135) -> P = 0 off-liquid,
+//   residual_kernel! (src/flip.jl:859-863) on the warm start -> r,
+//   the stencil codes and the level's tile flags, and |b|^2, |r|^2 for pressure!'s
+//   first tests (src/flip.jl:1090-1094).
+template <class Pr>
+__global__ void __launch_bounds__(TPB)
+    k_setup(SetupIn<typename Pr::V> a, Lev<typename Pr::M> L, typename Pr::V* __restrict__ diag,
+            typename Pr::V* __restrict__ b, typename Pr::V* __restrict__ r, Scalars* sc, double* partials,
+            unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
+    using V = typename Pr::V;
+    using M = typename Pr::M;
+    using C = typename Pr::C;
+    const int n1 = L.n1, n2 = L.n2, n3 = L.n3;
+    const int64_t N = (int64_t)n1 * n2 * n3;
+    const C dx = (C)a.dx;
+    const C gamma = (C)(sc->p.project ? sc->s.gamma : sc->p.gamma);
+    const bool sep_dg = (void*)L.dg != (void*)diag;
+    const bool sep_b = (void*)L.b != (void*)r;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
+        const int i = (int)(idx % n1);
+        const int j = (int)((idx / n1) % n2);
+        const int k = (int)(idx / ((int64_t)n1 * n2));
+        const uint8_t t = a.types[idx];
+        acc[2] += t == LIQUID ? 1.0 : 0.0;
+        const int64_t p = L.pos(i, j, k);
+        uint8_t code = 0;
+        C d = (C)0, bv = (C)0, rv = (C)0;
+        if (t == LIQUID) {
+            const int di[6] = {1, -1, 0, 0, 0, 0}, dj[6] = {0, 0, 1, -1, 0, 0}, dk[6] = {0, 0, 0, 0, 1, -1};
+            const C phc = a.phi ? (C)a.phi[idx] : (C)0;
+#pragma unroll
+            for (int m = 0; m < 6; m++) {
+                const int ii = i + di[m], jj = j + dj[m], kk = k + dk[m];
+                const uint8_t tn = typeat(a.types, n1, n2, n3, ii, jj, kk);
+                if (tn == LIQUID) {
+                    code |= (uint8_t)(1u << m);
+                    d += (C)1;
+                }
+                if (tn == AIR && a.phi)
+                    d += (C)1 / theta<C>(phc, (C)a.phi[(int64_t)ii + (int64_t)n1 * ((int64_t)jj + (int64_t)n2 * kk)]);
+            }
+            code |= SELF;
+            if (a.bnat) {
+                bv = (C)a.bnat[idx];
+            } else if (a.u) {
+                C div = (C)a.u[(int64_t)(i + 1) + (int64_t)(n1 + 1) * ((int64_t)j + (int64_t)n2 * k)] -
+                        (C)a.u[(int64_t)i + (int64_t)(n1 + 1) * ((int64_t)j + (int64_t)n2 * k)];
+                div = div + (C)a.v[(int64_t)i + (int64_t)n1 * ((int64_t)(j + 1) + (int64_t)(n2 + 1) * k)];
+                div = div - (C)a.v[(int64_t)i + (int64_t)n1 * ((int64_t)j + (int64_t)(n2 + 1) * k)];
+                div = div + (C)a.w[idx + (int64_t)n1 * n2];
+                div = div - (C)a.w[idx];
+                bv = (-dx) * div + (dx * dx) * gamma;
+            }
+            if (a.residual) {
+                C s = (C)0;
+#pragma unroll
+                for (int m = 0; m < 6; m++)
+                    if (code & (1u << m)) s += (C)a.P[(int64_t)(i + di[m]) + (int64_t)n1 * ((int64_t)(j + dj[m]) + (int64_t)n2 * (k + dk[m]))];
+                rv = bv - (d * (C)a.P[idx] - s);
+            }
+            L.tflag[L.tile_of(i, j, k)] = 1;
+        } else if (a.clear_P) {
+            a.P[idx] = (V)0;
+        }
+        L.code[p] = code;
+        st(diag + p, d);
+        if (sep_dg) st(L.dg + p, d);
+        st(b + p, bv);
+        if (a.residual) {
+            st(r + p, rv);
+            if (sep_b) st(L.b + p, rv);
+            acc[0] += (double)bv * (double)bv;
+            acc[1] += (double)rv * (double)rv;
+        }
+    }
+    if (!a.residual) return;
+    if (grid_sum<3>(acc, partials, counter) && threadIdx.x == 0) {
+        State& s = sc->s;
+        s.bnorm = sq<Pr>(acc[0]);
+        s.target = rs<Pr>((double)sc->p.tol * s.bnorm);
+        s.rnorm = sq<Pr>(acc[1]);
+        s.nliq = acc[2];
+        s.rscale = next_rscale(s.rnorm, s.nliq);
+        s.it = 0;
+        s.rho = 0.0;
+        s.beta = 0.0;
+        s.alpha = 0.0;
+        s.status = ST_OK;
+        s.done = 0;
+        if (!finite_d(s.bnorm) || !finite_d(s.rnorm)) {
+            s.status = ST_NONFINITE;
+            s.done = 1;
+        } else if (s.bnorm == 0.0 || s.rnorm <= s.target) {
+            s.done = 1;  // pressure! returns 0 (src/flip.jl:1091-1094)
+        }
+        set_cond(cond, use_cond, !s.done);
+    }
+}
+
+// coarsen_kernel! (src/flip.jl:880-889) for level l from level l-1, fused with the coarse
+// level's stencil codes, its diagonal (celldiag, src/flip.jl:843-850: the count of
+// non-SOLID neighbours) and its tile flags. One thread per coarse cell (natural order);
+// the neighbours' classes are coarsened again from their children, which are cached.
+__device__ __forceinline__ uint8_t coarsen_at(const uint8_t* __restrict__ tf, int f1, int f2, int f3, int I, int J,
+                                              int K) {
+    bool air = false, liquid = false;
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int b = 0; b < 2; b++)
+#pragma unroll
+            for (int a = 0; a < 2; a++) {
+                uint8_t t = typeat(tf, f1, f2, f3, 2 * I + a, 2 * J + b, 2 * K + c);
+                air |= t == AIR;
+                liquid |= t == LIQUID;
+            }
+    return air ? AIR : (liquid ? LIQUID : SOLID);
+}
+
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_level(const uint8_t* __restrict__ tf, int f1, int f2, int f3,
+                                               Lev<typename Pr::M> L, int split) {
+    const int n1 = L.n1, n2 = L.n2, n3 = L.n3;
+    const int64_t N = (int64_t)n1 * n2 * n3;
+    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
+        const int I = (int)(idx % n1), J = (int)((idx / n1) % n2), K = (int)(idx / ((int64_t)n1 * n2));
+        const uint8_t t = coarsen_at(tf, f1, f2, f3, I, J, K);
+        L.types[idx] = t;
+        uint8_t code = 0;
+        float d = 0.f;
+        if (t == LIQUID) {
+            const int di[6] = {1, -1, 0, 0, 0, 0}, dj[6] = {0, 0, 1, -1, 0, 0}, dk[6] = {0, 0, 0, 0, 1, -1};
+#pragma unroll
+            for (int m = 0; m < 6; m++) {
+                const int ii = I + di[m], jj = J + dj[m], kk = K + dk[m];
+                uint8_t tn = SOLID;
+                if (ii >= 0 && ii < n1 && jj >= 0 && jj < n2 && kk >= 0 && kk < n3)
+                    tn = coarsen_at(tf, f1, f2, f3, ii, jj, kk);
+                if (tn != SOLID) d += 1.f;
+                if (tn == LIQUID) code |= (uint8_t)(1u << m);
+            }
+            code |= SELF;
+            if (split) L.tflag[L.tile_of(I, J, K)] = 1;
+        }
+        if (split) {
+            const int64_t p = L.pos(I, J, K);
+            L.code[p] = code;
+            st(L.dg + p, d);
+        } else {  // a level of the one-CTA bottom solve: natural order
+            L.code[idx] = code;
+            L.dc[idx] = (uint8_t)d;
+        }
+    }
+}
+
+// restrict_kernel! (src/flip.jl:894-906) into the first level of the one-CTA bottom solve
+// (natural order, a few thousand cells), from the row-split level above: one thread per
+// coarse cell, its 64 code and residual loads issued together. Values in C precision
+// (the scaled forms without the factor 4).
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_restrict_bottom(Lev<typename Pr::M> F, Lev<typename Pr::M> L,
+                                                         typename Pr::C* __restrict__ bout) {
+    using C = typename Pr::C;
+    const int N = L.n1 * L.n2 * L.n3;
+    for (int c = blockIdx.x * TPB + threadIdx.x; c < N; c += gridDim.x * TPB) {
+        C v = (C)0;
+        if (L.code[c] & SELF) {
+            const int I = c % L.n1, J = (c / L.n1) % L.n2, K = c / (L.n1 * L.n2);
+            C s = (C)0;
+#pragma unroll
+            for (int c3 = 0; c3 < 4; c3++)
+#pragma unroll
+                for (int b3 = 0; b3 < 4; b3++)
+#pragma unroll
+                    for (int a3 = 0; a3 < 4; a3++) {
+                        const int i = 2 * I + a3 - 1, j = 2 * J + b3 - 1, k = 2 * K + c3 - 1;
+                        C rv = (C)0;
+                        if (i >= 0 && i < F.n1 && j >= 0 && j < F.n2 && k >= 0 && k < F.n3) {
+                            const int p = (int)F.pos(i, j, k);
+                            const uint8_t cd = F.code[p];
+                            const C r = ld<C>(F.r + p);
+                            rv = (cd & SELF) ? r : (C)0;
+                        }
+                        const C w = (a3 == 1 || a3 == 2 ? (C)0.375f : (C)0.125f) *
+                                    (b3 == 1 || b3 == 2 ? (C)0.375f : (C)0.125f) *
+                                    (c3 == 1 || c3 == 2 ? (C)0.375f : (C)0.125f);
+                        s += w * rv;
+                    }
+            v = Pr::scaled ? s : (C)4 * s;
+        }
+        bout[c] = v;
+    }
+}
+
+
+// project_kernel! (src/flip.jl:1113-1130) for all three face sets in one launch: a face
+// with no SOLID side and a LIQUID one gets u -= delta/dx (ghost fluid at air faces) and
+// valid = 1; every other face valid = 0. One thread per face site (i,j,k) of the
+// (nx+1, ny+1, nz+1) lattice, handling the u, v and w faces that exist there.
+__device__ __forceinline__ void face_update(float* __restrict__ u, uint8_t* __restrict__ f, int64_t fi,
+                                            const float* __restrict__ P, const uint8_t* __restrict__ types,
+                                            const float* __restrict__ phi, int n1, int n2, int n3, int a, int b,
+                                            int c, int i, int j, int k, float dx) {
+    const uint8_t t0 = typeat(types, n1, n2, n3, a, b, c), t1 = typeat(types, n1, n2, n3, i, j, k);
+    const bool ok = t0 != SOLID && t1 != SOLID && (t0 == LIQUID || t1 == LIQUID);
+    if (ok) {
+        const int64_t c0 = (int64_t)a + (int64_t)n1 * ((int64_t)b + (int64_t)n2 * c);
+        const int64_t c1 = (int64_t)i + (int64_t)n1 * ((int64_t)j + (int64_t)n2 * k);
+        float delta;
+        if (t0 == LIQUID && t1 == LIQUID) delta = P[c1] - P[c0];
+        else if (t0 == LIQUID) delta = (-P[c0]) / theta<float>(phi[c0], phi[c1]);
+        else delta = P[c1] / theta<float>(phi[c1], phi[c0]);
+        u[fi] = u[fi] - delta / dx;
+    }
+    f[fi] = ok ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(TPB) k_gradient(int n1, int n2, int n3, float* __restrict__ u, float* __restrict__ v,
+                                                  float* __restrict__ w, uint8_t* __restrict__ fu,
+                                                  uint8_t* __restrict__ fv, uint8_t* __restrict__ fw,
+                                                  const float* __restrict__ P, const uint8_t* __restrict__ types,
+                                                  const float* __restrict__ phi, float dx) {
+    const int m1 = n1 + 1, m2 = n2 + 1, m3 = n3 + 1;
+    const int64_t N = (int64_t)m1 * m2 * m3;
+    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
+        const int i = (int)(idx % m1), j = (int)((idx / m1) % m2), k = (int)(idx / ((int64_t)m1 * m2));
+        if (j < n2 && k < n3)
+            face_update(u, fu, (int64_t)i + (int64_t)m1 * ((int64_t)j + (int64_t)n2 * k), P, types, phi, n1, n2, n3,
+                        i - 1, j, k, i, j, k, dx);
+        if (i < n1 && k < n3)
+            face_update(v, fv, (int64_t)i + (int64_t)n1 * ((int64_t)j + (int64_t)m2 * k), P, types, phi, n1, n2, n3,
+                        i, j - 1, k, i, j, k, dx);
+        if (i < n1 && j < n2)
+            face_update(w, fw, (int64_t)i + (int64_t)n1 * ((int64_t)j + (int64_t)n2 * k), P, types, phi, n1, n2, n3,
+                        i, j, k - 1, i, j, k, dx);
+    }
+}
+
+// ---- layout conversions (natural <-> row-split) for the single-pass entry points ----
+template <class T, class S>
+__global__ void __launch_bounds__(TPB) k_to_split(Lev<float> L, T* __restrict__ dst, const S* __restrict__ src) {
+    const int64_t N = (int64_t)L.n1 * L.n2 * L.n3;
+    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
+        const int i = (int)(idx % L.n1), j = (int)((idx / L.n1) % L.n2), k = (int)(idx / ((int64_t)L.n1 * L.n2));
+        st(dst + L.pos(i, j, k), ld<double>(src + idx));
+    }
+}
+template <class T, class S>
+__global__ void __launch_bounds__(TPB) k_from_split(Lev<float> L, T* __restrict__ dst, const S* __restrict__ src) {
+    const int64_t N = (int64_t)L.n1 * L.n2 * L.n3;
+    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
+        const int i = (int)(idx % L.n1), j = (int)((idx / L.n1) % L.n2), k = (int)(idx / ((int64_t)L.n1 * L.n2));
+        st(dst + idx, ld<double>(src + L.pos(i, j, k)));
+    }
+}
+
+// P (float, natural) <-> the FP64 solution vector.
+__global__ void __launch_bounds__(TPB) k_widen(double* __restrict__ dst, const float* __restrict__ src, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * TPB + threadIdx.x; i < n; i += (int64_t)gridDim.x * TPB)
+        dst[i] = (double)src[i];
+}
+__global__ void __launch_bounds__(TPB) k_narrow(float* __restrict__ dst, const double* __restrict__ src, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * TPB + threadIdx.x; i < n; i += (int64_t)gridDim.x * TPB)
+        dst[i] = (float)src[i];
+}
+
+
+}  // namespace mpp

@@ -19,9 +19,11 @@ constexpr uint8_t SOLID = 0, LIQUID = 1, AIR = 2;
 // cell itself is. A cell whose code lacks SELF is never updated and never read.
 constexpr uint8_t SELF = 1u << 6;
 
-// Tiles: 16 (h) x 4 (j) x 4 (k) slots of 2 cells each (one per colour), so a tile is a
-// 32 x 4 x 4 block of cells; 256 threads, one slot each.
-constexpr int TH = 16, TY = 4, TZ = 4, TPB = 256;
+// Tiles: 32 (h) x 4 (j) x 2 (k) slots of 2 cells each (one per colour), so a tile is a
+// 64 x 4 x 2 block of cells; 256 threads, one slot each; a warp reads one row's 32
+// consecutive same-colour values (64-128 bytes).
+constexpr int TH = 32, TY = 4, TZ = 2, TPB = 256;
+static_assert(TH * TY * TZ == TPB, "one thread per tile slot");
 
 // Grid-wide sums: at most MAXK values per block, at most MAXBLOCKS_PER_SM blocks per SM
 // (the partial-sum buffer holds MAXK * MAXBLOCKS_PER_SM * SMs doubles).
@@ -95,6 +97,7 @@ struct Lev {
     M* b;            // right-hand side
     M* r;            // residual
     uint8_t* types;  // natural order (coarse levels)
+    uint8_t* dc;     // non-SOLID neighbour counts (bottom levels, natural order; their code is natural too)
     uint8_t* tflag;  // per-tile "has liquid" flags
     uint32_t* tiles; // active tile list
     int* count;      // its length (device)
@@ -111,42 +114,11 @@ struct Lev {
     }
 };
 
-// A thread's slot in a tile: column h (both colours), row j, plane k.
-struct Slot {
-    int h, j, k;
-    bool in;
-};
-template <class M>
-__device__ __forceinline__ Slot slot_of(const Lev<M>& L, uint32_t tile) {
-    int th = (int)(tile % (uint32_t)L.GH);
-    int tj = (int)((tile / (uint32_t)L.GH) % (uint32_t)L.GJ);
-    int tk = (int)(tile / ((uint32_t)L.GH * (uint32_t)L.GJ));
-    Slot s;
-    s.h = th * TH + (threadIdx.x & 15);
-    s.j = tj * TY + ((threadIdx.x >> 4) & 3);
-    s.k = tk * TZ + (threadIdx.x >> 6);
-    s.in = s.h < L.H && s.j < L.n2 && s.k < L.n3;
-    return s;
-}
-
-// Cell i of colour c in slot (h, j, k).
-__device__ __forceinline__ int cell_i(int h, int c, int j, int k) { return 2 * h + ((c + j + k + 1) & 1); }
-
-// Sum of x over the LIQUID neighbours of a row-split cell, in the reference's order
-// (liquidsum, src/flip.jl:852-857: s = 0, then +x,-x,+y,-y,+z,-z). `o` is the start of
-// the other colour's half of the cell's row; sy/sz the row and plane strides.
-template <class C, class T>
-__device__ __forceinline__ C nbsum(const T* __restrict__ x, uint8_t code, int64_t o, int i, int h, int64_t sy,
-                                   int64_t sz) {
-    C s = (C)0;
-    if (code & 1) s += ld<C>(x + o + ((i + 1) >> 1));
-    if (code & 2) s += ld<C>(x + o + ((i - 1) >> 1));
-    if (code & 4) s += ld<C>(x + o + sy + h);
-    if (code & 8) s += ld<C>(x + o - sy + h);
-    if (code & 16) s += ld<C>(x + o + sz + h);
-    if (code & 32) s += ld<C>(x + o - sz + h);
-    return s;
-}
+// A thread's slot in a tile (256 threads, one per slot): column h, row j, plane k offsets.
+// A warp covers TH consecutive columns of one row.
+__device__ __forceinline__ int slot_h() { return (int)threadIdx.x % TH; }
+__device__ __forceinline__ int slot_j() { return ((int)threadIdx.x / TH) % TY; }
+__device__ __forceinline__ int slot_k() { return (int)threadIdx.x / (TH * TY); }
 
 // ---- deterministic reductions ----
 // Block sums of K doubles (256 threads); the result is valid in thread 0.

@@ -1,0 +1,494 @@
+// The per-iteration kernels that stream a level's active tiles (sm_100a): start, one
+// colour of red-black Gauss-Seidel and the residual of the V-cycle, and the CG passes
+// (z.r, q = A p, the step, the true residual, A x).
+//
+// Load pattern. Every load a cell needs is issued at once, whatever its stencil code
+// says: the code is only read afterwards, to choose which loaded neighbours enter the
+// sums (in the reference's order, skipping the others, so the FP32 form still rounds as
+// the reference does). A thread therefore waits for one round trip per plane instead of
+// a chain of them (code, then data), and the next tile's id is fetched one step ahead.
+// Neighbour reads of level x arrays and the CG direction d may run past the array ends
+// at the box faces: those arrays are allocated with a zeroed guard of one plane plus a
+// margin on each side. The user's P is read with clamped indices.
+#pragma once
+
+#include "mpp_tiles.cuh"
+
+namespace mpp {
+
+// Guard elements on each side of the arrays read at neighbour offsets.
+__host__ __device__ constexpr int guard_of(int n1, int n2) { return (n1 * n2 + 64 + 63) / 64 * 64; }
+
+__device__ __forceinline__ int clampi(int p, int N) { return p < 0 ? 0 : (p >= N ? N - 1 : p); }
+
+// Walk this block's share of a level's tile list, the next tile id fetched one step ahead.
+#define FOR_TILES_PF(L, tile)                                                                  \
+    const int n_ = *(L).count, s_ = gridDim.x * TILES_PER_BLOCK;                                \
+    int t_ = blockIdx.x * TILES_PER_BLOCK + (int)(threadIdx.x / COLS);                          \
+    uint32_t tile = t_ < n_ ? (L).tiles[t_] : 0u;                                               \
+    for (uint32_t next_; t_ < n_; t_ += s_, tile = next_)                                       \
+        if ((next_ = (t_ + s_ < n_ ? (L).tiles[t_ + s_] : 0u)), true)
+
+// The six neighbours of a row-split cell in the order +x,-x,+y,-y,+z,-z: positions in the
+// other colour's half, o being the cell's own column there.
+template <class C, class T>
+__device__ __forceinline__ void load6(C (&v)[6], const T* x, int o, int ci, int sy, int sz) {
+    v[0] = ld<C>(x + o + ci);
+    v[1] = ld<C>(x + o + ci - 1);
+    v[2] = ld<C>(x + o + sy);
+    v[3] = ld<C>(x + o - sy);
+    v[4] = ld<C>(x + o + sz);
+    v[5] = ld<C>(x + o - sz);
+}
+// liquidsum (src/flip.jl:852-857): s = 0, then the LIQUID neighbours in order.
+template <class C>
+__device__ __forceinline__ C sum6(const C (&v)[6], uint8_t cd) {
+    C s = (C)0;
+#pragma unroll
+    for (int m = 0; m < 6; m++)
+        if (cd & (1u << m)) s += v[m];
+    return s;
+}
+
+// ---- the V-cycle (src/flip.jl:992-1014) on row-split levels ----
+
+// start_kernel! (src/flip.jl:965-973): colour-0 LIQUID cells get b/diag, every other cell 0.
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_start(Lev<typename Pr::M> L) {
+    using C = typename Pr::C;
+    const int sz = L.n1 * L.n2;
+    FOR_TILES_PF(L, tile) {
+        Col c;
+        if (!col_of(L, tile, c)) continue;
+        uint8_t cd[TZ];
+        C dv[TZ], bv[TZ];
+#pragma unroll
+        for (int q = 0; q < TZ; q++) {
+            cd[q] = 0;
+            if (q < c.kn) {
+                const int p = c.rb + q * sz + c.h;
+                cd[q] = L.code[p];
+                dv[q] = ld<C>(L.dg + p);
+                bv[q] = ld<C>(L.b + p);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < TZ; q++)
+            if (q < c.kn) {
+                const int p = c.rb + q * sz + c.h;
+                C v = (C)0;
+                if ((cd[q] & SELF) && dv[q] > (C)0) v = bv[q] / dv[q];
+                st(L.x + p, v);
+                st(L.x + p + L.H, (C)0);
+            }
+    }
+}
+
+// rbgs_kernel! (src/flip.jl:870-877): one colour of red-black Gauss-Seidel,
+// x = (b + sum_LIQ x_n) / diag on LIQUID cells of that colour.
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_rbgs(Lev<typename Pr::M> L, int colour) {
+    using C = typename Pr::C;
+    const int sy = L.n1, sz = L.n1 * L.n2;
+    const int own = colour * L.H, oth = (1 - colour) * L.H;
+    FOR_TILES_PF(L, tile) {
+        Col c;
+        if (!col_of(L, tile, c)) continue;
+        uint8_t cd[TZ];
+        C nb[TZ][6], dv[TZ], bv[TZ];
+#pragma unroll
+        for (int q = 0; q < TZ; q++) {
+            cd[q] = 0;
+            if (q < c.kn) {
+                const int rb = c.rb + q * sz;
+                cd[q] = L.code[rb + own + c.h];
+                dv[q] = ld<C>(L.dg + rb + own + c.h);
+                bv[q] = ld<C>(L.b + rb + own + c.h);
+                load6<C>(nb[q], L.x, rb + oth + c.h, ci_of(colour, c.j, c.k0 + q), sy, sz);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < TZ; q++)
+            if (cd[q] & SELF) {
+                const C s = sum6<C>(nb[q], cd[q]);
+                st(L.x + c.rb + q * sz + own + c.h, dv[q] > (C)0 ? (bv[q] + s) / dv[q] : (C)0);
+            }
+    }
+}
+
+// ---- vector form: 8 consecutive same-colour cells of a row per lane ----
+// A warp takes one tile: lane = (h chunk of 8) x (row j) x (plane k), so with TH = 32 a
+// tile is 4 x 4 x 2 lanes. Every array moves in 16-byte pieces (8 elements), which cuts
+// the memory instructions per cell by 8; it needs H to be a multiple of 8.
+constexpr int V8 = 8;
+constexpr int V8_LANES_H = TH / V8;  // 4
+static_assert(V8_LANES_H * TY * TZ == 32, "one warp per tile in the vector kernels");
+
+template <class T>
+struct Vec8 {
+    T v[V8];
+};
+template <class T>
+__device__ __forceinline__ Vec8<T> ld8(const T* p) {  // p 16-byte aligned
+    Vec8<T> r;
+    constexpr int n = (int)(sizeof(T) * V8 / 16);
+#pragma unroll
+    for (int q = 0; q < n; q++) reinterpret_cast<uint4*>(r.v)[q] = reinterpret_cast<const uint4*>(p)[q];
+    return r;
+}
+template <class T>
+__device__ __forceinline__ void st8(T* p, const Vec8<T>& r) {
+    constexpr int n = (int)(sizeof(T) * V8 / 16);
+#pragma unroll
+    for (int q = 0; q < n; q++) reinterpret_cast<uint4*>(p)[q] = reinterpret_cast<const uint4*>(r.v)[q];
+}
+
+// rbgs_kernel! (src/flip.jl:870-877), vector form. Own colour: code (8 bytes), diagonal,
+// b and x (kept where the cell is not LIQUID); other colour: the same 8 columns of this
+// row (the +x/-x neighbours, plus one element on each side) and of the rows at -+y, -+z.
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_rbgs_v8(Lev<typename Pr::M> L, int colour) {
+    using C = typename Pr::C;
+    using M = typename Pr::M;
+    const int sy = L.n1, sz = L.n1 * L.n2;
+    const int own = colour * L.H, oth = (1 - colour) * L.H;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = TPB / 32;
+    const int hq = lane % V8_LANES_H, lj = (lane / V8_LANES_H) % TY, lk = lane / (V8_LANES_H * TY);
+    const int n = *L.count;
+    for (int t = blockIdx.x * wpb + warp; t < n; t += gridDim.x * wpb) {
+        const uint32_t tile = L.tiles[t];
+        const int h = (int)(tile & 1023u) * TH + hq * V8, j = (int)((tile >> 10) & 1023u) * TY + lj,
+                  k = (int)(tile >> 20) * TZ + lk;
+        if (h >= L.H || j >= L.n2 || k >= L.n3) continue;
+        const int rb = (k * L.n2 + j) * L.n1;
+        const int p = rb + own + h, o = rb + oth + h;
+        const int ci = ci_of(colour, j, k);
+        const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
+        const Vec8<M> dv = ld8(L.dg + p), bv = ld8(L.b + p), xo = ld8(L.x + p);
+        const Vec8<M> xc = ld8(L.x + o), yp = ld8(L.x + o + sy), ym = ld8(L.x + o - sy), zp = ld8(L.x + o + sz),
+                      zm = ld8(L.x + o - sz);
+        const M xl = L.x[o - 1], xr = L.x[o + V8];
+        const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
+        Vec8<M> out;
+#pragma unroll
+        for (int q = 0; q < V8; q++) {
+            const int ip = q + ci, im = q + ci - 1;  // this cell's +x and -x columns
+            C nb[6];
+            nb[0] = ld<C>(ip < V8 ? &xc.v[ip] : &xr);
+            nb[1] = ld<C>(im >= 0 ? &xc.v[im] : &xl);
+            nb[2] = ld<C>(&yp.v[q]);
+            nb[3] = ld<C>(&ym.v[q]);
+            nb[4] = ld<C>(&zp.v[q]);
+            nb[5] = ld<C>(&zm.v[q]);
+            const C d = ld<C>(&dv.v[q]);
+            out.v[q] = xo.v[q];
+            if (cd[q] & SELF) st(&out.v[q], d > (C)0 ? (ld<C>(&bv.v[q]) + sum6<C>(nb, cd[q])) / d : (C)0);
+        }
+        st8(L.x + p, out);
+    }
+}
+
+// residual_kernel! (src/flip.jl:859-863): r = b - (diag x - sum_LIQ x_n) on LIQUID, else 0.
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_residual(Lev<typename Pr::M> L) {
+    using C = typename Pr::C;
+    const int sy = L.n1, sz = L.n1 * L.n2;
+    FOR_TILES_PF(L, tile) {
+        Col c;
+        if (!col_of(L, tile, c)) continue;
+#pragma unroll
+        for (int q = 0; q < TZ; q++) {
+            if (q >= c.kn) break;
+            const int rb = c.rb + q * sz;
+            uint8_t cd[2];
+            C nb[2][6], dv[2], bv[2], xv[2];
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                const int p = rb + cc * L.H + c.h;
+                cd[cc] = L.code[p];
+                dv[cc] = ld<C>(L.dg + p);
+                bv[cc] = ld<C>(L.b + p);
+                xv[cc] = ld<C>(L.x + p);
+                load6<C>(nb[cc], L.x, rb + (1 - cc) * L.H + c.h, ci_of(cc, c.j, c.k0 + q), sy, sz);
+            }
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                C v = (C)0;
+                if (cd[cc] & SELF) v = bv[cc] - (dv[cc] * xv[cc] - sum6<C>(nb[cc], cd[cc]));
+                st(L.r + rb + cc * L.H + c.h, v);
+            }
+        }
+    }
+}
+
+// ---- CG (src/flip.jl:1033-1111) over the fine level's active tiles ----
+
+// inner(s, z, r) after the V-cycle (src/flip.jl:1095-1096, 1105-1107): rho_new = z.r, then
+// beta = rho_new / rho (0 on the first pass). The flexible form also sums z.q and takes
+// the Polak-Ribiere beta = max(0, (rho_new - z.r_old) / rho) of the reference's flexible
+// CG (src/sflip.jl:1896-1897); as r = r_old - alpha q, z.r_old = rho_new + alpha z.q, so
+// no copy of r_old is kept.
+template <class Pr>
+__global__ void __launch_bounds__(TPB)
+    k_dot(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ q,
+          Scalars* sc, double* partials, unsigned* counter) {
+    if (sc->s.done) return;
+    const int sz = L.n1 * L.n2;
+    double acc[2] = {0.0, 0.0};
+    FOR_TILES_PF(L, tile) {
+        Col c;
+        if (!col_of(L, tile, c)) continue;
+        uint8_t cd[TZ][2];
+        double zv[TZ][2], rv[TZ][2], qv[TZ][2];
+#pragma unroll
+        for (int qq = 0; qq < TZ; qq++)
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                cd[qq][cc] = 0;
+                if (qq < c.kn) {
+                    const int p = c.rb + qq * sz + cc * L.H + c.h;
+                    cd[qq][cc] = L.code[p];
+                    zv[qq][cc] = ld<double>(L.x + p);
+                    rv[qq][cc] = (double)r[p];
+                    if constexpr (Pr::flexible) qv[qq][cc] = (double)q[p];
+                }
+            }
+#pragma unroll
+        for (int qq = 0; qq < TZ; qq++)
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++)
+                if (cd[qq][cc] & SELF) {
+                    acc[0] += zv[qq][cc] * rv[qq][cc];
+                    if constexpr (Pr::flexible) acc[1] += zv[qq][cc] * qv[qq][cc];
+                }
+    }
+    if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0) {
+        State& S = sc->s;
+        const double rho_new = rs<Pr>(acc[0]);
+        if (!finite_d(rho_new)) {
+            S.status = ST_NONFINITE;
+            S.done = 1;
+            return;
+        }
+        if constexpr (Pr::flexible) {
+            if (!(rho_new > 0.0)) {  // src/sflip.jl:1880,1896
+                S.status = ST_INDEFINITE;
+                S.done = 1;
+                return;
+            }
+            const double beta = S.it == 0 ? 0.0 : -S.alpha * acc[1] / S.rho;
+            S.beta = beta > 0.0 ? beta : 0.0;
+        } else {
+            S.beta = S.it == 0 ? 0.0 : dv<Pr>(rho_new, S.rho);
+        }
+        S.rho = rho_new;
+    }
+}
+
+// search_kernel! (src/flip.jl:1033-1054): p = z + beta d made where it is used, q = A p,
+// and p.q; then alpha = rho / p.q (src/flip.jl:1100).
+template <class Pr>
+__global__ void __launch_bounds__(TPB)
+    k_search(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ diag,
+             typename Pr::V* __restrict__ q, Scalars* sc, double* partials, unsigned* counter) {
+    using C = typename Pr::C;
+    if (sc->s.done) return;
+    const C beta = (C)sc->s.beta;
+    const bool first = sc->s.beta == 0.0;
+    const int sy = L.n1, sz = L.n1 * L.n2;
+    double acc[1] = {0.0};
+    FOR_TILES_PF(L, tile) {
+        Col c;
+        if (!col_of(L, tile, c)) continue;
+#pragma unroll
+        for (int qq = 0; qq < TZ; qq++) {
+            if (qq >= c.kn) break;
+            const int rb = c.rb + qq * sz;
+            uint8_t cd[2];
+            C zn[2][6], dn[2][6], zc[2], dc[2], gv[2];
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                const int p = rb + cc * L.H + c.h, o = rb + (1 - cc) * L.H + c.h, ci = ci_of(cc, c.j, c.k0 + qq);
+                cd[cc] = L.code[p];
+                gv[cc] = (C)diag[p];
+                zc[cc] = ld<C>(L.x + p);
+                load6<C>(zn[cc], L.x, o, ci, sy, sz);
+                if (!first) {
+                    dc[cc] = (C)dvec[p];
+                    load6<C>(dn[cc], dvec, o, ci, sy, sz);
+                }
+            }
+            C qv[2];
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                qv[cc] = (C)0;
+                if (cd[cc] & SELF) {
+                    const C pc = first ? zc[cc] : zc[cc] + beta * dc[cc];
+                    C a = (C)0;
+#pragma unroll
+                    for (int m = 0; m < 6; m++)
+                        if (cd[cc] & (1u << m)) a += first ? zn[cc][m] : zn[cc][m] + beta * dn[cc][m];
+                    qv[cc] = gv[cc] * pc - a;
+                    acc[0] += (double)pc * (double)qv[cc];
+                }
+            }
+            st(q + rb + c.h, qv[0]);
+            st(q + rb + L.H + c.h, qv[1]);
+        }
+    }
+    if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
+        State& S = sc->s;
+        S.pq = rs<Pr>(acc[0]);
+        if (!finite_d(S.pq)) {
+            S.status = ST_NONFINITE;
+            S.done = 1;
+        } else if (!(S.pq > 0.0)) {  // src/sflip.jl:1876-1877
+            S.status = ST_INDEFINITE;
+            S.done = 1;
+        } else {
+            S.alpha = dv<Pr>(S.rho, S.pq);
+        }
+    }
+}
+
+// advance_kernel! (src/flip.jl:1059-1073): d = z + beta d; P += alpha d; r -= alpha q; then
+// rnorm = sqrt(r.r) and the exit test rnorm <= tol |b| (src/flip.jl:1102-1103), or maxiter.
+// The 16-bit forms also store the (scaled) r in the V-cycle's precision for its next pass.
+template <class Pr>
+__global__ void __launch_bounds__(TPB)
+    k_advance(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ q,
+              typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
+              unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
+    using C = typename Pr::C;
+    if (sc->s.done) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(cond, use_cond, 0);
+        return;
+    }
+    const C beta = (C)sc->s.beta, alpha = (C)sc->s.alpha;
+    const bool first = sc->s.beta == 0.0;
+    const bool sep_b = (void*)L.b != (void*)r;
+    const C rsc = (C)sc->s.rscale;
+    const int sz = L.n1 * L.n2;
+    double acc[1] = {0.0};
+    FOR_TILES_PF(L, tile) {
+        Col c;
+        if (!col_of(L, tile, c)) continue;
+#pragma unroll
+        for (int qq = 0; qq < TZ; qq++) {
+            if (qq >= c.kn) break;
+            const int rb = c.rb + qq * sz;
+            uint8_t cd[2];
+            C zv[2], dd[2], qv[2], rv[2], pv[2];
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                const int p = rb + cc * L.H + c.h;
+                const int pn = rb + 2 * c.h + ci_of(cc, c.j, c.k0 + qq);
+                cd[cc] = L.code[p];
+                zv[cc] = ld<C>(L.x + p);
+                dd[cc] = (C)dvec[p];
+                qv[cc] = (C)q[p];
+                rv[cc] = (C)r[p];
+                pv[cc] = (C)P[pn];
+            }
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                if (!(cd[cc] & SELF)) continue;
+                const int p = rb + cc * L.H + c.h;
+                const int pn = rb + 2 * c.h + ci_of(cc, c.j, c.k0 + qq);
+                const C pc = first ? zv[cc] : zv[cc] + beta * dd[cc];
+                const C rl = rv[cc] - alpha * qv[cc];
+                st(dvec + p, pc);
+                st(P + pn, pv[cc] + alpha * pc);
+                st(r + p, rl);
+                if (sep_b) st(L.b + p, rl * rsc);
+                acc[0] += (double)rl * (double)rl;
+            }
+        }
+    }
+    if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
+        State& S = sc->s;
+        S.it += 1;
+        S.rnorm = sq<Pr>(acc[0]);
+        S.rscale = next_rscale(S.rnorm, S.nliq);
+        if (!finite_d(S.rnorm)) {
+            S.status = ST_NONFINITE;
+            S.done = 1;
+        } else if (S.rnorm <= S.target) {
+            S.status = ST_OK;
+            S.done = 1;
+        } else if (S.it >= sc->p.maxiter) {
+            S.status = ST_NOT_CONVERGED;
+            S.done = 1;
+        }
+        set_cond(cond, use_cond, !S.done);
+    }
+}
+
+// |b - A P| over the fine level: the true residual at exit (the reference's sparse
+// solver checks it the same way, src/fgmres.jl:101-103). P is the caller's array
+// (natural order, no guard), so its neighbour indices are clamped.
+template <class Pr>
+__global__ void __launch_bounds__(TPB)
+    k_true_residual(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ b, const typename Pr::V* __restrict__ diag,
+                    const typename Pr::V* __restrict__ P, typename Pr::V* __restrict__ rout, Scalars* sc,
+                    double* partials, unsigned* counter) {
+    using C = typename Pr::C;
+    const int n1 = L.n1, sz = L.n1 * L.n2, N = L.n1 * L.n2 * L.n3;
+    double acc[1] = {0.0};
+    FOR_TILES_PF(L, tile) {
+        Col c;
+        if (!col_of(L, tile, c)) continue;
+#pragma unroll
+        for (int qq = 0; qq < TZ; qq++) {
+            if (qq >= c.kn) break;
+            const int rb = c.rb + qq * sz;
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                const int p = rb + cc * L.H + c.h;
+                const int pn = rb + 2 * c.h + ci_of(cc, c.j, c.k0 + qq);
+                const uint8_t cd = L.code[p];
+                const C bv = (C)b[p], gv = (C)diag[p], pc = (C)P[pn];
+                C nb[6];
+                nb[0] = (C)P[clampi(pn + 1, N)];
+                nb[1] = (C)P[clampi(pn - 1, N)];
+                nb[2] = (C)P[clampi(pn + n1, N)];
+                nb[3] = (C)P[clampi(pn - n1, N)];
+                nb[4] = (C)P[clampi(pn + sz, N)];
+                nb[5] = (C)P[clampi(pn - sz, N)];
+                if (!(cd & SELF)) continue;
+                const C rv = bv - (gv * pc - sum6<C>(nb, cd));
+                if (rout) st(rout + p, rv);
+                acc[0] += (double)rv * (double)rv;
+            }
+        }
+    }
+    if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) sc->s.true_rr = acc[0];
+}
+
+// y = A x on the fine level (row-split, every cell of the active tiles; 0 off-liquid).
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_apply(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ x,
+                                               const typename Pr::V* __restrict__ diag, typename Pr::V* __restrict__ y) {
+    using C = typename Pr::C;
+    const int sy = L.n1, sz = L.n1 * L.n2;
+    FOR_TILES_PF(L, tile) {
+        Col c;
+        if (!col_of(L, tile, c)) continue;
+#pragma unroll
+        for (int qq = 0; qq < TZ; qq++) {
+            if (qq >= c.kn) break;
+            const int rb = c.rb + qq * sz;
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                const int p = rb + cc * L.H + c.h;
+                const uint8_t cd = L.code[p];
+                C nb[6];
+                load6<C>(nb, x, rb + (1 - cc) * L.H + c.h, ci_of(cc, c.j, c.k0 + qq), sy, sz);
+                const C v = (cd & SELF) ? (C)diag[p] * (C)x[p] - sum6<C>(nb, cd) : (C)0;
+                st(y + p, v);
+            }
+        }
+    }
+}
+
+}  // namespace mpp

@@ -1,0 +1,481 @@
+// The projection's per-iteration kernels (sm_100a): the V-cycle passes over each level's
+// active tiles, the small levels and the coarsest solve in one CTA, and the CG passes.
+//
+// Work layout. A tile is TH row-split columns (h) x TY rows (j) x TZ planes (k), i.e.
+// 2 TH x TY x TZ cells. Tile lists hold packed coordinates (th | tj << 10 | tk << 20). In
+// the column kernels a 256-thread block works on TILES_PER_BLOCK tiles at once; each
+// thread owns one (h, j) column of its tile and walks its TZ planes (both colours where
+// the pass covers both), first loading everything it needs for all planes, then
+// computing and storing. Indices are 32-bit.
+//
+// Arithmetic. Each cell's update is the reference kernel's, in its operation order
+// (sums over neighbours in the order +x,-x,+y,-y,+z,-z; restriction terms with a
+// innermost; prolongation terms m = 0..7), so the FP32 form rounds as the reference's
+// Float32 code does (the library is built with -fmad=false).
+#pragma once
+
+#include "mpp_base.cuh"
+
+namespace mpp {
+
+constexpr int COLS = TH * TY;                // threads per tile in the column kernels
+constexpr int TILES_PER_BLOCK = TPB / COLS;  // 4
+constexpr int BOTTOM_CELLS = 4096;           // levels this small are solved in one CTA (k_bottom)
+constexpr int BOTTOM_MAXLEV = 8;
+
+// ---- active-tile lists ----
+// One block per level compacts the level's tile flags in tile order (a block-wide scan),
+// so the lists, and the reductions over them, are the same on every run.
+struct TileTab {
+    int nlev;
+    int ntiles[16];
+    int GH[16], GJ[16];
+    uint8_t* flags[16];
+    uint32_t* tiles[16];
+    int* count[16];
+};
+__global__ void __launch_bounds__(1024) k_tilelists(TileTab tab) {
+    const int l = blockIdx.x;
+    if (l >= tab.nlev) return;
+    const int n = tab.ntiles[l], GH = tab.GH[l], GJ = tab.GJ[l];
+    const uint8_t* f = tab.flags[l];
+    const int chunk = (n + 1023) / 1024;
+    const int lo = min(n, (int)threadIdx.x * chunk), hi = min(n, lo + chunk);
+    int c = 0;
+    for (int t = lo; t < hi; t++) c += f[t] != 0;
+    __shared__ int sc[1024];
+    sc[threadIdx.x] = c;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int v = threadIdx.x >= (unsigned)o ? sc[threadIdx.x - o] : 0;
+        __syncthreads();
+        sc[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int w = sc[threadIdx.x] - c;
+    for (int t = lo; t < hi; t++)
+        if (f[t]) {
+            const uint32_t th = (uint32_t)(t % GH), tj = (uint32_t)((t / GH) % GJ), tk = (uint32_t)(t / (GH * GJ));
+            tab.tiles[l][w++] = th | (tj << 10) | (tk << 20);
+        }
+    if (threadIdx.x == 1023) *tab.count[l] = sc[1023];
+}
+
+// A thread's column: row-split column h, row j, planes k0 .. k0+kn-1; rb = start of row (j, k0).
+struct Col {
+    int h, j, k0, kn, rb;
+};
+template <class M>
+__device__ __forceinline__ bool col_of(const Lev<M>& L, uint32_t tile, Col& c) {
+    const int lane = threadIdx.x & (COLS - 1);
+    c.h = (int)(tile & 1023u) * TH + (lane & (TH - 1));
+    c.j = (int)((tile >> 10) & 1023u) * TY + lane / TH;
+    c.k0 = (int)(tile >> 20) * TZ;
+    c.kn = min(TZ, L.n3 - c.k0);
+    c.rb = (c.k0 * L.n2 + c.j) * L.n1;
+    return c.h < L.H && c.j < L.n2;
+}
+// colour-c cell of the column at plane k: i = 2h + ci
+__device__ __forceinline__ int ci_of(int c, int j, int k) { return (c + j + k + 1) & 1; }
+
+#define FOR_TILES(L)                                                                                  \
+    for (int t_ = blockIdx.x * TILES_PER_BLOCK + (int)(threadIdx.x / COLS), n_ = *(L).count; t_ < n_; \
+         t_ += gridDim.x * TILES_PER_BLOCK)
+
+// ---- the V-cycle (src/flip.jl:992-1014) on row-split levels ----
+
+// weightB (src/flip.jl:891): (1, 3, 3, 1) / 8.
+template <class C>
+__device__ __forceinline__ C wB(int a) {
+    return (a == 1 || a == 2) ? (C)0.375f : (C)0.125f;
+}
+
+// restrict_kernel! (src/flip.jl:894-906): b_c = 4 sum w_a w_b w_c r_f over the LIQUID fine
+// cells of the 4x4x4 block (a fastest); the scaled (16-bit) forms drop the factor 4.
+// One block per coarse tile: the tile's fine region (RX x RY x RZ cells) is staged in
+// shared memory, non-LIQUID cells as zero, then each thread sums its two coarse cells.
+constexpr int RX = 4 * TH + 2, RY = 2 * TY + 2, RZ = 2 * TZ + 2;
+
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_restrict(Lev<typename Pr::M> F, Lev<typename Pr::M> L) {
+    using C = typename Pr::C;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int n = *L.count;
+    const int lh = slot_h(), lj = slot_j(), lk = slot_k();
+    for (int t = blockIdx.x; t < n; t += gridDim.x) {
+        const uint32_t tile = L.tiles[t];
+        const int th = (int)(tile & 1023u), tj = (int)((tile >> 10) & 1023u), tk = (int)(tile >> 20);
+        const int i0 = 4 * TH * th - 1, j0 = 2 * TY * tj - 1, k0 = 2 * TZ * tk - 1;
+        __syncthreads();
+        for (int e = threadIdx.x; e < RX * RY * RZ; e += TPB) {
+            const int ii = e % RX, jj = (e / RX) % RY, kk = e / (RX * RY);
+            const int i = i0 + ii, j = j0 + jj, k = k0 + kk;
+            C v = (C)0;
+            if (i >= 0 && i < F.n1 && j >= 0 && j < F.n2 && k >= 0 && k < F.n3) {
+                const int p = (int)F.pos(i, j, k);
+                const uint8_t cd = F.code[p];  // both loads in flight at once; the select
+                const C rv = ld<C>(F.r + p);   // keeps a stale value of a non-LIQUID cell out
+                v = (cd & SELF) ? rv : (C)0;
+            }
+            sm[e] = v;
+        }
+        __syncthreads();
+        const int h = th * TH + lh, J = tj * TY + lj, K = tk * TZ + lk;
+        if (h < L.H && J < L.n2 && K < L.n3) {
+            const int rb = (K * L.n2 + J) * L.n1;
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                const int p = rb + cc * L.H + h;
+                C v = (C)0;
+                if (L.code[p] & SELF) {
+                    const int il = 2 * (2 * lh + ci_of(cc, J, K));
+                    C s = (C)0;
+#pragma unroll
+                    for (int c3 = 0; c3 < 4; c3++)
+#pragma unroll
+                        for (int b3 = 0; b3 < 4; b3++)
+#pragma unroll
+                            for (int a3 = 0; a3 < 4; a3++)
+                                s += wB<C>(a3) * wB<C>(b3) * wB<C>(c3) *
+                                     sm[((2 * lk + c3) * RY + 2 * lj + b3) * RX + il + a3];
+                    v = Pr::scaled ? s : (C)4 * s;
+                }
+                st(L.b + p, v);
+            }
+        }
+    }
+}
+
+// prolongweights (src/flip.jl:908-911), 0-based.
+template <class C>
+__device__ __forceinline__ void pweights(int i, int& c0, C& w0, int& c1, C& w1) {
+    const int I = i >> 1;
+    if ((i & 1) == 0) { c0 = I - 1; w0 = (C)0.25f; c1 = I; w1 = (C)0.75f; }
+    else { c0 = I; w0 = (C)0.75f; c1 = I + 1; w1 = (C)0.25f; }
+}
+
+// prolong_kernel! (src/flip.jl:914-929): x_f += sum over the LIQUID coarse cells of the
+// trilinear weights times x_c (m = 0..7; x4 in the scaled forms). Each tile's PX x PY x PZ
+// coarse cells are staged in shared memory, non-LIQUID as zero. The coarse level is
+// row-split, or the bottom level in natural order (`cnat`).
+constexpr int PX = TH + 2, PY = TY / 2 + 2, PZ = TZ / 2 + 2;
+
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_prolong(Lev<typename Pr::M> L, Lev<typename Pr::M> Cl, int cnat) {
+    using C = typename Pr::C;
+    __shared__ C sm[TILES_PER_BLOCK][PZ][PY][PX];
+    const int n = *L.count;
+    const int sub = threadIdx.x / COLS;
+    const int sz = L.n1 * L.n2;
+    for (int t0 = blockIdx.x * TILES_PER_BLOCK; t0 < n; t0 += gridDim.x * TILES_PER_BLOCK) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < TILES_PER_BLOCK * PX * PY * PZ; e += TPB) {
+            const int s = e / (PX * PY * PZ), r = e % (PX * PY * PZ);
+            const int ii = r % PX, jj = (r / PX) % PY, kk = r / (PX * PY);
+            C v = (C)0;
+            if (t0 + s < n) {
+                const uint32_t tile = L.tiles[t0 + s];
+                const int I = (int)(tile & 1023u) * TH - 1 + ii;
+                const int J = (int)((tile >> 10) & 1023u) * (TY / 2) - 1 + jj;
+                const int K = (int)(tile >> 20) * (TZ / 2) - 1 + kk;
+                if (I >= 0 && I < Cl.n1 && J >= 0 && J < Cl.n2 && K >= 0 && K < Cl.n3) {
+                    const int q = cnat ? (int)Cl.nat(I, J, K) : (int)Cl.pos(I, J, K);
+                    const uint8_t cd = Cl.code[q];  // natural or row-split, as the level is stored
+                    const C xv = ld<C>(Cl.x + q);
+                    v = (cd & SELF) ? xv : (C)0;
+                }
+            }
+            sm[s][kk][jj][ii] = v;
+        }
+        __syncthreads();
+        const int t = t0 + sub;
+        if (t >= n) continue;
+        Col c;
+        if (!col_of(L, L.tiles[t], c)) continue;
+        const int Ib = (int)(L.tiles[t] & 1023u) * TH - 1;  // coarse origin of the staged region
+        const int Jb = c.j - (c.j & (TY - 1));
+        int b0, b1;
+        C wb0, wb1;
+        pweights<C>(c.j, b0, wb0, b1, wb1);
+        b0 = b0 - (Jb / 2 - 1);
+        b1 = b1 - (Jb / 2 - 1);
+        C v[2][TZ];
+        bool live[2][TZ];
+#pragma unroll
+        for (int q = 0; q < TZ; q++) {
+            const int k = c.k0 + q;
+            int k0, k1;
+            C wc0, wc1;
+            pweights<C>(k, k0, wc0, k1, wc1);
+            k0 -= c.k0 / 2 - 1;
+            k1 -= c.k0 / 2 - 1;
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                live[cc][q] = false;
+                v[cc][q] = (C)0;
+                if (q < c.kn) {
+                    const int p = c.rb + q * sz + cc * L.H + c.h;
+                    if (L.code[p] & SELF) {
+                        live[cc][q] = true;
+                        const int i = 2 * c.h + ci_of(cc, c.j, k);
+                        int a0, a1;
+                        C wa0, wa1;
+                        pweights<C>(i, a0, wa0, a1, wa1);
+                        a0 -= Ib;
+                        a1 -= Ib;
+                        C s = (C)0;
+#pragma unroll
+                        for (int m = 0; m < 8; m++) {
+                            const int A = (m & 1) ? a1 : a0, B = (m & 2) ? b1 : b0, Kc = (m & 4) ? k1 : k0;
+                            const C wa = (m & 1) ? wa1 : wa0, wb = (m & 2) ? wb1 : wb0, wc = (m & 4) ? wc1 : wc0;
+                            s += wa * wb * wc * sm[sub][Kc][B][A];
+                        }
+                        v[cc][q] = ld<C>(L.x + p) + (Pr::scaled ? (C)4 * s : s);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < TZ; q++)
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++)
+                if (live[cc][q]) st(L.x + c.rb + q * sz + cc * L.H + c.h, v[cc][q]);
+    }
+}
+
+// ---- the small levels and the coarsest, in one CTA ----
+// Levels lb .. L-1 (each at most a few thousand cells) live in shared memory in natural
+// order for the whole of their part of the V-cycle: the restriction into lb from the
+// level above (restrict_kernel!), then for each level start, the down sweeps, residual
+// and restriction, the coarsest solve (coarse_kernel!, src/flip.jl:935-962: `sweeps`
+// red-black sweeps from zero and as many in reverse colour order, the accumulator
+// starting at b, the diagonal the count of non-SOLID neighbours), and back up:
+// prolongation and the up sweeps. Level lb's correction is written to global memory.
+struct BotLev {
+    int n1, n2, n3;
+    const uint8_t* code;  // stencil codes, natural order, global (k_level)
+    const uint8_t* dc;    // non-SOLID neighbour counts, natural order, global (k_level)
+    int ox, ob, orr, ocode, odc;  // shared-memory offsets (bytes)
+};
+struct BotArgs {
+    int nl;  // levels in shared memory, the last one the coarsest
+    int sweeps, coarse;
+    BotLev lv[BOTTOM_MAXLEV];
+};
+
+template <class Pr>
+__global__ void __launch_bounds__(1024) k_bottom(const typename Pr::C* __restrict__ bin, typename Pr::M* __restrict__ xout,
+                                                 BotArgs a) {
+    using C = typename Pr::C;
+    using CC = typename Pr::CC;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    const int T = blockDim.x, tid = threadIdx.x;
+    // codes and non-SOLID neighbour counts of every level, and level lb's right-hand side
+    // (restricted from the level above by k_restrict_bottom)
+    for (int l = 0; l < a.nl; l++) {
+        const BotLev& B = a.lv[l];
+        const int N = B.n1 * B.n2 * B.n3;
+        uint8_t* code = smraw + B.ocode;
+        uint8_t* dc = smraw + B.odc;
+        for (int c = tid; c < N; c += T) {
+            code[c] = B.code[c];
+            dc[c] = B.dc[c];
+        }
+    }
+    {
+        const BotLev& B = a.lv[0];
+        const int N = B.n1 * B.n2 * B.n3;
+        if (a.nl == 1) {
+            CC* b = reinterpret_cast<CC*>(smraw + B.ob);
+            for (int c = tid; c < N; c += T) b[c] = (CC)bin[c];
+        } else {
+            C* b = reinterpret_cast<C*>(smraw + B.ob);
+            for (int c = tid; c < N; c += T) b[c] = bin[c];
+        }
+    }
+    __syncthreads();
+    // restriction between shared-memory levels
+    auto restrict_into = [&](int l, auto* bout, auto getf) {
+        const BotLev& B = a.lv[l];
+        const int N = B.n1 * B.n2 * B.n3;
+        const uint8_t* code = smraw + B.ocode;
+        using T2 = typename std::remove_pointer<decltype(bout)>::type;
+        for (int c = tid; c < N; c += T) {
+            T2 v = (T2)0;
+            if (code[c] & SELF) {
+                const int I = c % B.n1, J = (c / B.n1) % B.n2, K = c / (B.n1 * B.n2);
+                C s = (C)0;
+                for (int c3 = 0; c3 < 4; c3++)
+                    for (int b3 = 0; b3 < 4; b3++)
+#pragma unroll
+                        for (int a3 = 0; a3 < 4; a3++)
+                            s += wB<C>(a3) * wB<C>(b3) * wB<C>(c3) * getf(2 * I + a3 - 1, 2 * J + b3 - 1, 2 * K + c3 - 1);
+                v = (T2)(Pr::scaled ? s : (C)4 * s);
+            }
+            bout[c] = v;
+        }
+    };
+    // smoothing passes on a shared-memory level
+    auto sweep = [&](int l, int colour) {
+        const BotLev& B = a.lv[l];
+        const int N = B.n1 * B.n2 * B.n3, sy = B.n1, sz = B.n1 * B.n2;
+        const uint8_t* code = smraw + B.ocode;
+        const uint8_t* dc = smraw + B.odc;
+        C* x = reinterpret_cast<C*>(smraw + B.ox);
+        const C* b = reinterpret_cast<const C*>(smraw + B.ob);
+        for (int c = tid; c < N; c += T) {
+            const uint8_t cd = code[c];
+            if (!(cd & SELF)) continue;
+            const int i = c % B.n1, j = (c / B.n1) % B.n2, k = c / sz;
+            if (((i + j + k + 1) & 1) != colour) continue;
+            C s = (C)0;
+            if (cd & 1) s += x[c + 1];
+            if (cd & 2) s += x[c - 1];
+            if (cd & 4) s += x[c + sy];
+            if (cd & 8) s += x[c - sy];
+            if (cd & 16) s += x[c + sz];
+            if (cd & 32) s += x[c - sz];
+            const C d = (C)dc[c];
+            x[c] = d > (C)0 ? (b[c] + s) / d : (C)0;
+        }
+        __syncthreads();
+    };
+    const int sw = a.sweeps;
+    for (int l = 0; l + 1 < a.nl; l++) {
+        const BotLev& B = a.lv[l];
+        const int N = B.n1 * B.n2 * B.n3, sy = B.n1, sz = B.n1 * B.n2;
+        const uint8_t* code = smraw + B.ocode;
+        const uint8_t* dc = smraw + B.odc;
+        C* x = reinterpret_cast<C*>(smraw + B.ox);
+        C* b = reinterpret_cast<C*>(smraw + B.ob);
+        C* r = reinterpret_cast<C*>(smraw + B.orr);
+        for (int c = tid; c < N; c += T) {  // start_kernel!
+            C v = (C)0;
+            const int i = c % B.n1, j = (c / B.n1) % B.n2, k = c / sz;
+            if (((i + j + k + 1) & 1) == 0 && (code[c] & SELF)) {
+                const C d = (C)dc[c];
+                if (d > (C)0) v = b[c] / d;
+            }
+            x[c] = v;
+        }
+        __syncthreads();
+        for (int q = 1; q < 2 * sw; q++) sweep(l, q & 1);  // down: colours 1, 0, 1, ...
+        for (int c = tid; c < N; c += T) {  // residual_kernel!
+            const uint8_t cd = code[c];
+            C v = (C)0;
+            if (cd & SELF) {
+                C s = (C)0;
+                if (cd & 1) s += x[c + 1];
+                if (cd & 2) s += x[c - 1];
+                if (cd & 4) s += x[c + sy];
+                if (cd & 8) s += x[c - sy];
+                if (cd & 16) s += x[c + sz];
+                if (cd & 32) s += x[c - sz];
+                v = b[c] - ((C)dc[c] * x[c] - s);
+            }
+            r[c] = v;
+        }
+        __syncthreads();
+        const uint8_t* fcode = code;
+        auto getL = [&](int i, int j, int k) -> C {
+            if (i < 0 || i >= B.n1 || j < 0 || j >= B.n2 || k < 0 || k >= B.n3) return (C)0;
+            const int p = i + B.n1 * (j + B.n2 * k);
+            return (fcode[p] & SELF) ? r[p] : (C)0;
+        };
+        if (l + 2 == a.nl) restrict_into(l + 1, reinterpret_cast<CC*>(smraw + a.lv[l + 1].ob), getL);
+        else restrict_into(l + 1, reinterpret_cast<C*>(smraw + a.lv[l + 1].ob), getL);
+        __syncthreads();
+    }
+    {  // coarse_kernel!
+        const BotLev& B = a.lv[a.nl - 1];
+        const int N = B.n1 * B.n2 * B.n3, sy = B.n1, sz = B.n1 * B.n2;
+        const uint8_t* code = smraw + B.ocode;
+        const uint8_t* dc = smraw + B.odc;
+        CC* x = reinterpret_cast<CC*>(smraw + B.ox);
+        const CC* b = reinterpret_cast<const CC*>(smraw + B.ob);
+        for (int c = tid; c < N; c += T) x[c] = (CC)0;
+        __syncthreads();
+        // one cell per thread (N <= 1024): the threads that own cells sync among themselves
+        const int nthreads = ((N + 31) / 32) * 32;
+        if (tid < nthreads) {
+            const bool mine = tid < N;
+            uint8_t cd = 0;
+            int mycol = 0;
+            CC bi = (CC)0, d = (CC)0, rd = (CC)0;
+            if (mine) {
+                cd = code[tid];
+                const int i = tid % B.n1, j = (tid / B.n1) % B.n2, k = tid / sz;
+                mycol = (i + j + k + 1) & 1;
+                bi = b[tid];
+                d = (CC)dc[tid];
+                rd = d > (CC)0 ? (CC)1 / d : (CC)0;
+            }
+            for (int s = 1; s <= 2 * a.coarse; s++)
+                for (int half = 0; half <= 1; half++) {
+                    const int colour = s <= a.coarse ? half : 1 - half;
+                    if (mine && (cd & SELF) && mycol == colour) {
+                        CC acc = bi;
+                        if (cd & 1) acc += x[tid + 1];
+                        if (cd & 2) acc += x[tid - 1];
+                        if (cd & 4) acc += x[tid + sy];
+                        if (cd & 8) acc += x[tid - sy];
+                        if (cd & 16) acc += x[tid + sz];
+                        if (cd & 32) acc += x[tid - sz];
+                        if constexpr (std::is_same<CC, float>::value) x[tid] = d > (CC)0 ? acc / d : (CC)0;
+                        else x[tid] = acc * rd;  // FP64 coarsest of the 16-bit forms
+                    }
+                    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+                }
+        }
+        __syncthreads();
+    }
+    // back up: prolongation and the up sweeps
+    for (int l = a.nl - 2; l >= 0; l--) {
+        const BotLev& B = a.lv[l];
+        const BotLev& Bc = a.lv[l + 1];
+        const int N = B.n1 * B.n2 * B.n3;
+        const uint8_t* code = smraw + B.ocode;
+        const uint8_t* ccode = smraw + Bc.ocode;
+        C* x = reinterpret_cast<C*>(smraw + B.ox);
+        const bool coarsest = l + 2 == a.nl;
+        for (int c = tid; c < N; c += T) {
+            if (!(code[c] & SELF)) continue;
+            const int i = c % B.n1, j = (c / B.n1) % B.n2, k = c / (B.n1 * B.n2);
+            int a0, a1, b0, b1, k0, k1;
+            C wa0, wa1, wb0, wb1, wc0, wc1;
+            pweights<C>(i, a0, wa0, a1, wa1);
+            pweights<C>(j, b0, wb0, b1, wb1);
+            pweights<C>(k, k0, wc0, k1, wc1);
+            C s = (C)0;
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                const int A = (m & 1) ? a1 : a0, Bj = (m & 2) ? b1 : b0, K = (m & 4) ? k1 : k0;
+                const C wa = (m & 1) ? wa1 : wa0, wb = (m & 2) ? wb1 : wb0, wc = (m & 4) ? wc1 : wc0;
+                if (A < 0 || A >= Bc.n1 || Bj < 0 || Bj >= Bc.n2 || K < 0 || K >= Bc.n3) continue;
+                const int q = A + Bc.n1 * (Bj + Bc.n2 * K);
+                if (!(ccode[q] & SELF)) continue;
+                const C xc = coarsest ? (C)reinterpret_cast<const CC*>(smraw + Bc.ox)[q]
+                                      : reinterpret_cast<const C*>(smraw + Bc.ox)[q];
+                s += wa * wb * wc * xc;
+            }
+            x[c] = x[c] + (Pr::scaled ? (C)4 * s : s);
+        }
+        __syncthreads();
+        for (int q = 0; q < 2 * sw; q++) sweep(l, (q & 1) ? 0 : 1);  // up: colours 1, 0, 1, 0, ...
+    }
+    // level lb's correction out, natural order
+    {
+        const BotLev& B = a.lv[0];
+        const int N = B.n1 * B.n2 * B.n3;
+        if (a.nl == 1) {
+            const CC* x = reinterpret_cast<const CC*>(smraw + B.ox);
+            for (int c = tid; c < N; c += T) st(xout + c, x[c]);
+        } else {
+            const C* x = reinterpret_cast<const C*>(smraw + B.ox);
+            for (int c = tid; c < N; c += T) st(xout + c, x[c]);
+        }
+    }
+}
+
+}  // namespace mpp

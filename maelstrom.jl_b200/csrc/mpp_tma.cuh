@@ -1,0 +1,179 @@
+// The red-black smoother as a TMA pipeline (sm_100a).
+//
+// rbgs_kernel! (src/flip.jl:870-877) streams three arrays of its own colour (b, the
+// diagonal, the stencil code) and the other colour's x with a one-cell halo. Issued as
+// plain loads, each thread waits on a chain of dependent loads (tile id -> codes ->
+// data) and HBM stays mostly idle. Here one thread per CTA moves whole tiles into shared
+// memory with cp.async.bulk.tensor (no multicast), S tiles ahead of the 256 threads that
+// compute, so every SM keeps tens of kilobytes of loads in flight.
+//
+// Tensor maps view a row-split level array as 4-D (h, colour, j, k) with h innermost.
+// Boxes: own colour {TH, 1, TY, TZ} at (TH th, c, TY tj, TZ tk); the other colour's x
+// {TH + 2 PAD, 1, TY + 2, TZ + 2} at (TH th - PAD, 1 - c, TY tj - 1, TZ tk - 1), PAD = 16 bytes of
+// elements so the innermost coordinate times the element size stays a multiple of 16
+// bytes. Coordinates outside the array read as zero; the stencil code (also zero there)
+// keeps them out of every sum.
+#pragma once
+
+#include <cuda.h>
+
+#include "mpp_stream.cuh"
+
+namespace mpp {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// A wait that gives up: MBAR_SPINS polls of try_wait (each returns within a bounded,
+// hardware-defined time), then false.
+constexpr int MBAR_SPINS = 1 << 18;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (int it = 0; it < MBAR_SPINS; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, uint64_t* bar, int c0, int c1, int c2,
+                                            int c3) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// The tensor maps of one row-split level.
+struct TmaLev {
+    CUtensorMap xh;    // x, box {TH + 2 PAD, 1, TY + 2, TZ + 2}
+    CUtensorMap b;     // b, box {TH, 1, TY, TZ}
+    CUtensorMap dg;    // smoother diagonal, box {TH, 1, TY, TZ}
+    CUtensorMap code;  // stencil codes, box {TH, 1, TY, TZ}
+};
+
+template <class M>
+struct TmaGeom {
+    static constexpr int PAD = 16 / (int)sizeof(M);
+    static constexpr int XW = TH + 2 * PAD;
+    static constexpr int XB = XW * (TY + 2) * (TZ + 2) * (int)sizeof(M);
+    static constexpr int BB = TH * TY * TZ * (int)sizeof(M);
+    static constexpr int CB = TH * TY * TZ;
+    static constexpr int up(int x) { return (x + 127) / 128 * 128; }
+    static constexpr int OXB = 0, OBB = up(XB), ODB = OBB + up(BB), OCB = ODB + up(BB);
+    static constexpr int STAGE = OCB + up(CB);
+    static constexpr int STAGES = 4;
+    static constexpr int SMEM = STAGES * STAGE + 128;  // + room to align the first stage
+    static constexpr uint32_t TX = (uint32_t)(XB + 2 * BB + CB);
+};
+
+// rbgs_kernel! on one row-split level, tiles streamed by TMA. Grid: persistent, block b
+// takes tiles b, b + G, b + 2G, ... of the level's active list. On a wait that times out
+// the block records `fault`, waits (bounded) for the copies it still has in flight, and
+// returns.
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_rbgs_tma(Lev<typename Pr::M> L, int colour, const __grid_constant__ TmaLev tm,
+                                                  int* fault) {
+    using C = typename Pr::C;
+    using M = typename Pr::M;
+    using G = TmaGeom<M>;
+    constexpr int S = G::STAGES;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    // TMA destinations 128-byte aligned whatever the dynamic region's start (SMEM has room)
+    unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~(uintptr_t)127);
+    __shared__ __align__(8) uint64_t full[S];
+    __shared__ uint32_t tid_of[S];
+    const int n = *L.count;
+    const int GB = gridDim.x;
+    const int mine = n > (int)blockIdx.x ? (n - 1 - (int)blockIdx.x) / GB + 1 : 0;
+    if (mine == 0) return;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int i) {  // thread 0 only
+        const int s = i % S;
+        const uint32_t tile = L.tiles[blockIdx.x + (size_t)i * GB];
+        tid_of[s] = tile;
+        const int h0 = (int)(tile & 1023u) * TH, j0 = (int)((tile >> 10) & 1023u) * TY, k0 = (int)(tile >> 20) * TZ;
+        unsigned char* stg = sm + s * G::STAGE;
+        mbar_expect_tx(&full[s], G::TX);
+        tma_load_4d(stg + G::OXB, &tm.xh, &full[s], h0 - G::PAD, 1 - colour, j0 - 1, k0 - 1);
+        tma_load_4d(stg + G::OBB, &tm.b, &full[s], h0, colour, j0, k0);
+        tma_load_4d(stg + G::ODB, &tm.dg, &full[s], h0, colour, j0, k0);
+        tma_load_4d(stg + G::OCB, &tm.code, &full[s], h0, colour, j0, k0);
+    };
+    int issued = 0;
+    if (threadIdx.x == 0)
+        for (; issued < S && issued < mine; issued++) issue(issued);
+    const int lh = slot_h(), lj = slot_j(), lk = slot_k();
+    const int xi = lh + G::PAD;  // this slot's column in the halo box
+    const int H = L.H, sz = L.n1 * L.n2;
+    int i = 0;
+    bool bad = false;
+    for (; i < mine; i++) {
+        const int s = i % S;
+        const bool ok = mbar_wait_bounded(&full[s], (uint32_t)((i / S) & 1));
+        if (__syncthreads_or(!ok)) {
+            bad = true;
+            break;
+        }
+        const unsigned char* stg = sm + s * G::STAGE;
+        const M* xh = reinterpret_cast<const M*>(stg + G::OXB);
+        const M* bb = reinterpret_cast<const M*>(stg + G::OBB);
+        const M* dd = reinterpret_cast<const M*>(stg + G::ODB);
+        const uint8_t* cc = stg + G::OCB;
+        const int own = (lk * TY + lj) * TH + lh;
+        const uint8_t cd = cc[own];
+        if (cd & SELF) {
+            const uint32_t tile = tid_of[s];
+            const int h = (int)(tile & 1023u) * TH + lh, j = (int)((tile >> 10) & 1023u) * TY + lj,
+                      k = (int)(tile >> 20) * TZ + lk;
+            const int ci = ci_of(colour, j, k);
+            auto X = [&](int kk, int jj, int ii) { return ld<C>(xh + (kk * (TY + 2) + jj) * G::XW + ii); };
+            C s2 = (C)0;
+            if (cd & 1) s2 += X(lk + 1, lj + 1, xi + ci);
+            if (cd & 2) s2 += X(lk + 1, lj + 1, xi + ci - 1);
+            if (cd & 4) s2 += X(lk + 1, lj + 2, xi);
+            if (cd & 8) s2 += X(lk + 1, lj, xi);
+            if (cd & 16) s2 += X(lk + 2, lj + 1, xi);
+            if (cd & 32) s2 += X(lk, lj + 1, xi);
+            const C d = ld<C>(dd + own);
+            const C v = d > (C)0 ? (ld<C>(bb + own) + s2) / d : (C)0;
+            st(L.x + (k * L.n2 + j) * L.n1 + colour * H + h, v);
+        }
+        __syncthreads();  // stage s fully read
+        if (threadIdx.x == 0 && issued < mine) {
+            fence_proxy_async_smem();
+            issue(issued);
+            issued++;
+        }
+    }
+    if (bad) {
+        if (threadIdx.x == 0) {
+            atomicExch(fault, 1);
+            // copies still in flight: tiles i .. i + S - 1 that were issued
+            for (int q = i; q < issued; q++) mbar_wait_bounded(&full[q % S], (uint32_t)((q / S) & 1));
+        }
+        __syncthreads();
+    }
+    (void)sz;
+}
+
+}  // namespace mpp
