@@ -118,6 +118,7 @@ struct mpp_ctx {
     bool tma_ok[MAXLEV];
     int tma_blocks;  // persistent grid of k_rbgs_tma
     int rbgs_mode;   // which smoother form runs on row-split levels (MPP_RBGS: v8, tma, column)
+    int vec_on;      // vector forms of the other passes (off with MPP_RBGS=column)
     // profiler
     int prof_on;
     std::vector<ProfRec> pending;
@@ -285,6 +286,13 @@ struct Run {
     int fam = 0, lvl = 0;
 
     unsigned* cnt(int i) { return c->counters + i; }
+    // vector (8 cells per lane) kernels on level l: rows of whole 8-element chunks
+    bool vec(int l) const { return c->vec_on && c->lv[l].H % V8 == 0; }
+    int grid_w(int l) const {
+        const int wpb = TPB / 32, cap = c->nsm * MAXBLOCKS_PER_SM;
+        const int g = (c->lv[l].ntiles + wpb - 1) / wpb;
+        return g < cap ? (g > 0 ? g : 1) : cap;
+    }
 
     void beg(int f, int l) {
         nk++;
@@ -312,6 +320,14 @@ struct Run {
     // The fine set-up pass, the coarse levels and the tile lists.
     void setup(const SetupIn<V>& in, cudaGraphConditionalHandle cond, int use_cond) {
         cudaMemsetAsync(c->tflag_all, 0, c->tflag_bytes, s);
+        // Level residuals and coarse corrections start at zero each projection, so every cell
+        // outside the active tiles reads as zero in the staged restriction/prolongation.
+        const size_t ms = msize(c->prec);
+        for (int l = 0; l < c->lb; l++) {
+            const size_t Nl = (size_t)c->lv[l].n[0] * c->lv[l].n[1] * c->lv[l].n[2];
+            cudaMemsetAsync(c->lv[l].r, 0, ms * Nl, s);
+            if (l > 0) cudaMemsetAsync(c->lv[l].x, 0, ms * Nl, s);
+        }
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
         beg(F_SETUP, -1);
         k_setup<Pr><<<grid_cells(c, N), TPB, 0, s>>>(in, view<M>(c, 0), (V*)c->diag, (V*)c->bvec, (V*)c->r, c->sc,
@@ -371,11 +387,13 @@ struct Run {
         const int lb = c->lb;
         for (int l = 0; l < lb; l++) {
             beg(F_START, l);
-            k_start<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l));
+            if (vec(l)) k_start_v8<Pr><<<grid_w(l), TPB, 0, s>>>(view<M>(c, l));
+            else k_start<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l));
             end();
             smooth(l, down);
             beg(F_RESID, l);
-            k_residual<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l));
+            if (vec(l)) k_residual_v8<Pr><<<grid_w(l), TPB, 0, s>>>(view<M>(c, l));
+            else k_residual<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l));
             end();
             if (l + 1 < lb) {
                 beg(F_RESTRICT, l + 1);
@@ -398,7 +416,10 @@ struct Run {
         end();
         for (int l = lb - 1; l >= 0; l--) {
             beg(F_PROLONG, l);
-            k_prolong<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l), view<M>(c, l + 1), l + 1 == lb ? 1 : 0);
+            if (vec(l))
+                k_prolong_v8<Pr><<<grid_w(l), TPB, 0, s>>>(view<M>(c, l), view<M>(c, l + 1), l + 1 == lb ? 1 : 0);
+            else
+                k_prolong<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l), view<M>(c, l + 1), l + 1 == lb ? 1 : 0);
             end();
             smooth(l, up);
         }
@@ -408,17 +429,31 @@ struct Run {
     // z = M^-1 r, rho/beta, q = A p and alpha, then the step and the exit test.
     void body(V* P, cudaGraphConditionalHandle cond, int use_cond) {
         vcycle();
+        const bool v = vec(0);
         beg(F_DOT, 0);
-        k_dot<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->r, (const V*)c->q, c->sc, c->partials,
+        if (v)
+            k_dot_v8<Pr><<<grid_w(0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->r, (const V*)c->q, c->sc, c->partials,
                                                     cnt(CNT_DOT));
+        else
+            k_dot<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->r, (const V*)c->q, c->sc,
+                                                        c->partials, cnt(CNT_DOT));
         end();
         beg(F_SEARCH, 0);
-        k_search<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q, c->sc,
-                                                       c->partials, cnt(CNT_SEARCH));
+        if (v)
+            k_search_v8<Pr><<<grid_w(0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q,
+                                                       c->sc, c->partials, cnt(CNT_SEARCH));
+        else
+            k_search<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q,
+                                                           c->sc, c->partials, cnt(CNT_SEARCH));
         end();
         beg(F_ADVANCE, 0);
-        k_advance<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (V*)c->d, (const V*)c->q, (V*)c->r, P, c->sc,
+        // the vector step moves P in 16-element runs: it needs a 16-byte aligned P
+        if (v && (reinterpret_cast<uintptr_t>(P) & 15) == 0)
+            k_advance_v8<Pr><<<grid_w(0), TPB, 0, s>>>(view<M>(c, 0), (V*)c->d, (const V*)c->q, (V*)c->r, P, c->sc,
                                                         c->partials, cnt(CNT_ADVANCE), cond, use_cond);
+        else
+            k_advance<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (V*)c->d, (const V*)c->q, (V*)c->r, P,
+                                                            c->sc, c->partials, cnt(CNT_ADVANCE), cond, use_cond);
         end();
     }
 
@@ -721,6 +756,7 @@ int build_tma(mpp_ctx* c) {
     const bool off = getenv("MPP_NO_TMA") != nullptr;
     const char* mode = getenv("MPP_RBGS");
     c->rbgs_mode = !mode ? RBGS_V8 : (!strcmp(mode, "tma") ? RBGS_TMA : (!strcmp(mode, "column") ? RBGS_COLUMN : RBGS_V8));
+    c->vec_on = c->rbgs_mode != RBGS_COLUMN;
     for (int l = 0; l < MAXLEV; l++) c->tma_ok[l] = false;
     for (int l = 0; l < c->lb; l++) {
         const LevelBuf& b = c->lv[l];

@@ -50,6 +50,68 @@ __device__ __forceinline__ C sum6(const C (&v)[6], uint8_t cd) {
     return s;
 }
 
+// ---- the scalar steps of pressure!, run by the last block of each reduction ----
+// After z.r (src/flip.jl:1095-1096, 1105-1107): rho_new and beta = rho_new / rho (0 on the
+// first pass); the flexible form takes the Polak-Ribiere beta (src/sflip.jl:1896-1897).
+template <class Pr>
+__device__ __forceinline__ void dot_finish(Scalars* sc, const double (&acc)[2]) {
+    State& S = sc->s;
+    const double rho_new = rs<Pr>(acc[0]);
+    if (!finite_d(rho_new)) {
+        S.status = ST_NONFINITE;
+        S.done = 1;
+        return;
+    }
+    if constexpr (Pr::flexible) {
+        if (!(rho_new > 0.0)) {  // src/sflip.jl:1880,1896
+            S.status = ST_INDEFINITE;
+            S.done = 1;
+            return;
+        }
+        const double beta = S.it == 0 ? 0.0 : -S.alpha * acc[1] / S.rho;
+        S.beta = beta > 0.0 ? beta : 0.0;
+    } else {
+        S.beta = S.it == 0 ? 0.0 : dv<Pr>(rho_new, S.rho);
+    }
+    S.rho = rho_new;
+}
+// After p.q: alpha = rho / p.q (src/flip.jl:1100), or a nonfinite/indefinite status.
+template <class Pr>
+__device__ __forceinline__ void search_finish(Scalars* sc, const double (&acc)[1]) {
+    State& S = sc->s;
+    S.pq = rs<Pr>(acc[0]);
+    if (!finite_d(S.pq)) {
+        S.status = ST_NONFINITE;
+        S.done = 1;
+    } else if (!(S.pq > 0.0)) {  // src/sflip.jl:1876-1877
+        S.status = ST_INDEFINITE;
+        S.done = 1;
+    } else {
+        S.alpha = dv<Pr>(S.rho, S.pq);
+    }
+}
+// After r.r: rnorm and the exit test rnorm <= tol |b| (src/flip.jl:1102-1103), or maxiter;
+// sets the graph's loop condition.
+template <class Pr>
+__device__ __forceinline__ void advance_finish(Scalars* sc, const double (&acc)[1], cudaGraphConditionalHandle cond,
+                                               int use_cond) {
+    State& S = sc->s;
+    S.it += 1;
+    S.rnorm = sq<Pr>(acc[0]);
+    S.rscale = next_rscale(S.rnorm, S.nliq);
+    if (!finite_d(S.rnorm)) {
+        S.status = ST_NONFINITE;
+        S.done = 1;
+    } else if (S.rnorm <= S.target) {
+        S.status = ST_OK;
+        S.done = 1;
+    } else if (S.it >= sc->p.maxiter) {
+        S.status = ST_NOT_CONVERGED;
+        S.done = 1;
+    }
+    set_cond(cond, use_cond, !S.done);
+}
+
 // ---- the V-cycle (src/flip.jl:992-1014) on row-split levels ----
 
 // start_kernel! (src/flip.jl:965-973): colour-0 LIQUID cells get b/diag, every other cell 0.
@@ -185,6 +247,338 @@ __global__ void __launch_bounds__(TPB) k_rbgs_v8(Lev<typename Pr::M> L, int colo
             if (cd[q] & SELF) st(&out.v[q], d > (C)0 ? (ld<C>(&bv.v[q]) + sum6<C>(nb, cd[q])) / d : (C)0);
         }
         st8(L.x + p, out);
+    }
+}
+
+// A lane's 8 columns in a tile (vector kernels): h .. h+7 of row j, plane k.
+struct Lane8 {
+    int h, j, k, rb;
+};
+template <class M>
+__device__ __forceinline__ bool lane8_of(const Lev<M>& L, uint32_t tile, Lane8& a) {
+    const int lane = threadIdx.x & 31;
+    a.h = (int)(tile & 1023u) * TH + (lane % V8_LANES_H) * V8;
+    a.j = (int)((tile >> 10) & 1023u) * TY + (lane / V8_LANES_H) % TY;
+    a.k = (int)(tile >> 20) * TZ + lane / (V8_LANES_H * TY);
+    a.rb = (a.k * L.n2 + a.j) * L.n1;
+    return a.h < L.H && a.j < L.n2 && a.k < L.n3;
+}
+#define FOR_TILES_W(L, tile)                                                                              \
+    for (int t_ = blockIdx.x * (TPB / 32) + (int)(threadIdx.x >> 5), n_ = *(L).count; t_ < n_;            \
+         t_ += gridDim.x * (TPB / 32))                                                                    \
+        if (const uint32_t tile = (L).tiles[t_]; true)
+
+// The other colour's values around a lane's 8 cells: the same 8 columns of this row
+// (the +x/-x neighbours) with one element on each side, and of the rows at +-y, +-z.
+template <class M>
+struct Nb8 {
+    Vec8<M> c, yp, ym, zp, zm;
+    M l, r;
+};
+template <class M>
+__device__ __forceinline__ Nb8<M> ld_nb8(const M* x, int o, int sy, int sz) {
+    Nb8<M> a;
+    a.c = ld8(x + o);
+    a.yp = ld8(x + o + sy);
+    a.ym = ld8(x + o - sy);
+    a.zp = ld8(x + o + sz);
+    a.zm = ld8(x + o - sz);
+    a.l = x[o - 1];
+    a.r = x[o + V8];
+    return a;
+}
+// neighbour m (+x,-x,+y,-y,+z,-z) of the lane's cell q; ci: its colour offset in the row
+// (q is a compile-time constant in the unrolled callers; ci selects between two
+// compile-time-indexed values, so nothing is indexed at run time.)
+template <class C, class M>
+__device__ __forceinline__ void nb6_of(C (&nb)[6], const Nb8<M>& a, int q, int ci) {
+    const M xp = ci ? (q + 1 < V8 ? a.c.v[q + 1 < V8 ? q + 1 : 0] : a.r) : a.c.v[q];
+    const M xm = ci ? a.c.v[q] : (q >= 1 ? a.c.v[q >= 1 ? q - 1 : 0] : a.l);
+    nb[0] = ld<C>(&xp);
+    nb[1] = ld<C>(&xm);
+    nb[2] = ld<C>(&a.yp.v[q]);
+    nb[3] = ld<C>(&a.ym.v[q]);
+    nb[4] = ld<C>(&a.zp.v[q]);
+    nb[5] = ld<C>(&a.zm.v[q]);
+}
+
+// start_kernel! (src/flip.jl:965-973), vector form.
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_start_v8(Lev<typename Pr::M> L) {
+    using C = typename Pr::C;
+    using M = typename Pr::M;
+    FOR_TILES_W(L, tile) {
+        Lane8 a;
+        if (!lane8_of(L, tile, a)) continue;
+        const int p0 = a.rb + a.h;
+        const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p0);
+        const Vec8<M> dv = ld8(L.dg + p0), bv = ld8(L.b + p0);
+        const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
+        Vec8<M> x0, x1;
+#pragma unroll
+        for (int q = 0; q < V8; q++) {
+            const C d = ld<C>(&dv.v[q]);
+            st(&x0.v[q], ((cd[q] & SELF) && d > (C)0) ? ld<C>(&bv.v[q]) / d : (C)0);
+            st(&x1.v[q], (C)0);
+        }
+        st8(L.x + p0, x0);
+        st8(L.x + p0 + L.H, x1);
+    }
+}
+
+// residual_kernel! (src/flip.jl:859-863), vector form: both colours of the lane's columns.
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_residual_v8(Lev<typename Pr::M> L) {
+    using C = typename Pr::C;
+    using M = typename Pr::M;
+    const int sy = L.n1, sz = L.n1 * L.n2;
+    FOR_TILES_W(L, tile) {
+        Lane8 a;
+        if (!lane8_of(L, tile, a)) continue;
+#pragma unroll
+        for (int cc = 0; cc < 2; cc++) {
+            const int p = a.rb + cc * L.H + a.h, o = a.rb + (1 - cc) * L.H + a.h;
+            const int ci = ci_of(cc, a.j, a.k);
+            const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
+            const Vec8<M> dv = ld8(L.dg + p), bv = ld8(L.b + p), xv = ld8(L.x + p);
+            const Nb8<M> nb = ld_nb8(L.x, o, sy, sz);
+            const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
+            Vec8<M> out;
+#pragma unroll
+            for (int q = 0; q < V8; q++) {
+                C v = (C)0;
+                if (cd[q] & SELF) {
+                    C n6[6];
+                    nb6_of(n6, nb, q, ci);
+                    v = ld<C>(&bv.v[q]) - (ld<C>(&dv.v[q]) * ld<C>(&xv.v[q]) - sum6<C>(n6, cd[q]));
+                }
+                st(&out.v[q], v);
+            }
+            st8(L.r + p, out);
+        }
+    }
+}
+
+// inner(s, z, r) and the flexible z.q (see k_dot), vector form.
+template <class Pr>
+__global__ void __launch_bounds__(TPB)
+    k_dot_v8(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ qv,
+             Scalars* sc, double* partials, unsigned* counter) {
+    using M = typename Pr::M;
+    using V = typename Pr::V;
+    if (sc->s.done) return;
+    double acc[2] = {0.0, 0.0};
+    FOR_TILES_W(L, tile) {
+        Lane8 a;
+        if (!lane8_of(L, tile, a)) continue;
+#pragma unroll
+        for (int cc = 0; cc < 2; cc++) {
+            const int p = a.rb + cc * L.H + a.h;
+            const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
+            const Vec8<M> zv = ld8(L.x + p);
+            const Vec8<V> rv = ld8(r + p);
+            Vec8<V> qq;
+            if constexpr (Pr::flexible) qq = ld8(qv + p);
+            const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
+#pragma unroll
+            for (int q = 0; q < V8; q++)
+                if (cd[q] & SELF) {
+                    const double z = ld<double>(&zv.v[q]);
+                    acc[0] += z * (double)rv.v[q];
+                    if constexpr (Pr::flexible) acc[1] += z * (double)qq.v[q];
+                }
+        }
+    }
+    if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0) dot_finish<Pr>(sc, acc);
+}
+
+// search_kernel! (src/flip.jl:1033-1054), vector form: colour by colour.
+template <class Pr>
+__global__ void __launch_bounds__(TPB)
+    k_search_v8(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ diag,
+                typename Pr::V* __restrict__ qout, Scalars* sc, double* partials, unsigned* counter) {
+    using C = typename Pr::C;
+    using M = typename Pr::M;
+    using V = typename Pr::V;
+    if (sc->s.done) return;
+    const C beta = (C)sc->s.beta;
+    const bool first = sc->s.beta == 0.0;
+    const int sy = L.n1, sz = L.n1 * L.n2;
+    double acc[1] = {0.0};
+    FOR_TILES_W(L, tile) {
+        Lane8 a;
+        if (!lane8_of(L, tile, a)) continue;
+#pragma unroll
+        for (int cc = 0; cc < 2; cc++) {
+            const int p = a.rb + cc * L.H + a.h, o = a.rb + (1 - cc) * L.H + a.h;
+            const int ci = ci_of(cc, a.j, a.k);
+            const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
+            const Vec8<V> gv = ld8(diag + p);
+            const Vec8<M> zc = ld8(L.x + p);
+            const Nb8<M> zn = ld_nb8(L.x, o, sy, sz);
+            Vec8<V> dc;
+            Nb8<V> dn;
+            if (!first) {
+                dc = ld8(dvec + p);
+                dn = ld_nb8(dvec, o, sy, sz);
+            }
+            const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
+            Vec8<V> out;
+#pragma unroll
+            for (int q = 0; q < V8; q++) {
+                C qv = (C)0;
+                if (cd[q] & SELF) {
+                    C z6[6], d6[6];
+                    nb6_of(z6, zn, q, ci);
+                    if (!first) nb6_of(d6, dn, q, ci);
+                    const C pc = first ? ld<C>(&zc.v[q]) : ld<C>(&zc.v[q]) + beta * (C)dc.v[q];
+                    C s = (C)0;
+#pragma unroll
+                    for (int m = 0; m < 6; m++)
+                        if (cd[q] & (1u << m)) s += first ? z6[m] : z6[m] + beta * d6[m];
+                    qv = (C)gv.v[q] * pc - s;
+                    acc[0] += (double)pc * (double)qv;
+                }
+                st(&out.v[q], qv);
+            }
+            st8(qout + p, out);
+        }
+    }
+    if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) search_finish<Pr>(sc, acc);
+}
+
+// advance_kernel! (src/flip.jl:1059-1073), vector form. The lane's 16 cells (both colours)
+// are 16 consecutive cells of the natural row, so P moves as one 16-element run.
+template <class Pr>
+__global__ void __launch_bounds__(TPB)
+    k_advance_v8(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ qv,
+                 typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
+                 unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
+    using C = typename Pr::C;
+    using M = typename Pr::M;
+    using V = typename Pr::V;
+    if (sc->s.done) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(cond, use_cond, 0);
+        return;
+    }
+    const C beta = (C)sc->s.beta, alpha = (C)sc->s.alpha;
+    const bool first = sc->s.beta == 0.0;
+    const bool sep_b = (void*)L.b != (void*)r;
+    const C rsc = (C)sc->s.rscale;
+    double acc[1] = {0.0};
+    FOR_TILES_W(L, tile) {
+        Lane8 a;
+        if (!lane8_of(L, tile, a)) continue;
+        const int pn = a.rb + 2 * a.h;  // natural run of the lane's 16 cells
+        Vec8<V> P0 = ld8(P + pn), P1 = ld8(P + pn + V8);
+#pragma unroll
+        for (int cc = 0; cc < 2; cc++) {
+            const int p = a.rb + cc * L.H + a.h;
+            const int ci = ci_of(cc, a.j, a.k);
+            const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
+            const Vec8<M> zv = ld8(L.x + p);
+            Vec8<V> dd = ld8(dvec + p), rr = ld8(r + p);
+            const Vec8<V> qq = ld8(qv + p);
+            const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
+            Vec8<M> rbv;
+            if (sep_b) rbv = ld8(L.b + p);
+#pragma unroll
+            for (int q = 0; q < V8; q++) {
+                if (!(cd[q] & SELF)) continue;
+                const C pc = first ? ld<C>(&zv.v[q]) : ld<C>(&zv.v[q]) + beta * (C)dd.v[q];
+                const C rl = (C)rr.v[q] - alpha * (C)qq.v[q];
+                st(&dd.v[q], pc);
+                st(&rr.v[q], rl);
+                if (sep_b) st(&rbv.v[q], rl * rsc);
+                // the cell's place in the natural run: 2q + ci (compile-time index per branch)
+                constexpr int dummy = 0;
+                (void)dummy;
+                if (ci == 0) {
+                    V& Pi = (2 * q < V8) ? P0.v[(2 * q) % V8] : P1.v[(2 * q) % V8];
+                    st(&Pi, (C)Pi + alpha * pc);
+                } else {
+                    V& Pi = (2 * q + 1 < V8) ? P0.v[(2 * q + 1) % V8] : P1.v[(2 * q + 1) % V8];
+                    st(&Pi, (C)Pi + alpha * pc);
+                }
+                acc[0] += (double)rl * (double)rl;
+            }
+            st8(dvec + p, dd);
+            st8(r + p, rr);
+            if (sep_b) st8(L.b + p, rbv);
+        }
+        st8(P + pn, P0);
+        st8(P + pn + V8, P1);
+    }
+    if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) advance_finish<Pr>(sc, acc, cond, use_cond);
+}
+
+// prolong_kernel! (src/flip.jl:914-929), vector form: one warp per fine tile stages the
+// tile's PX x PY x PZ coarse cells in its own slice of shared memory (non-LIQUID coarse
+// cells hold zero, as in k_prolong), then each lane adds the trilinear correction to its
+// 16 fine cells (8 columns, both colours) and writes them back in 16-byte pieces.
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_prolong_v8(Lev<typename Pr::M> L, Lev<typename Pr::M> Cl, int cnat) {
+    using C = typename Pr::C;
+    using M = typename Pr::M;
+    constexpr int WPB = TPB / 32, NE = PX * PY * PZ, PER = (NE + 31) / 32;
+    __shared__ C smw[WPB][PZ][PY][PX];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    C(*S)[PY][PX] = smw[warp];
+    const int n = *L.count;
+    for (int t = blockIdx.x * WPB + warp; t < n; t += gridDim.x * WPB) {
+        const uint32_t tile = L.tiles[t];
+        const int I0 = (int)(tile & 1023u) * TH - 1, J0 = (int)((tile >> 10) & 1023u) * (TY / 2) - 1,
+                  K0 = (int)(tile >> 20) * (TZ / 2) - 1;
+        C vals[PER];
+#pragma unroll
+        for (int u = 0; u < PER; u++) {
+            const int e = lane + 32 * u;
+            const int ii = e % PX, jj = (e / PX) % PY, kk = e / (PX * PY);
+            const int I = I0 + ii, J = J0 + jj, K = K0 + kk;
+            vals[u] = (C)0;
+            if (e < NE && I >= 0 && I < Cl.n1 && J >= 0 && J < Cl.n2 && K >= 0 && K < Cl.n3)
+                vals[u] = ld<C>(Cl.x + (cnat ? (int)Cl.nat(I, J, K) : (int)Cl.pos(I, J, K)));
+        }
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < PER; u++) {
+            const int e = lane + 32 * u;
+            if (e < NE) (&S[0][0][0])[e] = vals[u];
+        }
+        __syncwarp();
+        Lane8 a;
+        if (!lane8_of(L, tile, a)) continue;
+        int b0, b1, k0, k1;
+        C wb0, wb1, wc0, wc1;
+        pweights<C>(a.j, b0, wb0, b1, wb1);
+        pweights<C>(a.k, k0, wc0, k1, wc1);
+        b0 -= J0; b1 -= J0; k0 -= K0; k1 -= K0;
+#pragma unroll
+        for (int cc = 0; cc < 2; cc++) {
+            const int p = a.rb + cc * L.H + a.h;
+            const int ci = ci_of(cc, a.j, a.k);
+            const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
+            Vec8<M> xv = ld8(L.x + p);
+            const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
+#pragma unroll
+            for (int q = 0; q < V8; q++) {
+                if (!(cd[q] & SELF)) continue;
+                const int i = 2 * (a.h + q) + ci;
+                int a0, a1;
+                C wa0, wa1;
+                pweights<C>(i, a0, wa0, a1, wa1);
+                a0 -= I0; a1 -= I0;
+                C s = (C)0;
+#pragma unroll
+                for (int m = 0; m < 8; m++) {
+                    const int A = (m & 1) ? a1 : a0, B = (m & 2) ? b1 : b0, K = (m & 4) ? k1 : k0;
+                    const C wa = (m & 1) ? wa1 : wa0, wb = (m & 2) ? wb1 : wb0, wc = (m & 4) ? wc1 : wc0;
+                    s += wa * wb * wc * S[K][B][A];
+                }
+                st(&xv.v[q], ld<C>(&xv.v[q]) + (Pr::scaled ? (C)4 * s : s));
+            }
+            st8(L.x + p, xv);
+        }
     }
 }
 

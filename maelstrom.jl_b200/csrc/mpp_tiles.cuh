@@ -108,17 +108,24 @@ __global__ void __launch_bounds__(TPB) k_restrict(Lev<typename Pr::M> F, Lev<typ
         const int th = (int)(tile & 1023u), tj = (int)((tile >> 10) & 1023u), tk = (int)(tile >> 20);
         const int i0 = 4 * TH * th - 1, j0 = 2 * TY * tj - 1, k0 = 2 * TZ * tk - 1;
         __syncthreads();
-        for (int e = threadIdx.x; e < RX * RY * RZ; e += TPB) {
+        // Every non-LIQUID cell's r is zero (the residual pass writes zeros in active tiles
+        // and the set-up clears the array each projection), so r is staged unmasked: all of
+        // a thread's loads go out at once, then land in shared memory.
+        constexpr int NE = RX * RY * RZ, PER = (NE + TPB - 1) / TPB;
+        C vals[PER];
+#pragma unroll
+        for (int u = 0; u < PER; u++) {
+            const int e = (int)threadIdx.x + u * TPB;
             const int ii = e % RX, jj = (e / RX) % RY, kk = e / (RX * RY);
             const int i = i0 + ii, j = j0 + jj, k = k0 + kk;
-            C v = (C)0;
-            if (i >= 0 && i < F.n1 && j >= 0 && j < F.n2 && k >= 0 && k < F.n3) {
-                const int p = (int)F.pos(i, j, k);
-                const uint8_t cd = F.code[p];  // both loads in flight at once; the select
-                const C rv = ld<C>(F.r + p);   // keeps a stale value of a non-LIQUID cell out
-                v = (cd & SELF) ? rv : (C)0;
-            }
-            sm[e] = v;
+            vals[u] = (C)0;
+            if (e < NE && i >= 0 && i < F.n1 && j >= 0 && j < F.n2 && k >= 0 && k < F.n3)
+                vals[u] = ld<C>(F.r + (int)F.pos(i, j, k));
+        }
+#pragma unroll
+        for (int u = 0; u < PER; u++) {
+            const int e = (int)threadIdx.x + u * TPB;
+            if (e < NE) sm[e] = vals[u];
         }
         __syncthreads();
         const int h = th * TH + lh, J = tj * TY + lj, K = tk * TZ + lk;
@@ -170,23 +177,30 @@ __global__ void __launch_bounds__(TPB) k_prolong(Lev<typename Pr::M> L, Lev<type
     const int sz = L.n1 * L.n2;
     for (int t0 = blockIdx.x * TILES_PER_BLOCK; t0 < n; t0 += gridDim.x * TILES_PER_BLOCK) {
         __syncthreads();
-        for (int e = threadIdx.x; e < TILES_PER_BLOCK * PX * PY * PZ; e += TPB) {
+        // Every non-LIQUID coarse cell's x is zero (start writes zeros over active tiles, the
+        // set-up clears the arrays each projection, the bottom solve writes every cell), so
+        // x is staged unmasked, all of a thread's loads at once.
+        constexpr int NE = TILES_PER_BLOCK * PX * PY * PZ, PER = (NE + TPB - 1) / TPB;
+        C vals[PER];
+#pragma unroll
+        for (int u = 0; u < PER; u++) {
+            const int e = (int)threadIdx.x + u * TPB;
             const int s = e / (PX * PY * PZ), r = e % (PX * PY * PZ);
             const int ii = r % PX, jj = (r / PX) % PY, kk = r / (PX * PY);
-            C v = (C)0;
-            if (t0 + s < n) {
+            vals[u] = (C)0;
+            if (e < NE && t0 + s < n) {
                 const uint32_t tile = L.tiles[t0 + s];
                 const int I = (int)(tile & 1023u) * TH - 1 + ii;
                 const int J = (int)((tile >> 10) & 1023u) * (TY / 2) - 1 + jj;
                 const int K = (int)(tile >> 20) * (TZ / 2) - 1 + kk;
-                if (I >= 0 && I < Cl.n1 && J >= 0 && J < Cl.n2 && K >= 0 && K < Cl.n3) {
-                    const int q = cnat ? (int)Cl.nat(I, J, K) : (int)Cl.pos(I, J, K);
-                    const uint8_t cd = Cl.code[q];  // natural or row-split, as the level is stored
-                    const C xv = ld<C>(Cl.x + q);
-                    v = (cd & SELF) ? xv : (C)0;
-                }
+                if (I >= 0 && I < Cl.n1 && J >= 0 && J < Cl.n2 && K >= 0 && K < Cl.n3)
+                    vals[u] = ld<C>(Cl.x + (cnat ? (int)Cl.nat(I, J, K) : (int)Cl.pos(I, J, K)));
             }
-            sm[s][kk][jj][ii] = v;
+        }
+#pragma unroll
+        for (int u = 0; u < PER; u++) {
+            const int e = (int)threadIdx.x + u * TPB;
+            if (e < NE) (&sm[0][0][0][0])[e] = vals[u];
         }
         __syncthreads();
         const int t = t0 + sub;
@@ -396,34 +410,50 @@ __global__ void __launch_bounds__(1024) k_bottom(const typename Pr::C* __restric
         const CC* b = reinterpret_cast<const CC*>(smraw + B.ob);
         for (int c = tid; c < N; c += T) x[c] = (CC)0;
         __syncthreads();
-        // one cell per thread (N <= 1024): the threads that own cells sync among themselves
-        const int nthreads = ((N + 31) / 32) * 32;
+        // With n1 even a thread owns cells 2t and 2t+1 of one row, one of each colour, and each
+        // half-sweep updates the one of that colour (selected without branching); with n1 odd,
+        // one cell per thread. Only the threads that own cells meet at each barrier.
+        const int per = (B.n1 % 2 == 0) ? 2 : 1;
+        const int nthreads = (((N + per - 1) / per + 31) / 32) * 32;
         if (tid < nthreads) {
-            const bool mine = tid < N;
-            uint8_t cd = 0;
-            int mycol = 0;
-            CC bi = (CC)0, d = (CC)0, rd = (CC)0;
-            if (mine) {
-                cd = code[tid];
-                const int i = tid % B.n1, j = (tid / B.n1) % B.n2, k = tid / sz;
-                mycol = (i + j + k + 1) & 1;
-                bi = b[tid];
-                d = (CC)dc[tid];
-                rd = d > (CC)0 ? (CC)1 / d : (CC)0;
+            uint8_t cd[2] = {0, 0};
+            int cell[2] = {0, 0};
+            CC bi[2] = {(CC)0, (CC)0}, d[2] = {(CC)0, (CC)0}, rd[2] = {(CC)0, (CC)0};
+            int col0 = 0;
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int c = per * tid + u;
+                cell[u] = c;
+                if (u < per && c < N) {
+                    cd[u] = code[c];
+                    const int i = c % B.n1, j = (c / B.n1) % B.n2, k = c / sz;
+                    if (u == 0) col0 = (i + j + k + 1) & 1;
+                    bi[u] = b[c];
+                    d[u] = (CC)dc[c];
+                    rd[u] = d[u] > (CC)0 ? (CC)1 / d[u] : (CC)0;
+                }
             }
             for (int s = 1; s <= 2 * a.coarse; s++)
                 for (int half = 0; half <= 1; half++) {
                     const int colour = s <= a.coarse ? half : 1 - half;
-                    if (mine && (cd & SELF) && mycol == colour) {
-                        CC acc = bi;
-                        if (cd & 1) acc += x[tid + 1];
-                        if (cd & 2) acc += x[tid - 1];
-                        if (cd & 4) acc += x[tid + sy];
-                        if (cd & 8) acc += x[tid - sy];
-                        if (cd & 16) acc += x[tid + sz];
-                        if (cd & 32) acc += x[tid - sz];
-                        if constexpr (std::is_same<CC, float>::value) x[tid] = d > (CC)0 ? acc / d : (CC)0;
-                        else x[tid] = acc * rd;  // FP64 coarsest of the 16-bit forms
+                    // this thread's cell of `colour` (per == 1: its only cell, if that colour)
+                    const bool second = per == 2 && col0 != colour;
+                    const uint8_t cdv = (per == 1 && col0 != colour) ? (uint8_t)0 : (second ? cd[1] : cd[0]);
+                    if (cdv & SELF) {
+                        const int c = second ? cell[1] : cell[0];
+                        CC acc = second ? bi[1] : bi[0];
+                        if (cdv & 1) acc += x[c + 1];
+                        if (cdv & 2) acc += x[c - 1];
+                        if (cdv & 4) acc += x[c + sy];
+                        if (cdv & 8) acc += x[c - sy];
+                        if (cdv & 16) acc += x[c + sz];
+                        if (cdv & 32) acc += x[c - sz];
+                        if constexpr (std::is_same<CC, float>::value) {
+                            const CC dd = second ? d[1] : d[0];
+                            x[c] = dd > (CC)0 ? acc / dd : (CC)0;
+                        } else {
+                            x[c] = acc * (second ? rd[1] : rd[0]);  // FP64 coarsest of the 16-bit forms
+                        }
                     }
                     asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
                 }
