@@ -187,6 +187,23 @@ int grid_tiles1(const mpp_ctx* c, int l) {
     return g < cap ? (g > 0 ? g : 1) : cap;
 }
 
+// Kernel launches: programmatic dependent launch (see pdl_wait in mpp_common.cuh), so a
+// kernel's blocks can be scheduled while the previous kernel drains.
+template <typename... KArgs, typename... Args>
+void launch(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 Geo geo_of(const mpp_grid& g) {
     Geo o;
     for (int a = 0; a < 3; a++) { o.lo[a] = g.lo[a]; o.n[a] = g.n[a]; }
@@ -313,7 +330,7 @@ struct Run {
     void volume(const float* phi) {
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
         beg(F_VOLUME, -1);
-        k_volume<<<grid_cells(c, N), TPB, 0, s>>>(geo_of(c->grid), phi, c->sc, c->partials, cnt(CNT_VOLUME));
+        launch(k_volume, grid_cells(c, N), TPB, 0, s, geo_of(c->grid), phi, c->sc, c->partials, cnt(CNT_VOLUME));
         end();
     }
 
@@ -330,7 +347,7 @@ struct Run {
         }
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
         beg(F_SETUP, -1);
-        k_setup<Pr><<<grid_cells(c, N), TPB, 0, s>>>(in, view<M>(c, 0), (V*)c->diag, (V*)c->bvec, (V*)c->r, c->sc,
+        launch(k_setup<Pr>, grid_cells(c, N), TPB, 0, s, in, view<M>(c, 0), (V*)c->diag, (V*)c->bvec, (V*)c->r, c->sc,
                                                       c->partials, cnt(CNT_SETUP), cond, use_cond);
         end();
         for (int l = 1; l < c->L; l++) {
@@ -338,7 +355,7 @@ struct Run {
             const uint8_t* tf = l == 1 ? in.types : f.types;
             const int64_t Nl = (int64_t)c->lv[l].n[0] * c->lv[l].n[1] * c->lv[l].n[2];
             beg(F_LEVEL, l);
-            k_level<Pr><<<grid_cells(c, Nl), TPB, 0, s>>>(tf, f.n[0], f.n[1], f.n[2], view<M>(c, l),
+            launch(k_level<Pr>, grid_cells(c, Nl), TPB, 0, s, tf, f.n[0], f.n[1], f.n[2], view<M>(c, l),
                                                            c->lv[l].split ? 1 : 0);
             end();
         }
@@ -354,7 +371,7 @@ struct Run {
             tab.count[l] = c->lv[l].count;
         }
         beg(F_TILES, -1);
-        k_tilelists<<<tab.nlev, 1024, 0, s>>>(tab);
+        launch(k_tilelists, tab.nlev, 1024, 0, s, tab);
         end();
     }
 
@@ -363,15 +380,15 @@ struct Run {
             beg(F_RBGS, l);
             if (c->rbgs_mode == RBGS_TMA && c->tma_ok[l]) {
                 const int g = c->lv[l].ntiles < c->tma_blocks ? c->lv[l].ntiles : c->tma_blocks;
-                k_rbgs_tma<Pr><<<g > 0 ? g : 1, TPB, TmaGeom<M>::SMEM, s>>>(view<M>(c, l), col, c->tma[l],
+                launch(k_rbgs_tma<Pr>, g > 0 ? g : 1, TPB, TmaGeom<M>::SMEM, s, view<M>(c, l), col, c->tma[l],
                                                                            &c->sc->s.fault);
             } else if (c->rbgs_mode != RBGS_COLUMN && c->lv[l].H % V8 == 0) {
                 const int wpb = TPB / 32, cap = c->nsm * MAXBLOCKS_PER_SM;
                 int g = (c->lv[l].ntiles + wpb - 1) / wpb;
                 g = g < cap ? (g > 0 ? g : 1) : cap;
-                k_rbgs_v8<Pr><<<g, TPB, 0, s>>>(view<M>(c, l), col);
+                launch(k_rbgs_v8<Pr>, g, TPB, 0, s, view<M>(c, l), col);
             } else {
-                k_rbgs<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l), col);
+                launch(k_rbgs<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l), col);
             }
             end();
         }
@@ -387,17 +404,17 @@ struct Run {
         const int lb = c->lb;
         for (int l = 0; l < lb; l++) {
             beg(F_START, l);
-            if (vec(l)) k_start_v8<Pr><<<grid_w(l), TPB, 0, s>>>(view<M>(c, l));
-            else k_start<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l));
+            if (vec(l)) launch(k_start_v8<Pr>, grid_w(l), TPB, 0, s, view<M>(c, l));
+            else launch(k_start<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
             end();
             smooth(l, down);
             beg(F_RESID, l);
-            if (vec(l)) k_residual_v8<Pr><<<grid_w(l), TPB, 0, s>>>(view<M>(c, l));
-            else k_residual<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l));
+            if (vec(l)) launch(k_residual_v8<Pr>, grid_w(l), TPB, 0, s, view<M>(c, l));
+            else launch(k_residual<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
             end();
             if (l + 1 < lb) {
                 beg(F_RESTRICT, l + 1);
-                k_restrict<Pr><<<grid_tiles1(c, l + 1), TPB, c->restrict_smem, s>>>(view<M>(c, l), view<M>(c, l + 1));
+                launch(k_restrict<Pr>, grid_tiles1(c, l + 1), TPB, c->restrict_smem, s, view<M>(c, l), view<M>(c, l + 1));
                 end();
             }
         }
@@ -407,19 +424,19 @@ struct Run {
         {
             const int64_t Nb = (int64_t)c->lv[lb].n[0] * c->lv[lb].n[1] * c->lv[lb].n[2];
             beg(F_RESTRICT, lb);
-            k_restrict_bottom<Pr><<<grid_cells(c, Nb), TPB, 0, s>>>(view<M>(c, lb - 1), view<M>(c, lb),
+            launch(k_restrict_bottom<Pr>, grid_cells(c, Nb), TPB, 0, s, view<M>(c, lb - 1), view<M>(c, lb),
                                                                     (typename Pr::C*)c->botb);
             end();
         }
         beg(F_BOTTOM, lb);
-        k_bottom<Pr><<<1, 1024, c->bot_smem, s>>>((const typename Pr::C*)c->botb, (M*)c->lv[lb].x, ba);
+        launch(k_bottom<Pr>, 1, 1024, c->bot_smem, s, (const typename Pr::C*)c->botb, (M*)c->lv[lb].x, ba);
         end();
         for (int l = lb - 1; l >= 0; l--) {
             beg(F_PROLONG, l);
             if (vec(l))
-                k_prolong_v8<Pr><<<grid_w(l), TPB, 0, s>>>(view<M>(c, l), view<M>(c, l + 1), l + 1 == lb ? 1 : 0);
+                launch(k_prolong_v8<Pr>, grid_w(l), TPB, 0, s, view<M>(c, l), view<M>(c, l + 1), l + 1 == lb ? 1 : 0);
             else
-                k_prolong<Pr><<<grid_tiles(c, l), TPB, 0, s>>>(view<M>(c, l), view<M>(c, l + 1), l + 1 == lb ? 1 : 0);
+                launch(k_prolong<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l), view<M>(c, l + 1), l + 1 == lb ? 1 : 0);
             end();
             smooth(l, up);
         }
@@ -432,34 +449,34 @@ struct Run {
         const bool v = vec(0);
         beg(F_DOT, 0);
         if (v)
-            k_dot_v8<Pr><<<grid_w(0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->r, (const V*)c->q, c->sc, c->partials,
+            launch(k_dot_v8<Pr>, grid_w(0), TPB, 0, s, view<M>(c, 0), (const V*)c->r, (const V*)c->q, c->sc, c->partials,
                                                     cnt(CNT_DOT));
         else
-            k_dot<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->r, (const V*)c->q, c->sc,
+            launch(k_dot<Pr>, grid_tiles(c, 0), TPB, 0, s, view<M>(c, 0), (const V*)c->r, (const V*)c->q, c->sc,
                                                         c->partials, cnt(CNT_DOT));
         end();
         beg(F_SEARCH, 0);
         if (v)
-            k_search_v8<Pr><<<grid_w(0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q,
+            launch(k_search_v8<Pr>, grid_w(0), TPB, 0, s, view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q,
                                                        c->sc, c->partials, cnt(CNT_SEARCH));
         else
-            k_search<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q,
+            launch(k_search<Pr>, grid_tiles(c, 0), TPB, 0, s, view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q,
                                                            c->sc, c->partials, cnt(CNT_SEARCH));
         end();
         beg(F_ADVANCE, 0);
         // the vector step moves P in 16-element runs: it needs a 16-byte aligned P
         if (v && (reinterpret_cast<uintptr_t>(P) & 15) == 0)
-            k_advance_v8<Pr><<<grid_w(0), TPB, 0, s>>>(view<M>(c, 0), (V*)c->d, (const V*)c->q, (V*)c->r, P, c->sc,
+            launch(k_advance_v8<Pr>, grid_w(0), TPB, 0, s, view<M>(c, 0), (V*)c->d, (const V*)c->q, (V*)c->r, P, c->sc,
                                                         c->partials, cnt(CNT_ADVANCE), cond, use_cond);
         else
-            k_advance<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (V*)c->d, (const V*)c->q, (V*)c->r, P,
+            launch(k_advance<Pr>, grid_tiles(c, 0), TPB, 0, s, view<M>(c, 0), (V*)c->d, (const V*)c->q, (V*)c->r, P,
                                                             c->sc, c->partials, cnt(CNT_ADVANCE), cond, use_cond);
         end();
     }
 
     void true_residual(const V* P) {
         beg(F_TRUE, 0);
-        k_true_residual<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->bvec, (const V*)c->diag, P,
+        launch(k_true_residual<Pr>, grid_tiles(c, 0), TPB, 0, s, view<M>(c, 0), (const V*)c->bvec, (const V*)c->diag, P,
                                                               nullptr, c->sc, c->partials, cnt(CNT_TRUE));
         end();
     }
@@ -468,7 +485,7 @@ struct Run {
                   const uint8_t* types, const float* phi) {
         const int64_t N = (int64_t)(c->grid.n[0] + 1) * (c->grid.n[1] + 1) * (c->grid.n[2] + 1);
         beg(F_GRADIENT, -1);
-        k_gradient<<<grid_cells(c, N), TPB, 0, s>>>(c->grid.n[0], c->grid.n[1], c->grid.n[2], u, v, w, fu, fv, fw, P,
+        launch(k_gradient, grid_cells(c, N), TPB, 0, s, c->grid.n[0], c->grid.n[1], c->grid.n[2], u, v, w, fu, fv, fw, P,
                                                     types, phi, c->grid.dx);
         end();
     }
@@ -476,13 +493,13 @@ struct Run {
     void widen(const float* P) {
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
         beg(F_CONVERT, -1);
-        k_widen<<<grid_cells(c, N), TPB, 0, s>>>((double*)c->Pd, P, N);
+        launch(k_widen, grid_cells(c, N), TPB, 0, s, (double*)c->Pd, P, N);
         end();
     }
     void narrow(float* P) {
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
         beg(F_CONVERT, -1);
-        k_narrow<<<grid_cells(c, N), TPB, 0, s>>>(P, (const double*)c->Pd, N);
+        launch(k_narrow, grid_cells(c, N), TPB, 0, s, P, (const double*)c->Pd, N);
         end();
     }
 };
@@ -1144,7 +1161,7 @@ int mpp_rhs(mpp_ctx* c, float* b, const float* u, const float* v, const float* w
         if (int e = write_params(c, 1.f, 1.0, 1.0, 0, gamma, s)) return e;
         run.setup(in, 0, 0);
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
-        k_from_split<float, V><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), b, (const V*)c->bvec);
+        launch(k_from_split<float, V>, grid_cells(c, N), TPB, 0, s, fine_layout(c), b, (const V*)c->bvec);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s));
         c->launches += run.nk + 1;
@@ -1165,7 +1182,7 @@ int mpp_diag(mpp_ctx* c, float* diag, const uint8_t* types, const float* phi, mp
         Run<Pr> run{c, s};
         if (int e = operator_setup<Pr>(c, run, types, phi, nullptr, nullptr, nullptr, 0.f)) return e;
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
-        k_from_split<float, V><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), diag, (const V*)c->diag);
+        launch(k_from_split<float, V>, grid_cells(c, N), TPB, 0, s, fine_layout(c), diag, (const V*)c->diag);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s));
         c->launches += run.nk + 1;
@@ -1188,9 +1205,9 @@ int mpp_vcycle(mpp_ctx* c, float* z, const float* r, const uint8_t* types, const
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
         const size_t ms = msize(c->prec);
         CK(cudaMemsetAsync(c->lv[0].x, 0, ms * N, s));
-        k_to_split<M, float><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), (M*)c->lv[0].b, r);
+        launch(k_to_split<M, float>, grid_cells(c, N), TPB, 0, s, fine_layout(c), (M*)c->lv[0].b, r);
         run.vcycle();
-        k_from_split<float, M><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), z, (const M*)c->lv[0].x);
+        launch(k_from_split<float, M>, grid_cells(c, N), TPB, 0, s, fine_layout(c), z, (const M*)c->lv[0].x);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s));
         c->launches += run.nk + 2;
@@ -1214,9 +1231,9 @@ int mpp_apply(mpp_ctx* c, float* y, const float* x, const uint8_t* types, const 
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
         const size_t vs = vsize(c->prec);
         CK(cudaMemsetAsync(c->q, 0, vs * N, s));
-        k_to_split<V, float><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), (V*)c->d, x);
-        k_apply<Pr><<<grid_tiles(c, 0), TPB, 0, s>>>(view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q);
-        k_from_split<float, V><<<grid_cells(c, N), TPB, 0, s>>>(fine_layout(c), y, (const V*)c->q);
+        launch(k_to_split<V, float>, grid_cells(c, N), TPB, 0, s, fine_layout(c), (V*)c->d, x);
+        launch(k_apply<Pr>, grid_tiles(c, 0), TPB, 0, s, view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q);
+        launch(k_from_split<float, V>, grid_cells(c, N), TPB, 0, s, fine_layout(c), y, (const V*)c->q);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s));
         c->launches += run.nk + 3;
@@ -1282,6 +1299,8 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 // volume_kernel! + volume (src/flip.jl:261-279, 293), as k_volume, with the scratch laid
 // out in `scratch`: [counter u32 | result f64 | pad][partials f64 x blocks].
 __global__ void __launch_bounds__(TPB) k_volume_noalloc(Geo g, const float* __restrict__ phi, unsigned char* scratch) {
+    pdl_wait();
+    pdl_trigger();
     unsigned* counter = reinterpret_cast<unsigned*>(scratch);
     double* result = reinterpret_cast<double*>(scratch + 8);
     double* partials = reinterpret_cast<double*>(scratch + NOALLOC_HEADER);
@@ -1340,7 +1359,7 @@ extern "C" int mpp_volume_noalloc(const mpp_grid* grid, const float* phi, double
     // The counter must start at zero; an interrupted earlier call could have left it set.
     CK(cudaMemsetAsync(scratch, 0, NOALLOC_HEADER, s));
     const int blocks = (int)((N + NOALLOC_BLOCK_CELLS - 1) / NOALLOC_BLOCK_CELLS);
-    k_volume_noalloc<<<blocks, TPB, 0, s>>>(geo_of(*grid), phi, scratch);
+    launch(k_volume_noalloc, blocks, TPB, 0, s, geo_of(*grid), phi, scratch);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(volume, scratch + 8, sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));

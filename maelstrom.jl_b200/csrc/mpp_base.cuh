@@ -103,6 +103,8 @@ __device__ __forceinline__ uint8_t typeat(const uint8_t* __restrict__ t, int n1,
 // then gamma = clamp(loss / recover, -0.01/dt, 0.01/dt) with loss the relative volume loss.
 __global__ void __launch_bounds__(TPB) k_volume(Geo g, const float* __restrict__ phi, Scalars* sc,
                                                 double* partials, unsigned* counter) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t N = (int64_t)g.n[0] * g.n[1] * g.n[2];
     double acc[1] = {0.0};
     for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
@@ -154,6 +156,8 @@ __global__ void __launch_bounds__(TPB)
     k_setup(SetupIn<typename Pr::V> a, Lev<typename Pr::M> L, typename Pr::V* __restrict__ diag,
             typename Pr::V* __restrict__ b, typename Pr::V* __restrict__ r, Scalars* sc, double* partials,
             unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
+    pdl_wait();
+    pdl_trigger();
     using V = typename Pr::V;
     using M = typename Pr::M;
     using C = typename Pr::C;
@@ -268,6 +272,8 @@ __device__ __forceinline__ uint8_t coarsen_at(const uint8_t* __restrict__ tf, in
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_level(const uint8_t* __restrict__ tf, int f1, int f2, int f3,
                                                Lev<typename Pr::M> L, int split) {
+    pdl_wait();
+    pdl_trigger();
     const int n1 = L.n1, n2 = L.n2, n3 = L.n3;
     const int64_t N = (int64_t)n1 * n2 * n3;
     for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
@@ -308,6 +314,8 @@ __global__ void __launch_bounds__(TPB) k_level(const uint8_t* __restrict__ tf, i
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_restrict_bottom(Lev<typename Pr::M> F, Lev<typename Pr::M> L,
                                                          typename Pr::C* __restrict__ bout) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     const int N = L.n1 * L.n2 * L.n3;
     for (int c = blockIdx.x * TPB + threadIdx.x; c < N; c += gridDim.x * TPB) {
@@ -368,6 +376,8 @@ __global__ void __launch_bounds__(TPB) k_gradient(int n1, int n2, int n3, float*
                                                   uint8_t* __restrict__ fv, uint8_t* __restrict__ fw,
                                                   const float* __restrict__ P, const uint8_t* __restrict__ types,
                                                   const float* __restrict__ phi, float dx) {
+    pdl_wait();
+    pdl_trigger();
     const int m1 = n1 + 1, m2 = n2 + 1, m3 = n3 + 1;
     const int64_t N = (int64_t)m1 * m2 * m3;
     for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
@@ -387,6 +397,8 @@ __global__ void __launch_bounds__(TPB) k_gradient(int n1, int n2, int n3, float*
 // ---- layout conversions (natural <-> row-split) for the single-pass entry points ----
 template <class T, class S>
 __global__ void __launch_bounds__(TPB) k_to_split(Lev<float> L, T* __restrict__ dst, const S* __restrict__ src) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t N = (int64_t)L.n1 * L.n2 * L.n3;
     for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
         const int i = (int)(idx % L.n1), j = (int)((idx / L.n1) % L.n2), k = (int)(idx / ((int64_t)L.n1 * L.n2));
@@ -395,6 +407,8 @@ __global__ void __launch_bounds__(TPB) k_to_split(Lev<float> L, T* __restrict__ 
 }
 template <class T, class S>
 __global__ void __launch_bounds__(TPB) k_from_split(Lev<float> L, T* __restrict__ dst, const S* __restrict__ src) {
+    pdl_wait();
+    pdl_trigger();
     const int64_t N = (int64_t)L.n1 * L.n2 * L.n3;
     for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
         const int i = (int)(idx % L.n1), j = (int)((idx / L.n1) % L.n2), k = (int)(idx / ((int64_t)L.n1 * L.n2));
@@ -404,10 +418,14 @@ __global__ void __launch_bounds__(TPB) k_from_split(Lev<float> L, T* __restrict_
 
 // P (float, natural) <-> the FP64 solution vector.
 __global__ void __launch_bounds__(TPB) k_widen(double* __restrict__ dst, const float* __restrict__ src, int64_t n) {
+    pdl_wait();
+    pdl_trigger();
     for (int64_t i = (int64_t)blockIdx.x * TPB + threadIdx.x; i < n; i += (int64_t)gridDim.x * TPB)
         dst[i] = (double)src[i];
 }
 __global__ void __launch_bounds__(TPB) k_narrow(float* __restrict__ dst, const double* __restrict__ src, int64_t n) {
+    pdl_wait();
+    pdl_trigger();
     for (int64_t i = (int64_t)blockIdx.x * TPB + threadIdx.x; i < n; i += (int64_t)gridDim.x * TPB)
         dst[i] = (float)src[i];
 }

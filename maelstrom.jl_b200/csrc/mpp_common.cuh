@@ -114,6 +114,14 @@ struct Lev {
     }
 };
 
+// Programmatic dependent launch. Kernels are launched so that the next one may start while
+// the previous one drains; pdl_wait() (first thing in every kernel) blocks until the
+// previous kernel has completed and its writes are visible, and pdl_trigger() (after a
+// block's main work) lets the next kernel's blocks start launching. Both are no-ops in a
+// kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // A thread's slot in a tile (256 threads, one per slot): column h, row j, plane k offsets.
 // A warp covers TH consecutive columns of one row.
 __device__ __forceinline__ int slot_h() { return (int)threadIdx.x % TH; }

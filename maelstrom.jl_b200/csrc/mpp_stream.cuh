@@ -117,6 +117,8 @@ __device__ __forceinline__ void advance_finish(Scalars* sc, const double (&acc)[
 // start_kernel! (src/flip.jl:965-973): colour-0 LIQUID cells get b/diag, every other cell 0.
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_start(Lev<typename Pr::M> L) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     const int sz = L.n1 * L.n2;
     FOR_TILES_PF(L, tile) {
@@ -150,6 +152,8 @@ __global__ void __launch_bounds__(TPB) k_start(Lev<typename Pr::M> L) {
 // x = (b + sum_LIQ x_n) / diag on LIQUID cells of that colour.
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_rbgs(Lev<typename Pr::M> L, int colour) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     const int sy = L.n1, sz = L.n1 * L.n2;
     const int own = colour * L.H, oth = (1 - colour) * L.H;
@@ -210,6 +214,8 @@ __device__ __forceinline__ void st8(T* p, const Vec8<T>& r) {
 // row (the +x/-x neighbours, plus one element on each side) and of the rows at -+y, -+z.
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_rbgs_v8(Lev<typename Pr::M> L, int colour) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     using M = typename Pr::M;
     const int sy = L.n1, sz = L.n1 * L.n2;
@@ -305,6 +311,8 @@ __device__ __forceinline__ void nb6_of(C (&nb)[6], const Nb8<M>& a, int q, int c
 // start_kernel! (src/flip.jl:965-973), vector form.
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_start_v8(Lev<typename Pr::M> L) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     using M = typename Pr::M;
     FOR_TILES_W(L, tile) {
@@ -329,6 +337,8 @@ __global__ void __launch_bounds__(TPB) k_start_v8(Lev<typename Pr::M> L) {
 // residual_kernel! (src/flip.jl:859-863), vector form: both colours of the lane's columns.
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_residual_v8(Lev<typename Pr::M> L) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     using M = typename Pr::M;
     const int sy = L.n1, sz = L.n1 * L.n2;
@@ -364,6 +374,8 @@ template <class Pr>
 __global__ void __launch_bounds__(TPB)
     k_dot_v8(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ qv,
              Scalars* sc, double* partials, unsigned* counter) {
+    pdl_wait();
+    pdl_trigger();
     using M = typename Pr::M;
     using V = typename Pr::V;
     if (sc->s.done) return;
@@ -397,6 +409,8 @@ template <class Pr>
 __global__ void __launch_bounds__(TPB)
     k_search_v8(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ diag,
                 typename Pr::V* __restrict__ qout, Scalars* sc, double* partials, unsigned* counter) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     using M = typename Pr::M;
     using V = typename Pr::V;
@@ -454,6 +468,8 @@ __global__ void __launch_bounds__(TPB)
     k_advance_v8(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ qv,
                  typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
                  unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     using M = typename Pr::M;
     using V = typename Pr::V;
@@ -518,6 +534,8 @@ __global__ void __launch_bounds__(TPB)
 // 16 fine cells (8 columns, both colours) and writes them back in 16-byte pieces.
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_prolong_v8(Lev<typename Pr::M> L, Lev<typename Pr::M> Cl, int cnat) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     using M = typename Pr::M;
     constexpr int WPB = TPB / 32, NE = PX * PY * PZ, PER = (NE + 31) / 32;
@@ -585,6 +603,8 @@ __global__ void __launch_bounds__(TPB) k_prolong_v8(Lev<typename Pr::M> L, Lev<t
 // residual_kernel! (src/flip.jl:859-863): r = b - (diag x - sum_LIQ x_n) on LIQUID, else 0.
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_residual(Lev<typename Pr::M> L) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     const int sy = L.n1, sz = L.n1 * L.n2;
     FOR_TILES_PF(L, tile) {
@@ -626,6 +646,8 @@ template <class Pr>
 __global__ void __launch_bounds__(TPB)
     k_dot(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ q,
           Scalars* sc, double* partials, unsigned* counter) {
+    pdl_wait();
+    pdl_trigger();
     if (sc->s.done) return;
     const int sz = L.n1 * L.n2;
     double acc[2] = {0.0, 0.0};
@@ -685,6 +707,8 @@ template <class Pr>
 __global__ void __launch_bounds__(TPB)
     k_search(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ diag,
              typename Pr::V* __restrict__ q, Scalars* sc, double* partials, unsigned* counter) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     if (sc->s.done) return;
     const C beta = (C)sc->s.beta;
@@ -753,6 +777,8 @@ __global__ void __launch_bounds__(TPB)
     k_advance(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ q,
               typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
               unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     if (sc->s.done) {
         if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(cond, use_cond, 0);
@@ -826,6 +852,8 @@ __global__ void __launch_bounds__(TPB)
     k_true_residual(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ b, const typename Pr::V* __restrict__ diag,
                     const typename Pr::V* __restrict__ P, typename Pr::V* __restrict__ rout, Scalars* sc,
                     double* partials, unsigned* counter) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     const int n1 = L.n1, sz = L.n1 * L.n2, N = L.n1 * L.n2 * L.n3;
     double acc[1] = {0.0};
@@ -863,6 +891,8 @@ __global__ void __launch_bounds__(TPB)
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_apply(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ x,
                                                const typename Pr::V* __restrict__ diag, typename Pr::V* __restrict__ y) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     const int sy = L.n1, sz = L.n1 * L.n2;
     FOR_TILES_PF(L, tile) {

@@ -35,6 +35,8 @@ struct TileTab {
     int* count[16];
 };
 __global__ void __launch_bounds__(1024) k_tilelists(TileTab tab) {
+    pdl_wait();
+    pdl_trigger();
     const int l = blockIdx.x;
     if (l >= tab.nlev) return;
     const int n = tab.ntiles[l], GH = tab.GH[l], GJ = tab.GJ[l];
@@ -98,6 +100,8 @@ constexpr int RX = 4 * TH + 2, RY = 2 * TY + 2, RZ = 2 * TZ + 2;
 
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_restrict(Lev<typename Pr::M> F, Lev<typename Pr::M> L) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     extern __shared__ __align__(128) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
@@ -170,6 +174,8 @@ constexpr int PX = TH + 2, PY = TY / 2 + 2, PZ = TZ / 2 + 2;
 
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_prolong(Lev<typename Pr::M> L, Lev<typename Pr::M> Cl, int cnat) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     __shared__ C sm[TILES_PER_BLOCK][PZ][PY][PX];
     const int n = *L.count;
@@ -281,6 +287,8 @@ struct BotArgs {
 template <class Pr>
 __global__ void __launch_bounds__(1024) k_bottom(const typename Pr::C* __restrict__ bin, typename Pr::M* __restrict__ xout,
                                                  BotArgs a) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     using CC = typename Pr::CC;
     extern __shared__ __align__(128) unsigned char smraw[];

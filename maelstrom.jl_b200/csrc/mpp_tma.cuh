@@ -89,6 +89,8 @@ struct TmaGeom {
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_rbgs_tma(Lev<typename Pr::M> L, int colour, const __grid_constant__ TmaLev tm,
                                                   int* fault) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename Pr::C;
     using M = typename Pr::M;
     using G = TmaGeom<M>;
