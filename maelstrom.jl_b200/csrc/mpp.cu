@@ -8,11 +8,13 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "mpp.h"
 #include <cudaTypedefs.h>
 
+#include "mpp_fgmres.cuh"
 #include "mpp_tma.cuh"
 
 using namespace mpp;
@@ -39,7 +41,9 @@ void set_err(const char* fmt, ...) {
 
 constexpr int MAXLEV = 16;
 constexpr int NCOUNTERS = 8;
-enum { CNT_VOLUME, CNT_SETUP, CNT_DOT, CNT_SEARCH, CNT_ADVANCE, CNT_TRUE };
+enum { CNT_VOLUME, CNT_SETUP, CNT_DOT, CNT_SEARCH, CNT_ADVANCE, CNT_TRUE, CNT_FG };
+// longest FGMRES restart cycle (Krylov basis vectors kept)
+constexpr int FG_MAXR = 64;
 // Smoother forms: 8-wide vector loads (default), the TMA pipeline, the per-column form.
 enum { RBGS_V8 = 0, RBGS_TMA = 1, RBGS_COLUMN = 2 };
 
@@ -125,6 +129,15 @@ struct mpp_ctx {
     std::vector<cudaEvent_t> evfree, evall;
     ProfAcc prof[NFAM][MAXLEV + 1];
     int active[MAXLEV];
+    // FGMRES fallback workspace, allocated on its first use: basis V (fg_restart + 1
+    // vectors, row-split, type V), preconditioned vectors Z (guarded), Arnoldi scalars
+    void* fV;
+    void* fZ[FG_MAXR];
+    int fg_restart;
+    double* fgd;
+    double* fgd_host;  // pinned
+    int fg_used, fg_its;
+    double fg_residual;
 };
 
 namespace {
@@ -510,7 +523,8 @@ int write_params(mpp_ctx* c, float volume0, double dt, double recover, int proje
     p.tol = c->opts.tol;
     p.dt = dt;
     p.recover = recover;
-    p.maxiter = c->opts.maxiter;
+    // with the fallback on, CG gets at most cg_maxiter_with_fallback iterations (src/fgmres.jl:99)
+    p.maxiter = c->opts.fallback ? std::min(c->opts.maxiter, c->opts.cg_maxiter_with_fallback) : c->opts.maxiter;
     p.project = project;
     p.gamma = gamma;
     CK(cudaMemcpyAsync(&c->sc->p, &c->sc_host->p, sizeof(Params), cudaMemcpyHostToDevice, s));
@@ -581,7 +595,201 @@ void record_epilogue(Run<Pr>& run, const Call& k) {
     V* P = std::is_same<V, double>::value ? (V*)c->Pd : (V*)k.P;
     run.true_residual(P);
     if (std::is_same<V, double>::value) run.narrow(k.P);
-    if (k.kind == 1) run.gradient(k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.types, k.phi);
+    // with the fallback on, the gradient waits for the host's fallback decision
+    if (k.kind == 1 && !c->opts.fallback) run.gradient(k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.types, k.phi);
+}
+
+// ---- the FGMRES fallback (src/fgmres.jl:26-110, restated for the dense operator) ----
+Lev<float> fine_layout(mpp_ctx* c);
+
+// The Krylov workspace for `restart`, allocated on first use (outside any capture).
+int fg_workspace(mpp_ctx* c, int R) {
+    if (c->fg_restart >= R) return MPP_OK;
+    if (c->fg_restart > 0) {
+        set_err("the fallback's restart length cannot grow after its first use (%d > %d)", R, c->fg_restart);
+        return MPP_ERR_INVALID;
+    }
+    const size_t N = (size_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+    const size_t vs = vsize(c->prec), gd = guard_of(c->grid.n[0], c->grid.n[1]);
+    if (int e = alloc(c, &c->fV, vs * N * (size_t)(R + 1))) return e;
+    for (int j = 0; j < R; j++)
+        if (int e = alloc_guarded(c, &c->fZ[j], vs, N, gd)) return e;
+    if (int e = alloc(c, (void**)&c->fgd, sizeof(double) * (2 * (FG_MAXR + 1) + 1))) return e;
+    CK(cudaMallocHost((void**)&c->fgd_host, sizeof(double) * (2 * (FG_MAXR + 1) + 1)));
+    c->fg_restart = R;
+    return MPP_OK;
+}
+
+// Restarted right-preconditioned flexible GMRES: basis V (FP32, or FP64 in the FP64 form)
+// with two passes of modified Gram-Schmidt, z_j = M^-1 v_j by the V-cycle, FP64 Hessenberg
+// and Givens rotations on the host, the true residual checked after every cycle. The
+// Gram-Schmidt coefficients stay on the device (slot pass*(R+1)+i, the norm in slot
+// 2*(R+1)); the host reads a column once, after its last kernel. Sets `status` and `its`.
+template <class Pr>
+int fgmres(mpp_ctx* c, cudaStream_t s, typename Pr::V* P, int& its, int& status) {
+    using V = typename Pr::V;
+    using M = typename Pr::M;
+    Run<Pr> run{c, s};
+    const Lev<float> L = fine_layout(c);
+    const size_t N = (size_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+    const int R = c->opts.restart, maxit = c->opts.fallback_maxiter;
+    const int gtw = grid_tiles(c, 0);
+    const int NS = 2 * (FG_MAXR + 1) + 1, SN = 2 * (FG_MAXR + 1);
+    auto vec = [&](int i) { return reinterpret_cast<V*>(c->fV) + (size_t)i * N; };
+    auto zv = [&](int i) { return reinterpret_cast<V*>(c->fZ[i]); };
+    V* q = reinterpret_cast<V*>(c->q);
+    V* r = reinterpret_cast<V*>(c->r);
+    double residual = 0.0;
+    auto finish = [&]() -> int {
+        c->fg_residual = residual;
+        c->launches += run.nk;
+        run.nk = 0;
+        CK(cudaGetLastError());
+        return MPP_OK;
+    };
+    auto true_res = [&](double& res) -> int {  // r = b - A P and its norm (src/fgmres.jl:35-40)
+        run.nk++;
+        launch(k_true_residual<Pr>, grid_tiles(c, 0), TPB, 0, s, view<M>(c, 0), (const V*)c->bvec, (const V*)c->diag,
+               (const V*)P, r, c->sc, c->partials, run.cnt(CNT_TRUE));
+        if (int e = read_state(c, s)) return e;
+        res = sqrt(c->sc_host->s.true_rr);
+        return MPP_OK;
+    };
+    // the V-cycle's input is scaled so 16-bit storage keeps its precision (M^-1 is linear):
+    // a unit vector's entries are ~1/sqrt(n), scaled to ~1/4
+    const double nliq = c->sc_host->s.nliq > 0 ? (double)c->sc_host->s.nliq : 1.0;
+    const double cyc = Pr::scaled ? exp2(rint(log2(0.25 * sqrt(nliq)))) : 1.0;
+    const double bnorm = c->sc_host->s.bnorm;
+    its = 0;
+    status = MPP_OK;
+    if (!std::isfinite(bnorm)) {
+        status = MPP_NONFINITE;  // "Nonfinite pressure RHS" (src/fgmres.jl:31)
+        return MPP_OK;
+    }
+    if (bnorm == 0.0) {
+        run.nk++;
+        launch(k_fg_zero_P<V>, gtw, TPB, 0, s, L, P);
+        return finish();
+    }
+    if (int e = fg_workspace(c, R)) return e;
+    const double target = (double)c->opts.tol * bnorm;
+    if (int e = true_res(residual)) return e;
+    std::vector<double> H((size_t)(R + 1) * R), g(R + 1), cs(R), sn(R), y(R);
+    auto Hs = [&](int i, int j) -> double& { return H[(size_t)i * R + j]; };
+    while (residual > target && its < maxit) {
+        if (!std::isfinite(residual)) {
+            status = MPP_NONFINITE;  // "Nonfinite pressure residual" (src/fgmres.jl:46)
+            return finish();
+        }
+        std::fill(H.begin(), H.end(), 0.0);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = residual;
+        run.nk++;
+        launch(k_fg_scale<V>, gtw, TPB, 0, s, L, vec(0), (const V*)r, 1.0 / residual);
+        int used = 0;
+        for (int j = 0; j < R && its < maxit; j++) {
+            run.nk++;
+            launch(k_fg_to_cycle<M, V>, gtw, TPB, 0, s, L, (M*)c->lv[0].b, (const V*)vec(j), cyc);
+            run.vcycle();
+            run.nk += 2;
+            launch(k_fg_from_cycle<M, V>, gtw, TPB, 0, s, L, zv(j), (const M*)c->lv[0].x, 1.0 / cyc);
+            launch(k_apply<Pr>, grid_tiles(c, 0), TPB, 0, s, view<M>(c, 0), (const V*)zv(j), (const V*)c->diag, q);
+            // twice-repeated modified Gram-Schmidt (src/fgmres.jl:59-63)
+            for (int pass = 0; pass < 2; pass++)
+                for (int i = 0; i <= j; i++) {
+                    const int slot = pass * (FG_MAXR + 1) + i;
+                    run.nk += 2;
+                    launch(k_fg_dot<V>, gtw, TPB, 0, s, L, (const V*)q, (const V*)vec(i), c->fgd, slot, c->partials,
+                           run.cnt(CNT_FG));
+                    launch(k_fg_orth<V>, gtw, TPB, 0, s, L, q, (const V*)vec(i), (const double*)c->fgd, slot);
+                }
+            run.nk += 2;
+            launch(k_fg_dot<V>, gtw, TPB, 0, s, L, (const V*)q, (const V*)q, c->fgd, SN, c->partials, run.cnt(CNT_FG));
+            launch(k_fg_normalize<V>, gtw, TPB, 0, s, L, vec(j + 1), (const V*)q, (const double*)c->fgd, SN);
+            CK(cudaMemcpyAsync(c->fgd_host, c->fgd, sizeof(double) * NS, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            for (int i = 0; i <= j; i++) Hs(i, j) = c->fgd_host[i] + c->fgd_host[FG_MAXR + 1 + i];
+            const double hnext = sqrt(c->fgd_host[SN]);
+            if (!std::isfinite(hnext)) {
+                status = MPP_NONFINITE;  // "Nonfinite pressure Arnoldi vector" (src/fgmres.jl:65)
+                return finish();
+            }
+            Hs(j + 1, j) = hnext;
+            for (int i = 0; i < j; i++) {
+                const double a = Hs(i, j), b = Hs(i + 1, j);
+                Hs(i, j) = cs[i] * a + sn[i] * b;
+                Hs(i + 1, j) = -sn[i] * a + cs[i] * b;
+            }
+            const double a = Hs(j, j), b = Hs(j + 1, j);
+            const double hyp = std::hypot(a, b);
+            if (!(hyp > 0.0)) {
+                status = MPP_BREAKDOWN;  // "Pressure Arnoldi breakdown" (src/fgmres.jl:77)
+                return finish();
+            }
+            cs[j] = a / hyp;
+            sn[j] = b / hyp;
+            Hs(j, j) = hyp;
+            Hs(j + 1, j) = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            used = j + 1;
+            its++;
+            if (std::fabs(g[j + 1]) <= target || hnext == 0.0) break;
+        }
+        for (int i = used - 1; i >= 0; i--) {  // UpperTriangular(H) \ g (src/fgmres.jl:84)
+            double t = g[i];
+            for (int k = i + 1; k < used; k++) t -= Hs(i, k) * y[k];
+            y[i] = t / Hs(i, i);
+        }
+        for (int j = 0; j < used; j++) {
+            run.nk++;
+            launch(k_fg_update_P<V>, gtw, TPB, 0, s, L, P, (const V*)zv(j), y[j]);
+        }
+        if (int e = true_res(residual)) return e;
+    }
+    status = residual <= target ? MPP_OK : MPP_NOT_CONVERGED;  // src/fgmres.jl:90
+    return finish();
+}
+
+// After the CG solve with the fallback on (src/fgmres.jl:96-110): keep CG's pressure when its
+// true residual meets tol; else zero P if that residual is nonfinite or above 2|b|, run FGMRES,
+// and then (project!) the gradient update.
+template <class Pr>
+int fallback_and_finish(mpp_ctx* c, const Call& k, cudaStream_t s) {
+    using V = typename Pr::V;
+    State& S = c->sc_host->s;
+    c->fg_used = 0;
+    c->fg_its = 0;
+    const double target = (double)c->opts.tol * S.bnorm;
+    const double tres = sqrt(S.true_rr);
+    V* P = std::is_same<V, double>::value ? (V*)c->Pd : (V*)k.P;
+    const bool cg_ok = S.status == MPP_OK && (S.bnorm == 0.0 || tres <= target);
+    if (!cg_ok && std::isfinite(S.bnorm) && S.bnorm > 0.0) {
+        const Lev<float> L = fine_layout(c);
+        if (!std::isfinite(tres) || tres > 2.0 * S.bnorm) {
+            launch(k_fg_zero_P<V>, grid_tiles(c, 0), TPB, 0, s, L, P);
+            c->launches++;
+        }
+        int its = 0, st = 0;
+        if (int e = fgmres<Pr>(c, s, P, its, st)) return e;
+        c->fg_used = 1;
+        c->fg_its = its;
+        S.status = st;
+        S.true_rr = c->fg_residual * c->fg_residual;
+        if (std::is_same<V, double>::value) {
+            Run<Pr> run{c, s};
+            run.narrow(k.P);
+            c->launches += run.nk;
+        }
+    }
+    if (k.kind == 1) {
+        Run<Pr> run{c, s};
+        run.gradient(k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.types, k.phi);
+        c->launches += run.nk;
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    return MPP_OK;
 }
 
 template <class Pr>
@@ -667,6 +875,8 @@ int solve(mpp_ctx* c, const Call& k, cudaStream_t s) {
         set_err("a bounded device wait (TMA pipeline) gave up; results are not valid");
         return MPP_ERR_CUDA;
     }
+    c->fg_used = c->fg_its = 0;
+    if (c->opts.fallback) return fallback_and_finish<Pr>(c, k, s);
     return MPP_OK;
 }
 
@@ -694,6 +904,8 @@ void fill_result(mpp_ctx* c, mpp_result* res, int64_t launches) {
     res->volume = S.vol;
     res->gamma = S.gamma;
     res->kernel_launches = launches;
+    res->fallback_used = c->fg_used;
+    res->fallback_iterations = c->fg_its;
 }
 
 int check_ctx(mpp_ctx* c) {
@@ -835,6 +1047,7 @@ int mpp_ctx_destroy(mpp_ctx* c) {
     if (c->graph) cudaGraphDestroy(c->graph);
     for (void* p : c->allocs) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
+    if (c->fgd_host) cudaFreeHost(c->fgd_host);
     if (c->cap) cudaStreamDestroy(c->cap);
     for (cudaEvent_t e : c->evall) cudaEventDestroy(e);
     delete c;
@@ -872,6 +1085,11 @@ static int validate(const mpp_grid* g, const mpp_opts* o) {
         set_err("unknown precision %d", o->precision);
         return MPP_ERR_INVALID;
     }
+    if (o->fallback && (o->restart < 1 || o->restart > FG_MAXR || o->fallback_maxiter < 0 ||
+                        o->cg_maxiter_with_fallback < 0)) {
+        set_err("bad fallback options (restart must be in [1, %d])", FG_MAXR);
+        return MPP_ERR_INVALID;
+    }
     return MPP_OK;
 }
 
@@ -898,6 +1116,13 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
     c->prof_on = 0;
     memset(c->prof, 0, sizeof(c->prof));
     memset(c->active, 0, sizeof(c->active));
+    c->fV = nullptr;
+    memset(c->fZ, 0, sizeof(c->fZ));
+    c->fg_restart = 0;
+    c->fgd = nullptr;
+    c->fgd_host = nullptr;
+    c->fg_used = c->fg_its = 0;
+    c->fg_residual = 0.0;
     auto fail = [&](int e) {
         mpp_ctx_destroy(c);
         return e;
@@ -1045,7 +1270,8 @@ int mpp_ctx_set_opts(mpp_ctx* c, const mpp_opts* o) {
         set_err("precision is fixed at context creation");
         return MPP_ERR_INVALID;
     }
-    if (o->sweeps != c->opts.sweeps || o->coarse != c->opts.coarse || o->graph != c->opts.graph) {
+    if (o->sweeps != c->opts.sweeps || o->coarse != c->opts.coarse || o->graph != c->opts.graph ||
+        (o->fallback != 0) != (c->opts.fallback != 0)) {
         if (c->gexec) cudaGraphExecDestroy(c->gexec);
         if (c->graph) cudaGraphDestroy(c->graph);
         c->gexec = nullptr;

@@ -245,6 +245,10 @@ class FlipBasin:
 
 
 def _raise_or_warn(res: Result, bnorm_ok=True):
+    if res.status == _lib.NOT_CONVERGED and res.fallback_used:
+        # the fallback's own miss is an error (src/fgmres.jl:90)
+        raise RuntimeError(f"Pressure did not converge: {res.true_rel_residual:.3e} after "
+                           f"{res.iterations} + {res.fallback_iterations} iterations")
     if res.status == _lib.NOT_CONVERGED:
         warnings.warn(f"pressure solve did not converge: residual = {res.rel_residual:.3e}, "
                       f"iterations = {res.iterations}", RuntimeWarning, stacklevel=3)
@@ -262,7 +266,8 @@ def project(s: FlipBasin, dt, recover=0.5, sweeps=None) -> FlipBasin:
     if sweeps is not None and sweeps != p.opts.sweeps:
         p.set(sweeps=sweeps)
     res = p.project(s.u, s.v, s.w, s.fu, s.fv, s.fw, s.P, s.types, s.phi, s.volume0, dt, recover)
-    s.iterations.append(res.iterations)
+    # with the fallback, pressure! counts CG's and FGMRES's iterations (src/fgmres.jl:110)
+    s.iterations.append(res.iterations + res.fallback_iterations)
     s.last = res
     _raise_or_warn(res)
     return s
@@ -278,4 +283,4 @@ def pressure(s: FlipBasin, b, tol=None, maxiter=None, sweeps=None) -> int:
     res = p.pressure(s.P, b, s.types, s.phi)
     s.last = res
     _raise_or_warn(res)
-    return res.iterations
+    return res.iterations + res.fallback_iterations
