@@ -133,6 +133,27 @@ int mpp_pressure(mpp_ctx* ctx, float* P, const float* b, const uint8_t* types, c
 /* rhs_kernel! (src/flip.jl:817-822): b = -dx div u + dx^2 gamma on LIQUID, else 0. */
 int mpp_rhs(mpp_ctx* ctx, float* b, const float* u, const float* v, const float* w,
             const uint8_t* types, float gamma, mpp_stream stream);
+/* The adjoint of project! with respect to the face velocities (a vector-Jacobian product;
+ * the reference has no adjoint: this one is derived from its forward kernels,
+ * src/flip.jl:817-822 and 1113-1130). project! is affine in (u, v, w) for fixed types
+ * and phi, u_out = u - G A^-1 (-dx D u + dx^2 gamma), and A is symmetric, so for the
+ * cotangent (gu, gv, gw) of the output faces:
+ *   beta = dx G^T g on LIQUID cells, A mu = beta (the same solve, options and fallback
+ *   as the forward), g_in = g + D^T mu on every face.
+ * In: gu, gv, gw (face shapes as u, v, w), types, phi, mu (warm start of the adjoint
+ * pressure, natural order, any values). Out: ou, ov, ow = g_in (may be gu, gv, gw
+ * themselves), mu. gamma has no velocity derivative. Returns the solve status. */
+int mpp_project_vjp(mpp_ctx* ctx, const float* gu, const float* gv, const float* gw, float* ou, float* ov,
+                    float* ow, float* mu, const uint8_t* types, const float* phi, mpp_result* res,
+                    mpp_stream stream);
+
+/* The two passes of mpp_project_vjp on their own: beta = dx G^T g (natural, 0 off-liquid)
+ * and g_in = g + D^T mu. */
+int mpp_vjp_rhs(mpp_ctx* ctx, float* beta, const float* gu, const float* gv, const float* gw,
+                const uint8_t* types, const float* phi, mpp_stream stream);
+int mpp_vjp_faces(mpp_ctx* ctx, float* ou, float* ov, float* ow, const float* gu, const float* gv,
+                  const float* gw, const float* mu, const uint8_t* types, mpp_stream stream);
+
 /* diag_kernel! (src/flip.jl:824-836). */
 int mpp_diag(mpp_ctx* ctx, float* diag, const uint8_t* types, const float* phi, mpp_stream stream);
 /* vcycle!(s, z, r) (src/flip.jl:992-1014): z = M^-1 r for this types/phi. */

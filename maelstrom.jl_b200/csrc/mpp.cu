@@ -14,6 +14,7 @@
 #include "mpp.h"
 #include <cudaTypedefs.h>
 
+#include "mpp_adjoint.cuh"
 #include "mpp_fgmres.cuh"
 #include "mpp_tma.cuh"
 
@@ -74,6 +75,21 @@ enum { F_VOLUME, F_SETUP, F_LEVEL, F_TILES, F_START, F_RBGS, F_RESID, F_RESTRICT
 const char* const FAM_NAMES[NFAM] = {"volume",   "setup",    "coarsen", "tilelists", "start",         "rbgs",
                                      "residual", "restrict", "bottom",   "prolong",  "dot",           "search",
                                      "advance",  "true_residual", "gradient", "convert"};
+constexpr int NGRAPHS = 4;
+struct GraphEntry {
+    cudaGraphExec_t exec;
+    cudaGraph_t graph;
+    const void* key[11];
+    int kind;
+    int g_prologue, g_body, g_epilogue;  // kernel counts in the graph's parts
+    uint64_t used;                       // last use (LRU eviction)
+};
+void drop_graph(GraphEntry& e) {
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+    if (e.graph) cudaGraphDestroy(e.graph);
+    memset(&e, 0, sizeof(e));
+}
+
 struct ProfRec {
     int fam, level;
     cudaEvent_t a, b;
@@ -105,13 +121,11 @@ struct mpp_ctx {
     std::vector<void*> allocs;
     size_t bytes;
     int64_t launches;
-    // graph cache
-    cudaGraphExec_t gexec;
-    cudaGraph_t graph;
-    cudaStream_t cap;  // stream the graph is captured on (never the caller's)
-    const void* gkey[10];
-    int gkind;
-    int g_prologue, g_body, g_epilogue;  // kernel counts in the graph's parts
+    // graph cache: a few captured solves keyed by their arrays (a forward and an adjoint
+    // call alternate in a rollout without re-capturing)
+    GraphEntry gc[NGRAPHS];
+    uint64_t gclock;
+    cudaStream_t cap;  // stream the graphs are captured on (never the caller's)
     // levels lb .. L-1 are solved in one CTA's shared memory (k_bottom)
     int lb;
     BotArgs bot;
@@ -138,6 +152,7 @@ struct mpp_ctx {
     double* fgd_host;  // pinned
     int fg_used, fg_its;
     double fg_residual;
+    void* vjp_beta;  // the adjoint solve's right-hand side (natural, V's type), allocated on first use
 };
 
 namespace {
@@ -561,6 +576,7 @@ struct Call {
     const float* bnat;
     const uint8_t* types;
     const float* phi;
+    const double* bnat64;  // FP64 rhs (the FP64 adjoint), or null
 };
 
 template <class Pr>
@@ -571,6 +587,7 @@ SetupIn<typename Pr::V> setup_in(mpp_ctx* c, const Call& k) {
     in.v = k.kind == 1 ? k.v : nullptr;
     in.w = k.kind == 1 ? k.w : nullptr;
     in.bnat = k.kind == 1 ? nullptr : k.bnat;
+    in.bnat64 = k.kind == 1 ? nullptr : k.bnat64;
     in.P = std::is_same<V, double>::value ? (V*)c->Pd : (V*)k.P;
     in.types = k.types;
     in.phi = k.phi;
@@ -793,20 +810,13 @@ int fallback_and_finish(mpp_ctx* c, const Call& k, cudaStream_t s) {
 }
 
 template <class Pr>
-int build_graph(mpp_ctx* c, const Call& k) {
+int build_graph(mpp_ctx* c, const Call& k, GraphEntry& ge) {
     using V = typename Pr::V;
     cudaStream_t s = c->cap;
-    if (c->gexec) {
-        cudaGraphExecDestroy(c->gexec);
-        c->gexec = nullptr;
-    }
-    if (c->graph) {
-        cudaGraphDestroy(c->graph);
-        c->graph = nullptr;
-    }
+    drop_graph(ge);
     cudaGraph_t g;
     CK(cudaGraphCreate(&g, 0));
-    c->graph = g;
+    ge.graph = g;
     cudaGraphConditionalHandle cond;
     CK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
     Run<Pr> pro{c, s};
@@ -832,14 +842,40 @@ int build_graph(mpp_ctx* c, const Call& k) {
     CK(cudaStreamBeginCaptureToGraph(s, g, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
     record_epilogue<Pr>(epi, k);
     CK(cudaStreamEndCapture(s, &g));
-    CK(cudaGraphInstantiate(&c->gexec, g, 0));
-    c->g_prologue = pro.nk;
-    c->g_body = bod.nk;
-    c->g_epilogue = epi.nk;
-    const void* key[10] = {k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.bnat, k.types, k.phi};
-    memcpy(c->gkey, key, sizeof(key));
-    c->gkind = k.kind;
+    CK(cudaGraphInstantiate(&ge.exec, g, 0));
+    ge.g_prologue = pro.nk;
+    ge.g_body = bod.nk;
+    ge.g_epilogue = epi.nk;
+    const void* key[11] = {k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.bnat, k.types, k.phi, k.bnat64};
+    memcpy(ge.key, key, sizeof(key));
+    ge.kind = k.kind;
     return MPP_OK;
+}
+
+// The cached graph of this call, captured on a miss into the least recently used slot.
+template <class Pr>
+int graph_for(mpp_ctx* c, const Call& k, GraphEntry*& out) {
+    const void* key[11] = {k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.bnat, k.types, k.phi, k.bnat64};
+    GraphEntry* victim = &c->gc[0];
+    for (GraphEntry& e : c->gc) {
+        if (e.exec && e.kind == k.kind && memcmp(key, e.key, sizeof(key)) == 0) {
+            e.used = ++c->gclock;
+            out = &e;
+            return MPP_OK;
+        }
+        if (!e.exec || e.used < victim->used) victim = &e;
+    }
+    if (int e = build_graph<Pr>(c, k, *victim)) {
+        drop_graph(*victim);
+        return e;
+    }
+    victim->used = ++c->gclock;
+    out = victim;
+    return MPP_OK;
+}
+
+void drop_graphs(mpp_ctx* c) {
+    for (GraphEntry& e : c->gc) drop_graph(e);
 }
 
 template <class Pr>
@@ -848,13 +884,11 @@ int solve(mpp_ctx* c, const Call& k, cudaStream_t s) {
     int64_t launched = 0;
     CK(cudaMemsetAsync(&c->sc->s.fault, 0, sizeof(int), s));
     if (c->opts.graph && !c->prof_on) {
-        const void* key[10] = {k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.bnat, k.types, k.phi};
-        if (!c->gexec || c->gkind != k.kind || memcmp(key, c->gkey, sizeof(key)) != 0) {
-            if (int e = build_graph<Pr>(c, k)) return e;
-        }
-        CK(cudaGraphLaunch(c->gexec, s));
+        GraphEntry* ge = nullptr;
+        if (int e = graph_for<Pr>(c, k, ge)) return e;
+        CK(cudaGraphLaunch(ge->exec, s));
         if (int e = read_state(c, s)) return e;
-        launched = c->g_prologue + (int64_t)c->g_body * c->sc_host->s.it + c->g_epilogue;
+        launched = ge->g_prologue + (int64_t)ge->g_body * c->sc_host->s.it + ge->g_epilogue;
     } else {
         Run<Pr> run{c, s};
         record_prologue<Pr>(run, k, 0, 0);
@@ -1043,8 +1077,7 @@ const char* mpp_version(void) { return "libmpp 0.1 (sm_100a)"; }
 
 int mpp_ctx_destroy(mpp_ctx* c) {
     if (!c) return MPP_OK;
-    if (c->gexec) cudaGraphExecDestroy(c->gexec);
-    if (c->graph) cudaGraphDestroy(c->graph);
+    drop_graphs(c);
     for (void* p : c->allocs) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
     if (c->fgd_host) cudaFreeHost(c->fgd_host);
@@ -1107,8 +1140,8 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
     c->prec = o->precision;
     c->L = g->levels;
     c->diag = c->bvec = c->r = c->d = c->q = c->Pd = nullptr;
-    c->gexec = nullptr;
-    c->graph = nullptr;
+    memset(c->gc, 0, sizeof(c->gc));
+    c->gclock = 0;
     c->bytes = 0;
     c->launches = 0;
     c->sc_host = nullptr;
@@ -1123,6 +1156,7 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
     c->fgd_host = nullptr;
     c->fg_used = c->fg_its = 0;
     c->fg_residual = 0.0;
+    c->vjp_beta = nullptr;
     auto fail = [&](int e) {
         mpp_ctx_destroy(c);
         return e;
@@ -1272,10 +1306,7 @@ int mpp_ctx_set_opts(mpp_ctx* c, const mpp_opts* o) {
     }
     if (o->sweeps != c->opts.sweeps || o->coarse != c->opts.coarse || o->graph != c->opts.graph ||
         (o->fallback != 0) != (c->opts.fallback != 0)) {
-        if (c->gexec) cudaGraphExecDestroy(c->gexec);
-        if (c->graph) cudaGraphDestroy(c->graph);
-        c->gexec = nullptr;
-        c->graph = nullptr;
+        drop_graphs(c);
     }
     c->opts = *o;
     return MPP_OK;
@@ -1349,6 +1380,74 @@ int mpp_project(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8_t* 
     if (e < 0) return e;
     fill_result(c, res, c->launches - before);
     return c->sc_host->s.status;
+}
+
+int mpp_project_vjp(mpp_ctx* c, const float* gu, const float* gv, const float* gw, float* ou, float* ov, float* ow,
+                    float* mu, const uint8_t* types, const float* phi, mpp_result* res, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!gu || !gv || !gw || !ou || !ov || !ow || !mu || !types || !phi) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n1 = c->grid.n[0], n2 = c->grid.n[1], n3 = c->grid.n[2];
+    const int64_t N = (int64_t)n1 * n2 * n3, NF = (int64_t)(n1 + 1) * (n2 + 1) * (n3 + 1);
+    // the FP64 form keeps beta and mu in FP64 (mu's float copy is the warm start and output)
+    const bool f64 = c->prec == MPP_PREC_FP64;
+    if (!c->vjp_beta)
+        if (int e = alloc(c, &c->vjp_beta, (f64 ? sizeof(double) : sizeof(float)) * (size_t)N)) return e;
+    const int64_t before = c->launches;
+    if (f64) launch(k_vjp_rhs<double>, grid_cells(c, N), TPB, 0, s, n1, n2, n3, (double*)c->vjp_beta, gu, gv, gw, types, phi);
+    else launch(k_vjp_rhs<float>, grid_cells(c, N), TPB, 0, s, n1, n2, n3, (float*)c->vjp_beta, gu, gv, gw, types, phi);
+    c->launches++;
+    CK(cudaGetLastError());
+    if (int e = write_params(c, 1.f, 1.0, 1.0, 0, 0.f, s)) return e;
+    Call k{0,  nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, mu, f64 ? nullptr : (const float*)c->vjp_beta,
+           types, phi, f64 ? (const double*)c->vjp_beta : nullptr};
+    int e = dispatch(c->prec, [&](auto pr) { return solve<decltype(pr)>(c, k, s); });
+    if (e < 0) return e;
+    if (f64)
+        launch(k_vjp_faces<double>, grid_cells(c, NF), TPB, 0, s, n1, n2, n3, ou, ov, ow, gu, gv, gw,
+               (const double*)c->Pd, types);
+    else
+        launch(k_vjp_faces<float>, grid_cells(c, NF), TPB, 0, s, n1, n2, n3, ou, ov, ow, gu, gv, gw, (const float*)mu,
+               types);
+    c->launches++;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    fill_result(c, res, c->launches - before);
+    return c->sc_host->s.status;
+}
+
+int mpp_vjp_rhs(mpp_ctx* c, float* beta, const float* gu, const float* gv, const float* gw, const uint8_t* types,
+                const float* phi, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!beta || !gu || !gv || !gw || !types || !phi) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n1 = c->grid.n[0], n2 = c->grid.n[1], n3 = c->grid.n[2];
+    launch(k_vjp_rhs<float>, grid_cells(c, (int64_t)n1 * n2 * n3), TPB, 0, s, n1, n2, n3, beta, gu, gv, gw, types, phi);
+    c->launches++;
+    CK(cudaGetLastError());
+    return MPP_OK;
+}
+
+int mpp_vjp_faces(mpp_ctx* c, float* ou, float* ov, float* ow, const float* gu, const float* gv, const float* gw,
+                  const float* mu, const uint8_t* types, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!ou || !ov || !ow || !gu || !gv || !gw || !mu || !types) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n1 = c->grid.n[0], n2 = c->grid.n[1], n3 = c->grid.n[2];
+    launch(k_vjp_faces<float>, grid_cells(c, (int64_t)(n1 + 1) * (n2 + 1) * (n3 + 1)), TPB, 0, s, n1, n2, n3, ou, ov,
+           ow, gu, gv, gw, mu, types);
+    c->launches++;
+    CK(cudaGetLastError());
+    return MPP_OK;
 }
 
 int mpp_pressure(mpp_ctx* c, float* P, const float* b, const uint8_t* types, const float* phi, mpp_result* res,

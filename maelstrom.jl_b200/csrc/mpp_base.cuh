@@ -136,6 +136,7 @@ struct SetupIn {
     const float* v;
     const float* w;
     const float* bnat;  // given rhs (natural), or null
+    const double* bnat64;  // given FP64 rhs (natural; the FP64 adjoint), or null
     V* P;               // pressure (natural): warm start in
     const uint8_t* types;
     const float* phi;   // null: no ghost-fluid terms (rhs-only passes)
@@ -192,7 +193,9 @@ __global__ void __launch_bounds__(TPB)
                     d += (C)1 / theta<C>(phc, (C)a.phi[(int64_t)ii + (int64_t)n1 * ((int64_t)jj + (int64_t)n2 * kk)]);
             }
             code |= SELF;
-            if (a.bnat) {
+            if (a.bnat64) {
+                bv = (C)a.bnat64[idx];
+            } else if (a.bnat) {
                 bv = (C)a.bnat[idx];
             } else if (a.u) {
                 C div = (C)a.u[(int64_t)(i + 1) + (int64_t)(n1 + 1) * ((int64_t)j + (int64_t)n2 * k)] -

@@ -27,7 +27,7 @@ from . import _lib
 from ._lib import MppError, Result, check
 from . import scene
 
-__all__ = ["Projector", "FlipBasin", "project", "pressure", "MppError", "scene", "load"]
+__all__ = ["Projector", "FlipBasin", "project", "pressure", "project_vjp", "MppError", "scene", "load"]
 
 
 def load():
@@ -141,6 +141,43 @@ class Projector:
                                     _stream_ptr(stream)))
         return res
 
+    def project_vjp(self, gu, gv, gw, mu, types, phi, out=None, stream=None) -> Result:
+        """The adjoint of :meth:`project` w.r.t. (u, v, w) (``mpp_project_vjp``): the
+        cotangent (gu, gv, gw) of the output faces in, the input faces' cotangent out
+        (into ``out`` = (ou, ov, ow), default in place); ``mu`` is the adjoint pressure's
+        warm start and result."""
+        import torch
+
+        g = self.grid
+        for t, name, axis in ((gu, "gu", 0), (gv, "gv", 1), (gw, "gw", 2)):
+            _require(t, torch.float32, int(np.prod(g.face_shape(axis))), name)
+        ou, ov, ow = out if out is not None else (gu, gv, gw)
+        for t, name, axis in ((ou, "ou", 0), (ov, "ov", 1), (ow, "ow", 2)):
+            _require(t, torch.float32, int(np.prod(g.face_shape(axis))), name)
+        _require(mu, torch.float32, g.ncells, "mu")
+        _require(types, torch.uint8, g.ncells, "types")
+        _require(phi, torch.float32, g.ncells, "phi")
+        res = Result()
+        check(self.lib.mpp_project_vjp(self._ctx, _ptr(gu), _ptr(gv), _ptr(gw), _ptr(ou), _ptr(ov), _ptr(ow),
+                                       _ptr(mu), _ptr(types), _ptr(phi), ctypes.byref(res), _stream_ptr(stream)))
+        return res
+
+    def vjp_rhs(self, gu, gv, gw, types, phi, stream=None):
+        import torch
+
+        beta = torch.empty(self.grid.ncells, dtype=torch.float32, device=gu.device)
+        check(self.lib.mpp_vjp_rhs(self._ctx, _ptr(beta), _ptr(gu), _ptr(gv), _ptr(gw), _ptr(types), _ptr(phi),
+                                   _stream_ptr(stream)))
+        return beta
+
+    def vjp_faces(self, gu, gv, gw, mu, types, stream=None):
+        import torch
+
+        outs = [torch.empty_like(a) for a in (gu, gv, gw)]
+        check(self.lib.mpp_vjp_faces(self._ctx, *(_ptr(o) for o in outs), _ptr(gu), _ptr(gv), _ptr(gw), _ptr(mu),
+                                     _ptr(types), _stream_ptr(stream)))
+        return outs
+
     def volume(self, phi, stream=None) -> float:
         import torch
 
@@ -242,6 +279,23 @@ class FlipBasin:
         s.projector = Projector(g, **projector_kw)
         s.volume0 = s.projector.volume(s.phi)  # initialize!: s.volume0 = volume(s) (src/flip.jl:346)
         return s
+
+
+def project_vjp(s: FlipBasin, gu, gv, gw, mu=None):
+    """The pullback of ``project!(s, dt)`` w.r.t. (s.u, s.v, s.w) at the basin's current
+    types and phi (the rrule's pullback): the output faces' cotangent in, in place, the
+    input faces' cotangent out. ``mu`` (adjoint pressure) defaults to a zero start kept
+    on the basin for the next call's warm start."""
+    import torch
+
+    if mu is None:
+        if getattr(s, "mu", None) is None:
+            s.mu = torch.zeros(s.grid.ncells, dtype=torch.float32, device=s.P.device)
+        mu = s.mu
+    res = s.projector.project_vjp(gu, gv, gw, mu, s.types, s.phi)
+    s.last_vjp = res
+    _raise_or_warn(res)
+    return gu, gv, gw
 
 
 def _raise_or_warn(res: Result, bnorm_ok=True):

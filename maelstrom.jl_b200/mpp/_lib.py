@@ -60,6 +60,9 @@ SIGNATURES = {
     "mpp_volume_noalloc": (ctypes.c_int, [_G, P, ctypes.POINTER(F64), P]),
     "mpp_project": (ctypes.c_int, [P, P, P, P, P, P, P, P, P, P, F32, F64, F64, _R, P]),
     "mpp_pressure": (ctypes.c_int, [P, P, P, P, P, _R, P]),
+    "mpp_project_vjp": (ctypes.c_int, [P, P, P, P, P, P, P, P, P, P, _R, P]),
+    "mpp_vjp_rhs": (ctypes.c_int, [P, P, P, P, P, P, P, P]),
+    "mpp_vjp_faces": (ctypes.c_int, [P, P, P, P, P, P, P, P, P, P]),
     "mpp_rhs": (ctypes.c_int, [P, P, P, P, P, P, F32, P]),
     "mpp_diag": (ctypes.c_int, [P, P, P, P, P]),
     "mpp_vcycle": (ctypes.c_int, [P, P, P, P, P, P]),

@@ -58,6 +58,11 @@ def lib():
             "orc_pressure_f64": (i32, [G, P, P, P, P, d, i32, i32, i32, I]),
             "orc_project_f32": (i32, [G, P, P, P, P, P, P, P, P, P, f, d, d, f, i32, i32, i32, I]),
             "orc_project_f64": (i32, [G, P, P, P, P, P, P, P, P, P, d, d, d, d, i32, i32, i32, I]),
+            "orc_vjp_rhs_f32": (None, [G, P, P, P, P, P, P]), "orc_vjp_rhs_f64": (None, [G, P, P, P, P, P, P]),
+            "orc_vjp_faces_f32": (None, [G, P, P, P, P, P, P, P, P]),
+            "orc_vjp_faces_f64": (None, [G, P, P, P, P, P, P, P, P]),
+            "orc_project_vjp_f32": (i32, [G, P, P, P, P, P, P, f, i32, i32, i32, I]),
+            "orc_project_vjp_f64": (i32, [G, P, P, P, P, P, P, d, i32, i32, i32, I]),
             "orc_num_threads": (i32, []), "orc_set_num_threads": (None, [i32]),
         }
         for name, (res, args) in sig.items():
@@ -168,6 +173,43 @@ def project(basin, P=None, *, volume0=None, dt=1.0 / 48, recover=0.5, tol=1e-4, 
                                            _p(P), _p(np.ascontiguousarray(basin.types, dtype=np.uint8)), _p(phi),
                                            volume0, dt, recover, tol, maxiter, sweeps, coarse, ctypes.byref(info))
     return dict(u=u, v=v, w=w, fu=fu, fv=fv, fw=fw, P=P, info=info)
+
+
+def vjp_rhs(grid, gu, gv, gw, types, phi, prec=32):
+    """beta = dx G^T g on LIQUID cells (the adjoint of project_kernel!, src/flip.jl:1113-1130)."""
+    t = _ft(prec)
+    beta = np.zeros(grid.ncells, dtype=t)
+    getattr(lib(), f"orc_vjp_rhs_f{prec}")(ctypes.byref(_grid(grid)), _p(beta),
+                                           *(_p(np.ascontiguousarray(a, dtype=t)) for a in (gu, gv, gw)),
+                                           _p(np.ascontiguousarray(types, dtype=np.uint8)),
+                                           _p(np.ascontiguousarray(phi, dtype=t)))
+    return beta
+
+
+def vjp_faces(grid, gu, gv, gw, mu, types, prec=32):
+    """g_in = g + D^T mu (the adjoint of rhs_kernel!'s divergence, src/flip.jl:817-822)."""
+    t = _ft(prec)
+    outs = [np.zeros(np.size(a), dtype=t) for a in (gu, gv, gw)]
+    getattr(lib(), f"orc_vjp_faces_f{prec}")(ctypes.byref(_grid(grid)), *(_p(o) for o in outs),
+                                             *(_p(np.ascontiguousarray(a, dtype=t)) for a in (gu, gv, gw)),
+                                             _p(np.ascontiguousarray(mu, dtype=t)),
+                                             _p(np.ascontiguousarray(types, dtype=np.uint8)))
+    return outs
+
+
+def project_vjp(basin, gu, gv, gw, mu=None, *, tol=1e-4, maxiter=60, sweeps=2, coarse=40, prec=32):
+    """The adjoint of project! w.r.t. (u, v, w) at the basin's types and phi: returns
+    dict(gu, gv, gw, mu, info) for the output-face cotangent (gu, gv, gw)."""
+    g = basin.grid
+    t = _ft(prec)
+    gu, gv, gw = (np.array(a, dtype=t, copy=True) for a in (gu, gv, gw))
+    mu = np.zeros(g.ncells, dtype=t) if mu is None else np.array(mu, dtype=t, copy=True)
+    info = Info()
+    getattr(lib(), f"orc_project_vjp_f{prec}")(ctypes.byref(_grid(g)), _p(gu), _p(gv), _p(gw), _p(mu),
+                                               _p(np.ascontiguousarray(basin.types, dtype=np.uint8)),
+                                               _p(np.ascontiguousarray(basin.phi, dtype=t)), tol, maxiter, sweeps,
+                                               coarse, ctypes.byref(info))
+    return dict(gu=gu, gv=gv, gw=gw, mu=mu, info=info)
 
 
 def num_threads() -> int:

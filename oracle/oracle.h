@@ -93,6 +93,21 @@ int orc_project_f64(const orc_grid* g, double* u, double* v, double* w, uint8_t*
                     double dt, double recover, double tol, int maxiter, int sweeps, int coarse,
                     orc_info* info);
 
+/* The adjoint of project! w.r.t. the face velocities (derived from src/flip.jl:817-822 and
+ * 1113-1130; the reference has none): beta = dx G^T g, A mu = beta, g_in = g + D^T mu. */
+void orc_vjp_rhs_f32(const orc_grid* g, float* beta, const float* gu, const float* gv, const float* gw,
+                     const uint8_t* types, const float* phi);
+void orc_vjp_rhs_f64(const orc_grid* g, double* beta, const double* gu, const double* gv, const double* gw,
+                     const uint8_t* types, const double* phi);
+void orc_vjp_faces_f32(const orc_grid* g, float* ou, float* ov, float* ow, const float* gu, const float* gv,
+                       const float* gw, const float* mu, const uint8_t* types);
+void orc_vjp_faces_f64(const orc_grid* g, double* ou, double* ov, double* ow, const double* gu, const double* gv,
+                       const double* gw, const double* mu, const uint8_t* types);
+int orc_project_vjp_f32(const orc_grid* g, float* gu, float* gv, float* gw, float* mu, const uint8_t* types,
+                        const float* phi, float tol, int maxiter, int sweeps, int coarse, orc_info* info);
+int orc_project_vjp_f64(const orc_grid* g, double* gu, double* gv, double* gw, double* mu, const uint8_t* types,
+                        const double* phi, double tol, int maxiter, int sweeps, int coarse, orc_info* info);
+
 int orc_num_threads(void);
 void orc_set_num_threads(int n);
 

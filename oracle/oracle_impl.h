@@ -534,4 +534,77 @@ int FN(orc_project_)(const orc_grid* g, R* u, R* v, R* w, uint8_t* fu, uint8_t* 
     return its;
 }
 
+/* ---- the adjoint of project! w.r.t. the face velocities (not in the reference; derived
+ * from its forward kernels rhs_kernel! src/flip.jl:817-822 and project_kernel!
+ * src/flip.jl:1113-1130): beta = dx G^T g, A mu = beta, g_in = g + D^T mu. ---- */
+
+/* One face of LIQUID cell c seen from c: w g, w = 1 towards LIQUID, 1/theta towards AIR,
+ * the face dropped towards SOLID (project_kernel!'s `ok`). */
+static inline R FN(vjp_term_)(const R* gf, size_t fi, const uint8_t* t, const R* phi, int n1, int n2, int n3,
+                              size_t c, int a, int b, int cc) {
+    uint8_t tn = typeat(t, n1, n2, n3, a, b, cc);
+    if (tn == SOLID) return (R)0;
+    if (tn == LIQUID) return gf[fi];
+    return gf[fi] / FN(theta_)(phi[c], phi[ID(n1, n2, a, b, cc)]);
+}
+
+/* beta_c = (low faces) - (high faces) of w g, in the order -x, +x, -y, +y, -z, +z. */
+void FN(orc_vjp_rhs_)(const orc_grid* g, R* beta, const R* gu, const R* gv, const R* gw, const uint8_t* types,
+                      const R* phi) {
+    const int n1 = g->n[0], n2 = g->n[1], n3 = g->n[2];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < n3; k++)
+        for (int j = 0; j < n2; j++)
+            for (int i = 0; i < n1; i++) {
+                size_t c = ID(n1, n2, i, j, k);
+                R s = 0;
+                if (types[c] == LIQUID) {
+                    size_t fu = ID(n1 + 1, n2, i, j, k), fv = ID(n1, n2 + 1, i, j, k), fw = ID(n1, n2, i, j, k);
+                    s = s + FN(vjp_term_)(gu, fu, types, phi, n1, n2, n3, c, i - 1, j, k);
+                    s = s - FN(vjp_term_)(gu, ID(n1 + 1, n2, i + 1, j, k), types, phi, n1, n2, n3, c, i + 1, j, k);
+                    s = s + FN(vjp_term_)(gv, fv, types, phi, n1, n2, n3, c, i, j - 1, k);
+                    s = s - FN(vjp_term_)(gv, ID(n1, n2 + 1, i, j + 1, k), types, phi, n1, n2, n3, c, i, j + 1, k);
+                    s = s + FN(vjp_term_)(gw, fw, types, phi, n1, n2, n3, c, i, j, k - 1);
+                    s = s - FN(vjp_term_)(gw, ID(n1, n2, i, j, k + 1), types, phi, n1, n2, n3, c, i, j, k + 1);
+                }
+                beta[c] = s;
+            }
+}
+
+/* g_in = g + mu_before [before LIQUID] - mu_after [after LIQUID], one axis. */
+static void FN(vjp_axis_)(const orc_grid* g, R* out, const R* gf, const R* mu, const uint8_t* t, int axis) {
+    const int n1 = g->n[0], n2 = g->n[1], n3 = g->n[2];
+    const int e1 = n1 + (axis == 0), e2 = n2 + (axis == 1), e3 = n3 + (axis == 2);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < e3; k++)
+        for (int j = 0; j < e2; j++)
+            for (int i = 0; i < e1; i++) {
+                int a = i - (axis == 0), bb = j - (axis == 1), cc = k - (axis == 2);
+                size_t fi = ID(e1, e2, i, j, k);
+                R r = gf[fi];
+                if (typeat(t, n1, n2, n3, a, bb, cc) == LIQUID) r = r + mu[ID(n1, n2, a, bb, cc)];
+                if (typeat(t, n1, n2, n3, i, j, k) == LIQUID) r = r - mu[ID(n1, n2, i, j, k)];
+                out[fi] = r;
+            }
+}
+
+void FN(orc_vjp_faces_)(const orc_grid* g, R* ou, R* ov, R* ow, const R* gu, const R* gv, const R* gw,
+                        const R* mu, const uint8_t* types) {
+    FN(vjp_axis_)(g, ou, gu, mu, types, 0);
+    FN(vjp_axis_)(g, ov, gv, mu, types, 1);
+    FN(vjp_axis_)(g, ow, gw, mu, types, 2);
+}
+
+/* The whole adjoint: (gu, gv, gw) in, g_in out in place; mu the warm start in, out. */
+int FN(orc_project_vjp_)(const orc_grid* g, R* gu, R* gv, R* gw, R* mu, const uint8_t* types, const R* phi,
+                         R tol, int maxiter, int sweeps, int coarse, orc_info* info) {
+    const size_t N = (size_t)g->n[0] * g->n[1] * g->n[2];
+    R* beta = (R*)calloc(N, sizeof(R));
+    FN(orc_vjp_rhs_)(g, beta, gu, gv, gw, types, phi);
+    int its = FN(orc_pressure_)(g, mu, beta, types, phi, tol, maxiter, sweeps, coarse, info);
+    FN(orc_vjp_faces_)(g, gu, gv, gw, gu, gv, gw, mu, types);
+    free(beta);
+    return its;
+}
+
 #undef FN
