@@ -154,6 +154,23 @@ int mpp_vjp_rhs(mpp_ctx* ctx, float* beta, const float* gu, const float* gv, con
 int mpp_vjp_faces(mpp_ctx* ctx, float* ou, float* ov, float* ow, const float* gu, const float* gv,
                   const float* gw, const float* mu, const uint8_t* types, mpp_stream stream);
 
+/* advect! of the face velocities through themselves (advect_kernel!, src/flip.jl:357-369,
+ * 495-497): ou, ov, ow = u, v, w sampled at the nodes traced back over dt in RK2 sub-steps
+ * of at most a cell (at most 32). The outputs must not overlap the inputs. */
+int mpp_advect(mpp_ctx* ctx, float* ou, float* ov, float* ow, const float* u, const float* v, const float* w,
+               float dt, mpp_stream stream);
+/* The same for the cell-centred level set (COFF samples). */
+int mpp_advect_phi(mpp_ctx* ctx, float* ophi, const float* phi, const float* u, const float* v, const float* w,
+                   float dt, mpp_stream stream);
+/* The adjoint of mpp_advect (no reference counterpart; the reverse of its steps): the
+ * cotangent (gou, gov, gow) of its outputs in; du, dv, dw = the cotangent of (u, v, w),
+ * through both the sampled arrays and the traced positions. The sub-step count is
+ * piecewise constant and has no derivative; a clamp passes the derivative on its closed
+ * range. Sums are FP64 atomics rounded once to Float32 (not bitwise reproducible run to
+ * run). du, dv, dw may be gou, gov, gow. */
+int mpp_advect_vjp(mpp_ctx* ctx, const float* gou, const float* gov, const float* gow, const float* u,
+                   const float* v, const float* w, float dt, float* du, float* dv, float* dw, mpp_stream stream);
+
 /* diag_kernel! (src/flip.jl:824-836). */
 int mpp_diag(mpp_ctx* ctx, float* diag, const uint8_t* types, const float* phi, mpp_stream stream);
 /* vcycle!(s, z, r) (src/flip.jl:992-1014): z = M^-1 r for this types/phi. */

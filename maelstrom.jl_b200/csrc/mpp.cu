@@ -15,6 +15,7 @@
 #include <cudaTypedefs.h>
 
 #include "mpp_adjoint.cuh"
+#include "mpp_advect.cuh"
 #include "mpp_fgmres.cuh"
 #include "mpp_tma.cuh"
 
@@ -153,6 +154,7 @@ struct mpp_ctx {
     int fg_used, fg_its;
     double fg_residual;
     void* vjp_beta;  // the adjoint solve's right-hand side (natural, V's type), allocated on first use
+    double* adv_acc[3];  // FP64 accumulators of the advection adjoint (face shapes), on first use
 };
 
 namespace {
@@ -218,9 +220,9 @@ int grid_tiles1(const mpp_ctx* c, int l) {
 // Kernel launches: programmatic dependent launch (see pdl_wait in mpp_common.cuh), so a
 // kernel's blocks can be scheduled while the previous kernel drains.
 template <typename... KArgs, typename... Args>
-void launch(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
+void launch(void (*kern)(KArgs...), dim3 grid, int block, size_t smem, cudaStream_t st, Args... args) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)grid);
+    cfg.gridDim = grid;
     cfg.blockDim = dim3((unsigned)block);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
@@ -1157,6 +1159,7 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
     c->fg_used = c->fg_its = 0;
     c->fg_residual = 0.0;
     c->vjp_beta = nullptr;
+    for (int a = 0; a < 3; a++) c->adv_acc[a] = nullptr;
     auto fail = [&](int e) {
         mpp_ctx_destroy(c);
         return e;
@@ -1417,6 +1420,117 @@ int mpp_project_vjp(mpp_ctx* c, const float* gu, const float* gv, const float* g
     CK(cudaStreamSynchronize(s));
     fill_result(c, res, c->launches - before);
     return c->sc_host->s.status;
+}
+
+// ---- semi-Lagrangian advection and its adjoint ----
+static Flow flow_of(const mpp_ctx* c, const float* u, const float* v, const float* w) {
+    Flow fl;
+    const float* f[3] = {u, v, w};
+    for (int a = 0; a < 3; a++) {
+        fl.f[a] = f[a];
+        for (int e = 0; e < 3; e++) fl.d[a][e] = c->grid.n[e] + (a == e);
+        fl.lo[a] = c->grid.lo[a];
+    }
+    fl.dx = c->grid.dx;
+    return fl;
+}
+
+static void adv_slot(const mpp_ctx* c, AdvArrays& A, int slot, float* out, const float* src, int axis) {
+    A.out[slot] = out;
+    A.src[slot] = src;
+    A.n[slot] = 1;
+    for (int e = 0; e < 3; e++) {
+        A.d[slot][e] = c->grid.n[e] + (axis == e);
+        A.off[slot][e] = axis < 0 ? 0.5f : (axis == e ? 0.f : 0.5f);  // COFF, or UOFF/VOFF/WOFF
+        A.n[slot] *= A.d[slot][e];
+    }
+}
+
+static int grid_of(const mpp_ctx* c, const AdvArrays& A, int na) {
+    int64_t n = 0;
+    for (int a = 0; a < na; a++) n = A.n[a] > n ? A.n[a] : n;
+    return grid_cells(c, n);
+}
+
+static bool overlaps(const float* a, int64_t na, const float* b, int64_t nb) {
+    return a < b + nb && b < a + na;
+}
+
+int mpp_advect(mpp_ctx* c, float* ou, float* ov, float* ow, const float* u, const float* v, const float* w, float dt,
+               mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!ou || !ov || !ow || !u || !v || !w || !(dt >= 0.f)) {
+        set_err("null array or negative dt");
+        return MPP_ERR_INVALID;
+    }
+    AdvArrays A;
+    memset(&A, 0, sizeof(A));
+    float* outs[3] = {ou, ov, ow};
+    const float* ins[3] = {u, v, w};
+    for (int a = 0; a < 3; a++) adv_slot(c, A, a, outs[a], ins[a], a);
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+            if (overlaps(outs[a], A.n[a], ins[b], A.n[b])) {
+                set_err("advection output overlaps an input velocity array");
+                return MPP_ERR_INVALID;
+            }
+    cudaStream_t s = (cudaStream_t)stream;
+    launch(k_advect, dim3(grid_of(c, A, 3), 3), TPB, 0, s, flow_of(c, u, v, w), A, dt);
+    c->launches++;
+    CK(cudaGetLastError());
+    return MPP_OK;
+}
+
+int mpp_advect_phi(mpp_ctx* c, float* ophi, const float* phi, const float* u, const float* v, const float* w, float dt,
+                   mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!ophi || !phi || !u || !v || !w || !(dt >= 0.f)) {
+        set_err("null array or negative dt");
+        return MPP_ERR_INVALID;
+    }
+    AdvArrays A;
+    memset(&A, 0, sizeof(A));
+    adv_slot(c, A, 0, ophi, phi, -1);
+    if (overlaps(ophi, A.n[0], phi, A.n[0])) {
+        set_err("advection output overlaps its input");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    launch(k_advect, dim3(grid_of(c, A, 1), 1), TPB, 0, s, flow_of(c, u, v, w), A, dt);
+    c->launches++;
+    CK(cudaGetLastError());
+    return MPP_OK;
+}
+
+int mpp_advect_vjp(mpp_ctx* c, const float* gou, const float* gov, const float* gow, const float* u, const float* v,
+                   const float* w, float dt, float* du, float* dv, float* dw, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!gou || !gov || !gow || !u || !v || !w || !du || !dv || !dw || !(dt >= 0.f)) {
+        set_err("null array or negative dt");
+        return MPP_ERR_INVALID;
+    }
+    AdvArrays A;
+    memset(&A, 0, sizeof(A));
+    const float* gos[3] = {gou, gov, gow};
+    const float* ins[3] = {u, v, w};
+    float* outs[3] = {du, dv, dw};
+    for (int a = 0; a < 3; a++) adv_slot(c, A, a, const_cast<float*>(gos[a]), ins[a], a);
+    cudaStream_t s = (cudaStream_t)stream;
+    AdvAcc acc;
+    memset(&acc, 0, sizeof(acc));
+    for (int a = 0; a < 3; a++) {
+        if (!c->adv_acc[a])
+            if (int e = alloc(c, (void**)&c->adv_acc[a], sizeof(double) * (size_t)A.n[a])) return e;
+        CK(cudaMemsetAsync(c->adv_acc[a], 0, sizeof(double) * (size_t)A.n[a], s));
+        acc.src[a] = acc.flow[a] = c->adv_acc[a];
+    }
+    launch(k_advect_vjp, dim3(grid_of(c, A, 3) * 2, 3), 128, 0, s, flow_of(c, u, v, w), A, acc, dt);
+    for (int a = 0; a < 3; a++)
+        launch(k_acc_round, grid_cells(c, A.n[a]), TPB, 0, s, outs[a], (const double*)c->adv_acc[a],
+               (const float*)nullptr, A.n[a]);
+    c->launches += 4;
+    CK(cudaGetLastError());
+    return MPP_OK;
 }
 
 int mpp_vjp_rhs(mpp_ctx* c, float* beta, const float* gu, const float* gv, const float* gw, const uint8_t* types,

@@ -162,6 +162,38 @@ class Projector:
                                        _ptr(mu), _ptr(types), _ptr(phi), ctypes.byref(res), _stream_ptr(stream)))
         return res
 
+    def advect(self, u, v, w, dt, out=None, stream=None):
+        """advect! of the face velocities through themselves (``mpp_advect``): returns the
+        advected (u, v, w), into ``out`` when given (which must not overlap the inputs)."""
+        import torch
+
+        g = self.grid
+        for t, name, axis in ((u, "u", 0), (v, "v", 1), (w, "w", 2)):
+            _require(t, torch.float32, int(np.prod(g.face_shape(axis))), name)
+        outs = out if out is not None else [torch.empty_like(a) for a in (u, v, w)]
+        check(self.lib.mpp_advect(self._ctx, *(_ptr(o) for o in outs), _ptr(u), _ptr(v), _ptr(w), float(dt),
+                                  _stream_ptr(stream)))
+        return outs
+
+    def advect_phi(self, phi, u, v, w, dt, stream=None):
+        import torch
+
+        _require(phi, torch.float32, self.grid.ncells, "phi")
+        out = torch.empty_like(phi)
+        check(self.lib.mpp_advect_phi(self._ctx, _ptr(out), _ptr(phi), _ptr(u), _ptr(v), _ptr(w), float(dt),
+                                      _stream_ptr(stream)))
+        return out
+
+    def advect_vjp(self, gu, gv, gw, u, v, w, dt, out=None, stream=None):
+        """The adjoint of :meth:`advect` at velocity (u, v, w): the advected faces'
+        cotangent in, (u, v, w)'s out (into ``out``, which may be the cotangent itself)."""
+        import torch
+
+        outs = out if out is not None else [torch.empty_like(a) for a in (gu, gv, gw)]
+        check(self.lib.mpp_advect_vjp(self._ctx, _ptr(gu), _ptr(gv), _ptr(gw), _ptr(u), _ptr(v), _ptr(w), float(dt),
+                                      *(_ptr(o) for o in outs), _stream_ptr(stream)))
+        return outs
+
     def vjp_rhs(self, gu, gv, gw, types, phi, stream=None):
         import torch
 

@@ -62,6 +62,9 @@ SIGNATURES = {
     "mpp_pressure": (ctypes.c_int, [P, P, P, P, P, _R, P]),
     "mpp_project_vjp": (ctypes.c_int, [P, P, P, P, P, P, P, P, P, P, _R, P]),
     "mpp_vjp_rhs": (ctypes.c_int, [P, P, P, P, P, P, P, P]),
+    "mpp_advect": (ctypes.c_int, [P, P, P, P, P, P, P, F32, P]),
+    "mpp_advect_phi": (ctypes.c_int, [P, P, P, P, P, P, F32, P]),
+    "mpp_advect_vjp": (ctypes.c_int, [P, P, P, P, P, P, P, F32, P, P, P, P]),
     "mpp_vjp_faces": (ctypes.c_int, [P, P, P, P, P, P, P, P, P, P]),
     "mpp_rhs": (ctypes.c_int, [P, P, P, P, P, P, F32, P]),
     "mpp_diag": (ctypes.c_int, [P, P, P, P, P]),

@@ -63,6 +63,10 @@ def lib():
             "orc_vjp_faces_f64": (None, [G, P, P, P, P, P, P, P, P]),
             "orc_project_vjp_f32": (i32, [G, P, P, P, P, P, P, f, i32, i32, i32, I]),
             "orc_project_vjp_f64": (i32, [G, P, P, P, P, P, P, d, i32, i32, i32, I]),
+            "orc_advect_f32": (None, [G, P, P, P, P, P, P, P, f]),
+            "orc_advect_f64": (None, [G, P, P, P, P, P, P, P, d]),
+            "orc_advect_vjp_f32": (None, [G, P, P, P, P, P, P, P, f, P, P, P, P]),
+            "orc_advect_vjp_f64": (None, [G, P, P, P, P, P, P, P, d, P, P, P, P]),
             "orc_num_threads": (i32, []), "orc_set_num_threads": (None, [i32]),
         }
         for name, (res, args) in sig.items():
@@ -210,6 +214,76 @@ def project_vjp(basin, gu, gv, gw, mu=None, *, tol=1e-4, maxiter=60, sweeps=2, c
                                                _p(np.ascontiguousarray(basin.phi, dtype=t)), tol, maxiter, sweeps,
                                                coarse, ctypes.byref(info))
     return dict(gu=gu, gv=gv, gw=gw, mu=mu, info=info)
+
+
+UOFF, VOFF, WOFF, COFF = (0.0, 0.5, 0.5), (0.5, 0.0, 0.5), (0.5, 0.5, 0.0), (0.5, 0.5, 0.5)
+
+
+def _face_dims(grid, axis):
+    n = list(grid.n)
+    if axis is not None:
+        n[axis] += 1
+    return np.array(n, dtype=np.int32)
+
+
+def advect(grid, src, axis, u, v, w, dt, prec=32):
+    """advect_kernel! (src/flip.jl:357-369) of one array: a face array (axis 0, 1, 2) or the
+    cell-centred level set (axis None)."""
+    t = _ft(prec)
+    dims = _face_dims(grid, axis)
+    off = np.array((UOFF, VOFF, WOFF)[axis] if axis is not None else COFF, dtype=t)
+    out = np.zeros(int(np.prod(dims)), dtype=t)
+    getattr(lib(), f"orc_advect_f{prec}")(ctypes.byref(_grid(grid)), _p(out), _p(np.ascontiguousarray(src, dtype=t)),
+                                          _p(dims), _p(off),
+                                          *(_p(np.ascontiguousarray(a, dtype=t)) for a in (u, v, w)), dt)
+    return out
+
+
+def advect_velocity(grid, u, v, w, dt, prec=32):
+    """advect! of the three face arrays through themselves (src/flip.jl:495-497)."""
+    return [advect(grid, a, axis, u, v, w, dt, prec) for axis, a in enumerate((u, v, w))]
+
+
+def advect_velocity_vjp(grid, gou, gov, gow, u, v, w, dt, prec=32):
+    """The adjoint of advect_velocity: the cotangent of the advected faces in, that of
+    (u, v, w) out (through both the sampled arrays and the traced positions)."""
+    t = _ft(prec)
+    u, v, w = (np.ascontiguousarray(a, dtype=t) for a in (u, v, w))
+    gs = [np.zeros(a.size, dtype=t) for a in (u, v, w)]
+    for axis, (go, src) in enumerate(zip((gou, gov, gow), (u, v, w))):
+        dims = _face_dims(grid, axis)
+        off = np.array((UOFF, VOFF, WOFF)[axis], dtype=t)
+        getattr(lib(), f"orc_advect_vjp_f{prec}")(ctypes.byref(_grid(grid)), _p(np.ascontiguousarray(go, dtype=t)),
+                                                  _p(src), _p(dims), _p(off), _p(u), _p(v), _p(w), dt,
+                                                  _p(gs[axis]), _p(gs[0]), _p(gs[1]), _p(gs[2]))
+    return gs
+
+
+def rollout(basin, u, v, w, steps, dt, *, tol=1e-13, maxiter=400, prec=64, volume0=None, recover=0.5):
+    """`steps` steps of advect! (velocity) + project! from (u, v, w) on the basin's types and
+    phi: returns the list of per-step start velocities (checkpoints) plus the final one."""
+    import dataclasses
+
+    g = basin.grid
+    vol0 = volume(g, basin.phi) if volume0 is None else volume0
+    states = [[np.array(a, dtype=_ft(prec)) for a in (u, v, w)]]
+    for _ in range(steps):
+        a = advect_velocity(g, *states[-1], dt, prec)
+        bb = dataclasses.replace(basin, u=a[0], v=a[1], w=a[2])
+        r = project(bb, volume0=vol0, dt=dt, recover=recover, tol=tol, maxiter=maxiter, prec=prec)
+        states.append([r["u"], r["v"], r["w"]])
+    return states
+
+
+def rollout_vjp(basin, states, gu, gv, gw, dt, *, tol=1e-13, maxiter=400, prec=64):
+    """The reverse pass of `rollout`: the final velocity's cotangent in, the initial one's
+    out (projection adjoint, then advection adjoint at each step's checkpoint)."""
+    g = basin.grid
+    grad = [np.array(a, dtype=_ft(prec)) for a in (gu, gv, gw)]
+    for n in reversed(range(len(states) - 1)):
+        r = project_vjp(basin, *grad, tol=tol, maxiter=maxiter, prec=prec)
+        grad = advect_velocity_vjp(g, r["gu"], r["gv"], r["gw"], *states[n], dt, prec)
+    return grad
 
 
 def num_threads() -> int:

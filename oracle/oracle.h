@@ -108,6 +108,20 @@ int orc_project_vjp_f32(const orc_grid* g, float* gu, float* gv, float* gw, floa
 int orc_project_vjp_f64(const orc_grid* g, double* gu, double* gv, double* gw, double* mu, const uint8_t* types,
                         const double* phi, double tol, int maxiter, int sweeps, int coarse, orc_info* info);
 
+/* Semi-Lagrangian advection of one array (dims a, sample offset off) through the face
+ * velocities (advect_kernel!, src/flip.jl:357-369) and its adjoint (accumulates into
+ * gsrc, gu, gv, gw). */
+void orc_advect_f32(const orc_grid* g, float* out, const float* src, const int32_t a[3], const float off[3],
+                    const float* u, const float* v, const float* w, float dt);
+void orc_advect_f64(const orc_grid* g, double* out, const double* src, const int32_t a[3], const double off[3],
+                    const double* u, const double* v, const double* w, double dt);
+void orc_advect_vjp_f32(const orc_grid* g, const float* gout, const float* src, const int32_t a[3],
+                        const float off[3], const float* u, const float* v, const float* w, float dt, float* gsrc,
+                        float* gu, float* gv, float* gw);
+void orc_advect_vjp_f64(const orc_grid* g, const double* gout, const double* src, const int32_t a[3],
+                        const double off[3], const double* u, const double* v, const double* w, double dt,
+                        double* gsrc, double* gu, double* gv, double* gw);
+
 int orc_num_threads(void);
 void orc_set_num_threads(int n);
 

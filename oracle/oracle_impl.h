@@ -607,4 +607,182 @@ int FN(orc_project_vjp_)(const orc_grid* g, R* gu, R* gv, R* gw, R* mu, const ui
     return its;
 }
 
+/* ---- semi-Lagrangian advection (advect_kernel!, src/flip.jl:357-369; trilinear,
+ * src/interpolation.jl:4-17; nodepos/indexspace/velocity, src/flip.jl:76-81) and its
+ * adjoint (not in the reference; the reverse of the same steps). ---- */
+
+/* trilinear(A, q) on an a1 x a2 x a3 array (0-based index space, clamped to the array).
+ * With wts != NULL it also returns the 8 corner indices and weights and the gradient in
+ * q (zero along an axis whose coordinate was clamped). */
+static R FN(tri_)(const R* A, int a1, int a2, int a3, R qx, R qy, R qz, size_t* idx, R* wts, R* grad) {
+    R x = qx > (R)(a1 - 1) ? (R)(a1 - 1) : (qx < (R)0 ? (R)0 : qx);
+    R y = qy > (R)(a2 - 1) ? (R)(a2 - 1) : (qy < (R)0 ? (R)0 : qy);
+    R z = qz > (R)(a3 - 1) ? (R)(a3 - 1) : (qz < (R)0 ? (R)0 : qz);
+    int i = (int)x, j = (int)y, k = (int)z;
+    if (i > a1 - 2) i = a1 - 2;
+    if (j > a2 - 2) j = a2 - 2;
+    if (k > a3 - 2) k = a3 - 2;
+    R fx = x - (R)i, fy = y - (R)j, fz = z - (R)k;
+    size_t b000 = ID(a1, a2, i, j, k), sx = 1, sy = (size_t)a1, sz = (size_t)a1 * a2;
+    R A000 = A[b000], A100 = A[b000 + sx], A010 = A[b000 + sy], A110 = A[b000 + sx + sy];
+    R A001 = A[b000 + sz], A101 = A[b000 + sx + sz], A011 = A[b000 + sy + sz], A111 = A[b000 + sx + sy + sz];
+    R c00 = A000 * ((R)1 - fx) + A100 * fx;
+    R c10 = A010 * ((R)1 - fx) + A110 * fx;
+    R c01 = A001 * ((R)1 - fx) + A101 * fx;
+    R c11 = A011 * ((R)1 - fx) + A111 * fx;
+    R val = (c00 * ((R)1 - fy) + c10 * fy) * ((R)1 - fz) + (c01 * ((R)1 - fy) + c11 * fy) * fz;
+    if (wts) {
+        R gx = (R)1 - fx, gy = (R)1 - fy, gz = (R)1 - fz;
+        idx[0] = b000; wts[0] = gx * gy * gz;
+        idx[1] = b000 + sx; wts[1] = fx * gy * gz;
+        idx[2] = b000 + sy; wts[2] = gx * fy * gz;
+        idx[3] = b000 + sx + sy; wts[3] = fx * fy * gz;
+        idx[4] = b000 + sz; wts[4] = gx * gy * fz;
+        idx[5] = b000 + sx + sz; wts[5] = fx * gy * fz;
+        idx[6] = b000 + sy + sz; wts[6] = gx * fy * fz;
+        idx[7] = b000 + sx + sy + sz; wts[7] = fx * fy * fz;
+        /* clamp passes the derivative on its closed range (as ChainRules' and torch's rules) */
+        int inx = qx >= (R)0 && qx <= (R)(a1 - 1), iny = qy >= (R)0 && qy <= (R)(a2 - 1);
+        int inz = qz >= (R)0 && qz <= (R)(a3 - 1);
+        R dx_ = ((A100 - A000) * gy + (A110 - A010) * fy) * gz + ((A101 - A001) * gy + (A111 - A011) * fy) * fz;
+        R dy_ = (c10 - c00) * gz + (c11 - c01) * fz;
+        R dz_ = (c01 * gy + c11 * fy) - (c00 * gy + c10 * fy);
+        grad[0] = inx ? dx_ : (R)0;
+        grad[1] = iny ? dy_ : (R)0;
+        grad[2] = inz ? dz_ : (R)0;
+    }
+    return val;
+}
+
+typedef struct {
+    const R* f[3];  /* u, v, w */
+    int d[3][3];    /* their dims */
+    R off[3][3];    /* UOFF, VOFF, WOFF */
+    R lo[3], dx;
+} FN(flow_);
+
+static void FN(flow_init_)(FN(flow_) * fl, const orc_grid* g, const R* u, const R* v, const R* w) {
+    const int n1 = g->n[0], n2 = g->n[1], n3 = g->n[2];
+    fl->f[0] = u; fl->f[1] = v; fl->f[2] = w;
+    for (int c = 0; c < 3; c++) {
+        fl->d[c][0] = n1 + (c == 0); fl->d[c][1] = n2 + (c == 1); fl->d[c][2] = n3 + (c == 2);
+        for (int a = 0; a < 3; a++) fl->off[c][a] = a == c ? (R)0 : (R)0.5f;
+        fl->lo[c] = (R)g->lo[c];
+    }
+    fl->dx = (R)g->dx;
+}
+
+/* velocity(u, v, w, g, p) (src/flip.jl:80-81); with the *_g outputs, each component's
+ * corner indices/weights and its gradient in p. */
+static void FN(velocity_)(const FN(flow_) * fl, const R p[3], R out[3], size_t (*idx)[8], R (*wts)[8], R (*gp)[3]) {
+    for (int c = 0; c < 3; c++) {
+        R q[3];
+        for (int a = 0; a < 3; a++) q[a] = (p[a] - fl->lo[a]) / fl->dx - fl->off[c][a];
+        R gq[3];
+        out[c] = FN(tri_)(fl->f[c], fl->d[c][0], fl->d[c][1], fl->d[c][2], q[0], q[1], q[2], idx ? idx[c] : NULL,
+                          wts ? wts[c] : NULL, gq);
+        if (gp)
+            for (int a = 0; a < 3; a++) gp[c][a] = gq[a] / fl->dx;
+    }
+}
+
+/* substeps (src/flip.jl:372): clamp(trunc(ceil(cells)), 1, 32). */
+static int FN(substeps_)(R cells) {
+    R c = (R)ceil((double)cells);
+    if (!(c >= (R)1)) return 1;
+    if (c > (R)32) return 32;
+    return (int)c;
+}
+
+/* advect_kernel! for one array `src` (dims a[3], sample offset off[3]): out = src traced
+ * back through the flow in RK2 sub-steps. */
+void FN(orc_advect_)(const orc_grid* g, R* out, const R* src, const int32_t a[3], const R off[3], const R* u,
+                     const R* v, const R* w, R dt) {
+    FN(flow_) fl;
+    FN(flow_init_)(&fl, g, u, v, w);
+    const int a1 = a[0], a2 = a[1], a3 = a[2];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < a3; k++)
+        for (int j = 0; j < a2; j++)
+            for (int i = 0; i < a1; i++) {
+                R p[3] = {fl.lo[0] + ((R)i + off[0]) * fl.dx, fl.lo[1] + ((R)j + off[1]) * fl.dx,
+                          fl.lo[2] + ((R)k + off[2]) * fl.dx};
+                R vel[3];
+                FN(velocity_)(&fl, p, vel, NULL, NULL, NULL);
+                int m = FN(substeps_)((R)sqrt((double)(vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2])) * dt / fl.dx);
+                R h = dt / (R)m;
+                for (int s = 0; s < m; s++) {
+                    R v1[3], pm[3], v2[3];
+                    FN(velocity_)(&fl, p, v1, NULL, NULL, NULL);
+                    R hh = (R)0.5f * h;
+                    for (int c = 0; c < 3; c++) pm[c] = p[c] - hh * v1[c];
+                    FN(velocity_)(&fl, pm, v2, NULL, NULL, NULL);
+                    for (int c = 0; c < 3; c++) p[c] = p[c] - h * v2[c];
+                }
+                R q[3];
+                for (int c = 0; c < 3; c++) q[c] = (p[c] - fl.lo[c]) / fl.dx - off[c];
+                out[ID(a1, a2, i, j, k)] = FN(tri_)(src, a1, a2, a3, q[0], q[1], q[2], NULL, NULL, NULL);
+            }
+}
+
+/* The adjoint of orc_advect_: for the cotangent gout of `out`, adds d/d src into gsrc and
+ * d/d (u, v, w) through the traced positions into gu, gv, gw (sequential, so the sums are
+ * in a fixed order). The sub-step count is piecewise constant: no derivative. */
+void FN(orc_advect_vjp_)(const orc_grid* g, const R* gout, const R* src, const int32_t a[3], const R off[3],
+                         const R* u, const R* v, const R* w, R dt, R* gsrc, R* gu, R* gv, R* gw) {
+    FN(flow_) fl;
+    FN(flow_init_)(&fl, g, u, v, w);
+    R* gf[3] = {gu, gv, gw};
+    const int a1 = a[0], a2 = a[1], a3 = a[2];
+    R ps[33][3], pms[32][3];
+    for (int k = 0; k < a3; k++)
+        for (int j = 0; j < a2; j++)
+            for (int i = 0; i < a1; i++) {
+                const R go = gout[ID(a1, a2, i, j, k)];
+                R p[3] = {fl.lo[0] + ((R)i + off[0]) * fl.dx, fl.lo[1] + ((R)j + off[1]) * fl.dx,
+                          fl.lo[2] + ((R)k + off[2]) * fl.dx};
+                R vel[3];
+                FN(velocity_)(&fl, p, vel, NULL, NULL, NULL);
+                int m = FN(substeps_)((R)sqrt((double)(vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2])) * dt / fl.dx);
+                R h = dt / (R)m, hh = (R)0.5f * h;
+                for (int c = 0; c < 3; c++) ps[0][c] = p[c];
+                for (int s = 0; s < m; s++) {
+                    R v1[3], v2[3];
+                    FN(velocity_)(&fl, ps[s], v1, NULL, NULL, NULL);
+                    for (int c = 0; c < 3; c++) pms[s][c] = ps[s][c] - hh * v1[c];
+                    FN(velocity_)(&fl, pms[s], v2, NULL, NULL, NULL);
+                    for (int c = 0; c < 3; c++) ps[s + 1][c] = ps[s][c] - h * v2[c];
+                }
+                /* out = tri(src, q(p_m)) */
+                R q[3], gq[3], wt[8], pb[3];
+                size_t ix[8];
+                for (int c = 0; c < 3; c++) q[c] = (ps[m][c] - fl.lo[c]) / fl.dx - off[c];
+                FN(tri_)(src, a1, a2, a3, q[0], q[1], q[2], ix, wt, gq);
+                for (int t = 0; t < 8; t++) gsrc[ix[t]] += go * wt[t];
+                for (int c = 0; c < 3; c++) pb[c] = go * gq[c] / fl.dx;
+                for (int s = m - 1; s >= 0; s--) {
+                    /* p_{s+1} = p_s - h V(pm_s), pm_s = p_s - hh V(p_s) */
+                    R vv[3], gp[3][3], wv[3][8];
+                    size_t iv[3][8];
+                    R vb[3], pmb[3];
+                    for (int c = 0; c < 3; c++) vb[c] = -h * pb[c];
+                    FN(velocity_)(&fl, pms[s], vv, iv, wv, gp);
+                    for (int c = 0; c < 3; c++) pmb[c] = (R)0;
+                    for (int c = 0; c < 3; c++) {
+                        for (int t = 0; t < 8; t++) gf[c][iv[c][t]] += vb[c] * wv[c][t];
+                        for (int e = 0; e < 3; e++) pmb[e] += vb[c] * gp[c][e];
+                    }
+                    for (int c = 0; c < 3; c++) {
+                        pb[c] += pmb[c];
+                        vb[c] = -hh * pmb[c];
+                    }
+                    FN(velocity_)(&fl, ps[s], vv, iv, wv, gp);
+                    for (int c = 0; c < 3; c++) {
+                        for (int t = 0; t < 8; t++) gf[c][iv[c][t]] += vb[c] * wv[c][t];
+                        for (int e = 0; e < 3; e++) pb[e] += vb[c] * gp[c][e];
+                    }
+                }
+            }
+}
+
 #undef FN
