@@ -171,6 +171,55 @@ int mpp_advect_phi(mpp_ctx* ctx, float* ophi, const float* phi, const float* u, 
 int mpp_advect_vjp(mpp_ctx* ctx, const float* gou, const float* gov, const float* gow, const float* u,
                    const float* v, const float* w, float dt, float* du, float* dv, float* dw, mpp_stream stream);
 
+/* ---- batches: many independent basins in one graph launch ----
+ * Each basin keeps its own context (created from grids[i] and opts[i], or the defaults
+ * when opts is NULL). mpp_batch_project records every basin's project! (the same
+ * sequence as mpp_project, each with its device-side convergence loop) into one CUDA
+ * graph, cached by the basins' arrays, and launches it once: the basins' chains run
+ * concurrently on the GPU. A basin with the FGMRES fallback on finishes on the host after
+ * the launch. No reference counterpart (the reference steps basins one at a time). */
+typedef struct mpp_batch mpp_batch;
+typedef struct {
+    float *u, *v, *w;          /* faces, updated */
+    uint8_t *fu, *fv, *fw;     /* valid-face flags, written */
+    float* P;                  /* warm start in, pressure out */
+    const uint8_t* types;
+    const float* phi;
+    float volume0;
+} mpp_basin_arrays;
+int mpp_batch_create(mpp_batch** batch, int count, const mpp_grid* grids, const mpp_opts* opts);
+int mpp_batch_destroy(mpp_batch* batch);
+int mpp_batch_size(const mpp_batch* batch);
+/* Basin i's context (options, smoother, autotuning); using it drops the batch's graph. */
+mpp_ctx* mpp_batch_ctx(mpp_batch* batch, int i);
+/* project! of every basin with one graph launch; results[i] (may be NULL) per basin.
+ * Returns the largest solver status of the batch, or an error. */
+int mpp_batch_project(mpp_batch* batch, const mpp_basin_arrays* basins, double dt, double recover,
+                      mpp_result* results, mpp_stream stream);
+
+/* ---- smoother forms and the autotuner ---- */
+enum {
+    MPP_SMOOTHER_VECTOR = 0, /* warp per 64x4x2 tile, 8 same-colour cells per lane, 16-byte loads */
+    MPP_SMOOTHER_TMA = 1,    /* TMA-staged tiles (cp.async.bulk.tensor), persistent pipeline */
+    MPP_SMOOTHER_COLUMN = 2, /* thread per tile column, scalar loads */
+};
+int mpp_ctx_set_smoother(mpp_ctx* ctx, int form);
+int mpp_ctx_smoother(const mpp_ctx* ctx);
+typedef struct {
+    int32_t smoother;   /* MPP_SMOOTHER_* */
+    int32_t sweeps;     /* smoother sweeps per level and direction */
+    int32_t iterations; /* CG iterations to tol */
+    int32_t status;     /* solver status */
+    float ms;           /* time of the solve (CUDA events, graph launch) */
+} mpp_tune_entry;
+/* Time the basin's own pressure solve (rhs from u, v, w; zero start; the context's tol and
+ * precision) for every smoother form x sweeps in 1..3, keep the fastest that converges on
+ * the context, and return the number of candidates tried (table[0..capacity) gets them,
+ * *chosen the winner's index, -1 when none converged). Allocates two trial arrays for
+ * the call. */
+int mpp_autotune(mpp_ctx* ctx, const float* u, const float* v, const float* w, const uint8_t* types,
+                 const float* phi, mpp_tune_entry* table, int capacity, int* chosen, mpp_stream stream);
+
 /* diag_kernel! (src/flip.jl:824-836). */
 int mpp_diag(mpp_ctx* ctx, float* diag, const uint8_t* types, const float* phi, mpp_stream stream);
 /* vcycle!(s, z, r) (src/flip.jl:992-1014): z = M^-1 r for this types/phi. */

@@ -554,21 +554,6 @@ int read_state(mpp_ctx* c, cudaStream_t s) {
     return MPP_OK;
 }
 
-// Leaf nodes of a graph (nodes nothing depends on).
-int graph_leaves(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves) {
-    size_t n = 0;
-    CK(cudaGraphGetNodes(g, nullptr, &n));
-    std::vector<cudaGraphNode_t> nodes(n);
-    CK(cudaGraphGetNodes(g, nodes.data(), &n));
-    leaves.clear();
-    for (auto nd : nodes) {
-        size_t m = 0;
-        CK(cudaGraphNodeGetDependentNodes(nd, nullptr, &m));
-        if (m == 0) leaves.push_back(nd);
-    }
-    return MPP_OK;
-}
-
 struct Call {
     // project (kind 1) or pressure (kind 0)
     int kind;
@@ -811,43 +796,66 @@ int fallback_and_finish(mpp_ctx* c, const Call& k, cudaStream_t s) {
     return MPP_OK;
 }
 
+// Record one solve (prologue, the CG loop as a conditional WHILE node, epilogue) into
+// graph g as a chain of its own: its first nodes have no dependencies, so the chains of
+// several basins recorded into one graph run concurrently. counts = kernels per part.
 template <class Pr>
-int build_graph(mpp_ctx* c, const Call& k, GraphEntry& ge) {
+int record_solve(mpp_ctx* c, const Call& k, cudaGraph_t g, int counts[3]) {
     using V = typename Pr::V;
     cudaStream_t s = c->cap;
-    drop_graph(ge);
-    cudaGraph_t g;
-    CK(cudaGraphCreate(&g, 0));
-    ge.graph = g;
     cudaGraphConditionalHandle cond;
     CK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
     Run<Pr> pro{c, s};
     CK(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     record_prologue<Pr>(pro, k, cond, 1);
-    CK(cudaStreamEndCapture(s, &g));
-    std::vector<cudaGraphNode_t> leaves;
-    if (int e = graph_leaves(g, leaves)) return e;
+    // the prologue's last nodes: the capture's current dependencies
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaStreamCaptureStatus cst;
+    const cudaError_t qe = cudaStreamGetCaptureInfo(s, &cst, nullptr, nullptr, &deps, &nd);
+    std::vector<cudaGraphNode_t> tail;
+    if (qe == cudaSuccess) tail.assign(deps, deps + nd);
+    cudaGraph_t gg = g;
+    CK(cudaStreamEndCapture(s, &gg));
+    CK(qe);
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = cond;
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
     cudaGraphNode_t cnode;
-    CK(cudaGraphAddNode(&cnode, g, leaves.data(), leaves.size(), &cp));
+    CK(cudaGraphAddNode(&cnode, g, tail.data(), tail.size(), &cp));
     cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
     Run<Pr> bod{c, s};
     CK(cudaStreamBeginCaptureToGraph(s, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     V* P = std::is_same<V, double>::value ? (V*)c->Pd : (V*)k.P;
     bod.body(P, cond, 1);
+    const cudaError_t le = cudaGetLastError();  // a launch refused during the capture
     CK(cudaStreamEndCapture(s, &bodyg));
+    CK(le);
     Run<Pr> epi{c, s};
     CK(cudaStreamBeginCaptureToGraph(s, g, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
     record_epilogue<Pr>(epi, k);
-    CK(cudaStreamEndCapture(s, &g));
+    gg = g;
+    CK(cudaStreamEndCapture(s, &gg));
+    counts[0] = pro.nk;
+    counts[1] = bod.nk;
+    counts[2] = epi.nk;
+    return MPP_OK;
+}
+
+template <class Pr>
+int build_graph(mpp_ctx* c, const Call& k, GraphEntry& ge) {
+    drop_graph(ge);
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    ge.graph = g;
+    int counts[3];
+    if (int e = record_solve<Pr>(c, k, g, counts)) return e;
     CK(cudaGraphInstantiate(&ge.exec, g, 0));
-    ge.g_prologue = pro.nk;
-    ge.g_body = bod.nk;
-    ge.g_epilogue = epi.nk;
+    ge.g_prologue = counts[0];
+    ge.g_body = counts[1];
+    ge.g_epilogue = counts[2];
     const void* key[11] = {k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.bnat, k.types, k.phi, k.bnat64};
     memcpy(ge.key, key, sizeof(key));
     ge.kind = k.kind;
@@ -1262,9 +1270,18 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
         }
         c->bot_smem = o;
         c->restrict_smem = (size_t)RX * RY * RZ * cs;
+        int optin = 0;
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
+        if (c->bot_smem > (size_t)optin) {
+            set_err("the bottom levels need %zu bytes of shared memory; the device allows %d", c->bot_smem, optin);
+            return fail(MPP_ERR_INVALID);
+        }
         const int ea = dispatch(c->prec, [&](auto pr) -> int {
             using Pr = decltype(pr);
-            CK(cudaFuncSetAttribute(k_bottom<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->bot_smem));
+            // The limit is the function's, shared by every context of the process: raise it
+            // to the device's maximum once rather than to this basin's need, which would
+            // lower it under a larger basin created earlier.
+            CK(cudaFuncSetAttribute(k_bottom<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
             CK(cudaFuncSetAttribute(k_restrict<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)c->restrict_smem));
             return MPP_OK;
@@ -1420,6 +1437,241 @@ int mpp_project_vjp(mpp_ctx* c, const float* gu, const float* gv, const float* g
     CK(cudaStreamSynchronize(s));
     fill_result(c, res, c->launches - before);
     return c->sc_host->s.status;
+}
+
+// ---- batches: many basins, one graph launch ----
+// Each basin keeps its own context (workspace, levels, partial sums); the batch records
+// every basin's solve chain into ONE graph, so a projection of all of them is one graph
+// launch whose chains the GPU runs concurrently, each with its own device-side
+// convergence loop. The graph is cached by the basins' arrays.
+struct mpp_batch {
+    std::vector<mpp_ctx*> ctx;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void*> key;
+    std::vector<int> counts;  // per basin: prologue, body, epilogue kernels
+    int dev = -1;
+};
+
+static void batch_drop_graph(mpp_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->key.clear();
+}
+
+int mpp_batch_create(mpp_batch** out, int count, const mpp_grid* grids, const mpp_opts* opts) {
+    if (!out || count <= 0 || !grids) {
+        set_err("null output, grids or an empty batch");
+        return MPP_ERR_INVALID;
+    }
+    *out = nullptr;
+    mpp_batch* b = new mpp_batch();
+    CK(cudaGetDevice(&b->dev));
+    for (int i = 0; i < count; i++) {
+        mpp_opts o;
+        if (opts) o = opts[i];
+        else mpp_opts_default(&o);
+        mpp_ctx* c = nullptr;
+        if (int e = mpp_ctx_create(&c, &grids[i], &o)) {
+            for (mpp_ctx* x : b->ctx) mpp_ctx_destroy(x);
+            delete b;
+            return e;
+        }
+        b->ctx.push_back(c);
+    }
+    *out = b;
+    return MPP_OK;
+}
+
+int mpp_batch_destroy(mpp_batch* b) {
+    if (!b) return MPP_OK;
+    batch_drop_graph(b);
+    for (mpp_ctx* c : b->ctx) mpp_ctx_destroy(c);
+    delete b;
+    return MPP_OK;
+}
+
+int mpp_batch_size(const mpp_batch* b) { return b ? (int)b->ctx.size() : 0; }
+
+mpp_ctx* mpp_batch_ctx(mpp_batch* b, int i) {
+    if (!b || i < 0 || i >= (int)b->ctx.size()) return nullptr;
+    batch_drop_graph(b);  // the caller may change the basin's options
+    return b->ctx[i];
+}
+
+int mpp_batch_project(mpp_batch* b, const mpp_basin_arrays* basins, double dt, double recover, mpp_result* results,
+                      mpp_stream stream) {
+    if (!b || !basins) {
+        set_err("null batch or arrays");
+        return MPP_ERR_INVALID;
+    }
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev != b->dev) {
+        set_err("batch belongs to device %d, current device is %d", b->dev, dev);
+        return MPP_ERR_INVALID;
+    }
+    if (!(dt > 0.0) || !(recover > 0.0)) {
+        set_err("dt and recover must be positive");
+        return MPP_ERR_INVALID;
+    }
+    const int n = (int)b->ctx.size();
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<const void*> key;
+    for (int i = 0; i < n; i++) {
+        const mpp_basin_arrays& a = basins[i];
+        if (!a.u || !a.v || !a.w || !a.fu || !a.fv || !a.fw || !a.P || !a.types || !a.phi || !(a.volume0 != 0.f)) {
+            set_err("basin %d: null array or zero volume0", i);
+            return MPP_ERR_INVALID;
+        }
+        const void* k[9] = {a.u, a.v, a.w, a.fu, a.fv, a.fw, a.P, a.types, a.phi};
+        key.insert(key.end(), k, k + 9);
+    }
+    std::vector<int64_t> launches0(n);
+    for (int i = 0; i < n; i++) {
+        mpp_ctx* c = b->ctx[i];
+        launches0[i] = c->launches;
+        CK(cudaMemsetAsync(&c->sc->s.fault, 0, sizeof(int), s));
+        if (int e = write_params(c, basins[i].volume0, dt, recover, 1, 0.f, s)) return e;
+    }
+    if (!b->exec || key != b->key) {
+        batch_drop_graph(b);
+        CK(cudaGraphCreate(&b->graph, 0));
+        b->counts.assign(3 * n, 0);
+        for (int i = 0; i < n; i++) {
+            const mpp_basin_arrays& a = basins[i];
+            Call k{1, a.u, a.v, a.w, a.fu, a.fv, a.fw, a.P, nullptr, a.types, a.phi};
+            mpp_ctx* c = b->ctx[i];
+            int e = dispatch(c->prec, [&](auto pr) { return record_solve<decltype(pr)>(c, k, b->graph, &b->counts[3 * i]); });
+            if (e) {
+                batch_drop_graph(b);
+                return e;
+            }
+        }
+        CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+        b->key = key;
+    }
+    CK(cudaGraphLaunch(b->exec, s));
+    for (int i = 0; i < n; i++)
+        CK(cudaMemcpyAsync(&b->ctx[i]->sc_host->s, &b->ctx[i]->sc->s, sizeof(State), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    int worst = MPP_OK;
+    for (int i = 0; i < n; i++) {
+        mpp_ctx* c = b->ctx[i];
+        const int* k3 = &b->counts[3 * i];
+        c->launches += k3[0] + (int64_t)k3[1] * c->sc_host->s.it + k3[2];
+        if (c->sc_host->s.fault) {
+            set_err("basin %d: a bounded device wait (TMA pipeline) gave up; results are not valid", i);
+            return MPP_ERR_CUDA;
+        }
+        c->fg_used = c->fg_its = 0;
+        if (c->opts.fallback) {
+            const mpp_basin_arrays& a = basins[i];
+            Call k{1, a.u, a.v, a.w, a.fu, a.fv, a.fw, a.P, nullptr, a.types, a.phi};
+            int e = dispatch(c->prec, [&](auto pr) { return fallback_and_finish<decltype(pr)>(c, k, s); });
+            if (e) return e;
+        }
+        if (results) fill_result(c, &results[i], c->launches - launches0[i]);
+        const int st = c->sc_host->s.status;
+        if (st > worst) worst = st;
+    }
+    return worst;
+}
+
+// ---- the autotuner: smoother form x sweeps, timed on the basin's own solve ----
+int mpp_ctx_set_smoother(mpp_ctx* c, int form) {
+    if (int e = check_ctx(c)) return e;
+    if (form < MPP_SMOOTHER_VECTOR || form > MPP_SMOOTHER_COLUMN) {
+        set_err("unknown smoother form %d", form);
+        return MPP_ERR_INVALID;
+    }
+    c->rbgs_mode = form == MPP_SMOOTHER_VECTOR ? RBGS_V8 : (form == MPP_SMOOTHER_TMA ? RBGS_TMA : RBGS_COLUMN);
+    c->vec_on = c->rbgs_mode != RBGS_COLUMN;
+    drop_graphs(c);
+    return MPP_OK;
+}
+
+int mpp_ctx_smoother(const mpp_ctx* c) {
+    if (!c) return MPP_ERR_INVALID;
+    return c->rbgs_mode == RBGS_V8 ? MPP_SMOOTHER_VECTOR : (c->rbgs_mode == RBGS_TMA ? MPP_SMOOTHER_TMA : MPP_SMOOTHER_COLUMN);
+}
+
+int mpp_autotune(mpp_ctx* c, const float* u, const float* v, const float* w, const uint8_t* types, const float* phi,
+                 mpp_tune_entry* table, int capacity, int* chosen, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!u || !v || !w || !types || !phi) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+    const mpp_opts saved = c->opts;
+    const int saved_form = mpp_ctx_smoother(c);
+    bool any_tma = false;
+    for (int l = 0; l < c->lb; l++) any_tma = any_tma || c->tma_ok[l];
+    float *b = nullptr, *P = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::vector<mpp_tune_entry> tried;
+    int err = MPP_OK;
+    // trial buffers live only for the call
+    auto run = [&]() -> int {
+        CK(cudaMalloc(&b, sizeof(float) * (size_t)N));
+        CK(cudaMalloc(&P, sizeof(float) * (size_t)N));
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        if (int e = mpp_rhs(c, b, u, v, w, types, 0.f, stream)) return e;
+        for (int form = MPP_SMOOTHER_VECTOR; form <= MPP_SMOOTHER_COLUMN; form++) {
+            if (form == MPP_SMOOTHER_TMA && !any_tma) continue;
+            for (int sw = 1; sw <= 3; sw++) {
+                mpp_opts o = saved;
+                o.sweeps = sw;
+                o.graph = 1;
+                o.fallback = 0;
+                if (int e = mpp_ctx_set_opts(c, &o)) return e;
+                if (int e = mpp_ctx_set_smoother(c, form)) return e;
+                mpp_tune_entry t{form, sw, 0, MPP_OK, 0.f};
+                for (int rep = 0; rep < 3; rep++) {  // the first run captures the graph
+                    CK(cudaMemsetAsync(P, 0, sizeof(float) * (size_t)N, s));
+                    CK(cudaEventRecord(e0, s));
+                    mpp_result r;
+                    const int st = mpp_pressure(c, P, b, types, phi, &r, stream);
+                    if (st < 0) return st;
+                    CK(cudaEventRecord(e1, s));
+                    CK(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, e0, e1));
+                    if (rep > 0) t.ms += 0.5f * ms;
+                    t.iterations = r.iterations;
+                    t.status = st;
+                }
+                tried.push_back(t);
+            }
+        }
+        return MPP_OK;
+    };
+    err = run();
+    if (b) cudaFree(b);
+    if (P) cudaFree(P);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    int best = -1;
+    for (int i = 0; i < (int)tried.size(); i++)
+        if (tried[i].status == MPP_OK && (best < 0 || tried[i].ms < tried[best].ms)) best = i;
+    // apply the winner, or put the previous settings back
+    mpp_opts o = saved;
+    int form = saved_form;
+    if (err == MPP_OK && best >= 0) {
+        o.sweeps = tried[best].sweeps;
+        form = tried[best].smoother;
+    }
+    if (int e = mpp_ctx_set_opts(c, &o)) return e;
+    if (int e = mpp_ctx_set_smoother(c, form)) return e;
+    if (err) return err;
+    for (int i = 0; i < (int)tried.size() && i < capacity && table; i++) table[i] = tried[i];
+    if (chosen) *chosen = best;
+    return (int)tried.size();
 }
 
 // ---- semi-Lagrangian advection and its adjoint ----

@@ -46,6 +46,19 @@ class ProfEntry(ctypes.Structure):
                 ("cells", ctypes.c_int64)]
 
 
+class BasinArrays(ctypes.Structure):
+    _fields_ = [("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("w", ctypes.c_void_p), ("fu", ctypes.c_void_p),
+                ("fv", ctypes.c_void_p), ("fw", ctypes.c_void_p), ("P", ctypes.c_void_p), ("types", ctypes.c_void_p),
+                ("phi", ctypes.c_void_p), ("volume0", ctypes.c_float)]
+
+
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("smoother", ctypes.c_int32), ("sweeps", ctypes.c_int32), ("iterations", ctypes.c_int32),
+                ("status", ctypes.c_int32), ("ms", ctypes.c_float)]
+
+
+SMOOTHERS = {0: "vector", 1: "tma", 2: "column"}
+
 # name -> (restype, argtypes); every symbol include/mpp.h declares.
 P, I32, F32, F64, SZ = ctypes.c_void_p, ctypes.c_int32, ctypes.c_float, ctypes.c_double, ctypes.c_size_t
 _G, _O, _R = ctypes.POINTER(Grid), ctypes.POINTER(Opts), ctypes.POINTER(Result)
@@ -63,6 +76,15 @@ SIGNATURES = {
     "mpp_project_vjp": (ctypes.c_int, [P, P, P, P, P, P, P, P, P, P, _R, P]),
     "mpp_vjp_rhs": (ctypes.c_int, [P, P, P, P, P, P, P, P]),
     "mpp_advect": (ctypes.c_int, [P, P, P, P, P, P, P, F32, P]),
+    "mpp_batch_create": (ctypes.c_int, [ctypes.POINTER(P), ctypes.c_int, _G, _O]),
+    "mpp_batch_destroy": (ctypes.c_int, [P]),
+    "mpp_batch_size": (ctypes.c_int, [P]),
+    "mpp_batch_ctx": (P, [P, ctypes.c_int]),
+    "mpp_batch_project": (ctypes.c_int, [P, ctypes.POINTER(BasinArrays), F64, F64, _R, P]),
+    "mpp_ctx_set_smoother": (ctypes.c_int, [P, ctypes.c_int]),
+    "mpp_ctx_smoother": (ctypes.c_int, [P]),
+    "mpp_autotune": (ctypes.c_int, [P, P, P, P, P, P, ctypes.POINTER(TuneEntry), ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_int), P]),
     "mpp_advect_phi": (ctypes.c_int, [P, P, P, P, P, P, F32, P]),
     "mpp_advect_vjp": (ctypes.c_int, [P, P, P, P, P, P, P, F32, P, P, P, P]),
     "mpp_vjp_faces": (ctypes.c_int, [P, P, P, P, P, P, P, P, P, P]),

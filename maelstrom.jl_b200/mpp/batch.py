@@ -1,0 +1,157 @@
+"""Many independent basins: one graph launch per batched projection, the autotuner, and
+the partition of a batch over GPUs.
+
+:class:`Batch` owns an ``mpp_batch`` (one solver context per basin) and each basin's
+arrays on the device; :meth:`Batch.project` is ``project!`` of every basin as one CUDA
+graph launch. :meth:`Batch.autotune` times each distinct basin size's own solve over the
+smoother forms and sweep counts (``mpp_autotune``) and applies the winner to every basin
+of that size. :func:`lpt_partition` splits a batch over ranks (longest processing time
+first on cells x expected iterations): basins are independent, so ranks exchange
+nothing during the solves.
+"""
+from __future__ import annotations
+
+import ctypes
+import heapq
+
+import numpy as np
+
+from . import _lib, grid_struct, scene
+from ._lib import check
+
+
+def lpt_partition(costs, nranks: int) -> list:
+    """Greedy LPT: basins in decreasing cost, each to the least loaded rank. Returns one
+    list of basin indices per rank (each list in increasing index order)."""
+    heap = [(0.0, r) for r in range(nranks)]
+    parts = [[] for _ in range(nranks)]
+    for i in sorted(range(len(costs)), key=lambda i: (-costs[i], i)):
+        load, r = heapq.heappop(heap)
+        parts[r].append(i)
+        heapq.heappush(heap, (load + float(costs[i]), r))
+    return [sorted(p) for p in parts]
+
+
+def basin_cost(b: "scene.Basin") -> float:
+    """Expected solve cost: liquid cells x (levels + 4), a proxy for the iterations of a
+    multigrid-preconditioned solve of that size."""
+    liquid = float(np.count_nonzero(b.types == scene.LIQUID))
+    return liquid * (b.grid.levels + 4)
+
+
+class Batch:
+    def __init__(self, basins: list, device="cuda", *, tol=1e-6, maxiter=100, sweeps=2, coarse=40, precision="fp32",
+                 fallback=False):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("libmpp needs a CUDA device")
+        self.lib = _lib.load()
+        self.basins = basins
+        dev = torch.device(device)
+        n = len(basins)
+        grids = (_lib.Grid * n)(*(grid_struct(b.grid) for b in basins))
+        opts = (_lib.Opts * n)()
+        for o in opts:
+            self.lib.mpp_opts_default(ctypes.byref(o))
+            o.tol, o.maxiter, o.sweeps, o.coarse = tol, maxiter, sweeps, coarse
+            o.precision, o.graph, o.fallback = _lib.PREC[precision], 1, int(fallback)
+        self._opts = dict(tol=tol, maxiter=maxiter, coarse=coarse, precision=_lib.PREC[precision],
+                          fallback=int(fallback))
+        self._b = ctypes.c_void_p()
+        check(self.lib.mpp_batch_create(ctypes.byref(self._b), n, grids, opts))
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        self.arrays = []
+        for b in basins:
+            self.arrays.append(dict(u=t(b.u), v=t(b.v), w=t(b.w), fu=torch.zeros(b.u.size, dtype=torch.uint8, device=dev),
+                                    fv=torch.zeros(b.v.size, dtype=torch.uint8, device=dev),
+                                    fw=torch.zeros(b.w.size, dtype=torch.uint8, device=dev),
+                                    P=torch.zeros(b.grid.ncells, dtype=torch.float32, device=dev), types=t(b.types),
+                                    phi=t(b.phi)))
+        self.volume0 = []
+        for i, a in enumerate(self.arrays):
+            vol = ctypes.c_double()
+            check(self.lib.mpp_volume(self.ctx(i), ctypes.c_void_p(a["phi"].data_ptr()), ctypes.byref(vol),
+                                      ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+            self.volume0.append(vol.value)
+        self._structs = None
+        self.iterations = []
+
+    def ctx(self, i: int) -> ctypes.c_void_p:
+        return ctypes.c_void_p(self.lib.mpp_batch_ctx(self._b, i))
+
+    def close(self):
+        if getattr(self, "_b", None) and self._b.value:
+            self.lib.mpp_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _arrays(self):
+        n = len(self.arrays)
+        arr = (_lib.BasinArrays * n)()
+        for i, a in enumerate(self.arrays):
+            arr[i] = _lib.BasinArrays(*(ctypes.c_void_p(a[k].data_ptr()) for k in
+                                        ("u", "v", "w", "fu", "fv", "fw", "P", "types", "phi")),
+                                      float(self.volume0[i]))
+        return arr
+
+    def project(self, dt, recover=0.5, stream=None) -> list:
+        """``project!`` of every basin in one graph launch; returns the per-basin results."""
+        import torch
+
+        if self._structs is None:
+            self._structs = self._arrays()
+        n = len(self.arrays)
+        res = (_lib.Result * n)()
+        s = stream if stream is not None else torch.cuda.current_stream()
+        check(self.lib.mpp_batch_project(self._b, self._structs, float(dt), float(recover), res,
+                                         ctypes.c_void_p(s.cuda_stream)))
+        out = [r for r in res]
+        self.iterations.append([r.iterations + r.fallback_iterations for r in out])
+        return out
+
+    def autotune(self, stream=None) -> dict:
+        """Tune each distinct basin size on its first basin; apply the winner to every basin
+        of that size. Returns {dims: {"chosen": (smoother, sweeps), "table": [...]}}."""
+        import torch
+
+        s = stream if stream is not None else torch.cuda.current_stream()
+        groups = {}
+        for i, b in enumerate(self.basins):
+            groups.setdefault(tuple(b.grid.n), []).append(i)
+        report = {}
+        for dims, members in groups.items():
+            i0 = members[0]
+            a = self.arrays[i0]
+            table = (_lib.TuneEntry * 16)()
+            chosen = ctypes.c_int(-1)
+            ptr = lambda k: ctypes.c_void_p(a[k].data_ptr())
+            n = check(self.lib.mpp_autotune(self.ctx(i0), ptr("u"), ptr("v"), ptr("w"), ptr("types"), ptr("phi"),
+                                            table, 16, ctypes.byref(chosen), ctypes.c_void_p(s.cuda_stream)))
+            rows = [dict(smoother=_lib.SMOOTHERS[t.smoother], sweeps=t.sweeps, iterations=t.iterations,
+                         status=t.status, ms=t.ms) for t in table[:n]]
+            if chosen.value >= 0:
+                win = table[chosen.value]
+                for j in members[1:]:
+                    c = self.ctx(j)
+                    self._set_sweeps(c, win.sweeps)
+                    check(self.lib.mpp_ctx_set_smoother(c, win.smoother))
+                report[dims] = dict(chosen=(_lib.SMOOTHERS[win.smoother], win.sweeps), table=rows)
+            else:
+                report[dims] = dict(chosen=None, table=rows)
+        self._structs = None
+        return report
+
+    def _set_sweeps(self, c, sweeps):
+        # the batch's options are the ones it was created with; only the sweeps change
+        o = _lib.Opts()
+        self.lib.mpp_opts_default(ctypes.byref(o))
+        k = self._opts
+        o.tol, o.maxiter, o.sweeps, o.coarse = k["tol"], k["maxiter"], sweeps, k["coarse"]
+        o.precision, o.graph, o.fallback = k["precision"], 1, k["fallback"]
+        check(self.lib.mpp_ctx_set_opts(c, ctypes.byref(o)))

@@ -210,6 +210,24 @@ def box_basin(n, *, dx: float = 0.05, seed: int = 1001, wall: float = 0.45, heig
 
 
 # The workloads, by name: sizes and seeds as the benchmark configurations state them.
+BATCH_EDGES = (48, 64, 96, 128)
+
+
+def batch_basins(count: int = 48, seed: int = 1002) -> list:
+    """The batched workload: ``count`` independent cubic basins, edge drawn per basin from
+    {48, 64, 96, 128}, still-water height fraction uniform[0.3, 0.8], wall radius fraction
+    uniform[0.35, 0.48], faces uniform[-1, 1) m/s; everything from the one ``seed`` (basin
+    b's face seed is seed * 1000 + b)."""
+    out = []
+    for b in range(count):
+        r = uniform(seed, 900 + b, 3, 0.0, 1.0).astype(np.float64)  # three draws in [0, 1)
+        edge = BATCH_EDGES[min(int(r[0] * len(BATCH_EDGES)), len(BATCH_EDGES) - 1)]
+        height = 0.3 + 0.5 * float(r[1])
+        wall = 0.35 + 0.13 * float(r[2])
+        out.append(box_basin(edge, seed=seed * 1000 + b, wall=wall, height=height, name=f"batch{b}"))
+    return out
+
+
 def config_basin(name: str) -> Basin:
     """``plain64``: 64^3 (seed 1000); ``whirl256``: 256^3 plus a Rankine vortex
     (Gamma = 225 m^2/s, core 2.5 m; seed 1001); ``whirlpool384``: 384x384x256, surface
