@@ -333,6 +333,15 @@ def run_mpp(args):
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if rank == 0 and world == 1 and not args.no_extras:
+        # the other workloads, each timed on its own (not part of the headline value)
+        del proj
+        torch.cuda.empty_cache()
+        out["batched"] = bench_batched(max(3, min(args.steps, 10)))
+        torch.cuda.empty_cache()
+        out["adjoint"] = bench_adjoint(max(3, min(args.steps, 10)))
+        torch.cuda.empty_cache()
+        out["whirlpool384"] = bench_whirlpool(max(3, min(args.steps, 10)))
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(basin, max_seconds=args.cpu_seconds)
     if rank == 0:
@@ -344,6 +353,190 @@ def run_mpp(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def _events():
+    import torch
+
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def bench_batched(steps):
+    """48 basins (edges from {48, 64, 96, 128}), autotuned, one graph launch per batched
+    projection: total projections/s, cells/s and per-basin iterations."""
+    import torch
+
+    from mpp import scene
+    from mpp.batch import Batch
+
+    basins = scene.batch_basins()
+    cells = sum(b.grid.ncells for b in basins)
+    batch = Batch(basins, tol=TOL, maxiter=MAXITER, precision="fp32")
+    tune = batch.autotune()
+    init = [{k: a[k].clone() for k in ("u", "v", "w")} for a in batch.arrays]
+
+    def step():
+        for a, i0 in zip(batch.arrays, init):
+            for k in ("u", "v", "w"):
+                a[k].copy_(i0[k])
+            a["P"].zero_()
+        return batch.project(DT)
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    # the per-step copies of the 48 initial states are timed too (about 1.2 GB moved)
+    e0.record()
+    for _ in range(steps):
+        res = step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    launches = sum(r.kernel_launches for r in res)
+    return {"basins": len(basins), "cells": cells, "projections_per_s": round(len(basins) / (ms / 1e3), 2),
+            "cells_per_s": cells / (ms / 1e3), "ms_per_batch": round(ms, 3), "steps": steps,
+            "graph_launches_per_batch": 1, "gpu_launches_per_batch": launches,
+            "iterations": [r.iterations for r in res], "all_converged": all(r.status == 0 for r in res),
+            "max_true_rel_residual": max(r.true_rel_residual for r in res),
+            "autotune": {f"{d[0]}x{d[1]}x{d[2]}": v["chosen"] for d, v in tune.items()},
+            "edges": [b.grid.n[0] for b in basins], "precision": "fp32"}
+
+
+def bench_adjoint(steps):
+    """The adjoint at 128^3 (forward project! + its VJP, FP32 and mixed, error against the
+    FP64 form's gradient) and the 10-step 96^3 advect + project rollout's reverse pass."""
+    import numpy as np
+    import torch
+
+    import mpp
+    from mpp import scene
+    from mpp.rollout import Rollout
+
+    b = scene.box_basin(128, seed=1003)
+    rng = np.random.default_rng(1003)
+    ustar = [torch.from_numpy(rng.uniform(-1, 1, a.size).astype(np.float32)).cuda() for a in (b.u, b.v, b.w)]
+    out = {"workload": "128^3 basin (seed 1003), loss 1/2 |P(u) - u*|^2, u* uniform[-1, 1]"}
+    grads = {}
+    for prec in ("fp64", "fp32", "fp16"):
+        s = mpp.FlipBasin.from_scene(b, tol=1e-11 if prec == "fp64" else TOL, maxiter=300, precision=prec,
+                                     graph=True)
+        u0 = [a.clone() for a in (s.u, s.v, s.w)]
+        mu = torch.zeros(b.grid.ncells, dtype=torch.float32, device="cuda")
+
+        def fwd():
+            for a, x in zip((s.u, s.v, s.w), u0):
+                a.copy_(x)
+            s.P.zero_()
+            return s.projector.project(s.u, s.v, s.w, s.fu, s.fv, s.fw, s.P, s.types, s.phi, s.volume0, DT)
+
+        cot = [torch.empty_like(a) for a in u0]
+
+        def bwd():
+            for c, a, t in zip(cot, (s.u, s.v, s.w), ustar):
+                torch.sub(a, t, out=c)
+            mu.zero_()
+            return s.projector.project_vjp(*cot, mu, s.types, s.phi)
+
+        for _ in range(2):
+            fwd()
+            rb = bwd()
+        torch.cuda.synchronize()
+        n = 1 if prec == "fp64" else steps
+        e0, e1, e2 = _events() + (torch.cuda.Event(enable_timing=True),)
+        tf = tb = 0.0
+        for _ in range(n):
+            e0.record()
+            fwd()
+            e1.record()
+            rb = bwd()
+            e2.record()
+            torch.cuda.synchronize()
+            tf += e0.elapsed_time(e1)
+            tb += e1.elapsed_time(e2)
+        grads[prec] = np.concatenate([c.cpu().numpy().astype(np.float64) for c in cot])
+        if prec != "fp64":
+            ref = grads["fp64"]
+            out[prec] = {"forward_ms": round(tf / n, 3), "vjp_ms": round(tb / n, 3),
+                         "vjp_iterations": rb.iterations,
+                         "rel_error_vs_fp64_gradient": float(np.linalg.norm(grads[prec] - ref) / np.linalg.norm(ref))}
+        del s
+        torch.cuda.empty_cache()
+    # rollout
+    b96 = scene.box_basin(96, seed=1005)
+    u96 = [torch.from_numpy(scene.uniform(1005, 20 + a, int(np.prod(b96.grid.face_shape(a))))).cuda()
+           for a in range(3)]
+    star = [torch.from_numpy(rng.uniform(-1, 1, a.numel()).astype(np.float32)).cuda() for a in u96]
+    s = mpp.FlipBasin.from_scene(b96, tol=TOL, maxiter=MAXITER, precision="fp32", graph=True)
+    ro = Rollout(s, 10, 0.02)
+    for _ in range(2):
+        fin = ro.forward(*u96)
+        ro.backward(*[a - t for a, t in zip(fin, star)])
+    torch.cuda.synchronize()
+    e0, e1, e2 = _events() + (torch.cuda.Event(enable_timing=True),)
+    e0.record()
+    fin = ro.forward(*u96)
+    e1.record()
+    g = ro.backward(*[a - t for a, t in zip(fin, star)])
+    e2.record()
+    torch.cuda.synchronize()
+    out["rollout_96_10_steps"] = {"forward_ms": round(e0.elapsed_time(e1), 3), "backward_ms": round(e1.elapsed_time(e2), 3),
+                                  "iterations": ro.iterations, "adjoint_iterations": ro.adjoint_iterations,
+                                  "checkpoints_bytes": sum(c.numel() * 4 for ck in ro.ckpt for c in ck),
+                                  "grad_finite": bool(all(torch.isfinite(a).all() for a in g))}
+    return out
+
+
+def bench_whirlpool(steps):
+    """384 x 384 x 256 whirlpool, mixed precision with the FGMRES fallback to 1e-6: projections/s,
+    the FP64 form's pressure error, and achieved HBM GB/s per kernel family."""
+    import numpy as np
+    import torch
+
+    import mpp
+    from mpp import scene
+
+    b = scene.config_basin("whirlpool384")
+    s64 = mpp.FlipBasin.from_scene(b, tol=1e-11, maxiter=400, precision="fp64", graph=True)
+    mpp.project(s64, DT)
+    P64 = s64.projector.solution_f64()
+    del s64
+    torch.cuda.empty_cache()
+    s = mpp.FlipBasin.from_scene(b, tol=TOL, maxiter=MAXITER, precision="fp16", graph=True, fallback=True)
+    u0 = [a.clone() for a in (s.u, s.v, s.w)]
+
+    def step():
+        for a, x in zip((s.u, s.v, s.w), u0):
+            a.copy_(x)
+        s.P.zero_()
+        return s.projector.project(s.u, s.v, s.w, s.fu, s.fv, s.fw, s.P, s.types, s.phi, s.volume0, DT)
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(steps):
+        r = step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    err = float(np.linalg.norm(s.P.cpu().numpy() - P64) / np.linalg.norm(P64))
+    s.projector.profile(True)
+    step()
+    prof = s.projector.profile_read()
+    s.projector.profile(False)
+    fam = {}
+    for e in prof:
+        f = fam.setdefault(e["name"], [0.0, 0.0])
+        f[0] += e["bytes"]
+        f[1] += e["ms"]
+    per_kernel = {k: round(v[0] / (v[1] / 1e3) / 1e9, 1) for k, v in sorted(fam.items(), key=lambda kv: -kv[1][1])
+                  if v[1] > 0}
+    return {"cells": b.grid.ncells, "projections_per_s": round(1e3 / ms, 3), "ms_per_projection": round(ms, 3),
+            "iterations": r.iterations, "fallback_used": r.fallback_used, "status": r.status,
+            "true_rel_residual": r.true_rel_residual, "fp64_rel_error": err, "precision": "fp16",
+            "achieved_gbs_by_kernel": per_kernel, "steps": steps}
 
 
 def cpu_baseline(basin, max_seconds=30.0):
@@ -407,6 +600,7 @@ def main():
     ap.add_argument("--impl", default="mpp", choices=["mpp", "reference"])
     ap.add_argument("--precision", default="fp16", choices=["fp16", "bf16", "fp32"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched, adjoint and whirlpool workloads")
     ap.add_argument("--cpu-seconds", type=float, default=25.0)
     ap.add_argument("--reference-seconds", type=float, default=150.0)
     ap.add_argument("--profile-out", default=None)
