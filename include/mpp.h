@@ -203,17 +203,23 @@ enum {
     MPP_SMOOTHER_TMA = 1,    /* TMA-staged tiles (cp.async.bulk.tensor), persistent pipeline */
     MPP_SMOOTHER_COLUMN = 2, /* thread per tile column, scalar loads */
 };
-int mpp_ctx_set_smoother(mpp_ctx* ctx, int form);
-int mpp_ctx_smoother(const mpp_ctx* ctx);
+/* The smoother form of the fine level and of the coarser row-split levels (each level's
+ * other passes take the vector forms unless its smoother is the column form). */
+int mpp_ctx_set_smoothers(mpp_ctx* ctx, int fine, int coarse);
+int mpp_ctx_set_smoother(mpp_ctx* ctx, int form); /* both */
+int mpp_ctx_smoothers(const mpp_ctx* ctx, int* fine, int* coarse);
 typedef struct {
-    int32_t smoother;   /* MPP_SMOOTHER_* */
-    int32_t sweeps;     /* smoother sweeps per level and direction */
+    int32_t smoother;        /* MPP_SMOOTHER_* of the fine level */
+    int32_t coarse_smoother; /* MPP_SMOOTHER_* of the coarser row-split levels */
+    int32_t sweeps;          /* smoother sweeps per level and direction */
+    int32_t coarse_sweeps;   /* sweeps of the coarsest solve, each way */
     int32_t iterations; /* CG iterations to tol */
     int32_t status;     /* solver status */
     float ms;           /* time of the solve (CUDA events, graph launch) */
 } mpp_tune_entry;
 /* Time the basin's own pressure solve (rhs from u, v, w; zero start; the context's tol and
- * precision) for every smoother form x sweeps in 1..3, keep the fastest that converges on
+ * precision) for every fine x coarse smoother form x sweeps in 1..4 (and, in the 16-bit forms, 10
+ * instead of 40 coarsest sweeps), keep the fastest that converges on
  * the context, and return the number of candidates tried (table[0..capacity) gets them,
  * *chosen the winner's index, -1 when none converged). Allocates two trial arrays for
  * the call. */

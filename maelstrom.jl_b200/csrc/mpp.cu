@@ -46,8 +46,6 @@ constexpr int NCOUNTERS = 8;
 enum { CNT_VOLUME, CNT_SETUP, CNT_DOT, CNT_SEARCH, CNT_ADVANCE, CNT_TRUE, CNT_FG };
 // longest FGMRES restart cycle (Krylov basis vectors kept)
 constexpr int FG_MAXR = 64;
-// Smoother forms: 8-wide vector loads (default), the TMA pipeline, the per-column form.
-enum { RBGS_V8 = 0, RBGS_TMA = 1, RBGS_COLUMN = 2 };
 
 int vsize(int prec) { return prec == MPP_PREC_FP64 ? 8 : 4; }
 int msize(int prec) {
@@ -136,8 +134,10 @@ struct mpp_ctx {
     TmaLev tma[MAXLEV];
     bool tma_ok[MAXLEV];
     int tma_blocks;  // persistent grid of k_rbgs_tma
-    int rbgs_mode;   // which smoother form runs on row-split levels (MPP_RBGS: v8, tma, column)
-    int vec_on;      // vector forms of the other passes (off with MPP_RBGS=column)
+    // smoother form of the fine level and of the coarser row-split levels (MPP_SMOOTHER_*;
+    // the environment's MPP_RBGS / MPP_RBGS_COARSE: vector, tma, column); the other passes
+    // of a level take the vector forms unless its smoother is the column form
+    int form_fine, form_coarse;
     // profiler
     int prof_on;
     std::vector<ProfRec> pending;
@@ -334,7 +334,8 @@ struct Run {
 
     unsigned* cnt(int i) { return c->counters + i; }
     // vector (8 cells per lane) kernels on level l: rows of whole 8-element chunks
-    bool vec(int l) const { return c->vec_on && c->lv[l].H % V8 == 0; }
+    int form(int l) const { return l == 0 ? c->form_fine : c->form_coarse; }
+    bool vec(int l) const { return form(l) != MPP_SMOOTHER_COLUMN && c->lv[l].H % V8 == 0; }
     int grid_w(int l) const {
         const int wpb = TPB / 32, cap = c->nsm * MAXBLOCKS_PER_SM;
         const int g = (c->lv[l].ntiles + wpb - 1) / wpb;
@@ -408,11 +409,11 @@ struct Run {
     void smooth(int l, const std::vector<int>& colours) {
         for (int col : colours) {
             beg(F_RBGS, l);
-            if (c->rbgs_mode == RBGS_TMA && c->tma_ok[l]) {
+            if (form(l) == MPP_SMOOTHER_TMA && c->tma_ok[l]) {
                 const int g = c->lv[l].ntiles < c->tma_blocks ? c->lv[l].ntiles : c->tma_blocks;
                 launch(k_rbgs_tma<Pr>, g > 0 ? g : 1, TPB, TmaGeom<M>::SMEM, s, view<M>(c, l), col, c->tma[l],
                                                                            &c->sc->s.fault);
-            } else if (c->rbgs_mode != RBGS_COLUMN && c->lv[l].H % V8 == 0) {
+            } else if (form(l) != MPP_SMOOTHER_COLUMN && c->lv[l].H % V8 == 0) {
                 const int wpb = TPB / 32, cap = c->nsm * MAXBLOCKS_PER_SM;
                 int g = (c->lv[l].ntiles + wpb - 1) / wpb;
                 g = g < cap ? (g > 0 ? g : 1) : cap;
@@ -1028,8 +1029,13 @@ int build_tma(mpp_ctx* c) {
     const int pad = 16 / (int)ms;
     const bool off = getenv("MPP_NO_TMA") != nullptr;
     const char* mode = getenv("MPP_RBGS");
-    c->rbgs_mode = !mode ? RBGS_V8 : (!strcmp(mode, "tma") ? RBGS_TMA : (!strcmp(mode, "column") ? RBGS_COLUMN : RBGS_V8));
-    c->vec_on = c->rbgs_mode != RBGS_COLUMN;
+    auto parse = [](const char* m, int dflt) {
+        return !m ? dflt
+                  : (!strcmp(m, "tma") ? MPP_SMOOTHER_TMA
+                                       : (!strcmp(m, "column") ? MPP_SMOOTHER_COLUMN : MPP_SMOOTHER_VECTOR));
+    };
+    c->form_fine = parse(mode, MPP_SMOOTHER_VECTOR);
+    c->form_coarse = parse(getenv("MPP_RBGS_COARSE"), c->form_fine);
     for (int l = 0; l < MAXLEV; l++) c->tma_ok[l] = false;
     for (int l = 0; l < c->lb; l++) {
         const LevelBuf& b = c->lv[l];
@@ -1269,7 +1275,7 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
             B.odc = take(Nl);
         }
         c->bot_smem = o;
-        c->restrict_smem = (size_t)RX * RY * RZ * cs;
+        c->restrict_smem = (size_t)R_ROWS * R_W * cs;
         int optin = 0;
         CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
         if (c->bot_smem > (size_t)optin) {
@@ -1581,21 +1587,29 @@ int mpp_batch_project(mpp_batch* b, const mpp_basin_arrays* basins, double dt, d
 }
 
 // ---- the autotuner: smoother form x sweeps, timed on the basin's own solve ----
-int mpp_ctx_set_smoother(mpp_ctx* c, int form) {
+int mpp_ctx_set_smoothers(mpp_ctx* c, int fine, int coarse) {
     if (int e = check_ctx(c)) return e;
-    if (form < MPP_SMOOTHER_VECTOR || form > MPP_SMOOTHER_COLUMN) {
-        set_err("unknown smoother form %d", form);
-        return MPP_ERR_INVALID;
-    }
-    c->rbgs_mode = form == MPP_SMOOTHER_VECTOR ? RBGS_V8 : (form == MPP_SMOOTHER_TMA ? RBGS_TMA : RBGS_COLUMN);
-    c->vec_on = c->rbgs_mode != RBGS_COLUMN;
+    for (int f : {fine, coarse})
+        if (f < MPP_SMOOTHER_VECTOR || f > MPP_SMOOTHER_COLUMN) {
+            set_err("unknown smoother form %d", f);
+            return MPP_ERR_INVALID;
+        }
+    c->form_fine = fine;
+    c->form_coarse = coarse;
     drop_graphs(c);
     return MPP_OK;
 }
 
-int mpp_ctx_smoother(const mpp_ctx* c) {
-    if (!c) return MPP_ERR_INVALID;
-    return c->rbgs_mode == RBGS_V8 ? MPP_SMOOTHER_VECTOR : (c->rbgs_mode == RBGS_TMA ? MPP_SMOOTHER_TMA : MPP_SMOOTHER_COLUMN);
+int mpp_ctx_set_smoother(mpp_ctx* c, int form) { return mpp_ctx_set_smoothers(c, form, form); }
+
+int mpp_ctx_smoothers(const mpp_ctx* c, int* fine, int* coarse) {
+    if (!c) {
+        set_err("null context");
+        return MPP_ERR_INVALID;
+    }
+    if (fine) *fine = c->form_fine;
+    if (coarse) *coarse = c->form_coarse;
+    return MPP_OK;
 }
 
 int mpp_autotune(mpp_ctx* c, const float* u, const float* v, const float* w, const uint8_t* types, const float* phi,
@@ -1608,13 +1622,12 @@ int mpp_autotune(mpp_ctx* c, const float* u, const float* v, const float* w, con
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
     const mpp_opts saved = c->opts;
-    const int saved_form = mpp_ctx_smoother(c);
-    bool any_tma = false;
-    for (int l = 0; l < c->lb; l++) any_tma = any_tma || c->tma_ok[l];
+    const int saved_fine = c->form_fine, saved_coarse = c->form_coarse;
+    bool tma0 = c->tma_ok[0], tma1 = false;
+    for (int l = 1; l < c->lb; l++) tma1 = tma1 || c->tma_ok[l];
     float *b = nullptr, *P = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     std::vector<mpp_tune_entry> tried;
-    int err = MPP_OK;
     // trial buffers live only for the call
     auto run = [&]() -> int {
         CK(cudaMalloc(&b, sizeof(float) * (size_t)N));
@@ -1622,36 +1635,46 @@ int mpp_autotune(mpp_ctx* c, const float* u, const float* v, const float* w, con
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
         if (int e = mpp_rhs(c, b, u, v, w, types, 0.f, stream)) return e;
-        for (int form = MPP_SMOOTHER_VECTOR; form <= MPP_SMOOTHER_COLUMN; form++) {
-            if (form == MPP_SMOOTHER_TMA && !any_tma) continue;
-            for (int sw = 1; sw <= 3; sw++) {
-                mpp_opts o = saved;
-                o.sweeps = sw;
-                o.graph = 1;
-                o.fallback = 0;
-                if (int e = mpp_ctx_set_opts(c, &o)) return e;
-                if (int e = mpp_ctx_set_smoother(c, form)) return e;
-                mpp_tune_entry t{form, sw, 0, MPP_OK, 0.f};
-                for (int rep = 0; rep < 3; rep++) {  // the first run captures the graph
-                    CK(cudaMemsetAsync(P, 0, sizeof(float) * (size_t)N, s));
-                    CK(cudaEventRecord(e0, s));
-                    mpp_result r;
-                    const int st = mpp_pressure(c, P, b, types, phi, &r, stream);
-                    if (st < 0) return st;
-                    CK(cudaEventRecord(e1, s));
-                    CK(cudaEventSynchronize(e1));
-                    float ms = 0.f;
-                    CK(cudaEventElapsedTime(&ms, e0, e1));
-                    if (rep > 0) t.ms += 0.5f * ms;
-                    t.iterations = r.iterations;
-                    t.status = st;
+        for (int fine = MPP_SMOOTHER_VECTOR; fine <= MPP_SMOOTHER_COLUMN; fine++) {
+            if (fine == MPP_SMOOTHER_TMA && !tma0) continue;
+            for (int coarse = MPP_SMOOTHER_VECTOR; coarse <= MPP_SMOOTHER_COLUMN; coarse++) {
+                if (coarse == MPP_SMOOTHER_TMA && !tma1) continue;
+                if (c->lb < 2 && coarse != fine) continue;  // no coarse row-split level
+                for (int k = 0; k < 8; k++) {
+                    const int sw = 1 + (k >> 1);  // sweeps 1..4
+                    // the coarsest solve's sweeps: the reference's 40, or 10 (16-bit forms only:
+                    // the FP32 form keeps the reference's V-cycle)
+                    const int coarse_sweeps = (k & 1) ? 10 : saved.coarse;
+                    if ((k & 1) && !(c->prec == MPP_PREC_MIXED_FP16 || c->prec == MPP_PREC_MIXED_BF16)) continue;
+                    mpp_opts o = saved;
+                    o.sweeps = sw;
+                    o.coarse = coarse_sweeps;
+                    o.graph = 1;
+                    o.fallback = 0;
+                    if (int e = mpp_ctx_set_opts(c, &o)) return e;
+                    if (int e = mpp_ctx_set_smoothers(c, fine, coarse)) return e;
+                    mpp_tune_entry t{fine, coarse, sw, coarse_sweeps, 0, MPP_OK, 0.f};
+                    for (int rep = 0; rep < 3; rep++) {  // the first run captures the graph
+                        CK(cudaMemsetAsync(P, 0, sizeof(float) * (size_t)N, s));
+                        CK(cudaEventRecord(e0, s));
+                        mpp_result r;
+                        const int st = mpp_pressure(c, P, b, types, phi, &r, stream);
+                        if (st < 0) return st;
+                        CK(cudaEventRecord(e1, s));
+                        CK(cudaEventSynchronize(e1));
+                        float ms = 0.f;
+                        CK(cudaEventElapsedTime(&ms, e0, e1));
+                        if (rep > 0) t.ms += 0.5f * ms;
+                        t.iterations = r.iterations;
+                        t.status = st;
+                    }
+                    tried.push_back(t);
                 }
-                tried.push_back(t);
             }
         }
         return MPP_OK;
     };
-    err = run();
+    const int err = run();
     if (b) cudaFree(b);
     if (P) cudaFree(P);
     if (e0) cudaEventDestroy(e0);
@@ -1661,13 +1684,15 @@ int mpp_autotune(mpp_ctx* c, const float* u, const float* v, const float* w, con
         if (tried[i].status == MPP_OK && (best < 0 || tried[i].ms < tried[best].ms)) best = i;
     // apply the winner, or put the previous settings back
     mpp_opts o = saved;
-    int form = saved_form;
+    int fine = saved_fine, coarse = saved_coarse;
     if (err == MPP_OK && best >= 0) {
         o.sweeps = tried[best].sweeps;
-        form = tried[best].smoother;
+        o.coarse = tried[best].coarse_sweeps;
+        fine = tried[best].smoother;
+        coarse = tried[best].coarse_smoother;
     }
     if (int e = mpp_ctx_set_opts(c, &o)) return e;
-    if (int e = mpp_ctx_set_smoother(c, form)) return e;
+    if (int e = mpp_ctx_set_smoothers(c, fine, coarse)) return e;
     if (err) return err;
     for (int i = 0; i < (int)tried.size() && i < capacity && table; i++) table[i] = tried[i];
     if (chosen) *chosen = best;

@@ -315,10 +315,8 @@ __global__ void __launch_bounds__(TPB) k_level(const uint8_t* __restrict__ tf, i
 // coarse cell, its 64 code and residual loads issued together. Values in C precision
 // (the scaled forms without the factor 4).
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_restrict_bottom(Lev<typename Pr::M> F, Lev<typename Pr::M> L,
+__device__ __forceinline__ void restrict_bottom_body(Lev<typename Pr::M> F, Lev<typename Pr::M> L,
                                                          typename Pr::C* __restrict__ bout) {
-    pdl_wait();
-    pdl_trigger();
     using C = typename Pr::C;
     const int N = L.n1 * L.n2 * L.n3;
     for (int c = blockIdx.x * TPB + threadIdx.x; c < N; c += gridDim.x * TPB) {
@@ -349,6 +347,13 @@ __global__ void __launch_bounds__(TPB) k_restrict_bottom(Lev<typename Pr::M> F, 
         }
         bout[c] = v;
     }
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_restrict_bottom(Lev<typename Pr::M> F, Lev<typename Pr::M> L,
+                                                         typename Pr::C* __restrict__ bout) {
+    pdl_wait();
+    pdl_trigger();
+    restrict_bottom_body<Pr>(F, L, bout);
 }
 
 

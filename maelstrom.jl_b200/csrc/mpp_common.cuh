@@ -22,7 +22,13 @@ constexpr uint8_t SELF = 1u << 6;
 // Tiles: 32 (h) x 4 (j) x 2 (k) slots of 2 cells each (one per colour), so a tile is a
 // 64 x 4 x 2 block of cells; 256 threads, one slot each; a warp reads one row's 32
 // consecutive same-colour values (64-128 bytes).
-constexpr int TH = 32, TY = 4, TZ = 2, TPB = 256;
+#ifndef MPP_TILE_H
+#define MPP_TILE_H 32
+#define MPP_TILE_Y 4
+#define MPP_TILE_Z 2
+#endif
+constexpr int TH = MPP_TILE_H, TY = MPP_TILE_Y, TZ = MPP_TILE_Z, TPB = 256;
+static_assert(TY % 2 == 0 && TZ % 2 == 0, "prolongation maps a tile's rows and planes onto whole coarse ones");
 static_assert(TH * TY * TZ == TPB, "one thread per tile slot");
 
 // Grid-wide sums: at most MAXK values per block, at most MAXBLOCKS_PER_SM blocks per SM

@@ -116,9 +116,7 @@ __device__ __forceinline__ void advance_finish(Scalars* sc, const double (&acc)[
 
 // start_kernel! (src/flip.jl:965-973): colour-0 LIQUID cells get b/diag, every other cell 0.
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_start(Lev<typename Pr::M> L) {
-    pdl_wait();
-    pdl_trigger();
+__device__ __forceinline__ void start_body(Lev<typename Pr::M> L) {
     using C = typename Pr::C;
     const int sz = L.n1 * L.n2;
     FOR_TILES_PF(L, tile) {
@@ -147,13 +145,17 @@ __global__ void __launch_bounds__(TPB) k_start(Lev<typename Pr::M> L) {
             }
     }
 }
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_start(Lev<typename Pr::M> L) {
+    pdl_wait();
+    pdl_trigger();
+    start_body<Pr>(L);
+}
 
 // rbgs_kernel! (src/flip.jl:870-877): one colour of red-black Gauss-Seidel,
 // x = (b + sum_LIQ x_n) / diag on LIQUID cells of that colour.
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_rbgs(Lev<typename Pr::M> L, int colour) {
-    pdl_wait();
-    pdl_trigger();
+__device__ __forceinline__ void rbgs_body(Lev<typename Pr::M> L, int colour) {
     using C = typename Pr::C;
     const int sy = L.n1, sz = L.n1 * L.n2;
     const int own = colour * L.H, oth = (1 - colour) * L.H;
@@ -180,6 +182,12 @@ __global__ void __launch_bounds__(TPB) k_rbgs(Lev<typename Pr::M> L, int colour)
                 st(L.x + c.rb + q * sz + own + c.h, dv[q] > (C)0 ? (bv[q] + s) / dv[q] : (C)0);
             }
     }
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_rbgs(Lev<typename Pr::M> L, int colour) {
+    pdl_wait();
+    pdl_trigger();
+    rbgs_body<Pr>(L, colour);
 }
 
 // ---- vector form: 8 consecutive same-colour cells of a row per lane ----
@@ -213,9 +221,7 @@ __device__ __forceinline__ void st8(T* p, const Vec8<T>& r) {
 // b and x (kept where the cell is not LIQUID); other colour: the same 8 columns of this
 // row (the +x/-x neighbours, plus one element on each side) and of the rows at -+y, -+z.
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_rbgs_v8(Lev<typename Pr::M> L, int colour) {
-    pdl_wait();
-    pdl_trigger();
+__device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) {
     using C = typename Pr::C;
     using M = typename Pr::M;
     const int sy = L.n1, sz = L.n1 * L.n2;
@@ -254,6 +260,12 @@ __global__ void __launch_bounds__(TPB) k_rbgs_v8(Lev<typename Pr::M> L, int colo
         }
         st8(L.x + p, out);
     }
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_rbgs_v8(Lev<typename Pr::M> L, int colour) {
+    pdl_wait();
+    pdl_trigger();
+    rbgs_v8_body<Pr>(L, colour);
 }
 
 // A lane's 8 columns in a tile (vector kernels): h .. h+7 of row j, plane k.
@@ -310,9 +322,7 @@ __device__ __forceinline__ void nb6_of(C (&nb)[6], const Nb8<M>& a, int q, int c
 
 // start_kernel! (src/flip.jl:965-973), vector form.
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_start_v8(Lev<typename Pr::M> L) {
-    pdl_wait();
-    pdl_trigger();
+__device__ __forceinline__ void start_v8_body(Lev<typename Pr::M> L) {
     using C = typename Pr::C;
     using M = typename Pr::M;
     FOR_TILES_W(L, tile) {
@@ -333,12 +343,16 @@ __global__ void __launch_bounds__(TPB) k_start_v8(Lev<typename Pr::M> L) {
         st8(L.x + p0 + L.H, x1);
     }
 }
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_start_v8(Lev<typename Pr::M> L) {
+    pdl_wait();
+    pdl_trigger();
+    start_v8_body<Pr>(L);
+}
 
 // residual_kernel! (src/flip.jl:859-863), vector form: both colours of the lane's columns.
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_residual_v8(Lev<typename Pr::M> L) {
-    pdl_wait();
-    pdl_trigger();
+__device__ __forceinline__ void residual_v8_body(Lev<typename Pr::M> L) {
     using C = typename Pr::C;
     using M = typename Pr::M;
     const int sy = L.n1, sz = L.n1 * L.n2;
@@ -367,6 +381,12 @@ __global__ void __launch_bounds__(TPB) k_residual_v8(Lev<typename Pr::M> L) {
             st8(L.r + p, out);
         }
     }
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_residual_v8(Lev<typename Pr::M> L) {
+    pdl_wait();
+    pdl_trigger();
+    residual_v8_body<Pr>(L);
 }
 
 // inner(s, z, r) and the flexible z.q (see k_dot), vector form.
@@ -533,9 +553,7 @@ __global__ void __launch_bounds__(TPB)
 // cells hold zero, as in k_prolong), then each lane adds the trilinear correction to its
 // 16 fine cells (8 columns, both colours) and writes them back in 16-byte pieces.
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_prolong_v8(Lev<typename Pr::M> L, Lev<typename Pr::M> Cl, int cnat) {
-    pdl_wait();
-    pdl_trigger();
+__device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typename Pr::M> Cl, int cnat) {
     using C = typename Pr::C;
     using M = typename Pr::M;
     constexpr int WPB = TPB / 32, NE = PX * PY * PZ, PER = (NE + 31) / 32;
@@ -599,12 +617,16 @@ __global__ void __launch_bounds__(TPB) k_prolong_v8(Lev<typename Pr::M> L, Lev<t
         }
     }
 }
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_prolong_v8(Lev<typename Pr::M> L, Lev<typename Pr::M> Cl, int cnat) {
+    pdl_wait();
+    pdl_trigger();
+    prolong_v8_body<Pr>(L, Cl, cnat);
+}
 
 // residual_kernel! (src/flip.jl:859-863): r = b - (diag x - sum_LIQ x_n) on LIQUID, else 0.
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_residual(Lev<typename Pr::M> L) {
-    pdl_wait();
-    pdl_trigger();
+__device__ __forceinline__ void residual_body(Lev<typename Pr::M> L) {
     using C = typename Pr::C;
     const int sy = L.n1, sz = L.n1 * L.n2;
     FOR_TILES_PF(L, tile) {
@@ -633,6 +655,12 @@ __global__ void __launch_bounds__(TPB) k_residual(Lev<typename Pr::M> L) {
             }
         }
     }
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_residual(Lev<typename Pr::M> L) {
+    pdl_wait();
+    pdl_trigger();
+    residual_body<Pr>(L);
 }
 
 // ---- CG (src/flip.jl:1033-1111) over the fine level's active tiles ----

@@ -96,40 +96,65 @@ __device__ __forceinline__ C wB(int a) {
 // cells of the 4x4x4 block (a fastest); the scaled (16-bit) forms drop the factor 4.
 // One block per coarse tile: the tile's fine region (RX x RY x RZ cells) is staged in
 // shared memory, non-LIQUID cells as zero, then each thread sums its two coarse cells.
+// The region is staged as the fine level stores it: per fine row (j, k) and colour, the
+// R_W row-split columns from 2 TH th - 1 on, one warp per row, so the loads are contiguous
+// runs and carry no per-element index arithmetic. In those terms fine cell (2I-1+a, 2J-1+b,
+// 2K-1+c) of coarse cell (I, J, K) has colour (a+b+c) & 1 and column I - 2 TH th + {0,1,1,2}[a].
 constexpr int RX = 4 * TH + 2, RY = 2 * TY + 2, RZ = 2 * TZ + 2;
+constexpr int R_W = 2 * TH + 2, R_ROWS = 2 * RY * RZ;  // staged columns per row, rows (x2 colours)
+
+// Term t = 16 c + 4 b + a of a coarse cell: weight w_a w_b w_c (exact dyadic constants,
+// associated as the reference's (w_a w_b) w_c) and its offset from the coarse cell's
+// first staged element.
+template <class C>
+__host__ __device__ constexpr C rw(int t) {
+    return (((t & 3) == 1 || (t & 3) == 2) ? (C)0.375f : (C)0.125f) *
+           ((((t >> 2) & 3) == 1 || ((t >> 2) & 3) == 2) ? (C)0.375f : (C)0.125f) *
+           (((t >> 4) == 1 || (t >> 4) == 2) ? (C)0.375f : (C)0.125f);
+}
+__host__ __device__ constexpr int roff(int t) {
+    return (((t >> 4) * RY + ((t >> 2) & 3)) * 2 + (((t & 3) + ((t >> 2) & 3) + (t >> 4)) & 1)) * R_W + ((t & 3) + 1) / 2;
+}
 
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_restrict(Lev<typename Pr::M> F, Lev<typename Pr::M> L) {
-    pdl_wait();
-    pdl_trigger();
+__device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typename Pr::M> L) {
     using C = typename Pr::C;
     extern __shared__ __align__(128) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
+    constexpr int WPB = TPB / 32, RPW = (R_ROWS + WPB - 1) / WPB, NS = (R_W + 31) / 32;
     const int n = *L.count;
     const int lh = slot_h(), lj = slot_j(), lk = slot_k();
+    const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31;
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
         const uint32_t tile = L.tiles[t];
         const int th = (int)(tile & 1023u), tj = (int)((tile >> 10) & 1023u), tk = (int)(tile >> 20);
-        const int i0 = 4 * TH * th - 1, j0 = 2 * TY * tj - 1, k0 = 2 * TZ * tk - 1;
+        const int hbase = 2 * TH * th - 1, j0 = 2 * TY * tj - 1, k0 = 2 * TZ * tk - 1;
         __syncthreads();
         // Every non-LIQUID cell's r is zero (the residual pass writes zeros in active tiles
         // and the set-up clears the array each projection), so r is staged unmasked: all of
         // a thread's loads go out at once, then land in shared memory.
-        constexpr int NE = RX * RY * RZ, PER = (NE + TPB - 1) / TPB;
-        C vals[PER];
+        C vals[RPW][NS];
 #pragma unroll
-        for (int u = 0; u < PER; u++) {
-            const int e = (int)threadIdx.x + u * TPB;
-            const int ii = e % RX, jj = (e / RX) % RY, kk = e / (RX * RY);
-            const int i = i0 + ii, j = j0 + jj, k = k0 + kk;
-            vals[u] = (C)0;
-            if (e < NE && i >= 0 && i < F.n1 && j >= 0 && j < F.n2 && k >= 0 && k < F.n3)
-                vals[u] = ld<C>(F.r + (int)F.pos(i, j, k));
+        for (int u = 0; u < RPW; u++) {
+            const int r = warp + u * WPB;
+            const int col = r & 1, jk = r >> 1, j = j0 + jk % RY, k = k0 + jk / RY;
+            const bool row = r < R_ROWS && j >= 0 && j < F.n2 && k >= 0 && k < F.n3;
+            const int base = row ? (k * F.n2 + j) * F.n1 + col * F.H : 0;
+#pragma unroll
+            for (int q = 0; q < NS; q++) {
+                const int off = lane + 32 * q, h = hbase + off;
+                vals[u][q] = (C)0;
+                if (row && off < R_W && h >= 0 && h < F.H) vals[u][q] = ld<C>(F.r + base + h);
+            }
         }
 #pragma unroll
-        for (int u = 0; u < PER; u++) {
-            const int e = (int)threadIdx.x + u * TPB;
-            if (e < NE) sm[e] = vals[u];
+        for (int u = 0; u < RPW; u++) {
+            const int r = warp + u * WPB;
+#pragma unroll
+            for (int q = 0; q < NS; q++) {
+                const int off = lane + 32 * q;
+                if (r < R_ROWS && off < R_W) sm[r * R_W + off] = vals[u][q];
+            }
         }
         __syncthreads();
         const int h = th * TH + lh, J = tj * TY + lj, K = tk * TZ + lk;
@@ -140,22 +165,23 @@ __global__ void __launch_bounds__(TPB) k_restrict(Lev<typename Pr::M> F, Lev<typ
                 const int p = rb + cc * L.H + h;
                 C v = (C)0;
                 if (L.code[p] & SELF) {
-                    const int il = 2 * (2 * lh + ci_of(cc, J, K));
+                    const C* base = sm + ((2 * lk * RY + 2 * lj) * 2) * R_W + 2 * lh + ci_of(cc, J, K);
                     C s = (C)0;
 #pragma unroll
-                    for (int c3 = 0; c3 < 4; c3++)
-#pragma unroll
-                        for (int b3 = 0; b3 < 4; b3++)
-#pragma unroll
-                            for (int a3 = 0; a3 < 4; a3++)
-                                s += wB<C>(a3) * wB<C>(b3) * wB<C>(c3) *
-                                     sm[((2 * lk + c3) * RY + 2 * lj + b3) * RX + il + a3];
+                    for (int t = 0; t < 64; t++)  // c outer, a inner: the reference's order
+                        s += rw<C>(t) * base[roff(t)];
                     v = Pr::scaled ? s : (C)4 * s;
                 }
                 st(L.b + p, v);
             }
         }
     }
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_restrict(Lev<typename Pr::M> F, Lev<typename Pr::M> L) {
+    pdl_wait();
+    pdl_trigger();
+    restrict_body<Pr>(F, L);
 }
 
 // prolongweights (src/flip.jl:908-911), 0-based.
@@ -173,9 +199,7 @@ __device__ __forceinline__ void pweights(int i, int& c0, C& w0, int& c1, C& w1) 
 constexpr int PX = TH + 2, PY = TY / 2 + 2, PZ = TZ / 2 + 2;
 
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_prolong(Lev<typename Pr::M> L, Lev<typename Pr::M> Cl, int cnat) {
-    pdl_wait();
-    pdl_trigger();
+__device__ __forceinline__ void prolong_body(Lev<typename Pr::M> L, Lev<typename Pr::M> Cl, int cnat) {
     using C = typename Pr::C;
     __shared__ C sm[TILES_PER_BLOCK][PZ][PY][PX];
     const int n = *L.count;
@@ -262,6 +286,12 @@ __global__ void __launch_bounds__(TPB) k_prolong(Lev<typename Pr::M> L, Lev<type
             for (int cc = 0; cc < 2; cc++)
                 if (live[cc][q]) st(L.x + c.rb + q * sz + cc * L.H + c.h, v[cc][q]);
     }
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_prolong(Lev<typename Pr::M> L, Lev<typename Pr::M> Cl, int cnat) {
+    pdl_wait();
+    pdl_trigger();
+    prolong_body<Pr>(L, Cl, cnat);
 }
 
 // ---- the small levels and the coarsest, in one CTA ----

@@ -53,8 +53,9 @@ class BasinArrays(ctypes.Structure):
 
 
 class TuneEntry(ctypes.Structure):
-    _fields_ = [("smoother", ctypes.c_int32), ("sweeps", ctypes.c_int32), ("iterations", ctypes.c_int32),
-                ("status", ctypes.c_int32), ("ms", ctypes.c_float)]
+    _fields_ = [("smoother", ctypes.c_int32), ("coarse_smoother", ctypes.c_int32), ("sweeps", ctypes.c_int32),
+                ("coarse_sweeps", ctypes.c_int32), ("iterations", ctypes.c_int32), ("status", ctypes.c_int32),
+                ("ms", ctypes.c_float)]
 
 
 SMOOTHERS = {0: "vector", 1: "tma", 2: "column"}
@@ -82,7 +83,8 @@ SIGNATURES = {
     "mpp_batch_ctx": (P, [P, ctypes.c_int]),
     "mpp_batch_project": (ctypes.c_int, [P, ctypes.POINTER(BasinArrays), F64, F64, _R, P]),
     "mpp_ctx_set_smoother": (ctypes.c_int, [P, ctypes.c_int]),
-    "mpp_ctx_smoother": (ctypes.c_int, [P]),
+    "mpp_ctx_set_smoothers": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int]),
+    "mpp_ctx_smoothers": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "mpp_autotune": (ctypes.c_int, [P, P, P, P, P, P, ctypes.POINTER(TuneEntry), ctypes.c_int,
                                     ctypes.POINTER(ctypes.c_int), P]),
     "mpp_advect_phi": (ctypes.c_int, [P, P, P, P, P, P, F32, P]),

@@ -78,7 +78,7 @@ def test_autotune(cuda):
         assert rep["chosen"] is not None
         assert len(rep["table"]) >= 6  # vector and column forms x 3 sweep counts at least
         best = min((r for r in rep["table"] if r["status"] == 0), key=lambda r: r["ms"])
-        assert rep["chosen"] == (best["smoother"], best["sweeps"])
+        assert rep["chosen"] == (best["smoother"], best["coarse_smoother"], best["sweeps"], best["coarse_sweeps"])
     res = batch.project(1 / 48)
     assert all(r.status == 0 for r in res)
 
