@@ -213,8 +213,14 @@ def run_mpp(args):
     if args.ncu:
         # profiling mode: the headline projection only, its CG loop run from the host so a
         # profiler sees each kernel launch (kernels inside the graph's WHILE node are not
-        # reported one by one); no timing is printed
+        # reported one by one); no timing is printed. --tuned gives the autotuner's choice
+        # (fine form, coarse form, sweeps, coarsest sweeps) without running it.
         proj = make(prec, False)
+        if args.tuned:
+            fine, coarse, sw, swc, csw = args.tuned.split(",")
+            forms = {"vector": 0, "tma": 1, "column": 2}
+            proj.set(sweeps=int(sw), sweeps_coarse=int(swc), coarse=int(csw))
+            proj.lib.mpp_ctx_set_smoothers(proj._ctx, forms[fine], forms[coarse])
         vol0 = proj.volume(phi)
         for _ in range(args.steps):
             u.copy_(u0); v.copy_(v0); w.copy_(w0); P.zero_()
@@ -616,6 +622,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=25.0)
     ap.add_argument("--reference-seconds", type=float, default=150.0)
     ap.add_argument("--profile-out", default=None)
+    ap.add_argument("--tuned", default=None,
+                    help="--ncu mode: fine,coarse,sweeps,coarse-level sweeps,coarsest (e.g. vector,column,4,2,10)")
     ap.add_argument("--ncu", action="store_true",
                     help="profiling mode: --steps headline projections from the host loop, nothing timed")
     args = ap.parse_args()

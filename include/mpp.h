@@ -81,6 +81,7 @@ typedef struct {
     int32_t restart;        /* FGMRES restart length (default 8, src/fgmres.jl:26) */
     int32_t fallback_maxiter; /* FGMRES iterations (default 240) */
     int32_t cg_maxiter_with_fallback; /* CG iterations before the fallback (default 80, src/fgmres.jl:99) */
+    int32_t sweeps_coarse;  /* sweeps on the levels below the fine one (0: `sweeps`, the reference's) */
 } mpp_opts;
 
 typedef struct {
@@ -211,15 +212,17 @@ int mpp_ctx_smoothers(const mpp_ctx* ctx, int* fine, int* coarse);
 typedef struct {
     int32_t smoother;        /* MPP_SMOOTHER_* of the fine level */
     int32_t coarse_smoother; /* MPP_SMOOTHER_* of the coarser row-split levels */
-    int32_t sweeps;          /* smoother sweeps per level and direction */
+    int32_t sweeps;          /* smoother sweeps of the fine level, each way */
+    int32_t sweeps_coarse;   /* of the coarser levels */
     int32_t coarse_sweeps;   /* sweeps of the coarsest solve, each way */
     int32_t iterations; /* CG iterations to tol */
     int32_t status;     /* solver status */
     float ms;           /* time of the solve (CUDA events, graph launch) */
 } mpp_tune_entry;
 /* Time the basin's own pressure solve (rhs from u, v, w; zero start; the context's tol and
- * precision) for every fine x coarse smoother form x sweeps in 1..4 (and, in the 16-bit forms, 10
- * instead of 40 coarsest sweeps), keep the fastest that converges on
+ * precision): first every fine x coarse smoother form at the context's sweeps, then with the
+ * fastest forms fine sweeps 1..5 x coarse-level sweeps 1..4 (and, in the 16-bit forms, 10
+ * instead of 40 coarsest sweeps); keep the fastest that converges on
  * the context, and return the number of candidates tried (table[0..capacity) gets them,
  * *chosen the winner's index, -1 when none converged). Allocates two trial arrays for
  * the call. */

@@ -66,6 +66,8 @@ struct LevelBuf {
     uint8_t* tflag;
     uint32_t* tiles;
     int* count;
+    void* di;   // reciprocal diagonal (16-bit forms)
+    int* edge;  // LIQUID cell on an x/y face (device flag, set during set-up)
 };
 
 // Kernel families, for the profiler.
@@ -112,6 +114,7 @@ struct mpp_ctx {
     void *diag, *bvec, *r, *d, *q;
     void* Pd;  // FP64 solution (natural), FP64 contexts only
     uint8_t* tflag_all;
+    int* edges;  // the levels' edge flags
     size_t tflag_bytes;
     Scalars* sc;
     Scalars* sc_host;  // pinned
@@ -196,6 +199,7 @@ Lev<M> view(const mpp_ctx* c, int l) {
     v.code = b.code;
     v.dg = (M*)b.dg; v.x = (M*)b.x; v.b = (M*)b.b; v.r = (M*)b.r;
     v.types = b.types; v.dc = b.dc; v.tflag = b.tflag; v.tiles = b.tiles; v.count = b.count;
+    v.di = (M*)b.di; v.edge = b.edge;
     return v;
 }
 
@@ -368,6 +372,7 @@ struct Run {
     // The fine set-up pass, the coarse levels and the tile lists.
     void setup(const SetupIn<V>& in, cudaGraphConditionalHandle cond, int use_cond) {
         cudaMemsetAsync(c->tflag_all, 0, c->tflag_bytes, s);
+        cudaMemsetAsync(c->edges, 0, sizeof(int) * MAXLEV, s);
         // Level residuals and coarse corrections start at zero each projection, so every cell
         // outside the active tiles reads as zero in the staged restriction/prolongation.
         const size_t ms = msize(c->prec);
@@ -427,18 +432,23 @@ struct Run {
 
     // vcycle! (src/flip.jl:992-1014): z = M^-1 r from zero.
     void vcycle() {
-        const int sw = c->opts.sweeps;
-        std::vector<int> down, up;
+        // sweeps of the fine level and of the coarser ones (the reference's one `sweeps`
+        // unless sweeps_coarse is set)
+        const int swf = c->opts.sweeps, sw = c->opts.sweeps_coarse > 0 ? c->opts.sweeps_coarse : swf;
+        std::vector<int> down, up, down0, up0;
         for (int q = 0; q < sw; q++) { down.push_back(0); down.push_back(1); }
         down.erase(down.begin());  // the start kernel is the first colour's first sweep
         for (int q = 0; q < sw; q++) { up.push_back(1); up.push_back(0); }
+        for (int q = 0; q < swf; q++) { down0.push_back(0); down0.push_back(1); }
+        down0.erase(down0.begin());
+        for (int q = 0; q < swf; q++) { up0.push_back(1); up0.push_back(0); }
         const int lb = c->lb;
         for (int l = 0; l < lb; l++) {
             beg(F_START, l);
             if (vec(l)) launch(k_start_v8<Pr>, grid_w(l), TPB, 0, s, view<M>(c, l));
             else launch(k_start<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
             end();
-            smooth(l, down);
+            smooth(l, l == 0 ? down0 : down);
             beg(F_RESID, l);
             if (vec(l)) launch(k_residual_v8<Pr>, grid_w(l), TPB, 0, s, view<M>(c, l));
             else launch(k_residual<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
@@ -469,7 +479,7 @@ struct Run {
             else
                 launch(k_prolong<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l), view<M>(c, l + 1), l + 1 == lb ? 1 : 0);
             end();
-            smooth(l, up);
+            smooth(l, l == 0 ? up0 : up);
         }
     }
 
@@ -1043,7 +1053,7 @@ int build_tma(mpp_ctx* c) {
         TmaLev& t = c->tma[l];
         c->tma_ok[l] = encode_level(&t.xh, dt, b.x, ms, b, TH + 2 * pad, TY + 2, TZ + 2) &&
                        encode_level(&t.b, dt, b.b, ms, b, TH, TY, TZ) &&
-                       encode_level(&t.dg, dt, b.dg, ms, b, TH, TY, TZ) &&
+                       encode_level(&t.dg, dt, ms == 2 ? b.di : b.dg, ms, b, TH, TY, TZ) &&
                        encode_level(&t.code, CU_TENSOR_MAP_DATA_TYPE_UINT8, b.code, 1, b, TH, TY, TZ);
     }
     return dispatch(c->prec, [&](auto pr) -> int {
@@ -1069,6 +1079,7 @@ void mpp_opts_default(mpp_opts* o) {
     o->tol = 1e-4f;
     o->maxiter = 60;
     o->sweeps = 2;
+    o->sweeps_coarse = 0;
     o->coarse = 40;
     o->precision = MPP_PREC_FP32;
     o->graph = 0;
@@ -1126,7 +1137,8 @@ static int validate(const mpp_grid* g, const mpp_opts* o) {
         set_err("dx must be positive");
         return MPP_ERR_INVALID;
     }
-    if (o->sweeps < 1 || o->sweeps > 16 || o->coarse < 0 || o->maxiter < 0 || !(o->tol >= 0.f)) {
+    if (o->sweeps < 1 || o->sweeps > 16 || o->sweeps_coarse < 0 || o->sweeps_coarse > 16 || o->coarse < 0 ||
+        o->maxiter < 0 || !(o->tol >= 0.f)) {
         set_err("bad solver options");
         return MPP_ERR_INVALID;
     }
@@ -1231,12 +1243,15 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
                 if ((e = alloc(c, &b.dg, ms * Nl))) return fail(e);
                 if ((e = alloc(c, &b.b, ms * Nl))) return fail(e);
             }
+            if (ms == 2 && (e = alloc(c, &b.di, ms * Nl))) return fail(e);
         } else {  // a level of the one-CTA bottom solve: natural order
             if ((e = alloc(c, &b.x, ms * Nl))) return fail(e);
             if ((e = alloc(c, (void**)&b.code, Nl))) return fail(e);
             if ((e = alloc(c, (void**)&b.dc, Nl))) return fail(e);
         }
     }
+    if ((e = alloc(c, (void**)&c->edges, sizeof(int) * MAXLEV))) return fail(e);
+    for (int l = 0; l < c->L; l++) c->lv[l].edge = c->edges + l;
     {
         const LevelBuf& b = c->lv[c->lb];
         const size_t cs = c->prec == MPP_PREC_FP64 ? 8 : 4;
@@ -1330,7 +1345,8 @@ int mpp_ctx_set_opts(mpp_ctx* c, const mpp_opts* o) {
         set_err("precision is fixed at context creation");
         return MPP_ERR_INVALID;
     }
-    if (o->sweeps != c->opts.sweeps || o->coarse != c->opts.coarse || o->graph != c->opts.graph ||
+    if (o->sweeps != c->opts.sweeps || o->sweeps_coarse != c->opts.sweeps_coarse || o->coarse != c->opts.coarse ||
+        o->graph != c->opts.graph ||
         (o->fallback != 0) != (c->opts.fallback != 0)) {
         drop_graphs(c);
     }
@@ -1635,43 +1651,62 @@ int mpp_autotune(mpp_ctx* c, const float* u, const float* v, const float* w, con
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
         if (int e = mpp_rhs(c, b, u, v, w, types, 0.f, stream)) return e;
+        auto trial = [&](int fine, int coarse, int sw, int swc, int csw) -> int {
+            mpp_opts o = saved;
+            o.sweeps = sw;
+            o.sweeps_coarse = swc;
+            o.coarse = csw;
+            o.graph = 1;
+            o.fallback = 0;
+            if (int e = mpp_ctx_set_opts(c, &o)) return e;
+            if (int e = mpp_ctx_set_smoothers(c, fine, coarse)) return e;
+            mpp_tune_entry t{fine, coarse, sw, swc, csw, 0, MPP_OK, 0.f};
+            for (int rep = 0; rep < 3; rep++) {  // the first run captures the graph
+                CK(cudaMemsetAsync(P, 0, sizeof(float) * (size_t)N, s));
+                CK(cudaEventRecord(e0, s));
+                mpp_result r;
+                const int st = mpp_pressure(c, P, b, types, phi, &r, stream);
+                if (st < 0) return st;
+                CK(cudaEventRecord(e1, s));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                if (rep > 0) t.ms += 0.5f * ms;
+                t.iterations = r.iterations;
+                t.status = st;
+            }
+            tried.push_back(t);
+            return MPP_OK;
+        };
+        auto best_of = [&](size_t from) {
+            int bi = -1;
+            for (size_t i = from; i < tried.size(); i++)
+                if (tried[i].status == MPP_OK && (bi < 0 || tried[i].ms < tried[bi].ms)) bi = (int)i;
+            return bi;
+        };
+        // 1: the smoother forms, at the context's sweeps
+        const int sw0 = saved.sweeps, swc0 = saved.sweeps_coarse, csw0 = saved.coarse;
         for (int fine = MPP_SMOOTHER_VECTOR; fine <= MPP_SMOOTHER_COLUMN; fine++) {
             if (fine == MPP_SMOOTHER_TMA && !tma0) continue;
             for (int coarse = MPP_SMOOTHER_VECTOR; coarse <= MPP_SMOOTHER_COLUMN; coarse++) {
                 if (coarse == MPP_SMOOTHER_TMA && !tma1) continue;
                 if (c->lb < 2 && coarse != fine) continue;  // no coarse row-split level
-                for (int k = 0; k < 8; k++) {
-                    const int sw = 1 + (k >> 1);  // sweeps 1..4
-                    // the coarsest solve's sweeps: the reference's 40, or 10 (16-bit forms only:
-                    // the FP32 form keeps the reference's V-cycle)
-                    const int coarse_sweeps = (k & 1) ? 10 : saved.coarse;
-                    if ((k & 1) && !(c->prec == MPP_PREC_MIXED_FP16 || c->prec == MPP_PREC_MIXED_BF16)) continue;
-                    mpp_opts o = saved;
-                    o.sweeps = sw;
-                    o.coarse = coarse_sweeps;
-                    o.graph = 1;
-                    o.fallback = 0;
-                    if (int e = mpp_ctx_set_opts(c, &o)) return e;
-                    if (int e = mpp_ctx_set_smoothers(c, fine, coarse)) return e;
-                    mpp_tune_entry t{fine, coarse, sw, coarse_sweeps, 0, MPP_OK, 0.f};
-                    for (int rep = 0; rep < 3; rep++) {  // the first run captures the graph
-                        CK(cudaMemsetAsync(P, 0, sizeof(float) * (size_t)N, s));
-                        CK(cudaEventRecord(e0, s));
-                        mpp_result r;
-                        const int st = mpp_pressure(c, P, b, types, phi, &r, stream);
-                        if (st < 0) return st;
-                        CK(cudaEventRecord(e1, s));
-                        CK(cudaEventSynchronize(e1));
-                        float ms = 0.f;
-                        CK(cudaEventElapsedTime(&ms, e0, e1));
-                        if (rep > 0) t.ms += 0.5f * ms;
-                        t.iterations = r.iterations;
-                        t.status = st;
-                    }
-                    tried.push_back(t);
-                }
+                if (int e = trial(fine, coarse, sw0, swc0, csw0)) return e;
             }
         }
+        const int bf = best_of(0);
+        if (bf < 0) return MPP_OK;
+        const int fine = tried[bf].smoother, coarse = tried[bf].coarse_smoother;
+        // 2: with those forms, the fine and coarse sweeps and (16-bit forms: the FP32 form
+        // keeps the reference's V-cycle) 10 instead of 40 coarsest sweeps
+        const bool half = c->prec == MPP_PREC_MIXED_FP16 || c->prec == MPP_PREC_MIXED_BF16;
+        for (int sw = 1; sw <= 5; sw++)
+            for (int swc = 1; swc <= 4; swc++)
+                for (int csw : {csw0, 10}) {
+                    if (csw == 10 && (!half || csw0 == 10)) continue;
+                    if (sw == sw0 && swc == (swc0 > 0 ? swc0 : sw0) && csw == csw0) continue;  // tried in 1
+                    if (int e = trial(fine, coarse, sw, swc, csw)) return e;
+                }
         return MPP_OK;
     };
     const int err = run();
@@ -1687,6 +1722,7 @@ int mpp_autotune(mpp_ctx* c, const float* u, const float* v, const float* w, con
     int fine = saved_fine, coarse = saved_coarse;
     if (err == MPP_OK && best >= 0) {
         o.sweeps = tried[best].sweeps;
+        o.sweeps_coarse = tried[best].sweeps_coarse;
         o.coarse = tried[best].coarse_sweeps;
         fine = tried[best].smoother;
         coarse = tried[best].coarse_smoother;

@@ -39,10 +39,8 @@ __global__ void __launch_bounds__(TPB) k_vjp_rhs(int n1, int n2, int n3, C* __re
                                                  const float* __restrict__ phi) {
     pdl_wait();
     pdl_trigger();
-    const int64_t N = (int64_t)n1 * n2 * n3;
     const int m1 = n1 + 1, m2 = n2 + 1;
-    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
-        const int i = (int)(idx % n1), j = (int)((idx / n1) % n2), k = (int)(idx / ((int64_t)n1 * n2));
+    FOR_CELLS(n1, n2, n3, i, j, k, idx) {
         C s = (C)0;
         if (types[idx] == LIQUID) {
             const int64_t fu = (int64_t)i + (int64_t)m1 * ((int64_t)j + (int64_t)n2 * k);
@@ -80,10 +78,9 @@ __global__ void __launch_bounds__(TPB) k_vjp_faces(int n1, int n2, int n3, float
                                                    const C* __restrict__ mu, const uint8_t* __restrict__ types) {
     pdl_wait();
     pdl_trigger();
-    const int m1 = n1 + 1, m2 = n2 + 1, m3 = n3 + 1;
-    const int64_t N = (int64_t)m1 * m2 * m3;
-    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
-        const int i = (int)(idx % m1), j = (int)((idx / m1) % m2), k = (int)(idx / ((int64_t)m1 * m2));
+    const int m1 = n1 + 1, m2 = n2 + 1;
+    FOR_CELLS(n1 + 1, n2 + 1, n3 + 1, i, j, k, idx) {
+        (void)idx;
         if (j < n2 && k < n3)
             vjp_face(ou, gu, (int64_t)i + (int64_t)m1 * ((int64_t)j + (int64_t)n2 * k), mu, types, n1, n2, n3, i - 1, j,
                      k, i, j, k);

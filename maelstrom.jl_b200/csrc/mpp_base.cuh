@@ -105,12 +105,8 @@ __global__ void __launch_bounds__(TPB) k_volume(Geo g, const float* __restrict__
                                                 double* partials, unsigned* counter) {
     pdl_wait();
     pdl_trigger();
-    const int64_t N = (int64_t)g.n[0] * g.n[1] * g.n[2];
     double acc[1] = {0.0};
-    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
-        int i = (int)(idx % g.n[0]);
-        int j = (int)((idx / g.n[0]) % g.n[1]);
-        int k = (int)(idx / ((int64_t)g.n[0] * g.n[1]));
+    FOR_CELLS(g.n[0], g.n[1], g.n[2], i, j, k, idx) {
         if (!issolidcell(g, i, j, k)) {
             float x = 0.5f - phi[idx] / g.dx;
             acc[0] += (double)(x > 1.f ? 1.f : (x < 0.f ? 0.f : x));
@@ -163,16 +159,12 @@ __global__ void __launch_bounds__(TPB)
     using M = typename Pr::M;
     using C = typename Pr::C;
     const int n1 = L.n1, n2 = L.n2, n3 = L.n3;
-    const int64_t N = (int64_t)n1 * n2 * n3;
     const C dx = (C)a.dx;
     const C gamma = (C)(sc->p.project ? sc->s.gamma : sc->p.gamma);
     const bool sep_dg = (void*)L.dg != (void*)diag;
     const bool sep_b = (void*)L.b != (void*)r;
     double acc[3] = {0.0, 0.0, 0.0};
-    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
-        const int i = (int)(idx % n1);
-        const int j = (int)((idx / n1) % n2);
-        const int k = (int)(idx / ((int64_t)n1 * n2));
+    FOR_CELLS(n1, n2, n3, i, j, k, idx) {
         const uint8_t t = a.types[idx];
         acc[2] += t == LIQUID ? 1.0 : 0.0;
         const int64_t p = L.pos(i, j, k);
@@ -214,12 +206,14 @@ __global__ void __launch_bounds__(TPB)
                 rv = bv - (d * (C)a.P[idx] - s);
             }
             L.tflag[L.tile_of(i, j, k)] = 1;
+            if (i == 0 || i == n1 - 1 || j == 0 || j == n2 - 1) atomicOr(L.edge, 1);
         } else if (a.clear_P) {
             a.P[idx] = (V)0;
         }
         L.code[p] = code;
         st(diag + p, d);
         if (sep_dg) st(L.dg + p, d);
+        if (L.di) st(L.di + p, d > (C)0 ? (C)1 / d : (C)0);
         st(b + p, bv);
         if (a.residual) {
             st(r + p, rv);
@@ -278,9 +272,7 @@ __global__ void __launch_bounds__(TPB) k_level(const uint8_t* __restrict__ tf, i
     pdl_wait();
     pdl_trigger();
     const int n1 = L.n1, n2 = L.n2, n3 = L.n3;
-    const int64_t N = (int64_t)n1 * n2 * n3;
-    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
-        const int I = (int)(idx % n1), J = (int)((idx / n1) % n2), K = (int)(idx / ((int64_t)n1 * n2));
+    FOR_CELLS(n1, n2, n3, I, J, K, idx) {
         const uint8_t t = coarsen_at(tf, f1, f2, f3, I, J, K);
         L.types[idx] = t;
         uint8_t code = 0;
@@ -298,11 +290,13 @@ __global__ void __launch_bounds__(TPB) k_level(const uint8_t* __restrict__ tf, i
             }
             code |= SELF;
             if (split) L.tflag[L.tile_of(I, J, K)] = 1;
+            if (split && (I == 0 || I == n1 - 1 || J == 0 || J == n2 - 1)) atomicOr(L.edge, 1);
         }
         if (split) {
             const int64_t p = L.pos(I, J, K);
             L.code[p] = code;
             st(L.dg + p, d);
+            if (L.di) st(L.di + p, d > 0.f ? 1.f / d : 0.f);
         } else {  // a level of the one-CTA bottom solve: natural order
             L.code[idx] = code;
             L.dc[idx] = (uint8_t)d;
@@ -386,10 +380,9 @@ __global__ void __launch_bounds__(TPB) k_gradient(int n1, int n2, int n3, float*
                                                   const float* __restrict__ phi, float dx) {
     pdl_wait();
     pdl_trigger();
-    const int m1 = n1 + 1, m2 = n2 + 1, m3 = n3 + 1;
-    const int64_t N = (int64_t)m1 * m2 * m3;
-    for (int64_t idx = (int64_t)blockIdx.x * TPB + threadIdx.x; idx < N; idx += (int64_t)gridDim.x * TPB) {
-        const int i = (int)(idx % m1), j = (int)((idx / m1) % m2), k = (int)(idx / ((int64_t)m1 * m2));
+    const int m1 = n1 + 1, m2 = n2 + 1;
+    FOR_CELLS(n1 + 1, n2 + 1, n3 + 1, i, j, k, idx) {
+        (void)idx;
         if (j < n2 && k < n3)
             face_update(u, fu, (int64_t)i + (int64_t)m1 * ((int64_t)j + (int64_t)n2 * k), P, types, phi, n1, n2, n3,
                         i - 1, j, k, i, j, k, dx);

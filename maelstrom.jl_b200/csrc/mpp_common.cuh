@@ -87,6 +87,14 @@ __device__ __forceinline__ C theta(C pi, C pj) {
     return t > (C)1 ? (C)1 : (t < (C)0.01f ? (C)0.01f : t);
 }
 
+// Walk an n1 x n2 x n3 box row by row: blocks stride over the rows (j, k), a block's
+// threads over i. The row's (j, k) is one 32-bit division per row, not three 64-bit ones
+// per cell, and a warp's cells are consecutive.
+#define FOR_CELLS(n1, n2, n3, i, j, k, idx)                                                     \
+    for (int r_ = (int)blockIdx.x, nr_ = (n2) * (n3); r_ < nr_; r_ += (int)gridDim.x)           \
+        for (int i = (int)threadIdx.x, j = r_ % (n2), k = r_ / (n2); i < (n1); i += (int)blockDim.x) \
+            if (const int64_t idx = (int64_t)r_ * (n1) + i; true)
+
 // One multigrid level as the kernels see it. Levels other than the coarsest are stored
 // row-split: each x-row of n1 cells holds its colour-0 cells (in i order) and then its
 // colour-1 cells, so cell (i,j,k) sits at row(j,k) + colour*H + i/2 with
@@ -107,6 +115,8 @@ struct Lev {
     uint8_t* tflag;  // per-tile "has liquid" flags
     uint32_t* tiles; // active tile list
     int* count;      // its length (device)
+    M* di;           // 1/diagonal (0 off-liquid) for the 16-bit forms' smoother, else null (split)
+    int* edge;       // nonzero when a LIQUID cell lies on the level's x or y faces (device)
 
     __device__ __forceinline__ int64_t row(int j, int k) const { return ((int64_t)k * n2 + j) * n1; }
     __device__ __forceinline__ int64_t pos(int i, int j, int k) const {

@@ -50,6 +50,18 @@ __device__ __forceinline__ C sum6(const C (&v)[6], uint8_t cd) {
     return s;
 }
 
+// liquidsum (src/flip.jl:849-857) for a cell whose six neighbour values are loaded. Every
+// non-LIQUID cell of these arrays holds exactly 0 (start, smoother, prolongation and the
+// CG step write only LIQUID cells; the rest is cleared), so adding all six in the same
+// order rounds exactly as adding the LIQUID ones. The one exception is a read past the
+// row or plane at the level's x/y faces, which lands in a neighbouring row: when a LIQUID
+// cell lies there (`edge`), the code's mask is applied.
+template <class C>
+__device__ __forceinline__ C nsum6(const C (&v)[6], uint8_t cd, bool edge) {
+    if (edge) return sum6<C>(v, cd);
+    return ((((v[0] + v[1]) + v[2]) + v[3]) + v[4]) + v[5];
+}
+
 // ---- the scalar steps of pressure!, run by the last block of each reduction ----
 // After z.r (src/flip.jl:1095-1096, 1105-1107): rho_new and beta = rho_new / rho (0 on the
 // first pass); the flexible form takes the Polak-Ribiere beta (src/sflip.jl:1896-1897).
@@ -130,7 +142,7 @@ __device__ __forceinline__ void start_body(Lev<typename Pr::M> L) {
             if (q < c.kn) {
                 const int p = c.rb + q * sz + c.h;
                 cd[q] = L.code[p];
-                dv[q] = ld<C>(L.dg + p);
+                dv[q] = ld<C>((Pr::scaled ? L.di : L.dg) + p);
                 bv[q] = ld<C>(L.b + p);
             }
         }
@@ -139,7 +151,12 @@ __device__ __forceinline__ void start_body(Lev<typename Pr::M> L) {
             if (q < c.kn) {
                 const int p = c.rb + q * sz + c.h;
                 C v = (C)0;
-                if ((cd[q] & SELF) && dv[q] > (C)0) v = bv[q] / dv[q];
+                // the 16-bit forms multiply by the stored reciprocal (0 where the diagonal is)
+                if constexpr (Pr::scaled) {
+                    if (cd[q] & SELF) v = bv[q] * dv[q];
+                } else {
+                    if ((cd[q] & SELF) && dv[q] > (C)0) v = bv[q] / dv[q];
+                }
                 st(L.x + p, v);
                 st(L.x + p + L.H, (C)0);
             }
@@ -159,6 +176,7 @@ __device__ __forceinline__ void rbgs_body(Lev<typename Pr::M> L, int colour) {
     using C = typename Pr::C;
     const int sy = L.n1, sz = L.n1 * L.n2;
     const int own = colour * L.H, oth = (1 - colour) * L.H;
+    const bool edge = *L.edge != 0;
     FOR_TILES_PF(L, tile) {
         Col c;
         if (!col_of(L, tile, c)) continue;
@@ -170,7 +188,7 @@ __device__ __forceinline__ void rbgs_body(Lev<typename Pr::M> L, int colour) {
             if (q < c.kn) {
                 const int rb = c.rb + q * sz;
                 cd[q] = L.code[rb + own + c.h];
-                dv[q] = ld<C>(L.dg + rb + own + c.h);
+                dv[q] = ld<C>((Pr::scaled ? L.di : L.dg) + rb + own + c.h);
                 bv[q] = ld<C>(L.b + rb + own + c.h);
                 load6<C>(nb[q], L.x, rb + oth + c.h, ci_of(colour, c.j, c.k0 + q), sy, sz);
             }
@@ -178,8 +196,11 @@ __device__ __forceinline__ void rbgs_body(Lev<typename Pr::M> L, int colour) {
 #pragma unroll
         for (int q = 0; q < TZ; q++)
             if (cd[q] & SELF) {
-                const C s = sum6<C>(nb[q], cd[q]);
-                st(L.x + c.rb + q * sz + own + c.h, dv[q] > (C)0 ? (bv[q] + s) / dv[q] : (C)0);
+                const C s = nsum6<C>(nb[q], cd[q], edge);
+                C v;
+                if constexpr (Pr::scaled) v = (bv[q] + s) * dv[q];
+                else v = dv[q] > (C)0 ? (bv[q] + s) / dv[q] : (C)0;
+                st(L.x + c.rb + q * sz + own + c.h, v);
             }
     }
 }
@@ -229,6 +250,7 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = TPB / 32;
     const int hq = lane % V8_LANES_H, lj = (lane / V8_LANES_H) % TY, lk = lane / (V8_LANES_H * TY);
     const int n = *L.count;
+    const bool edge = *L.edge != 0;
     for (int t = blockIdx.x * wpb + warp; t < n; t += gridDim.x * wpb) {
         const uint32_t tile = L.tiles[t];
         const int h = (int)(tile & 1023u) * TH + hq * V8, j = (int)((tile >> 10) & 1023u) * TY + lj,
@@ -238,7 +260,7 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
         const int p = rb + own + h, o = rb + oth + h;
         const int ci = ci_of(colour, j, k);
         const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
-        const Vec8<M> dv = ld8(L.dg + p), bv = ld8(L.b + p), xo = ld8(L.x + p);
+        const Vec8<M> dv = ld8((Pr::scaled ? L.di : L.dg) + p), bv = ld8(L.b + p), xo = ld8(L.x + p);
         const Vec8<M> xc = ld8(L.x + o), yp = ld8(L.x + o + sy), ym = ld8(L.x + o - sy), zp = ld8(L.x + o + sz),
                       zm = ld8(L.x + o - sz);
         const M xl = L.x[o - 1], xr = L.x[o + V8];
@@ -256,7 +278,12 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
             nb[5] = ld<C>(&zm.v[q]);
             const C d = ld<C>(&dv.v[q]);
             out.v[q] = xo.v[q];
-            if (cd[q] & SELF) st(&out.v[q], d > (C)0 ? (ld<C>(&bv.v[q]) + sum6<C>(nb, cd[q])) / d : (C)0);
+            if (cd[q] & SELF) {
+                const C s = nsum6<C>(nb, cd[q], edge);
+                // the 16-bit forms multiply by the stored reciprocal (0 where the diagonal is)
+                if constexpr (Pr::scaled) st(&out.v[q], (ld<C>(&bv.v[q]) + s) * d);
+                else st(&out.v[q], d > (C)0 ? (ld<C>(&bv.v[q]) + s) / d : (C)0);
+            }
         }
         st8(L.x + p, out);
     }
@@ -330,13 +357,14 @@ __device__ __forceinline__ void start_v8_body(Lev<typename Pr::M> L) {
         if (!lane8_of(L, tile, a)) continue;
         const int p0 = a.rb + a.h;
         const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p0);
-        const Vec8<M> dv = ld8(L.dg + p0), bv = ld8(L.b + p0);
+        const Vec8<M> dv = ld8((Pr::scaled ? L.di : L.dg) + p0), bv = ld8(L.b + p0);
         const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
         Vec8<M> x0, x1;
 #pragma unroll
         for (int q = 0; q < V8; q++) {
             const C d = ld<C>(&dv.v[q]);
-            st(&x0.v[q], ((cd[q] & SELF) && d > (C)0) ? ld<C>(&bv.v[q]) / d : (C)0);
+            if constexpr (Pr::scaled) st(&x0.v[q], (cd[q] & SELF) ? ld<C>(&bv.v[q]) * d : (C)0);
+            else st(&x0.v[q], ((cd[q] & SELF) && d > (C)0) ? ld<C>(&bv.v[q]) / d : (C)0);
             st(&x1.v[q], (C)0);
         }
         st8(L.x + p0, x0);
@@ -356,6 +384,7 @@ __device__ __forceinline__ void residual_v8_body(Lev<typename Pr::M> L) {
     using C = typename Pr::C;
     using M = typename Pr::M;
     const int sy = L.n1, sz = L.n1 * L.n2;
+    const bool edge = *L.edge != 0;
     FOR_TILES_W(L, tile) {
         Lane8 a;
         if (!lane8_of(L, tile, a)) continue;
@@ -374,7 +403,7 @@ __device__ __forceinline__ void residual_v8_body(Lev<typename Pr::M> L) {
                 if (cd[q] & SELF) {
                     C n6[6];
                     nb6_of(n6, nb, q, ci);
-                    v = ld<C>(&bv.v[q]) - (ld<C>(&dv.v[q]) * ld<C>(&xv.v[q]) - sum6<C>(n6, cd[q]));
+                    v = ld<C>(&bv.v[q]) - (ld<C>(&dv.v[q]) * ld<C>(&xv.v[q]) - nsum6<C>(n6, cd[q], edge));
                 }
                 st(&out.v[q], v);
             }
@@ -438,6 +467,7 @@ __global__ void __launch_bounds__(TPB)
     const C beta = (C)sc->s.beta;
     const bool first = sc->s.beta == 0.0;
     const int sy = L.n1, sz = L.n1 * L.n2;
+    const bool edge = *L.edge != 0;
     double acc[1] = {0.0};
     FOR_TILES_W(L, tile) {
         Lane8 a;
@@ -466,10 +496,12 @@ __global__ void __launch_bounds__(TPB)
                     nb6_of(z6, zn, q, ci);
                     if (!first) nb6_of(d6, dn, q, ci);
                     const C pc = first ? ld<C>(&zc.v[q]) : ld<C>(&zc.v[q]) + beta * (C)dc.v[q];
-                    C s = (C)0;
+                    C s = (C)0;  // nsum6 over p = z + beta d, formed term by term
 #pragma unroll
-                    for (int m = 0; m < 6; m++)
-                        if (cd[q] & (1u << m)) s += first ? z6[m] : z6[m] + beta * d6[m];
+                    for (int m = 0; m < 6; m++) {
+                        const C pm = first ? z6[m] : z6[m] + beta * d6[m];
+                        if (!edge || (cd[q] & (1u << m))) s += pm;
+                    }
                     qv = (C)gv.v[q] * pc - s;
                     acc[0] += (double)pc * (double)qv;
                 }
@@ -629,6 +661,7 @@ template <class Pr>
 __device__ __forceinline__ void residual_body(Lev<typename Pr::M> L) {
     using C = typename Pr::C;
     const int sy = L.n1, sz = L.n1 * L.n2;
+    const bool edge = *L.edge != 0;
     FOR_TILES_PF(L, tile) {
         Col c;
         if (!col_of(L, tile, c)) continue;
@@ -650,7 +683,7 @@ __device__ __forceinline__ void residual_body(Lev<typename Pr::M> L) {
 #pragma unroll
             for (int cc = 0; cc < 2; cc++) {
                 C v = (C)0;
-                if (cd[cc] & SELF) v = bv[cc] - (dv[cc] * xv[cc] - sum6<C>(nb[cc], cd[cc]));
+                if (cd[cc] & SELF) v = bv[cc] - (dv[cc] * xv[cc] - nsum6<C>(nb[cc], cd[cc], edge));
                 st(L.r + rb + cc * L.H + c.h, v);
             }
         }

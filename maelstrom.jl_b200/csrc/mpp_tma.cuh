@@ -156,8 +156,10 @@ __global__ void __launch_bounds__(TPB) k_rbgs_tma(Lev<typename Pr::M> L, int col
             if (cd & 8) s2 += X(lk + 1, lj, xi);
             if (cd & 16) s2 += X(lk + 2, lj + 1, xi);
             if (cd & 32) s2 += X(lk, lj + 1, xi);
-            const C d = ld<C>(dd + own);
-            const C v = d > (C)0 ? (ld<C>(bb + own) + s2) / d : (C)0;
+            const C d = ld<C>(dd + own);  // the 16-bit forms' map holds the reciprocal
+            C v;
+            if constexpr (Pr::scaled) v = (ld<C>(bb + own) + s2) * d;
+            else v = d > (C)0 ? (ld<C>(bb + own) + s2) / d : (C)0;
             st(L.x + (k * L.n2 + j) * L.n1 + colour * H + h, v);
         }
         __syncthreads();  // stage s fully read

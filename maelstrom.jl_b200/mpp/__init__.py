@@ -255,17 +255,18 @@ class Projector:
     def autotune(self, u, v, w, types, phi, stream=None) -> dict:
         """``mpp_autotune`` on this basin's own solve: keeps the fastest smoother forms and
         sweep counts on the context; returns {"chosen": {...}, "table": [...]}."""
-        n = 96
+        n = 128
         table = (_lib.TuneEntry * n)()
         chosen = ctypes.c_int(-1)
         k = check(self.lib.mpp_autotune(self._ctx, _ptr(u), _ptr(v), _ptr(w), _ptr(types), _ptr(phi), table, n,
                                         ctypes.byref(chosen), _stream_ptr(stream)))
         rows = [dict(smoother=_lib.SMOOTHERS[t.smoother], coarse_smoother=_lib.SMOOTHERS[t.coarse_smoother],
-                     sweeps=t.sweeps, coarse_sweeps=t.coarse_sweeps, iterations=t.iterations, status=t.status,
+                     sweeps=t.sweeps, sweeps_coarse=t.sweeps_coarse, coarse_sweeps=t.coarse_sweeps, iterations=t.iterations, status=t.status,
                      ms=round(t.ms, 4)) for t in table[:k]]
         best = rows[chosen.value] if chosen.value >= 0 else None
         if best:
-            self.opts.sweeps, self.opts.coarse = best["sweeps"], best["coarse_sweeps"]
+            self.opts.sweeps, self.opts.sweeps_coarse = best["sweeps"], best["sweeps_coarse"]
+            self.opts.coarse = best["coarse_sweeps"]
         return {"chosen": best, "table": rows}
 
     # ---- per-kernel timing ----

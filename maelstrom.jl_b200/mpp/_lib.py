@@ -25,7 +25,7 @@ class Opts(ctypes.Structure):
     _fields_ = [("tol", ctypes.c_float), ("maxiter", ctypes.c_int32), ("sweeps", ctypes.c_int32),
                 ("coarse", ctypes.c_int32), ("precision", ctypes.c_int32), ("graph", ctypes.c_int32),
                 ("fallback", ctypes.c_int32), ("restart", ctypes.c_int32), ("fallback_maxiter", ctypes.c_int32),
-                ("cg_maxiter_with_fallback", ctypes.c_int32)]
+                ("cg_maxiter_with_fallback", ctypes.c_int32), ("sweeps_coarse", ctypes.c_int32)]
 
 
 class Result(ctypes.Structure):
@@ -54,8 +54,8 @@ class BasinArrays(ctypes.Structure):
 
 class TuneEntry(ctypes.Structure):
     _fields_ = [("smoother", ctypes.c_int32), ("coarse_smoother", ctypes.c_int32), ("sweeps", ctypes.c_int32),
-                ("coarse_sweeps", ctypes.c_int32), ("iterations", ctypes.c_int32), ("status", ctypes.c_int32),
-                ("ms", ctypes.c_float)]
+                ("sweeps_coarse", ctypes.c_int32), ("coarse_sweeps", ctypes.c_int32), ("iterations", ctypes.c_int32),
+                ("status", ctypes.c_int32), ("ms", ctypes.c_float)]
 
 
 SMOOTHERS = {0: "vector", 1: "tma", 2: "column"}

@@ -128,32 +128,33 @@ class Batch:
         for dims, members in groups.items():
             i0 = members[0]
             a = self.arrays[i0]
-            table = (_lib.TuneEntry * 96)()
+            table = (_lib.TuneEntry * 128)()
             chosen = ctypes.c_int(-1)
             ptr = lambda k: ctypes.c_void_p(a[k].data_ptr())
             n = check(self.lib.mpp_autotune(self.ctx(i0), ptr("u"), ptr("v"), ptr("w"), ptr("types"), ptr("phi"),
-                                            table, 96, ctypes.byref(chosen), ctypes.c_void_p(s.cuda_stream)))
+                                            table, 128, ctypes.byref(chosen), ctypes.c_void_p(s.cuda_stream)))
             rows = [dict(smoother=_lib.SMOOTHERS[t.smoother], coarse_smoother=_lib.SMOOTHERS[t.coarse_smoother],
-                         sweeps=t.sweeps, coarse_sweeps=t.coarse_sweeps, iterations=t.iterations, status=t.status,
+                         sweeps=t.sweeps, sweeps_coarse=t.sweeps_coarse, coarse_sweeps=t.coarse_sweeps, iterations=t.iterations, status=t.status,
                          ms=t.ms) for t in table[:n]]
             if chosen.value >= 0:
                 win = table[chosen.value]
                 for j in members[1:]:
                     c = self.ctx(j)
-                    self._set_sweeps(c, win.sweeps, win.coarse_sweeps)
+                    self._set_sweeps(c, win.sweeps, win.sweeps_coarse, win.coarse_sweeps)
                     check(self.lib.mpp_ctx_set_smoothers(c, win.smoother, win.coarse_smoother))
                 report[dims] = dict(chosen=(_lib.SMOOTHERS[win.smoother], _lib.SMOOTHERS[win.coarse_smoother],
-                                            win.sweeps, win.coarse_sweeps), table=rows)
+                                            win.sweeps, win.sweeps_coarse, win.coarse_sweeps), table=rows)
             else:
                 report[dims] = dict(chosen=None, table=rows)
         self._structs = None
         return report
 
-    def _set_sweeps(self, c, sweeps, coarse):
+    def _set_sweeps(self, c, sweeps, sweeps_coarse, coarse):
         # the batch's options are the ones it was created with; only the sweeps change
         o = _lib.Opts()
         self.lib.mpp_opts_default(ctypes.byref(o))
         k = self._opts
         o.tol, o.maxiter, o.sweeps, o.coarse = k["tol"], k["maxiter"], sweeps, coarse
+        o.sweeps_coarse = sweeps_coarse
         o.precision, o.graph, o.fallback = k["precision"], 1, k["fallback"]
         check(self.lib.mpp_ctx_set_opts(c, ctypes.byref(o)))

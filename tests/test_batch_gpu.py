@@ -76,9 +76,10 @@ def test_autotune(cuda):
     assert set(report) == {(64, 64, 64), (32, 32, 32)}
     for dims, rep in report.items():
         assert rep["chosen"] is not None
-        assert len(rep["table"]) >= 6  # vector and column forms x 3 sweep counts at least
+        assert len(rep["table"]) >= 20  # the forms, then fine x coarse-level sweeps
         best = min((r for r in rep["table"] if r["status"] == 0), key=lambda r: r["ms"])
-        assert rep["chosen"] == (best["smoother"], best["coarse_smoother"], best["sweeps"], best["coarse_sweeps"])
+        assert rep["chosen"] == (best["smoother"], best["coarse_smoother"], best["sweeps"], best["sweeps_coarse"],
+                                 best["coarse_sweeps"])
     res = batch.project(1 / 48)
     assert all(r.status == 0 for r in res)
 
