@@ -272,7 +272,9 @@ __global__ void __launch_bounds__(TPB) k_level(const uint8_t* __restrict__ tf, i
     pdl_wait();
     pdl_trigger();
     const int n1 = L.n1, n2 = L.n2, n3 = L.n3;
-    FOR_CELLS(n1, n2, n3, I, J, K, idx) {
+    const int N = n1 * n2 * n3;  // coarse levels: short rows, so one flat 32-bit index
+    for (int idx = (int)(blockIdx.x * TPB + threadIdx.x); idx < N; idx += (int)(gridDim.x * TPB)) {
+        const int I = idx % n1, JK = idx / n1, J = JK % n2, K = JK / n2;
         const uint8_t t = coarsen_at(tf, f1, f2, f3, I, J, K);
         L.types[idx] = t;
         uint8_t code = 0;

@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(TPB)
     FOR_TILES_W(L, tile) {
         Lane8 a;
         if (!lane8_of(L, tile, a)) continue;
-#pragma unroll
+#pragma unroll 1  // one colour at a time: half the live registers
         for (int cc = 0; cc < 2; cc++) {
             const int p = a.rb + cc * L.H + a.h, o = a.rb + (1 - cc) * L.H + a.h;
             const int ci = ci_of(cc, a.j, a.k);
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(TPB)
 // advance_kernel! (src/flip.jl:1059-1073), vector form. The lane's 16 cells (both colours)
 // are 16 consecutive cells of the natural row, so P moves as one 16-element run.
 template <class Pr>
-__global__ void __launch_bounds__(TPB)
+__global__ void __launch_bounds__(TPB, 3)
     k_advance_v8(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ qv,
                  typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
                  unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {

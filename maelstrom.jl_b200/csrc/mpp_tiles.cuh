@@ -97,9 +97,9 @@ __device__ __forceinline__ C wB(int a) {
 // One block per coarse tile: the tile's fine region (RX x RY x RZ cells) is staged in
 // shared memory, non-LIQUID cells as zero, then each thread sums its two coarse cells.
 // The region is staged as the fine level stores it: per fine row (j, k) and colour, the
-// R_W row-split columns from 2 TH th - 1 on, one warp per row, so the loads are contiguous
-// runs and carry no per-element index arithmetic. In those terms fine cell (2I-1+a, 2J-1+b,
-// 2K-1+c) of coarse cell (I, J, K) has colour (a+b+c) & 1 and column I - 2 TH th + {0,1,1,2}[a].
+// R_W row-split columns from 2 TH th - 1 on, so a warp's loads are contiguous runs. In
+// those terms fine cell (2I-1+a, 2J-1+b, 2K-1+c) of coarse cell (I, J, K) has colour
+// (a+b+c) & 1 and column I - 2 TH th + {0,1,1,2}[a].
 constexpr int RX = 4 * TH + 2, RY = 2 * TY + 2, RZ = 2 * TZ + 2;
 constexpr int R_W = 2 * TH + 2, R_ROWS = 2 * RY * RZ;  // staged columns per row, rows (x2 colours)
 
@@ -121,10 +121,8 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
     using C = typename Pr::C;
     extern __shared__ __align__(128) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
-    constexpr int WPB = TPB / 32, RPW = (R_ROWS + WPB - 1) / WPB, NS = (R_W + 31) / 32;
     const int n = *L.count;
     const int lh = slot_h(), lj = slot_j(), lk = slot_k();
-    const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31;
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
         const uint32_t tile = L.tiles[t];
         const int th = (int)(tile & 1023u), tj = (int)((tile >> 10) & 1023u), tk = (int)(tile >> 20);
@@ -133,27 +131,24 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
         // Every non-LIQUID cell's r is zero (the residual pass writes zeros in active tiles
         // and the set-up clears the array each projection), so r is staged unmasked: all of
         // a thread's loads go out at once, then land in shared memory.
-        C vals[RPW][NS];
+        // in batches of RB loads a thread, so few registers hold them and more blocks fit
+        constexpr int NE = R_ROWS * R_W, PER = (NE + TPB - 1) / TPB, RB = 8;
 #pragma unroll
-        for (int u = 0; u < RPW; u++) {
-            const int r = warp + u * WPB;
-            const int col = r & 1, jk = r >> 1, j = j0 + jk % RY, k = k0 + jk / RY;
-            const bool row = r < R_ROWS && j >= 0 && j < F.n2 && k >= 0 && k < F.n3;
-            const int base = row ? (k * F.n2 + j) * F.n1 + col * F.H : 0;
+        for (int u0 = 0; u0 < PER; u0 += RB) {
+            C vals[RB];
 #pragma unroll
-            for (int q = 0; q < NS; q++) {
-                const int off = lane + 32 * q, h = hbase + off;
-                vals[u][q] = (C)0;
-                if (row && off < R_W && h >= 0 && h < F.H) vals[u][q] = ld<C>(F.r + base + h);
+            for (int q = 0; q < RB; q++) {
+                const int e = (int)threadIdx.x + (u0 + q) * TPB;
+                const int r = e / R_W, off = e - r * R_W;  // staged row (jk, colour), column
+                const int col = r & 1, jk = r >> 1, j = j0 + jk % RY, k = k0 + jk / RY, h = hbase + off;
+                vals[q] = (C)0;
+                if (u0 + q < PER && e < NE && j >= 0 && j < F.n2 && k >= 0 && k < F.n3 && h >= 0 && h < F.H)
+                    vals[q] = ld<C>(F.r + (k * F.n2 + j) * F.n1 + col * F.H + h);
             }
-        }
 #pragma unroll
-        for (int u = 0; u < RPW; u++) {
-            const int r = warp + u * WPB;
-#pragma unroll
-            for (int q = 0; q < NS; q++) {
-                const int off = lane + 32 * q;
-                if (r < R_ROWS && off < R_W) sm[r * R_W + off] = vals[u][q];
+            for (int q = 0; q < RB; q++) {
+                const int e = (int)threadIdx.x + (u0 + q) * TPB;
+                if (u0 + q < PER && e < NE) sm[e] = vals[q];
             }
         }
         __syncthreads();
@@ -177,8 +172,10 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
         }
     }
 }
+// Shared memory of k_restrict (elements of C): the staged rows.
+__host__ __device__ constexpr int restrict_smem_elems(bool) { return R_ROWS * R_W; }
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_restrict(Lev<typename Pr::M> F, Lev<typename Pr::M> L) {
+__global__ void __launch_bounds__(TPB, 4) k_restrict(Lev<typename Pr::M> F, Lev<typename Pr::M> L) {
     pdl_wait();
     pdl_trigger();
     restrict_body<Pr>(F, L);
