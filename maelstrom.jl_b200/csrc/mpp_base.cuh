@@ -106,10 +106,26 @@ __global__ void __launch_bounds__(TPB) k_volume(Geo g, const float* __restrict__
     pdl_wait();
     pdl_trigger();
     double acc[1] = {0.0};
-    FOR_CELLS(g.n[0], g.n[1], g.n[2], i, j, k, idx) {
-        if (!issolidcell(g, i, j, k)) {
-            float x = 0.5f - phi[idx] / g.dx;
-            acc[0] += (double)(x > 1.f ? 1.f : (x < 0.f ? 0.f : x));
+    if (g.n[0] % 8 == 0 && (reinterpret_cast<uintptr_t>(phi) & 15) == 0) {  // 8 cells of a row a thread
+        const int nq = g.n[0] / 8, nch = nq * g.n[1] * g.n[2];
+        for (int ch = (int)(blockIdx.x * TPB + threadIdx.x); ch < nch; ch += (int)(gridDim.x * TPB)) {
+            const int q8 = ch % nq, rw = ch / nq, j = rw % g.n[1], k = rw / g.n[1], i0 = 8 * q8;
+            const float4* p4 = reinterpret_cast<const float4*>(phi + (int64_t)rw * g.n[0] + i0);
+            const float4 a = p4[0], b = p4[1];
+            const float ph[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int m = 0; m < 8; m++)
+                if (!issolidcell(g, i0 + m, j, k)) {
+                    float x = 0.5f - ph[m] / g.dx;
+                    acc[0] += (double)(x > 1.f ? 1.f : (x < 0.f ? 0.f : x));
+                }
+        }
+    } else {
+        FOR_CELLS(g.n[0], g.n[1], g.n[2], i, j, k, idx) {
+            if (!issolidcell(g, i, j, k)) {
+                float x = 0.5f - phi[idx] / g.dx;
+                acc[0] += (double)(x > 1.f ? 1.f : (x < 0.f ? 0.f : x));
+            }
         }
     }
     if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
@@ -140,6 +156,32 @@ struct SetupIn {
     int clear_P;   // clearair (src/flip.jl:1132-1135)
     int residual;  // 1: r = b - A P and the norms; 0: operator only
 };
+
+// pressure!'s opening (src/flip.jl:1086-1094), by the set-up's last block: |b|, |r| of the
+// warm start, the tolerance's target, and the loop's first test.
+template <class Pr>
+__device__ __forceinline__ void setup_finish(Scalars* sc, const double (&acc)[3], cudaGraphConditionalHandle cond,
+                                             int use_cond) {
+    State& s = sc->s;
+    s.bnorm = sq<Pr>(acc[0]);
+    s.target = rs<Pr>((double)sc->p.tol * s.bnorm);
+    s.rnorm = sq<Pr>(acc[1]);
+    s.nliq = acc[2];
+    s.rscale = next_rscale(s.rnorm, s.nliq);
+    s.it = 0;
+    s.rho = 0.0;
+    s.beta = 0.0;
+    s.alpha = 0.0;
+    s.status = ST_OK;
+    s.done = 0;
+    if (!finite_d(s.bnorm) || !finite_d(s.rnorm)) {
+        s.status = ST_NONFINITE;
+        s.done = 1;
+    } else if (s.bnorm == 0.0 || s.rnorm <= s.target) {
+        s.done = 1;  // pressure! returns 0 (src/flip.jl:1091-1094)
+    }
+    set_cond(cond, use_cond, !s.done);
+}
 
 // The fine level's set-up, one pass over every cell (natural order):
 //   diag_kernel! (src/flip.jl:824-836) -> diag (and the smoother's copy),
@@ -223,27 +265,186 @@ __global__ void __launch_bounds__(TPB)
         }
     }
     if (!a.residual) return;
-    if (grid_sum<3>(acc, partials, counter) && threadIdx.x == 0) {
-        State& s = sc->s;
-        s.bnorm = sq<Pr>(acc[0]);
-        s.target = rs<Pr>((double)sc->p.tol * s.bnorm);
-        s.rnorm = sq<Pr>(acc[1]);
-        s.nliq = acc[2];
-        s.rscale = next_rscale(s.rnorm, s.nliq);
-        s.it = 0;
-        s.rho = 0.0;
-        s.beta = 0.0;
-        s.alpha = 0.0;
-        s.status = ST_OK;
-        s.done = 0;
-        if (!finite_d(s.bnorm) || !finite_d(s.rnorm)) {
-            s.status = ST_NONFINITE;
-            s.done = 1;
-        } else if (s.bnorm == 0.0 || s.rnorm <= s.target) {
-            s.done = 1;  // pressure! returns 0 (src/flip.jl:1091-1094)
-        }
-        set_cond(cond, use_cond, !s.done);
+    if (grid_sum<3>(acc, partials, counter) && threadIdx.x == 0) setup_finish<Pr>(sc, acc, cond, use_cond);
+}
+
+// k_setup with 8 consecutive cells of a row per thread (rows a multiple of 8 long): the
+// classes, velocities and warm start come in as 8-wide row pieces, and the outputs leave
+// as 4-wide pieces of each colour's half of the row-split rows. Same arithmetic, in the
+// same order, as k_setup.
+template <class T>
+struct Row8 {
+    T v[8];
+};
+template <class T>
+__device__ __forceinline__ Row8<T> ld_row8(const T* p) {  // 8-element aligned
+    Row8<T> r;
+    constexpr int n = (int)(sizeof(T) * 8 / 16);
+    if constexpr (n == 0) {
+        *reinterpret_cast<uint2*>(r.v) = *reinterpret_cast<const uint2*>(p);
+    } else {
+#pragma unroll
+        for (int q = 0; q < n; q++) reinterpret_cast<uint4*>(r.v)[q] = reinterpret_cast<const uint4*>(p)[q];
     }
+    return r;
+}
+template <class T>
+__device__ __forceinline__ void st_quad(T* p, const T (&v)[4]) {  // 4-element aligned
+    if constexpr (sizeof(T) == 1) *reinterpret_cast<uint32_t*>(p) = *reinterpret_cast<const uint32_t*>(v);
+    else if constexpr (sizeof(T) == 2) *reinterpret_cast<uint2*>(p) = *reinterpret_cast<const uint2*>(v);
+    else if constexpr (sizeof(T) == 4) *reinterpret_cast<uint4*>(p) = *reinterpret_cast<const uint4*>(v);
+    else {
+        reinterpret_cast<uint4*>(p)[0] = reinterpret_cast<const uint4*>(v)[0];
+        reinterpret_cast<uint4*>(p)[1] = reinterpret_cast<const uint4*>(v)[1];
+    }
+}
+
+template <class Pr>
+__global__ void __launch_bounds__(TPB)
+    k_setup_v8(SetupIn<typename Pr::V> a, Lev<typename Pr::M> L, typename Pr::V* __restrict__ diag,
+               typename Pr::V* __restrict__ b, typename Pr::V* __restrict__ r, Scalars* sc, double* partials,
+               unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
+    pdl_wait();
+    pdl_trigger();
+    using V = typename Pr::V;
+    using M = typename Pr::M;
+    using C = typename Pr::C;
+    const int n1 = L.n1, n2 = L.n2, n3 = L.n3, nq = n1 / 8, sz = n1 * n2;
+    const C dx = (C)a.dx;
+    const C gamma = (C)(sc->p.project ? sc->s.gamma : sc->p.gamma);
+    const bool sep_dg = (void*)L.dg != (void*)diag;
+    const bool sep_b = (void*)L.b != (void*)r;
+    double acc[3] = {0.0, 0.0, 0.0};
+    const int nch = nq * n2 * n3;
+    for (int ch = (int)(blockIdx.x * TPB + threadIdx.x); ch < nch; ch += (int)(gridDim.x * TPB)) {
+        const int q8 = ch % nq, rw = ch / nq, j = rw % n2, k = rw / n2, i0 = 8 * q8;
+        const int row = rw * n1, idx0 = row + i0;
+        Row8<uint8_t> tc = ld_row8(a.types + idx0), tym, typ, tzm, tzp;
+#pragma unroll
+        for (int m = 0; m < 8; m++) tym.v[m] = typ.v[m] = tzm.v[m] = tzp.v[m] = SOLID;
+        if (j > 0) tym = ld_row8(a.types + idx0 - n1);
+        if (j + 1 < n2) typ = ld_row8(a.types + idx0 + n1);
+        if (k > 0) tzm = ld_row8(a.types + idx0 - sz);
+        if (k + 1 < n3) tzp = ld_row8(a.types + idx0 + sz);
+        const uint8_t txm = i0 > 0 ? a.types[idx0 - 1] : (uint8_t)SOLID;
+        const uint8_t txp = i0 + 8 < n1 ? a.types[idx0 + 8] : (uint8_t)SOLID;
+        bool any = false;
+#pragma unroll
+        for (int m = 0; m < 8; m++) any |= tc.v[m] == LIQUID;
+        uint8_t code[8];
+        C d[8], bv[8], rv[8];
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            code[m] = 0;
+            d[m] = bv[m] = rv[m] = (C)0;
+        }
+        if (any) {
+            // rhs inputs (aligned rows of v and w; u rows are n1 + 1 long: element loads)
+            Row8<float> vlo, vhi, wlo, whi;
+            float ur[9];
+            const bool rhs = !a.bnat64 && !a.bnat && a.u;
+            if (rhs) {
+                const int ub = (n1 + 1) * (j + n2 * k) + i0;
+#pragma unroll
+                for (int m = 0; m < 9; m++) ur[m] = a.u[ub + m];
+                vlo = ld_row8(a.v + (int64_t)n1 * (j + (n2 + 1) * k) + i0);
+                vhi = ld_row8(a.v + (int64_t)n1 * (j + 1 + (n2 + 1) * k) + i0);
+                wlo = ld_row8(a.w + idx0);
+                whi = ld_row8(a.w + idx0 + sz);
+            }
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                if (tc.v[m] != LIQUID) continue;
+                const int i = i0 + m, idx = idx0 + m;
+                const uint8_t tn[6] = {m < 7 ? tc.v[m < 7 ? m + 1 : 0] : txp, m > 0 ? tc.v[m > 0 ? m - 1 : 0] : txm,
+                                       typ.v[m], tym.v[m], tzp.v[m], tzm.v[m]};
+                const int off[6] = {1, -1, n1, -n1, sz, -sz};
+                C dd = (C)0;
+                uint8_t cd = 0;
+                const C phc = a.phi ? (C)a.phi[idx] : (C)0;
+#pragma unroll
+                for (int n = 0; n < 6; n++) {
+                    if (tn[n] == LIQUID) {
+                        cd |= (uint8_t)(1u << n);
+                        dd += (C)1;
+                    }
+                    if (tn[n] == AIR && a.phi) dd += (C)1 / theta<C>(phc, (C)a.phi[idx + off[n]]);
+                }
+                cd |= SELF;
+                code[m] = cd;
+                d[m] = dd;
+                C bb = (C)0;
+                if (a.bnat64) {
+                    bb = (C)a.bnat64[idx];
+                } else if (a.bnat) {
+                    bb = (C)a.bnat[idx];
+                } else if (rhs) {
+                    C div = (C)ur[m + 1] - (C)ur[m];
+                    div = div + (C)vhi.v[m];
+                    div = div - (C)vlo.v[m];
+                    div = div + (C)whi.v[m];
+                    div = div - (C)wlo.v[m];
+                    bb = (-dx) * div + (dx * dx) * gamma;
+                }
+                bv[m] = bb;
+                if (a.residual) {
+                    C s = (C)0;
+#pragma unroll
+                    for (int n = 0; n < 6; n++)
+                        if (cd & (1u << n)) s += (C)a.P[idx + off[n]];
+                    rv[m] = bb - (dd * (C)a.P[idx] - s);
+                }
+                L.tflag[L.tile_of(i, j, k)] = 1;
+                if (i == 0 || i == n1 - 1 || j == 0 || j == n2 - 1) atomicOr(L.edge, 1);
+                acc[2] += 1.0;
+            }
+        }
+        if (a.clear_P) {
+#pragma unroll
+            for (int m = 0; m < 8; m++)
+                if (tc.v[m] != LIQUID) a.P[idx0 + m] = (V)0;
+        }
+        // the two colours' halves: colour c holds the cells m = p, p + 2, p + 4, p + 6
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            const int p0 = (c + j + k + 1) & 1;
+            const int pos = row + c * L.H + i0 / 2;
+            uint8_t cq[4];
+            V dq[4], bq[4], rq[4];
+            M gq[4], iq[4], lq[4];
+#pragma unroll
+            for (int s2 = 0; s2 < 4; s2++) {
+                const int m = p0 + 2 * s2;  // p0 is 0 or 1: pick by select, not by index
+                const uint8_t cm = p0 ? code[(2 * s2 + 1) & 7] : code[2 * s2];
+                const C dm = p0 ? d[(2 * s2 + 1) & 7] : d[2 * s2];
+                const C bm = p0 ? bv[(2 * s2 + 1) & 7] : bv[2 * s2];
+                const C rm = p0 ? rv[(2 * s2 + 1) & 7] : rv[2 * s2];
+                (void)m;
+                cq[s2] = cm;
+                st(&dq[s2], dm);
+                st(&bq[s2], bm);
+                st(&rq[s2], rm);
+                st(&gq[s2], dm);
+                st(&iq[s2], dm > (C)0 ? (C)1 / dm : (C)0);
+                st(&lq[s2], rm);
+                if (a.residual && (cm & SELF)) {
+                    acc[0] += (double)bm * (double)bm;
+                    acc[1] += (double)rm * (double)rm;
+                }
+            }
+            st_quad(L.code + pos, cq);
+            st_quad(diag + pos, dq);
+            if (sep_dg) st_quad(L.dg + pos, gq);
+            if (L.di) st_quad(L.di + pos, iq);
+            st_quad(b + pos, bq);
+            if (a.residual) {
+                st_quad(r + pos, rq);
+                if (sep_b) st_quad(L.b + pos, lq);
+            }
+        }
+    }
+    if (!a.residual) return;
+    if (grid_sum<3>(acc, partials, counter) && threadIdx.x == 0) setup_finish<Pr>(sc, acc, cond, use_cond);
 }
 
 // coarsen_kernel! (src/flip.jl:880-889) for level l from level l-1, fused with the coarse
