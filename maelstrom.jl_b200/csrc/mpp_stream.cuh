@@ -251,8 +251,11 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
     const int hq = lane % V8_LANES_H, lj = (lane / V8_LANES_H) % TY, lk = lane / (V8_LANES_H * TY);
     const int n = *L.count;
     const bool edge = *L.edge != 0;
+    // the next tile's id is fetched one step ahead, off the critical path
+    uint32_t tile_next = blockIdx.x * wpb + warp < n ? L.tiles[blockIdx.x * wpb + warp] : 0u;
     for (int t = blockIdx.x * wpb + warp; t < n; t += gridDim.x * wpb) {
-        const uint32_t tile = L.tiles[t];
+        const uint32_t tile = tile_next;
+        tile_next = t + gridDim.x * wpb < n ? L.tiles[t + gridDim.x * wpb] : 0u;
         const int h = (int)(tile & 1023u) * TH + hq * V8, j = (int)((tile >> 10) & 1023u) * TY + lj,
                   k = (int)(tile >> 20) * TZ + lk;
         if (h >= L.H || j >= L.n2 || k >= L.n3) continue;
@@ -308,10 +311,13 @@ __device__ __forceinline__ bool lane8_of(const Lev<M>& L, uint32_t tile, Lane8& 
     a.rb = (a.k * L.n2 + a.j) * L.n1;
     return a.h < L.H && a.j < L.n2 && a.k < L.n3;
 }
+// (the next tile's id fetched one step ahead)
 #define FOR_TILES_W(L, tile)                                                                              \
-    for (int t_ = blockIdx.x * (TPB / 32) + (int)(threadIdx.x >> 5), n_ = *(L).count; t_ < n_;            \
-         t_ += gridDim.x * (TPB / 32))                                                                    \
-        if (const uint32_t tile = (L).tiles[t_]; true)
+    const int n_ = *(L).count, s_ = gridDim.x * (TPB / 32);                                               \
+    int t_ = blockIdx.x * (TPB / 32) + (int)(threadIdx.x >> 5);                                           \
+    uint32_t tile = t_ < n_ ? (L).tiles[t_] : 0u;                                                         \
+    for (uint32_t next_; t_ < n_; t_ += s_, tile = next_)                                                 \
+        if ((next_ = (t_ + s_ < n_ ? (L).tiles[t_ + s_] : 0u)), true)
 
 // The other colour's values around a lane's 8 cells: the same 8 columns of this row
 // (the +x/-x neighbours) with one element on each side, and of the rows at +-y, +-z.
