@@ -315,12 +315,16 @@ def run_mpp(args):
     key = f"{dom['name']}@{dom['level']}"
     traffic = ncu_traffic(key)
     # bytes per CG iteration (every kernel inside the loop) over the loop's time
-    loop = [e for e in prof if e["name"] in ("start", "rbgs", "residual", "restrict", "coarsest", "prolong", "dot",
-                                             "search", "advance")]
+    loop_names = ("start", "rbgs", "residual", "restrict", "bottom", "prolong", "dot", "search", "advance")
+    loop = [e for e in prof if e["name"] in loop_names]
     nit = max(1, 2 * rprof.iterations)
     it_bytes = sum(e["bytes"] for e in loop) / nit
     it_ms = sum(e["ms"] for e in loop) / nit
     total_prof_ms = sum(e["ms"] for e in prof)
+    # the graph's own per-iteration time: the timed projection less the once-per-projection
+    # passes (as profiled), over its iterations
+    fixed_ms = sum(e["ms"] for e in prof if e["name"] not in loop_names) / 2
+    graph_it_ms = max(1e-6, (ms / args.steps - fixed_ms) / max(1, its[-1]))
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -345,9 +349,16 @@ def run_mpp(args):
                      "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes,
                      "launch_ms": round(per_launch_ms, 5),
                      "share_of_profiled_time": round(dom["ms"] / total_prof_ms, 4)},
-        "iteration_roofline": {"bytes_per_iteration": it_bytes, "ms_per_iteration": round(it_ms, 4),
-                               "achieved": round(it_bytes / (it_ms / 1e3) / 1e9, 1), "peak": hbm,
-                               "frac": round(it_bytes / (it_ms / 1e3) / 1e9 / hbm, 4)},
+        "iteration_roofline": {"bytes_per_iteration": it_bytes,
+                               "profiled": {"ms_per_iteration": round(it_ms, 4),
+                                            "achieved": round(it_bytes / (it_ms / 1e3) / 1e9, 1),
+                                            "frac": round(it_bytes / (it_ms / 1e3) / 1e9 / hbm, 4),
+                                            "note": "each kernel timed alone with CUDA events, host loop"},
+                               "graph": {"ms_per_iteration": round(graph_it_ms, 4),
+                                         "achieved": round(it_bytes / (graph_it_ms / 1e3) / 1e9, 1),
+                                         "frac": round(it_bytes / (graph_it_ms / 1e3) / 1e9 / hbm, 4),
+                                         "note": "timed graph projection less the profiled once-per-projection passes"},
+                               "peak": hbm},
         "gpu_launches": launches,
         "clocks": clocks,
     }
