@@ -18,6 +18,7 @@
 #include "mpp_advect.cuh"
 #include "mpp_fgmres.cuh"
 #include "mpp_tma.cuh"
+#include "mpp_cmg.cuh"
 
 using namespace mpp;
 
@@ -72,10 +73,10 @@ struct LevelBuf {
 
 // Kernel families, for the profiler.
 enum { F_VOLUME, F_SETUP, F_LEVEL, F_TILES, F_START, F_RBGS, F_RESID, F_RESTRICT, F_BOTTOM, F_PROLONG, F_DOT,
-       F_SEARCH, F_ADVANCE, F_TRUE, F_GRADIENT, F_CONVERT, NFAM };
+       F_SEARCH, F_ADVANCE, F_TRUE, F_GRADIENT, F_CONVERT, F_CMG, NFAM };
 const char* const FAM_NAMES[NFAM] = {"volume",   "setup",    "coarsen", "tilelists", "start",         "rbgs",
                                      "residual", "restrict", "bottom",   "prolong",  "dot",           "search",
-                                     "advance",  "true_residual", "gradient", "convert"};
+                                     "advance",  "true_residual", "gradient", "convert", "cluster"};
 constexpr int NGRAPHS = 4;
 struct GraphEntry {
     cudaGraphExec_t exec;
@@ -133,6 +134,10 @@ struct mpp_ctx {
     BotArgs bot;
     size_t bot_smem, restrict_smem;
     void* botb;  // level lb's right-hand side (natural order, stencil precision)
+    // levels cmg_ls .. lb-1 resident in one cluster of cmg_cs CTAs (k_cmg), when cmg_ls > 0
+    int cmg_ls, cmg_cs;
+    size_t cmg_smem;
+    CmgSlab cmg_slab[CMG_MAXLEV];
     // TMA tensor maps of the row-split levels the smoother streams with cp.async.bulk.tensor
     TmaLev tma[MAXLEV];
     bool tma_ok[MAXLEV];
@@ -238,6 +243,27 @@ void launch(void (*kern)(KArgs...), dim3 grid, int block, size_t smem, cudaStrea
     cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
+// A launch of one thread-block cluster of `cs` CTAs (k_cmg), with programmatic dependent
+// launch like the others.
+template <typename... KArgs, typename... Args>
+void launch_cluster(void (*kern)(KArgs...), int cs, int block, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cs);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    at[1].id = cudaLaunchAttributeClusterDimension;
+    at[1].val.clusterDim.x = (unsigned)cs;
+    at[1].val.clusterDim.y = 1;
+    at[1].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 2;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 Geo geo_of(const mpp_grid& g) {
     Geo o;
     for (int a = 0; a < 3; a++) { o.lo[a] = g.lo[a]; o.n[a] = g.n[a]; }
@@ -297,6 +323,21 @@ void prof_size(const mpp_ctx* c, int fam, int level, double& bytes, int64_t& cel
         case F_TRUE: cells = act(level); bpc = 1 + 2 * v + p; break;
         case F_GRADIENT: cells = N; bpc = 1 + 4 + 4 + 24 + 3; break;
         case F_CONVERT: cells = N; bpc = 12; break;
+        case F_CMG: {  // levels cmg_ls .. lb-1 in shared memory: what crosses to global memory
+            cells = 0;
+            double b = 0;
+            for (int l = c->cmg_ls; l < c->lb; l++) {
+                const double n = (double)lcells(l);
+                cells += lcells(l);
+                // down: code, diagonal(s), b of level ls in; x and b of the others out (x of ls);
+                // up: code, diagonal(s), x, b in, x of ls out
+                const double dgs = (m == 2 ? 2 : 1) * m;
+                b += level == 0 ? n * (1 + dgs + (l == c->cmg_ls ? m : 0) + m + (l > c->cmg_ls ? m : 0))
+                                : n * (1 + dgs + 2 * m + (l == c->cmg_ls ? m : 0));
+            }
+            bpc = cells > 0 ? b / (double)cells : 0;
+            break;
+        }
         default: cells = 0; bpc = 0;
     }
     bytes = bpc * (double)cells;
@@ -450,7 +491,8 @@ struct Run {
         down0.erase(down0.begin());
         for (int q = 0; q < swf; q++) { up0.push_back(1); up0.push_back(0); }
         const int lb = c->lb;
-        for (int l = 0; l < lb; l++) {
+        const int ls = c->cmg_ls > 0 ? c->cmg_ls : lb;  // levels ls .. lb-1 in the cluster
+        for (int l = 0; l < ls; l++) {
             beg(F_START, l);
             if (vec(l)) launch(k_start_v8<Pr>, grid_w(l), TPB, 0, s, view<M>(c, l));
             else launch(k_start<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
@@ -469,7 +511,18 @@ struct Run {
         BotArgs ba = c->bot;
         ba.sweeps = sw;
         ba.coarse = c->opts.coarse;
-        {
+        CmgArgs<M> ca;
+        if (ls < lb) {
+            memset(&ca, 0, sizeof(ca));
+            ca.nl = lb - ls;
+            ca.sweeps = sw;
+            ca.botb = c->botb;
+            for (int l = ls; l <= lb; l++) ca.g[l - ls] = view<M>(c, l);
+            for (int l = ls; l < lb; l++) ca.s[l - ls] = c->cmg_slab[l - ls];
+            beg(F_CMG, 0);
+            launch_cluster(k_cmg<Pr, 0>, c->cmg_cs, CMG_THREADS, c->cmg_smem, s, ca);
+            end();
+        } else {
             const int64_t Nb = (int64_t)c->lv[lb].n[0] * c->lv[lb].n[1] * c->lv[lb].n[2];
             beg(F_RESTRICT, lb);
             launch(k_restrict_bottom<Pr>, grid_cells(c, Nb), TPB, 0, s, view<M>(c, lb - 1), view<M>(c, lb),
@@ -479,7 +532,12 @@ struct Run {
         beg(F_BOTTOM, lb);
         launch(k_bottom<Pr>, 1, 1024, c->bot_smem, s, (const typename Pr::C*)c->botb, (M*)c->lv[lb].x, ba);
         end();
-        for (int l = lb - 1; l >= 0; l--) {
+        if (ls < lb) {
+            beg(F_CMG, 1);
+            launch_cluster(k_cmg<Pr, 1>, c->cmg_cs, CMG_THREADS, c->cmg_smem, s, ca);
+            end();
+        }
+        for (int l = ls - 1; l >= 0; l--) {
             beg(F_PROLONG, l);
             if (vec(l))
                 launch(k_prolong_v8<Pr>, grid_w(l), TPB, 0, s, view<M>(c, l), view<M>(c, l + 1), l + 1 == lb ? 1 : 0);
@@ -1037,6 +1095,108 @@ bool encode_level(CUtensorMap* m, CUtensorMapDataType dt, void* base, size_t es,
 // Tensor maps for every row-split level whose rows are whole tiles (h extent a multiple of
 // 16, so every box start is 16-byte aligned) and whose j and k extents hold a halo box.
 // Levels without them, or with MPP_NO_TMA set in the environment, use k_rbgs.
+// The cluster-resident small levels: the lowest first level ls >= 1 of at most 32^3 cells
+// whose levels ls .. lb-1 fit, as z-slabs, in the shared memory of a cluster of 16 CTAs (8,
+// 4 or 2 when 16 does not divide their plane counts or does not run). In the environment
+// MPP_CMG=0 keeps the per-level launches, MPP_CMG_MAXCELLS sets the size bound and
+// MPP_CMG_CS the largest cluster.
+int build_cmg(mpp_ctx* c) {
+    c->cmg_ls = 0;
+    c->cmg_cs = 0;
+    c->cmg_smem = 0;
+    const char* env = getenv("MPP_CMG");
+    if ((env && !strcmp(env, "0")) || c->lb < 2) return MPP_OK;
+    // a level joins the cluster from this many cells down: 16 SMs run a pass over 32^3 cells
+    // in well under the latency of one launch over the whole GPU, over 64^3 cells they do not
+    int64_t maxcells = 32768;
+    if (const char* mc = getenv("MPP_CMG_MAXCELLS")) maxcells = atoll(mc);
+    int csmax = 16;
+    if (const char* cm = getenv("MPP_CMG_CS")) csmax = atoi(cm);
+    int optin = 0;
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
+    const size_t ms = msize(c->prec);
+    const bool half = ms == 2;
+    return dispatch(c->prec, [&](auto pr) -> int {
+        using Pr = decltype(pr);
+        cudaFuncAttributes fa0, fa1;
+        CK(cudaFuncGetAttributes(&fa0, k_cmg<Pr, 0>));
+        CK(cudaFuncGetAttributes(&fa1, k_cmg<Pr, 1>));
+        const size_t stat = fa0.sharedSizeBytes > fa1.sharedSizeBytes ? fa0.sharedSizeBytes : fa1.sharedSizeBytes;
+        for (int ls = 1; ls < c->lb; ls++) {
+            if (c->lb - ls > CMG_MAXLEV) continue;
+            if ((int64_t)c->lv[ls].n[0] * c->lv[ls].n[1] * c->lv[ls].n[2] > maxcells) continue;
+            for (int cs : {16, 8, 4, 2}) {
+                if (cs > csmax) continue;
+                bool ok = true;
+                size_t off = CMG_HEADER;  // the active-row counts
+                CmgSlab sl[CMG_MAXLEV];
+                auto take = [&](size_t bytes) {
+                    const unsigned o = (unsigned)off;
+                    off += (bytes + 15) / 16 * 16;
+                    return o;
+                };
+                for (int l = ls; l < c->lb && ok; l++) {
+                    const LevelBuf& b = c->lv[l];
+                    if (!b.split || b.n[0] % 2 || b.n[0] < 4 || b.n[2] % cs || b.n[1] > 65535) {
+                        ok = false;
+                        break;
+                    }
+                    CmgSlab& S = sl[l - ls];
+                    S.n1 = b.n[0];
+                    S.n2 = b.n[1];
+                    S.n3 = b.n[2];
+                    S.P = b.n[2] / cs;
+                    S.H = S.n1 / 2;
+                    auto magic = [](int d) { return d > 1 ? 0xFFFFFFFFu / (unsigned)d + 1u : 0u; };
+                    S.mH = magic(S.H);
+                    S.mN = magic(S.n1);
+                    S.mP = magic(S.P);
+                    const size_t n = (size_t)S.P * S.n1 * S.n2;
+                    if (n >= 65536) {  // items of a pass are counted in 16 bits
+                        ok = false;
+                        break;
+                    }
+                    S.ox = take(ms * n);
+                    S.ob = take(ms * n);
+                    S.orr = take(ms * n);
+                    S.ocode = take(n);
+                    S.odg = take(ms * n);
+                    S.odi = half ? take(ms * n) : 0;
+                    S.orows = take(sizeof(uint32_t) * (size_t)S.P * S.n2);
+                }
+                if (!ok || off + stat > (size_t)optin) continue;
+                for (auto kern : {k_cmg<Pr, 0>, k_cmg<Pr, 1>}) {  // the limit is the function's: the device's
+                    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)stat));
+                    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+                }
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3((unsigned)cs);
+                cfg.blockDim = dim3((unsigned)CMG_THREADS);
+                cfg.dynamicSmemBytes = off;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = (unsigned)cs;
+                at[0].val.clusterDim.y = 1;
+                at[0].val.clusterDim.z = 1;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                int nc = 0;
+                if (cudaOccupancyMaxActiveClusters(&nc, k_cmg<Pr, 0>, &cfg) != cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+                if (nc < 1) continue;
+                c->cmg_ls = ls;
+                c->cmg_cs = cs;
+                c->cmg_smem = off;
+                for (int l = ls; l < c->lb; l++) c->cmg_slab[l - ls] = sl[l - ls];
+                return MPP_OK;
+            }
+        }
+        return MPP_OK;
+    });
+}
+
 int build_tma(mpp_ctx* c) {
     const size_t ms = msize(c->prec);
     const CUtensorMapDataType dt = c->prec == MPP_PREC_FP64        ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
@@ -1209,11 +1369,16 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
     int e;
     // level geometry
     size_t tflag_total = 0;
-    // the first level small enough for the one-CTA bottom solve
+    // the first level small enough for the one-CTA bottom solve: 4096 cells, or 512 when the
+    // levels above it can run in a thread-block cluster (k_cmg takes a 16^3 level's passes in
+    // well under the time one CTA needs); MPP_BOTTOM_CELLS in the environment lowers the bound
+    const char* cmg_env = getenv("MPP_CMG");
+    int64_t botcells = (cmg_env && !strcmp(cmg_env, "0")) ? BOTTOM_CELLS : BOTTOM_CELLS / 8;
+    if (const char* bc = getenv("MPP_BOTTOM_CELLS")) botcells = std::min<int64_t>(BOTTOM_CELLS, atoll(bc));
     c->lb = c->L - 1;
     for (int l = 1; l < c->L; l++) {
         const int64_t Nl = (int64_t)(g->n[0] >> l) * (g->n[1] >> l) * (g->n[2] >> l);
-        if (Nl <= BOTTOM_CELLS) {
+        if (Nl <= botcells) {
             c->lb = l;
             break;
         }
@@ -1277,7 +1442,7 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
         memset(&ba, 0, sizeof(ba));
         ba.nl = c->L - c->lb;
         if (ba.nl > BOTTOM_MAXLEV) {
-            set_err("%d levels below %d cells; at most %d are supported", ba.nl, BOTTOM_CELLS, BOTTOM_MAXLEV);
+            set_err("%d levels below %lld cells; at most %d are supported", ba.nl, (long long)botcells, BOTTOM_MAXLEV);
             return fail(MPP_ERR_INVALID);
         }
         for (int q = 0; q < ba.nl; q++) {
@@ -1326,6 +1491,7 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
         c->lv[0].b = c->r;
     }
     if ((e = build_tma(c))) return fail(e);
+    if ((e = build_cmg(c))) return fail(e);
     if (c->prec == MPP_PREC_FP64 && (e = alloc(c, &c->Pd, sizeof(double) * N))) return fail(e);
     if ((e = alloc(c, (void**)&c->sc, sizeof(Scalars)))) return fail(e);
     if ((e = alloc(c, (void**)&c->partials, sizeof(double) * MAXK * (size_t)c->nsm * MAXBLOCKS_PER_SM))) return fail(e);
