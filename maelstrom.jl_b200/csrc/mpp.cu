@@ -467,7 +467,7 @@ struct Run {
                 launch(k_rbgs_tma<Pr>, g > 0 ? g : 1, TPB, TmaGeom<M>::SMEM, s, view<M>(c, l), col, c->tma[l],
                                                                            &c->sc->s.fault);
             } else if (form(l) != MPP_SMOOTHER_COLUMN && c->lv[l].H % V8 == 0) {
-                const int wpb = TPB / 32, cap = c->nsm * MAXBLOCKS_PER_SM;
+                const int wpb = TPB / 32, cap = c->nsm * RBGS_V8_BLOCKS;
                 int g = (c->lv[l].ntiles + wpb - 1) / wpb;
                 g = g < cap ? (g > 0 ? g : 1) : cap;
                 launch(k_rbgs_v8<Pr>, g, TPB, 0, s, view<M>(c, l), col);

@@ -241,8 +241,46 @@ __device__ __forceinline__ void st8(T* p, const Vec8<T>& r) {
 // rbgs_kernel! (src/flip.jl:870-877), vector form. Own colour: code (8 bytes), diagonal,
 // b and x (kept where the cell is not LIQUID); other colour: the same 8 columns of this
 // row (the +x/-x neighbours, plus one element on each side) and of the rows at -+y, -+z.
+// Software-pipelined: a warp issues the next tile's loads before this tile's arithmetic
+// (tile ids two ahead), so its loads stay in flight while it computes; two blocks of 256
+// per SM hold both tiles' registers, and the grid is exactly that many blocks. The 4- and
+// 8-byte forms (twice the registers a tile) take one tile at a time.
+template <class M>
+struct RbLd {
+    uint2 cdw;
+    Vec8<M> dv, bv, xo, xc, yp, ym, zp, zm;
+    M xl, xr;
+    int p, ci;
+    bool ok;
+};
 template <class Pr>
-__device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) {
+__device__ __forceinline__ void rbgs_fetch(const Lev<typename Pr::M>& L, int colour, uint32_t tile, int hq, int lj,
+                                           int lk, RbLd<typename Pr::M>& a) {
+    const int sy = L.n1, sz = L.n1 * L.n2;
+    const int own = colour * L.H, oth = (1 - colour) * L.H;
+    const int h = (int)(tile & 1023u) * TH + hq * V8, j = (int)((tile >> 10) & 1023u) * TY + lj,
+              k = (int)(tile >> 20) * TZ + lk;
+    a.ok = h < L.H && j < L.n2 && k < L.n3;
+    if (!a.ok) return;
+    const int rb = (k * L.n2 + j) * L.n1;
+    const int p = rb + own + h, o = rb + oth + h;
+    a.p = p;
+    a.ci = ci_of(colour, j, k);
+    a.cdw = *reinterpret_cast<const uint2*>(L.code + p);
+    a.dv = ld8((Pr::scaled ? L.di : L.dg) + p);
+    a.bv = ld8(L.b + p);
+    a.xo = ld8(L.x + p);
+    a.xc = ld8(L.x + o);
+    a.yp = ld8(L.x + o + sy);
+    a.ym = ld8(L.x + o - sy);
+    a.zp = ld8(L.x + o + sz);
+    a.zm = ld8(L.x + o - sz);
+    a.xl = L.x[o - 1];
+    a.xr = L.x[o + V8];
+}
+// The 4- and 8-byte forms: one tile at a time.
+template <class Pr>
+__device__ __forceinline__ void rbgs_v8_single(Lev<typename Pr::M> L, int colour) {
     using C = typename Pr::C;
     using M = typename Pr::M;
     const int sy = L.n1, sz = L.n1 * L.n2;
@@ -291,11 +329,69 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
         st8(L.x + p, out);
     }
 }
+
+template <class C, class M>
+__device__ __forceinline__ Vec8<M> rbgs_tile(const RbLd<M>& cur, bool edge, bool scaled) {
+    Vec8<M> out;
+#pragma unroll
+    for (int q = 0; q < V8; q++) {
+        // constant element indices only (selects), so the tile stays in registers
+        const uint8_t cd = (uint8_t)(((q < 4 ? cur.cdw.x : cur.cdw.y) >> (8 * (q & 3))) & 0xffu);
+        const M xp = cur.ci ? (q + 1 < V8 ? cur.xc.v[q + 1 < V8 ? q + 1 : 0] : cur.xr) : cur.xc.v[q];
+        const M xm = cur.ci ? cur.xc.v[q] : (q > 0 ? cur.xc.v[q > 0 ? q - 1 : 0] : cur.xl);
+        C nb[6];
+        nb[0] = ld<C>(&xp);
+        nb[1] = ld<C>(&xm);
+        nb[2] = ld<C>(&cur.yp.v[q]);
+        nb[3] = ld<C>(&cur.ym.v[q]);
+        nb[4] = ld<C>(&cur.zp.v[q]);
+        nb[5] = ld<C>(&cur.zm.v[q]);
+        const C d = ld<C>(&cur.dv.v[q]);
+        out.v[q] = cur.xo.v[q];
+        if (cd & SELF) {
+            const C s = nsum6<C>(nb, cd, edge);
+            // the 16-bit forms multiply by the stored reciprocal (0 where the diagonal is)
+            if (scaled) st(&out.v[q], (ld<C>(&cur.bv.v[q]) + s) * d);
+            else st(&out.v[q], d > (C)0 ? (ld<C>(&cur.bv.v[q]) + s) / d : (C)0);
+        }
+    }
+    return out;
+}
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_rbgs_v8(Lev<typename Pr::M> L, int colour) {
+__device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) {
+    using C = typename Pr::C;
+    using M = typename Pr::M;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = TPB / 32;
+    const int hq = lane % V8_LANES_H, lj = (lane / V8_LANES_H) % TY, lk = lane / (V8_LANES_H * TY);
+    const int n = *L.count;
+    const bool edge = *L.edge != 0;
+    const int stride = gridDim.x * wpb;
+    int t = blockIdx.x * wpb + warp;
+    if (t >= n) return;
+    uint32_t tile1 = t + stride < n ? L.tiles[t + stride] : 0u;
+    RbLd<M> cur;
+    rbgs_fetch<Pr>(L, colour, L.tiles[t], hq, lj, lk, cur);
+    for (; t < n; t += stride) {
+        // the next tile's loads first (a tile's own-colour cells are no other tile's, and
+        // the other colour is only read, so they may pass this tile's stores)
+        RbLd<M> nxt;
+        nxt.ok = false;
+        const uint32_t tile2 = t + 2 * stride < n ? L.tiles[t + 2 * stride] : 0u;
+        if (t + stride < n) rbgs_fetch<Pr>(L, colour, tile1, hq, lj, lk, nxt);
+        tile1 = tile2;
+        if (cur.ok) st8(L.x + cur.p, rbgs_tile<C, M>(cur, edge, Pr::scaled));
+        cur = nxt;
+    }
+}
+// blocks per SM of k_rbgs_v8, and its grid: exactly the blocks that are resident at once
+// (two of 256 threads at up to 128 registers a thread)
+constexpr int RBGS_V8_BLOCKS = 2;
+template <class Pr>
+__global__ void __launch_bounds__(TPB, RBGS_V8_BLOCKS) k_rbgs_v8(Lev<typename Pr::M> L, int colour) {
     pdl_wait();
     pdl_trigger();
-    rbgs_v8_body<Pr>(L, colour);
+    if constexpr (sizeof(typename Pr::M) <= 2) rbgs_v8_body<Pr>(L, colour);
+    else rbgs_v8_single<Pr>(L, colour);
 }
 
 // A lane's 8 columns in a tile (vector kernels): h .. h+7 of row j, plane k.
