@@ -238,9 +238,10 @@ __device__ __forceinline__ void st8(T* p, const Vec8<T>& r) {
     for (int q = 0; q < n; q++) reinterpret_cast<uint4*>(p)[q] = reinterpret_cast<const uint4*>(r.v)[q];
 }
 
-// rbgs_kernel! (src/flip.jl:870-877), vector form. Own colour: code (8 bytes), diagonal,
-// b and x (kept where the cell is not LIQUID); other colour: the same 8 columns of this
-// row (the +x/-x neighbours, plus one element on each side) and of the rows at -+y, -+z.
+// rbgs_kernel! (src/flip.jl:870-877), vector form. Own colour: code (8 bytes), diagonal
+// and b in, x out (zero where the cell is not LIQUID, which is what every such cell holds,
+// so its old value need not be read); other colour: the same 8 columns of this row (the
+// +x/-x neighbours, plus one element on each side) and of the rows at -+y, -+z.
 // Software-pipelined: a warp issues the next tile's loads before this tile's arithmetic
 // (tile ids two ahead), so its loads stay in flight while it computes; two blocks of 256
 // per SM hold both tiles' registers, and the grid is exactly that many blocks. The 4- and
@@ -248,7 +249,7 @@ __device__ __forceinline__ void st8(T* p, const Vec8<T>& r) {
 template <class M>
 struct RbLd {
     uint2 cdw;
-    Vec8<M> dv, bv, xo, xc, yp, ym, zp, zm;
+    Vec8<M> dv, bv, xc, yp, ym, zp, zm;
     M xl, xr;
     int p, ci;
     bool ok;
@@ -269,7 +270,6 @@ __device__ __forceinline__ void rbgs_fetch(const Lev<typename Pr::M>& L, int col
     a.cdw = *reinterpret_cast<const uint2*>(L.code + p);
     a.dv = ld8((Pr::scaled ? L.di : L.dg) + p);
     a.bv = ld8(L.b + p);
-    a.xo = ld8(L.x + p);
     a.xc = ld8(L.x + o);
     a.yp = ld8(L.x + o + sy);
     a.ym = ld8(L.x + o - sy);
@@ -301,7 +301,7 @@ __device__ __forceinline__ void rbgs_v8_single(Lev<typename Pr::M> L, int colour
         const int p = rb + own + h, o = rb + oth + h;
         const int ci = ci_of(colour, j, k);
         const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
-        const Vec8<M> dv = ld8((Pr::scaled ? L.di : L.dg) + p), bv = ld8(L.b + p), xo = ld8(L.x + p);
+        const Vec8<M> dv = ld8((Pr::scaled ? L.di : L.dg) + p), bv = ld8(L.b + p);
         const Vec8<M> xc = ld8(L.x + o), yp = ld8(L.x + o + sy), ym = ld8(L.x + o - sy), zp = ld8(L.x + o + sz),
                       zm = ld8(L.x + o - sz);
         const M xl = L.x[o - 1], xr = L.x[o + V8];
@@ -318,7 +318,7 @@ __device__ __forceinline__ void rbgs_v8_single(Lev<typename Pr::M> L, int colour
             nb[4] = ld<C>(&zp.v[q]);
             nb[5] = ld<C>(&zm.v[q]);
             const C d = ld<C>(&dv.v[q]);
-            out.v[q] = xo.v[q];
+            st(&out.v[q], (C)0);
             if (cd[q] & SELF) {
                 const C s = nsum6<C>(nb, cd[q], edge);
                 // the 16-bit forms multiply by the stored reciprocal (0 where the diagonal is)
@@ -347,7 +347,7 @@ __device__ __forceinline__ Vec8<M> rbgs_tile(const RbLd<M>& cur, bool edge, bool
         nb[4] = ld<C>(&cur.zp.v[q]);
         nb[5] = ld<C>(&cur.zm.v[q]);
         const C d = ld<C>(&cur.dv.v[q]);
-        out.v[q] = cur.xo.v[q];
+        st(&out.v[q], (C)0);
         if (cd & SELF) {
             const C s = nsum6<C>(nb, cd, edge);
             // the 16-bit forms multiply by the stored reciprocal (0 where the diagonal is)

@@ -116,13 +116,24 @@ __host__ __device__ constexpr int roff(int t) {
     return (((t >> 4) * RY + ((t >> 2) & 3)) * 2 + (((t & 3) + ((t >> 2) & 3) + (t >> 4)) & 1)) * R_W + ((t & 3) + 1) / 2;
 }
 
+// 16 bytes of elements of type M.
+template <class M>
+union Vec16 {
+    uint4 u;
+    M m[16 / sizeof(M)];
+    __device__ Vec16() {}
+};
+
 template <class Pr>
 __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typename Pr::M> L) {
     using C = typename Pr::C;
     extern __shared__ __align__(128) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
+    using M = typename Pr::M;
     const int n = *L.count;
     const int lh = slot_h(), lj = slot_j(), lk = slot_k();
+    const bool vec = F.H % (16 / (int)sizeof(M)) == 0 && F.n1 % (16 / (int)sizeof(M)) == 0 &&
+                     (reinterpret_cast<uintptr_t>(F.r) & 15) == 0;
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
         const uint32_t tile = L.tiles[t];
         const int th = (int)(tile & 1023u), tj = (int)((tile >> 10) & 1023u), tk = (int)(tile >> 20);
@@ -131,6 +142,40 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
         // Every non-LIQUID cell's r is zero (the residual pass writes zeros in active tiles
         // and the set-up clears the array each projection), so r is staged unmasked: all of
         // a thread's loads go out at once, then land in shared memory.
+        if (vec) {
+            // 16-byte pieces: each staged row's columns from the aligned column below hbase,
+            // a piece wholly inside the row [0, H) or wholly outside it (read as zeros)
+            constexpr int CH = 16 / (int)sizeof(M), NCH = (R_W + 2 * CH - 2) / CH + 1;
+            constexpr int NV = R_ROWS * NCH, PERV = (NV + TPB - 1) / TPB;
+            const int h8 = hbase + 1 - CH;  // hbase + 1 = 2 TH th is a multiple of CH
+            constexpr int VB = 3;  // pieces a thread has in flight
+#pragma unroll 1
+            for (int u0 = 0; u0 < PERV; u0 += VB) {
+                Vec16<M> v[VB];
+                int rr[VB], hh[VB];
+#pragma unroll
+                for (int u = 0; u < VB; u++) {
+                    const int e = (int)threadIdx.x + (u0 + u) * TPB;
+                    const int r = e / NCH, ch = e - r * NCH;
+                    const int col = r & 1, jk = r >> 1, j = j0 + jk % RY, k = k0 + jk / RY, h = h8 + ch * CH;
+                    rr[u] = e < NV ? r : -1;
+                    hh[u] = h;
+                    v[u].u = make_uint4(0u, 0u, 0u, 0u);
+                    if (e < NV && j >= 0 && j < F.n2 && k >= 0 && k < F.n3 && h >= 0 && h < F.H)
+                        v[u].u = *reinterpret_cast<const uint4*>(F.r + (k * F.n2 + j) * F.n1 + col * F.H + h);
+                }
+#pragma unroll
+                for (int u = 0; u < VB; u++) {
+                    if (rr[u] < 0) continue;
+#pragma unroll
+                    for (int q = 0; q < CH; q++) {
+                        const int off = hh[u] + q - hbase;
+                        if (off >= 0 && off < R_W) sm[rr[u] * R_W + off] = ld<C>(&v[u].m[q]);
+                    }
+                }
+            }
+            __syncthreads();
+        } else {
         // in batches of RB loads a thread, so few registers hold them and more blocks fit
         constexpr int NE = R_ROWS * R_W, PER = (NE + TPB - 1) / TPB, RB = 8;
 #pragma unroll
@@ -152,6 +197,7 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
             }
         }
         __syncthreads();
+        }
         const int h = th * TH + lh, J = tj * TY + lj, K = tk * TZ + lk;
         if (h < L.H && J < L.n2 && K < L.n3) {
             const int rb = (K * L.n2 + J) * L.n1;
