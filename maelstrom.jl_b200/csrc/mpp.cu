@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "mpp.h"
@@ -381,6 +382,26 @@ struct Run {
     // vector (8 cells per lane) kernels on level l: rows of whole 8-element chunks
     int form(int l) const { return l == 0 ? c->form_fine : c->form_coarse; }
     bool vec(int l) const { return form(l) != MPP_SMOOTHER_COLUMN && c->lv[l].H % V8 == 0; }
+    // a pipelined vector kernel's grid: the blocks resident at once (no second wave), at
+    // most one warp per tile
+    int grid_res(const void* kern, int l) const {
+        static std::mutex mu;
+        static std::vector<std::pair<const void*, int>> occ;
+        int nb = 0;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            for (auto& e : occ)
+                if (e.first == kern) nb = e.second;
+            if (nb == 0) {
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, TPB, 0) != cudaSuccess || nb < 1) nb = 1;
+                if (nb > MAXBLOCKS_PER_SM) nb = MAXBLOCKS_PER_SM;  // the partial-sum buffer's bound
+                occ.emplace_back(kern, nb);
+            }
+        }
+        const int wpb = TPB / 32, cap = c->nsm * nb;
+        const int g = (c->lv[l].ntiles + wpb - 1) / wpb;
+        return g < cap ? (g > 0 ? g : 1) : cap;
+    }
     int grid_w(int l) const {
         const int wpb = TPB / 32, cap = c->nsm * MAXBLOCKS_PER_SM;
         const int g = (c->lv[l].ntiles + wpb - 1) / wpb;
@@ -555,7 +576,7 @@ struct Run {
         const bool v = vec(0);
         beg(F_DOT, 0);
         if (v)
-            launch(k_dot_v8<Pr>, grid_w(0), TPB, 0, s, view<M>(c, 0), (const V*)c->r, (const V*)c->q, c->sc, c->partials,
+            launch(k_dot_v8<Pr>, grid_res((const void*)k_dot_v8<Pr>, 0), TPB, 0, s, view<M>(c, 0), (const V*)c->r, (const V*)c->q, c->sc, c->partials,
                                                     cnt(CNT_DOT));
         else
             launch(k_dot<Pr>, grid_tiles(c, 0), TPB, 0, s, view<M>(c, 0), (const V*)c->r, (const V*)c->q, c->sc,

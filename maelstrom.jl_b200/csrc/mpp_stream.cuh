@@ -520,7 +520,39 @@ __global__ void __launch_bounds__(TPB) k_residual_v8(Lev<typename Pr::M> L) {
     residual_v8_body<Pr>(L);
 }
 
-// inner(s, z, r) and the flexible z.q (see k_dot), vector form.
+// Walk this warp's share of a level's tile list in units (tile, sub-unit < NU), the loads
+// of the next unit issued before the arithmetic of this one and its tile id fetched two
+// units ahead (the rbgs_v8 pipeline, for passes whose units do not overlap in what they
+// write): fetch(tile, sub, Ld&) issues a unit's loads, compute(const Ld&) consumes them.
+template <int NU, class Ld, class FetchF, class ComputeF>
+__device__ __forceinline__ void walk_tiles_pipelined(const uint32_t* tiles, int n, FetchF&& fetch, ComputeF&& compute) {
+    const int wpb = TPB / 32, warp = threadIdx.x >> 5;
+    const int stride = gridDim.x * wpb, total = n * NU;
+    int u = blockIdx.x * wpb + warp;
+    if (u >= total) return;
+    uint32_t tile1 = u + stride < total ? tiles[(u + stride) / NU] : 0u;
+    Ld cur;
+    fetch(tiles[u / NU], u % NU, cur);
+    for (; u < total; u += stride) {
+        Ld nxt;
+        const uint32_t tile2 = u + 2 * stride < total ? tiles[(u + 2 * stride) / NU] : 0u;
+        if (u + stride < total) fetch(tile1, (u + stride) % NU, nxt);
+        tile1 = tile2;
+        compute(cur);
+        cur = nxt;
+    }
+}
+
+// inner(s, z, r) and the flexible z.q (see k_dot), vector form: one colour of a tile a
+// unit, pipelined.
+template <class M, class V, bool FLEX>
+struct DotLd {
+    uint2 cdw;
+    Vec8<M> zv;
+    Vec8<V> rv;
+    Vec8<V> qq;  // (flexible form only)
+    bool ok;
+};
 template <class Pr>
 __global__ void __launch_bounds__(TPB)
     k_dot_v8(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ qv,
@@ -529,29 +561,33 @@ __global__ void __launch_bounds__(TPB)
     pdl_trigger();
     using M = typename Pr::M;
     using V = typename Pr::V;
+    using Ld = DotLd<M, V, Pr::flexible>;
     if (sc->s.done) return;
     double acc[2] = {0.0, 0.0};
-    FOR_TILES_W(L, tile) {
-        Lane8 a;
-        if (!lane8_of(L, tile, a)) continue;
+    walk_tiles_pipelined<2, Ld>(
+        L.tiles, *L.count,
+        [&](uint32_t tile, int cc, Ld& a) {
+            Lane8 l8;
+            a.ok = lane8_of(L, tile, l8);
+            if (!a.ok) return;
+            const int p = l8.rb + cc * L.H + l8.h;
+            a.cdw = *reinterpret_cast<const uint2*>(L.code + p);
+            a.zv = ld8(L.x + p);
+            a.rv = ld8(r + p);
+            if constexpr (Pr::flexible) a.qq = ld8(qv + p);
+        },
+        [&](const Ld& a) {
+            if (!a.ok) return;
 #pragma unroll
-        for (int cc = 0; cc < 2; cc++) {
-            const int p = a.rb + cc * L.H + a.h;
-            const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
-            const Vec8<M> zv = ld8(L.x + p);
-            const Vec8<V> rv = ld8(r + p);
-            Vec8<V> qq;
-            if constexpr (Pr::flexible) qq = ld8(qv + p);
-            const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
-#pragma unroll
-            for (int q = 0; q < V8; q++)
-                if (cd[q] & SELF) {
-                    const double z = ld<double>(&zv.v[q]);
-                    acc[0] += z * (double)rv.v[q];
-                    if constexpr (Pr::flexible) acc[1] += z * (double)qq.v[q];
+            for (int q = 0; q < V8; q++) {
+                const uint8_t cd = (uint8_t)(((q < 4 ? a.cdw.x : a.cdw.y) >> (8 * (q & 3))) & 0xffu);
+                if (cd & SELF) {
+                    const double z = ld<double>(&a.zv.v[q]);
+                    acc[0] += z * (double)a.rv.v[q];
+                    if constexpr (Pr::flexible) acc[1] += z * (double)a.qq.v[q];
                 }
-        }
-    }
+            }
+        });
     if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0) dot_finish<Pr>(sc, acc);
 }
 
