@@ -584,7 +584,7 @@ struct Run {
         end();
         beg(F_SEARCH, 0);
         if (v)
-            launch(k_search_v8<Pr>, grid_w(0), TPB, 0, s, view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q,
+            launch(k_search_v8<Pr>, grid_res((const void*)k_search_v8<Pr>, 0), TPB, 0, s, view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q,
                                                        c->sc, c->partials, cnt(CNT_SEARCH));
         else
             launch(k_search<Pr>, grid_tiles(c, 0), TPB, 0, s, view<M>(c, 0), (const V*)c->d, (const V*)c->diag, (V*)c->q,

@@ -244,8 +244,10 @@ __device__ __forceinline__ void st8(T* p, const Vec8<T>& r) {
 // +x/-x neighbours, plus one element on each side) and of the rows at -+y, -+z.
 // Software-pipelined: a warp issues the next tile's loads before this tile's arithmetic
 // (tile ids two ahead), so its loads stay in flight while it computes; two blocks of 256
-// per SM hold both tiles' registers, and the grid is exactly that many blocks. The 4- and
-// 8-byte forms (twice the registers a tile) take one tile at a time.
+// per SM hold both tiles' registers, and the grid is exactly that many blocks. Before its
+// programmatic-dependent-launch wait, a warp already loads its first tile's id, code,
+// diagonal and b: the preceding kernel (a colour pass, start or prolongation) writes only
+// x, and everything older is complete once that kernel has passed its own wait.
 template <class M>
 struct RbLd {
     uint2 cdw;
@@ -254,22 +256,28 @@ struct RbLd {
     int p, ci;
     bool ok;
 };
+// A tile's loads in two parts: what no pass of the smoother writes (the code, diagonal and
+// b of the own colour; issued before the kernel waits on its predecessor), then the other
+// colour's x.
 template <class Pr>
-__device__ __forceinline__ void rbgs_fetch(const Lev<typename Pr::M>& L, int colour, uint32_t tile, int hq, int lj,
-                                           int lk, RbLd<typename Pr::M>& a) {
-    const int sy = L.n1, sz = L.n1 * L.n2;
-    const int own = colour * L.H, oth = (1 - colour) * L.H;
+__device__ __forceinline__ void rbgs_fetch_s(const Lev<typename Pr::M>& L, int colour, uint32_t tile, int hq, int lj,
+                                             int lk, RbLd<typename Pr::M>& a) {
     const int h = (int)(tile & 1023u) * TH + hq * V8, j = (int)((tile >> 10) & 1023u) * TY + lj,
               k = (int)(tile >> 20) * TZ + lk;
     a.ok = h < L.H && j < L.n2 && k < L.n3;
     if (!a.ok) return;
-    const int rb = (k * L.n2 + j) * L.n1;
-    const int p = rb + own + h, o = rb + oth + h;
+    const int p = (k * L.n2 + j) * L.n1 + colour * L.H + h;
     a.p = p;
     a.ci = ci_of(colour, j, k);
     a.cdw = *reinterpret_cast<const uint2*>(L.code + p);
     a.dv = ld8((Pr::scaled ? L.di : L.dg) + p);
     a.bv = ld8(L.b + p);
+}
+template <class Pr>
+__device__ __forceinline__ void rbgs_fetch_x(const Lev<typename Pr::M>& L, int colour, RbLd<typename Pr::M>& a) {
+    if (!a.ok) return;
+    const int sy = L.n1, sz = L.n1 * L.n2;
+    const int o = a.p + (1 - 2 * colour) * L.H;  // the same columns in the other colour's half
     a.xc = ld8(L.x + o);
     a.yp = ld8(L.x + o + sy);
     a.ym = ld8(L.x + o - sy);
@@ -277,57 +285,6 @@ __device__ __forceinline__ void rbgs_fetch(const Lev<typename Pr::M>& L, int col
     a.zm = ld8(L.x + o - sz);
     a.xl = L.x[o - 1];
     a.xr = L.x[o + V8];
-}
-// The 4- and 8-byte forms: one tile at a time.
-template <class Pr>
-__device__ __forceinline__ void rbgs_v8_single(Lev<typename Pr::M> L, int colour) {
-    using C = typename Pr::C;
-    using M = typename Pr::M;
-    const int sy = L.n1, sz = L.n1 * L.n2;
-    const int own = colour * L.H, oth = (1 - colour) * L.H;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = TPB / 32;
-    const int hq = lane % V8_LANES_H, lj = (lane / V8_LANES_H) % TY, lk = lane / (V8_LANES_H * TY);
-    const int n = *L.count;
-    const bool edge = *L.edge != 0;
-    // the next tile's id is fetched one step ahead, off the critical path
-    uint32_t tile_next = blockIdx.x * wpb + warp < n ? L.tiles[blockIdx.x * wpb + warp] : 0u;
-    for (int t = blockIdx.x * wpb + warp; t < n; t += gridDim.x * wpb) {
-        const uint32_t tile = tile_next;
-        tile_next = t + gridDim.x * wpb < n ? L.tiles[t + gridDim.x * wpb] : 0u;
-        const int h = (int)(tile & 1023u) * TH + hq * V8, j = (int)((tile >> 10) & 1023u) * TY + lj,
-                  k = (int)(tile >> 20) * TZ + lk;
-        if (h >= L.H || j >= L.n2 || k >= L.n3) continue;
-        const int rb = (k * L.n2 + j) * L.n1;
-        const int p = rb + own + h, o = rb + oth + h;
-        const int ci = ci_of(colour, j, k);
-        const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
-        const Vec8<M> dv = ld8((Pr::scaled ? L.di : L.dg) + p), bv = ld8(L.b + p);
-        const Vec8<M> xc = ld8(L.x + o), yp = ld8(L.x + o + sy), ym = ld8(L.x + o - sy), zp = ld8(L.x + o + sz),
-                      zm = ld8(L.x + o - sz);
-        const M xl = L.x[o - 1], xr = L.x[o + V8];
-        const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
-        Vec8<M> out;
-#pragma unroll
-        for (int q = 0; q < V8; q++) {
-            const int ip = q + ci, im = q + ci - 1;  // this cell's +x and -x columns
-            C nb[6];
-            nb[0] = ld<C>(ip < V8 ? &xc.v[ip] : &xr);
-            nb[1] = ld<C>(im >= 0 ? &xc.v[im] : &xl);
-            nb[2] = ld<C>(&yp.v[q]);
-            nb[3] = ld<C>(&ym.v[q]);
-            nb[4] = ld<C>(&zp.v[q]);
-            nb[5] = ld<C>(&zm.v[q]);
-            const C d = ld<C>(&dv.v[q]);
-            st(&out.v[q], (C)0);
-            if (cd[q] & SELF) {
-                const C s = nsum6<C>(nb, cd[q], edge);
-                // the 16-bit forms multiply by the stored reciprocal (0 where the diagonal is)
-                if constexpr (Pr::scaled) st(&out.v[q], (ld<C>(&bv.v[q]) + s) * d);
-                else st(&out.v[q], d > (C)0 ? (ld<C>(&bv.v[q]) + s) / d : (C)0);
-            }
-        }
-        st8(L.x + p, out);
-    }
 }
 
 template <class C, class M>
@@ -357,30 +314,52 @@ __device__ __forceinline__ Vec8<M> rbgs_tile(const RbLd<M>& cur, bool edge, bool
     }
     return out;
 }
+// The kernel's body, PDL wait included: the first tile's static loads go out before it.
+// The 16-bit forms keep two tiles in flight; the 4- and 8-byte forms (twice the registers
+// a tile) one.
 template <class Pr>
 __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) {
     using C = typename Pr::C;
     using M = typename Pr::M;
+    constexpr bool PIPE = sizeof(M) <= 2;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = TPB / 32;
     const int hq = lane % V8_LANES_H, lj = (lane / V8_LANES_H) % TY, lk = lane / (V8_LANES_H * TY);
-    const int n = *L.count;
+    const int n = *L.count;  // tile lists and codes date from the set-up
     const bool edge = *L.edge != 0;
     const int stride = gridDim.x * wpb;
     int t = blockIdx.x * wpb + warp;
-    if (t >= n) return;
-    uint32_t tile1 = t + stride < n ? L.tiles[t + stride] : 0u;
     RbLd<M> cur;
-    rbgs_fetch<Pr>(L, colour, L.tiles[t], hq, lj, lk, cur);
+    uint32_t tile1 = 0u;
+    if (t < n) {
+        tile1 = t + stride < n ? L.tiles[t + stride] : 0u;
+        rbgs_fetch_s<Pr>(L, colour, L.tiles[t], hq, lj, lk, cur);
+    }
+    pdl_wait();
+    pdl_trigger();
+    if (t >= n) return;
+    rbgs_fetch_x<Pr>(L, colour, cur);
     for (; t < n; t += stride) {
-        // the next tile's loads first (a tile's own-colour cells are no other tile's, and
-        // the other colour is only read, so they may pass this tile's stores)
-        RbLd<M> nxt;
-        nxt.ok = false;
         const uint32_t tile2 = t + 2 * stride < n ? L.tiles[t + 2 * stride] : 0u;
-        if (t + stride < n) rbgs_fetch<Pr>(L, colour, tile1, hq, lj, lk, nxt);
+        if constexpr (PIPE) {
+            // the next tile's loads first (a tile's own-colour cells are no other tile's, and
+            // the other colour is only read, so they may pass this tile's stores)
+            RbLd<M> nxt;
+            nxt.ok = false;
+            if (t + stride < n) {
+                rbgs_fetch_s<Pr>(L, colour, tile1, hq, lj, lk, nxt);
+                rbgs_fetch_x<Pr>(L, colour, nxt);
+            }
+            if (cur.ok) st8(L.x + cur.p, rbgs_tile<C, M>(cur, edge, Pr::scaled));
+            cur = nxt;
+        } else {
+            if (cur.ok) st8(L.x + cur.p, rbgs_tile<C, M>(cur, edge, Pr::scaled));
+            cur.ok = false;
+            if (t + stride < n) {
+                rbgs_fetch_s<Pr>(L, colour, tile1, hq, lj, lk, cur);
+                rbgs_fetch_x<Pr>(L, colour, cur);
+            }
+        }
         tile1 = tile2;
-        if (cur.ok) st8(L.x + cur.p, rbgs_tile<C, M>(cur, edge, Pr::scaled));
-        cur = nxt;
     }
 }
 // blocks per SM of k_rbgs_v8, and its grid: exactly the blocks that are resident at once
@@ -388,10 +367,7 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
 constexpr int RBGS_V8_BLOCKS = 2;
 template <class Pr>
 __global__ void __launch_bounds__(TPB, RBGS_V8_BLOCKS) k_rbgs_v8(Lev<typename Pr::M> L, int colour) {
-    pdl_wait();
-    pdl_trigger();
-    if constexpr (sizeof(typename Pr::M) <= 2) rbgs_v8_body<Pr>(L, colour);
-    else rbgs_v8_single<Pr>(L, colour);
+    rbgs_v8_body<Pr>(L, colour);
 }
 
 // A lane's 8 columns in a tile (vector kernels): h .. h+7 of row j, plane k.
@@ -523,20 +499,31 @@ __global__ void __launch_bounds__(TPB) k_residual_v8(Lev<typename Pr::M> L) {
 // Walk this warp's share of a level's tile list in units (tile, sub-unit < NU), the loads
 // of the next unit issued before the arithmetic of this one and its tile id fetched two
 // units ahead (the rbgs_v8 pipeline, for passes whose units do not overlap in what they
-// write): fetch(tile, sub, Ld&) issues a unit's loads, compute(const Ld&) consumes them.
-template <int NU, class Ld, class FetchF, class ComputeF>
-__device__ __forceinline__ void walk_tiles_pipelined(const uint32_t* tiles, int n, FetchF&& fetch, ComputeF&& compute) {
+// write). fetch_s(tile, sub, Ld&) issues the loads of arrays the preceding kernel does not
+// write, fetch_d(Ld&) the rest; the first unit's fetch_s runs before gate() (the
+// programmatic-dependent-launch wait; false: the pass has nothing to do), and
+// compute(const Ld&) consumes a unit.
+template <int NU, class Ld, class FetchS, class FetchD, class Gate, class Compute>
+__device__ __forceinline__ void walk_tiles_pipelined(const uint32_t* tiles, int n, FetchS&& fetch_s, FetchD&& fetch_d,
+                                                     Gate&& gate, Compute&& compute) {
     const int wpb = TPB / 32, warp = threadIdx.x >> 5;
     const int stride = gridDim.x * wpb, total = n * NU;
     int u = blockIdx.x * wpb + warp;
-    if (u >= total) return;
-    uint32_t tile1 = u + stride < total ? tiles[(u + stride) / NU] : 0u;
+    uint32_t tile1 = 0u;
     Ld cur;
-    fetch(tiles[u / NU], u % NU, cur);
+    if (u < total) {
+        tile1 = u + stride < total ? tiles[(u + stride) / NU] : 0u;
+        fetch_s(tiles[u / NU], u % NU, cur);
+    }
+    if (!gate() || u >= total) return;
+    fetch_d(cur);
     for (; u < total; u += stride) {
         Ld nxt;
         const uint32_t tile2 = u + 2 * stride < total ? tiles[(u + 2 * stride) / NU] : 0u;
-        if (u + stride < total) fetch(tile1, (u + stride) % NU, nxt);
+        if (u + stride < total) {
+            fetch_s(tile1, (u + stride) % NU, nxt);
+            fetch_d(nxt);
+        }
         tile1 = tile2;
         compute(cur);
         cur = nxt;
@@ -551,30 +538,39 @@ struct DotLd {
     Vec8<M> zv;
     Vec8<V> rv;
     Vec8<V> qq;  // (flexible form only)
+    int p;
     bool ok;
 };
 template <class Pr>
 __global__ void __launch_bounds__(TPB)
     k_dot_v8(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ qv,
              Scalars* sc, double* partials, unsigned* counter) {
-    pdl_wait();
-    pdl_trigger();
     using M = typename Pr::M;
     using V = typename Pr::V;
     using Ld = DotLd<M, V, Pr::flexible>;
-    if (sc->s.done) return;
     double acc[2] = {0.0, 0.0};
+    bool done = false;
+    // r and q date from the previous iteration's step and search; z is the V-cycle's last
+    // pass's output, loaded after the wait
     walk_tiles_pipelined<2, Ld>(
         L.tiles, *L.count,
         [&](uint32_t tile, int cc, Ld& a) {
             Lane8 l8;
             a.ok = lane8_of(L, tile, l8);
             if (!a.ok) return;
-            const int p = l8.rb + cc * L.H + l8.h;
-            a.cdw = *reinterpret_cast<const uint2*>(L.code + p);
-            a.zv = ld8(L.x + p);
-            a.rv = ld8(r + p);
-            if constexpr (Pr::flexible) a.qq = ld8(qv + p);
+            a.p = l8.rb + cc * L.H + l8.h;
+            a.cdw = *reinterpret_cast<const uint2*>(L.code + a.p);
+            a.rv = ld8(r + a.p);
+            if constexpr (Pr::flexible) a.qq = ld8(qv + a.p);
+        },
+        [&](Ld& a) {
+            if (a.ok) a.zv = ld8(L.x + a.p);
+        },
+        [&]() {
+            pdl_wait();
+            pdl_trigger();
+            done = sc->s.done != 0;
+            return !done;
         },
         [&](const Ld& a) {
             if (!a.ok) return;
@@ -588,65 +584,94 @@ __global__ void __launch_bounds__(TPB)
                 }
             }
         });
+    if (done) return;
     if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0) dot_finish<Pr>(sc, acc);
 }
 
-// search_kernel! (src/flip.jl:1033-1054), vector form: colour by colour.
+// search_kernel! (src/flip.jl:1033-1054), vector form: one colour of a tile a unit. Every
+// array it reads dates from before the preceding kernel (z·r, which writes only the
+// scalars), so a warp loads its first unit before the programmatic-dependent-launch wait;
+// beta is read after it (d is loaded on the first pass too, and not used).
+template <class M, class V>
+struct SearchLd {
+    uint2 cdw;
+    Vec8<V> gv, dc;
+    Vec8<M> zc;
+    Nb8<M> zn;
+    Nb8<V> dn;
+    int p, ci;
+    bool ok;
+};
 template <class Pr>
-__global__ void __launch_bounds__(TPB)
+__device__ __forceinline__ void search_fetch(const Lev<typename Pr::M>& L, const typename Pr::V* dvec,
+                                             const typename Pr::V* diag, uint32_t tile, int cc,
+                                             SearchLd<typename Pr::M, typename Pr::V>& a) {
+    Lane8 l8;
+    a.ok = lane8_of(L, tile, l8);
+    if (!a.ok) return;
+    const int sy = L.n1, sz = L.n1 * L.n2;
+    const int p = l8.rb + cc * L.H + l8.h, o = l8.rb + (1 - cc) * L.H + l8.h;
+    a.p = p;
+    a.ci = ci_of(cc, l8.j, l8.k);
+    a.cdw = *reinterpret_cast<const uint2*>(L.code + p);
+    a.gv = ld8(diag + p);
+    a.zc = ld8(L.x + p);
+    a.zn = ld_nb8(L.x, o, sy, sz);
+    a.dc = ld8(dvec + p);
+    a.dn = ld_nb8(dvec, o, sy, sz);
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB, 2)
     k_search_v8(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ diag,
                 typename Pr::V* __restrict__ qout, Scalars* sc, double* partials, unsigned* counter) {
-    pdl_wait();
-    pdl_trigger();
     using C = typename Pr::C;
     using M = typename Pr::M;
     using V = typename Pr::V;
+    const int wpb = TPB / 32, warp = threadIdx.x >> 5;
+    const int n = *L.count, total = 2 * n, stride = gridDim.x * wpb;
+    int u = blockIdx.x * wpb + warp;
+    SearchLd<M, V> a;
+    uint32_t tile1 = 0u;
+    if (u < total) {
+        tile1 = u + stride < total ? L.tiles[(u + stride) >> 1] : 0u;
+        search_fetch<Pr>(L, dvec, diag, L.tiles[u >> 1], u & 1, a);
+    }
+    pdl_wait();
+    pdl_trigger();
     if (sc->s.done) return;
     const C beta = (C)sc->s.beta;
     const bool first = sc->s.beta == 0.0;
-    const int sy = L.n1, sz = L.n1 * L.n2;
     const bool edge = *L.edge != 0;
     double acc[1] = {0.0};
-    FOR_TILES_W(L, tile) {
-        Lane8 a;
-        if (!lane8_of(L, tile, a)) continue;
-#pragma unroll 1  // one colour at a time: half the live registers
-        for (int cc = 0; cc < 2; cc++) {
-            const int p = a.rb + cc * L.H + a.h, o = a.rb + (1 - cc) * L.H + a.h;
-            const int ci = ci_of(cc, a.j, a.k);
-            const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
-            const Vec8<V> gv = ld8(diag + p);
-            const Vec8<M> zc = ld8(L.x + p);
-            const Nb8<M> zn = ld_nb8(L.x, o, sy, sz);
-            Vec8<V> dc;
-            Nb8<V> dn;
-            if (!first) {
-                dc = ld8(dvec + p);
-                dn = ld_nb8(dvec, o, sy, sz);
-            }
-            const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
+    for (; u < total; u += stride) {
+        const uint32_t tile2 = u + 2 * stride < total ? L.tiles[(u + 2 * stride) >> 1] : 0u;
+        if (a.ok) {
             Vec8<V> out;
 #pragma unroll
             for (int q = 0; q < V8; q++) {
+                const uint8_t cd = (uint8_t)(((q < 4 ? a.cdw.x : a.cdw.y) >> (8 * (q & 3))) & 0xffu);
                 C qv = (C)0;
-                if (cd[q] & SELF) {
+                if (cd & SELF) {
                     C z6[6], d6[6];
-                    nb6_of(z6, zn, q, ci);
-                    if (!first) nb6_of(d6, dn, q, ci);
-                    const C pc = first ? ld<C>(&zc.v[q]) : ld<C>(&zc.v[q]) + beta * (C)dc.v[q];
+                    nb6_of(z6, a.zn, q, a.ci);
+                    if (!first) nb6_of(d6, a.dn, q, a.ci);
+                    const C pc = first ? ld<C>(&a.zc.v[q]) : ld<C>(&a.zc.v[q]) + beta * (C)a.dc.v[q];
                     C s = (C)0;  // nsum6 over p = z + beta d, formed term by term
 #pragma unroll
                     for (int m = 0; m < 6; m++) {
                         const C pm = first ? z6[m] : z6[m] + beta * d6[m];
-                        if (!edge || (cd[q] & (1u << m))) s += pm;
+                        if (!edge || (cd & (1u << m))) s += pm;
                     }
-                    qv = (C)gv.v[q] * pc - s;
+                    qv = (C)a.gv.v[q] * pc - s;
                     acc[0] += (double)pc * (double)qv;
                 }
                 st(&out.v[q], qv);
             }
-            st8(qout + p, out);
+            st8(qout + a.p, out);
         }
+        a.ok = false;
+        if (u + stride < total) search_fetch<Pr>(L, dvec, diag, tile1, (u + stride) & 1, a);
+        tile1 = tile2;
     }
     if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) search_finish<Pr>(sc, acc);
 }
