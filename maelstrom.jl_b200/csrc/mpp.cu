@@ -520,7 +520,7 @@ struct Run {
             end();
             smooth(l, l == 0 ? down0 : down);
             beg(F_RESID, l);
-            if (vec(l)) launch(k_residual_v8<Pr>, grid_w(l), TPB, 0, s, view<M>(c, l));
+            if (vec(l)) launch(k_residual_v8<Pr>, grid_res((const void*)k_residual_v8<Pr>, l), TPB, 0, s, view<M>(c, l));
             else launch(k_residual<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
             end();
             if (l + 1 < lb) {

@@ -135,9 +135,10 @@ __device__ __forceinline__ void cmg_zero(unsigned off, size_t bytes) {
     for (int u = (int)threadIdx.x; u < n16; u += CMG_THREADS) s[u] = make_uint4(0, 0, 0, 0);
 }
 
-// Fill slab q from its level's global arrays (b and x, or zeros; r zeros when asked).
+// Fill slab q from its level's global arrays (b: 1 loaded, 0 zeros, -1 left alone; x loaded
+// or zeros; r zeros when asked).
 template <class Pr>
-__device__ __forceinline__ void cmg_load(const CmgSlab& S, const Lev<typename Pr::M>& G, int me, bool ldb, bool ldx,
+__device__ __forceinline__ void cmg_load(const CmgSlab& S, const Lev<typename Pr::M>& G, int me, int ldb, bool ldx,
                                          bool clr) {
     using M = typename Pr::M;
     const int n = S.P * S.n2 * S.n1;
@@ -145,8 +146,8 @@ __device__ __forceinline__ void cmg_load(const CmgSlab& S, const Lev<typename Pr
     cmg_copy<uint8_t, true>(cmg_ptr<uint8_t>(S.ocode), G.code + g0, n);
     cmg_copy<M, true>(cmg_ptr<M>(S.odg), G.dg + g0, n);
     if (Pr::scaled) cmg_copy<M, true>(cmg_ptr<M>(S.odi), G.di + g0, n);
-    if (ldb) cmg_copy<M, true>(cmg_ptr<M>(S.ob), G.b + g0, n);
-    else cmg_zero(S.ob, sizeof(M) * n);
+    if (ldb > 0) cmg_copy<M, true>(cmg_ptr<M>(S.ob), G.b + g0, n);
+    else if (ldb == 0) cmg_zero(S.ob, sizeof(M) * n);
     if (ldx) cmg_copy<M, true>(cmg_ptr<M>(S.ox), G.x + g0, n);
     else cmg_zero(S.ox, sizeof(M) * n);
     if (clr) cmg_zero(S.orr, sizeof(M) * n);
@@ -493,12 +494,21 @@ __device__ __forceinline__ void cmg_prolong(const CmgSlab& F, int qf, const CmgS
 
 template <class Pr, int UP>
 __global__ void __launch_bounds__(CMG_THREADS, 1) k_cmg(const __grid_constant__ CmgArgs<typename Pr::M> a) {
+    using C = typename Pr::C;
+    using M = typename Pr::M;
+    const int me = (int)blockIdx.x, cs = (int)gridDim.x, nl = a.nl;
+    // Loaded before the programmatic-dependent-launch wait: what the preceding kernel does
+    // not write. Down follows the restriction into level ls (its b, loaded after the wait);
+    // up follows the bottom solve (the bottom level's x, read by the first prolongation).
+    if (threadIdx.x < CMG_MAXLEV) cmg_count((int)threadIdx.x) = 0;
+    for (int q = 0; q < nl; q++) cmg_load<Pr>(a.s[q], a.g[q], me, UP ? 1 : (q == 0 ? -1 : 0), UP, !UP);
     pdl_wait();
     pdl_trigger();
-    using C = typename Pr::C;
-    const int me = (int)blockIdx.x, cs = (int)gridDim.x, nl = a.nl;
-    if (threadIdx.x < CMG_MAXLEV) cmg_count((int)threadIdx.x) = 0;
-    for (int q = 0; q < nl; q++) cmg_load<Pr>(a.s[q], a.g[q], me, UP || q == 0, UP, !UP);
+    if (!UP) {
+        const CmgSlab& S = a.s[0];
+        const int n = S.P * S.n2 * S.n1;
+        cmg_copy<M, true>(cmg_ptr<M>(S.ob), a.g[0].b + (int64_t)me * n, n);
+    }
     __syncthreads();
     for (int q = 0; q < nl; q++) cmg_rows(a.s[q], q);
     cluster_barrier();

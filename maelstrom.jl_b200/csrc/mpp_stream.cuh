@@ -391,6 +391,40 @@ __device__ __forceinline__ bool lane8_of(const Lev<M>& L, uint32_t tile, Lane8& 
     for (uint32_t next_; t_ < n_; t_ += s_, tile = next_)                                                 \
         if ((next_ = (t_ + s_ < n_ ? (L).tiles[t_ + s_] : 0u)), true)
 
+// Walk this warp's share of a level's tile list in units (tile, sub-unit < NU), the loads
+// of the next unit issued before the arithmetic of this one and its tile id fetched two
+// units ahead (the rbgs_v8 pipeline, for passes whose units do not overlap in what they
+// write). fetch_s(tile, sub, Ld&) issues the loads of arrays the preceding kernel does not
+// write, fetch_d(Ld&) the rest; the first unit's fetch_s runs before gate() (the
+// programmatic-dependent-launch wait; false: the pass has nothing to do), and
+// compute(const Ld&) consumes a unit.
+template <int NU, class Ld, class FetchS, class FetchD, class Gate, class Compute>
+__device__ __forceinline__ void walk_tiles_pipelined(const uint32_t* tiles, int n, FetchS&& fetch_s, FetchD&& fetch_d,
+                                                     Gate&& gate, Compute&& compute) {
+    const int wpb = TPB / 32, warp = threadIdx.x >> 5;
+    const int stride = gridDim.x * wpb, total = n * NU;
+    int u = blockIdx.x * wpb + warp;
+    uint32_t tile1 = 0u;
+    Ld cur;
+    if (u < total) {
+        tile1 = u + stride < total ? tiles[(u + stride) / NU] : 0u;
+        fetch_s(tiles[u / NU], u % NU, cur);
+    }
+    if (!gate() || u >= total) return;
+    fetch_d(cur);
+    for (; u < total; u += stride) {
+        Ld nxt;
+        const uint32_t tile2 = u + 2 * stride < total ? tiles[(u + 2 * stride) / NU] : 0u;
+        if (u + stride < total) {
+            fetch_s(tile1, (u + stride) % NU, nxt);
+            fetch_d(nxt);
+        }
+        tile1 = tile2;
+        compute(cur);
+        cur = nxt;
+    }
+}
+
 // The other colour's values around a lane's 8 cells: the same 8 columns of this row
 // (the +x/-x neighbours) with one element on each side, and of the rows at +-y, +-z.
 template <class M>
@@ -456,78 +490,66 @@ __global__ void __launch_bounds__(TPB) k_start_v8(Lev<typename Pr::M> L) {
     start_v8_body<Pr>(L);
 }
 
-// residual_kernel! (src/flip.jl:859-863), vector form: both colours of the lane's columns.
+// residual_kernel! (src/flip.jl:859-863), vector form: one colour of a tile a unit,
+// pipelined; code, diagonal and b (older than the preceding colour pass) load before the
+// programmatic-dependent-launch wait, x after it.
+template <class M>
+struct ResLd {
+    uint2 cdw;
+    Vec8<M> dv, bv, xv;
+    Nb8<M> nb;
+    int p, o, ci;
+    bool ok;
+};
 template <class Pr>
 __device__ __forceinline__ void residual_v8_body(Lev<typename Pr::M> L) {
     using C = typename Pr::C;
     using M = typename Pr::M;
     const int sy = L.n1, sz = L.n1 * L.n2;
     const bool edge = *L.edge != 0;
-    FOR_TILES_W(L, tile) {
-        Lane8 a;
-        if (!lane8_of(L, tile, a)) continue;
-#pragma unroll
-        for (int cc = 0; cc < 2; cc++) {
-            const int p = a.rb + cc * L.H + a.h, o = a.rb + (1 - cc) * L.H + a.h;
-            const int ci = ci_of(cc, a.j, a.k);
-            const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
-            const Vec8<M> dv = ld8(L.dg + p), bv = ld8(L.b + p), xv = ld8(L.x + p);
-            const Nb8<M> nb = ld_nb8(L.x, o, sy, sz);
-            const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
+    walk_tiles_pipelined<2, ResLd<M>>(
+        L.tiles, *L.count,
+        [&](uint32_t tile, int cc, ResLd<M>& a) {
+            Lane8 l8;
+            a.ok = lane8_of(L, tile, l8);
+            if (!a.ok) return;
+            a.p = l8.rb + cc * L.H + l8.h;
+            a.o = l8.rb + (1 - cc) * L.H + l8.h;
+            a.ci = ci_of(cc, l8.j, l8.k);
+            a.cdw = *reinterpret_cast<const uint2*>(L.code + a.p);
+            a.dv = ld8(L.dg + a.p);
+            a.bv = ld8(L.b + a.p);
+        },
+        [&](ResLd<M>& a) {
+            if (!a.ok) return;
+            a.xv = ld8(L.x + a.p);
+            a.nb = ld_nb8(L.x, a.o, sy, sz);
+        },
+        [&]() {
+            pdl_wait();
+            pdl_trigger();
+            return true;
+        },
+        [&](const ResLd<M>& a) {
+            if (!a.ok) return;
             Vec8<M> out;
 #pragma unroll
             for (int q = 0; q < V8; q++) {
+                const uint8_t cd = (uint8_t)(((q < 4 ? a.cdw.x : a.cdw.y) >> (8 * (q & 3))) & 0xffu);
                 C v = (C)0;
-                if (cd[q] & SELF) {
+                if (cd & SELF) {
                     C n6[6];
-                    nb6_of(n6, nb, q, ci);
-                    v = ld<C>(&bv.v[q]) - (ld<C>(&dv.v[q]) * ld<C>(&xv.v[q]) - nsum6<C>(n6, cd[q], edge));
+                    nb6_of(n6, a.nb, q, a.ci);
+                    v = ld<C>(&a.bv.v[q]) - (ld<C>(&a.dv.v[q]) * ld<C>(&a.xv.v[q]) - nsum6<C>(n6, cd, edge));
                 }
                 st(&out.v[q], v);
             }
-            st8(L.r + p, out);
-        }
-    }
+            st8(L.r + a.p, out);
+        });
 }
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_residual_v8(Lev<typename Pr::M> L) {
-    pdl_wait();
-    pdl_trigger();
     residual_v8_body<Pr>(L);
-}
-
-// Walk this warp's share of a level's tile list in units (tile, sub-unit < NU), the loads
-// of the next unit issued before the arithmetic of this one and its tile id fetched two
-// units ahead (the rbgs_v8 pipeline, for passes whose units do not overlap in what they
-// write). fetch_s(tile, sub, Ld&) issues the loads of arrays the preceding kernel does not
-// write, fetch_d(Ld&) the rest; the first unit's fetch_s runs before gate() (the
-// programmatic-dependent-launch wait; false: the pass has nothing to do), and
-// compute(const Ld&) consumes a unit.
-template <int NU, class Ld, class FetchS, class FetchD, class Gate, class Compute>
-__device__ __forceinline__ void walk_tiles_pipelined(const uint32_t* tiles, int n, FetchS&& fetch_s, FetchD&& fetch_d,
-                                                     Gate&& gate, Compute&& compute) {
-    const int wpb = TPB / 32, warp = threadIdx.x >> 5;
-    const int stride = gridDim.x * wpb, total = n * NU;
-    int u = blockIdx.x * wpb + warp;
-    uint32_t tile1 = 0u;
-    Ld cur;
-    if (u < total) {
-        tile1 = u + stride < total ? tiles[(u + stride) / NU] : 0u;
-        fetch_s(tiles[u / NU], u % NU, cur);
-    }
-    if (!gate() || u >= total) return;
-    fetch_d(cur);
-    for (; u < total; u += stride) {
-        Ld nxt;
-        const uint32_t tile2 = u + 2 * stride < total ? tiles[(u + 2 * stride) / NU] : 0u;
-        if (u + stride < total) {
-            fetch_s(tile1, (u + stride) % NU, nxt);
-            fetch_d(nxt);
-        }
-        tile1 = tile2;
-        compute(cur);
-        cur = nxt;
-    }
 }
 
 // inner(s, z, r) and the flexible z.q (see k_dot), vector form: one colour of a tile a
