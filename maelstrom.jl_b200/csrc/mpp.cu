@@ -515,7 +515,7 @@ struct Run {
         const int ls = c->cmg_ls > 0 ? c->cmg_ls : lb;  // levels ls .. lb-1 in the cluster
         for (int l = 0; l < ls; l++) {
             beg(F_START, l);
-            if (vec(l)) launch(k_start_v8<Pr>, grid_w(l), TPB, 0, s, view<M>(c, l));
+            if (vec(l)) launch(k_start_v8<Pr>, grid_res((const void*)k_start_v8<Pr>, l), TPB, 0, s, view<M>(c, l));
             else launch(k_start<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
             end();
             smooth(l, l == 0 ? down0 : down);

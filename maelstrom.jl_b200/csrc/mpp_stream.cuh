@@ -459,34 +459,55 @@ __device__ __forceinline__ void nb6_of(C (&nb)[6], const Nb8<M>& a, int q, int c
     nb[5] = ld<C>(&a.zm.v[q]);
 }
 
-// start_kernel! (src/flip.jl:965-973), vector form.
+template <class M>
+struct StartLd {
+    uint2 cdw;
+    Vec8<M> dv, bv;
+    int p;
+    bool ok;
+};
+// start_kernel! (src/flip.jl:965-973), vector form, pipelined: code and diagonal load
+// before the programmatic-dependent-launch wait, b (the preceding restriction's or CG
+// step's output) after it.
 template <class Pr>
 __device__ __forceinline__ void start_v8_body(Lev<typename Pr::M> L) {
     using C = typename Pr::C;
     using M = typename Pr::M;
-    FOR_TILES_W(L, tile) {
-        Lane8 a;
-        if (!lane8_of(L, tile, a)) continue;
-        const int p0 = a.rb + a.h;
-        const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p0);
-        const Vec8<M> dv = ld8((Pr::scaled ? L.di : L.dg) + p0), bv = ld8(L.b + p0);
-        const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
-        Vec8<M> x0, x1;
+    walk_tiles_pipelined<1, StartLd<M>>(
+        L.tiles, *L.count,
+        [&](uint32_t tile, int, StartLd<M>& a) {
+            Lane8 l8;
+            a.ok = lane8_of(L, tile, l8);
+            if (!a.ok) return;
+            a.p = l8.rb + l8.h;
+            a.cdw = *reinterpret_cast<const uint2*>(L.code + a.p);
+            a.dv = ld8((Pr::scaled ? L.di : L.dg) + a.p);
+        },
+        [&](StartLd<M>& a) {
+            if (a.ok) a.bv = ld8(L.b + a.p);
+        },
+        [&]() {
+            pdl_wait();
+            pdl_trigger();
+            return true;
+        },
+        [&](const StartLd<M>& a) {
+            if (!a.ok) return;
+            Vec8<M> x0, x1;
 #pragma unroll
-        for (int q = 0; q < V8; q++) {
-            const C d = ld<C>(&dv.v[q]);
-            if constexpr (Pr::scaled) st(&x0.v[q], (cd[q] & SELF) ? ld<C>(&bv.v[q]) * d : (C)0);
-            else st(&x0.v[q], ((cd[q] & SELF) && d > (C)0) ? ld<C>(&bv.v[q]) / d : (C)0);
-            st(&x1.v[q], (C)0);
-        }
-        st8(L.x + p0, x0);
-        st8(L.x + p0 + L.H, x1);
-    }
+            for (int q = 0; q < V8; q++) {
+                const uint8_t cd = (uint8_t)(((q < 4 ? a.cdw.x : a.cdw.y) >> (8 * (q & 3))) & 0xffu);
+                const C d = ld<C>(&a.dv.v[q]);
+                if constexpr (Pr::scaled) st(&x0.v[q], (cd & SELF) ? ld<C>(&a.bv.v[q]) * d : (C)0);
+                else st(&x0.v[q], ((cd & SELF) && d > (C)0) ? ld<C>(&a.bv.v[q]) / d : (C)0);
+                st(&x1.v[q], (C)0);
+            }
+            st8(L.x + a.p, x0);
+            st8(L.x + a.p + L.H, x1);
+        });
 }
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_start_v8(Lev<typename Pr::M> L) {
-    pdl_wait();
-    pdl_trigger();
     start_v8_body<Pr>(L);
 }
 
@@ -705,11 +726,15 @@ __global__ void __launch_bounds__(TPB, 3)
     k_advance_v8(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ qv,
                  typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
                  unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
-    pdl_wait();
-    pdl_trigger();
     using C = typename Pr::C;
     using M = typename Pr::M;
     using V = typename Pr::V;
+    // the first tile id (the tile lists date from the set-up) before the wait
+    const int n_ = *L.count, s_ = gridDim.x * (TPB / 32);
+    int t_ = blockIdx.x * (TPB / 32) + (int)(threadIdx.x >> 5);
+    uint32_t tile = t_ < n_ ? L.tiles[t_] : 0u;
+    pdl_wait();
+    pdl_trigger();
     if (sc->s.done) {
         if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(cond, use_cond, 0);
         return;
@@ -719,7 +744,8 @@ __global__ void __launch_bounds__(TPB, 3)
     const bool sep_b = (void*)L.b != (void*)r;
     const C rsc = (C)sc->s.rscale;
     double acc[1] = {0.0};
-    FOR_TILES_W(L, tile) {
+    for (uint32_t next_; t_ < n_; t_ += s_, tile = next_) {
+        next_ = t_ + s_ < n_ ? L.tiles[t_ + s_] : 0u;
         Lane8 a;
         if (!lane8_of(L, tile, a)) continue;
         const int pn = a.rb + 2 * a.h;  // natural run of the lane's 16 cells
@@ -777,9 +803,15 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
     __shared__ C smw[WPB][PZ][PY][PX];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     C(*S)[PY][PX] = smw[warp];
-    const int n = *L.count;
-    for (int t = blockIdx.x * WPB + warp; t < n; t += gridDim.x * WPB) {
-        const uint32_t tile = L.tiles[t];
+    const int n = *L.count, stride = gridDim.x * WPB;
+    // the first tile id before the programmatic-dependent-launch wait (the tile lists date
+    // from the set-up; the coarse x is the preceding kernel's output)
+    int t = blockIdx.x * WPB + warp;
+    uint32_t tile = t < n ? L.tiles[t] : 0u;
+    pdl_wait();
+    pdl_trigger();
+    for (; t < n; t += stride) {
+        const uint32_t tile_next = t + stride < n ? L.tiles[t + stride] : 0u;
         const int I0 = (int)(tile & 1023u) * TH - 1, J0 = (int)((tile >> 10) & 1023u) * (TY / 2) - 1,
                   K0 = (int)(tile >> 20) * (TZ / 2) - 1;
         C vals[PER];
@@ -792,6 +824,19 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
             if (e < NE && I >= 0 && I < Cl.n1 && J >= 0 && J < Cl.n2 && K >= 0 && K < Cl.n3)
                 vals[u] = ld<C>(Cl.x + (cnat ? (int)Cl.nat(I, J, K) : (int)Cl.pos(I, J, K)));
         }
+        // this lane's fine cells, loaded beside the staging loads
+        Lane8 a;
+        const bool ok = lane8_of(L, tile, a);
+        uint2 cdw[2];
+        Vec8<M> xv[2];
+        if (ok) {
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                const int p = a.rb + cc * L.H + a.h;
+                cdw[cc] = *reinterpret_cast<const uint2*>(L.code + p);
+                xv[cc] = ld8(L.x + p);
+            }
+        }
         __syncwarp();
 #pragma unroll
         for (int u = 0; u < PER; u++) {
@@ -799,8 +844,8 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
             if (e < NE) (&S[0][0][0])[e] = vals[u];
         }
         __syncwarp();
-        Lane8 a;
-        if (!lane8_of(L, tile, a)) continue;
+        tile = tile_next;
+        if (!ok) continue;
         int b0, b1, k0, k1;
         C wb0, wb1, wc0, wc1;
         pweights<C>(a.j, b0, wb0, b1, wb1);
@@ -810,12 +855,10 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
         for (int cc = 0; cc < 2; cc++) {
             const int p = a.rb + cc * L.H + a.h;
             const int ci = ci_of(cc, a.j, a.k);
-            const uint2 cdw = *reinterpret_cast<const uint2*>(L.code + p);
-            Vec8<M> xv = ld8(L.x + p);
-            const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
 #pragma unroll
             for (int q = 0; q < V8; q++) {
-                if (!(cd[q] & SELF)) continue;
+                const uint8_t cd = (uint8_t)(((q < 4 ? cdw[cc].x : cdw[cc].y) >> (8 * (q & 3))) & 0xffu);
+                if (!(cd & SELF)) continue;
                 const int i = 2 * (a.h + q) + ci;
                 int a0, a1;
                 C wa0, wa1;
@@ -828,16 +871,14 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
                     const C wa = (m & 1) ? wa1 : wa0, wb = (m & 2) ? wb1 : wb0, wc = (m & 4) ? wc1 : wc0;
                     s += wa * wb * wc * S[K][B][A];
                 }
-                st(&xv.v[q], ld<C>(&xv.v[q]) + (Pr::scaled ? (C)4 * s : s));
+                st(&xv[cc].v[q], ld<C>(&xv[cc].v[q]) + (Pr::scaled ? (C)4 * s : s));
             }
-            st8(L.x + p, xv);
+            st8(L.x + p, xv[cc]);
         }
     }
 }
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_prolong_v8(Lev<typename Pr::M> L, Lev<typename Pr::M> Cl, int cnat) {
-    pdl_wait();
-    pdl_trigger();
     prolong_v8_body<Pr>(L, Cl, cnat);
 }
 
