@@ -449,7 +449,8 @@ struct Run {
         // 8 cells of a row per thread, with 8- and 16-byte loads of the caller's classes and faces
         if (c->grid.n[0] % 8 == 0 && al(in.types, 8) && (!in.v || al(in.v, 16)) && (!in.w || al(in.w, 16)) &&
             al(in.P, 16) && (!in.phi || al(in.phi, 16)))
-            launch(k_setup_v8<Pr>, grid_cells(c, N / 8), TPB, 0, s, in, view<M>(c, 0), (V*)c->diag, (V*)c->bvec,
+            launch(k_setup_v8<Pr>, grid_cells(c, (N / 8) * TPB / SETUP_V8_TPB), SETUP_V8_TPB, 0, s, in, view<M>(c, 0),
+                   (V*)c->diag, (V*)c->bvec,
                    (V*)c->r, c->sc, c->partials, cnt(CNT_SETUP), cond, use_cond);
         else
             launch(k_setup<Pr>, grid_cells(c, N), TPB, 0, s, in, view<M>(c, 0), (V*)c->diag, (V*)c->bvec, (V*)c->r,

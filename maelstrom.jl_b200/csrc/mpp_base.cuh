@@ -98,6 +98,18 @@ __device__ __forceinline__ uint8_t typeat(const uint8_t* __restrict__ t, int n1,
                : SOLID;
 }
 
+// A cell's liquid fraction clamp(0.5 - phi/dx, 0, 1) (src/flip.jl:268). Outside the
+// band |phi| < dx/2 it is 0 or 1 without the division: 0.5 dx is exact, correctly rounded
+// division is monotone and 0.5 is representable, so phi >= dx/2 gives phi/dx >= 0.5 and
+// phi <= -dx/2 gives phi/dx <= -0.5 (NaN takes the division, as before).
+__device__ __forceinline__ float liquid_fraction(float ph, float dx) {
+    const float h = 0.5f * dx;
+    if (ph >= h) return 0.f;
+    if (ph <= -h) return 1.f;
+    const float x = 0.5f - ph / dx;
+    return x > 1.f ? 1.f : (x < 0.f ? 0.f : x);
+}
+
 // volume_kernel! + volume + the gamma of project! (src/flip.jl:261-279, 293, 1146-1147):
 // liquid volume sum clamp(0.5 - phi/dx, 0, 1) dx^3 over cells whose centre is not solid,
 // then gamma = clamp(loss / recover, -0.01/dt, 0.01/dt) with loss the relative volume loss.
@@ -115,17 +127,11 @@ __global__ void __launch_bounds__(TPB) k_volume(Geo g, const float* __restrict__
             const float ph[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
             for (int m = 0; m < 8; m++)
-                if (!issolidcell(g, i0 + m, j, k)) {
-                    float x = 0.5f - ph[m] / g.dx;
-                    acc[0] += (double)(x > 1.f ? 1.f : (x < 0.f ? 0.f : x));
-                }
+                if (!issolidcell(g, i0 + m, j, k)) acc[0] += (double)liquid_fraction(ph[m], g.dx);
         }
     } else {
         FOR_CELLS(g.n[0], g.n[1], g.n[2], i, j, k, idx) {
-            if (!issolidcell(g, i, j, k)) {
-                float x = 0.5f - phi[idx] / g.dx;
-                acc[0] += (double)(x > 1.f ? 1.f : (x < 0.f ? 0.f : x));
-            }
+            if (!issolidcell(g, i, j, k)) acc[0] += (double)liquid_fraction(phi[idx], g.dx);
         }
     }
     if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
@@ -299,8 +305,10 @@ __device__ __forceinline__ void st_quad(T* p, const T (&v)[4]) {  // 4-element a
     }
 }
 
+// 128-thread blocks: at this kernel's register count, 12 warps a SM instead of 8.
+constexpr int SETUP_V8_TPB = 128;
 template <class Pr>
-__global__ void __launch_bounds__(TPB)
+__global__ void __launch_bounds__(SETUP_V8_TPB)
     k_setup_v8(SetupIn<typename Pr::V> a, Lev<typename Pr::M> L, typename Pr::V* __restrict__ diag,
                typename Pr::V* __restrict__ b, typename Pr::V* __restrict__ r, Scalars* sc, double* partials,
                unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
@@ -316,7 +324,7 @@ __global__ void __launch_bounds__(TPB)
     const bool sep_b = (void*)L.b != (void*)r;
     double acc[3] = {0.0, 0.0, 0.0};
     const int nch = nq * n2 * n3;
-    for (int ch = (int)(blockIdx.x * TPB + threadIdx.x); ch < nch; ch += (int)(gridDim.x * TPB)) {
+    for (int ch = (int)(blockIdx.x * SETUP_V8_TPB + threadIdx.x); ch < nch; ch += (int)(gridDim.x * SETUP_V8_TPB)) {
         const int q8 = ch % nq, rw = ch / nq, j = rw % n2, k = rw / n2, i0 = 8 * q8;
         const int row = rw * n1, idx0 = row + i0;
         Row8<uint8_t> tc = ld_row8(a.types + idx0), tym, typ, tzm, tzp;

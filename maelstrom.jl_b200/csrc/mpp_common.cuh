@@ -161,7 +161,7 @@ __device__ __forceinline__ void block_sum(double (&v)[K]) {
     if (w == 0) {
 #pragma unroll
         for (int q = 0; q < K; q++) {
-            double a = lane < TPB / 32 ? ws[q][lane] : 0.0;
+            double a = lane < (int)(blockDim.x >> 5) ? ws[q][lane] : 0.0;  // blocks of <= TPB threads
 #pragma unroll
             for (int o = 4; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
             v[q] = a;
