@@ -613,8 +613,14 @@ struct Run {
                   const uint8_t* types, const float* phi) {
         const int64_t N = (int64_t)(c->grid.n[0] + 1) * (c->grid.n[1] + 1) * (c->grid.n[2] + 1);
         beg(F_GRADIENT, -1);
-        launch(k_gradient, grid_cells(c, N), TPB, 0, s, c->grid.n[0], c->grid.n[1], c->grid.n[2], u, v, w, fu, fv, fw, P,
-                                                    types, phi, c->grid.dx);
+        auto al = [](const void* q, uintptr_t a) { return (reinterpret_cast<uintptr_t>(q) & (a - 1)) == 0; };
+        if (c->grid.n[0] % 4 == 0 && phi && al(P, 16) && al(phi, 16) && al(v, 16) && al(w, 16) && al(types, 4) &&
+            al(fv, 4) && al(fw, 4))
+            launch(k_gradient_v4, grid_cells(c, N / 4), TPB, 0, s, c->grid.n[0], c->grid.n[1], c->grid.n[2], u, v, w,
+                   fu, fv, fw, P, types, phi, c->grid.dx);
+        else
+            launch(k_gradient, grid_cells(c, N), TPB, 0, s, c->grid.n[0], c->grid.n[1], c->grid.n[2], u, v, w, fu, fv,
+                   fw, P, types, phi, c->grid.dx);
         end();
     }
 

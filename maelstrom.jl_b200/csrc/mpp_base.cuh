@@ -606,6 +606,112 @@ __global__ void __launch_bounds__(TPB) k_gradient(int n1, int n2, int n3, float*
     }
 }
 
+// One face's update from its two cells' class, pressure and level set (face_update's
+// arithmetic; (t0, p0, f0) the cell on the low side).
+__device__ __forceinline__ bool face_delta(uint8_t t0, uint8_t t1, float p0, float p1, float f0, float f1, float dx,
+                                           float& u) {
+    const bool ok = t0 != SOLID && t1 != SOLID && (t0 == LIQUID || t1 == LIQUID);
+    if (ok) {
+        float delta;
+        if (t0 == LIQUID && t1 == LIQUID) delta = p1 - p0;
+        else if (t0 == LIQUID) delta = (-p0) / theta<float>(f0, f1);
+        else delta = p1 / theta<float>(f1, f0);
+        u = u - delta / dx;
+    }
+    return ok;
+}
+
+// k_gradient with 4 consecutive cells of a row per thread (rows a multiple of 4 long, the
+// arrays aligned): each thread updates the u, v and w faces on the low side of its cells
+// (4-wide loads of the classes, P and phi of its cells and of the rows below in y and z),
+// and a second loop clears the flags of the faces on the box's high sides (i = n1, j = n2,
+// k = n3), which have a cell outside the grid and so are never valid. A chunk whose cells
+// and low neighbours hold no LIQUID cell only writes its flags.
+__global__ void __launch_bounds__(TPB) k_gradient_v4(int n1, int n2, int n3, float* __restrict__ u,
+                                                     float* __restrict__ v, float* __restrict__ w,
+                                                     uint8_t* __restrict__ fu, uint8_t* __restrict__ fv,
+                                                     uint8_t* __restrict__ fw, const float* __restrict__ P,
+                                                     const uint8_t* __restrict__ types, const float* __restrict__ phi,
+                                                     float dx) {
+    pdl_wait();
+    pdl_trigger();
+    const int nq = n1 / 4, sz = n1 * n2, nch = nq * n2 * n3;
+    for (int ch = (int)(blockIdx.x * TPB + threadIdx.x); ch < nch; ch += (int)(gridDim.x * TPB)) {
+        const int q4 = ch % nq, rw = ch / nq, j = rw % n2, k = rw / n2, i0 = 4 * q4;
+        const int c = rw * n1 + i0;  // the first cell
+        const uchar4 tc = *reinterpret_cast<const uchar4*>(types + c);
+        const uint8_t t[4] = {tc.x, tc.y, tc.z, tc.w};
+        const uint8_t tx = i0 > 0 ? types[c - 1] : (uint8_t)SOLID;
+        uint8_t ty[4] = {SOLID, SOLID, SOLID, SOLID}, tz[4] = {SOLID, SOLID, SOLID, SOLID};
+        if (j > 0) {
+            const uchar4 a = *reinterpret_cast<const uchar4*>(types + c - n1);
+            ty[0] = a.x; ty[1] = a.y; ty[2] = a.z; ty[3] = a.w;
+        }
+        if (k > 0) {
+            const uchar4 a = *reinterpret_cast<const uchar4*>(types + c - sz);
+            tz[0] = a.x; tz[1] = a.y; tz[2] = a.z; tz[3] = a.w;
+        }
+        bool any = tx == LIQUID;
+#pragma unroll
+        for (int m = 0; m < 4; m++) any |= t[m] == LIQUID || ty[m] == LIQUID || tz[m] == LIQUID;
+        const int64_t ui = (int64_t)i0 + (int64_t)(n1 + 1) * ((int64_t)j + (int64_t)n2 * k);
+        const int64_t vi = (int64_t)i0 + (int64_t)n1 * ((int64_t)j + (int64_t)(n2 + 1) * k);
+        const int64_t wi = (int64_t)c;  // i0 + n1 (j + n2 k): w's layout has n3 + 1 planes
+        uint8_t ok_u[4] = {0, 0, 0, 0}, ok_v[4] = {0, 0, 0, 0}, ok_w[4] = {0, 0, 0, 0};
+        if (any) {
+            const float4 p4 = *reinterpret_cast<const float4*>(P + c), f4 = *reinterpret_cast<const float4*>(phi + c);
+            const float pc[4] = {p4.x, p4.y, p4.z, p4.w}, fc[4] = {f4.x, f4.y, f4.z, f4.w};
+            const float px = i0 > 0 ? P[c - 1] : 0.f, fx = i0 > 0 ? phi[c - 1] : 0.f;
+            float py[4] = {0.f, 0.f, 0.f, 0.f}, fy[4] = {0.f, 0.f, 0.f, 0.f};
+            float pz[4] = {0.f, 0.f, 0.f, 0.f}, fz[4] = {0.f, 0.f, 0.f, 0.f};
+            if (j > 0) {
+                const float4 a = *reinterpret_cast<const float4*>(P + c - n1), b = *reinterpret_cast<const float4*>(phi + c - n1);
+                py[0] = a.x; py[1] = a.y; py[2] = a.z; py[3] = a.w;
+                fy[0] = b.x; fy[1] = b.y; fy[2] = b.z; fy[3] = b.w;
+            }
+            if (k > 0) {
+                const float4 a = *reinterpret_cast<const float4*>(P + c - sz), b = *reinterpret_cast<const float4*>(phi + c - sz);
+                pz[0] = a.x; pz[1] = a.y; pz[2] = a.z; pz[3] = a.w;
+                fz[0] = b.x; fz[1] = b.y; fz[2] = b.z; fz[3] = b.w;
+            }
+            float uu[4];
+#pragma unroll
+            for (int m = 0; m < 4; m++) uu[m] = u[ui + m];
+            float4 v4 = *reinterpret_cast<const float4*>(v + vi), w4 = *reinterpret_cast<const float4*>(w + wi);
+            float vv[4] = {v4.x, v4.y, v4.z, v4.w}, ww[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                const uint8_t tl = m > 0 ? t[m > 0 ? m - 1 : 0] : tx;
+                const float pl = m > 0 ? pc[m > 0 ? m - 1 : 0] : px, fl = m > 0 ? fc[m > 0 ? m - 1 : 0] : fx;
+                ok_u[m] = face_delta(tl, t[m], pl, pc[m], fl, fc[m], dx, uu[m]);
+                ok_v[m] = face_delta(ty[m], t[m], py[m], pc[m], fy[m], fc[m], dx, vv[m]);
+                ok_w[m] = face_delta(tz[m], t[m], pz[m], pc[m], fz[m], fc[m], dx, ww[m]);
+            }
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                if (ok_u[m]) u[ui + m] = uu[m];
+            *reinterpret_cast<float4*>(v + vi) = make_float4(vv[0], vv[1], vv[2], vv[3]);
+            *reinterpret_cast<float4*>(w + wi) = make_float4(ww[0], ww[1], ww[2], ww[3]);
+        }
+#pragma unroll
+        for (int m = 0; m < 4; m++) fu[ui + m] = ok_u[m];
+        *reinterpret_cast<uchar4*>(fv + vi) = make_uchar4(ok_v[0], ok_v[1], ok_v[2], ok_v[3]);
+        *reinterpret_cast<uchar4*>(fw + wi) = make_uchar4(ok_w[0], ok_w[1], ok_w[2], ok_w[3]);
+    }
+    // the high-side faces: u at i = n1, v at j = n2, w at k = n3
+    const int bu = n2 * n3, bv = n1 * n3, bw = n1 * n2;
+    for (int e = (int)(blockIdx.x * TPB + threadIdx.x); e < bu + bv + bw; e += (int)(gridDim.x * TPB)) {
+        if (e < bu) {
+            fu[(int64_t)n1 + (int64_t)(n1 + 1) * e] = 0;  // e = j + n2 k
+        } else if (e < bu + bv) {
+            const int f = e - bu, i = f % n1, k = f / n1;
+            fv[(int64_t)i + (int64_t)n1 * ((int64_t)n2 + (int64_t)(n2 + 1) * k)] = 0;
+        } else {
+            fw[(int64_t)(e - bu - bv) + (int64_t)n1 * n2 * n3] = 0;  // i + n1 j on plane n3
+        }
+    }
+}
+
 // ---- layout conversions (natural <-> row-split) for the single-pass entry points ----
 template <class T, class S>
 __global__ void __launch_bounds__(TPB) k_to_split(Lev<float> L, T* __restrict__ dst, const S* __restrict__ src) {
