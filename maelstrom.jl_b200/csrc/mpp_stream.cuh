@@ -261,7 +261,7 @@ struct RbLd {
 // colour's x.
 template <class Pr>
 __device__ __forceinline__ void rbgs_fetch_s(const Lev<typename Pr::M>& L, int colour, uint32_t tile, int hq, int lj,
-                                             int lk, RbLd<typename Pr::M>& a) {
+                                             int lk, bool need_code, RbLd<typename Pr::M>& a) {
     const int h = (int)(tile & 1023u) * TH + hq * V8, j = (int)((tile >> 10) & 1023u) * TY + lj,
               k = (int)(tile >> 20) * TZ + lk;
     a.ok = h < L.H && j < L.n2 && k < L.n3;
@@ -269,7 +269,7 @@ __device__ __forceinline__ void rbgs_fetch_s(const Lev<typename Pr::M>& L, int c
     const int p = (k * L.n2 + j) * L.n1 + colour * L.H + h;
     a.p = p;
     a.ci = ci_of(colour, j, k);
-    a.cdw = *reinterpret_cast<const uint2*>(L.code + p);
+    if (need_code) a.cdw = *reinterpret_cast<const uint2*>(L.code + p);
     a.dv = ld8((Pr::scaled ? L.di : L.dg) + p);
     a.bv = ld8(L.b + p);
 }
@@ -287,13 +287,20 @@ __device__ __forceinline__ void rbgs_fetch_x(const Lev<typename Pr::M>& L, int c
     a.xr = L.x[o + V8];
 }
 
+// by_di: the 16-bit forms on a level with no LIQUID cell on its x/y faces, whose stencil
+// codes are not read. There the unmasked neighbour sum needs no code, and a cell is LIQUID
+// exactly when its stored reciprocal diagonal is nonzero: the set-up stores 0 off-liquid,
+// and a LIQUID cell's diagonal is at most 6 x 100 (theta >= 0.01), so its reciprocal is a
+// normal FP16 number. The one exception, a LIQUID cell with no open face (diagonal 0), gets
+// +0 where (b + s) * 0 could give -0.
 template <class C, class M>
-__device__ __forceinline__ Vec8<M> rbgs_tile(const RbLd<M>& cur, bool edge, bool scaled) {
+__device__ __forceinline__ Vec8<M> rbgs_tile(const RbLd<M>& cur, bool edge, bool scaled, bool by_di) {
     Vec8<M> out;
 #pragma unroll
     for (int q = 0; q < V8; q++) {
         // constant element indices only (selects), so the tile stays in registers
-        const uint8_t cd = (uint8_t)(((q < 4 ? cur.cdw.x : cur.cdw.y) >> (8 * (q & 3))) & 0xffu);
+        const uint8_t cd = by_di ? (uint8_t)(ld<C>(&cur.dv.v[q]) != (C)0 ? SELF : 0)
+                                 : (uint8_t)(((q < 4 ? cur.cdw.x : cur.cdw.y) >> (8 * (q & 3))) & 0xffu);
         const M xp = cur.ci ? (q + 1 < V8 ? cur.xc.v[q + 1 < V8 ? q + 1 : 0] : cur.xr) : cur.xc.v[q];
         const M xm = cur.ci ? cur.xc.v[q] : (q > 0 ? cur.xc.v[q > 0 ? q - 1 : 0] : cur.xl);
         C nb[6];
@@ -326,13 +333,14 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
     const int hq = lane % V8_LANES_H, lj = (lane / V8_LANES_H) % TY, lk = lane / (V8_LANES_H * TY);
     const int n = *L.count;  // tile lists and codes date from the set-up
     const bool edge = *L.edge != 0;
+    const bool by_di = Pr::scaled && !edge, need_code = !by_di;
     const int stride = gridDim.x * wpb;
     int t = blockIdx.x * wpb + warp;
     RbLd<M> cur;
     uint32_t tile1 = 0u;
     if (t < n) {
         tile1 = t + stride < n ? L.tiles[t + stride] : 0u;
-        rbgs_fetch_s<Pr>(L, colour, L.tiles[t], hq, lj, lk, cur);
+        rbgs_fetch_s<Pr>(L, colour, L.tiles[t], hq, lj, lk, need_code, cur);
     }
     pdl_wait();
     pdl_trigger();
@@ -346,16 +354,16 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
             RbLd<M> nxt;
             nxt.ok = false;
             if (t + stride < n) {
-                rbgs_fetch_s<Pr>(L, colour, tile1, hq, lj, lk, nxt);
+                rbgs_fetch_s<Pr>(L, colour, tile1, hq, lj, lk, need_code, nxt);
                 rbgs_fetch_x<Pr>(L, colour, nxt);
             }
-            if (cur.ok) st8(L.x + cur.p, rbgs_tile<C, M>(cur, edge, Pr::scaled));
+            if (cur.ok) st8(L.x + cur.p, rbgs_tile<C, M>(cur, edge, Pr::scaled, by_di));
             cur = nxt;
         } else {
-            if (cur.ok) st8(L.x + cur.p, rbgs_tile<C, M>(cur, edge, Pr::scaled));
+            if (cur.ok) st8(L.x + cur.p, rbgs_tile<C, M>(cur, edge, Pr::scaled, by_di));
             cur.ok = false;
             if (t + stride < n) {
-                rbgs_fetch_s<Pr>(L, colour, tile1, hq, lj, lk, cur);
+                rbgs_fetch_s<Pr>(L, colour, tile1, hq, lj, lk, need_code, cur);
                 rbgs_fetch_x<Pr>(L, colour, cur);
             }
         }
