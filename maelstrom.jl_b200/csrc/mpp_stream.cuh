@@ -812,6 +812,10 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     C(*S)[PY][PX] = smw[warp];
     const int n = *L.count, stride = gridDim.x * WPB;
+    constexpr int CH = 16 / (int)sizeof(M), NCHK = (TH / 2 + 2 * CH) / CH, NV = PY * PZ * 2 * NCHK,
+                  NVL = (NV + 31) / 32;
+    static_assert((TH / 2) % CH == 0, "pieces aligned to the tile's coarse columns");
+    const bool vec = !cnat && Cl.n1 % (2 * CH) == 0 && (reinterpret_cast<uintptr_t>(Cl.x) & 15) == 0;
     // the first tile id before the programmatic-dependent-launch wait (the tile lists date
     // from the set-up; the coarse x is the preceding kernel's output)
     int t = blockIdx.x * WPB + warp;
@@ -822,15 +826,33 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
         const uint32_t tile_next = t + stride < n ? L.tiles[t + stride] : 0u;
         const int I0 = (int)(tile & 1023u) * TH - 1, J0 = (int)((tile >> 10) & 1023u) * (TY / 2) - 1,
                   K0 = (int)(tile >> 20) * (TZ / 2) - 1;
+        const int ps = (int)(tile & 1023u) * (TH / 2) - CH;  // first piece's position
         C vals[PER];
+        Vec16<M> vv[NVL];
+        if (vec) {
+            // row-split coarse rows in 16-byte pieces: the region's natural columns I0 ..
+            // I0 + PX - 1 sit at positions (TH / 2) th - 1 .. (TH / 2)(th + 1) of each colour's
+            // half-row, covered by NCHK aligned pieces from (TH / 2) th - CH; a piece lies
+            // wholly inside [0, H) or wholly outside it (read as zeros)
 #pragma unroll
-        for (int u = 0; u < PER; u++) {
-            const int e = lane + 32 * u;
-            const int ii = e % PX, jj = (e / PX) % PY, kk = e / (PX * PY);
-            const int I = I0 + ii, J = J0 + jj, K = K0 + kk;
-            vals[u] = (C)0;
-            if (e < NE && I >= 0 && I < Cl.n1 && J >= 0 && J < Cl.n2 && K >= 0 && K < Cl.n3)
-                vals[u] = ld<C>(Cl.x + (cnat ? (int)Cl.nat(I, J, K) : (int)Cl.pos(I, J, K)));
+            for (int u = 0; u < NVL; u++) {
+                const int e = lane + 32 * u, rr = e / (2 * NCHK), rem = e - rr * 2 * NCHK;
+                const int c = rem / NCHK, ch = rem - c * NCHK;
+                const int J = J0 + rr % PY, K = K0 + rr / PY, pos0 = ps + ch * CH;
+                vv[u].u = make_uint4(0u, 0u, 0u, 0u);
+                if (e < NV && J >= 0 && J < Cl.n2 && K >= 0 && K < Cl.n3 && pos0 >= 0 && pos0 < Cl.H)
+                    vv[u].u = *reinterpret_cast<const uint4*>(Cl.x + (K * Cl.n2 + J) * Cl.n1 + c * Cl.H + pos0);
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < PER; u++) {
+                const int e = lane + 32 * u;
+                const int ii = e % PX, jj = (e / PX) % PY, kk = e / (PX * PY);
+                const int I = I0 + ii, J = J0 + jj, K = K0 + kk;
+                vals[u] = (C)0;
+                if (e < NE && I >= 0 && I < Cl.n1 && J >= 0 && J < Cl.n2 && K >= 0 && K < Cl.n3)
+                    vals[u] = ld<C>(Cl.x + (cnat ? (int)Cl.nat(I, J, K) : (int)Cl.pos(I, J, K)));
+            }
         }
         // this lane's fine cells, loaded beside the staging loads
         Lane8 a;
@@ -846,10 +868,25 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
             }
         }
         __syncwarp();
+        if (vec) {
 #pragma unroll
-        for (int u = 0; u < PER; u++) {
-            const int e = lane + 32 * u;
-            if (e < NE) (&S[0][0][0])[e] = vals[u];
+            for (int u = 0; u < NVL; u++) {
+                const int e = lane + 32 * u, rr = e / (2 * NCHK), rem = e - rr * 2 * NCHK;
+                const int c = rem / NCHK, ch = rem - c * NCHK;
+                const int jj = rr % PY, kk = rr / PY, par = (c + J0 + jj + K0 + kk + 1) & 1;
+                if (e >= NV) continue;
+#pragma unroll
+                for (int q = 0; q < CH; q++) {
+                    const int ii = 2 * (ps + ch * CH + q) + par - I0;  // natural column in the region
+                    if (ii >= 0 && ii < PX) S[kk][jj][ii] = ld<C>(&vv[u].m[q]);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < PER; u++) {
+                const int e = lane + 32 * u;
+                if (e < NE) (&S[0][0][0])[e] = vals[u];
+            }
         }
         __syncwarp();
         tile = tile_next;
@@ -863,21 +900,24 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
         for (int cc = 0; cc < 2; cc++) {
             const int p = a.rb + cc * L.H + a.h;
             const int ci = ci_of(cc, a.j, a.k);
+            // prolongweights of i = 2 (h + q) + ci: coarse columns h + q - 1 + ci and the next,
+            // weights by the parity ci alone; the 8 products (w_a w_b) w_c are exact dyadic
+            // numbers, formed once for the lane's cells of this colour
+            const C wa0 = ci ? (C)0.75f : (C)0.25f, wa1 = ci ? (C)0.25f : (C)0.75f;
+            C wt[8];
+#pragma unroll
+            for (int m = 0; m < 8; m++)
+                wt[m] = ((m & 1) ? wa1 : wa0) * ((m & 2) ? wb1 : wb0) * ((m & 4) ? wc1 : wc0);
+            const int abase = a.h - 1 + ci - I0;
 #pragma unroll
             for (int q = 0; q < V8; q++) {
                 const uint8_t cd = (uint8_t)(((q < 4 ? cdw[cc].x : cdw[cc].y) >> (8 * (q & 3))) & 0xffu);
                 if (!(cd & SELF)) continue;
-                const int i = 2 * (a.h + q) + ci;
-                int a0, a1;
-                C wa0, wa1;
-                pweights<C>(i, a0, wa0, a1, wa1);
-                a0 -= I0; a1 -= I0;
                 C s = (C)0;
 #pragma unroll
                 for (int m = 0; m < 8; m++) {
-                    const int A = (m & 1) ? a1 : a0, B = (m & 2) ? b1 : b0, K = (m & 4) ? k1 : k0;
-                    const C wa = (m & 1) ? wa1 : wa0, wb = (m & 2) ? wb1 : wb0, wc = (m & 4) ? wc1 : wc0;
-                    s += wa * wb * wc * S[K][B][A];
+                    const int A = abase + q + (m & 1), B = (m & 2) ? b1 : b0, K = (m & 4) ? k1 : k0;
+                    s += wt[m] * S[K][B][A];
                 }
                 st(&xv[cc].v[q], ld<C>(&xv[cc].v[q]) + (Pr::scaled ? (C)4 * s : s));
             }
