@@ -446,12 +446,13 @@ struct Run {
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
         beg(F_SETUP, -1);
         auto al = [](const void* q, uintptr_t a) { return (reinterpret_cast<uintptr_t>(q) & (a - 1)) == 0; };
-        // 8 cells of a row per thread, with 8- and 16-byte loads of the caller's classes and faces
-        if (c->grid.n[0] % 8 == 0 && al(in.types, 8) && (!in.v || al(in.v, 16)) && (!in.w || al(in.w, 16)) &&
-            al(in.P, 16) && (!in.phi || al(in.phi, 16)))
-            launch(k_setup_v8<Pr>, grid_cells(c, (N / 8) * TPB / SETUP_V8_TPB), SETUP_V8_TPB, 0, s, in, view<M>(c, 0),
-                   (V*)c->diag, (V*)c->bvec,
-                   (V*)c->r, c->sc, c->partials, cnt(CNT_SETUP), cond, use_cond);
+        // SETUP_W cells of a row per thread, with SETUP_W-byte loads of the caller's classes and
+        // 16-byte ones of its faces
+        if (c->grid.n[0] % SETUP_W == 0 && al(in.types, SETUP_W) && (!in.v || al(in.v, 16)) &&
+            (!in.w || al(in.w, 16)) && al(in.P, 16) && (!in.phi || al(in.phi, 16)))
+            launch(k_setup_v8<Pr, SETUP_W>, grid_cells(c, (N / SETUP_W) * TPB / SETUP_V8_TPB), SETUP_V8_TPB, 0, s, in,
+                   view<M>(c, 0), (V*)c->diag, (V*)c->bvec, (V*)c->r, c->sc, c->partials, cnt(CNT_SETUP), cond,
+                   use_cond);
         else
             launch(k_setup<Pr>, grid_cells(c, N), TPB, 0, s, in, view<M>(c, 0), (V*)c->diag, (V*)c->bvec, (V*)c->r,
                    c->sc, c->partials, cnt(CNT_SETUP), cond, use_cond);

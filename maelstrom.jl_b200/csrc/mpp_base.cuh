@@ -278,36 +278,38 @@ __global__ void __launch_bounds__(TPB)
 // classes, velocities and warm start come in as 8-wide row pieces, and the outputs leave
 // as 4-wide pieces of each colour's half of the row-split rows. Same arithmetic, in the
 // same order, as k_setup.
-template <class T>
-struct Row8 {
-    T v[8];
+template <class T, int W>
+struct RowW {
+    T v[W];
 };
-template <class T>
-__device__ __forceinline__ Row8<T> ld_row8(const T* p) {  // 8-element aligned
-    Row8<T> r;
-    constexpr int n = (int)(sizeof(T) * 8 / 16);
-    if constexpr (n == 0) {
-        *reinterpret_cast<uint2*>(r.v) = *reinterpret_cast<const uint2*>(p);
-    } else {
+// N-element pieces (aligned to their size) moved as one access of that size, or 16-byte ones.
+template <int BYTES>
+__device__ __forceinline__ void copy_piece(void* dst, const void* src) {
+    if constexpr (BYTES == 2) *reinterpret_cast<uint16_t*>(dst) = *reinterpret_cast<const uint16_t*>(src);
+    else if constexpr (BYTES == 4) *reinterpret_cast<uint32_t*>(dst) = *reinterpret_cast<const uint32_t*>(src);
+    else if constexpr (BYTES == 8) *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(src);
+    else {
+        static_assert(BYTES % 16 == 0, "pieces of 2, 4, 8 or a multiple of 16 bytes");
 #pragma unroll
-        for (int q = 0; q < n; q++) reinterpret_cast<uint4*>(r.v)[q] = reinterpret_cast<const uint4*>(p)[q];
+        for (int q = 0; q < BYTES / 16; q++)
+            reinterpret_cast<uint4*>(dst)[q] = reinterpret_cast<const uint4*>(src)[q];
     }
+}
+template <int W, class T>
+__device__ __forceinline__ RowW<T, W> ld_row(const T* p) {  // W-element aligned
+    RowW<T, W> r;
+    copy_piece<(int)sizeof(T) * W>(r.v, p);
     return r;
 }
-template <class T>
-__device__ __forceinline__ void st_quad(T* p, const T (&v)[4]) {  // 4-element aligned
-    if constexpr (sizeof(T) == 1) *reinterpret_cast<uint32_t*>(p) = *reinterpret_cast<const uint32_t*>(v);
-    else if constexpr (sizeof(T) == 2) *reinterpret_cast<uint2*>(p) = *reinterpret_cast<const uint2*>(v);
-    else if constexpr (sizeof(T) == 4) *reinterpret_cast<uint4*>(p) = *reinterpret_cast<const uint4*>(v);
-    else {
-        reinterpret_cast<uint4*>(p)[0] = reinterpret_cast<const uint4*>(v)[0];
-        reinterpret_cast<uint4*>(p)[1] = reinterpret_cast<const uint4*>(v)[1];
-    }
+template <int N, class T>
+__device__ __forceinline__ void st_piece(T* p, const T (&v)[N]) {  // N-element aligned
+    copy_piece<(int)sizeof(T) * N>(p, v);
 }
 
-// 128-thread blocks: at this kernel's register count, 12 warps a SM instead of 8.
-constexpr int SETUP_V8_TPB = 128;
-template <class Pr>
+// W = 4 or 8 cells of a row a thread; 128-thread blocks (at this kernel's register count
+// the finer-grained blocks fill more of each SM).
+constexpr int SETUP_V8_TPB = 128, SETUP_W = 4;
+template <class Pr, int W>
 __global__ void __launch_bounds__(SETUP_V8_TPB)
     k_setup_v8(SetupIn<typename Pr::V> a, Lev<typename Pr::M> L, typename Pr::V* __restrict__ diag,
                typename Pr::V* __restrict__ b, typename Pr::V* __restrict__ r, Scalars* sc, double* partials,
@@ -317,7 +319,7 @@ __global__ void __launch_bounds__(SETUP_V8_TPB)
     using V = typename Pr::V;
     using M = typename Pr::M;
     using C = typename Pr::C;
-    const int n1 = L.n1, n2 = L.n2, n3 = L.n3, nq = n1 / 8, sz = n1 * n2;
+    const int n1 = L.n1, n2 = L.n2, n3 = L.n3, nq = n1 / W, sz = n1 * n2;
     const C dx = (C)a.dx;
     const C gamma = (C)(sc->p.project ? sc->s.gamma : sc->p.gamma);
     const bool sep_dg = (void*)L.dg != (void*)diag;
@@ -325,46 +327,46 @@ __global__ void __launch_bounds__(SETUP_V8_TPB)
     double acc[3] = {0.0, 0.0, 0.0};
     const int nch = nq * n2 * n3;
     for (int ch = (int)(blockIdx.x * SETUP_V8_TPB + threadIdx.x); ch < nch; ch += (int)(gridDim.x * SETUP_V8_TPB)) {
-        const int q8 = ch % nq, rw = ch / nq, j = rw % n2, k = rw / n2, i0 = 8 * q8;
+        const int q8 = ch % nq, rw = ch / nq, j = rw % n2, k = rw / n2, i0 = W * q8;
         const int row = rw * n1, idx0 = row + i0;
-        Row8<uint8_t> tc = ld_row8(a.types + idx0), tym, typ, tzm, tzp;
+        RowW<uint8_t, W> tc = ld_row<W>(a.types + idx0), tym, typ, tzm, tzp;
 #pragma unroll
-        for (int m = 0; m < 8; m++) tym.v[m] = typ.v[m] = tzm.v[m] = tzp.v[m] = SOLID;
-        if (j > 0) tym = ld_row8(a.types + idx0 - n1);
-        if (j + 1 < n2) typ = ld_row8(a.types + idx0 + n1);
-        if (k > 0) tzm = ld_row8(a.types + idx0 - sz);
-        if (k + 1 < n3) tzp = ld_row8(a.types + idx0 + sz);
+        for (int m = 0; m < W; m++) tym.v[m] = typ.v[m] = tzm.v[m] = tzp.v[m] = SOLID;
+        if (j > 0) tym = ld_row<W>(a.types + idx0 - n1);
+        if (j + 1 < n2) typ = ld_row<W>(a.types + idx0 + n1);
+        if (k > 0) tzm = ld_row<W>(a.types + idx0 - sz);
+        if (k + 1 < n3) tzp = ld_row<W>(a.types + idx0 + sz);
         const uint8_t txm = i0 > 0 ? a.types[idx0 - 1] : (uint8_t)SOLID;
-        const uint8_t txp = i0 + 8 < n1 ? a.types[idx0 + 8] : (uint8_t)SOLID;
+        const uint8_t txp = i0 + W < n1 ? a.types[idx0 + W] : (uint8_t)SOLID;
         bool any = false;
 #pragma unroll
-        for (int m = 0; m < 8; m++) any |= tc.v[m] == LIQUID;
-        uint8_t code[8];
-        C d[8], bv[8], rv[8];
+        for (int m = 0; m < W; m++) any |= tc.v[m] == LIQUID;
+        uint8_t code[W];
+        C d[W], bv[W], rv[W];
 #pragma unroll
-        for (int m = 0; m < 8; m++) {
+        for (int m = 0; m < W; m++) {
             code[m] = 0;
             d[m] = bv[m] = rv[m] = (C)0;
         }
         if (any) {
             // rhs inputs (aligned rows of v and w; u rows are n1 + 1 long: element loads)
-            Row8<float> vlo, vhi, wlo, whi;
-            float ur[9];
+            RowW<float, W> vlo, vhi, wlo, whi;
+            float ur[W + 1];
             const bool rhs = !a.bnat64 && !a.bnat && a.u;
             if (rhs) {
                 const int ub = (n1 + 1) * (j + n2 * k) + i0;
 #pragma unroll
-                for (int m = 0; m < 9; m++) ur[m] = a.u[ub + m];
-                vlo = ld_row8(a.v + (int64_t)n1 * (j + (n2 + 1) * k) + i0);
-                vhi = ld_row8(a.v + (int64_t)n1 * (j + 1 + (n2 + 1) * k) + i0);
-                wlo = ld_row8(a.w + idx0);
-                whi = ld_row8(a.w + idx0 + sz);
+                for (int m = 0; m < W + 1; m++) ur[m] = a.u[ub + m];
+                vlo = ld_row<W>(a.v + (int64_t)n1 * (j + (n2 + 1) * k) + i0);
+                vhi = ld_row<W>(a.v + (int64_t)n1 * (j + 1 + (n2 + 1) * k) + i0);
+                wlo = ld_row<W>(a.w + idx0);
+                whi = ld_row<W>(a.w + idx0 + sz);
             }
 #pragma unroll
-            for (int m = 0; m < 8; m++) {
+            for (int m = 0; m < W; m++) {
                 if (tc.v[m] != LIQUID) continue;
                 const int i = i0 + m, idx = idx0 + m;
-                const uint8_t tn[6] = {m < 7 ? tc.v[m < 7 ? m + 1 : 0] : txp, m > 0 ? tc.v[m > 0 ? m - 1 : 0] : txm,
+                const uint8_t tn[6] = {m < W - 1 ? tc.v[m < W - 1 ? m + 1 : 0] : txp, m > 0 ? tc.v[m > 0 ? m - 1 : 0] : txm,
                                        typ.v[m], tym.v[m], tzp.v[m], tzm.v[m]};
                 const int off[6] = {1, -1, n1, -n1, sz, -sz};
                 C dd = (C)0;
@@ -409,7 +411,7 @@ __global__ void __launch_bounds__(SETUP_V8_TPB)
         }
         if (a.clear_P) {
 #pragma unroll
-            for (int m = 0; m < 8; m++)
+            for (int m = 0; m < W; m++)
                 if (tc.v[m] != LIQUID) a.P[idx0 + m] = (V)0;
         }
         // the two colours' halves: colour c holds the cells m = p, p + 2, p + 4, p + 6
@@ -417,16 +419,16 @@ __global__ void __launch_bounds__(SETUP_V8_TPB)
         for (int c = 0; c < 2; c++) {
             const int p0 = (c + j + k + 1) & 1;
             const int pos = row + c * L.H + i0 / 2;
-            uint8_t cq[4];
-            V dq[4], bq[4], rq[4];
-            M gq[4], iq[4], lq[4];
+            uint8_t cq[W / 2];
+            V dq[W / 2], bq[W / 2], rq[W / 2];
+            M gq[W / 2], iq[W / 2], lq[W / 2];
 #pragma unroll
-            for (int s2 = 0; s2 < 4; s2++) {
+            for (int s2 = 0; s2 < W / 2; s2++) {
                 const int m = p0 + 2 * s2;  // p0 is 0 or 1: pick by select, not by index
-                const uint8_t cm = p0 ? code[(2 * s2 + 1) & 7] : code[2 * s2];
-                const C dm = p0 ? d[(2 * s2 + 1) & 7] : d[2 * s2];
-                const C bm = p0 ? bv[(2 * s2 + 1) & 7] : bv[2 * s2];
-                const C rm = p0 ? rv[(2 * s2 + 1) & 7] : rv[2 * s2];
+                const uint8_t cm = p0 ? code[(2 * s2 + 1) & (W - 1)] : code[2 * s2];
+                const C dm = p0 ? d[(2 * s2 + 1) & (W - 1)] : d[2 * s2];
+                const C bm = p0 ? bv[(2 * s2 + 1) & (W - 1)] : bv[2 * s2];
+                const C rm = p0 ? rv[(2 * s2 + 1) & (W - 1)] : rv[2 * s2];
                 (void)m;
                 cq[s2] = cm;
                 st(&dq[s2], dm);
@@ -440,14 +442,14 @@ __global__ void __launch_bounds__(SETUP_V8_TPB)
                     acc[1] += (double)rm * (double)rm;
                 }
             }
-            st_quad(L.code + pos, cq);
-            st_quad(diag + pos, dq);
-            if (sep_dg) st_quad(L.dg + pos, gq);
-            if (L.di) st_quad(L.di + pos, iq);
-            st_quad(b + pos, bq);
+            st_piece<W / 2>(L.code + pos, cq);
+            st_piece<W / 2>(diag + pos, dq);
+            if (sep_dg) st_piece<W / 2>(L.dg + pos, gq);
+            if (L.di) st_piece<W / 2>(L.di + pos, iq);
+            st_piece<W / 2>(b + pos, bq);
             if (a.residual) {
-                st_quad(r + pos, rq);
-                if (sep_b) st_quad(L.b + pos, lq);
+                st_piece<W / 2>(r + pos, rq);
+                if (sep_b) st_piece<W / 2>(L.b + pos, lq);
             }
         }
     }
