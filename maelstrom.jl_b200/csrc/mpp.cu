@@ -482,7 +482,9 @@ struct Run {
         end();
     }
 
-    void smooth(int l, const std::vector<int>& colours) {
+    // b_late: the first pass follows a kernel that wrote the level's b (the restriction
+    // with the level's start fused in)
+    void smooth(int l, const std::vector<int>& colours, bool b_late = false) {
         for (int col : colours) {
             beg(F_RBGS, l);
             if (form(l) == MPP_SMOOTHER_TMA && c->tma_ok[l]) {
@@ -493,7 +495,8 @@ struct Run {
                 const int wpb = TPB / 32, cap = c->nsm * RBGS_V8_BLOCKS;
                 int g = (c->lv[l].ntiles + wpb - 1) / wpb;
                 g = g < cap ? (g > 0 ? g : 1) : cap;
-                launch(k_rbgs_v8<Pr>, g, TPB, 0, s, view<M>(c, l), col);
+                launch(k_rbgs_v8<Pr>, g, TPB, 0, s, view<M>(c, l), col, b_late ? 1 : 0);
+                b_late = false;
             } else {
                 launch(k_rbgs<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l), col);
             }
@@ -516,18 +519,21 @@ struct Run {
         const int lb = c->lb;
         const int ls = c->cmg_ls > 0 ? c->cmg_ls : lb;  // levels ls .. lb-1 in the cluster
         for (int l = 0; l < ls; l++) {
-            beg(F_START, l);
-            if (vec(l)) launch(k_start_v8<Pr>, grid_res((const void*)k_start_v8<Pr>, l), TPB, 0, s, view<M>(c, l));
-            else launch(k_start<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
-            end();
-            smooth(l, l == 0 ? down0 : down);
+            if (l == 0) {  // the coarser levels' starts ride on the restriction into them
+                beg(F_START, l);
+                if (vec(l)) launch(k_start_v8<Pr>, grid_res((const void*)k_start_v8<Pr>, l), TPB, 0, s, view<M>(c, l));
+                else launch(k_start<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
+                end();
+            }
+            smooth(l, l == 0 ? down0 : down, l > 0);
             beg(F_RESID, l);
             if (vec(l)) launch(k_residual_v8<Pr>, grid_res((const void*)k_residual_v8<Pr>, l), TPB, 0, s, view<M>(c, l));
             else launch(k_residual<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
             end();
             if (l + 1 < lb) {
                 beg(F_RESTRICT, l + 1);
-                launch(k_restrict<Pr>, grid_tiles1(c, l + 1), TPB, c->restrict_smem, s, view<M>(c, l), view<M>(c, l + 1));
+                launch(k_restrict<Pr>, grid_tiles1(c, l + 1), TPB, c->restrict_smem, s, view<M>(c, l), view<M>(c, l + 1),
+                       l + 1 < ls ? 1 : 0);
                 end();
             }
         }

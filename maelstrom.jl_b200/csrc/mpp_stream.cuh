@@ -247,7 +247,8 @@ __device__ __forceinline__ void st8(T* p, const Vec8<T>& r) {
 // per SM hold both tiles' registers, and the grid is exactly that many blocks. Before its
 // programmatic-dependent-launch wait, a warp already loads its first tile's id, code,
 // diagonal and b: the preceding kernel (a colour pass, start or prolongation) writes only
-// x, and everything older is complete once that kernel has passed its own wait.
+// x, and everything older is complete once that kernel has passed its own wait. After a
+// restriction that also started the level (b_late), b waits too.
 template <class M>
 struct RbLd {
     uint2 cdw;
@@ -261,7 +262,7 @@ struct RbLd {
 // colour's x.
 template <class Pr>
 __device__ __forceinline__ void rbgs_fetch_s(const Lev<typename Pr::M>& L, int colour, uint32_t tile, int hq, int lj,
-                                             int lk, bool need_code, RbLd<typename Pr::M>& a) {
+                                             int lk, bool need_code, bool with_b, RbLd<typename Pr::M>& a) {
     const int h = (int)(tile & 1023u) * TH + hq * V8, j = (int)((tile >> 10) & 1023u) * TY + lj,
               k = (int)(tile >> 20) * TZ + lk;
     a.ok = h < L.H && j < L.n2 && k < L.n3;
@@ -271,11 +272,12 @@ __device__ __forceinline__ void rbgs_fetch_s(const Lev<typename Pr::M>& L, int c
     a.ci = ci_of(colour, j, k);
     if (need_code) a.cdw = *reinterpret_cast<const uint2*>(L.code + p);
     a.dv = ld8((Pr::scaled ? L.di : L.dg) + p);
-    a.bv = ld8(L.b + p);
+    if (with_b) a.bv = ld8(L.b + p);
 }
 template <class Pr>
-__device__ __forceinline__ void rbgs_fetch_x(const Lev<typename Pr::M>& L, int colour, RbLd<typename Pr::M>& a) {
+__device__ __forceinline__ void rbgs_fetch_x(const Lev<typename Pr::M>& L, int colour, bool with_b, RbLd<typename Pr::M>& a) {
     if (!a.ok) return;
+    if (with_b) a.bv = ld8(L.b + a.p);
     const int sy = L.n1, sz = L.n1 * L.n2;
     const int o = a.p + (1 - 2 * colour) * L.H;  // the same columns in the other colour's half
     a.xc = ld8(L.x + o);
@@ -325,7 +327,7 @@ __device__ __forceinline__ Vec8<M> rbgs_tile(const RbLd<M>& cur, bool edge, bool
 // The 16-bit forms keep two tiles in flight; the 4- and 8-byte forms (twice the registers
 // a tile) one.
 template <class Pr>
-__device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) {
+__device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour, int b_late) {
     using C = typename Pr::C;
     using M = typename Pr::M;
     constexpr bool PIPE = sizeof(M) <= 2;
@@ -340,12 +342,12 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
     uint32_t tile1 = 0u;
     if (t < n) {
         tile1 = t + stride < n ? L.tiles[t + stride] : 0u;
-        rbgs_fetch_s<Pr>(L, colour, L.tiles[t], hq, lj, lk, need_code, cur);
+        rbgs_fetch_s<Pr>(L, colour, L.tiles[t], hq, lj, lk, need_code, !b_late, cur);
     }
     pdl_wait();
     pdl_trigger();
     if (t >= n) return;
-    rbgs_fetch_x<Pr>(L, colour, cur);
+    rbgs_fetch_x<Pr>(L, colour, b_late != 0, cur);
     for (; t < n; t += stride) {
         const uint32_t tile2 = t + 2 * stride < n ? L.tiles[t + 2 * stride] : 0u;
         if constexpr (PIPE) {
@@ -354,8 +356,8 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
             RbLd<M> nxt;
             nxt.ok = false;
             if (t + stride < n) {
-                rbgs_fetch_s<Pr>(L, colour, tile1, hq, lj, lk, need_code, nxt);
-                rbgs_fetch_x<Pr>(L, colour, nxt);
+                rbgs_fetch_s<Pr>(L, colour, tile1, hq, lj, lk, need_code, true, nxt);
+                rbgs_fetch_x<Pr>(L, colour, false, nxt);
             }
             if (cur.ok) st8(L.x + cur.p, rbgs_tile<C, M>(cur, edge, Pr::scaled, by_di));
             cur = nxt;
@@ -363,8 +365,8 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
             if (cur.ok) st8(L.x + cur.p, rbgs_tile<C, M>(cur, edge, Pr::scaled, by_di));
             cur.ok = false;
             if (t + stride < n) {
-                rbgs_fetch_s<Pr>(L, colour, tile1, hq, lj, lk, need_code, cur);
-                rbgs_fetch_x<Pr>(L, colour, cur);
+                rbgs_fetch_s<Pr>(L, colour, tile1, hq, lj, lk, need_code, true, cur);
+                rbgs_fetch_x<Pr>(L, colour, false, cur);
             }
         }
         tile1 = tile2;
@@ -374,8 +376,8 @@ __device__ __forceinline__ void rbgs_v8_body(Lev<typename Pr::M> L, int colour) 
 // (two of 256 threads at up to 128 registers a thread)
 constexpr int RBGS_V8_BLOCKS = 2;
 template <class Pr>
-__global__ void __launch_bounds__(TPB, RBGS_V8_BLOCKS) k_rbgs_v8(Lev<typename Pr::M> L, int colour) {
-    rbgs_v8_body<Pr>(L, colour);
+__global__ void __launch_bounds__(TPB, RBGS_V8_BLOCKS) k_rbgs_v8(Lev<typename Pr::M> L, int colour, int b_late) {
+    rbgs_v8_body<Pr>(L, colour, b_late);
 }
 
 // A lane's 8 columns in a tile (vector kernels): h .. h+7 of row j, plane k.
@@ -767,8 +769,11 @@ __global__ void __launch_bounds__(TPB, 3)
             Vec8<V> dd = ld8(dvec + p), rr = ld8(r + p);
             const Vec8<V> qq = ld8(qv + p);
             const uint8_t* cd = reinterpret_cast<const uint8_t*>(&cdw);
+            // the V-cycle's right-hand side is written whole: zero off-liquid, which is what it
+            // holds there (the set-up writes zeros, every later writer only LIQUID cells)
             Vec8<M> rbv;
-            if (sep_b) rbv = ld8(L.b + p);
+#pragma unroll
+            for (int q = 0; q < V8; q++) st(&rbv.v[q], (C)0);
 #pragma unroll
             for (int q = 0; q < V8; q++) {
                 if (!(cd[q] & SELF)) continue;
@@ -778,8 +783,6 @@ __global__ void __launch_bounds__(TPB, 3)
                 st(&rr.v[q], rl);
                 if (sep_b) st(&rbv.v[q], rl * rsc);
                 // the cell's place in the natural run: 2q + ci (compile-time index per branch)
-                constexpr int dummy = 0;
-                (void)dummy;
                 if (ci == 0) {
                     V& Pi = (2 * q < V8) ? P0.v[(2 * q) % V8] : P1.v[(2 * q) % V8];
                     st(&Pi, (C)Pi + alpha * pc);

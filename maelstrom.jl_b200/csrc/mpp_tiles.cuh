@@ -125,7 +125,7 @@ union Vec16 {
 };
 
 template <class Pr>
-__device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typename Pr::M> L) {
+__device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typename Pr::M> L, int start) {
     using C = typename Pr::C;
     extern __shared__ __align__(128) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
@@ -214,6 +214,19 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
                     v = Pr::scaled ? s : (C)4 * s;
                 }
                 st(L.b + p, v);
+                if (start) {
+                    // start_kernel! on the coarse level, fused: x = b / diag on its colour-0
+                    // LIQUID cells (b as stored, in the level's element type), 0 elsewhere
+                    C xv = (C)0;
+                    if (cc == 0 && (L.code[p] & SELF)) {
+                        M bm;
+                        st(&bm, v);
+                        const C bb = ld<C>(&bm), d = ld<C>((Pr::scaled ? L.di : L.dg) + p);
+                        if constexpr (Pr::scaled) xv = bb * d;
+                        else xv = d > (C)0 ? bb / d : (C)0;
+                    }
+                    st(L.x + p, xv);
+                }
             }
         }
     }
@@ -221,10 +234,10 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
 // Shared memory of k_restrict (elements of C): the staged rows.
 __host__ __device__ constexpr int restrict_smem_elems(bool) { return R_ROWS * R_W; }
 template <class Pr>
-__global__ void __launch_bounds__(TPB, 4) k_restrict(Lev<typename Pr::M> F, Lev<typename Pr::M> L) {
+__global__ void __launch_bounds__(TPB, 4) k_restrict(Lev<typename Pr::M> F, Lev<typename Pr::M> L, int start) {
     pdl_wait();
     pdl_trigger();
-    restrict_body<Pr>(F, L);
+    restrict_body<Pr>(F, L, start);
 }
 
 // prolongweights (src/flip.jl:908-911), 0-based.
