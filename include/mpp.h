@@ -221,7 +221,7 @@ typedef struct {
 } mpp_tune_entry;
 /* Time the basin's own pressure solve (rhs from u, v, w; zero start; the context's tol and
  * precision): first every fine x coarse smoother form at the context's sweeps, then with the
- * fastest forms fine sweeps 1..5 x coarse-level sweeps 1..4 (and, in the 16-bit forms, 10
+ * fastest forms fine sweeps 1..6 x coarse-level sweeps 1..8 (and, in the 16-bit forms, 10
  * instead of 40 coarsest sweeps); keep the fastest that converges on
  * the context, and return the number of candidates tried (table[0..capacity) gets them,
  * *chosen the winner's index, -1 when none converged). Allocates two trial arrays for

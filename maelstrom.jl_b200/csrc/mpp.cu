@@ -1908,8 +1908,8 @@ int mpp_autotune(mpp_ctx* c, const float* u, const float* v, const float* w, con
         // 2: with those forms, the fine and coarse sweeps and (16-bit forms: the FP32 form
         // keeps the reference's V-cycle) 10 instead of 40 coarsest sweeps
         const bool half = c->prec == MPP_PREC_MIXED_FP16 || c->prec == MPP_PREC_MIXED_BF16;
-        for (int sw = 1; sw <= 5; sw++)
-            for (int swc = 1; swc <= 4; swc++)
+        for (int sw = 1; sw <= 6; sw++)  // at most 9 + 96 candidates in all
+            for (int swc = 1; swc <= 8; swc++)
                 for (int csw : {csw0, 10}) {
                     if (csw == 10 && (!half || csw0 == 10)) continue;
                     if (sw == sw0 && swc == (swc0 > 0 ? swc0 : sw0) && csw == csw0) continue;  // tried in 1
