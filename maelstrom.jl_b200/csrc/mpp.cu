@@ -130,6 +130,9 @@ struct mpp_ctx {
     GraphEntry gc[NGRAPHS];
     uint64_t gclock;
     cudaStream_t cap;  // stream the graphs are captured on (never the caller's)
+    // second stream for the coarse levels' set-up, beside the fine set-up pass
+    cudaStream_t aux;
+    cudaEvent_t ev_fork, ev_join;
     // levels lb .. L-1 are solved in one CTA's shared memory (k_bottom)
     int lb;
     BotArgs bot;
@@ -443,6 +446,23 @@ struct Run {
             cudaMemsetAsync(c->lv[l].r, 0, ms * Nl, s);
             if (l > 0) cudaMemsetAsync(c->lv[l].x, 0, ms * Nl, s);
         }
+        // The coarse levels need only the classes: they are built on a second stream beside
+        // the fine set-up pass, joined before the tile lists.
+        const cudaStream_t s0 = s;
+        cudaEventRecord(c->ev_fork, s);
+        cudaStreamWaitEvent(c->aux, c->ev_fork, 0);
+        s = c->aux;
+        for (int l = 1; l < c->L; l++) {
+            const LevelBuf& f = c->lv[l - 1];
+            const uint8_t* tf = l == 1 ? in.types : f.types;
+            const int64_t Nl = (int64_t)c->lv[l].n[0] * c->lv[l].n[1] * c->lv[l].n[2];
+            beg(F_LEVEL, l);
+            launch(k_level<Pr>, grid_cells(c, Nl), TPB, 0, s, tf, f.n[0], f.n[1], f.n[2], view<M>(c, l),
+                                                           c->lv[l].split ? 1 : 0);
+            end();
+        }
+        cudaEventRecord(c->ev_join, c->aux);
+        s = s0;
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
         beg(F_SETUP, -1);
         auto al = [](const void* q, uintptr_t a) { return (reinterpret_cast<uintptr_t>(q) & (a - 1)) == 0; };
@@ -457,15 +477,7 @@ struct Run {
             launch(k_setup<Pr>, grid_cells(c, N), TPB, 0, s, in, view<M>(c, 0), (V*)c->diag, (V*)c->bvec, (V*)c->r,
                    c->sc, c->partials, cnt(CNT_SETUP), cond, use_cond);
         end();
-        for (int l = 1; l < c->L; l++) {
-            const LevelBuf& f = c->lv[l - 1];
-            const uint8_t* tf = l == 1 ? in.types : f.types;
-            const int64_t Nl = (int64_t)c->lv[l].n[0] * c->lv[l].n[1] * c->lv[l].n[2];
-            beg(F_LEVEL, l);
-            launch(k_level<Pr>, grid_cells(c, Nl), TPB, 0, s, tf, f.n[0], f.n[1], f.n[2], view<M>(c, l),
-                                                           c->lv[l].split ? 1 : 0);
-            end();
-        }
+        cudaStreamWaitEvent(s, c->ev_join, 0);
         TileTab tab;
         memset(&tab, 0, sizeof(tab));
         tab.nlev = c->lb;
@@ -1311,6 +1323,9 @@ int mpp_ctx_destroy(mpp_ctx* c) {
     if (c->sc_host) cudaFreeHost(c->sc_host);
     if (c->fgd_host) cudaFreeHost(c->fgd_host);
     if (c->cap) cudaStreamDestroy(c->cap);
+    if (c->aux) cudaStreamDestroy(c->aux);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     for (cudaEvent_t e : c->evall) cudaEventDestroy(e);
     delete c;
     return MPP_OK;
@@ -1376,6 +1391,8 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
     c->launches = 0;
     c->sc_host = nullptr;
     c->cap = nullptr;
+    c->aux = nullptr;
+    c->ev_fork = c->ev_join = nullptr;
     c->prof_on = 0;
     memset(c->prof, 0, sizeof(c->prof));
     memset(c->active, 0, sizeof(c->active));
@@ -1538,6 +1555,9 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
     }
     memset(c->sc_host, 0, sizeof(Scalars));
     ce = cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (ce != cudaSuccess) {
         set_err("cudaStreamCreate: %s", cudaGetErrorString(ce));
         return fail(MPP_ERR_CUDA);
