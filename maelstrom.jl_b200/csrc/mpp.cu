@@ -720,10 +720,19 @@ void record_epilogue(Run<Pr>& run, const Call& k) {
     using V = typename Pr::V;
     mpp_ctx* c = run.c;
     V* P = std::is_same<V, double>::value ? (V*)c->Pd : (V*)k.P;
+    // the true residual (read only for the result and the fallback decision) on the second
+    // stream, beside the gradient update; both only read the final P
+    const cudaStream_t s0 = run.s;
+    cudaEventRecord(c->ev_fork, s0);
+    cudaStreamWaitEvent(c->aux, c->ev_fork, 0);
+    run.s = c->aux;
     run.true_residual(P);
+    cudaEventRecord(c->ev_join, c->aux);
+    run.s = s0;
     if (std::is_same<V, double>::value) run.narrow(k.P);
     // with the fallback on, the gradient waits for the host's fallback decision
     if (k.kind == 1 && !c->opts.fallback) run.gradient(k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.types, k.phi);
+    cudaStreamWaitEvent(s0, c->ev_join, 0);
 }
 
 // ---- the FGMRES fallback (src/fgmres.jl:26-110, restated for the dense operator) ----
