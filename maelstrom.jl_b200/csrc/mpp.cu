@@ -129,10 +129,14 @@ struct mpp_ctx {
     // call alternate in a rollout without re-capturing)
     GraphEntry gc[NGRAPHS];
     uint64_t gclock;
+    uint64_t gen;  // bumped whenever the captured solves are dropped (options, smoothers)
     cudaStream_t cap;  // stream the graphs are captured on (never the caller's)
-    // second stream for the coarse levels' set-up, beside the fine set-up pass
+    // second stream for the coarse levels' set-up, beside the fine set-up pass, and for the
+    // true residual beside the gradient; not used by a batch's contexts (whose graph already
+    // runs every basin's solve side by side: measured, the extra branches cost throughput)
     cudaStream_t aux;
     cudaEvent_t ev_fork, ev_join;
+    bool in_batch;
     // levels lb .. L-1 are solved in one CTA's shared memory (k_bottom)
     int lb;
     BotArgs bot;
@@ -449,9 +453,12 @@ struct Run {
         // The coarse levels need only the classes: they are built on a second stream beside
         // the fine set-up pass, joined before the tile lists.
         const cudaStream_t s0 = s;
-        cudaEventRecord(c->ev_fork, s);
-        cudaStreamWaitEvent(c->aux, c->ev_fork, 0);
-        s = c->aux;
+        const bool fork = !c->in_batch;
+        if (fork) {
+            cudaEventRecord(c->ev_fork, s);
+            cudaStreamWaitEvent(c->aux, c->ev_fork, 0);
+            s = c->aux;
+        }
         for (int l = 1; l < c->L; l++) {
             const LevelBuf& f = c->lv[l - 1];
             const uint8_t* tf = l == 1 ? in.types : f.types;
@@ -461,7 +468,7 @@ struct Run {
                                                            c->lv[l].split ? 1 : 0);
             end();
         }
-        cudaEventRecord(c->ev_join, c->aux);
+        if (fork) cudaEventRecord(c->ev_join, c->aux);
         s = s0;
         const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
         beg(F_SETUP, -1);
@@ -477,7 +484,7 @@ struct Run {
             launch(k_setup<Pr>, grid_cells(c, N), TPB, 0, s, in, view<M>(c, 0), (V*)c->diag, (V*)c->bvec, (V*)c->r,
                    c->sc, c->partials, cnt(CNT_SETUP), cond, use_cond);
         end();
-        cudaStreamWaitEvent(s, c->ev_join, 0);
+        if (fork) cudaStreamWaitEvent(s, c->ev_join, 0);
         TileTab tab;
         memset(&tab, 0, sizeof(tab));
         tab.nlev = c->lb;
@@ -723,16 +730,19 @@ void record_epilogue(Run<Pr>& run, const Call& k) {
     // the true residual (read only for the result and the fallback decision) on the second
     // stream, beside the gradient update; both only read the final P
     const cudaStream_t s0 = run.s;
-    cudaEventRecord(c->ev_fork, s0);
-    cudaStreamWaitEvent(c->aux, c->ev_fork, 0);
-    run.s = c->aux;
+    const bool fork = !c->in_batch;
+    if (fork) {
+        cudaEventRecord(c->ev_fork, s0);
+        cudaStreamWaitEvent(c->aux, c->ev_fork, 0);
+        run.s = c->aux;
+    }
     run.true_residual(P);
-    cudaEventRecord(c->ev_join, c->aux);
+    if (fork) cudaEventRecord(c->ev_join, c->aux);
     run.s = s0;
     if (std::is_same<V, double>::value) run.narrow(k.P);
     // with the fallback on, the gradient waits for the host's fallback decision
     if (k.kind == 1 && !c->opts.fallback) run.gradient(k.u, k.v, k.w, k.fu, k.fv, k.fw, k.P, k.types, k.phi);
-    cudaStreamWaitEvent(s0, c->ev_join, 0);
+    if (fork) cudaStreamWaitEvent(s0, c->ev_join, 0);
 }
 
 // ---- the FGMRES fallback (src/fgmres.jl:26-110, restated for the dense operator) ----
@@ -1018,6 +1028,7 @@ int graph_for(mpp_ctx* c, const Call& k, GraphEntry*& out) {
 
 void drop_graphs(mpp_ctx* c) {
     for (GraphEntry& e : c->gc) drop_graph(e);
+    c->gen++;  // a batch's graph over this context is stale too
 }
 
 template <class Pr>
@@ -1396,12 +1407,14 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
     c->diag = c->bvec = c->r = c->d = c->q = c->Pd = nullptr;
     memset(c->gc, 0, sizeof(c->gc));
     c->gclock = 0;
+    c->gen = 0;
     c->bytes = 0;
     c->launches = 0;
     c->sc_host = nullptr;
     c->cap = nullptr;
     c->aux = nullptr;
     c->ev_fork = c->ev_join = nullptr;
+    c->in_batch = false;
     c->prof_on = 0;
     memset(c->prof, 0, sizeof(c->prof));
     memset(c->active, 0, sizeof(c->active));
@@ -1738,6 +1751,7 @@ int mpp_batch_create(mpp_batch** out, int count, const mpp_grid* grids, const mp
             delete b;
             return e;
         }
+        c->in_batch = true;
         b->ctx.push_back(c);
     }
     *out = b;
@@ -1785,8 +1799,9 @@ int mpp_batch_project(mpp_batch* b, const mpp_basin_arrays* basins, double dt, d
             set_err("basin %d: null array or zero volume0", i);
             return MPP_ERR_INVALID;
         }
-        const void* k[9] = {a.u, a.v, a.w, a.fu, a.fv, a.fw, a.P, a.types, a.phi};
-        key.insert(key.end(), k, k + 9);
+        const void* k[10] = {a.u, a.v, a.w, a.fu, a.fv, a.fw, a.P, a.types, a.phi,
+                             reinterpret_cast<const void*>((uintptr_t)b->ctx[i]->gen)};
+        key.insert(key.end(), k, k + 10);
     }
     std::vector<int64_t> launches0(n);
     for (int i = 0; i < n; i++) {
