@@ -4,7 +4,7 @@
 // diagonal, the stencil code) and the other colour's x with a one-cell halo. Issued as
 // plain loads, each thread waits on a chain of dependent loads (tile id -> codes ->
 // data) and HBM stays mostly idle. Here one thread per CTA moves whole tiles into shared
-// memory with cp.async.bulk.tensor (no multicast), S tiles ahead of the 256 threads that
+// memory with cp.async.bulk.tensor (into its own CTA only), S tiles ahead of the 256 threads that
 // compute, so every SM keeps tens of kilobytes of loads in flight.
 //
 // Tensor maps view a row-split level array as 4-D (h, colour, j, k) with h innermost.
