@@ -371,6 +371,8 @@ def run_mpp(args):
         out["adjoint"] = bench_adjoint(max(3, min(args.steps, 10)))
         torch.cuda.empty_cache()
         out["whirlpool384"] = bench_whirlpool(max(3, min(args.steps, 10)))
+        torch.cuda.empty_cache()
+        out["extrapolate"] = bench_extrapolate(max(3, min(args.steps, 10)))
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(basin, max_seconds=args.cpu_seconds)
     if rank == 0:
@@ -514,6 +516,49 @@ def bench_adjoint(steps):
                                   "checkpoints_bytes": sum(c.numel() * 4 for ck in ro.ckpt for c in ck),
                                   "grad_finite": bool(all(torch.isfinite(a).all() for a in g))}
     return out
+
+
+def bench_extrapolate(steps):
+    """extrapolate!(s; layers = 6) after the 256^3 whirlpool's projection, as step! runs it
+    (src/flip.jl:1403-1404): ms a call and HBM GB/s at 10 algorithmic bytes a face a layer
+    (the value and flag read, the value and flag written; neighbours come through the
+    caches). The projected arrays are restored before each call, outside the timed events;
+    the 3 x 253 MB of faces and flags are larger than L2."""
+    import torch
+
+    import mpp
+    from mpp import scene
+
+    b = scene.config_basin("whirl256")
+    s = mpp.FlipBasin.from_scene(b, tol=TOL, maxiter=MAXITER, precision="fp16", graph=True)
+    mpp.project(s, DT)
+    arrs = (s.u, s.v, s.w, s.fu, s.fv, s.fw)
+    saved = [a.clone() for a in arrs]
+    layers = 6
+
+    def call():
+        for a, x in zip(arrs, saved):
+            a.copy_(x)
+        e0, e1 = _events()
+        e0.record()
+        s.projector.extrapolate(*arrs, layers=layers)
+        e1.record()
+        return e0, e1
+
+    for _ in range(3):
+        call()
+    ev = [call() for _ in range(steps)]
+    torch.cuda.synchronize()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev) / steps
+    faces = sum(int(a.numel()) for a in (s.u, s.v, s.w))
+    reached = sum(int(torch.count_nonzero(f)) for f in (s.fu, s.fv, s.fw))
+    flagged = sum(int(torch.count_nonzero(f)) for f in saved[3:])
+    hbm, src = peaks()
+    gbs = 10.0 * faces * layers / (ms / 1e3) / 1e9
+    return {"workload": "whirl256 after its projection (fp16 graph), layers 6", "faces": faces,
+            "flagged_before": flagged, "reached_after": reached, "ms": round(ms, 4), "launches": layers,
+            "algorithmic_bytes": 10 * faces * layers, "achieved_gbs": round(gbs, 1), "peak_gbs": hbm,
+            "frac": round(gbs / hbm, 4), "peak_source": src, "steps": steps}
 
 
 def bench_whirlpool(steps):

@@ -163,6 +163,17 @@ int mpp_advect(mpp_ctx* ctx, float* ou, float* ov, float* ow, const float* u, co
 /* The same for the cell-centred level set (COFF samples). */
 int mpp_advect_phi(mpp_ctx* ctx, float* ophi, const float* phi, const float* u, const float* v, const float* w,
                    float dt, mpp_stream stream);
+/* extrapolate! (src/flip.jl:1192-1206), in place, after mpp_project: `layers` layers of
+ * extrapolate_kernel! (:1161-1177) carry the velocity out from the faces flagged in fu, fv,
+ * fw (an unflagged face that is not walled takes the Float32 mean of its flagged neighbours
+ * in the same array, summed +x, -x, +y, -y, +z, -z, and becomes flagged); then every face no
+ * layer reached is zeroed (unreached_kernel!, :1181-1184) and every walled face too
+ * (solidify!, :801-806). fu, fv, fw end as the reached flags. The six arrays must not
+ * overlap; layers <= 0 runs no layer (the zeroing only). The first call with layers > 0
+ * allocates the context's scratch: two copies of the three face arrays and their flags. */
+int mpp_extrapolate(mpp_ctx* ctx, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv, uint8_t* fw,
+                    int layers, mpp_stream stream);
+
 /* The adjoint of mpp_advect (no reference counterpart; the reverse of its steps): the
  * cotangent (gou, gov, gow) of its outputs in; du, dv, dw = the cotangent of (u, v, w),
  * through both the sampled arrays and the traced positions. The sub-step count is

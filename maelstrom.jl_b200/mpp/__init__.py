@@ -175,6 +175,20 @@ class Projector:
                                   _stream_ptr(stream)))
         return outs
 
+    def extrapolate(self, u, v, w, fu, fv, fw, layers=4, stream=None):
+        """extrapolate! (``mpp_extrapolate``, src/flip.jl:1192-1206) in place: the velocity
+        carried ``layers`` faces out from the faces flagged in (fu, fv, fw), zero on the
+        faces no layer reached and on walled faces; the flags end as the reached ones."""
+        import torch
+
+        g = self.grid
+        for t, name, axis in ((u, "u", 0), (v, "v", 1), (w, "w", 2)):
+            _require(t, torch.float32, int(np.prod(g.face_shape(axis))), name)
+        for t, name, axis in ((fu, "fu", 0), (fv, "fv", 1), (fw, "fw", 2)):
+            _require(t, torch.uint8, int(np.prod(g.face_shape(axis))), name)
+        check(self.lib.mpp_extrapolate(self._ctx, _ptr(u), _ptr(v), _ptr(w), _ptr(fu), _ptr(fv), _ptr(fw),
+                                       int(layers), _stream_ptr(stream)))
+
     def advect_phi(self, phi, u, v, w, dt, stream=None):
         import torch
 
@@ -373,6 +387,13 @@ def project(s: FlipBasin, dt, recover=0.5, sweeps=None) -> FlipBasin:
     s.iterations.append(res.iterations + res.fallback_iterations)
     s.last = res
     _raise_or_warn(res)
+    return s
+
+
+def extrapolate(s: FlipBasin, layers=4) -> FlipBasin:
+    """``extrapolate!(s; layers = 4)`` (src/flip.jl:1192-1206); ``step!`` calls it with
+    ``layers = 6`` right after ``project!`` (:1403-1404)."""
+    s.projector.extrapolate(s.u, s.v, s.w, s.fu, s.fv, s.fw, layers)
     return s
 
 

@@ -88,6 +88,7 @@ SIGNATURES = {
     "mpp_autotune": (ctypes.c_int, [P, P, P, P, P, P, ctypes.POINTER(TuneEntry), ctypes.c_int,
                                     ctypes.POINTER(ctypes.c_int), P]),
     "mpp_advect_phi": (ctypes.c_int, [P, P, P, P, P, P, F32, P]),
+    "mpp_extrapolate": (ctypes.c_int, [P, P, P, P, P, P, P, ctypes.c_int, P]),
     "mpp_advect_vjp": (ctypes.c_int, [P, P, P, P, P, P, P, F32, P, P, P, P]),
     "mpp_vjp_faces": (ctypes.c_int, [P, P, P, P, P, P, P, P, P, P]),
     "mpp_rhs": (ctypes.c_int, [P, P, P, P, P, P, F32, P]),

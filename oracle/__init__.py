@@ -67,6 +67,7 @@ def lib():
             "orc_advect_f64": (None, [G, P, P, P, P, P, P, P, d]),
             "orc_advect_vjp_f32": (None, [G, P, P, P, P, P, P, P, f, P, P, P, P]),
             "orc_advect_vjp_f64": (None, [G, P, P, P, P, P, P, P, d, P, P, P, P]),
+            "orc_extrapolate": (None, [G, P, P, P, P, P, P, i32]),
             "orc_num_threads": (i32, []), "orc_set_num_threads": (None, [i32]),
         }
         for name, (res, args) in sig.items():
@@ -292,3 +293,17 @@ def num_threads() -> int:
 
 def set_num_threads(n: int) -> None:
     lib().orc_set_num_threads(n)
+
+
+def extrapolate(grid, u, v, w, fu, fv, fw, layers=6):
+    """extrapolate!(s; layers) (src/flip.jl:1192-1206) in Float32: returns new (u, v, w, fu,
+    fv, fw), the velocity carried ``layers`` faces out from the flagged faces, zero beyond
+    and on walled faces; the flags are the reached ones."""
+    out = [np.array(a, dtype=np.float32, copy=True).ravel() for a in (u, v, w)]
+    fl = [np.array(a, dtype=np.uint8, copy=True).ravel() for a in (fu, fv, fw)]
+    for axis in range(3):
+        n = int(np.prod(_face_dims(grid, axis)))
+        if out[axis].size != n or fl[axis].size != n:
+            raise ValueError(f"face array {axis} has {out[axis].size} / {fl[axis].size} elements, not {n}")
+    lib().orc_extrapolate(ctypes.byref(_grid(grid)), *(_p(a) for a in out), *(_p(a) for a in fl), int(layers))
+    return (*out, *fl)

@@ -122,6 +122,12 @@ void orc_advect_vjp_f64(const orc_grid* g, const double* gout, const double* src
                         const double off[3], const double* u, const double* v, const double* w, double dt,
                         double* gsrc, double* gu, double* gv, double* gw);
 
+/* extrapolate! (src/flip.jl:1192-1206) in Float32, in place: `layers` layers of
+ * extrapolate_kernel! per face array, the unreached faces zeroed, then solidify!. fu, fv,
+ * fw (the projection's valid flags on entry) end as the reached flags. */
+void orc_extrapolate(const orc_grid* g, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv, uint8_t* fw,
+                     int layers);
+
 int orc_num_threads(void);
 void orc_set_num_threads(int n);
 
