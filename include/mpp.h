@@ -169,8 +169,9 @@ int mpp_advect_phi(mpp_ctx* ctx, float* ophi, const float* phi, const float* u, 
  * in the same array, summed +x, -x, +y, -y, +z, -z, and becomes flagged); then every face no
  * layer reached is zeroed (unreached_kernel!, :1181-1184) and every walled face too
  * (solidify!, :801-806). fu, fv, fw end as the reached flags. The six arrays must not
- * overlap; layers <= 0 runs no layer (the zeroing only). The first call with layers > 0
- * allocates the context's scratch: two copies of the three face arrays and their flags. */
+ * overlap; layers <= 0 runs no layer (the zeroing only; the flags stay as they are), and
+ * more than 254 layers is refused (MPP_ERR_INVALID). The first call with layers > 0
+ * allocates the context's scratch: a byte for each face of the three arrays. */
 int mpp_extrapolate(mpp_ctx* ctx, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv, uint8_t* fw,
                     int layers, mpp_stream stream);
 

@@ -118,10 +118,9 @@ struct mpp_ctx {
     void* Pd;  // FP64 solution (natural), FP64 contexts only
     uint8_t* tflag_all;
     int* edges;  // the levels' edge flags
-    // extrapolation scratch (allocated at the first mpp_extrapolate): two copies of the three
-    // face arrays and of their flags, ext_n faces each
-    float* ext_v;
-    uint8_t* ext_f;
+    // extrapolation scratch (allocated at the first mpp_extrapolate with layers): a reach
+    // code for each of the three face arrays' ext_n faces
+    uint8_t* ext_r;
     int64_t ext_n;
     size_t tflag_bytes;
     Scalars* sc;
@@ -1421,8 +1420,7 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
     c->aux = nullptr;
     c->ev_fork = c->ev_join = nullptr;
     c->in_batch = false;
-    c->ext_v = nullptr;
-    c->ext_f = nullptr;
+    c->ext_r = nullptr;
     c->ext_n = 0;
     c->prof_on = 0;
     memset(c->prof, 0, sizeof(c->prof));
@@ -2063,24 +2061,30 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
         return MPP_ERR_INVALID;
     }
     if (layers < 0) layers = 0;  // `for _ in 1:layers` runs no layer
-    float* A[3] = {u, v, w};
-    uint8_t* Fl[3] = {fu, fv, fw};
+    if (layers > EXTRAP_MAX_LAYERS) {
+        set_err("at most %d extrapolation layers", EXTRAP_MAX_LAYERS);
+        return MPP_ERR_INVALID;
+    }
     ExtArrays E;
     memset(&E, 0, sizeof(E));
-    int64_t n[3], tot = 0;
+    float* X[3] = {u, v, w};
+    uint8_t* Fl[3] = {fu, fv, fw};
+    int64_t n[3], tot = 0, rows = 0;
     for (int a = 0; a < 3; a++) {
         n[a] = 1;
         for (int e = 0; e < 3; e++) {
             E.d[a][e] = c->grid.n[e] + (a == e);
             n[a] *= E.d[a][e];
         }
+        if (n[a] >= ((int64_t)1 << 31)) {
+            set_err("face array of 2^31 or more faces");
+            return MPP_ERR_INVALID;
+        }
+        const int64_t ra = (int64_t)E.d[a][1] * E.d[a][2];
+        rows = ra > rows ? ra : rows;
         tot += n[a];
     }
-    if (n[0] >= ((int64_t)1 << 31) || n[1] >= ((int64_t)1 << 31) || n[2] >= ((int64_t)1 << 31)) {
-        set_err("face array of 2^31 or more faces");
-        return MPP_ERR_INVALID;
-    }
-    // a layer reads its neighbours' faces while the others are written: no two of the six
+    // a layer reads its neighbours' faces while others are written: no two of the six
     // arrays may share memory
     const char* lo[6] = {(const char*)u, (const char*)v, (const char*)w, (const char*)fu, (const char*)fv,
                          (const char*)fw};
@@ -2092,46 +2096,23 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
                 return MPP_ERR_INVALID;
             }
     if (layers > 0 && c->ext_n < tot) {
-        int e;
-        if ((e = alloc(c, (void**)&c->ext_v, 2 * sizeof(float) * (size_t)tot))) return e;
-        if ((e = alloc(c, (void**)&c->ext_f, 2 * (size_t)tot))) return e;
+        if (int e = alloc(c, (void**)&c->ext_r, (size_t)tot)) return e;
         c->ext_n = tot;
     }
-    float* Tv[2][3];
-    uint8_t* Tf[2][3];
     int64_t o = 0;
-    for (int p = 0; p < 2; p++)
-        for (int a = 0; a < 3; a++) {
-            Tv[p][a] = c->ext_v ? c->ext_v + o : nullptr;
-            Tf[p][a] = c->ext_f ? c->ext_f + o : nullptr;
-            o += n[a];
-        }
-    cudaStream_t s = (cudaStream_t)stream;
-    int64_t nmax = n[0] > n[1] ? n[0] : n[1];
-    nmax = nmax > n[2] ? nmax : n[2];
-    const dim3 grid(grid_cells(c, nmax), 3);
-    const Geo g = geo_of(c->grid);
-    auto pass = [&](float* const* sv, uint8_t* const* sf, float* const* dv, uint8_t* const* df, int mode) {
-        for (int a = 0; a < 3; a++) {
-            E.src[a] = sv[a];
-            E.fin[a] = sf[a];
-            E.dst[a] = dv[a];
-            E.fout[a] = df[a];
-        }
-        launch(k_extrapolate, grid, TPB, 0, s, g, E, mode);
-        c->launches++;
-    };
-    // layer 1 from the caller's arrays, the middle ones between the scratch copies, the last
-    // one (with the zeroing) back into the caller's arrays; with one layer, the zeroing alone
-    // copies it back; with none, it runs in place
-    if (layers == 0) {
-        pass(A, Fl, A, Fl, 2);
-    } else {
-        pass(A, Fl, Tv[0], Tf[0], 0);
-        for (int l = 2; l < layers; l++) pass(Tv[l % 2], Tf[l % 2], Tv[(l + 1) % 2], Tf[(l + 1) % 2], 0);
-        if (layers == 1) pass(Tv[0], Tf[0], A, Fl, 2);
-        else pass(Tv[layers % 2], Tf[layers % 2], A, Fl, 1);
+    for (int a = 0; a < 3; a++) {
+        E.x[a] = X[a];
+        E.f[a] = Fl[a];
+        E.reach[a] = c->ext_r ? c->ext_r + o : nullptr;
+        o += n[a];
     }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int cap = c->nsm * MAXBLOCKS_PER_SM;
+    const dim3 grid((unsigned)(rows < cap ? rows : cap), 3);
+    const Geo g = geo_of(c->grid);
+    for (int l = 1; l <= layers; l++) launch(k_extrap_layer, grid, TPB, 0, s, g, E, l);
+    launch(k_extrap_final, grid, TPB, 0, s, g, E, layers == 0 ? 1 : 0);
+    c->launches += layers + 1;
     CK(cudaGetLastError());
     return MPP_OK;
 }

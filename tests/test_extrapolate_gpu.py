@@ -69,3 +69,12 @@ def test_overlapping_arrays_are_refused(cuda):
     s = mpp.FlipBasin.from_scene(b)
     with pytest.raises(Exception, match="overlap"):
         s.projector.extrapolate(s.u, s.u, s.w, s.fu, s.fv, s.fw, layers=2)
+
+
+def test_too_many_layers_are_refused(cuda):
+    import mpp
+
+    b = scene.box_basin(16, seed=5102)
+    s = mpp.FlipBasin.from_scene(b)
+    with pytest.raises(Exception, match="layers"):
+        s.projector.extrapolate(s.u, s.v, s.w, s.fu, s.fv, s.fw, layers=255)
