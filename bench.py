@@ -521,9 +521,10 @@ def bench_adjoint(steps):
 def bench_extrapolate(steps):
     """extrapolate!(s; layers = 6) after the 256^3 whirlpool's projection, as step! runs it
     (src/flip.jl:1403-1404): ms a call, and HBM GB/s at the bytes the reach-code design must
-    move: a byte a face a layer (the flags, then the codes), a code read and a flag written a
-    face in the last pass, and 4 bytes for each value written (the faces a layer reaches and
-    the faces zeroed); neighbours come through the caches. `reference_pass_gbs` is the same
+    move: a flag read and a code written a face in the first pass, a code read a face a
+    layer, a code read and a flag written a face in the last pass, and 4 bytes for each value
+    written (the faces a layer reaches and the faces zeroed); neighbours come through the
+    caches. `reference_pass_gbs` is the same
     time at the reference's ping-pong structure (10 bytes a face a layer). The projected
     arrays are restored before each call, outside the timed events; the 3 x 253 MB of faces
     and flags are larger than L2."""
@@ -557,10 +558,10 @@ def bench_extrapolate(steps):
     reached = sum(int(torch.count_nonzero(f)) for f in (s.fu, s.fv, s.fw))
     flagged = sum(int(torch.count_nonzero(f)) for f in saved[3:])
     hbm, src = peaks()
-    nbytes = faces * (layers + 3) + 4 * ((reached - flagged) + (faces - reached))
+    nbytes = faces * (layers + 4) + 4 * ((reached - flagged) + (faces - reached))
     gbs = nbytes / (ms / 1e3) / 1e9
     return {"workload": "whirl256 after its projection (fp16 graph), layers 6", "faces": faces,
-            "flagged_before": flagged, "reached_after": reached, "ms": round(ms, 4), "launches": layers + 1,
+            "flagged_before": flagged, "reached_after": reached, "ms": round(ms, 4), "launches": layers + 2,
             "algorithmic_bytes": nbytes, "achieved_gbs": round(gbs, 1), "peak_gbs": hbm,
             "frac": round(gbs / hbm, 4), "peak_source": src,
             "reference_pass_gbs": round(10.0 * faces * layers / (ms / 1e3) / 1e9, 1), "steps": steps}

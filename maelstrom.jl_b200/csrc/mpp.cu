@@ -2061,28 +2061,31 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
         return MPP_ERR_INVALID;
     }
     if (layers < 0) layers = 0;  // `for _ in 1:layers` runs no layer
-    if (layers > EXTRAP_MAX_LAYERS) {
-        set_err("at most %d extrapolation layers", EXTRAP_MAX_LAYERS);
+    if (layers > EXTRAP_MAX_LAYERS16) {
+        set_err("at most %d extrapolation layers", EXTRAP_MAX_LAYERS16);
         return MPP_ERR_INVALID;
     }
-    ExtArrays E;
+    ExtChunks E;
     memset(&E, 0, sizeof(E));
     float* X[3] = {u, v, w};
     uint8_t* Fl[3] = {fu, fv, fw};
-    int64_t n[3], tot = 0, rows = 0;
+    int64_t n[3], cb[3], ctot = 0, nthreads = 0;
     for (int a = 0; a < 3; a++) {
         n[a] = 1;
         for (int e = 0; e < 3; e++) {
             E.d[a][e] = c->grid.n[e] + (a == e);
             n[a] *= E.d[a][e];
         }
-        if (n[a] >= ((int64_t)1 << 31)) {
+        E.pitch[a] = (E.d[a][0] + EXT_CHUNK - 1) / EXT_CHUNK * EXT_CHUNK;
+        const int64_t rows = (int64_t)E.d[a][1] * E.d[a][2];
+        cb[a] = rows * E.pitch[a];
+        if (n[a] >= ((int64_t)1 << 31) || cb[a] >= ((int64_t)1 << 31)) {
             set_err("face array of 2^31 or more faces");
             return MPP_ERR_INVALID;
         }
-        const int64_t ra = (int64_t)E.d[a][1] * E.d[a][2];
-        rows = ra > rows ? ra : rows;
-        tot += n[a];
+        const int64_t th = rows * (E.pitch[a] / EXT_CHUNK);
+        nthreads = th > nthreads ? th : nthreads;
+        ctot += cb[a];
     }
     // a layer reads its neighbours' faces while others are written: no two of the six
     // arrays may share memory
@@ -2095,24 +2098,24 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
                 set_err("extrapolation arrays overlap");
                 return MPP_ERR_INVALID;
             }
-    if (layers > 0 && c->ext_n < tot) {
-        if (int e = alloc(c, (void**)&c->ext_r, (size_t)tot)) return e;
-        c->ext_n = tot;
+    if (c->ext_n < ctot) {
+        if (int e = alloc(c, (void**)&c->ext_r, (size_t)ctot)) return e;
+        c->ext_n = ctot;
     }
-    int64_t o = 0;
+    int64_t o = 0;  // each array's codes start 16-byte aligned (cb is a multiple of 16)
     for (int a = 0; a < 3; a++) {
         E.x[a] = X[a];
         E.f[a] = Fl[a];
-        E.reach[a] = c->ext_r ? c->ext_r + o : nullptr;
-        o += n[a];
+        E.code[a] = c->ext_r + o;
+        o += cb[a];
     }
     cudaStream_t s = (cudaStream_t)stream;
-    const int cap = c->nsm * MAXBLOCKS_PER_SM;
-    const dim3 grid((unsigned)(rows < cap ? rows : cap), 3);
+    const dim3 grid(grid_cells(c, nthreads), 3);
     const Geo g = geo_of(c->grid);
-    for (int l = 1; l <= layers; l++) launch(k_extrap_layer, grid, TPB, 0, s, g, E, l);
-    launch(k_extrap_final, grid, TPB, 0, s, g, E, layers == 0 ? 1 : 0);
-    c->launches += layers + 1;
+    launch(k_extrap_codes, grid, TPB, 0, s, g, E);
+    for (int l = 1; l <= layers; l++) launch(k_extrap_layer16, grid, TPB, 0, s, E, l);
+    launch(k_extrap_final16, grid, TPB, 0, s, g, E, layers == 0 ? 1 : 0);
+    c->launches += layers + 2;
     CK(cudaGetLastError());
     return MPP_OK;
 }

@@ -13,9 +13,8 @@
 // is read by no other face in layer l (its code was UNREACHED and becomes l, neither below
 // l). So each layer matches the reference's bit for bit, and moves about a byte a face (the
 // codes) plus the values of the faces it reaches. A last pass writes the 0/1 flags and
-// zeroes what no layer reached and every walled face. One launch a layer covers all three
-// arrays (blockIdx.y is the array); a block takes one row of faces at a time, so a face's
-// (j, k) and its row's part of the solid test cost nothing per face.
+// zeroes what no layer reached and every walled face. One launch a pass covers all three
+// arrays (blockIdx.y is the array); a thread takes 16 consecutive faces of a row.
 #pragma once
 
 #include "mpp_base.cuh"
@@ -23,14 +22,6 @@
 namespace mpp {
 
 constexpr uint8_t UNREACHED = 0xFF;
-constexpr int EXTRAP_MAX_LAYERS = 254;  // codes 1 .. 254; 255 is UNREACHED
-
-struct ExtArrays {
-    float* x[3];        // the caller's face values, updated in place
-    uint8_t* f[3];      // the caller's flags
-    uint8_t* reach[3];  // scratch reach codes
-    int d[3][3];        // each array's dims
-};
 
 // walled (src/flip.jl:784-789) for the faces of one row (j, k) of the array along `ax`: the
 // grid's own edge, or a SOLID cell on either side (issolidcell, src/flip.jl:64-66, with the
@@ -70,75 +61,167 @@ __device__ __forceinline__ T pick3(int ax, T a, T b, T c) {
     return ax == 0 ? a : (ax == 1 ? b : c);
 }
 
-// Layer `layer` (1 .. EXTRAP_MAX_LAYERS). Layer 1 reads the caller's flags and writes every
-// face's code; later layers read the codes and write those of the faces they reach.
-__global__ void __launch_bounds__(TPB) k_extrap_layer(Geo g, ExtArrays E, int layer) {
-    const int ax = blockIdx.y;
-    const int a1 = pick3(ax, E.d[0][0], E.d[1][0], E.d[2][0]), a2 = pick3(ax, E.d[0][1], E.d[1][1], E.d[2][1]),
-              a3 = pick3(ax, E.d[0][2], E.d[1][2], E.d[2][2]);
-    const unsigned rows = (unsigned)a2 * (unsigned)a3, s1 = (unsigned)a1, s2 = (unsigned)a1 * (unsigned)a2;
-    float* x = pick3(ax, E.x[0], E.x[1], E.x[2]);
-    const uint8_t* fin = pick3(ax, E.f[0], E.f[1], E.f[2]);
-    uint8_t* R = pick3(ax, E.reach[0], E.reach[1], E.reach[2]);
-    const bool first = layer == 1;
+// ---- chunked form: 16 faces a thread ----
+// The codes live in rows padded to a multiple of 16 bytes (pitch P), so a thread reads the
+// codes of 16 consecutive faces of a row, and of the same 16 columns in the rows at -+y and
+// -+z, as five 16-byte loads (one round trip), and loads values only for the faces it
+// reaches. Padding reads as UNREACHED. A conversion pass writes the first codes: 0 for a
+// face flagged on entry, WALLED for an unflagged walled face (never reached, so the layers
+// skip the geometry), UNREACHED otherwise.
+constexpr uint8_t WALLED = 0xFE;
+constexpr int EXTRAP_MAX_LAYERS16 = 253;  // codes 1 .. 253
+constexpr int EXT_CHUNK = 16;
+
+struct ExtChunks {
+    float* x[3];
+    uint8_t* f[3];
+    uint8_t* code[3];  // rows of `pitch[a]` bytes
+    int d[3][3];
+    int pitch[3];
+};
+
+struct Chunk {
+    int ax, a1, a2, a3, P;
+    unsigned r;  // row
+    int j, k, i0;
+    bool on;
+};
+__device__ __forceinline__ Chunk chunk_of(const ExtChunks& E, unsigned t) {
+    Chunk c;
+    c.ax = blockIdx.y;
+    c.a1 = pick3(c.ax, E.d[0][0], E.d[1][0], E.d[2][0]);
+    c.a2 = pick3(c.ax, E.d[0][1], E.d[1][1], E.d[2][1]);
+    c.a3 = pick3(c.ax, E.d[0][2], E.d[1][2], E.d[2][2]);
+    c.P = pick3(c.ax, E.pitch[0], E.pitch[1], E.pitch[2]);
+    const unsigned cpr = (unsigned)c.P / EXT_CHUNK, rows = (unsigned)c.a2 * (unsigned)c.a3;
+    c.r = t / cpr;
+    c.on = c.r < rows;
+    c.i0 = (int)(t % cpr) * EXT_CHUNK;
+    c.j = (int)(c.r % (unsigned)c.a2);
+    c.k = (int)(c.r / (unsigned)c.a2);
+    return c;
+}
+__device__ __forceinline__ unsigned chunk_threads(const ExtChunks& E, int ax) {
+    const int a2 = pick3(ax, E.d[0][1], E.d[1][1], E.d[2][1]), a3 = pick3(ax, E.d[0][2], E.d[1][2], E.d[2][2]);
+    const int P = pick3(ax, E.pitch[0], E.pitch[1], E.pitch[2]);
+    return (unsigned)a2 * (unsigned)a3 * (unsigned)(P / EXT_CHUNK);
+}
+union Code16 {
+    uint4 v;
+    uint8_t b[16];
+};
+
+// The first codes, from the caller's flags.
+__global__ void __launch_bounds__(TPB) k_extrap_codes(Geo g, ExtChunks E) {
     pdl_wait();
     pdl_trigger();
-    for (unsigned r = blockIdx.x; r < rows; r += gridDim.x) {
-        const int j = (int)(r % (unsigned)a2), k = (int)(r / (unsigned)a2);
-        const RowWall w = row_wall(g, ax, j, k);
-        const unsigned base = r * s1;
-        for (int i = threadIdx.x; i < a1; i += blockDim.x) {
-            const unsigned id = base + (unsigned)i;
-            int rc = first ? (fin[id] ? 0 : UNREACHED) : R[id];
-            if (rc == UNREACHED && !walled_in_row(g, w, ax, i)) {
-                // the mean of the neighbours reached before this layer, in neighbour order
-                // (+x, -x, +y, -y, +z, -z)
-                float s = 0.f;
-                int m = 0;
-                auto take = [&](unsigned n) {
-                    if (first ? fin[n] != 0 : (int)R[n] < layer) {
-                        s = __fadd_rn(s, x[n]);
-                        m++;
-                    }
-                };
-                if (i + 1 < a1) take(id + 1);
-                if (i > 0) take(id - 1);
-                if (j + 1 < a2) take(id + s1);
-                if (j > 0) take(id - s1);
-                if (k + 1 < a3) take(id + s2);
-                if (k > 0) take(id - s2);
-                if (m > 0) {
-                    x[id] = __fdiv_rn(s, (float)m);
-                    rc = layer;
-                }
-            }
-            if (first || rc == layer) R[id] = (uint8_t)rc;
+    const unsigned n = chunk_threads(E, blockIdx.y);
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const Chunk c = chunk_of(E, t);
+        const uint8_t* fin = pick3(c.ax, E.f[0], E.f[1], E.f[2]);
+        uint8_t* R = pick3(c.ax, E.code[0], E.code[1], E.code[2]);
+        const unsigned base = c.r * (unsigned)c.a1;
+        uint8_t fl[EXT_CHUNK];
+#pragma unroll
+        for (int q = 0; q < EXT_CHUNK; q++) fl[q] = c.i0 + q < c.a1 ? fin[base + c.i0 + q] : (uint8_t)0;
+        const RowWall w = row_wall(g, c.ax, c.j, c.k);
+        Code16 out;
+#pragma unroll
+        for (int q = 0; q < EXT_CHUNK; q++) {
+            const int i = c.i0 + q;
+            out.b[q] = i >= c.a1 ? UNREACHED : (fl[q] ? (uint8_t)0 : (walled_in_row(g, w, c.ax, i) ? WALLED : UNREACHED));
         }
+        *reinterpret_cast<uint4*>(R + c.r * (unsigned)c.P + c.i0) = out.v;
     }
 }
 
-// The last pass: zero every face no layer reached and every walled face, and write the
-// reached flags. from_fin (no layer ran): reached means flagged on entry, and the flags stay
-// as they are.
-__global__ void __launch_bounds__(TPB) k_extrap_final(Geo g, ExtArrays E, int from_fin) {
-    const int ax = blockIdx.y;
-    const int a1 = pick3(ax, E.d[0][0], E.d[1][0], E.d[2][0]), a2 = pick3(ax, E.d[0][1], E.d[1][1], E.d[2][1]),
-              a3 = pick3(ax, E.d[0][2], E.d[1][2], E.d[2][2]);
-    const unsigned rows = (unsigned)a2 * (unsigned)a3, s1 = (unsigned)a1;
-    float* x = pick3(ax, E.x[0], E.x[1], E.x[2]);
-    uint8_t* f = pick3(ax, E.f[0], E.f[1], E.f[2]);
-    const uint8_t* R = pick3(ax, E.reach[0], E.reach[1], E.reach[2]);
+// Layer `layer` (1 .. EXTRAP_MAX_LAYERS16) on the codes.
+__global__ void __launch_bounds__(TPB, 4) k_extrap_layer16(ExtChunks E, int layer) {
     pdl_wait();
     pdl_trigger();
-    for (unsigned r = blockIdx.x; r < rows; r += gridDim.x) {
-        const int j = (int)(r % (unsigned)a2), k = (int)(r / (unsigned)a2);
-        const RowWall w = row_wall(g, ax, j, k);
-        const unsigned base = r * s1;
-        for (int i = threadIdx.x; i < a1; i += blockDim.x) {
-            const unsigned id = base + (unsigned)i;
-            const bool reached = from_fin ? f[id] != 0 : R[id] != UNREACHED;
-            if (!reached || walled_in_row(g, w, ax, i)) x[id] = 0.f;
-            if (!from_fin) f[id] = reached ? 1 : 0;
+    const unsigned n = chunk_threads(E, blockIdx.y);
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const Chunk c = chunk_of(E, t);
+        uint8_t* R = pick3(c.ax, E.code[0], E.code[1], E.code[2]);
+        float* x = pick3(c.ax, E.x[0], E.x[1], E.x[2]);
+        const unsigned rowoff = c.r * (unsigned)c.P + (unsigned)c.i0;
+        const unsigned P = (unsigned)c.P, PZ = (unsigned)c.P * (unsigned)c.a2;
+        Code16 own, yp, ym, zp, zm;
+        const uint4 none = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+        own.v = *reinterpret_cast<const uint4*>(R + rowoff);
+        yp.v = c.j + 1 < c.a2 ? *reinterpret_cast<const uint4*>(R + rowoff + P) : none;
+        ym.v = c.j > 0 ? *reinterpret_cast<const uint4*>(R + rowoff - P) : none;
+        zp.v = c.k + 1 < c.a3 ? *reinterpret_cast<const uint4*>(R + rowoff + PZ) : none;
+        zm.v = c.k > 0 ? *reinterpret_cast<const uint4*>(R + rowoff - PZ) : none;
+        const uint8_t left = c.i0 > 0 ? R[rowoff - 1] : UNREACHED;
+        const uint8_t right = c.i0 + EXT_CHUNK < c.a1 ? R[rowoff + EXT_CHUNK] : UNREACHED;
+        // the neighbours each face takes (reached before this layer), +x -x +y -y +z -z
+        unsigned take[EXT_CHUNK];
+        bool any = false;
+#pragma unroll
+        for (int q = 0; q < EXT_CHUNK; q++) {
+            take[q] = 0;
+            if (own.b[q] == UNREACHED) {  // padding is UNREACHED too, but has no reached neighbour
+                const uint8_t nb[6] = {q + 1 < EXT_CHUNK ? own.b[q + 1] : right, q > 0 ? own.b[q - 1] : left,
+                                       yp.b[q], ym.b[q], zp.b[q], zm.b[q]};
+#pragma unroll
+                for (int e = 0; e < 6; e++)
+                    if ((int)nb[e] < layer) take[q] |= 1u << e;
+                if (c.i0 + q >= c.a1) take[q] = 0;
+                any = any || take[q] != 0;
+            }
+        }
+        if (!any) continue;
+        const unsigned s1 = (unsigned)c.a1, s2 = (unsigned)c.a1 * (unsigned)c.a2;
+        const unsigned base = c.r * s1 + (unsigned)c.i0;
+        // the taken values, eight faces' loads at a time before their stores
+#pragma unroll
+        for (int h = 0; h < EXT_CHUNK; h += 8) {
+            float sum[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const unsigned id = base + h + q;
+                const unsigned nbi[6] = {id + 1, id - 1, id + s1, id - s1, id + s2, id - s2};
+                sum[q] = 0.f;
+#pragma unroll
+                for (int e = 0; e < 6; e++)
+                    if (take[h + q] & (1u << e)) sum[q] = __fadd_rn(sum[q], x[nbi[e]]);
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (take[h + q]) {
+                    x[base + h + q] = __fdiv_rn(sum[q], (float)__popc(take[h + q]));
+                    own.b[h + q] = (uint8_t)layer;
+                }
+        }
+        *reinterpret_cast<uint4*>(R + rowoff) = own.v;
+    }
+}
+
+// The last pass on the codes: zero every face not reached and every walled one, and write
+// the reached flags (unless keep_flags: no layer ran, and the flags stay as they are).
+__global__ void __launch_bounds__(TPB) k_extrap_final16(Geo g, ExtChunks E, int keep_flags) {
+    pdl_wait();
+    pdl_trigger();
+    const unsigned n = chunk_threads(E, blockIdx.y);
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const Chunk c = chunk_of(E, t);
+        const uint8_t* R = pick3(c.ax, E.code[0], E.code[1], E.code[2]);
+        float* x = pick3(c.ax, E.x[0], E.x[1], E.x[2]);
+        uint8_t* f = pick3(c.ax, E.f[0], E.f[1], E.f[2]);
+        Code16 own;
+        own.v = *reinterpret_cast<const uint4*>(R + c.r * (unsigned)c.P + c.i0);
+        const RowWall w = row_wall(g, c.ax, c.j, c.k);
+        const unsigned base = c.r * (unsigned)c.a1 + (unsigned)c.i0;
+#pragma unroll
+        for (int q = 0; q < EXT_CHUNK; q++) {
+            const int i = c.i0 + q;
+            if (i >= c.a1) continue;
+            const uint8_t cd = own.b[q];
+            const bool reached = cd < WALLED;
+            // only a face flagged on entry (code 0) can be both reached and walled
+            if (!reached || (cd == 0 && walled_in_row(g, w, c.ax, i))) x[base + q] = 0.f;
+            if (!keep_flags) f[base + q] = reached ? 1 : 0;
         }
     }
 }
