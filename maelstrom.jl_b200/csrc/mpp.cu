@@ -2061,8 +2061,8 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
         return MPP_ERR_INVALID;
     }
     if (layers < 0) layers = 0;  // `for _ in 1:layers` runs no layer
-    if (layers > EXTRAP_MAX_LAYERS16) {
-        set_err("at most %d extrapolation layers", EXTRAP_MAX_LAYERS16);
+    if (layers > EXTRAP_MAX_LAYERS) {
+        set_err("at most %d extrapolation layers", EXTRAP_MAX_LAYERS);
         return MPP_ERR_INVALID;
     }
     ExtChunks E;
@@ -2113,8 +2113,8 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
     const dim3 grid(grid_cells(c, nthreads), 3);
     const Geo g = geo_of(c->grid);
     launch(k_extrap_codes, grid, TPB, 0, s, g, E);
-    for (int l = 1; l <= layers; l++) launch(k_extrap_layer16, grid, TPB, 0, s, E, l);
-    launch(k_extrap_final16, grid, TPB, 0, s, g, E, layers == 0 ? 1 : 0);
+    for (int l = 1; l <= layers; l++) launch(k_extrap_layer, grid, TPB, 0, s, E, l);
+    launch(k_extrap_final, grid, TPB, 0, s, g, E, layers == 0 ? 1 : 0);
     c->launches += layers + 2;
     CK(cudaGetLastError());
     return MPP_OK;

@@ -61,7 +61,6 @@ __device__ __forceinline__ T pick3(int ax, T a, T b, T c) {
     return ax == 0 ? a : (ax == 1 ? b : c);
 }
 
-// ---- chunked form: 16 faces a thread ----
 // The codes live in rows padded to a multiple of 16 bytes (pitch P), so a thread reads the
 // codes of 16 consecutive faces of a row, and of the same 16 columns in the rows at -+y and
 // -+z, as five 16-byte loads (one round trip), and loads values only for the faces it
@@ -69,7 +68,7 @@ __device__ __forceinline__ T pick3(int ax, T a, T b, T c) {
 // face flagged on entry, WALLED for an unflagged walled face (never reached, so the layers
 // skip the geometry), UNREACHED otherwise.
 constexpr uint8_t WALLED = 0xFE;
-constexpr int EXTRAP_MAX_LAYERS16 = 253;  // codes 1 .. 253
+constexpr int EXTRAP_MAX_LAYERS = 253;  // codes 1 .. 253
 constexpr int EXT_CHUNK = 16;
 
 struct ExtChunks {
@@ -84,7 +83,6 @@ struct Chunk {
     int ax, a1, a2, a3, P;
     unsigned r;  // row
     int j, k, i0;
-    bool on;
 };
 __device__ __forceinline__ Chunk chunk_of(const ExtChunks& E, unsigned t) {
     Chunk c;
@@ -93,9 +91,8 @@ __device__ __forceinline__ Chunk chunk_of(const ExtChunks& E, unsigned t) {
     c.a2 = pick3(c.ax, E.d[0][1], E.d[1][1], E.d[2][1]);
     c.a3 = pick3(c.ax, E.d[0][2], E.d[1][2], E.d[2][2]);
     c.P = pick3(c.ax, E.pitch[0], E.pitch[1], E.pitch[2]);
-    const unsigned cpr = (unsigned)c.P / EXT_CHUNK, rows = (unsigned)c.a2 * (unsigned)c.a3;
+    const unsigned cpr = (unsigned)c.P / EXT_CHUNK;
     c.r = t / cpr;
-    c.on = c.r < rows;
     c.i0 = (int)(t % cpr) * EXT_CHUNK;
     c.j = (int)(c.r % (unsigned)c.a2);
     c.k = (int)(c.r / (unsigned)c.a2);
@@ -135,8 +132,8 @@ __global__ void __launch_bounds__(TPB) k_extrap_codes(Geo g, ExtChunks E) {
     }
 }
 
-// Layer `layer` (1 .. EXTRAP_MAX_LAYERS16) on the codes.
-__global__ void __launch_bounds__(TPB, 4) k_extrap_layer16(ExtChunks E, int layer) {
+// Layer `layer` (1 .. EXTRAP_MAX_LAYERS) on the codes.
+__global__ void __launch_bounds__(TPB, 4) k_extrap_layer(ExtChunks E, int layer) {
     pdl_wait();
     pdl_trigger();
     const unsigned n = chunk_threads(E, blockIdx.y);
@@ -200,7 +197,7 @@ __global__ void __launch_bounds__(TPB, 4) k_extrap_layer16(ExtChunks E, int laye
 
 // The last pass on the codes: zero every face not reached and every walled one, and write
 // the reached flags (unless keep_flags: no layer ran, and the flags stay as they are).
-__global__ void __launch_bounds__(TPB) k_extrap_final16(Geo g, ExtChunks E, int keep_flags) {
+__global__ void __launch_bounds__(TPB) k_extrap_final(Geo g, ExtChunks E, int keep_flags) {
     pdl_wait();
     pdl_trigger();
     const unsigned n = chunk_threads(E, blockIdx.y);
