@@ -171,7 +171,8 @@ int mpp_advect_phi(mpp_ctx* ctx, float* ophi, const float* phi, const float* u, 
  * (solidify!, :801-806). fu, fv, fw end as the reached flags. The six arrays must not
  * overlap; layers <= 0 runs no layer (the zeroing only; the flags stay as they are), and
  * more than 253 layers is refused (MPP_ERR_INVALID). The first call allocates the
- * context's scratch: a byte for each face of the three arrays (rows padded to 16). */
+ * context's scratch, a byte for each face of the three arrays (rows padded to 16): make it
+ * outside any stream capture. */
 int mpp_extrapolate(mpp_ctx* ctx, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv, uint8_t* fw,
                     int layers, mpp_stream stream);
 
