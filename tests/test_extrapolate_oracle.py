@@ -126,3 +126,41 @@ def test_projection_flags_reach_and_zero():
         keep = (fl[ax] != 0) & ~walled
         assert np.array_equal(a[keep], vel[ax][keep])
         assert np.count_nonzero(f) > np.count_nonzero(fl[ax])  # it did carry the water's velocity out
+
+
+def test_no_layer_keeps_flag_values_and_zeroes():
+    """layers = 0: no extrapolate_kernel! runs, so the flags stay byte for byte (any nonzero
+    value counts as flagged) and only unreached_kernel! and solidify! act."""
+    b = scene.box_basin((10, 8, 6), seed=5002)
+    g = b.grid
+    rng = np.random.default_rng(11)
+    vel = [rng.uniform(-1, 1, int(np.prod(g.face_shape(a)))).astype(F) for a in range(3)]
+    fl = [rng.integers(0, 4, int(np.prod(g.face_shape(a)))).astype(np.uint8) for a in range(3)]
+    got = oracle.extrapolate(g, *vel, *fl, layers=0)
+    for ax in range(3):
+        assert np.array_equal(got[3 + ax], fl[ax])
+        walled = np.array([_walled(g, (i, j, k), ax) for k in range(g.face_shape(ax)[2])
+                           for j in range(g.face_shape(ax)[1]) for i in range(g.face_shape(ax)[0])])
+        keep = (fl[ax] != 0) & ~walled
+        assert np.array_equal(got[ax][keep], vel[ax][keep])
+        assert np.all(got[ax][~keep] == 0)
+
+
+def test_flagged_walled_face_is_a_source_then_zero():
+    """A walled face flagged on entry lends its value to its neighbours in the first layer
+    (extrapolate_kernel! reads any flagged neighbour), and solidify! zeroes it at the end."""
+    b = scene.box_basin((10, 8, 6), seed=5003)
+    g = b.grid
+    a1, a2, a3 = g.face_shape(0)
+    vel = [np.zeros(int(np.prod(g.face_shape(a))), dtype=F) for a in range(3)]
+    fl = [np.zeros(int(np.prod(g.face_shape(a))), dtype=np.uint8) for a in range(3)]
+    # a walled u face whose +x neighbour in the same row is not walled (the cylinder's wall)
+    j, k = a2 // 2, a3 // 2
+    i = next(i for i in range(a1 - 1) if _walled(g, (i, j, k), 0) and not _walled(g, (i + 1, j, k), 0))
+    src = i + a1 * (j + a2 * k)
+    dst = src + 1
+    vel[0][src] = F(0.75)
+    fl[0][src] = 1
+    got = oracle.extrapolate(g, *vel, *fl, layers=1)
+    assert got[0][dst] == F(0.75) and got[3][dst] == 1
+    assert got[0][src] == 0 and got[3][src] == 1
