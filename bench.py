@@ -526,8 +526,8 @@ def bench_extrapolate(steps):
     written (the faces a layer reaches and the faces zeroed); neighbours come through the
     caches. `reference_pass_gbs` is the same
     time at the reference's ping-pong structure (10 bytes a face a layer). The projected
-    arrays are restored before each call, outside the timed events; the 3 x 253 MB of faces
-    and flags are larger than L2."""
+    arrays are restored before each call, outside the timed events; the three arrays' faces
+    and flags (253 MB) are larger than L2."""
     import torch
 
     import mpp
