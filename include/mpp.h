@@ -170,9 +170,11 @@ int mpp_advect_phi(mpp_ctx* ctx, float* ophi, const float* phi, const float* u, 
  * layer reached is zeroed (unreached_kernel!, :1181-1184) and every walled face too
  * (solidify!, :801-806). fu, fv, fw end as the reached flags. The six arrays must not
  * overlap; layers <= 0 runs no layer (the zeroing only; the flags stay as they are), and
- * more than 253 layers is refused (MPP_ERR_INVALID). The first call allocates the
- * context's scratch, a byte for each face of the three arrays (rows padded to 16): make it
- * outside any stream capture. */
+ * more than 253 layers is refused (MPP_ERR_INVALID). The first call on a context, whatever
+ * `layers` is, allocates the context's scratch, a byte for each face of the three arrays
+ * (rows padded to 16): make it outside any stream capture. That scratch belongs to the
+ * context while each call runs on the caller's stream, so calls on one context must not
+ * overlap on the GPU (two streams at once race on it). */
 int mpp_extrapolate(mpp_ctx* ctx, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv, uint8_t* fw,
                     int layers, mpp_stream stream);
 
@@ -257,15 +259,16 @@ int mpp_gradient(mpp_ctx* ctx, float* u, float* v, float* w, uint8_t* fu, uint8_
 /* FP64 pressure of the last mpp_pressure/mpp_project on an MPP_PREC_FP64 context. */
 int mpp_solution_f64(mpp_ctx* ctx, double* out_host);
 
-/* The liquid volume without allocating anything (no counterpart in the reference; it is
- * volume(s), src/flip.jl:293, for callers that cannot allocate device memory when they
- * want it, such as a monitoring or render callback under a fixed memory budget, where
- * creating a context, which allocates the solver's whole workspace, is not an option).
- * Its scratch is a static device array of 33,024 bytes that every GPU loading this
- * library holds until exit; it handles grids of at most 16,777,216 cells (256^3) and
- * returns MPP_ERR_INVALID beyond. All calls share that array: calls overlapping on the
- * GPU race. The first call on a device sets up its address there, so make it before any
- * stream capture. Synchronises `stream`; `volume` is a host pointer. */
+/* The liquid volume without allocating anything: the sum over the non-solid cells of
+ * clamp(0.5 - phi/dx, 0, 1), times dx^3, in m^3. It has no counterpart in the reference. It
+ * is for callers that cannot allocate device memory when they want the volume, such as a
+ * monitoring or render callback under a fixed memory budget, where creating a context
+ * (which allocates the solver's whole workspace) is not an option. Its scratch is a static
+ * device array of 33,024 bytes that every GPU loading this library holds until exit; it
+ * handles grids of at most 16,777,216 cells (256^3) and returns MPP_ERR_INVALID beyond.
+ * All calls share that array: calls overlapping on the GPU race. Each call looks the
+ * array's address up on the current device. It synchronises `stream` before returning, so
+ * it must not be called while `stream` is being captured. `volume` is a host pointer. */
 int mpp_volume_noalloc(const mpp_grid* grid, const float* phi, double* volume, mpp_stream stream);
 
 /* ---- per-kernel timing (the reference has none: bakeflip only logs @elapsed per

@@ -118,8 +118,8 @@ struct mpp_ctx {
     void* Pd;  // FP64 solution (natural), FP64 contexts only
     uint8_t* tflag_all;
     int* edges;  // the levels' edge flags
-    // extrapolation scratch (allocated at the first mpp_extrapolate with layers): a reach
-    // code for each of the three face arrays' ext_n faces
+    // extrapolation scratch (allocated at the first mpp_extrapolate, whatever its layer
+    // count): a reach code for each of the three face arrays' ext_n faces
     uint8_t* ext_r;
     int64_t ext_n;
     size_t tflag_bytes;
@@ -2361,9 +2361,10 @@ int mpp_solution_f64(mpp_ctx* c, double* out) {
 // Each block sums a fixed run of NOALLOC_BLOCK_CELLS cells, so the scratch bounds the
 // grid: at most NOALLOC_MAX_BLOCKS * NOALLOC_BLOCK_CELLS = 16,777,216 cells (256^3).
 // Every call shares the array, so calls that overlap on the GPU (on different streams
-// at once) race and give wrong results; calls in sequence are fine. The first call on a
-// device looks the array's address up once for that device (cudaGetSymbolAddress), so
-// that first call should come before any stream capture.
+// at once) race and give wrong results; calls in sequence are fine. Every call looks the
+// array's address up on the current device (cudaGetSymbolAddress) rather than keeping it,
+// so a device reset between calls, which may move the array, is harmless. A call ends by
+// synchronising its stream, so it must not be made while that stream is being captured.
 namespace {
 
 constexpr int NOALLOC_BLOCK_CELLS = 4096;  // cells per block: 256 threads x 16
@@ -2374,8 +2375,9 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = NOALLOC_HEADER + sizeof(double) * NOALL
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-// volume_kernel! + volume (src/flip.jl:261-279, 293), as k_volume, with the scratch laid
-// out in `scratch`: [counter u32 | result f64 | pad][partials f64 x blocks].
+// The liquid volume of phi over the non-solid cells, times dx^3 (the sum k_volume forms),
+// with the scratch laid out in `scratch`: [counter u32 | result f64 | pad][partials f64 x
+// blocks].
 __global__ void __launch_bounds__(TPB) k_volume_noalloc(Geo g, const float* __restrict__ phi, unsigned char* scratch) {
     pdl_wait();
     pdl_trigger();
@@ -2399,10 +2401,6 @@ __global__ void __launch_bounds__(TPB) k_volume_noalloc(Geo g, const float* __re
         *result = (double)((float)acc[0] * (g.dx * g.dx * g.dx));
 }
 
-// The array's device address, looked up once per device.
-constexpr int NOALLOC_MAX_DEVICES = 64;
-unsigned char* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
-
 }  // namespace
 
 extern "C" int mpp_volume_noalloc(const mpp_grid* grid, const float* phi, double* volume, mpp_stream stream) {
@@ -2421,18 +2419,11 @@ extern "C" int mpp_volume_noalloc(const mpp_grid* grid, const float* phi, double
                 (long long)NOALLOC_MAX_CELLS, NOALLOC_MAX_BLOCKS, NOALLOC_BLOCK_CELLS, (long long)N);
         return MPP_ERR_INVALID;
     }
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
-        set_err("device %d is beyond the %d devices mpp_volume_noalloc keeps addresses for", dev, NOALLOC_MAX_DEVICES);
-        return MPP_ERR_INVALID;
-    }
-    if (!g_noalloc_ptr[dev]) {
-        void* ptr = nullptr;
-        CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-        g_noalloc_ptr[dev] = static_cast<unsigned char*>(ptr);
-    }
-    unsigned char* scratch = g_noalloc_ptr[dev];
+    // the array's address on the current device, looked up on every call: a cached address
+    // would outlive a device reset that reloads the module
+    void* ptr = nullptr;
+    CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    unsigned char* scratch = static_cast<unsigned char*>(ptr);
     cudaStream_t s = (cudaStream_t)stream;
     // The counter must start at zero; an interrupted earlier call could have left it set.
     CK(cudaMemsetAsync(scratch, 0, NOALLOC_HEADER, s));
