@@ -121,8 +121,17 @@ def coarsen(nf, tf):
     return tc
 
 
-def vcycle(grid, r, types, diag_, sweeps=2, coarse=40, prec=32):
+def _sweeps(sweeps, sweeps_coarse):
+    """The C side's packed sweep counts (ORC_SWEEPS in oracle.h): the fine level's, and the
+    coarser levels' when given (0: the same as the fine level's, as the reference)."""
+    if not (1 <= sweeps <= 255 and 0 <= sweeps_coarse <= 255):
+        raise ValueError("sweep counts must be in 1..255")
+    return int(sweeps) | (int(sweeps_coarse) << 8)
+
+
+def vcycle(grid, r, types, diag_, sweeps=2, coarse=40, prec=32, sweeps_coarse=0):
     t = _ft(prec)
+    sweeps = _sweeps(sweeps, sweeps_coarse)
     z = np.zeros(grid.ncells, dtype=t)
     getattr(lib(), f"orc_vcycle_f{prec}")(ctypes.byref(_grid(grid)), _p(z), _p(np.ascontiguousarray(r, dtype=t)),
                                           _p(np.ascontiguousarray(types, dtype=np.uint8)),
@@ -139,9 +148,10 @@ def apply(grid, x, types, diag_, prec=32):
     return y
 
 
-def pressure(grid, P, b, types, phi, tol=1e-4, maxiter=60, sweeps=2, coarse=40, prec=32):
+def pressure(grid, P, b, types, phi, tol=1e-4, maxiter=60, sweeps=2, coarse=40, prec=32, sweeps_coarse=0):
     """pressure! on copies: returns (P, info)."""
     t = _ft(prec)
+    sweeps = _sweeps(sweeps, sweeps_coarse)
     P = np.array(P, dtype=t, copy=True)
     info = Info()
     getattr(lib(), f"orc_pressure_f{prec}")(ctypes.byref(_grid(grid)), _p(P), _p(np.ascontiguousarray(b, dtype=t)),
@@ -163,9 +173,10 @@ def gradient(grid, u, v, w, P, types, phi, prec=32):
 
 
 def project(basin, P=None, *, volume0=None, dt=1.0 / 48, recover=0.5, tol=1e-4, maxiter=60, sweeps=2, coarse=40,
-            prec=32):
+            prec=32, sweeps_coarse=0):
     """project! on copies of a scene.Basin: returns dict(u, v, w, fu, fv, fw, P, info)."""
     g = basin.grid
+    sweeps = _sweeps(sweeps, sweeps_coarse)
     t = _ft(prec)
     u, v, w = (np.array(a, dtype=t, copy=True) for a in (basin.u, basin.v, basin.w))
     fu, fv, fw = (np.zeros(a.size, dtype=np.uint8) for a in (u, v, w))

@@ -64,7 +64,10 @@ void orc_diag_f32(const orc_grid* g, float* diag, const uint8_t* types, const fl
 void orc_diag_f64(const orc_grid* g, double* diag, const uint8_t* types, const double* phi);
 void orc_coarsen(const int32_t nf[3], uint8_t* tc, const uint8_t* tf);
 /* z = M^-1 r, one V-cycle (src/flip.jl:992-1014). level_types[l] for l=1..L-1 are the
- * coarsened types (level 0 is `types`). */
+ * coarsened types (level 0 is `types`). Every `sweeps` argument of this file packs the
+ * fine level's sweep count in its low byte and, when bits 8-15 are not zero, the coarser
+ * levels' count there (ORC_SWEEPS); the reference has the one count for all levels. */
+#define ORC_SWEEPS(fine, coarser) ((fine) | ((coarser) << 8))
 void orc_vcycle_f32(const orc_grid* g, float* z, const float* r, const uint8_t* types,
                     const float* diag, int sweeps, int coarse);
 void orc_vcycle_f64(const orc_grid* g, double* z, const double* r, const uint8_t* types,

@@ -265,26 +265,28 @@ static void FN(hier_free_)(FN(hier_) * h) {
 }
 
 /* vcycle! (src/flip.jl:992-1014): down [start, 1, 0, 1], residual, restrict; the coarsest
- * solve; up: prolong, [1, 0, 1, 0] (for sweeps = 2). */
+ * solve; up: prolong, [1, 0, 1, 0] (for sweeps = 2). `sweeps` packs two counts: its low byte
+ * is the fine level's (the reference's one `sweeps`), and bits 8-15, when not zero, the
+ * coarser levels' (ORC_SWEEPS); the same colour schedule runs at each level's count. */
 static void FN(vcycle_h_)(FN(hier_) * h, R* z, const R* r, const R* diag, int sweeps, int coarse) {
     const int L = h->L;
     h->x[0] = z;
     h->b[0] = (R*)r;
-    int down[64], nd = 0, up[64], nu = 0;
-    for (int s = 0; s < sweeps; s++) { down[nd++] = 0; down[nd++] = 1; }
-    for (int s = 0; s < sweeps; s++) { up[nu++] = 1; up[nu++] = 0; }
+    const int swf = sweeps & 0xff, swc = (sweeps >> 8) & 0xff ? (sweeps >> 8) & 0xff : swf;
     for (int l = 0; l < L - 1; l++) {
         const R* dg = l == 0 ? diag : NULL;
+        const int sw = l == 0 ? swf : swc;
         FN(start_)(h->n[l], h->x[l], h->b[l], h->t[l], dg);
-        for (int s = 1; s < nd; s++) FN(rbgs_)(h->n[l], h->x[l], h->b[l], h->t[l], dg, down[s]);
+        for (int s = 1; s < 2 * sw; s++) FN(rbgs_)(h->n[l], h->x[l], h->b[l], h->t[l], dg, s & 1);
         FN(residual_)(h->n[l], h->r[l], h->x[l], h->b[l], h->t[l], dg);
         FN(restrict_)(h->n[l + 1], h->b[l + 1], h->r[l], h->t[l], h->t[l + 1]);
     }
     FN(coarsest_)(h->n[L - 1], h->x[L - 1], h->b[L - 1], h->t[L - 1], coarse);
     for (int l = L - 2; l >= 0; l--) {
         const R* dg = l == 0 ? diag : NULL;
+        const int sw = l == 0 ? swf : swc;
         FN(prolong_)(h->n[l], h->x[l], h->x[l + 1], h->t[l], h->t[l + 1]);
-        for (int s = 0; s < nu; s++) FN(rbgs_)(h->n[l], h->x[l], h->b[l], h->t[l], dg, up[s]);
+        for (int s = 0; s < 2 * sw; s++) FN(rbgs_)(h->n[l], h->x[l], h->b[l], h->t[l], dg, 1 - (s & 1));
     }
 }
 

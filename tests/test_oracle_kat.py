@@ -121,18 +121,33 @@ def test_operator_symmetric(b24):
     assert x @ ax > 0
 
 
-def test_vcycle_symmetric_positive(b24):
+@pytest.mark.parametrize("sweeps,sweeps_coarse,coarse", [(2, 0, 40), (5, 6, 10), (1, 3, 4)])
+def test_vcycle_symmetric_positive(b24, sweeps, sweeps_coarse, coarse):
     """The V-cycle reverses its colour order on the way up (src/flip.jl:996) and solves the
-    coarsest level symmetrically (:945), so M is symmetric positive definite."""
+    coarsest level symmetrically (:945), so M is symmetric positive definite; that holds
+    level by level, so for any per-level sweep counts (the autotuner's) too."""
     g = b24.grid
     d = oracle.diag(g, b24.types, b24.phi, prec=64)
     live = b24.types == scene.LIQUID
     x = scene.uniform(3, 3, g.ncells).astype(np.float64) * live
     y = scene.uniform(4, 4, g.ncells).astype(np.float64) * live
-    mx = oracle.vcycle(g, x, b24.types, d, prec=64)
-    my = oracle.vcycle(g, y, b24.types, d, prec=64)
+    kw = dict(sweeps=sweeps, sweeps_coarse=sweeps_coarse, coarse=coarse, prec=64)
+    mx = oracle.vcycle(g, x, b24.types, d, **kw)
+    my = oracle.vcycle(g, y, b24.types, d, **kw)
     assert abs(mx @ y - x @ my) <= 1e-10 * abs(mx @ y)
     assert mx @ x > 0 and my @ y > 0
+
+
+def test_vcycle_coarse_sweeps_default_is_the_reference(b24):
+    """A coarser-level count of 0, or equal to the fine one, is the reference's one `sweeps`;
+    a different one changes the result once the grid has a level between fine and coarsest."""
+    g = b24.grid
+    d = oracle.diag(g, b24.types, b24.phi)
+    r = scene.uniform(5, 5, g.ncells) * (b24.types == scene.LIQUID)
+    base = oracle.vcycle(g, r, b24.types, d, sweeps=3)
+    np.testing.assert_array_equal(oracle.vcycle(g, r, b24.types, d, sweeps=3, sweeps_coarse=3), base)
+    assert g.levels >= 3
+    assert not np.array_equal(oracle.vcycle(g, r, b24.types, d, sweeps=3, sweeps_coarse=1), base)
 
 
 def test_projection_removes_divergence(b24):
