@@ -27,7 +27,6 @@ import json
 import math
 import os
 import re
-import subprocess
 import sys
 import time
 
@@ -74,50 +73,83 @@ def ncu_traffic(kernel_key):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled while the timed region runs."""
+    """SM clocks and throttle reasons of this process's GPU, sampled through NVML in a
+    background thread while the timed region runs (one sample at start, one at stop, and
+    every `period_s` between them, so even a 100 ms region has several). The GPU is found
+    by its UUID (CUDA and NVML number devices differently under CUDA_VISIBLE_DEVICES)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
-    def __init__(self, index):
+    def __init__(self, index, period_s=0.01):
         self.index = index
-        self.proc = None
+        self.period = period_s
+        self.handle = None
+        self.err = None
+        self.samples = []
+        self.thread = None
+        self.stop_flag = None
+        try:
+            import pynvml
+            import torch
+
+            self.nvml = pynvml
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(index).uuid)
+            uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+            self.handle = pynvml.nvmlDeviceGetHandleByUUID(uuid)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+        except Exception as e:  # no NVML: the line says so
+            self.err = f"nvml unavailable: {type(e).__name__}: {e}"
+
+    def _sample(self):
+        n = self.nvml
+        sm = float(n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM))
+        mask = int(n.nvmlDeviceGetCurrentClocksEventReasons(self.handle))
+        try:
+            watts = n.nvmlDeviceGetPowerUsage(self.handle) / 1000.0
+        except Exception:
+            watts = None
+        self.samples.append((sm, mask, watts))
 
     def start(self):
-        try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "50"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except Exception:
-            self.proc = None
+        import threading
+
+        if self.handle is None:
+            return
+        self.samples = []
+        self.stop_flag = threading.Event()
+        self._sample()
+
+        def loop():
+            while not self.stop_flag.wait(self.period):
+                try:
+                    self._sample()
+                except Exception:
+                    pass
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            out, _ = self.proc.communicate(timeout=5)
-        except Exception:
-            self.proc.kill()
-            out, _ = self.proc.communicate()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for name, val in zip(names, f[5:9]):
-                if val.lower().startswith("active"):
+        if self.handle is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.err or "nvml unavailable"], "samples": 0}
+        self.stop_flag.set()
+        self.thread.join(timeout=5)
+        self._sample()
+        sm = sorted(x[0] for x in self.samples)
+        reasons = set()
+        for _, mask, _ in self.samples:
+            for name, attr in self.REASONS:
+                bit = getattr(self.nvml, attr, 0)
+                if bit and mask & bit:
                     reasons.add(name)
-        sm.sort()
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        watts = [x[2] for x in self.samples if x[2] is not None]
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.max_mhz, "reasons": sorted(reasons),
+                "samples": len(sm), "sm_mhz_min": sm[0], "power_w_max": round(max(watts), 1) if watts else None,
+                "source": "nvml"}
 
 
 def dist_init():
@@ -262,43 +294,39 @@ def run_mpp(args):
     err_mixed = float(np.linalg.norm(P_mixed - P64) / nrm)
     err_fp32 = float(np.linalg.norm(P_fp32 - P64) / nrm)
 
-    # e2e: the public call with host buffers, copies inside the timed region
+    # e2e: the public API with the basin's arrays in pinned host memory, every step's copies
+    # inside the timed region; mpp.pipeline.HostPipeline overlaps step i+1's upload and step
+    # i-1's download with step i's solve (three device buffer sets, three streams)
+    from mpp.pipeline import HostPipeline, OUT_NAMES
+
     pin = lambda t: t.detach().cpu().pin_memory()
     h_in = {"u": pin(u0), "v": pin(v0), "w": pin(w0), "types": pin(types), "phi": pin(phi),
             "P": pin(torch.zeros_like(P))}
-    h_out = {k: torch.empty(t.numel(), dtype=t.dtype).pin_memory() for k, t in
-             (("u", u0), ("v", v0), ("w", w0), ("fu", fu), ("fv", fv), ("fw", fw), ("P", P))}
-    d_types, d_phi = torch.empty_like(types), torch.empty_like(phi)
-    h2d = sum(t.numel() * t.element_size() for t in h_in.values())
-    d2h = sum(t.numel() * t.element_size() for t in h_out.values())
+    shapes = {"u": u0, "v": v0, "w": w0, "fu": fu, "fv": fv, "fw": fw, "P": P}
+    h_out = [{k: torch.empty(shapes[k].numel(), dtype=shapes[k].dtype).pin_memory() for k in OUT_NAMES}
+             for _ in range(3)]
+    pipe = HostPipeline(proj, dev)
+    h2d, d2h = HostPipeline.bytes_per_step(h_in, h_out[0])
     vol0 = proj.volume(phi)
     e2e_steps = max(1, min(args.steps, 50))
-
-    def e2e_step():
-        u.copy_(h_in["u"], non_blocking=True)
-        v.copy_(h_in["v"], non_blocking=True)
-        w.copy_(h_in["w"], non_blocking=True)
-        d_types.copy_(h_in["types"], non_blocking=True)
-        d_phi.copy_(h_in["phi"], non_blocking=True)
-        P.copy_(h_in["P"], non_blocking=True)
-        r = proj.project(u, v, w, fu, fv, fw, P, d_types, d_phi, vol0, DT)
-        for k, t in (("u", u), ("v", v), ("w", w), ("fu", fu), ("fv", fv), ("fw", fw), ("P", P)):
-            h_out[k].copy_(t, non_blocking=True)
-        return r
-
-    for _ in range(min(args.warmup, 2)):
-        e2e_step()
+    ins = [h_in] * e2e_steps
+    outs = [h_out[i % 3] for i in range(e2e_steps)]
+    pipe.run([h_in] * max(3, min(args.warmup, 6)), [h_out[i % 3] for i in range(max(3, min(args.warmup, 6)))],
+             vol0, DT)
     torch.cuda.synchronize()
     barrier(world)
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
-    for _ in range(e2e_steps):
-        e2e_step()
+    e2e_res = pipe.run(ins, outs, vol0, DT, stream=stream)
     f1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     ms_e2e = max_over_ranks(f0.elapsed_time(f1), world)
     e2e_value = world * e2e_steps / (ms_e2e / 1e3)
+    # the downloaded result of the last step is the device-resident headline's result
+    e2e_ok = all(r.status == 0 for r in e2e_res) and bool(
+        np.array_equal(outs[-1]["P"].numpy(), P_mixed))
+    del pipe
 
     # live per-kernel timing (CUDA events on the launching stream), one profiled projection
     proj.profile(True)
@@ -342,7 +370,8 @@ def run_mpp(args):
                              "autotuned": tune32["chosen"]},
         "fp64_oracle": {"iterations": res64.iterations, "true_rel_residual": res64.true_rel_residual},
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "steps": e2e_steps},
+                "steps": e2e_steps, "overlap": "upload i+1 / solve i / download i-1 on three streams",
+                "result_matches_device_run": e2e_ok},
         "roofline": {"bound": "hbm", "kernel": key, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"
                      if peak_src == "measured" else "fallback 6.65 TB/s",
@@ -650,9 +679,11 @@ def run_reference(args):
     threads = oracle.num_threads()
     vol0 = oracle.volume(basin.grid, basin.phi)
     run = lambda: oracle.project(basin, volume0=vol0, dt=DT, tol=TOL, maxiter=MAXITER)
+    warm = max(1, args.warmup)  # W warm-up projections, untimed (each takes seconds on the CPU)
     t0 = time.perf_counter()
-    run()  # one warm-up projection whatever W is: each takes seconds on the CPU
-    first = time.perf_counter() - t0
+    for _ in range(warm):
+        run()
+    first = (time.perf_counter() - t0) / warm
     budget = args.reference_seconds
     steps = max(1, min(args.steps, int(budget / max(first, 1e-3))))
     t0 = time.perf_counter()
@@ -661,12 +692,12 @@ def run_reference(args):
     el = time.perf_counter() - t0
     value = steps / el
     out = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-           "steps_timed": steps, "warmup": 1, "ms_per_step": round(1e3 * el / steps, 2), "higher_is_better": True,
+           "steps_timed": steps, "warmup": warm, "ms_per_step": round(1e3 * el / steps, 2), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset exists)",
            "impl": "reference", "config": workload_config("fp32", False), "iterations": info.iterations,
            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
                             "sample": f"{steps} full whirl256 projection(s) timed (of {args.steps} asked, within "
-                                      f"{budget:.0f} s) after 1 warm-up, C/OpenMP restatement of src/flip.jl"
+                                      f"{budget:.0f} s) after {warm} warm-up(s), C/OpenMP restatement of src/flip.jl"
                                       f":1144-1156 (the Julia/Vulkan reference cannot run here)"},
            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)

@@ -266,6 +266,17 @@ class Projector:
         check(self.lib.mpp_gradient(self._ctx, _ptr(u), _ptr(v), _ptr(w), _ptr(fu), _ptr(fv), _ptr(fw), _ptr(P),
                                     _ptr(types), _ptr(phi), _stream_ptr(stream)))
 
+    def set_smoothers(self, fine: str, coarse: str | None = None):
+        """The smoother form of the fine level and of the coarser row-split levels
+        ("vector", "tma" or "column"; ``mpp_ctx_set_smoothers``)."""
+        forms = {name: code for code, name in _lib.SMOOTHERS.items()}
+        check(self.lib.mpp_ctx_set_smoothers(self._ctx, forms[fine], forms[coarse or fine]))
+
+    def smoothers(self) -> tuple:
+        f, c = ctypes.c_int(), ctypes.c_int()
+        check(self.lib.mpp_ctx_smoothers(self._ctx, ctypes.byref(f), ctypes.byref(c)))
+        return _lib.SMOOTHERS[f.value], _lib.SMOOTHERS[c.value]
+
     def autotune(self, u, v, w, types, phi, stream=None) -> dict:
         """``mpp_autotune`` on this basin's own solve: keeps the fastest smoother forms and
         sweep counts on the context; returns {"chosen": {...}, "table": [...]}."""
