@@ -402,6 +402,8 @@ def run_mpp(args):
         out["whirlpool384"] = bench_whirlpool(max(3, min(args.steps, 10)))
         torch.cuda.empty_cache()
         out["extrapolate"] = bench_extrapolate(max(3, min(args.steps, 10)))
+        torch.cuda.empty_cache()
+        out["levelset"] = bench_levelset(max(3, min(args.steps, 10)))
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(basin, max_seconds=args.cpu_seconds)
     if rank == 0:
@@ -594,6 +596,73 @@ def bench_extrapolate(steps):
             "algorithmic_bytes": nbytes, "achieved_gbs": round(gbs, 1), "peak_gbs": hbm,
             "frac": round(gbs / hbm, 4), "peak_source": src,
             "reference_pass_gbs": round(10.0 * faces * layers / (ms / 1e3) / 1e9, 1), "steps": steps}
+
+
+def bench_levelset(steps):
+    """step!'s level-set phase before the projection (src/flip.jl:1399-1401) on the 256^3
+    whirlpool: redistance! (band + 3 = 7 Jacobi sweeps, classify! fused into the last) and
+    filltrapped! (device-side round loop), each timed with CUDA events. The level set is the
+    basin's, made wavy and noisy with sealed air pockets under the surface, so the sweeps
+    have surface, far-field and clamped cells and the fill has pockets to fill. Algorithmic
+    bytes: a sweep reads and writes phi once (8 bytes a cell), classify! writes a class
+    (1); filltrapped! reads the classes once (1), keeps a bit a cell for the air and the
+    reached cells (0.25 written, 0.25 read by the fill) and rewrites the cells it fills."""
+    import numpy as np
+    import torch
+
+    import mpp
+    from mpp import scene
+
+    b = scene.config_basin("whirl256")
+    g = b.grid
+    n1, n2, n3 = g.n
+    rng = np.random.default_rng(1001)
+    phi = b.phi.reshape(n3, n2, n1) + (0.3 * np.sin(0.2 * np.arange(n1))[None, None, :] * g.dx)
+    phi = (phi + rng.uniform(-0.2, 0.2, phi.shape) * g.dx).astype(np.float32)
+    types = b.types.reshape(n3, n2, n1).copy()
+    types[(types == scene.LIQUID) & (rng.random(types.shape) < 0.02)] = scene.AIR
+    phi[types == scene.AIR] = np.abs(phi[types == scene.AIR])
+    dev = torch.device("cuda")
+    phi0_h = torch.from_numpy(phi.reshape(-1)).to(dev)
+    types0_h = torch.from_numpy(types.reshape(-1)).to(dev)
+    p = mpp.Projector(g)
+    d_phi, d_phi0 = phi0_h.clone(), torch.empty_like(phi0_h)
+    d_types = types0_h.clone()
+    it = 7
+    N = g.ncells
+
+    def run():
+        d_phi.copy_(phi0_h)
+        d_types.copy_(types0_h)
+        e0, e1, e2 = _events() + (torch.cuda.Event(enable_timing=True),)
+        e0.record()
+        out = p.redistance(d_phi, d_phi0, it, types=d_types)
+        e1.record()
+        p.filltrapped(d_types, out, 32, rounds=False)
+        e2.record()
+        return e0, e1, e2
+
+    for _ in range(3):
+        run()
+    ev = [run() for _ in range(steps)]
+    torch.cuda.synchronize()
+    ms_r = sum(a.elapsed_time(b_) for a, b_, _ in ev) / steps
+    ms_f = sum(b_.elapsed_time(c) for _, b_, c in ev) / steps
+    d_phi.copy_(phi0_h)
+    out = p.redistance(d_phi, d_phi0, it, types=d_types)
+    classified = d_types.clone()
+    rounds = p.filltrapped(d_types, out, 32)
+    filled = int(torch.count_nonzero(d_types != classified))
+    hbm, src = peaks()
+    bytes_r = N * (8.0 * it + 1.0)
+    bytes_f = N * (1.0 + 0.5) + 5.0 * filled
+    return {"workload": "whirl256 level set (wavy, noisy, 2% of the water made air pockets)", "cells": N,
+            "redistance_sweeps": it, "redistance_classify_ms": round(ms_r, 4),
+            "redistance_gbs": round(bytes_r / (ms_r / 1e3) / 1e9, 1),
+            "redistance_frac": round(bytes_r / (ms_r / 1e3) / 1e9 / hbm, 4),
+            "filltrapped_ms": round(ms_f, 4), "filltrapped_rounds": rounds, "cells_filled": filled,
+            "filltrapped_gbs": round(bytes_f / (ms_f / 1e3) / 1e9, 1), "peak_gbs": hbm, "peak_source": src,
+            "steps": steps}
 
 
 def bench_whirlpool(steps):

@@ -171,12 +171,37 @@ int mpp_advect_phi(mpp_ctx* ctx, float* ophi, const float* phi, const float* u, 
  * (solidify!, :801-806). fu, fv, fw end as the reached flags. The six arrays must not
  * overlap; layers <= 0 runs no layer (the zeroing only; the flags stay as they are), and
  * more than 253 layers is refused (MPP_ERR_INVALID). The first call on a context, whatever
- * `layers` is, allocates the context's scratch, a byte for each face of the three arrays
- * (rows padded to 16): make it outside any stream capture. That scratch belongs to the
+ * `layers` is, allocates the context's scratch, three bit masks over the faces of the three
+ * arrays (rows padded to 32 faces), and builds the wall mask: make it outside any stream
+ * capture. That scratch belongs to the
  * context while each call runs on the caller's stream, so calls on one context must not
  * overlap on the GPU (two streams at once race on it). */
 int mpp_extrapolate(mpp_ctx* ctx, float* u, float* v, float* w, uint8_t* fu, uint8_t* fv, uint8_t* fw,
                     int layers, mpp_stream stream);
+
+/* ---- the level-set passes step! runs before the projection (src/flip.jl:1399-1401) ---- */
+/* redistance!(s; iterations) (src/flip.jl:673-680): `iterations` Jacobi sweeps of
+ * reinit_kernel! (:631-666) with phimax = (iterations + 1) dx, between phi and phi0 as the
+ * reference swaps s.phi and s.phi0: sweep 1 reads phi and writes phi0, sweep 2 reads phi0
+ * and writes phi, and so on, so the result is in phi0 when `iterations` is odd and in phi
+ * when it is even (the caller swaps its two arrays `iterations` times, as redistance!
+ * does). `types` (may be NULL) gets classify! of the result (src/flip.jl:682-686), fused
+ * into the last sweep (with iterations = 0, classify! of phi). Bit-identical to the
+ * reference's Float32 arithmetic. phi and phi0 must not overlap. */
+int mpp_redistance(mpp_ctx* ctx, float* phi, float* phi0, int iterations, uint8_t* types, mpp_stream stream);
+/* classify!(s) (src/flip.jl:682-686): SOLID where the cell centre is outside the walls, else
+ * LIQUID where phi < 0, else AIR. */
+int mpp_classify(mpp_ctx* ctx, uint8_t* types, const float* phi, mpp_stream stream);
+/* filltrapped!(s; maxrounds) (src/flip.jl:747-760), in place: air is reached from the
+ * grid's top layer by rounds of sweeps along z, x and y (each fills every run of air along
+ * a line that holds a reached cell) until a round reaches nothing or `maxrounds` rounds
+ * have run; the air left becomes LIQUID with phi = min(phi, -2 dx). The round loop runs on
+ * the device (a CUDA graph whose condition the last kernel of a round sets): no host round
+ * trip. `rounds` (a host pointer, may be NULL) gets the rounds run, which synchronises
+ * `stream`. The first call on a context allocates its masks (a bit a cell, twice) and
+ * captures the round loop: make it outside any stream capture. Calls on one context must
+ * not overlap on the GPU. */
+int mpp_filltrapped(mpp_ctx* ctx, uint8_t* types, float* phi, int maxrounds, int* rounds, mpp_stream stream);
 
 /* The adjoint of mpp_advect (no reference counterpart; the reverse of its steps): the
  * cotangent (gou, gov, gow) of its outputs in; du, dv, dw = the cotangent of (u, v, w),

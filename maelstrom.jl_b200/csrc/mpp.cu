@@ -19,6 +19,7 @@
 #include "mpp_advect.cuh"
 #include "mpp_extrap.cuh"
 #include "mpp_fgmres.cuh"
+#include "mpp_levelset.cuh"
 #include "mpp_tma.cuh"
 #include "mpp_cmg.cuh"
 
@@ -119,7 +120,7 @@ struct mpp_ctx {
     uint8_t* tflag_all;
     int* edges;  // the levels' edge flags
     // extrapolation scratch (allocated at the first mpp_extrapolate, whatever its layer
-    // count): a reach code for each of the three face arrays' ext_n faces
+    // count): ext_n mask words, three masks (open, reach ping and pong) per face array
     uint8_t* ext_r;
     int64_t ext_n;
     size_t tflag_bytes;
@@ -176,6 +177,12 @@ struct mpp_ctx {
     double fg_residual;
     void* vjp_beta;  // the adjoint solve's right-hand side (natural, V's type), allocated on first use
     double* adv_acc[3];  // FP64 accumulators of the advection adjoint (face shapes), on first use
+    // trapped-air fill (mpp_filltrapped), on first use: AIR and reached bit masks, the round
+    // loop's state, and the graph of the round loop (a conditional WHILE node)
+    uint32_t *trap_air, *trap_reach;
+    TrapState* trap_st;
+    cudaGraph_t trap_graph;
+    cudaGraphExec_t trap_exec;
 };
 
 namespace {
@@ -1344,6 +1351,8 @@ const char* mpp_version(void) { return "libmpp 0.1 (sm_100a)"; }
 int mpp_ctx_destroy(mpp_ctx* c) {
     if (!c) return MPP_OK;
     drop_graphs(c);
+    if (c->trap_exec) cudaGraphExecDestroy(c->trap_exec);
+    if (c->trap_graph) cudaGraphDestroy(c->trap_graph);
     for (void* p : c->allocs) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
     if (c->fgd_host) cudaFreeHost(c->fgd_host);
@@ -1434,6 +1443,10 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
     c->fg_residual = 0.0;
     c->vjp_beta = nullptr;
     for (int a = 0; a < 3; a++) c->adv_acc[a] = nullptr;
+    c->trap_air = c->trap_reach = nullptr;
+    c->trap_st = nullptr;
+    c->trap_graph = nullptr;
+    c->trap_exec = nullptr;
     auto fail = [&](int e) {
         mpp_ctx_destroy(c);
         return e;
@@ -2065,27 +2078,26 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
         set_err("at most %d extrapolation layers", EXTRAP_MAX_LAYERS);
         return MPP_ERR_INVALID;
     }
-    ExtChunks E;
+    ExtBits E;
     memset(&E, 0, sizeof(E));
     float* X[3] = {u, v, w};
     uint8_t* Fl[3] = {fu, fv, fw};
-    int64_t n[3], cb[3], ctot = 0, nthreads = 0;
+    int64_t n[3], words[3], wtot = 0, bytes_max = 0, words_max = 0;
     for (int a = 0; a < 3; a++) {
         n[a] = 1;
         for (int e = 0; e < 3; e++) {
             E.d[a][e] = c->grid.n[e] + (a == e);
             n[a] *= E.d[a][e];
         }
-        E.pitch[a] = (E.d[a][0] + EXT_CHUNK - 1) / EXT_CHUNK * EXT_CHUNK;
-        const int64_t rows = (int64_t)E.d[a][1] * E.d[a][2];
-        cb[a] = rows * E.pitch[a];
-        if (n[a] >= ((int64_t)1 << 31) || cb[a] >= ((int64_t)1 << 31)) {
+        E.W[a] = (E.d[a][0] + 31) / 32;
+        words[a] = (int64_t)E.W[a] * E.d[a][1] * E.d[a][2];
+        if (n[a] >= ((int64_t)1 << 31) || 4 * words[a] >= ((int64_t)1 << 31)) {
             set_err("face array of 2^31 or more faces");
             return MPP_ERR_INVALID;
         }
-        const int64_t th = rows * (E.pitch[a] / EXT_CHUNK);
-        nthreads = th > nthreads ? th : nthreads;
-        ctot += cb[a];
+        wtot += words[a];
+        bytes_max = std::max<int64_t>(bytes_max, 4 * words[a]);
+        words_max = std::max<int64_t>(words_max, words[a]);
     }
     // a layer reads its neighbours' faces while others are written: no two of the six
     // arrays may share memory
@@ -2098,23 +2110,31 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
                 set_err("extrapolation arrays overlap");
                 return MPP_ERR_INVALID;
             }
-    if (c->ext_n < ctot) {
-        if (int e = alloc(c, (void**)&c->ext_r, (size_t)ctot)) return e;
-        c->ext_n = ctot;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Geo g = geo_of(c->grid);
+    const bool first = c->ext_n == 0;
+    if (first) {  // the masks (open, and the two reach masks), on the first call
+        if (int e = alloc(c, (void**)&c->ext_r, sizeof(uint32_t) * (size_t)(3 * wtot))) return e;
+        c->ext_n = 3 * wtot;
     }
-    int64_t o = 0;  // each array's codes start 16-byte aligned (cb is a multiple of 16)
+    int64_t o = 0;
+    uint32_t* M = reinterpret_cast<uint32_t*>(c->ext_r);
     for (int a = 0; a < 3; a++) {
         E.x[a] = X[a];
         E.f[a] = Fl[a];
-        E.code[a] = c->ext_r + o;
-        o += cb[a];
+        E.open[a] = M + o;
+        E.ra[a] = M + o + words[a];
+        E.rb[a] = M + o + 2 * words[a];
+        o += 3 * words[a];
     }
-    cudaStream_t s = (cudaStream_t)stream;
-    const dim3 grid(grid_cells(c, nthreads), 3);
-    const Geo g = geo_of(c->grid);
-    launch(k_extrap_codes, grid, TPB, 0, s, g, E);
-    for (int l = 1; l <= layers; l++) launch(k_extrap_layer, grid, TPB, 0, s, E, l);
-    launch(k_extrap_final, grid, TPB, 0, s, g, E, layers == 0 ? 1 : 0);
+    if (first) {  // the walls are the grid's geometry: the open mask is built once
+        launch(k_extrap_open, dim3(grid_cells(c, words_max), 3), TPB, 0, s, g, E);
+        c->launches++;
+    }
+    launch(k_extrap_flags, dim3(grid_cells(c, words_max), 3), TPB, 0, s, E);
+    const dim3 grid(grid_cells(c, bytes_max), 3);
+    for (int l = 1; l <= layers; l++) launch(k_extrap_layer, grid, TPB, 0, s, E, l & 1);
+    launch(k_extrap_final, grid, TPB, 0, s, E, layers % 2 == 0 ? 1 : 0, layers == 0 ? 1 : 0);
     c->launches += layers + 2;
     CK(cudaGetLastError());
     return MPP_OK;
@@ -2200,6 +2220,121 @@ int mpp_vjp_faces(mpp_ctx* c, float* ou, float* ov, float* ow, const float* gu, 
            ow, gu, gv, gw, mu, types);
     c->launches++;
     CK(cudaGetLastError());
+    return MPP_OK;
+}
+
+int mpp_redistance(mpp_ctx* c, float* phi, float* phi0, int iterations, uint8_t* types, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!phi || (iterations > 0 && !phi0) || iterations < 0) {
+        set_err("null array or negative iteration count");
+        return MPP_ERR_INVALID;
+    }
+    const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+    if (iterations > 0 && phi0 < phi + N && phi < phi0 + N) {
+        set_err("phi and phi0 overlap");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const Geo g = geo_of(c->grid);
+    if (iterations == 0) {
+        if (types) {
+            launch(k_classify, grid_cells(c, N), TPB, 0, s, g, (const float*)phi, types);
+            c->launches++;
+        }
+        CK(cudaGetLastError());
+        return MPP_OK;
+    }
+    // phimax = Float32((iterations + 1) * dx) (src/flip.jl:674)
+    const float phimax = (float)(iterations + 1) * c->grid.dx;
+    auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+    const bool v4 = c->grid.n[0] % 4 == 0 && al(phi) && al(phi0) && (!types || (reinterpret_cast<uintptr_t>(types) & 3) == 0);
+    float* src = phi;
+    float* dst = phi0;
+    for (int it = 0; it < iterations; it++) {
+        uint8_t* ty = it + 1 == iterations ? types : nullptr;
+        if (v4) launch(k_reinit<4>, grid_cells(c, N / 4), TPB, 0, s, g, (const float*)src, dst, phimax, ty);
+        else launch(k_reinit<1>, grid_cells(c, N), TPB, 0, s, g, (const float*)src, dst, phimax, ty);
+        std::swap(src, dst);
+    }
+    c->launches += iterations;
+    CK(cudaGetLastError());
+    return MPP_OK;
+}
+
+int mpp_classify(mpp_ctx* c, uint8_t* types, const float* phi, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!types || !phi) {
+        set_err("null array");
+        return MPP_ERR_INVALID;
+    }
+    const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+    launch(k_classify, grid_cells(c, N), TPB, 0, (cudaStream_t)stream, geo_of(c->grid), phi, types);
+    c->launches++;
+    CK(cudaGetLastError());
+    return MPP_OK;
+}
+
+int mpp_filltrapped(mpp_ctx* c, uint8_t* types, float* phi, int maxrounds, int* rounds, mpp_stream stream) {
+    if (int e = check_ctx(c)) return e;
+    if (!types || !phi || maxrounds < 0) {
+        set_err("null array or negative maxrounds");
+        return MPP_ERR_INVALID;
+    }
+    const int n1 = c->grid.n[0], n2 = c->grid.n[1], n3 = c->grid.n[2];
+    const int W1 = (n1 + 31) / 32;
+    const int64_t words = (int64_t)W1 * n2 * n3;
+    if (!c->trap_air) {  // the masks and the round loop's graph, on the first call
+        if (int e = alloc(c, (void**)&c->trap_air, sizeof(uint32_t) * (size_t)words)) return e;
+        if (int e = alloc(c, (void**)&c->trap_reach, sizeof(uint32_t) * (size_t)words)) return e;
+        if (int e = alloc(c, (void**)&c->trap_st, sizeof(TrapState))) return e;
+    }
+    TrapMasks T{c->trap_air, c->trap_reach, n1, n2, n3, W1};
+    const int64_t rows = (int64_t)n2 * n3;
+    const int wpb = TPB / 32;
+    auto blocks = [&](int64_t units, int per_block) {
+        const int64_t b = (units + per_block - 1) / per_block, cap = (int64_t)c->nsm * MAXBLOCKS_PER_SM;
+        return (int)(b < 1 ? 1 : (b < cap ? b : cap));
+    };
+    if (!c->trap_exec) {
+        cudaGraph_t g;
+        CK(cudaGraphCreate(&g, 0));
+        c->trap_graph = g;
+        cudaGraphConditionalHandle cond;
+        CK(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CK(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        // one round (src/flip.jl:751-757): sweeps along z, x, y, then the round's end
+        CK(cudaStreamBeginCaptureToGraph(c->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        launch(k_trap_sweep_col, blocks((int64_t)W1 * n2, wpb), TPB, 0, c->cap, T, c->trap_st, 2);
+        launch(k_trap_sweep_x, blocks(rows, TPB), TPB, 0, c->cap, T, c->trap_st);
+        launch(k_trap_sweep_col, blocks((int64_t)W1 * n3, wpb), TPB, 0, c->cap, T, c->trap_st, 1);
+        launch(k_trap_round, 1, 1, 0, c->cap, c->trap_st, cond);
+        const cudaError_t le = cudaGetLastError();
+        CK(cudaStreamEndCapture(c->cap, &body));
+        CK(le);
+        CK(cudaGraphInstantiate(&c->trap_exec, g, 0));
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool vec = n1 % 32 == 0 && (reinterpret_cast<uintptr_t>(types) & 15) == 0;
+    launch(k_trap_pack, blocks(words, TPB), TPB, 0, s, T, (const uint8_t*)types, c->trap_st, maxrounds, vec ? 1 : 0);
+    c->launches++;
+    if (maxrounds > 0) {
+        CK(cudaGraphLaunch(c->trap_exec, s));
+    }
+    launch(k_trap_fill, blocks(words, TPB), TPB, 0, s, T, types, phi, 2.0f * c->grid.dx);
+    c->launches++;
+    CK(cudaGetLastError());
+    if (rounds) {
+        CK(cudaMemcpyAsync(rounds, &c->trap_st->rounds, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        c->launches += 4 * (int64_t)*rounds;
+    }
     return MPP_OK;
 }
 

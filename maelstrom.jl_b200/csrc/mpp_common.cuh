@@ -79,6 +79,25 @@ __device__ __forceinline__ void st(T* p, C v) {
     else *p = (T)v;
 }
 
+// c + a for a stored value a and an arithmetic value c: for the 16-bit storage forms one
+// mixed-precision add (PTX add.rn.f32.f16 / .bf16: a is widened exactly inside the add,
+// which rounds once), the same bits as widening a first and adding in FP32, in one
+// instruction instead of two.
+template <class C, class T>
+__device__ __forceinline__ C addm(T a, C c) {
+    if constexpr (std::is_same<T, __half>::value && std::is_same<C, float>::value) {
+        float d;
+        asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(d) : "h"(__half_as_ushort(a)), "f"(c));
+        return d;
+    } else if constexpr (std::is_same<T, __nv_bfloat16>::value && std::is_same<C, float>::value) {
+        float d;
+        asm("add.rn.f32.bf16 %0, %1, %2;" : "=f"(d) : "h"(__bfloat16_as_ushort(a)), "f"(c));
+        return d;
+    } else {
+        return ld<C>(&a) + c;
+    }
+}
+
 // theta (src/flip.jl:113): the free surface's fraction of the way from a liquid cell
 // centre to an air one, clamp(phi_i / (phi_i - phi_j), 0.01, 1) in Julia's clamp order.
 template <class C>

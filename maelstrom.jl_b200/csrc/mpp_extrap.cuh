@@ -5,23 +5,23 @@
 // projection's gradient pass leaves them with their valid flags fu, fv, fw.
 //
 // The reference ping-pongs every face's value and flag through a scratch copy each layer
-// (10 bytes a face a layer). Here a one-byte reach code a face replaces the copies: 0 for a
-// face flagged on entry, l for a face first reached by layer l, UNREACHED otherwise. Layer l
-// takes a face that is not yet reached and not walled to the mean of its neighbours whose
-// code is below l, and writes its value in place: those neighbours' values are final (a
-// value is written once, in the layer that reaches its face), and a face written in layer l
-// is read by no other face in layer l (its code was UNREACHED and becomes l, neither below
-// l). So each layer matches the reference's bit for bit, and moves about a byte a face (the
-// codes) plus the values of the faces it reaches. A last pass writes the 0/1 flags and
-// zeroes what no layer reached and every walled face. One launch a pass covers all three
-// arrays (blockIdx.y is the array); a thread takes 16 consecutive faces of a row.
+// (10 bytes a face a layer). Here the flags are bit masks, 32 faces of a row per word (rows
+// padded to whole words): R_l, the faces valid after layer l (R_0: flagged on entry), and
+// O, the faces that are not walled (the grid's geometry alone, built once per context). A
+// layer is a bit dilation: D_l = (R_{l-1} moved one face along each of the six directions)
+// & O & ~R_{l-1} are the faces it reaches, R_l = R_{l-1} | D_l (ping-pong masks). Only the
+// faces of D_l load values: each takes the Float32 mean of its neighbours in R_{l-1},
+// summed +x, -x, +y, -y, +z, -z, whose values are final (a value is written once, in the
+// layer that reaches its face, and no face of D_l is in R_{l-1}). So every layer matches the
+// reference's bit for bit, and moves a bit a face (the masks, which stay in L2) plus the
+// values on the front. A last pass writes the 0/1 flags and zeroes what no layer reached
+// and every walled face. One launch a pass covers all three arrays (blockIdx.y is the
+// array); a thread takes one byte of a mask: 8 consecutive faces of a row.
 #pragma once
 
 #include "mpp_base.cuh"
 
 namespace mpp {
-
-constexpr uint8_t UNREACHED = 0xFF;
 
 // walled (src/flip.jl:784-789) for the faces of one row (j, k) of the array along `ax`: the
 // grid's own edge, or a SOLID cell on either side (issolidcell, src/flip.jl:64-66, with the
@@ -61,163 +61,171 @@ __device__ __forceinline__ T pick3(int ax, T a, T b, T c) {
     return ax == 0 ? a : (ax == 1 ? b : c);
 }
 
-// The codes live in rows padded to a multiple of 16 bytes (pitch P), so a thread reads the
-// codes of 16 consecutive faces of a row, and of the same 16 columns in the rows at -+y and
-// -+z, as five 16-byte loads (one round trip), and loads values only for the faces it
-// reaches. Padding reads as UNREACHED. A conversion pass writes the first codes: 0 for a
-// face flagged on entry, WALLED for an unflagged walled face (never reached, so the layers
-// skip the geometry), UNREACHED otherwise.
-constexpr uint8_t WALLED = 0xFE;
-constexpr int EXTRAP_MAX_LAYERS = 253;  // codes 1 .. 253
-constexpr int EXT_CHUNK = 16;
+constexpr int EXTRAP_MAX_LAYERS = 253;
 
-struct ExtChunks {
+// The three arrays, their masks (W words a row, rows in the arrays' row order) and dims.
+struct ExtBits {
     float* x[3];
     uint8_t* f[3];
-    uint8_t* code[3];  // rows of `pitch[a]` bytes
+    uint32_t* open[3];  // O: in range and not walled
+    uint32_t* ra[3];    // R, ping
+    uint32_t* rb[3];    // R, pong
     int d[3][3];
-    int pitch[3];
+    int W[3];
 };
 
-struct Chunk {
-    int ax, a1, a2, a3, P;
-    unsigned r;  // row
-    int j, k, i0;
+// A thread's byte of a mask: row r (j, k) of array ax, word wx, bits sh .. sh+7.
+struct ExtByte {
+    int ax, a1, a2, a3, W;
+    unsigned r;
+    int j, k, wx, sh;
 };
-__device__ __forceinline__ Chunk chunk_of(const ExtChunks& E, unsigned t) {
-    Chunk c;
-    c.ax = blockIdx.y;
-    c.a1 = pick3(c.ax, E.d[0][0], E.d[1][0], E.d[2][0]);
-    c.a2 = pick3(c.ax, E.d[0][1], E.d[1][1], E.d[2][1]);
-    c.a3 = pick3(c.ax, E.d[0][2], E.d[1][2], E.d[2][2]);
-    c.P = pick3(c.ax, E.pitch[0], E.pitch[1], E.pitch[2]);
-    const unsigned cpr = (unsigned)c.P / EXT_CHUNK;
-    c.r = t / cpr;
-    c.i0 = (int)(t % cpr) * EXT_CHUNK;
-    c.j = (int)(c.r % (unsigned)c.a2);
-    c.k = (int)(c.r / (unsigned)c.a2);
-    return c;
-}
-__device__ __forceinline__ unsigned chunk_threads(const ExtChunks& E, int ax) {
+__device__ __forceinline__ unsigned ext_bytes(const ExtBits& E, int ax) {
     const int a2 = pick3(ax, E.d[0][1], E.d[1][1], E.d[2][1]), a3 = pick3(ax, E.d[0][2], E.d[1][2], E.d[2][2]);
-    const int P = pick3(ax, E.pitch[0], E.pitch[1], E.pitch[2]);
-    return (unsigned)a2 * (unsigned)a3 * (unsigned)(P / EXT_CHUNK);
+    return (unsigned)a2 * (unsigned)a3 * (unsigned)pick3(ax, E.W[0], E.W[1], E.W[2]) * 4u;
 }
-union Code16 {
-    uint4 v;
-    uint8_t b[16];
-};
+__device__ __forceinline__ ExtByte ext_byte(const ExtBits& E, unsigned t) {
+    ExtByte b;
+    b.ax = blockIdx.y;
+    b.a1 = pick3(b.ax, E.d[0][0], E.d[1][0], E.d[2][0]);
+    b.a2 = pick3(b.ax, E.d[0][1], E.d[1][1], E.d[2][1]);
+    b.a3 = pick3(b.ax, E.d[0][2], E.d[1][2], E.d[2][2]);
+    b.W = pick3(b.ax, E.W[0], E.W[1], E.W[2]);
+    const unsigned bpr = 4u * (unsigned)b.W;
+    b.r = t / bpr;
+    const int q = (int)(t % bpr);
+    b.wx = q >> 2;
+    b.sh = 8 * (q & 3);
+    b.j = (int)(b.r % (unsigned)b.a2);
+    b.k = (int)(b.r / (unsigned)b.a2);
+    return b;
+}
 
-// The first codes, from the caller's flags.
-__global__ void __launch_bounds__(TPB) k_extrap_codes(Geo g, ExtChunks E) {
+// The open mask O (in range and not walled): the grid's geometry only, once per context.
+// A thread a word.
+__global__ void __launch_bounds__(TPB) k_extrap_open(Geo g, ExtBits E) {
     pdl_wait();
     pdl_trigger();
-    const unsigned n = chunk_threads(E, blockIdx.y);
+    const int ax = blockIdx.y;
+    const int a1 = pick3(ax, E.d[0][0], E.d[1][0], E.d[2][0]), a2 = pick3(ax, E.d[0][1], E.d[1][1], E.d[2][1]);
+    const int a3 = pick3(ax, E.d[0][2], E.d[1][2], E.d[2][2]), W = pick3(ax, E.W[0], E.W[1], E.W[2]);
+    uint32_t* O = pick3(ax, E.open[0], E.open[1], E.open[2]);
+    const unsigned n = (unsigned)W * (unsigned)a2 * (unsigned)a3;
     for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const Chunk c = chunk_of(E, t);
-        const uint8_t* fin = pick3(c.ax, E.f[0], E.f[1], E.f[2]);
-        uint8_t* R = pick3(c.ax, E.code[0], E.code[1], E.code[2]);
-        const unsigned base = c.r * (unsigned)c.a1;
-        uint8_t fl[EXT_CHUNK];
-#pragma unroll
-        for (int q = 0; q < EXT_CHUNK; q++) fl[q] = c.i0 + q < c.a1 ? fin[base + c.i0 + q] : (uint8_t)0;
-        const RowWall w = row_wall(g, c.ax, c.j, c.k);
-        Code16 out;
-#pragma unroll
-        for (int q = 0; q < EXT_CHUNK; q++) {
-            const int i = c.i0 + q;
-            out.b[q] = i >= c.a1 ? UNREACHED : (fl[q] ? (uint8_t)0 : (walled_in_row(g, w, c.ax, i) ? WALLED : UNREACHED));
+        const unsigned r = t / (unsigned)W;
+        const int wx = (int)(t % (unsigned)W);
+        const RowWall w = row_wall(g, ax, (int)(r % (unsigned)a2), (int)(r / (unsigned)a2));
+        uint32_t o = 0;
+        for (int b = 0; b < 32; b++) {
+            const int i = 32 * wx + b;
+            if (i < a1 && !walled_in_row(g, w, ax, i)) o |= 1u << b;
         }
-        *reinterpret_cast<uint4*>(R + c.r * (unsigned)c.P + c.i0) = out.v;
+        O[t] = o;
     }
 }
 
-// Layer `layer` (1 .. EXTRAP_MAX_LAYERS) on the codes.
-__global__ void __launch_bounds__(TPB, 4) k_extrap_layer(ExtChunks E, int layer) {
+// R_0 from the caller's flags (a face is valid when its flag is not 0). A thread a word.
+__global__ void __launch_bounds__(TPB) k_extrap_flags(ExtBits E) {
     pdl_wait();
     pdl_trigger();
-    const unsigned n = chunk_threads(E, blockIdx.y);
+    const int ax = blockIdx.y;
+    const int a1 = pick3(ax, E.d[0][0], E.d[1][0], E.d[2][0]), a2 = pick3(ax, E.d[0][1], E.d[1][1], E.d[2][1]);
+    const int a3 = pick3(ax, E.d[0][2], E.d[1][2], E.d[2][2]), W = pick3(ax, E.W[0], E.W[1], E.W[2]);
+    const uint8_t* fin = pick3(ax, E.f[0], E.f[1], E.f[2]);
+    uint32_t* R = pick3(ax, E.ra[0], E.ra[1], E.ra[2]);
+    const unsigned n = (unsigned)W * (unsigned)a2 * (unsigned)a3;
     for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const Chunk c = chunk_of(E, t);
-        uint8_t* R = pick3(c.ax, E.code[0], E.code[1], E.code[2]);
-        float* x = pick3(c.ax, E.x[0], E.x[1], E.x[2]);
-        const unsigned rowoff = c.r * (unsigned)c.P + (unsigned)c.i0;
-        const unsigned P = (unsigned)c.P, PZ = (unsigned)c.P * (unsigned)c.a2;
-        Code16 own, yp, ym, zp, zm;
-        const uint4 none = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
-        own.v = *reinterpret_cast<const uint4*>(R + rowoff);
-        yp.v = c.j + 1 < c.a2 ? *reinterpret_cast<const uint4*>(R + rowoff + P) : none;
-        ym.v = c.j > 0 ? *reinterpret_cast<const uint4*>(R + rowoff - P) : none;
-        zp.v = c.k + 1 < c.a3 ? *reinterpret_cast<const uint4*>(R + rowoff + PZ) : none;
-        zm.v = c.k > 0 ? *reinterpret_cast<const uint4*>(R + rowoff - PZ) : none;
-        const uint8_t left = c.i0 > 0 ? R[rowoff - 1] : UNREACHED;
-        const uint8_t right = c.i0 + EXT_CHUNK < c.a1 ? R[rowoff + EXT_CHUNK] : UNREACHED;
-        // the neighbours each face takes (reached before this layer), +x -x +y -y +z -z
-        unsigned take[EXT_CHUNK];
-        bool any = false;
+        const unsigned r = t / (unsigned)W;
+        const int wx = (int)(t % (unsigned)W);
+        const uint8_t* row = fin + r * (unsigned)a1 + 32u * (unsigned)wx;
+        const int cnt = a1 - 32 * wx < 32 ? a1 - 32 * wx : 32;
+        uint8_t fl[32];
 #pragma unroll
-        for (int q = 0; q < EXT_CHUNK; q++) {
-            take[q] = 0;
-            if (own.b[q] == UNREACHED) {  // padding is UNREACHED too, but has no reached neighbour
-                const uint8_t nb[6] = {q + 1 < EXT_CHUNK ? own.b[q + 1] : right, q > 0 ? own.b[q - 1] : left,
-                                       yp.b[q], ym.b[q], zp.b[q], zm.b[q]};
+        for (int b = 0; b < 32; b++) fl[b] = b < cnt ? row[b] : (uint8_t)0;
+        uint32_t m = 0;
 #pragma unroll
-                for (int e = 0; e < 6; e++)
-                    if ((int)nb[e] < layer) take[q] |= 1u << e;
-                if (c.i0 + q >= c.a1) take[q] = 0;
-                any = any || take[q] != 0;
-            }
-        }
-        if (!any) continue;
-        const unsigned s1 = (unsigned)c.a1, s2 = (unsigned)c.a1 * (unsigned)c.a2;
-        const unsigned base = c.r * s1 + (unsigned)c.i0;
-        // the taken values, eight faces' loads at a time before their stores
+        for (int b = 0; b < 32; b++)
+            if (fl[b]) m |= 1u << b;
+        R[t] = m;
+    }
+}
+
+// Layer `layer` (1-based): Rn = R | D, and the values of the faces D reaches. `from_a`: the
+// layer reads ra and writes rb (else the other way round).
+__global__ void __launch_bounds__(TPB) k_extrap_layer(ExtBits E, int from_a) {
+    pdl_wait();
+    pdl_trigger();
+    const unsigned n = ext_bytes(E, blockIdx.y);
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const ExtByte b = ext_byte(E, t);
+        const uint32_t* R = from_a ? pick3(b.ax, E.ra[0], E.ra[1], E.ra[2]) : pick3(b.ax, E.rb[0], E.rb[1], E.rb[2]);
+        uint32_t* Rn = from_a ? pick3(b.ax, E.rb[0], E.rb[1], E.rb[2]) : pick3(b.ax, E.ra[0], E.ra[1], E.ra[2]);
+        const uint32_t* O = pick3(b.ax, E.open[0], E.open[1], E.open[2]);
+        const unsigned w = b.r * (unsigned)b.W + (unsigned)b.wx;
+        const unsigned PY = (unsigned)b.W, PZ = (unsigned)b.W * (unsigned)b.a2;
+        const uint32_t rc = R[w], o = O[w];
+        const uint32_t rl = b.wx > 0 ? R[w - 1] : 0u, rr = b.wx + 1 < b.W ? R[w + 1] : 0u;
+        const uint32_t ryp = b.j + 1 < b.a2 ? R[w + PY] : 0u, rym = b.j > 0 ? R[w - PY] : 0u;
+        const uint32_t rzp = b.k + 1 < b.a3 ? R[w + PZ] : 0u, rzm = b.k > 0 ? R[w - PZ] : 0u;
+        // neighbour validity, bit i of each: the face at +x, -x, +y, -y, +z, -z of face i
+        const uint32_t vxp = (rc >> 1) | (rr << 31), vxm = (rc << 1) | (rl >> 31);
+        const uint32_t reach = (vxp | vxm | ryp | rym | rzp | rzm) & o & ~rc;
+        const uint32_t d = (reach >> b.sh) & 0xffu;
+        reinterpret_cast<uint8_t*>(Rn)[4u * w + (unsigned)(b.sh >> 3)] = (uint8_t)(((rc | reach) >> b.sh) & 0xffu);
+        if (!d) continue;
+        float* x = pick3(b.ax, E.x[0], E.x[1], E.x[2]);
+        const unsigned s1 = (unsigned)b.a1, s2 = (unsigned)b.a1 * (unsigned)b.a2;
+        const unsigned base = b.r * s1 + 32u * (unsigned)b.wx + (unsigned)b.sh;
+        float sum[8];
+        int cnt[8];
 #pragma unroll
-        for (int h = 0; h < EXT_CHUNK; h += 8) {
-            float sum[8];
+        for (int q = 0; q < 8; q++) {
+            sum[q] = 0.f;
+            cnt[q] = 0;
+            if (!(d & (1u << q))) continue;
+            const int bit = b.sh + q;
+            const unsigned id = base + q;
+            const bool take[6] = {((vxp >> bit) & 1u) != 0, ((vxm >> bit) & 1u) != 0, ((ryp >> bit) & 1u) != 0,
+                                  ((rym >> bit) & 1u) != 0, ((rzp >> bit) & 1u) != 0, ((rzm >> bit) & 1u) != 0};
+            const unsigned nbi[6] = {id + 1, id - 1, id + s1, id - s1, id + s2, id - s2};
 #pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const unsigned id = base + h + q;
-                const unsigned nbi[6] = {id + 1, id - 1, id + s1, id - s1, id + s2, id - s2};
-                sum[q] = 0.f;
-#pragma unroll
-                for (int e = 0; e < 6; e++)
-                    if (take[h + q] & (1u << e)) sum[q] = __fadd_rn(sum[q], x[nbi[e]]);
-            }
-#pragma unroll
-            for (int q = 0; q < 8; q++)
-                if (take[h + q]) {
-                    x[base + h + q] = __fdiv_rn(sum[q], (float)__popc(take[h + q]));
-                    own.b[h + q] = (uint8_t)layer;
+            for (int e = 0; e < 6; e++)
+                if (take[e]) {
+                    sum[q] = __fadd_rn(sum[q], x[nbi[e]]);
+                    cnt[q]++;
                 }
         }
-        *reinterpret_cast<uint4*>(R + rowoff) = own.v;
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+            if (d & (1u << q)) x[base + q] = __fdiv_rn(sum[q], (float)cnt[q]);
     }
 }
 
-// The last pass on the codes: zero every face not reached and every walled one, and write
-// the reached flags (unless keep_flags: no layer ran, and the flags stay as they are).
-__global__ void __launch_bounds__(TPB) k_extrap_final(Geo g, ExtChunks E, int keep_flags) {
+// The last pass: zero every face not reached and every walled one, and write the reached
+// flags (unless keep_flags: no layer ran, and the flags stay as they are). R: the last
+// layer's mask (ra or rb).
+__global__ void __launch_bounds__(TPB) k_extrap_final(ExtBits E, int in_a, int keep_flags) {
     pdl_wait();
     pdl_trigger();
-    const unsigned n = chunk_threads(E, blockIdx.y);
+    const unsigned n = ext_bytes(E, blockIdx.y);
     for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const Chunk c = chunk_of(E, t);
-        const uint8_t* R = pick3(c.ax, E.code[0], E.code[1], E.code[2]);
-        float* x = pick3(c.ax, E.x[0], E.x[1], E.x[2]);
-        uint8_t* f = pick3(c.ax, E.f[0], E.f[1], E.f[2]);
-        Code16 own;
-        own.v = *reinterpret_cast<const uint4*>(R + c.r * (unsigned)c.P + c.i0);
-        const RowWall w = row_wall(g, c.ax, c.j, c.k);
-        const unsigned base = c.r * (unsigned)c.a1 + (unsigned)c.i0;
+        const ExtByte b = ext_byte(E, t);
+        const int i0 = 32 * b.wx + b.sh;
+        if (i0 >= b.a1) continue;
+        const uint32_t* R = in_a ? pick3(b.ax, E.ra[0], E.ra[1], E.ra[2]) : pick3(b.ax, E.rb[0], E.rb[1], E.rb[2]);
+        const uint32_t* O = pick3(b.ax, E.open[0], E.open[1], E.open[2]);
+        const unsigned w = b.r * (unsigned)b.W + (unsigned)b.wx;
+        const uint32_t rv = (R[w] >> b.sh) & 0xffu, ov = (O[w] >> b.sh) & 0xffu;
+        float* x = pick3(b.ax, E.x[0], E.x[1], E.x[2]);
+        uint8_t* f = pick3(b.ax, E.f[0], E.f[1], E.f[2]);
+        const unsigned base = b.r * (unsigned)b.a1 + (unsigned)i0;
+        const int cnt = b.a1 - i0 < 8 ? b.a1 - i0 : 8;
 #pragma unroll
-        for (int q = 0; q < EXT_CHUNK; q++) {
-            const int i = c.i0 + q;
-            if (i >= c.a1) continue;
-            const uint8_t cd = own.b[q];
-            const bool reached = cd < WALLED;
-            // only a face flagged on entry (code 0) can be both reached and walled
-            if (!reached || (cd == 0 && walled_in_row(g, w, c.ax, i))) x[base + q] = 0.f;
+        for (int q = 0; q < 8; q++) {
+            if (q >= cnt) break;
+            const bool reached = (rv >> q) & 1u;
+            // unreached_kernel!, then solidify! (a walled face is zero, reached or not)
+            if (!reached || !((ov >> q) & 1u)) x[base + q] = 0.f;
             if (!keep_flags) f[base + q] = reached ? 1 : 0;
         }
     }

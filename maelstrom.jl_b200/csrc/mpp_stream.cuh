@@ -301,25 +301,31 @@ __device__ __forceinline__ Vec8<M> rbgs_tile(const RbLd<M>& cur, bool edge, bool
 #pragma unroll
     for (int q = 0; q < V8; q++) {
         // constant element indices only (selects), so the tile stays in registers
-        const uint8_t cd = by_di ? (uint8_t)(ld<C>(&cur.dv.v[q]) != (C)0 ? SELF : 0)
+        const C d = ld<C>(&cur.dv.v[q]);
+        const uint8_t cd = by_di ? (uint8_t)(d != (C)0 ? SELF : 0)
                                  : (uint8_t)(((q < 4 ? cur.cdw.x : cur.cdw.y) >> (8 * (q & 3))) & 0xffu);
         const M xp = cur.ci ? (q + 1 < V8 ? cur.xc.v[q + 1 < V8 ? q + 1 : 0] : cur.xr) : cur.xc.v[q];
         const M xm = cur.ci ? cur.xc.v[q] : (q > 0 ? cur.xc.v[q > 0 ? q - 1 : 0] : cur.xl);
-        C nb[6];
-        nb[0] = ld<C>(&xp);
-        nb[1] = ld<C>(&xm);
-        nb[2] = ld<C>(&cur.yp.v[q]);
-        nb[3] = ld<C>(&cur.ym.v[q]);
-        nb[4] = ld<C>(&cur.zp.v[q]);
-        nb[5] = ld<C>(&cur.zm.v[q]);
-        const C d = ld<C>(&cur.dv.v[q]);
-        st(&out.v[q], (C)0);
+        const M nb[6] = {xp, xm, cur.yp.v[q], cur.ym.v[q], cur.zp.v[q], cur.zm.v[q]};
+        C v = (C)0;
         if (cd & SELF) {
-            const C s = nsum6<C>(nb, cd, edge);
+            // liquidsum in the reference's order, each stored neighbour widened inside its add
+            C s;
+            if (edge) {
+                s = (C)0;
+#pragma unroll
+                for (int m = 0; m < 6; m++)
+                    if (cd & (1u << m)) s = addm(nb[m], s);
+            } else {
+                s = ld<C>(&nb[0]);
+#pragma unroll
+                for (int m = 1; m < 6; m++) s = addm(nb[m], s);
+            }
             // the 16-bit forms multiply by the stored reciprocal (0 where the diagonal is)
-            if (scaled) st(&out.v[q], (ld<C>(&cur.bv.v[q]) + s) * d);
-            else st(&out.v[q], d > (C)0 ? (ld<C>(&cur.bv.v[q]) + s) / d : (C)0);
+            if (scaled) v = addm(cur.bv.v[q], s) * d;
+            else v = d > (C)0 ? addm(cur.bv.v[q], s) / d : (C)0;
         }
+        st(&out.v[q], v);
     }
     return out;
 }

@@ -27,7 +27,8 @@ from . import _lib
 from ._lib import MppError, Result, check
 from . import scene
 
-__all__ = ["Projector", "FlipBasin", "project", "pressure", "project_vjp", "MppError", "scene", "load"]
+__all__ = ["Projector", "FlipBasin", "project", "pressure", "project_vjp", "extrapolate", "redistance", "classify",
+           "filltrapped", "MppError", "scene", "load"]
 
 
 def load():
@@ -189,6 +190,42 @@ class Projector:
         check(self.lib.mpp_extrapolate(self._ctx, _ptr(u), _ptr(v), _ptr(w), _ptr(fu), _ptr(fv), _ptr(fw),
                                        int(layers), _stream_ptr(stream)))
 
+    def redistance(self, phi, phi0, iterations, types=None, stream=None):
+        """redistance! (``mpp_redistance``, src/flip.jl:673-680): ``iterations`` Jacobi sweeps
+        between phi and phi0 (the reference's two level-set arrays); returns the one holding
+        the result (phi0 when ``iterations`` is odd). ``types``, when given, gets classify!
+        of the result, fused into the last sweep."""
+        import torch
+
+        N = self.grid.ncells
+        _require(phi, torch.float32, N, "phi")
+        _require(phi0, torch.float32, N, "phi0")
+        if types is not None:
+            _require(types, torch.uint8, N, "types")
+        check(self.lib.mpp_redistance(self._ctx, _ptr(phi), _ptr(phi0), int(iterations),
+                                      _ptr(types) if types is not None else None, _stream_ptr(stream)))
+        return phi0 if int(iterations) % 2 else phi
+
+    def classify(self, types, phi, stream=None):
+        """classify! (``mpp_classify``, src/flip.jl:682-686) into ``types``."""
+        import torch
+
+        _require(types, torch.uint8, self.grid.ncells, "types")
+        _require(phi, torch.float32, self.grid.ncells, "phi")
+        check(self.lib.mpp_classify(self._ctx, _ptr(types), _ptr(phi), _stream_ptr(stream)))
+
+    def filltrapped(self, types, phi, maxrounds=32, stream=None, rounds=True):
+        """filltrapped! (``mpp_filltrapped``, src/flip.jl:747-760) in place; returns the sweep
+        rounds run (which synchronises the stream), or None with ``rounds=False``."""
+        import torch
+
+        _require(types, torch.uint8, self.grid.ncells, "types")
+        _require(phi, torch.float32, self.grid.ncells, "phi")
+        out = ctypes.c_int(-1)
+        check(self.lib.mpp_filltrapped(self._ctx, _ptr(types), _ptr(phi), int(maxrounds),
+                                       ctypes.byref(out) if rounds else None, _stream_ptr(stream)))
+        return out.value if rounds else None
+
     def advect_phi(self, phi, u, v, w, dt, stream=None):
         import torch
 
@@ -336,6 +373,8 @@ class FlipBasin:
     volume0: float
     iterations: list
     projector: Projector | None = None
+    band: int = 4  # the narrow band's width in cells (FlipBasin(...; band = 4), src/flip.jl:189)
+    phi0: object = None  # the level set's second buffer (s.phi0), allocated by redistance
 
     @classmethod
     def from_scene(cls, basin: "scene.Basin", device="cuda", **projector_kw) -> "FlipBasin":
@@ -405,6 +444,34 @@ def extrapolate(s: FlipBasin, layers=4) -> FlipBasin:
     """``extrapolate!(s; layers = 4)`` (src/flip.jl:1192-1206); ``step!`` calls it with
     ``layers = 6`` right after ``project!`` (:1403-1404)."""
     s.projector.extrapolate(s.u, s.v, s.w, s.fu, s.fv, s.fw, layers)
+    return s
+
+
+def redistance(s: FlipBasin, iterations=None) -> FlipBasin:
+    """``redistance!(s; iterations = s.band + 3)`` (src/flip.jl:673-680): the Jacobi sweeps
+    ping-pong between ``s.phi`` and ``s.phi0`` and the two swap as the reference's do, so
+    ``s.phi`` holds the result."""
+    import torch
+
+    it = s.band + 3 if iterations is None else int(iterations)
+    if s.phi0 is None:
+        s.phi0 = torch.empty_like(s.phi)
+    out = s.projector.redistance(s.phi, s.phi0, it)
+    if out is not s.phi:
+        s.phi, s.phi0 = s.phi0, s.phi
+    return s
+
+
+def classify(s: FlipBasin) -> FlipBasin:
+    """``classify!(s)`` (src/flip.jl:682-686)."""
+    s.projector.classify(s.types, s.phi)
+    return s
+
+
+def filltrapped(s: FlipBasin, maxrounds=32) -> FlipBasin:
+    """``filltrapped!(s; maxrounds = 32)`` (src/flip.jl:747-760); the rounds it ran are kept
+    in ``s.trap_rounds``."""
+    s.trap_rounds = s.projector.filltrapped(s.types, s.phi, maxrounds)
     return s
 
 

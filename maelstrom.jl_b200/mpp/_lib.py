@@ -89,6 +89,9 @@ SIGNATURES = {
                                     ctypes.POINTER(ctypes.c_int), P]),
     "mpp_advect_phi": (ctypes.c_int, [P, P, P, P, P, P, F32, P]),
     "mpp_extrapolate": (ctypes.c_int, [P, P, P, P, P, P, P, ctypes.c_int, P]),
+    "mpp_redistance": (ctypes.c_int, [P, P, P, ctypes.c_int, P, P]),
+    "mpp_classify": (ctypes.c_int, [P, P, P, P]),
+    "mpp_filltrapped": (ctypes.c_int, [P, P, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), P]),
     "mpp_advect_vjp": (ctypes.c_int, [P, P, P, P, P, P, P, F32, P, P, P, P]),
     "mpp_vjp_faces": (ctypes.c_int, [P, P, P, P, P, P, P, P, P, P]),
     "mpp_rhs": (ctypes.c_int, [P, P, P, P, P, P, F32, P]),

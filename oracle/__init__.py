@@ -68,6 +68,8 @@ def lib():
             "orc_advect_vjp_f32": (None, [G, P, P, P, P, P, P, P, f, P, P, P, P]),
             "orc_advect_vjp_f64": (None, [G, P, P, P, P, P, P, P, d, P, P, P, P]),
             "orc_extrapolate": (None, [G, P, P, P, P, P, P, i32]),
+            "orc_redistance": (None, [G, P, i32]), "orc_classify": (None, [G, P, P]),
+            "orc_filltrapped": (i32, [G, P, P, i32]),
             "orc_num_threads": (i32, []), "orc_set_num_threads": (None, [i32]),
         }
         for name, (res, args) in sig.items():
@@ -318,3 +320,25 @@ def extrapolate(grid, u, v, w, fu, fv, fw, layers=6):
             raise ValueError(f"face array {axis} has {out[axis].size} / {fl[axis].size} elements, not {n}")
     lib().orc_extrapolate(ctypes.byref(_grid(grid)), *(_p(a) for a in out), *(_p(a) for a in fl), int(layers))
     return (*out, *fl)
+
+
+def redistance(grid, phi, iterations):
+    """redistance!(s; iterations) (src/flip.jl:673-680): returns the new phi (Float32)."""
+    out = np.array(phi, dtype=np.float32, copy=True).ravel()
+    lib().orc_redistance(ctypes.byref(_grid(grid)), _p(out), int(iterations))
+    return out
+
+
+def classify(grid, phi):
+    """classify!(s) (src/flip.jl:682-686): the cell classes from phi and the walls."""
+    types = np.zeros(grid.ncells, dtype=np.uint8)
+    lib().orc_classify(ctypes.byref(_grid(grid)), _p(types), _p(np.ascontiguousarray(phi, dtype=np.float32)))
+    return types
+
+
+def filltrapped(grid, types, phi, maxrounds=32):
+    """filltrapped!(s; maxrounds) (src/flip.jl:747-760): returns (types, phi, rounds)."""
+    t = np.array(types, dtype=np.uint8, copy=True).ravel()
+    f = np.array(phi, dtype=np.float32, copy=True).ravel()
+    rounds = lib().orc_filltrapped(ctypes.byref(_grid(grid)), _p(t), _p(f), int(maxrounds))
+    return t, f, rounds

@@ -134,6 +134,15 @@ void orc_extrapolate(const orc_grid* g, float* u, float* v, float* w, uint8_t* f
 int orc_num_threads(void);
 void orc_set_num_threads(int n);
 
+/* ---- the level-set passes before the projection (levelset.c; src/flip.jl:608-760) ---- */
+/* redistance!(s; iterations): `iterations` Jacobi sweeps of reinit_kernel!, result in phi. */
+void orc_redistance(const orc_grid* g, float* phi, int iterations);
+/* classify!(s): SOLID where the cell centre is solid, else LIQUID where phi < 0, else AIR. */
+void orc_classify(const orc_grid* g, uint8_t* types, const float* phi);
+/* filltrapped!(s; maxrounds): air not reached from the top layer becomes LIQUID (phi at
+ * most -2 dx); returns the sweep rounds run. */
+int orc_filltrapped(const orc_grid* g, uint8_t* types, float* phi, int maxrounds);
+
 #ifdef __cplusplus
 }
 #endif
