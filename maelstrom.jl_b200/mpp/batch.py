@@ -7,11 +7,14 @@ graph launch. :meth:`Batch.autotune` times each distinct basin size's own solve 
 smoother forms and sweep counts (``mpp_autotune``) and applies the winner to every basin
 of that size. :func:`lpt_partition` splits a batch over ranks (longest processing time
 first on cells x expected iterations): basins are independent, so ranks exchange
-nothing during the solves.
+nothing during the solves. :func:`project_partitioned` is that multi-rank runner: each
+rank solves its share (one batched graph launch on its own GPU) and only the per-basin
+results are gathered.
 """
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 import heapq
 
 import numpy as np
@@ -221,3 +224,85 @@ class Batch:
         o.sweeps_coarse = sweeps_coarse
         o.precision, o.graph, o.fallback = k["precision"], 1, k["fallback"]
         check(self.lib.mpp_ctx_set_opts(c, ctypes.byref(o)))
+
+
+@dataclasses.dataclass
+class BasinOutcome:
+    """One basin's result, as gathered from the rank that solved it."""
+
+    index: int
+    rank: int
+    iterations: int
+    status: int
+    true_rel_residual: float
+    fallback_used: int = 0
+
+
+def solve_with_batch(basins, indices, *, dt, tol, maxiter, precision="fp32", autotune=True, steps=1,
+                     timer=None):
+    """The per-rank solve on this process's GPU: the share's basins in one :class:`Batch`
+    (autotuned per size), ``steps`` batched projections (the last one's results returned).
+    ``timer(fn)`` may time the projections (it gets a callable that runs them)."""
+    share = [basins[i] for i in indices]
+    if not share:
+        if timer is not None:
+            timer(lambda: None)  # the timed region is collective: an idle rank takes part
+        return []
+    batch = Batch(share, tol=tol, maxiter=maxiter, precision=precision)
+    if autotune:
+        batch.autotune()
+    init = [{k: a[k].clone() for k in ("u", "v", "w")} for a in batch.arrays]
+    last = []
+
+    def run():
+        nonlocal last
+        for _ in range(steps):
+            for a, i0 in zip(batch.arrays, init):
+                for k in ("u", "v", "w"):
+                    a[k].copy_(i0[k])
+                a["P"].zero_()
+            last = batch.project(dt)
+
+    run()  # the graph's capture and a warm-up
+    if timer is not None:
+        timer(run)
+    else:
+        run()
+    return [dict(iterations=r.iterations + r.fallback_iterations, status=r.status,
+                 true_rel_residual=r.true_rel_residual, fallback_used=r.fallback_used) for r in last]
+
+
+def project_partitioned(basins, rank: int, world: int, *, solve=None, gather=None, **solve_kw) -> list:
+    """Project a batch spread over ``world`` ranks: the basins are split by
+    :func:`lpt_partition` on :func:`basin_cost`, this rank solves its share with ``solve``
+    (default :func:`solve_with_batch`: one batched graph launch on this rank's GPU), and the
+    per-basin results are gathered to every rank (``gather``: default
+    ``torch.distributed.all_gather_object``; basins are independent, so nothing else
+    crosses ranks). Returns the :class:`BasinOutcome` of every basin, in basin order."""
+    parts = lpt_partition([basin_cost(b) for b in basins], world)
+    mine = parts[rank]
+    solve = solve or solve_with_batch
+    local = solve(basins, mine, **solve_kw)
+    if len(local) != len(mine):
+        raise RuntimeError(f"rank {rank} solved {len(local)} of its {len(mine)} basins")
+    payload = [(i, rank, r) for i, r in zip(mine, local)]
+    if world > 1:
+        if gather is None:
+            import torch.distributed as dist
+
+            gathered = [None] * world
+            dist.all_gather_object(gathered, payload)
+        else:
+            gathered = gather(payload)
+    else:
+        gathered = [payload]
+    out = [None] * len(basins)
+    for part in gathered:
+        for i, r_, res in part:
+            if out[i] is not None:
+                raise RuntimeError(f"basin {i} solved twice")
+            out[i] = BasinOutcome(index=i, rank=r_, **res)
+    missing = [i for i, o in enumerate(out) if o is None]
+    if missing:
+        raise RuntimeError(f"basins {missing} were not solved")
+    return out

@@ -36,33 +36,49 @@ def test_lpt_partition(nranks):
     assert max(loads) <= 4 / 3 * max(costs.sum() / nranks, costs.max()) + 1e-9
 
 
+def _small_batch():
+    sizes = [(16, 0.5, 0.45), (32, 0.6, 0.40), (24, 0.7, 0.36), (16, 0.3, 0.47), (32, 0.5, 0.42), (24, 0.8, 0.35),
+             (16, 0.65, 0.41)]
+    return [scene.box_basin(n, seed=800 + i, height=h, wall=w) for i, (n, h, w) in enumerate(sizes)]
+
+
+def oracle_solve(basins, indices, *, dt, tol, maxiter):
+    """A rank's share solved on the CPU by the oracle's projection (the test's stand-in for
+    the rank's GPU; the partition and the gathering are the product's)."""
+    import oracle
+
+    out = []
+    for i in indices:
+        r = oracle.project(basins[i], dt=dt, tol=tol, maxiter=maxiter)
+        info = r["info"]
+        out.append(dict(iterations=int(info.iterations), status=0 if info.converged else 1,
+                        true_rel_residual=float(info.rnorm / info.bnorm) if info.bnorm else 0.0, fallback_used=0))
+    return out
+
+
 def _rank_main(rank, world, port, out):
     import torch.distributed as dist
 
+    from mpp.batch import project_partitioned
+
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    basins = scene.batch_basins(12, seed=3)
-    parts = lpt_partition([basin_cost(b) for b in basins], world)
-    mine = parts[rank]
-    # stand-in for the per-rank solve: a deterministic digest of each basin's inputs
-    local = {i: float(basins[i].u.astype(np.float64).sum()) for i in mine}
-    gathered = [None] * world
-    dist.all_gather_object(gathered, local)
+    basins = _small_batch()
+    res = project_partitioned(basins, rank, world, solve=oracle_solve, dt=1 / 48, tol=1e-6, maxiter=100)
     # max over ranks of a per-rank time, as the benchmark reports it
     import torch
 
     t = torch.tensor([float(rank + 1)])
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     if rank == 0:
-        merged = {}
-        for g in gathered:
-            assert not set(g) & set(merged)
-            merged.update(g)
-        out.put((sorted(merged), float(t)))
+        out.put(([(o.index, o.rank, o.iterations, o.status) for o in res], float(t)))
     dist.destroy_process_group()
 
 
 def test_two_ranks_split_a_batch():
+    """Two gloo ranks each project their LPT share (the oracle standing in for a rank's GPU)
+    and gather the per-basin results: every basin solved once, by the rank the partition
+    gave it, with the iterations a serial solve of the whole batch gives."""
     import multiprocessing as mp
     import socket
 
@@ -74,9 +90,32 @@ def test_two_ranks_split_a_batch():
     procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
     for p in procs:
         p.start()
-    got = q.get(timeout=120)
+    got, tmax = q.get(timeout=300)
     for p in procs:
         p.join(timeout=120)
         assert p.exitcode == 0
-    assert got[0] == list(range(12))
-    assert got[1] == 2.0
+    basins = _small_batch()
+    parts = lpt_partition([basin_cost(b) for b in basins], 2)
+    assert all(parts)  # both ranks have work
+    serial = oracle_solve(basins, range(len(basins)), dt=1 / 48, tol=1e-6, maxiter=100)
+    assert [g[0] for g in got] == list(range(len(basins)))
+    for i, r_, its, st in got:
+        assert i in parts[r_]
+        assert its == serial[i]["iterations"] and st == 0
+    assert tmax == 2.0
+
+
+def test_partitioned_single_rank_and_errors():
+    from mpp.batch import project_partitioned
+
+    basins = _small_batch()[:3]
+    res = project_partitioned(basins, 0, 1, solve=oracle_solve, dt=1 / 48, tol=1e-6, maxiter=100)
+    assert [o.index for o in res] == [0, 1, 2] and all(o.rank == 0 for o in res)
+    # a rank that drops a basin of its share is an error, not a silent gap
+    with pytest.raises(RuntimeError, match="solved 2 of its 3"):
+        project_partitioned(basins, 0, 1, solve=lambda b, idx, **kw: oracle_solve(b, idx[:-1], **kw), dt=1 / 48,
+                            tol=1e-6, maxiter=100)
+    # results gathered twice for one basin are refused
+    with pytest.raises(RuntimeError, match="solved twice"):
+        project_partitioned(basins, 0, 2, solve=oracle_solve, gather=lambda p: [p, p], dt=1 / 48, tol=1e-6,
+                            maxiter=100)
