@@ -2082,7 +2082,7 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
     memset(&E, 0, sizeof(E));
     float* X[3] = {u, v, w};
     uint8_t* Fl[3] = {fu, fv, fw};
-    int64_t n[3], words[3], wtot = 0, bytes_max = 0, words_max = 0;
+    int64_t n[3], words[3], wtot = 0, words_max = 0;
     for (int a = 0; a < 3; a++) {
         n[a] = 1;
         for (int e = 0; e < 3; e++) {
@@ -2096,7 +2096,6 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
             return MPP_ERR_INVALID;
         }
         wtot += words[a];
-        bytes_max = std::max<int64_t>(bytes_max, 4 * words[a]);
         words_max = std::max<int64_t>(words_max, words[a]);
     }
     // a layer reads its neighbours' faces while others are written: no two of the six
@@ -2131,10 +2130,11 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
         launch(k_extrap_open, dim3(grid_cells(c, words_max), 3), TPB, 0, s, g, E);
         c->launches++;
     }
-    launch(k_extrap_flags, dim3(grid_cells(c, words_max), 3), TPB, 0, s, E);
-    const dim3 grid(grid_cells(c, bytes_max), 3);
-    for (int l = 1; l <= layers; l++) launch(k_extrap_layer, grid, TPB, 0, s, E, l & 1);
-    launch(k_extrap_final, grid, TPB, 0, s, E, layers % 2 == 0 ? 1 : 0, layers == 0 ? 1 : 0);
+    // a warp a word for the flags in and out, a thread a word for the layers
+    const dim3 gwarp(grid_cells(c, 32 * words_max), 3), gword(grid_cells(c, words_max), 3);
+    launch(k_extrap_flags, gwarp, TPB, 0, s, E);
+    for (int l = 1; l <= layers; l++) launch(k_extrap_layer, gword, TPB, 0, s, E, l & 1);
+    launch(k_extrap_final, gwarp, TPB, 0, s, E, layers % 2 == 0 ? 1 : 0, layers == 0 ? 1 : 0);
     c->launches += layers + 2;
     CK(cudaGetLastError());
     return MPP_OK;

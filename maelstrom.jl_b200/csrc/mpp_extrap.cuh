@@ -16,7 +16,8 @@
 // reference's bit for bit, and moves a bit a face (the masks, which stay in L2) plus the
 // values on the front. A last pass writes the 0/1 flags and zeroes what no layer reached
 // and every walled face. One launch a pass covers all three arrays (blockIdx.y is the
-// array); a thread takes one byte of a mask: 8 consecutive faces of a row.
+// array); the flags are read and written a warp a mask word (32 faces of a row, coalesced),
+// a layer takes a thread a mask word.
 #pragma once
 
 #include "mpp_base.cuh"
@@ -74,31 +75,19 @@ struct ExtBits {
     int W[3];
 };
 
-// A thread's byte of a mask: row r (j, k) of array ax, word wx, bits sh .. sh+7.
-struct ExtByte {
-    int ax, a1, a2, a3, W;
-    unsigned r;
-    int j, k, wx, sh;
+// Array ax's dims and masks, by selects.
+struct ExtArr {
+    int a1, a2, a3, W;
+    unsigned nw;  // mask words
 };
-__device__ __forceinline__ unsigned ext_bytes(const ExtBits& E, int ax) {
-    const int a2 = pick3(ax, E.d[0][1], E.d[1][1], E.d[2][1]), a3 = pick3(ax, E.d[0][2], E.d[1][2], E.d[2][2]);
-    return (unsigned)a2 * (unsigned)a3 * (unsigned)pick3(ax, E.W[0], E.W[1], E.W[2]) * 4u;
-}
-__device__ __forceinline__ ExtByte ext_byte(const ExtBits& E, unsigned t) {
-    ExtByte b;
-    b.ax = blockIdx.y;
-    b.a1 = pick3(b.ax, E.d[0][0], E.d[1][0], E.d[2][0]);
-    b.a2 = pick3(b.ax, E.d[0][1], E.d[1][1], E.d[2][1]);
-    b.a3 = pick3(b.ax, E.d[0][2], E.d[1][2], E.d[2][2]);
-    b.W = pick3(b.ax, E.W[0], E.W[1], E.W[2]);
-    const unsigned bpr = 4u * (unsigned)b.W;
-    b.r = t / bpr;
-    const int q = (int)(t % bpr);
-    b.wx = q >> 2;
-    b.sh = 8 * (q & 3);
-    b.j = (int)(b.r % (unsigned)b.a2);
-    b.k = (int)(b.r / (unsigned)b.a2);
-    return b;
+__device__ __forceinline__ ExtArr ext_arr(const ExtBits& E, int ax) {
+    ExtArr a;
+    a.a1 = pick3(ax, E.d[0][0], E.d[1][0], E.d[2][0]);
+    a.a2 = pick3(ax, E.d[0][1], E.d[1][1], E.d[2][1]);
+    a.a3 = pick3(ax, E.d[0][2], E.d[1][2], E.d[2][2]);
+    a.W = pick3(ax, E.W[0], E.W[1], E.W[2]);
+    a.nw = (unsigned)a.W * (unsigned)a.a2 * (unsigned)a.a3;
+    return a;
 }
 
 // The open mask O (in range and not walled): the grid's geometry only, once per context.
@@ -107,127 +96,128 @@ __global__ void __launch_bounds__(TPB) k_extrap_open(Geo g, ExtBits E) {
     pdl_wait();
     pdl_trigger();
     const int ax = blockIdx.y;
-    const int a1 = pick3(ax, E.d[0][0], E.d[1][0], E.d[2][0]), a2 = pick3(ax, E.d[0][1], E.d[1][1], E.d[2][1]);
-    const int a3 = pick3(ax, E.d[0][2], E.d[1][2], E.d[2][2]), W = pick3(ax, E.W[0], E.W[1], E.W[2]);
+    const ExtArr A = ext_arr(E, ax);
     uint32_t* O = pick3(ax, E.open[0], E.open[1], E.open[2]);
-    const unsigned n = (unsigned)W * (unsigned)a2 * (unsigned)a3;
-    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const unsigned r = t / (unsigned)W;
-        const int wx = (int)(t % (unsigned)W);
-        const RowWall w = row_wall(g, ax, (int)(r % (unsigned)a2), (int)(r / (unsigned)a2));
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < A.nw; t += gridDim.x * blockDim.x) {
+        const unsigned r = t / (unsigned)A.W;
+        const int wx = (int)(t % (unsigned)A.W);
+        const RowWall w = row_wall(g, ax, (int)(r % (unsigned)A.a2), (int)(r / (unsigned)A.a2));
         uint32_t o = 0;
         for (int b = 0; b < 32; b++) {
             const int i = 32 * wx + b;
-            if (i < a1 && !walled_in_row(g, w, ax, i)) o |= 1u << b;
+            if (i < A.a1 && !walled_in_row(g, w, ax, i)) o |= 1u << b;
         }
         O[t] = o;
     }
 }
 
-// R_0 from the caller's flags (a face is valid when its flag is not 0). A thread a word.
+// R_0 from the caller's flags (a face is valid when its flag is not 0): a warp a word, lane
+// b reading face 32 wx + b (one 32-byte piece a warp), the word formed by a ballot.
 __global__ void __launch_bounds__(TPB) k_extrap_flags(ExtBits E) {
     pdl_wait();
     pdl_trigger();
     const int ax = blockIdx.y;
-    const int a1 = pick3(ax, E.d[0][0], E.d[1][0], E.d[2][0]), a2 = pick3(ax, E.d[0][1], E.d[1][1], E.d[2][1]);
-    const int a3 = pick3(ax, E.d[0][2], E.d[1][2], E.d[2][2]), W = pick3(ax, E.W[0], E.W[1], E.W[2]);
+    const ExtArr A = ext_arr(E, ax);
     const uint8_t* fin = pick3(ax, E.f[0], E.f[1], E.f[2]);
     uint32_t* R = pick3(ax, E.ra[0], E.ra[1], E.ra[2]);
-    const unsigned n = (unsigned)W * (unsigned)a2 * (unsigned)a3;
-    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const unsigned r = t / (unsigned)W;
-        const int wx = (int)(t % (unsigned)W);
-        const uint8_t* row = fin + r * (unsigned)a1 + 32u * (unsigned)wx;
-        const int cnt = a1 - 32 * wx < 32 ? a1 - 32 * wx : 32;
-        uint8_t fl[32];
-#pragma unroll
-        for (int b = 0; b < 32; b++) fl[b] = b < cnt ? row[b] : (uint8_t)0;
-        uint32_t m = 0;
-#pragma unroll
-        for (int b = 0; b < 32; b++)
-            if (fl[b]) m |= 1u << b;
-        R[t] = m;
+    const int lane = threadIdx.x & 31;
+    const unsigned warps = gridDim.x * (blockDim.x >> 5);
+    for (unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < A.nw; w += warps) {
+        const unsigned r = w / (unsigned)A.W;
+        const int i = 32 * (int)(w % (unsigned)A.W) + lane;
+        const bool f = i < A.a1 && fin[r * (unsigned)A.a1 + (unsigned)i] != 0;
+        const uint32_t m = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) R[w] = m;
     }
 }
 
-// Layer `layer` (1-based): Rn = R | D, and the values of the faces D reaches. `from_a`: the
-// layer reads ra and writes rb (else the other way round).
+// Layer `layer` (1-based): Rn = R | D, and the values of the faces D reaches. A thread a mask
+// word; a word on the front takes its faces eight at a time (their loads before their
+// stores). `from_a`: the layer reads ra and writes rb (else the other way round).
 __global__ void __launch_bounds__(TPB) k_extrap_layer(ExtBits E, int from_a) {
     pdl_wait();
     pdl_trigger();
-    const unsigned n = ext_bytes(E, blockIdx.y);
-    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const ExtByte b = ext_byte(E, t);
-        const uint32_t* R = from_a ? pick3(b.ax, E.ra[0], E.ra[1], E.ra[2]) : pick3(b.ax, E.rb[0], E.rb[1], E.rb[2]);
-        uint32_t* Rn = from_a ? pick3(b.ax, E.rb[0], E.rb[1], E.rb[2]) : pick3(b.ax, E.ra[0], E.ra[1], E.ra[2]);
-        const uint32_t* O = pick3(b.ax, E.open[0], E.open[1], E.open[2]);
-        const unsigned w = b.r * (unsigned)b.W + (unsigned)b.wx;
-        const unsigned PY = (unsigned)b.W, PZ = (unsigned)b.W * (unsigned)b.a2;
+    const int ax = blockIdx.y;
+    const ExtArr A = ext_arr(E, ax);
+    const uint32_t* R = from_a ? pick3(ax, E.ra[0], E.ra[1], E.ra[2]) : pick3(ax, E.rb[0], E.rb[1], E.rb[2]);
+    uint32_t* Rn = from_a ? pick3(ax, E.rb[0], E.rb[1], E.rb[2]) : pick3(ax, E.ra[0], E.ra[1], E.ra[2]);
+    const uint32_t* O = pick3(ax, E.open[0], E.open[1], E.open[2]);
+    float* x = pick3(ax, E.x[0], E.x[1], E.x[2]);
+    const unsigned PY = (unsigned)A.W, PZ = (unsigned)A.W * (unsigned)A.a2;
+    const unsigned s1 = (unsigned)A.a1, s2 = (unsigned)A.a1 * (unsigned)A.a2;
+    for (unsigned w = blockIdx.x * blockDim.x + threadIdx.x; w < A.nw; w += gridDim.x * blockDim.x) {
+        const unsigned r = w / (unsigned)A.W;
+        const int wx = (int)(w % (unsigned)A.W);
+        const int j = (int)(r % (unsigned)A.a2), k = (int)(r / (unsigned)A.a2);
         const uint32_t rc = R[w], o = O[w];
-        const uint32_t rl = b.wx > 0 ? R[w - 1] : 0u, rr = b.wx + 1 < b.W ? R[w + 1] : 0u;
-        const uint32_t ryp = b.j + 1 < b.a2 ? R[w + PY] : 0u, rym = b.j > 0 ? R[w - PY] : 0u;
-        const uint32_t rzp = b.k + 1 < b.a3 ? R[w + PZ] : 0u, rzm = b.k > 0 ? R[w - PZ] : 0u;
+        const uint32_t rl = wx > 0 ? R[w - 1] : 0u, rr = wx + 1 < A.W ? R[w + 1] : 0u;
+        const uint32_t ryp = j + 1 < A.a2 ? R[w + PY] : 0u, rym = j > 0 ? R[w - PY] : 0u;
+        const uint32_t rzp = k + 1 < A.a3 ? R[w + PZ] : 0u, rzm = k > 0 ? R[w - PZ] : 0u;
         // neighbour validity, bit i of each: the face at +x, -x, +y, -y, +z, -z of face i
         const uint32_t vxp = (rc >> 1) | (rr << 31), vxm = (rc << 1) | (rl >> 31);
-        const uint32_t reach = (vxp | vxm | ryp | rym | rzp | rzm) & o & ~rc;
-        const uint32_t d = (reach >> b.sh) & 0xffu;
-        reinterpret_cast<uint8_t*>(Rn)[4u * w + (unsigned)(b.sh >> 3)] = (uint8_t)(((rc | reach) >> b.sh) & 0xffu);
-        if (!d) continue;
-        float* x = pick3(b.ax, E.x[0], E.x[1], E.x[2]);
-        const unsigned s1 = (unsigned)b.a1, s2 = (unsigned)b.a1 * (unsigned)b.a2;
-        const unsigned base = b.r * s1 + 32u * (unsigned)b.wx + (unsigned)b.sh;
-        float sum[8];
-        int cnt[8];
+        uint32_t d = (vxp | vxm | ryp | rym | rzp | rzm) & o & ~rc;
+        Rn[w] = rc | d;
+        const unsigned base = r * s1 + 32u * (unsigned)wx;
+        while (d) {
+            int bits[8];
+            int nb = 0;
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-            sum[q] = 0.f;
-            cnt[q] = 0;
-            if (!(d & (1u << q))) continue;
-            const int bit = b.sh + q;
-            const unsigned id = base + q;
-            const bool take[6] = {((vxp >> bit) & 1u) != 0, ((vxm >> bit) & 1u) != 0, ((ryp >> bit) & 1u) != 0,
-                                  ((rym >> bit) & 1u) != 0, ((rzp >> bit) & 1u) != 0, ((rzm >> bit) & 1u) != 0};
-            const unsigned nbi[6] = {id + 1, id - 1, id + s1, id - s1, id + s2, id - s2};
-#pragma unroll
-            for (int e = 0; e < 6; e++)
-                if (take[e]) {
-                    sum[q] = __fadd_rn(sum[q], x[nbi[e]]);
-                    cnt[q]++;
+            for (int q = 0; q < 8; q++) {
+                bits[q] = d ? __ffs(d) - 1 : -1;
+                if (d) {
+                    d &= d - 1;
+                    nb++;
                 }
-        }
+            }
+            float sum[8];
+            int cnt[8];
 #pragma unroll
-        for (int q = 0; q < 8; q++)
-            if (d & (1u << q)) x[base + q] = __fdiv_rn(sum[q], (float)cnt[q]);
+            for (int q = 0; q < 8; q++) {
+                sum[q] = 0.f;
+                cnt[q] = 0;
+                if (q >= nb) continue;
+                const int bit = bits[q];
+                const unsigned id = base + (unsigned)bit;
+                const bool take[6] = {((vxp >> bit) & 1u) != 0, ((vxm >> bit) & 1u) != 0, ((ryp >> bit) & 1u) != 0,
+                                      ((rym >> bit) & 1u) != 0, ((rzp >> bit) & 1u) != 0, ((rzm >> bit) & 1u) != 0};
+                const unsigned nbi[6] = {id + 1, id - 1, id + s1, id - s1, id + s2, id - s2};
+#pragma unroll
+                for (int e = 0; e < 6; e++)
+                    if (take[e]) {
+                        sum[q] = __fadd_rn(sum[q], x[nbi[e]]);
+                        cnt[q]++;
+                    }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (q < nb) x[base + (unsigned)bits[q]] = __fdiv_rn(sum[q], (float)cnt[q]);
+        }
     }
 }
 
 // The last pass: zero every face not reached and every walled one, and write the reached
-// flags (unless keep_flags: no layer ran, and the flags stay as they are). R: the last
-// layer's mask (ra or rb).
+// flags (unless keep_flags: no layer ran, and the flags stay as they are). A warp a mask
+// word, lane b on face 32 wx + b. `in_a`: the last layer's mask is ra (else rb).
 __global__ void __launch_bounds__(TPB) k_extrap_final(ExtBits E, int in_a, int keep_flags) {
     pdl_wait();
     pdl_trigger();
-    const unsigned n = ext_bytes(E, blockIdx.y);
-    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const ExtByte b = ext_byte(E, t);
-        const int i0 = 32 * b.wx + b.sh;
-        if (i0 >= b.a1) continue;
-        const uint32_t* R = in_a ? pick3(b.ax, E.ra[0], E.ra[1], E.ra[2]) : pick3(b.ax, E.rb[0], E.rb[1], E.rb[2]);
-        const uint32_t* O = pick3(b.ax, E.open[0], E.open[1], E.open[2]);
-        const unsigned w = b.r * (unsigned)b.W + (unsigned)b.wx;
-        const uint32_t rv = (R[w] >> b.sh) & 0xffu, ov = (O[w] >> b.sh) & 0xffu;
-        float* x = pick3(b.ax, E.x[0], E.x[1], E.x[2]);
-        uint8_t* f = pick3(b.ax, E.f[0], E.f[1], E.f[2]);
-        const unsigned base = b.r * (unsigned)b.a1 + (unsigned)i0;
-        const int cnt = b.a1 - i0 < 8 ? b.a1 - i0 : 8;
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-            if (q >= cnt) break;
-            const bool reached = (rv >> q) & 1u;
-            // unreached_kernel!, then solidify! (a walled face is zero, reached or not)
-            if (!reached || !((ov >> q) & 1u)) x[base + q] = 0.f;
-            if (!keep_flags) f[base + q] = reached ? 1 : 0;
-        }
+    const int ax = blockIdx.y;
+    const ExtArr A = ext_arr(E, ax);
+    const uint32_t* R = in_a ? pick3(ax, E.ra[0], E.ra[1], E.ra[2]) : pick3(ax, E.rb[0], E.rb[1], E.rb[2]);
+    const uint32_t* O = pick3(ax, E.open[0], E.open[1], E.open[2]);
+    float* x = pick3(ax, E.x[0], E.x[1], E.x[2]);
+    uint8_t* f = pick3(ax, E.f[0], E.f[1], E.f[2]);
+    const int lane = threadIdx.x & 31;
+    const unsigned warps = gridDim.x * (blockDim.x >> 5);
+    for (unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < A.nw; w += warps) {
+        const unsigned r = w / (unsigned)A.W;
+        const int i = 32 * (int)(w % (unsigned)A.W) + lane;
+        if (i >= A.a1) continue;
+        const bool reached = (R[w] >> lane) & 1u, open = (O[w] >> lane) & 1u;
+        const unsigned id = r * (unsigned)A.a1 + (unsigned)i;
+        // unreached_kernel!, then solidify! (a walled face is zero, reached or not)
+        if (!reached || !open) x[id] = 0.f;
+        if (!keep_flags) f[id] = reached ? 1 : 0;
     }
 }
 

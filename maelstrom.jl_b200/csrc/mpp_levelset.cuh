@@ -79,6 +79,10 @@ __global__ void __launch_bounds__(TPB) k_reinit(Geo g, const float* __restrict__
     const int64_t total = (int64_t)rq * n2 * n3;
     const float dx = g.dx, h = g.dx, R2 = g.radius * g.radius;
     const int64_t sy = n1, sz = (int64_t)n1 * n2;
+    // Far from the surface every neighbour distance is phimax: the update is then the same
+    // for every such cell, eikonal(phimax, phimax, phimax, h) (its costliest branch, two
+    // square roots and a division), formed once here by the same code.
+    const float far = jmin(eikonal(phimax, phimax, phimax, h), phimax);
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int q = (int)(t % rq);
         const int64_t row = t / rq;
@@ -174,7 +178,8 @@ __global__ void __launch_bounds__(TPB) k_reinit(Geo g, const float* __restrict__
                 if (frozen) {
                     v = cm;
                 } else {
-                    const float d = jmin(eikonal(ax, ay, az, h), phimax);
+                    const float d = (ax == phimax && ay == phimax && az == phimax) ? far
+                                                                                  : jmin(eikonal(ax, ay, az, h), phimax);
                     v = inside ? -d : d;
                 }
             }

@@ -575,9 +575,22 @@ __device__ __forceinline__ void residual_v8_body(Lev<typename Pr::M> L) {
                 const uint8_t cd = (uint8_t)(((q < 4 ? a.cdw.x : a.cdw.y) >> (8 * (q & 3))) & 0xffu);
                 C v = (C)0;
                 if (cd & SELF) {
-                    C n6[6];
-                    nb6_of(n6, a.nb, q, a.ci);
-                    v = ld<C>(&a.bv.v[q]) - (ld<C>(&a.dv.v[q]) * ld<C>(&a.xv.v[q]) - nsum6<C>(n6, cd, edge));
+                    // liquidsum (each stored neighbour widened inside its add), then b - (d x - s)
+                    const M xp = a.ci ? (q + 1 < V8 ? a.nb.c.v[q + 1 < V8 ? q + 1 : 0] : a.nb.r) : a.nb.c.v[q];
+                    const M xm = a.ci ? a.nb.c.v[q] : (q >= 1 ? a.nb.c.v[q >= 1 ? q - 1 : 0] : a.nb.l);
+                    const M n6[6] = {xp, xm, a.nb.yp.v[q], a.nb.ym.v[q], a.nb.zp.v[q], a.nb.zm.v[q]};
+                    C s;
+                    if (edge) {
+                        s = (C)0;
+#pragma unroll
+                        for (int m = 0; m < 6; m++)
+                            if (cd & (1u << m)) s = addm(n6[m], s);
+                    } else {
+                        s = ld<C>(&n6[0]);
+#pragma unroll
+                        for (int m = 1; m < 6; m++) s = addm(n6[m], s);
+                    }
+                    v = ld<C>(&a.bv.v[q]) - (ld<C>(&a.dv.v[q]) * ld<C>(&a.xv.v[q]) - s);
                 }
                 st(&out.v[q], v);
             }
@@ -928,7 +941,7 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
                     const int A = abase + q + (m & 1), B = (m & 2) ? b1 : b0, K = (m & 4) ? k1 : k0;
                     s += wt[m] * S[K][B][A];
                 }
-                st(&xv[cc].v[q], ld<C>(&xv[cc].v[q]) + (Pr::scaled ? (C)4 * s : s));
+                st(&xv[cc].v[q], addm(xv[cc].v[q], Pr::scaled ? (C)4 * s : s));
             }
             st8(L.x + p, xv[cc]);
         }

@@ -125,7 +125,12 @@ def whirl():
 
 def test_whirl256_fp32_matches_oracle(cuda, whirl):
     """The headline configuration (256^3, Rankine vortex, tol 1e-6) in the reference's
-    arithmetic, against the oracle's whole projection."""
+    arithmetic, against the oracle's whole projection. At this size the two FP32 solves part
+    by more than rounding: the oracle sums its dot products in 256-wide FP32 trees as the
+    reference does, the library in FP64, and the solve's conditioning amplifies that
+    difference in alpha and beta into ~4e-4 of the pressure. Both stop on the same test; so
+    the check is the same iteration count (+-1), the same flags, and a pressure at least as
+    close to the exact (FP64, tol 1e-12) solution as the oracle's."""
     import mpp
 
     b = whirl
@@ -135,11 +140,18 @@ def test_whirl256_fp32_matches_oracle(cuda, whirl):
     s.volume0 = vol0
     mpp.project(s, 1 / 48)
     assert abs(s.iterations[-1] - ref["info"].iterations) <= 1, (s.iterations, ref["info"].iterations)
-    P = _np(s.P)
-    rel = np.linalg.norm(P - ref["P"]) / np.linalg.norm(ref["P"])
-    assert rel <= PRESSURE_RTOL, rel
     for got, want in zip((s.fu, s.fv, s.fw), (ref["fu"], ref["fv"], ref["fw"])):
         np.testing.assert_array_equal(_np(got), want)
+    s64 = mpp.FlipBasin.from_scene(b, tol=1e-12, maxiter=400, precision="fp64", graph=True)
+    s64.volume0 = vol0
+    mpp.project(s64, 1 / 48)
+    P64 = s64.projector.solution_f64()
+    nrm = np.linalg.norm(P64)
+    err_gpu = np.linalg.norm(_np(s.P).astype(np.float64) - P64) / nrm
+    err_ref = np.linalg.norm(ref["P"].astype(np.float64) - P64) / nrm
+    assert err_gpu <= max(err_ref, 1e-4), (err_gpu, err_ref)
+    rel = np.linalg.norm(_np(s.P) - ref["P"]) / np.linalg.norm(ref["P"])
+    assert rel <= err_gpu + err_ref + 1e-6, (rel, err_gpu, err_ref)
 
 
 # The contract of the mixed form at the headline's settings: it stops on the reference's test
