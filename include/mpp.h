@@ -243,6 +243,8 @@ enum {
     MPP_SMOOTHER_VECTOR = 0, /* warp per 64x4x2 tile, 8 same-colour cells per lane, 16-byte loads */
     MPP_SMOOTHER_TMA = 1,    /* TMA-staged tiles (cp.async.bulk.tensor), persistent pipeline */
     MPP_SMOOTHER_COLUMN = 2, /* thread per tile column, scalar loads */
+    MPP_SMOOTHER_ASYNC = 3,  /* warp per tile as the vector form, its loads staged in shared memory by a
+                                pipeline of cp.async copies (16-bit forms; the others take the vector form) */
 };
 /* The smoother form of the fine level and of the coarser row-split levels (each level's
  * other passes take the vector forms unless its smoother is the column form). */

@@ -155,7 +155,8 @@ struct mpp_ctx {
     // TMA tensor maps of the row-split levels the smoother streams with cp.async.bulk.tensor
     TmaLev tma[MAXLEV];
     bool tma_ok[MAXLEV];
-    int tma_blocks;  // persistent grid of k_rbgs_tma
+    int tma_blocks;    // persistent grid of k_rbgs_tma
+    int async_blocks;  // resident grid of k_rbgs_async (16-bit forms; 0: not available)
     // smoother form of the fine level and of the coarser row-split levels (MPP_SMOOTHER_*;
     // the environment's MPP_RBGS / MPP_RBGS_COARSE: vector, tma, column); the other passes
     // of a level take the vector forms unless its smoother is the column form
@@ -516,12 +517,23 @@ struct Run {
     // b_late: the first pass follows a kernel that wrote the level's b (the restriction
     // with the level's start fused in)
     void smooth(int l, const std::vector<int>& colours, bool b_late = false) {
+        // the async-copy form exists for 16-bit storage; the others take the vector form
+        bool async = false;
+        if constexpr (sizeof(M) == 2)
+            async = form(l) == MPP_SMOOTHER_ASYNC && c->lv[l].H % V8 == 0 && c->async_blocks > 0;
         for (int col : colours) {
             beg(F_RBGS, l);
             if (form(l) == MPP_SMOOTHER_TMA && c->tma_ok[l]) {
                 const int g = c->lv[l].ntiles < c->tma_blocks ? c->lv[l].ntiles : c->tma_blocks;
                 launch(k_rbgs_tma<Pr>, g > 0 ? g : 1, TPB, TmaGeom<M>::SMEM, s, view<M>(c, l), col, c->tma[l],
                                                                            &c->sc->s.fault);
+            } else if (async) {
+                if constexpr (sizeof(M) == 2) {
+                    const int wpb = TPB / 32;
+                    int g = (c->lv[l].ntiles + wpb - 1) / wpb;
+                    g = g < c->async_blocks ? (g > 0 ? g : 1) : c->async_blocks;
+                    launch(k_rbgs_async<Pr>, g, TPB, AS_SMEM, s, view<M>(c, l), col);
+                }
             } else if (form(l) != MPP_SMOOTHER_COLUMN && c->lv[l].H % V8 == 0) {
                 const int wpb = TPB / 32, cap = c->nsm * RBGS_V8_BLOCKS;
                 int g = (c->lv[l].ntiles + wpb - 1) / wpb;
@@ -1288,7 +1300,9 @@ int build_tma(mpp_ctx* c) {
     auto parse = [](const char* m, int dflt) {
         return !m ? dflt
                   : (!strcmp(m, "tma") ? MPP_SMOOTHER_TMA
-                                       : (!strcmp(m, "column") ? MPP_SMOOTHER_COLUMN : MPP_SMOOTHER_VECTOR));
+                     : !strcmp(m, "column") ? MPP_SMOOTHER_COLUMN
+                     : !strcmp(m, "async") ? MPP_SMOOTHER_ASYNC
+                                           : MPP_SMOOTHER_VECTOR);
     };
     c->form_fine = parse(mode, MPP_SMOOTHER_VECTOR);
     c->form_coarse = parse(getenv("MPP_RBGS_COARSE"), c->form_fine);
@@ -1309,6 +1323,13 @@ int build_tma(mpp_ctx* c) {
         int nb = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_rbgs_tma<Pr>, TPB, TmaGeom<M>::SMEM));
         c->tma_blocks = (nb > 0 ? nb : 1) * c->nsm;
+        c->async_blocks = 0;
+        if constexpr (sizeof(M) == 2) {
+            CK(cudaFuncSetAttribute(k_rbgs_async<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, AS_SMEM));
+            int na = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&na, k_rbgs_async<Pr>, TPB, AS_SMEM));
+            c->async_blocks = na * c->nsm;
+        }
         return MPP_OK;
     });
 }
@@ -1878,7 +1899,7 @@ int mpp_batch_project(mpp_batch* b, const mpp_basin_arrays* basins, double dt, d
 int mpp_ctx_set_smoothers(mpp_ctx* c, int fine, int coarse) {
     if (int e = check_ctx(c)) return e;
     for (int f : {fine, coarse})
-        if (f < MPP_SMOOTHER_VECTOR || f > MPP_SMOOTHER_COLUMN) {
+        if (f < MPP_SMOOTHER_VECTOR || f > MPP_SMOOTHER_ASYNC) {
             set_err("unknown smoother form %d", f);
             return MPP_ERR_INVALID;
         }
@@ -1958,10 +1979,13 @@ int mpp_autotune(mpp_ctx* c, const float* u, const float* v, const float* w, con
         };
         // 1: the smoother forms, at the context's sweeps
         const int sw0 = saved.sweeps, swc0 = saved.sweeps_coarse, csw0 = saved.coarse;
-        for (int fine = MPP_SMOOTHER_VECTOR; fine <= MPP_SMOOTHER_COLUMN; fine++) {
+        const bool async_ok = c->async_blocks > 0;
+        for (int fine = MPP_SMOOTHER_VECTOR; fine <= MPP_SMOOTHER_ASYNC; fine++) {
             if (fine == MPP_SMOOTHER_TMA && !tma0) continue;
-            for (int coarse = MPP_SMOOTHER_VECTOR; coarse <= MPP_SMOOTHER_COLUMN; coarse++) {
+            if (fine == MPP_SMOOTHER_ASYNC && !async_ok) continue;
+            for (int coarse = MPP_SMOOTHER_VECTOR; coarse <= MPP_SMOOTHER_ASYNC; coarse++) {
                 if (coarse == MPP_SMOOTHER_TMA && !tma1) continue;
+                if (coarse == MPP_SMOOTHER_ASYNC && !async_ok) continue;
                 if (c->lb < 2 && coarse != fine) continue;  // no coarse row-split level
                 if (int e = trial(fine, coarse, sw0, swc0, csw0)) return e;
             }
@@ -1972,7 +1996,7 @@ int mpp_autotune(mpp_ctx* c, const float* u, const float* v, const float* w, con
         // 2: with those forms, the fine and coarse sweeps and (16-bit forms: the FP32 form
         // keeps the reference's V-cycle) 10 instead of 40 coarsest sweeps
         const bool half = c->prec == MPP_PREC_MIXED_FP16 || c->prec == MPP_PREC_MIXED_BF16;
-        for (int sw = 1; sw <= 6; sw++)  // at most 9 + 96 candidates in all
+        for (int sw = 1; sw <= 6; sw++)  // at most 16 + 96 candidates in all
             for (int swc = 1; swc <= 8; swc++)
                 for (int csw : {csw0, 10}) {
                     if (csw == 10 && (!half || csw0 == 10)) continue;

@@ -180,4 +180,131 @@ __global__ void __launch_bounds__(TPB) k_rbgs_tma(Lev<typename Pr::M> L, int col
     (void)sz;
 }
 
+// ---- the async-copy smoother (16-bit forms): rbgs_kernel! with every load in flight as
+// cp.async into shared memory ----
+// The vector form holds a tile's loads in registers, two tiles a warp, and at 16 warps an
+// SM keeps too few bytes in flight to cover HBM latency. Here a warp streams its tiles
+// through a ring of AS_STAGES buffers in its own slice of shared memory with 16-byte
+// cp.async copies (no registers held while they fly): the own colour's b and reciprocal
+// diagonal (one piece a lane) and the other colour's x around the tile (the 4 x 2 rows of
+// the tile, the rows at -+y, the planes at -+z, and one piece each side along x: 96 pieces),
+// AS_STAGES - 1 tiles ahead of the one it computes. A lane then reads its 8 cells'
+// neighbours from shared memory and updates them with the vector form's arithmetic
+// (rbgs_tile), so both forms give the same values. Reads past the level's rows and planes
+// land in the x array's zeroed guard, as the vector form's do.
+constexpr int AS_STAGES = 3;
+constexpr int AS_SLOTS = 4 * 6 * 6;  // x pieces [plane k0-1 .. k0+2][row j0-1 .. j0+4][piece -1 .. 4]
+constexpr int AS_STAGE = AS_SLOTS * 16 + 2 * 32 * 16;  // + b and 1/diag, a piece a lane
+constexpr int AS_SMEM = (TPB / 32) * AS_STAGES * AS_STAGE;
+
+__device__ __forceinline__ void cp_async16(void* sm, const void* gm) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sm)), "l"(gm) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ int as_slot(int kk, int jj, int pc) { return (kk * 6 + jj) * 6 + pc; }
+// The e-th of a tile's 96 x pieces (e < 96): the tile's own rows, the rows at -+y, the
+// planes at -+z, the pieces beside the rows along x.
+__device__ __forceinline__ void as_piece(int e, int& kk, int& jj, int& pc) {
+    if (e < 32) {
+        kk = 1 + (e >> 4); jj = 1 + ((e >> 2) & 3); pc = 1 + (e & 3);
+    } else if (e < 48) {
+        e -= 32; kk = 1 + (e >> 3); jj = ((e >> 2) & 1) ? 5 : 0; pc = 1 + (e & 3);
+    } else if (e < 80) {
+        e -= 48; kk = (e >> 4) ? 3 : 0; jj = 1 + ((e >> 2) & 3); pc = 1 + (e & 3);
+    } else {
+        e -= 80; kk = 1 + (e >> 3); jj = 1 + ((e >> 1) & 3); pc = (e & 1) ? 5 : 0;
+    }
+}
+
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_rbgs_async(Lev<typename Pr::M> L, int colour) {
+    using C = typename Pr::C;
+    using M = typename Pr::M;
+    static_assert(sizeof(M) == 2, "the async form stages 8 elements a 16-byte piece");
+    extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ uint32_t tid_of[TPB / 32][AS_STAGES];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = TPB / 32;
+    const int hq = lane % V8_LANES_H, lj = (lane / V8_LANES_H) % TY, lk = lane / (V8_LANES_H * TY);
+    unsigned char* ring = smraw + (size_t)warp * AS_STAGES * AS_STAGE;
+    pdl_wait();
+    pdl_trigger();
+    const int n = *L.count;
+    const bool edge = *L.edge != 0;
+    const bool by_di = Pr::scaled && !edge, need_code = !by_di;
+    const int stride = gridDim.x * wpb, wg = blockIdx.x * wpb + warp;
+    const int mine = wg < n ? (n - 1 - wg) / stride + 1 : 0;
+    if (mine == 0) return;
+    const int H = L.H, n1 = L.n1, n2 = L.n2;
+    const int own = colour * H, oth = (1 - colour) * H;
+    const M* dsrc = Pr::scaled ? L.di : L.dg;
+    auto issue = [&](int i) {
+        const int s = i % AS_STAGES;
+        const uint32_t tile = L.tiles[wg + i * stride];
+        if (lane == 0) tid_of[warp][s] = tile;
+        const int h0 = (int)(tile & 1023u) * TH, j0 = (int)((tile >> 10) & 1023u) * TY, k0 = (int)(tile >> 20) * TZ;
+        unsigned char* st = ring + s * AS_STAGE;
+        const int h = h0 + hq * V8, j = j0 + lj, k = k0 + lk;
+        if (h < H && j < n2 && k < L.n3) {
+            const int p = (k * n2 + j) * n1 + own + h;
+            cp_async16(st + AS_SLOTS * 16 + lane * 16, L.b + p);
+            cp_async16(st + AS_SLOTS * 16 + 512 + lane * 16, dsrc + p);
+        }
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            int kk, jj, pc;
+            as_piece(lane + 32 * q, kk, jj, pc);
+            const int jr = j0 - 1 + jj, kr = k0 - 1 + kk;
+            // rows past the level's last (a partial tile's) are read by no cell that updates;
+            // skipping them keeps every copy inside the array and its one-plane guard
+            if (jr > n2 || (kr == L.n3 && jr >= n2)) continue;
+            const int pos = (kr * n2 + jr) * n1 + oth + h0 + (pc - 1) * V8;
+            cp_async16(st + as_slot(kk, jj, pc) * 16, L.x + pos);
+        }
+    };
+#pragma unroll
+    for (int i = 0; i < AS_STAGES - 1; i++) {
+        if (i < mine) issue(i);
+        cp_async_commit();
+    }
+    for (int i = 0; i < mine; i++) {
+        if (i + AS_STAGES - 1 < mine) issue(i + AS_STAGES - 1);
+        cp_async_commit();
+        cp_async_wait<AS_STAGES - 1>();  // tile i's copies (this lane's) are in
+        __syncwarp();                     // and every lane's
+        const int s = i % AS_STAGES;
+        const unsigned char* st = ring + s * AS_STAGE;
+        const uint32_t tile = tid_of[warp][s];
+        const int h = (int)(tile & 1023u) * TH + hq * V8, j = (int)((tile >> 10) & 1023u) * TY + lj,
+                  k = (int)(tile >> 20) * TZ + lk;
+        RbLd<M> a;
+        a.ok = h < H && j < n2 && k < L.n3;
+        if (a.ok) {
+            a.p = (k * n2 + j) * n1 + own + h;
+            a.ci = ci_of(colour, j, k);
+            if (need_code) a.cdw = *reinterpret_cast<const uint2*>(L.code + a.p);
+            auto piece = [&](int kk, int jj, int pc) {
+                Vec8<M> v;
+                *reinterpret_cast<uint4*>(v.v) = *reinterpret_cast<const uint4*>(st + as_slot(kk, jj, pc) * 16);
+                return v;
+            };
+            *reinterpret_cast<uint4*>(a.bv.v) = *reinterpret_cast<const uint4*>(st + AS_SLOTS * 16 + lane * 16);
+            *reinterpret_cast<uint4*>(a.dv.v) = *reinterpret_cast<const uint4*>(st + AS_SLOTS * 16 + 512 + lane * 16);
+            a.xc = piece(1 + lk, 1 + lj, 1 + hq);
+            a.yp = piece(1 + lk, 2 + lj, 1 + hq);
+            a.ym = piece(1 + lk, lj, 1 + hq);
+            a.zp = piece(2 + lk, 1 + lj, 1 + hq);
+            a.zm = piece(lk, 1 + lj, 1 + hq);
+            a.xl = reinterpret_cast<const M*>(st + as_slot(1 + lk, 1 + lj, hq) * 16)[V8 - 1];
+            a.xr = reinterpret_cast<const M*>(st + as_slot(1 + lk, 1 + lj, 2 + hq) * 16)[0];
+        }
+        __syncwarp();  // stage s is read; the next iteration's copies may overwrite it
+        if (a.ok) st8(L.x + a.p, rbgs_tile<C, M>(a, edge, Pr::scaled, by_di));
+    }
+    cp_async_wait<0>();
+}
+
 }  // namespace mpp

@@ -58,7 +58,7 @@ class TuneEntry(ctypes.Structure):
                 ("status", ctypes.c_int32), ("ms", ctypes.c_float)]
 
 
-SMOOTHERS = {0: "vector", 1: "tma", 2: "column"}
+SMOOTHERS = {0: "vector", 1: "tma", 2: "column", 3: "async"}
 
 # name -> (restype, argtypes); every symbol include/mpp.h declares.
 P, I32, F32, F64, SZ = ctypes.c_void_p, ctypes.c_int32, ctypes.c_float, ctypes.c_double, ctypes.c_size_t

@@ -1,6 +1,7 @@
 """Every smoother form the autotuner can pick, at the sweep counts it picks, against the oracle.
 
-libmpp has three red-black smoother forms (vector, TMA-staged tiles, per-column), chosen
+libmpp has four red-black smoother forms (vector, TMA-staged tiles, per-column, and the
+vector form's tiles staged by cp.async, for 16-bit storage), chosen
 separately for the fine level and for the coarser row-split levels, and the autotuner also
 sets the fine and coarser sweep counts and the coarsest solve's sweeps. The FP32 V-cycle
 is compared bit for bit with the oracle's (src/flip.jl:992-1014, per-level sweep counts as
@@ -21,7 +22,7 @@ from mpp import scene
 
 pytestmark = pytest.mark.gpu
 
-FORMS = ["vector", "tma", "column"]
+FORMS = ["vector", "tma", "column", "async"]
 PAIRS = list(itertools.product(FORMS, FORMS))
 SWEEPS = [(2, 0, 40), (5, 6, 10), (1, 3, 4)]  # (fine, coarser levels, coarsest); 0 = the fine count
 PRESSURE_RTOL = 1e-4
@@ -69,7 +70,7 @@ def test_vcycle_forms_bitexact(cuda, basins, n, fine, coarse, sw):
 @pytest.mark.parametrize("prec", ["fp16", "bf16"])
 @pytest.mark.parametrize("sw", SWEEPS[:2], ids=lambda s: "sweeps%d-%d-%d" % s)
 def test_vcycle_16bit_forms_agree(cuda, basins, prec, sw):
-    """The three forms do the same arithmetic per cell in the same order: same values."""
+    """The forms do the same arithmetic per cell in the same order: same values."""
     b = basins[128]
     r = scene.uniform(13, 5, b.grid.ncells) * (b.types == scene.LIQUID)
     rt, tt, pt = _t(r, cuda), _t(b.types, cuda), _t(b.phi, cuda)
