@@ -196,7 +196,7 @@ def run_mpp(args):
 
     world, rank, local = dist_init()
     dev = torch.device("cuda", local)
-    basin = scene.config_basin(WORKLOAD)
+    basin = scene.config_basin(args.workload if args.ncu else WORKLOAD)
     g = basin.grid
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     types, phi = T(basin.types), T(basin.phi)
@@ -448,20 +448,31 @@ def bench_batched(steps):
             a["P"].zero_()
         return batch.project(DT)
 
-    for _ in range(3):
-        step()
-    torch.cuda.synchronize()
-    e0, e1 = _events()
-    # the per-step copies of the 48 initial states are timed too (about 1.2 GB moved)
-    e0.record()
-    for _ in range(steps):
-        res = step()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
+    def timed():
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        # the per-step copies of the 48 initial states are timed too (about 1.2 GB moved)
+        e0.record()
+        for _ in range(steps):
+            res = step()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, res
+
+    ms, res = timed()
+    groups = batch.groups
+    its_grouped = [r.iterations for r in res]
+    # the same batch with every basin as its own chain of launches, for comparison
+    batch.set_grouped(False)
+    ms_chains, res_c = timed()
+    batch.set_grouped(True)
     launches = sum(r.kernel_launches for r in res)
     return {"basins": len(basins), "cells": cells, "projections_per_s": round(len(basins) / (ms / 1e3), 2),
             "cells_per_s": cells / (ms / 1e3), "ms_per_batch": round(ms, 3), "steps": steps,
+            "groups": groups, "chains_projections_per_s": round(len(basins) / (ms_chains / 1e3), 2),
+            "chains_same_iterations": its_grouped == [r.iterations for r in res_c],
             "graph_launches_per_batch": 1, "gpu_launches_per_batch": launches,
             "iterations": [r.iterations for r in res], "all_converged": all(r.status == 0 for r in res),
             "max_true_rel_residual": max(r.true_rel_residual for r in res),
@@ -828,6 +839,8 @@ def main():
                     help="--ncu mode: fine,coarse,sweeps,coarse-level sweeps,coarsest (e.g. vector,column,4,2,10)")
     ap.add_argument("--ncu", action="store_true",
                     help="profiling mode: --steps headline projections from the host loop, nothing timed")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "plain64", "box128"],
+                    help="--ncu mode: the basin profiled (a smaller one to size a capture)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "mpp" and not args.ncu:
         ap.error("--warmup must be at least 3")

@@ -231,6 +231,15 @@ typedef struct {
 int mpp_batch_create(mpp_batch** batch, int count, const mpp_grid* grids, const mpp_opts* opts);
 int mpp_batch_destroy(mpp_batch* batch);
 int mpp_batch_size(const mpp_batch* batch);
+/* Group the batch's basins (on, the default) or give each basin its own chain (off). A group
+ * is at most 16 basins with the same grid, precision, sweeps, smoother forms and level split
+ * (not FP64, not the TMA form): each pass of their CG loops is one launch over all of them
+ * (the basin is the launch's second grid dimension, every basin keeping its own grid width,
+ * arithmetic and reductions, so results are bit-identical either way), converged basins skip
+ * the remaining passes, and the group's loop is one conditional node that ends when all are
+ * done. mpp_batch_groups: groups in the last recorded graph. */
+int mpp_batch_set_grouped(mpp_batch* batch, int on);
+int mpp_batch_groups(const mpp_batch* batch);
 /* Basin i's context (options, smoother, autotuning); using it drops the batch's graph. */
 mpp_ctx* mpp_batch_ctx(mpp_batch* batch, int i);
 /* project! of every basin with one graph launch; results[i] (may be NULL) per basin.

@@ -22,6 +22,7 @@
 #include "mpp_levelset.cuh"
 #include "mpp_tma.cuh"
 #include "mpp_cmg.cuh"
+#include "mpp_group.cuh"
 
 using namespace mpp;
 
@@ -687,6 +688,207 @@ struct Run {
         end();
     }
 };
+
+// A launch of `ny` thread-block clusters of `cs` CTAs side by side (blockIdx.y: the basin of
+// a group), with programmatic dependent launch.
+template <typename... KArgs, typename... Args>
+void launch_clusters(void (*kern)(KArgs...), int cs, int ny, int block, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cs, (unsigned)ny);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    at[1].id = cudaLaunchAttributeClusterDimension;
+    at[1].val.clusterDim.x = (unsigned)cs;
+    at[1].val.clusterDim.y = 1;
+    at[1].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 2;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
+// A group's CG loop body: Run<Pr>::body's launch sequence with every launch covering the
+// group's basins (grid y), each basin's grid width as its own solve's (run0 computes them for
+// the first basin; every basin of a group has the same grid, options and forms).
+template <class Pr>
+struct GroupRun {
+    using V = typename Pr::V;
+    using M = typename Pr::M;
+    using C = typename Pr::C;
+    std::vector<mpp_ctx*> cs;
+    std::vector<V*> P;  // each basin's pressure (the caller's array)
+    cudaStream_t s;
+    int nk = 0;
+    Run<Pr> run0;
+
+    GroupRun(const std::vector<mpp_ctx*>& ctxs, const std::vector<V*>& Ps, cudaStream_t st)
+        : cs(ctxs), P(Ps), s(st), run0{ctxs[0], st} {}
+    int nb() const { return (int)cs.size(); }
+    const mpp_ctx* c0() const { return cs[0]; }
+    dim3 g2(int gx) const { return dim3((unsigned)gx, (unsigned)nb()); }
+    static const int* done_of(const mpp_ctx* c) { return &c->sc->s.done; }
+
+    Grp<GLev<M>> lev(int l) const {
+        Grp<GLev<M>> g;
+        memset(&g, 0, sizeof(g));
+        for (int i = 0; i < nb(); i++) g.a[i] = GLev<M>{view<M>(cs[i], l), done_of(cs[i])};
+        return g;
+    }
+    Grp<GLev2<M>> lev2(int f, int cl) const {
+        Grp<GLev2<M>> g;
+        memset(&g, 0, sizeof(g));
+        for (int i = 0; i < nb(); i++) g.a[i] = GLev2<M>{view<M>(cs[i], f), view<M>(cs[i], cl), done_of(cs[i])};
+        return g;
+    }
+    Grp<GCg<M, V>> cg() const {
+        Grp<GCg<M, V>> g;
+        memset(&g, 0, sizeof(g));
+        for (int i = 0; i < nb(); i++) {
+            mpp_ctx* c = cs[i];
+            g.a[i] = GCg<M, V>{view<M>(c, 0), (V*)c->r, (V*)c->q, (V*)c->d, P[i], (const V*)c->diag,
+                               c->sc, c->partials, c->counters};
+        }
+        return g;
+    }
+    // the counters of a CG pass (each basin's own, at the same index as its single solve's)
+    Grp<GCg<M, V>> cg_at(int cnt) const {
+        Grp<GCg<M, V>> g = cg();
+        for (int i = 0; i < nb(); i++) g.a[i].counter = cs[i]->counters + cnt;
+        return g;
+    }
+
+    void smooth(int l, const std::vector<int>& colours, bool b_late) {
+        const mpp_ctx* c = c0();
+        bool async = false;
+        if constexpr (sizeof(M) == 2)
+            async = run0.form(l) == MPP_SMOOTHER_ASYNC && c->lv[l].H % V8 == 0 && c->async_blocks > 0;
+        const auto g = lev(l);
+        for (int col : colours) {
+            nk++;
+            if (async) {
+                if constexpr (sizeof(M) == 2) {
+                    const int wpb = TPB / 32;
+                    int gx = (c->lv[l].ntiles + wpb - 1) / wpb;
+                    gx = gx < c->async_blocks ? (gx > 0 ? gx : 1) : c->async_blocks;
+                    launch(k_rbgs_async_g<Pr>, g2(gx), TPB, AS_SMEM, s, g, col);
+                }
+            } else if (run0.form(l) != MPP_SMOOTHER_COLUMN && c->lv[l].H % V8 == 0) {
+                const int wpb = TPB / 32, cap = c->nsm * RBGS_V8_BLOCKS;
+                int gx = (c->lv[l].ntiles + wpb - 1) / wpb;
+                gx = gx < cap ? (gx > 0 ? gx : 1) : cap;
+                launch(k_rbgs_v8_g<Pr>, g2(gx), TPB, 0, s, g, col, b_late ? 1 : 0);
+                b_late = false;
+            } else {
+                launch(k_rbgs_g<Pr>, g2(grid_tiles(c, l)), TPB, 0, s, g, col);
+            }
+        }
+    }
+
+    void vcycle() {
+        const mpp_ctx* c = c0();
+        const int swf = c->opts.sweeps, sw = c->opts.sweeps_coarse > 0 ? c->opts.sweeps_coarse : swf;
+        std::vector<int> down, up, down0, up0;
+        for (int q = 0; q < sw; q++) { down.push_back(0); down.push_back(1); }
+        down.erase(down.begin());
+        for (int q = 0; q < sw; q++) { up.push_back(1); up.push_back(0); }
+        for (int q = 0; q < swf; q++) { down0.push_back(0); down0.push_back(1); }
+        down0.erase(down0.begin());
+        for (int q = 0; q < swf; q++) { up0.push_back(1); up0.push_back(0); }
+        const int lb = c->lb;
+        const int ls = c->cmg_ls > 0 ? c->cmg_ls : lb;
+        for (int l = 0; l < ls; l++) {
+            if (l == 0) {
+                nk++;
+                if (run0.vec(l))
+                    launch(k_start_v8_g<Pr>, g2(run0.grid_res((const void*)k_start_v8<Pr>, l)), TPB, 0, s, lev(l));
+                else
+                    launch(k_start_g<Pr>, g2(grid_tiles(c, l)), TPB, 0, s, lev(l));
+            }
+            smooth(l, l == 0 ? down0 : down, l > 0);
+            nk++;
+            if (run0.vec(l))
+                launch(k_residual_v8_g<Pr>, g2(run0.grid_res((const void*)k_residual_v8<Pr>, l)), TPB, 0, s, lev(l));
+            else
+                launch(k_residual_g<Pr>, g2(grid_tiles(c, l)), TPB, 0, s, lev(l));
+            if (l + 1 < lb) {
+                nk++;
+                launch(k_restrict_g<Pr>, g2(grid_tiles1(c, l + 1)), TPB, c->restrict_smem, s, lev2(l, l + 1),
+                       l + 1 < ls ? 1 : 0);
+            }
+        }
+        Grp<GCmg<M>> gc;
+        memset(&gc, 0, sizeof(gc));
+        if (ls < lb) {
+            for (int i = 0; i < nb(); i++) {
+                mpp_ctx* ci = cs[i];
+                CmgArgs<M>& ca = gc.a[i].a;
+                ca.nl = lb - ls;
+                ca.sweeps = sw;
+                ca.botb = ci->botb;
+                for (int l = ls; l <= lb; l++) ca.g[l - ls] = view<M>(ci, l);
+                for (int l = ls; l < lb; l++) ca.s[l - ls] = ci->cmg_slab[l - ls];
+                gc.a[i].done = done_of(ci);
+            }
+            nk++;
+            launch_clusters(k_cmg_g<Pr, 0>, c->cmg_cs, nb(), CMG_THREADS, c->cmg_smem, s, gc);
+        } else {
+            Grp<GRestrictBottom<M, C>> gr;
+            memset(&gr, 0, sizeof(gr));
+            for (int i = 0; i < nb(); i++)
+                gr.a[i] = GRestrictBottom<M, C>{view<M>(cs[i], lb - 1), view<M>(cs[i], lb), (C*)cs[i]->botb,
+                                                done_of(cs[i])};
+            const int64_t Nb = (int64_t)c->lv[lb].n[0] * c->lv[lb].n[1] * c->lv[lb].n[2];
+            nk++;
+            launch(k_restrict_bottom_g<Pr>, g2(grid_cells(c, Nb)), TPB, 0, s, gr);
+        }
+        Grp<GBottom<M, C>> gb;
+        memset(&gb, 0, sizeof(gb));
+        for (int i = 0; i < nb(); i++) {
+            BotArgs ba = cs[i]->bot;
+            ba.sweeps = sw;
+            ba.coarse = cs[i]->opts.coarse;
+            gb.a[i] = GBottom<M, C>{(const C*)cs[i]->botb, (M*)cs[i]->lv[lb].x, ba, done_of(cs[i])};
+        }
+        nk++;
+        launch(k_bottom_g<Pr>, g2(1), 1024, c->bot_smem, s, gb);
+        if (ls < lb) {
+            nk++;
+            launch_clusters(k_cmg_g<Pr, 1>, c->cmg_cs, nb(), CMG_THREADS, c->cmg_smem, s, gc);
+        }
+        for (int l = ls - 1; l >= 0; l--) {
+            nk++;
+            if (run0.vec(l))
+                launch(k_prolong_v8_g<Pr>, g2(run0.grid_w(l)), TPB, 0, s, lev2(l, l + 1), l + 1 == lb ? 1 : 0);
+            else
+                launch(k_prolong_g<Pr>, g2(grid_tiles(c, l)), TPB, 0, s, lev2(l, l + 1), l + 1 == lb ? 1 : 0);
+            smooth(l, l == 0 ? up0 : up, false);
+        }
+    }
+
+    // Run<Pr>::body for the group, then the group's loop condition.
+    void body(cudaGraphConditionalHandle cond) {
+        const mpp_ctx* c = c0();
+        vcycle();
+        const bool v = run0.vec(0);
+        nk += 4;
+        if (v) launch(k_dot_v8_g<Pr>, g2(run0.grid_res((const void*)k_dot_v8<Pr>, 0)), TPB, 0, s, cg_at(CNT_DOT));
+        else launch(k_dot_g<Pr>, g2(grid_tiles(c, 0)), TPB, 0, s, cg_at(CNT_DOT));
+        if (v) launch(k_search_v8_g<Pr>, g2(run0.grid_res((const void*)k_search_v8<Pr>, 0)), TPB, 0, s, cg_at(CNT_SEARCH));
+        else launch(k_search_g<Pr>, g2(grid_tiles(c, 0)), TPB, 0, s, cg_at(CNT_SEARCH));
+        bool aligned = true;  // the vector step moves P in 16-element runs
+        for (V* p : P) aligned = aligned && (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+        if (v && aligned) launch(k_advance_v8_g<Pr>, g2(run0.grid_w(0)), TPB, 0, s, cg_at(CNT_ADVANCE));
+        else launch(k_advance_g<Pr>, g2(grid_tiles(c, 0)), TPB, 0, s, cg_at(CNT_ADVANCE));
+        Grp<const int*> d;
+        memset(&d, 0, sizeof(d));
+        for (int i = 0; i < nb(); i++) d.a[i] = done_of(cs[i]);
+        launch(k_group_cond, 1, 1, 0, s, d, nb(), cond);
+    }
+};
+static_assert(sizeof(Grp<GCmg<double>>) < 32000, "a group launch's arguments fit the kernel parameter space");
 
 int write_params(mpp_ctx* c, float volume0, double dt, double recover, int project, float gamma, cudaStream_t s) {
     Params& p = c->sc_host->p;
@@ -1764,7 +1966,100 @@ struct mpp_batch {
     std::vector<const void*> key;
     std::vector<int> counts;  // per basin: prologue, body, epilogue kernels
     int dev = -1;
+    int grouped = 1;              // run basins that share a size and settings as groups
+    std::vector<int> group_of;    // per basin: its group in the recorded graph, -1 alone
+    int ngroups = 0;
 };
+
+extern "C++" {
+namespace {
+// Basins that may share a group's launches: the same grid, precision, sweeps, smoother forms
+// and level split (so the same launch sequence and grid widths); FP64 and the TMA form keep
+// their own chains.
+bool groupable(const mpp_ctx* c) {
+    return c->prec != MPP_PREC_FP64 && c->form_fine != MPP_SMOOTHER_TMA && c->form_coarse != MPP_SMOOTHER_TMA;
+}
+bool same_group(const mpp_ctx* a, const mpp_ctx* b) {
+    return a->prec == b->prec && a->grid.n[0] == b->grid.n[0] && a->grid.n[1] == b->grid.n[1] &&
+           a->grid.n[2] == b->grid.n[2] && a->L == b->L && a->opts.sweeps == b->opts.sweeps &&
+           a->opts.sweeps_coarse == b->opts.sweeps_coarse && a->opts.coarse == b->opts.coarse &&
+           a->form_fine == b->form_fine && a->form_coarse == b->form_coarse && a->lb == b->lb &&
+           a->cmg_ls == b->cmg_ls && a->cmg_cs == b->cmg_cs && a->cmg_smem == b->cmg_smem &&
+           a->bot_smem == b->bot_smem && a->async_blocks == b->async_blocks;
+}
+
+// The group kernels' shared-memory limits, as their single-basin twins'.
+template <class Pr>
+int group_attrs(const mpp_ctx* c) {
+    int optin = 0;
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
+    CK(cudaFuncSetAttribute(k_bottom_g<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    CK(cudaFuncSetAttribute(k_restrict_g<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->restrict_smem));
+    for (auto kern : {k_cmg_g<Pr, 0>, k_cmg_g<Pr, 1>}) {
+        cudaFuncAttributes fa;
+        CK(cudaFuncGetAttributes(&fa, kern));
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
+    if constexpr (sizeof(typename Pr::M) == 2)
+        CK(cudaFuncSetAttribute(k_rbgs_async_g<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, AS_SMEM));
+    return MPP_OK;
+}
+
+// Record a group's solves into graph g: each basin's prologue as a chain of its own, one
+// conditional WHILE node over the group's loop body (GroupRun) after all of them, then each
+// basin's epilogue. counts: per basin, kernels in prologue, body, epilogue.
+template <class Pr>
+int record_group(const std::vector<mpp_ctx*>& cs, const std::vector<Call>& ks, cudaGraph_t g, int* counts) {
+    using V = typename Pr::V;
+    if (int e = group_attrs<Pr>(cs[0])) return e;
+    cudaStream_t s = cs[0]->cap;
+    std::vector<cudaGraphNode_t> tails;
+    for (size_t i = 0; i < cs.size(); i++) {
+        Run<Pr> pro{cs[i], s};
+        CK(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        record_prologue<Pr>(pro, ks[i], 0, 0);
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        cudaStreamCaptureStatus cst;
+        const cudaError_t qe = cudaStreamGetCaptureInfo(s, &cst, nullptr, nullptr, &deps, &nd);
+        if (qe == cudaSuccess) tails.insert(tails.end(), deps, deps + nd);
+        cudaGraph_t gg = g;
+        CK(cudaStreamEndCapture(s, &gg));
+        CK(qe);
+        counts[3 * i] = pro.nk;
+    }
+    cudaGraphConditionalHandle cond;
+    CK(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CK(cudaGraphAddNode(&cnode, g, tails.data(), tails.size(), &cp));
+    cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+    std::vector<V*> Ps;
+    for (const Call& k : ks) Ps.push_back((V*)k.P);
+    GroupRun<Pr> gr(cs, Ps, s);
+    CK(cudaStreamBeginCaptureToGraph(s, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    gr.body(cond);
+    const cudaError_t le = cudaGetLastError();  // a launch refused during the capture
+    CK(cudaStreamEndCapture(s, &bodyg));
+    CK(le);
+    for (size_t i = 0; i < cs.size(); i++) {
+        Run<Pr> epi{cs[i], s};
+        CK(cudaStreamBeginCaptureToGraph(s, g, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
+        record_epilogue<Pr>(epi, ks[i]);
+        cudaGraph_t gg = g;
+        CK(cudaStreamEndCapture(s, &gg));
+        counts[3 * i + 1] = gr.nk;
+        counts[3 * i + 2] = epi.nk;
+    }
+    return MPP_OK;
+}
+}  // namespace
+}  // extern "C++"
 
 static void batch_drop_graph(mpp_batch* b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
@@ -1808,6 +2103,18 @@ int mpp_batch_destroy(mpp_batch* b) {
 }
 
 int mpp_batch_size(const mpp_batch* b) { return b ? (int)b->ctx.size() : 0; }
+
+int mpp_batch_set_grouped(mpp_batch* b, int on) {
+    if (!b) {
+        set_err("null batch");
+        return MPP_ERR_INVALID;
+    }
+    if (b->grouped != (on ? 1 : 0)) batch_drop_graph(b);
+    b->grouped = on ? 1 : 0;
+    return MPP_OK;
+}
+
+int mpp_batch_groups(const mpp_batch* b) { return b ? b->ngroups : 0; }
 
 mpp_ctx* mpp_batch_ctx(mpp_batch* b, int i) {
     if (!b || i < 0 || i >= (int)b->ctx.size()) return nullptr;
@@ -1855,9 +2162,45 @@ int mpp_batch_project(mpp_batch* b, const mpp_basin_arrays* basins, double dt, d
         batch_drop_graph(b);
         CK(cudaGraphCreate(&b->graph, 0));
         b->counts.assign(3 * n, 0);
-        for (int i = 0; i < n; i++) {
+        b->group_of.assign(n, -1);
+        b->ngroups = 0;
+        auto call_of = [&](int i) {
             const mpp_basin_arrays& a = basins[i];
-            Call k{1, a.u, a.v, a.w, a.fu, a.fv, a.fw, a.P, nullptr, a.types, a.phi};
+            return Call{1, a.u, a.v, a.w, a.fu, a.fv, a.fw, a.P, nullptr, a.types, a.phi};
+        };
+        // groups of basins with the same launch sequence (at most GRP_MAX each), in basin order
+        std::vector<std::vector<int>> groups;
+        if (b->grouped)
+            for (int i = 0; i < n; i++) {
+                mpp_ctx* c = b->ctx[i];
+                if (!groupable(c) || b->group_of[i] >= 0) continue;
+                std::vector<int> g{i};
+                for (int j = i + 1; j < n && (int)g.size() < GRP_MAX; j++)
+                    if (b->group_of[j] < 0 && groupable(b->ctx[j]) && same_group(c, b->ctx[j])) g.push_back(j);
+                if (g.size() < 2) continue;
+                for (int j : g) b->group_of[j] = (int)groups.size();
+                groups.push_back(g);
+            }
+        b->ngroups = (int)groups.size();
+        for (const auto& g : groups) {
+            std::vector<mpp_ctx*> cs;
+            std::vector<Call> ks;
+            for (int j : g) {
+                cs.push_back(b->ctx[j]);
+                ks.push_back(call_of(j));
+            }
+            std::vector<int> cnt(3 * g.size());
+            int e = dispatch(cs[0]->prec, [&](auto pr) { return record_group<decltype(pr)>(cs, ks, b->graph, cnt.data()); });
+            if (e) {
+                batch_drop_graph(b);
+                return e;
+            }
+            for (size_t q = 0; q < g.size(); q++)
+                for (int r = 0; r < 3; r++) b->counts[3 * g[q] + r] = cnt[3 * q + r];
+        }
+        for (int i = 0; i < n; i++) {
+            if (b->group_of[i] >= 0) continue;
+            const Call k = call_of(i);
             mpp_ctx* c = b->ctx[i];
             int e = dispatch(c->prec, [&](auto pr) { return record_solve<decltype(pr)>(c, k, b->graph, &b->counts[3 * i]); });
             if (e) {

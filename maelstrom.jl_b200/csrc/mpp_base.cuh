@@ -556,11 +556,16 @@ __device__ __forceinline__ void restrict_bottom_body(Lev<typename Pr::M> F, Lev<
     }
 }
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_restrict_bottom(Lev<typename Pr::M> F, Lev<typename Pr::M> L,
+__device__ __forceinline__ void restrict_bottom_dev(Lev<typename Pr::M> F, Lev<typename Pr::M> L,
                                                          typename Pr::C* __restrict__ bout) {
     pdl_wait();
     pdl_trigger();
     restrict_bottom_body<Pr>(F, L, bout);
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_restrict_bottom(Lev<typename Pr::M> F, Lev<typename Pr::M> L,
+                                                         typename Pr::C* __restrict__ bout) {
+    restrict_bottom_dev<Pr>(F, L, bout);
 }
 
 

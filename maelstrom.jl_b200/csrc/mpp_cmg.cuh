@@ -493,7 +493,7 @@ __device__ __forceinline__ void cmg_prolong(const CmgSlab& F, int qf, const CmgS
 }
 
 template <class Pr, int UP>
-__global__ void __launch_bounds__(CMG_THREADS, 1) k_cmg(const __grid_constant__ CmgArgs<typename Pr::M> a) {
+__device__ __forceinline__ void cmg_dev(const CmgArgs<typename Pr::M>& a) {
     using C = typename Pr::C;
     using M = typename Pr::M;
     const int me = (int)blockIdx.x, cs = (int)gridDim.x, nl = a.nl;
@@ -541,6 +541,10 @@ __global__ void __launch_bounds__(CMG_THREADS, 1) k_cmg(const __grid_constant__ 
         cmg_store<Pr>(a.s[0], a.g[0], me, false);
     }
     // (every CTA passed the last barrier after its last read of another CTA's memory)
+}
+template <class Pr, int UP>
+__global__ void __launch_bounds__(CMG_THREADS, 1) k_cmg(const __grid_constant__ CmgArgs<typename Pr::M> a) {
+    cmg_dev<Pr, UP>(a);
 }
 
 }  // namespace mpp

@@ -614,8 +614,7 @@ struct DotLd {
     bool ok;
 };
 template <class Pr>
-__global__ void __launch_bounds__(TPB)
-    k_dot_v8(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ qv,
+__device__ __forceinline__ void dot_v8_dev(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ qv,
              Scalars* sc, double* partials, unsigned* counter) {
     using M = typename Pr::M;
     using V = typename Pr::V;
@@ -659,6 +658,11 @@ __global__ void __launch_bounds__(TPB)
     if (done) return;
     if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0) dot_finish<Pr>(sc, acc);
 }
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_dot_v8(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ qv,
+             Scalars* sc, double* partials, unsigned* counter) {
+    dot_v8_dev<Pr>(L, r, qv, sc, partials, counter);
+}
 
 // search_kernel! (src/flip.jl:1033-1054), vector form: one colour of a tile a unit. Every
 // array it reads dates from before the preceding kernel (z·r, which writes only the
@@ -693,8 +697,7 @@ __device__ __forceinline__ void search_fetch(const Lev<typename Pr::M>& L, const
     a.dn = ld_nb8(dvec, o, sy, sz);
 }
 template <class Pr>
-__global__ void __launch_bounds__(TPB, 2)
-    k_search_v8(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ diag,
+__device__ __forceinline__ void search_v8_dev(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ diag,
                 typename Pr::V* __restrict__ qout, Scalars* sc, double* partials, unsigned* counter) {
     using C = typename Pr::C;
     using M = typename Pr::M;
@@ -747,12 +750,16 @@ __global__ void __launch_bounds__(TPB, 2)
     }
     if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) search_finish<Pr>(sc, acc);
 }
+template <class Pr>
+__global__ void __launch_bounds__(TPB, 2) k_search_v8(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ diag,
+                typename Pr::V* __restrict__ qout, Scalars* sc, double* partials, unsigned* counter) {
+    search_v8_dev<Pr>(L, dvec, diag, qout, sc, partials, counter);
+}
 
 // advance_kernel! (src/flip.jl:1059-1073), vector form. The lane's 16 cells (both colours)
 // are 16 consecutive cells of the natural row, so P moves as one 16-element run.
 template <class Pr>
-__global__ void __launch_bounds__(TPB, 3)
-    k_advance_v8(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ qv,
+__device__ __forceinline__ void advance_v8_dev(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ qv,
                  typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
                  unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
     using C = typename Pr::C;
@@ -819,6 +826,12 @@ __global__ void __launch_bounds__(TPB, 3)
         st8(P + pn + V8, P1);
     }
     if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) advance_finish<Pr>(sc, acc, cond, use_cond);
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB, 3) k_advance_v8(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ qv,
+                 typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
+                 unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
+    advance_v8_dev<Pr>(L, dvec, qv, r, P, sc, partials, counter, cond, use_cond);
 }
 
 // prolong_kernel! (src/flip.jl:914-929), vector form: one warp per fine tile stages the
@@ -1000,8 +1013,7 @@ __global__ void __launch_bounds__(TPB) k_residual(Lev<typename Pr::M> L) {
 // CG (src/sflip.jl:1896-1897); as r = r_old - alpha q, z.r_old = rho_new + alpha z.q, so
 // no copy of r_old is kept.
 template <class Pr>
-__global__ void __launch_bounds__(TPB)
-    k_dot(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ q,
+__device__ __forceinline__ void dot_dev(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ q,
           Scalars* sc, double* partials, unsigned* counter) {
     pdl_wait();
     pdl_trigger();
@@ -1057,12 +1069,16 @@ __global__ void __launch_bounds__(TPB)
         S.rho = rho_new;
     }
 }
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_dot(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ r, const typename Pr::V* __restrict__ q,
+          Scalars* sc, double* partials, unsigned* counter) {
+    dot_dev<Pr>(L, r, q, sc, partials, counter);
+}
 
 // search_kernel! (src/flip.jl:1033-1054): p = z + beta d made where it is used, q = A p,
 // and p.q; then alpha = rho / p.q (src/flip.jl:1100).
 template <class Pr>
-__global__ void __launch_bounds__(TPB)
-    k_search(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ diag,
+__device__ __forceinline__ void search_dev(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ diag,
              typename Pr::V* __restrict__ q, Scalars* sc, double* partials, unsigned* counter) {
     pdl_wait();
     pdl_trigger();
@@ -1125,13 +1141,17 @@ __global__ void __launch_bounds__(TPB)
         }
     }
 }
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_search(Lev<typename Pr::M> L, const typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ diag,
+             typename Pr::V* __restrict__ q, Scalars* sc, double* partials, unsigned* counter) {
+    search_dev<Pr>(L, dvec, diag, q, sc, partials, counter);
+}
 
 // advance_kernel! (src/flip.jl:1059-1073): d = z + beta d; P += alpha d; r -= alpha q; then
 // rnorm = sqrt(r.r) and the exit test rnorm <= tol |b| (src/flip.jl:1102-1103), or maxiter.
 // The 16-bit forms also store the (scaled) r in the V-cycle's precision for its next pass.
 template <class Pr>
-__global__ void __launch_bounds__(TPB)
-    k_advance(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ q,
+__device__ __forceinline__ void advance_dev(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ q,
               typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
               unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
     pdl_wait();
@@ -1199,6 +1219,12 @@ __global__ void __launch_bounds__(TPB)
         }
         set_cond(cond, use_cond, !S.done);
     }
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_advance(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ q,
+              typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
+              unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
+    advance_dev<Pr>(L, dvec, q, r, P, sc, partials, counter, cond, use_cond);
 }
 
 // |b - A P| over the fine level: the true residual at exit (the reference's sparse

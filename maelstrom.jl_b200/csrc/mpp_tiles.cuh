@@ -371,8 +371,8 @@ struct BotArgs {
 };
 
 template <class Pr>
-__global__ void __launch_bounds__(1024) k_bottom(const typename Pr::C* __restrict__ bin, typename Pr::M* __restrict__ xout,
-                                                 BotArgs a) {
+__device__ __forceinline__ void bottom_dev(const typename Pr::C* __restrict__ bin, typename Pr::M* __restrict__ xout,
+                                           const BotArgs& a) {
     pdl_wait();
     pdl_trigger();
     using C = typename Pr::C;
@@ -600,6 +600,11 @@ __global__ void __launch_bounds__(1024) k_bottom(const typename Pr::C* __restric
             for (int c = tid; c < N; c += T) st(xout + c, x[c]);
         }
     }
+}
+template <class Pr>
+__global__ void __launch_bounds__(1024) k_bottom(const typename Pr::C* __restrict__ bin, typename Pr::M* __restrict__ xout,
+                                                 const __grid_constant__ BotArgs a) {
+    bottom_dev<Pr>(bin, xout, a);
 }
 
 }  // namespace mpp

@@ -221,7 +221,7 @@ __device__ __forceinline__ void as_piece(int e, int& kk, int& jj, int& pc) {
 }
 
 template <class Pr>
-__global__ void __launch_bounds__(TPB) k_rbgs_async(Lev<typename Pr::M> L, int colour) {
+__device__ __forceinline__ void rbgs_async_dev(Lev<typename Pr::M> L, int colour) {
     using C = typename Pr::C;
     using M = typename Pr::M;
     static_assert(sizeof(M) == 2, "the async form stages 8 elements a 16-byte piece");
@@ -305,6 +305,10 @@ __global__ void __launch_bounds__(TPB) k_rbgs_async(Lev<typename Pr::M> L, int c
         if (a.ok) st8(L.x + a.p, rbgs_tile<C, M>(a, edge, Pr::scaled, by_di));
     }
     cp_async_wait<0>();
+}
+template <class Pr>
+__global__ void __launch_bounds__(TPB) k_rbgs_async(Lev<typename Pr::M> L, int colour) {
+    rbgs_async_dev<Pr>(L, colour);
 }
 
 }  // namespace mpp

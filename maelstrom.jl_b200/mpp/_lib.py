@@ -80,6 +80,8 @@ SIGNATURES = {
     "mpp_batch_create": (ctypes.c_int, [ctypes.POINTER(P), ctypes.c_int, _G, _O]),
     "mpp_batch_destroy": (ctypes.c_int, [P]),
     "mpp_batch_size": (ctypes.c_int, [P]),
+    "mpp_batch_set_grouped": (ctypes.c_int, [P, ctypes.c_int]),
+    "mpp_batch_groups": (ctypes.c_int, [P]),
     "mpp_batch_ctx": (P, [P, ctypes.c_int]),
     "mpp_batch_project": (ctypes.c_int, [P, ctypes.POINTER(BasinArrays), F64, F64, _R, P]),
     "mpp_ctx_set_smoother": (ctypes.c_int, [P, ctypes.c_int]),

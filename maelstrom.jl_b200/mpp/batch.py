@@ -3,7 +3,8 @@ the partition of a batch over GPUs.
 
 :class:`Batch` owns an ``mpp_batch`` (one solver context per basin) and each basin's
 arrays on the device; :meth:`Batch.project` is ``project!`` of every basin as one CUDA
-graph launch. :meth:`Batch.autotune` times each distinct basin size's own solve over the
+graph launch, basins of one size and settings grouped so each pass of their CG loops is one
+launch over the group. :meth:`Batch.autotune` times each distinct basin size's own solve over the
 smoother forms and sweep counts (``mpp_autotune``) and applies the winner to every basin
 of that size. :func:`lpt_partition` splits a batch over ranks (longest processing time
 first on cells x expected iterations): basins are independent, so ranks exchange
@@ -82,6 +83,16 @@ class Batch:
 
     def ctx(self, i: int) -> ctypes.c_void_p:
         return ctypes.c_void_p(self.lib.mpp_batch_ctx(self._b, i))
+
+    def set_grouped(self, on: bool = True):
+        """Run basins of one size and settings as groups (one launch a pass for the group;
+        the default) or each basin as its own chain (``mpp_batch_set_grouped``)."""
+        check(self.lib.mpp_batch_set_grouped(self._b, 1 if on else 0))
+
+    @property
+    def groups(self) -> int:
+        """Groups in the last recorded batch graph."""
+        return int(self.lib.mpp_batch_groups(self._b))
 
     def close(self):
         if getattr(self, "_b", None) and self._b.value:

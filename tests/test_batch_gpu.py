@@ -16,18 +16,22 @@ def _small_batch():
     return [scene.box_basin(n, seed=6000 + i, height=h, wall=w) for i, (n, h, w) in enumerate(sizes)]
 
 
+@pytest.mark.parametrize("grouped", [True, False])
 @pytest.mark.parametrize("precision", ["fp32", "fp16"])
-def test_batch_equals_one_by_one(cuda, precision):
-    """One graph launch for all basins gives each basin's own project! bit for bit."""
+def test_batch_equals_one_by_one(cuda, precision, grouped):
+    """One graph launch for all basins gives each basin's own project! bit for bit, whether
+    basins of one size run as a group (one launch a pass for all of them) or as chains."""
     import mpp
     from mpp.batch import Batch
 
     basins = _small_batch()
     batch = Batch(basins, tol=1e-6, maxiter=100, precision=precision)
+    batch.set_grouped(grouped)
     for _ in range(2):  # the second call reuses the captured graph (warm starts from the first)
         res = batch.project(1 / 48)
         ones = []
         assert all(r.status == 0 for r in res), [r.as_dict() for r in res]
+    assert batch.groups == (2 if grouped else 0)  # the two 16^3 and the two 32^3 basins
     for i, b in enumerate(basins):
         s = mpp.FlipBasin.from_scene(b, tol=1e-6, maxiter=100, precision=precision, graph=True)
         its = []
@@ -97,3 +101,30 @@ def test_batched_workload(cuda):
     res = batch.project(1 / 48)
     assert len(res) == 48
     assert all(r.status == 0 and r.true_rel_residual <= 2e-6 for r in res), [r.as_dict() for r in res if r.status]
+
+
+@pytest.mark.parametrize("forms", [("vector", "vector"), ("column", "column"), ("async", "vector")])
+def test_grouped_forms_and_uneven_iterations(cuda, forms):
+    """Groups of basins converging after different iteration counts (the done ones skip the
+    remaining passes) equal each basin's own solve, for the forms a group may run."""
+    import mpp
+    from mpp.batch import Batch
+
+    basins = [scene.box_basin(32, seed=6300 + i, height=h, wall=w)
+              for i, (h, w) in enumerate([(0.3, 0.45), (0.8, 0.40), (0.55, 0.36), (0.7, 0.47)])]
+    batch = Batch(basins, tol=1e-7, maxiter=100, precision="fp16")
+    for i in range(len(basins)):
+        from mpp import _lib
+
+        _lib.check(batch.lib.mpp_ctx_set_smoothers(batch.ctx(i), *(
+            {v: k for k, v in _lib.SMOOTHERS.items()}[f] for f in forms)))
+    res = batch.project(1 / 48)
+    assert batch.groups == 1
+    its = [r.iterations for r in res]
+    for i, b in enumerate(basins):
+        s = mpp.FlipBasin.from_scene(b, tol=1e-7, maxiter=100, precision="fp16", graph=True)
+        s.projector.set_smoothers(*forms)
+        mpp.project(s, 1 / 48)
+        assert its[i] == s.iterations[-1]
+        for k in ("u", "v", "w", "fu", "fv", "fw", "P"):
+            np.testing.assert_array_equal(_np(batch.arrays[i][k]), _np(getattr(s, k)), err_msg=f"basin {i} {k}")
