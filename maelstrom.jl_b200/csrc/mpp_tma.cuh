@@ -188,13 +188,13 @@ __global__ void __launch_bounds__(TPB) k_rbgs_tma(Lev<typename Pr::M> L, int col
 // cp.async copies (no registers held while they fly): the own colour's b and reciprocal
 // diagonal (one piece a lane) and the other colour's x around the tile (the 4 x 2 rows of
 // the tile, the rows at -+y, the planes at -+z, and one piece each side along x: 96 pieces),
-// AS_STAGES - 1 tiles ahead of the one it computes. A lane then reads its 8 cells'
+// AS_STAGES - 1 tiles ahead of the one it computes, in slots of exactly those 96 pieces. A lane then reads its 8 cells'
 // neighbours from shared memory and updates them with the vector form's arithmetic
 // (rbgs_tile), so both forms give the same values. Reads past the level's rows and planes
 // land in the x array's zeroed guard, as the vector form's do.
-constexpr int AS_STAGES = 3;
-constexpr int AS_SLOTS = 4 * 6 * 6;  // x pieces [plane k0-1 .. k0+2][row j0-1 .. j0+4][piece -1 .. 4]
-constexpr int AS_STAGE = AS_SLOTS * 16 + 2 * 32 * 16;  // + b and 1/diag, a piece a lane
+constexpr int AS_STAGES = 4;
+constexpr int AS_PIECES = 96;  // x pieces a tile needs
+constexpr int AS_STAGE = AS_PIECES * 16 + 2 * 32 * 16;  // + b and 1/diag, a piece a lane
 constexpr int AS_SMEM = (TPB / 32) * AS_STAGES * AS_STAGE;
 
 __device__ __forceinline__ void cp_async16(void* sm, const void* gm) {
@@ -205,9 +205,10 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
-__device__ __forceinline__ int as_slot(int kk, int jj, int pc) { return (kk * 6 + jj) * 6 + pc; }
-// The e-th of a tile's 96 x pieces (e < 96): the tile's own rows, the rows at -+y, the
-// planes at -+z, the pieces beside the rows along x.
+// The e-th of a tile's 96 x pieces (slot e of a stage), as (plane kk, row jj, piece pc)
+// around the tile (kk: planes k0-1 .. k0+2, jj: rows j0-1 .. j0+4, pc: pieces -1 .. 4): the
+// tile's own rows (e < 32, e = the lane that owns the piece: 16 (kk-1) + 4 (jj-1) + pc-1),
+// the rows at -+y, the planes at -+z, the pieces beside the rows along x.
 __device__ __forceinline__ void as_piece(int e, int& kk, int& jj, int& pc) {
     if (e < 32) {
         kk = 1 + (e >> 4); jj = 1 + ((e >> 2) & 3); pc = 1 + (e & 3);
@@ -250,8 +251,8 @@ __device__ __forceinline__ void rbgs_async_dev(Lev<typename Pr::M> L, int colour
         const int h = h0 + hq * V8, j = j0 + lj, k = k0 + lk;
         if (h < H && j < n2 && k < L.n3) {
             const int p = (k * n2 + j) * n1 + own + h;
-            cp_async16(st + AS_SLOTS * 16 + lane * 16, L.b + p);
-            cp_async16(st + AS_SLOTS * 16 + 512 + lane * 16, dsrc + p);
+            cp_async16(st + AS_PIECES * 16 + lane * 16, L.b + p);
+            cp_async16(st + AS_PIECES * 16 + 512 + lane * 16, dsrc + p);
         }
 #pragma unroll
         for (int q = 0; q < 3; q++) {
@@ -262,7 +263,7 @@ __device__ __forceinline__ void rbgs_async_dev(Lev<typename Pr::M> L, int colour
             // skipping them keeps every copy inside the array and its one-plane guard
             if (jr > n2 || (kr == L.n3 && jr >= n2)) continue;
             const int pos = (kr * n2 + jr) * n1 + oth + h0 + (pc - 1) * V8;
-            cp_async16(st + as_slot(kk, jj, pc) * 16, L.x + pos);
+            cp_async16(st + (lane + 32 * q) * 16, L.x + pos);
         }
     };
 #pragma unroll
@@ -286,20 +287,23 @@ __device__ __forceinline__ void rbgs_async_dev(Lev<typename Pr::M> L, int colour
             a.p = (k * n2 + j) * n1 + own + h;
             a.ci = ci_of(colour, j, k);
             if (need_code) a.cdw = *reinterpret_cast<const uint2*>(L.code + a.p);
-            auto piece = [&](int kk, int jj, int pc) {
+            auto piece = [&](int e) {
                 Vec8<M> v;
-                *reinterpret_cast<uint4*>(v.v) = *reinterpret_cast<const uint4*>(st + as_slot(kk, jj, pc) * 16);
+                *reinterpret_cast<uint4*>(v.v) = *reinterpret_cast<const uint4*>(st + e * 16);
                 return v;
             };
-            *reinterpret_cast<uint4*>(a.bv.v) = *reinterpret_cast<const uint4*>(st + AS_SLOTS * 16 + lane * 16);
-            *reinterpret_cast<uint4*>(a.dv.v) = *reinterpret_cast<const uint4*>(st + AS_SLOTS * 16 + 512 + lane * 16);
-            a.xc = piece(1 + lk, 1 + lj, 1 + hq);
-            a.yp = piece(1 + lk, 2 + lj, 1 + hq);
-            a.ym = piece(1 + lk, lj, 1 + hq);
-            a.zp = piece(2 + lk, 1 + lj, 1 + hq);
-            a.zm = piece(lk, 1 + lj, 1 + hq);
-            a.xl = reinterpret_cast<const M*>(st + as_slot(1 + lk, 1 + lj, hq) * 16)[V8 - 1];
-            a.xr = reinterpret_cast<const M*>(st + as_slot(1 + lk, 1 + lj, 2 + hq) * 16)[0];
+            // the lane's own piece is slot `lane`; its neighbours' are the adjacent lanes'
+            // slots inside the tile, the halo slots at its edges
+            *reinterpret_cast<uint4*>(a.bv.v) = *reinterpret_cast<const uint4*>(st + AS_PIECES * 16 + lane * 16);
+            *reinterpret_cast<uint4*>(a.dv.v) =
+                *reinterpret_cast<const uint4*>(st + AS_PIECES * 16 + 512 + lane * 16);
+            a.xc = piece(lane);
+            a.yp = piece(lj < TY - 1 ? lane + 4 : 32 + 8 * lk + 4 + hq);
+            a.ym = piece(lj > 0 ? lane - 4 : 32 + 8 * lk + hq);
+            a.zp = piece(lk == 0 ? lane + 16 : 64 + 4 * lj + hq);
+            a.zm = piece(lk == 1 ? lane - 16 : 48 + 4 * lj + hq);
+            a.xl = reinterpret_cast<const M*>(st + (hq > 0 ? lane - 1 : 80 + 8 * lk + 2 * lj) * 16)[V8 - 1];
+            a.xr = reinterpret_cast<const M*>(st + (hq < V8_LANES_H - 1 ? lane + 1 : 81 + 8 * lk + 2 * lj) * 16)[0];
         }
         __syncwarp();  // stage s is read; the next iteration's copies may overwrite it
         if (a.ok) st8(L.x + a.p, rbgs_tile<C, M>(a, edge, Pr::scaled, by_di));
