@@ -250,7 +250,7 @@ def run_mpp(args):
         proj = make(prec, False)
         if args.tuned:
             fine, coarse, sw, swc, csw = args.tuned.split(",")
-            forms = {"vector": 0, "tma": 1, "column": 2}
+            forms = {"vector": 0, "tma": 1, "column": 2, "async": 3}
             proj.set(sweeps=int(sw), sweeps_coarse=int(swc), coarse=int(csw))
             proj.lib.mpp_ctx_set_smoothers(proj._ctx, forms[fine], forms[coarse])
         vol0 = proj.volume(phi)
@@ -366,6 +366,8 @@ def run_mpp(args):
                        "fp64_rel_error": err_fp32, "graph": False, "gpu_launches": launches32},
         "mixed_over_fp32": round(value / value32, 3),
         "autotuned": tune["chosen"],
+        "autotune_forms_ms": {f"{r['smoother']}/{r['coarse_smoother']}": r["ms"] for r in tune["table"]
+                              if (r["sweeps"], r["sweeps_coarse"], r["coarse_sweeps"]) == (2, 0, 40)},
         "fp32_graph_tuned": {"value": round(value32g, 3), "unit": UNIT, "iterations": its32g[-1],
                              "autotuned": tune32["chosen"]},
         "fp64_oracle": {"iterations": res64.iterations, "true_rel_residual": res64.true_rel_residual},
@@ -461,18 +463,21 @@ def bench_batched(steps):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / steps, res
 
+    chosen = batch.max_group
     ms, res = timed()
     groups = batch.groups
-    its_grouped = [r.iterations for r in res]
-    # the same batch with every basin as its own chain of launches, for comparison
-    batch.set_grouped(False)
-    ms_chains, res_c = timed()
-    batch.set_grouped(True)
+    its = [r.iterations for r in res]
+    # the other grouping, for comparison: groups of 16 if chains won, else chains
+    batch.set_grouped(16 if chosen < 2 else 0)
+    ms_other, res_o = timed()
+    batch.set_grouped(chosen)
     launches = sum(r.kernel_launches for r in res)
     return {"basins": len(basins), "cells": cells, "projections_per_s": round(len(basins) / (ms / 1e3), 2),
             "cells_per_s": cells / (ms / 1e3), "ms_per_batch": round(ms, 3), "steps": steps,
-            "groups": groups, "chains_projections_per_s": round(len(basins) / (ms_chains / 1e3), 2),
-            "chains_same_iterations": its_grouped == [r.iterations for r in res_c],
+            "grouping": {"chosen_max_group": chosen, "groups": groups, "autotune_ms": batch.grouping,
+                         "other": {"max_group": 16 if chosen < 2 else 0,
+                                   "projections_per_s": round(len(basins) / (ms_other / 1e3), 2),
+                                   "same_iterations": its == [r.iterations for r in res_o]}},
             "graph_launches_per_batch": 1, "gpu_launches_per_batch": launches,
             "iterations": [r.iterations for r in res], "all_converged": all(r.status == 0 for r in res),
             "max_true_rel_residual": max(r.true_rel_residual for r in res),

@@ -231,14 +231,18 @@ typedef struct {
 int mpp_batch_create(mpp_batch** batch, int count, const mpp_grid* grids, const mpp_opts* opts);
 int mpp_batch_destroy(mpp_batch* batch);
 int mpp_batch_size(const mpp_batch* batch);
-/* Group the batch's basins (on, the default) or give each basin its own chain (off). A group
- * is at most 16 basins with the same grid, precision, sweeps, smoother forms and level split
- * (not FP64, not the TMA form): each pass of their CG loops is one launch over all of them
- * (the basin is the launch's second grid dimension, every basin keeping its own grid width,
- * arithmetic and reductions, so results are bit-identical either way), converged basins skip
- * the remaining passes, and the group's loop is one conditional node that ends when all are
- * done. mpp_batch_groups: groups in the last recorded graph. */
-int mpp_batch_set_grouped(mpp_batch* batch, int on);
+/* Group the batch's basins: groups of at most `max_group` (2 .. 16; the default 16) basins
+ * with the same grid, precision, sweeps, smoother forms and level split (not FP64, not the
+ * TMA form), or, with max_group < 2, a chain of launches for each basin. Each pass of a
+ * group's CG loops is one launch over all of its basins (the basin is the launch's second
+ * grid dimension, every basin keeping its own grid width, arithmetic and reductions, so the
+ * results are bit-identical either way), converged basins skip the remaining passes, and the
+ * group's loop is one conditional node that ends when all are done. Fewer launches, but the
+ * basins of a group move through the V-cycle's phases together, where chains overlap one
+ * basin's latency-bound small levels with another's bandwidth-bound fine level: which is
+ * faster depends on the batch (Batch.autotune in the Python binding times the choices).
+ * mpp_batch_groups: groups in the last recorded graph. */
+int mpp_batch_set_grouped(mpp_batch* batch, int max_group);
 int mpp_batch_groups(const mpp_batch* batch);
 /* Basin i's context (options, smoother, autotuning); using it drops the batch's graph. */
 mpp_ctx* mpp_batch_ctx(mpp_batch* batch, int i);

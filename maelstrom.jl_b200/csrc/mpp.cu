@@ -1966,7 +1966,7 @@ struct mpp_batch {
     std::vector<const void*> key;
     std::vector<int> counts;  // per basin: prologue, body, epilogue kernels
     int dev = -1;
-    int grouped = 1;              // run basins that share a size and settings as groups
+    int grouped = GRP_MAX;        // largest group of basins that share a size and settings (< 2: none)
     std::vector<int> group_of;    // per basin: its group in the recorded graph, -1 alone
     int ngroups = 0;
 };
@@ -2104,13 +2104,14 @@ int mpp_batch_destroy(mpp_batch* b) {
 
 int mpp_batch_size(const mpp_batch* b) { return b ? (int)b->ctx.size() : 0; }
 
-int mpp_batch_set_grouped(mpp_batch* b, int on) {
+int mpp_batch_set_grouped(mpp_batch* b, int max_group) {
     if (!b) {
         set_err("null batch");
         return MPP_ERR_INVALID;
     }
-    if (b->grouped != (on ? 1 : 0)) batch_drop_graph(b);
-    b->grouped = on ? 1 : 0;
+    const int g = max_group < 2 ? 0 : (max_group > GRP_MAX ? GRP_MAX : max_group);
+    if (b->grouped != g) batch_drop_graph(b);
+    b->grouped = g;
     return MPP_OK;
 }
 
@@ -2170,12 +2171,12 @@ int mpp_batch_project(mpp_batch* b, const mpp_basin_arrays* basins, double dt, d
         };
         // groups of basins with the same launch sequence (at most GRP_MAX each), in basin order
         std::vector<std::vector<int>> groups;
-        if (b->grouped)
+        if (b->grouped >= 2)
             for (int i = 0; i < n; i++) {
                 mpp_ctx* c = b->ctx[i];
                 if (!groupable(c) || b->group_of[i] >= 0) continue;
                 std::vector<int> g{i};
-                for (int j = i + 1; j < n && (int)g.size() < GRP_MAX; j++)
+                for (int j = i + 1; j < n && (int)g.size() < b->grouped; j++)
                     if (b->group_of[j] < 0 && groupable(b->ctx[j]) && same_group(c, b->ctx[j])) g.push_back(j);
                 if (g.size() < 2) continue;
                 for (int j : g) b->group_of[j] = (int)groups.size();
@@ -2597,6 +2598,10 @@ int mpp_redistance(mpp_ctx* c, float* phi, float* phi0, int iterations, uint8_t*
         return MPP_ERR_INVALID;
     }
     const int64_t N = (int64_t)c->grid.n[0] * c->grid.n[1] * c->grid.n[2];
+    if (N >= ((int64_t)1 << 31)) {
+        set_err("grids of 2^31 or more cells are not supported here");
+        return MPP_ERR_INVALID;
+    }
     if (iterations > 0 && phi0 < phi + N && phi < phi0 + N) {
         set_err("phi and phi0 overlap");
         return MPP_ERR_INVALID;
@@ -2650,6 +2655,10 @@ int mpp_filltrapped(mpp_ctx* c, uint8_t* types, float* phi, int maxrounds, int* 
     const int n1 = c->grid.n[0], n2 = c->grid.n[1], n3 = c->grid.n[2];
     const int W1 = (n1 + 31) / 32;
     const int64_t words = (int64_t)W1 * n2 * n3;
+    if ((int64_t)n1 * n2 * n3 >= ((int64_t)1 << 31)) {
+        set_err("grids of 2^31 or more cells are not supported here");
+        return MPP_ERR_INVALID;
+    }
     if (!c->trap_air) {  // the masks and the round loop's graph, on the first call
         if (int e = alloc(c, (void**)&c->trap_air, sizeof(uint32_t) * (size_t)words)) return e;
         if (int e = alloc(c, (void**)&c->trap_reach, sizeof(uint32_t) * (size_t)words)) return e;

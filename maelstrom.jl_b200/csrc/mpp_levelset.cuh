@@ -75,20 +75,22 @@ __global__ void __launch_bounds__(TPB) k_reinit(Geo g, const float* __restrict__
     pdl_wait();
     pdl_trigger();
     const int n1 = g.n[0], n2 = g.n[1], n3 = g.n[2];
-    const int rq = n1 / W;
-    const int64_t total = (int64_t)rq * n2 * n3;
+    const unsigned rq = (unsigned)(n1 / W);
+    const unsigned total = rq * (unsigned)n2 * (unsigned)n3;  // the host checks the grid fits 32 bits
     const float dx = g.dx, h = g.dx, R2 = g.radius * g.radius;
-    const int64_t sy = n1, sz = (int64_t)n1 * n2;
+    const unsigned sy = (unsigned)n1, sz = (unsigned)n1 * (unsigned)n2;
     // Far from the surface every neighbour distance is phimax: the update is then the same
     // for every such cell, eikonal(phimax, phimax, phimax, h) (its costliest branch, two
     // square roots and a division), formed once here by the same code.
     const float far = jmin(eikonal(phimax, phimax, phimax, h), phimax);
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-        const int q = (int)(t % rq);
-        const int64_t row = t / rq;
-        const int j = (int)(row % n2), k = (int)(row / n2);
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        // 32-bit index arithmetic: a 64-bit division costs more than the cell's update
+        const unsigned row = t / rq;
+        const int q = (int)(t - row * rq);
+        const unsigned kq = row / (unsigned)n2;
+        const int j = (int)(row - kq * (unsigned)n2), k = (int)kq;
         const int i0 = q * W;
-        const int64_t base = row * n1 + i0;
+        const unsigned base = row * (unsigned)n1 + (unsigned)i0;
         // the wall test (issolidcell, src/flip.jl:64-66) of cells i0-1 .. i0+W and of the
         // rows at -+y, -+z
         float pxx[W + 2];
@@ -234,9 +236,9 @@ __global__ void __launch_bounds__(TPB) k_trap_pack(TrapMasks T, const uint8_t* _
         st->maxrounds = maxrounds;
     }
     for (int64_t t = t0; t < words; t += (int64_t)gridDim.x * blockDim.x) {
-        const int wx = (int)(t % T.W1);
-        const int64_t row = t / T.W1;
-        const int k = (int)(row / T.n2);
+        const unsigned row = (unsigned)t / (unsigned)T.W1;  // the host checks the masks fit 32 bits
+        const int wx = (int)((unsigned)t - row * (unsigned)T.W1);
+        const int k = (int)(row / (unsigned)T.n2);
         const int i0 = wx * 32;
         const uint8_t* p = types + row * T.n1 + i0;
         uint32_t a = 0;

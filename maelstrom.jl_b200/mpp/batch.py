@@ -80,14 +80,19 @@ class Batch:
             self.volume0.append(vol.value)
         self._structs = None
         self.iterations = []
+        self.max_group = 16
+        self.grouping = None  # the autotuner's grouping choice and timings
 
     def ctx(self, i: int) -> ctypes.c_void_p:
         return ctypes.c_void_p(self.lib.mpp_batch_ctx(self._b, i))
 
-    def set_grouped(self, on: bool = True):
-        """Run basins of one size and settings as groups (one launch a pass for the group;
-        the default) or each basin as its own chain (``mpp_batch_set_grouped``)."""
-        check(self.lib.mpp_batch_set_grouped(self._b, 1 if on else 0))
+    def set_grouped(self, max_group=16):
+        """Run basins of one size and settings in groups of at most ``max_group`` (one launch a
+        pass for the group; True: 16, the default) or, with ``max_group`` < 2 or False, each
+        basin as its own chain (``mpp_batch_set_grouped``)."""
+        n = 16 if max_group is True else (0 if max_group is False else int(max_group))
+        check(self.lib.mpp_batch_set_grouped(self._b, n))
+        self.max_group = n
 
     @property
     def groups(self) -> int:
@@ -167,7 +172,44 @@ class Batch:
         self._structs = None
         if refine > 1:
             self._refine(groups, report, refine, s)
+            self._choose_grouping(report, s)
         return report
+
+    def _choose_grouping(self, report, stream, options=(0, 4, 8, 16)):
+        """Time the batch with its basins as chains and in groups of 4, 8 and 16, keep the
+        fastest (recorded in self.grouping)."""
+        import time
+
+        import torch
+
+        saved = [{n: a[n].clone() for n in ("u", "v", "w", "P")} for a in self.arrays]
+        hist = len(self.iterations)
+        times = {}
+        for g in options:
+            self.set_grouped(g)
+            best = float("inf")
+            for rep in range(3):  # the first launch captures the batch's graph
+                for a, sv in zip(self.arrays, saved):
+                    for n, t in sv.items():
+                        a[n].copy_(t)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                res = self.project(1 / 48, stream=stream)
+                torch.cuda.synchronize()
+                if any(r.status != 0 for r in res):
+                    best = float("inf")
+                    break
+                if rep:
+                    best = min(best, time.perf_counter() - t0)
+            times[g] = best
+        choice = min(times, key=times.get)
+        self.set_grouped(choice)
+        self.grouping = {"chosen": choice, "batch_ms": {str(k): round(1e3 * v, 3) for k, v in times.items()}}
+        for a, sv in zip(self.arrays, saved):
+            for n, t in sv.items():
+                a[n].copy_(t)
+        del self.iterations[hist:]
+        torch.cuda.synchronize()
 
     def _apply(self, members, cfg):
         fine, coarse, sw, swc, csw = cfg

@@ -87,7 +87,11 @@ def test_autotune(cuda):
                 for r in sorted((r for r in rep["table"] if r["status"] == 0), key=lambda r: r["ms"])]
         timed = {tuple(int(x) if x.isdigit() else x for x in k.split(",")): v for k, v in rep["batch_ms"].items()}
         assert set(timed) <= set(conv) and conv[0] in timed
-        assert rep["chosen"] == min(timed, key=timed.get)
+        # the fastest with the batch in flight (the timings are rounded: ties allowed)
+        assert timed[rep["chosen"]] == min(timed.values())
+    # then the grouping: chains, or groups of 4, 8, 16 basins, the fastest kept
+    assert batch.grouping is not None and set(batch.grouping["batch_ms"]) == {"0", "4", "8", "16"}
+    assert batch.grouping["chosen"] == batch.max_group
     res = batch.project(1 / 48)
     assert all(r.status == 0 for r in res)
 
