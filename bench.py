@@ -365,6 +365,9 @@ def run_mpp(args):
                        "iterations": its32[-1], "true_rel_residual": res32.true_rel_residual,
                        "fp64_rel_error": err_fp32, "graph": False, "gpu_launches": launches32},
         "mixed_over_fp32": round(value / value32, 3),
+        # the split of that gain: the graph and the autotuned sweeps (FP32 + graph + tuned over
+        # plain FP32) and the 16-bit storage alone (mixed over FP32 + graph + tuned)
+        "gain_split": {"graph_and_tuning": round(value32g / value32, 3), "precision": round(value / value32g, 3)},
         "autotuned": tune["chosen"],
         "autotune_forms_ms": {f"{r['smoother']}/{r['coarse_smoother']}": r["ms"] for r in tune["table"]
                               if (r["sweeps"], r["sweeps_coarse"], r["coarse_sweeps"]) == (2, 0, 40)},
