@@ -2499,7 +2499,7 @@ int mpp_extrapolate(mpp_ctx* c, float* u, float* v, float* w, uint8_t* fu, uint8
         c->launches++;
     }
     // a warp a word for the flags in and out, a thread a word for the layers
-    const dim3 gwarp(grid_cells(c, 32 * words_max), 3), gword(grid_cells(c, words_max), 3);
+    const dim3 gwarp(grid_cells(c, 32 * ((words_max + EXT_WW - 1) / EXT_WW)), 3), gword(grid_cells(c, words_max), 3);
     launch(k_extrap_flags, gwarp, TPB, 0, s, E);
     for (int l = 1; l <= layers; l++) launch(k_extrap_layer, gword, TPB, 0, s, E, l & 1);
     launch(k_extrap_final, gwarp, TPB, 0, s, E, layers % 2 == 0 ? 1 : 0, layers == 0 ? 1 : 0);

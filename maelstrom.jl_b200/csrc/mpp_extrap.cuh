@@ -111,8 +111,10 @@ __global__ void __launch_bounds__(TPB) k_extrap_open(Geo g, ExtBits E) {
     }
 }
 
-// R_0 from the caller's flags (a face is valid when its flag is not 0): a warp a word, lane
-// b reading face 32 wx + b (one 32-byte piece a warp), the word formed by a ballot.
+// R_0 from the caller's flags (a face is valid when its flag is not 0): a warp takes EXT_WW
+// consecutive words at a time, lane b reading face 32 wx + b of each (a 32-byte piece a word,
+// the EXT_WW loads in flight together), each word formed by a ballot.
+constexpr int EXT_WW = 8;
 __global__ void __launch_bounds__(TPB) k_extrap_flags(ExtBits E) {
     pdl_wait();
     pdl_trigger();
@@ -122,12 +124,21 @@ __global__ void __launch_bounds__(TPB) k_extrap_flags(ExtBits E) {
     uint32_t* R = pick3(ax, E.ra[0], E.ra[1], E.ra[2]);
     const int lane = threadIdx.x & 31;
     const unsigned warps = gridDim.x * (blockDim.x >> 5);
-    for (unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < A.nw; w += warps) {
-        const unsigned r = w / (unsigned)A.W;
-        const int i = 32 * (int)(w % (unsigned)A.W) + lane;
-        const bool f = i < A.a1 && fin[r * (unsigned)A.a1 + (unsigned)i] != 0;
-        const uint32_t m = __ballot_sync(0xffffffffu, f);
-        if (lane == 0) R[w] = m;
+    for (unsigned w0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * EXT_WW; w0 < A.nw;
+         w0 += warps * EXT_WW) {
+        bool f[EXT_WW];
+#pragma unroll
+        for (int q = 0; q < EXT_WW; q++) {
+            const unsigned w = w0 + q;
+            const unsigned r = w / (unsigned)A.W;
+            const int i = 32 * (int)(w - r * (unsigned)A.W) + lane;
+            f[q] = w < A.nw && i < A.a1 && fin[r * (unsigned)A.a1 + (unsigned)i] != 0;
+        }
+#pragma unroll
+        for (int q = 0; q < EXT_WW; q++) {
+            const uint32_t m = __ballot_sync(0xffffffffu, f[q]);
+            if (lane == q && w0 + q < A.nw) R[w0 + q] = m;
+        }
     }
 }
 
@@ -196,8 +207,9 @@ __global__ void __launch_bounds__(TPB) k_extrap_layer(ExtBits E, int from_a) {
 }
 
 // The last pass: zero every face not reached and every walled one, and write the reached
-// flags (unless keep_flags: no layer ran, and the flags stay as they are). A warp a mask
-// word, lane b on face 32 wx + b. `in_a`: the last layer's mask is ra (else rb).
+// flags (unless keep_flags: no layer ran, and the flags stay as they are). A warp takes
+// EXT_WW consecutive mask words at a time, lane b on face 32 wx + b of each. `in_a`: the last
+// layer's mask is ra (else rb).
 __global__ void __launch_bounds__(TPB) k_extrap_final(ExtBits E, int in_a, int keep_flags) {
     pdl_wait();
     pdl_trigger();
@@ -209,15 +221,27 @@ __global__ void __launch_bounds__(TPB) k_extrap_final(ExtBits E, int in_a, int k
     uint8_t* f = pick3(ax, E.f[0], E.f[1], E.f[2]);
     const int lane = threadIdx.x & 31;
     const unsigned warps = gridDim.x * (blockDim.x >> 5);
-    for (unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < A.nw; w += warps) {
-        const unsigned r = w / (unsigned)A.W;
-        const int i = 32 * (int)(w % (unsigned)A.W) + lane;
-        if (i >= A.a1) continue;
-        const bool reached = (R[w] >> lane) & 1u, open = (O[w] >> lane) & 1u;
-        const unsigned id = r * (unsigned)A.a1 + (unsigned)i;
-        // unreached_kernel!, then solidify! (a walled face is zero, reached or not)
-        if (!reached || !open) x[id] = 0.f;
-        if (!keep_flags) f[id] = reached ? 1 : 0;
+    for (unsigned w0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * EXT_WW; w0 < A.nw;
+         w0 += warps * EXT_WW) {
+        uint32_t rv[EXT_WW], ov[EXT_WW];
+#pragma unroll
+        for (int q = 0; q < EXT_WW; q++) {
+            const bool in = w0 + q < A.nw;
+            rv[q] = in ? R[w0 + q] : 0u;
+            ov[q] = in ? O[w0 + q] : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < EXT_WW; q++) {
+            const unsigned w = w0 + q;
+            const unsigned r = w / (unsigned)A.W;
+            const int i = 32 * (int)(w - r * (unsigned)A.W) + lane;
+            if (w >= A.nw || i >= A.a1) continue;
+            const bool reached = (rv[q] >> lane) & 1u, open = (ov[q] >> lane) & 1u;
+            const unsigned id = r * (unsigned)A.a1 + (unsigned)i;
+            // unreached_kernel!, then solidify! (a walled face is zero, reached or not)
+            if (!reached || !open) x[id] = 0.f;
+            if (!keep_flags) f[id] = reached ? 1 : 0;
+        }
     }
 }
 

@@ -166,17 +166,26 @@ __global__ void __launch_bounds__(TPB) k_reinit(Geo g, const float* __restrict__
                 v = found ? lowest : (cm > phimax ? phimax : (cm < -phimax ? -phimax : cm));
             } else {
                 const bool inside = cm < 0.0f;
-                bool frozen = false;
-                float ax = phimax, ay = phimax, az = phimax;
+                // far from the surface every open neighbour is at least phimax away on this
+                // cell's side: then nothing is frozen, ax = ay = az = phimax exactly, and the
+                // update is `far`, without the minimum chains below
+                bool fast = true;
 #pragma unroll
                 for (int e = 0; e < 6; e++)
-                    if (ok[e]) {
-                        if ((f[e] < 0.0f) != inside) frozen = true;
-                        const float d = fabsf(f[e]);
-                        if (e < 2) ax = jmin(ax, d);
-                        else if (e < 4) ay = jmin(ay, d);
-                        else az = jmin(az, d);
-                    }
+                    if (ok[e]) fast = fast && fabsf(f[e]) >= phimax && (f[e] < 0.0f) == inside;
+                bool frozen = false;
+                float ax = phimax, ay = phimax, az = phimax;
+                if (!fast) {
+#pragma unroll
+                    for (int e = 0; e < 6; e++)
+                        if (ok[e]) {
+                            if ((f[e] < 0.0f) != inside) frozen = true;
+                            const float d = fabsf(f[e]);
+                            if (e < 2) ax = jmin(ax, d);
+                            else if (e < 4) ay = jmin(ay, d);
+                            else az = jmin(az, d);
+                        }
+                }
                 if (frozen) {
                     v = cm;
                 } else {

@@ -242,6 +242,16 @@ __device__ __forceinline__ void rbgs_async_dev(Lev<typename Pr::M> L, int colour
     const int H = L.H, n1 = L.n1, n2 = L.n2;
     const int own = colour * H, oth = (1 - colour) * H;
     const M* dsrc = Pr::scaled ? L.di : L.dg;
+    // this lane's three x pieces, relative to the tile's corner: the same for every tile
+    int pj[3], pk[3], poff[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        int kk, jj, pc;
+        as_piece(lane + 32 * q, kk, jj, pc);
+        pj[q] = jj - 1;
+        pk[q] = kk - 1;
+        poff[q] = (pk[q] * n2 + pj[q]) * n1 + (pc - 1) * V8;
+    }
     auto issue = [&](int i) {
         const int s = i % AS_STAGES;
         const uint32_t tile = L.tiles[wg + i * stride];
@@ -254,16 +264,14 @@ __device__ __forceinline__ void rbgs_async_dev(Lev<typename Pr::M> L, int colour
             cp_async16(st + AS_PIECES * 16 + lane * 16, L.b + p);
             cp_async16(st + AS_PIECES * 16 + 512 + lane * 16, dsrc + p);
         }
+        const int tbase = (k0 * n2 + j0) * n1 + oth + h0;
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-            int kk, jj, pc;
-            as_piece(lane + 32 * q, kk, jj, pc);
-            const int jr = j0 - 1 + jj, kr = k0 - 1 + kk;
+            const int jr = j0 + pj[q], kr = k0 + pk[q];
             // rows past the level's last (a partial tile's) are read by no cell that updates;
             // skipping them keeps every copy inside the array and its one-plane guard
             if (jr > n2 || (kr == L.n3 && jr >= n2)) continue;
-            const int pos = (kr * n2 + jr) * n1 + oth + h0 + (pc - 1) * V8;
-            cp_async16(st + (lane + 32 * q) * 16, L.x + pos);
+            cp_async16(st + (lane + 32 * q) * 16, L.x + tbase + poff[q]);
         }
     };
 #pragma unroll
