@@ -19,7 +19,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libmpp.so")
 SOURCES = ["mpp.cu"]
-HEADERS = ["mpp_common.cuh", "mpp_base.cuh", "mpp_tiles.cuh", "mpp_stream.cuh", "mpp_tma.cuh", "mpp_fgmres.cuh", "mpp_adjoint.cuh", "mpp_advect.cuh", "mpp_cmg.cuh", "mpp_extrap.cuh", "mpp_levelset.cuh"]
+HEADERS = ["mpp_common.cuh", "mpp_base.cuh", "mpp_tiles.cuh", "mpp_stream.cuh", "mpp_tma.cuh", "mpp_fgmres.cuh", "mpp_adjoint.cuh", "mpp_advect.cuh", "mpp_cmg.cuh", "mpp_extrap.cuh", "mpp_levelset.cuh", "mpp_group.cuh"]
 
 
 def nvcc() -> str:

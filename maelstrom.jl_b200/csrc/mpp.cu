@@ -1779,7 +1779,7 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
             B.odc = take(Nl);
         }
         c->bot_smem = o;
-        c->restrict_smem = (size_t)restrict_smem_elems(msize(c->prec) == 2) * cs;
+        c->restrict_smem = (size_t)restrict_smem_bytes((int)msize(c->prec), (int)cs);
         int optin = 0;
         CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
         if (c->bot_smem > (size_t)optin) {

@@ -157,6 +157,21 @@ struct Lev {
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Asynchronous 16-byte copies global -> shared (cp.async, L2 only), committed and waited on
+// in groups. The zero-filling form copies `bytes` (0 or 16) and fills the rest with zeros.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async16(void* sm, const void* gm) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sm)), "l"(gm) : "memory");
+}
+__device__ __forceinline__ void cp_async16_zfill(void* sm, const void* gm, uint32_t bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(sm)), "l"(gm), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // A thread's slot in a tile (256 threads, one per slot): column h, row j, plane k offsets.
 // A warp covers TH consecutive columns of one row.
 __device__ __forceinline__ int slot_h() { return (int)threadIdx.x % TH; }

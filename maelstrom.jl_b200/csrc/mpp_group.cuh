@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(TPB) k_residual_g(const __grid_constant__ Grp<
     residual_body<Pr>(a.L);
 }
 template <class Pr>
-__global__ void __launch_bounds__(TPB, 4) k_restrict_g(const __grid_constant__ Grp<GLev2<typename Pr::M>> g, int start) {
+__global__ void __launch_bounds__(TPB, 3) k_restrict_g(const __grid_constant__ Grp<GLev2<typename Pr::M>> g, int start) {
     const auto& a = g.a[blockIdx.y];
     if (grp_skip(a.done)) return;
     pdl_trigger();

@@ -130,25 +130,15 @@ __global__ void __launch_bounds__(TPB) k_reinit(Geo g, const float* __restrict__
         }
         const float xl = i0 > 0 ? phi[base - 1] : 0.f;
         const float xr = i0 + W < n1 ? phi[base + W] : 0.f;
-        // Each cell is one of: a wall cell (the lowest open neighbour, or its own value
-        // clamped), a far cell (every open neighbour at least phimax away on its side: the
-        // update is `far`), or a near cell (the minimum chains and the eikonal). The cheap
-        // cases are formed first for the thread's cells; the costly parts run under branches
-        // that a warp takes only when one of its cells needs them (rows near the surface or
-        // along the wall), so the rest of the grid never executes them.
         float o[W];
         uint8_t ty[W];
-        bool solid[W], near[W], wall[W];
-        bool okm[W][6];
-        float fm[W][6];
-        bool any_near = false, any_wall = false;
 #pragma unroll
         for (int m = 0; m < W; m++) {
             const int i = i0 + m;
             const float cm = c[m];
             // neighbours in `neighbour`'s order (src/flip.jl:84-92): +x, -x, +y, -y, +z, -z
-            float* f = fm[m];
-            bool* ok = okm[m];
+            float f[6];
+            bool ok[6];
             f[0] = m + 1 < W ? c[m + 1 < W ? m + 1 : 0] : xr;
             f[1] = m > 0 ? c[m > 0 ? m - 1 : 0] : xl;
             f[2] = yp[m];
@@ -161,68 +151,43 @@ __global__ void __launch_bounds__(TPB) k_reinit(Geo g, const float* __restrict__
             ok[3] = ly && !(pxx[m + 1] + pyym > R2 || zs);
             ok[4] = hz && !(pxx[m + 1] + pyy > R2 || zsp);
             ok[5] = lz && !(pxx[m + 1] + pyy > R2 || zsm);
-            solid[m] = pxx[m + 1] + pyy > R2 || zs;
-            const bool inside = cm < 0.0f;
-            bool fast = true, anyok = false;
+            const bool solid = pxx[m + 1] + pyy > R2 || zs;
+            float v;
+            if (solid) {
+                // a wall cell takes the lowest value of the water next to it
+                float lowest = cm;
+                bool found = false;
 #pragma unroll
-            for (int e = 0; e < 6; e++) {
-                anyok = anyok || ok[e];
-                if (ok[e]) fast = fast && fabsf(f[e]) >= phimax && (f[e] < 0.0f) == inside;
-            }
-            wall[m] = solid[m] && anyok;
-            near[m] = !solid[m] && !fast;
-            any_near = any_near || near[m];
-            any_wall = any_wall || wall[m];
-            // the cheap results: a wall cell with no open neighbour, a far cell
-            o[m] = solid[m] ? (cm > phimax ? phimax : (cm < -phimax ? -phimax : cm)) : (inside ? -far : far);
-        }
-        const unsigned act = __activemask();
-        if (__any_sync(act, any_wall)) {
-#pragma unroll
-            for (int m = 0; m < W; m++)
-                if (wall[m]) {
-                    // a wall cell takes the lowest value of the water next to it
-                    float lowest = 0.f;
-                    bool found = false;
-#pragma unroll
-                    for (int e = 0; e < 6; e++)
-                        if (okm[m][e]) {
-                            lowest = found ? jmin(lowest, fm[m][e]) : fm[m][e];
-                            found = true;
-                        }
-                    o[m] = lowest;
-                }
-        }
-        if (__any_sync(act, any_near)) {
-#pragma unroll
-            for (int m = 0; m < W; m++)
-                if (near[m]) {
-                    const float cm = c[m];
-                    const bool inside = cm < 0.0f;
-                    bool frozen = false;
-                    float ax = phimax, ay = phimax, az = phimax;
-#pragma unroll
-                    for (int e = 0; e < 6; e++)
-                        if (okm[m][e]) {
-                            const float fe = fm[m][e];
-                            if ((fe < 0.0f) != inside) frozen = true;
-                            const float d = fabsf(fe);
-                            if (e < 2) ax = jmin(ax, d);
-                            else if (e < 4) ay = jmin(ay, d);
-                            else az = jmin(az, d);
-                        }
-                    if (frozen) {
-                        o[m] = cm;
-                    } else {
-                        const float d = (ax == phimax && ay == phimax && az == phimax)
-                                            ? far
-                                            : jmin(eikonal(ax, ay, az, h), phimax);
-                        o[m] = inside ? -d : d;
+                for (int e = 0; e < 6; e++)
+                    if (ok[e]) {
+                        lowest = found ? jmin(lowest, f[e]) : f[e];
+                        found = true;
                     }
-                }
-        }
+                v = found ? lowest : (cm > phimax ? phimax : (cm < -phimax ? -phimax : cm));
+            } else {
+                const bool inside = cm < 0.0f;
+                bool frozen = false;
+                float ax = phimax, ay = phimax, az = phimax;
 #pragma unroll
-        for (int m = 0; m < W; m++) ty[m] = solid[m] ? SOLID : (o[m] < 0.0f ? LIQUID : AIR);
+                for (int e = 0; e < 6; e++)
+                    if (ok[e]) {
+                        if ((f[e] < 0.0f) != inside) frozen = true;
+                        const float d = fabsf(f[e]);
+                        if (e < 2) ax = jmin(ax, d);
+                        else if (e < 4) ay = jmin(ay, d);
+                        else az = jmin(az, d);
+                    }
+                if (frozen) {
+                    v = cm;
+                } else {
+                    const float d = (ax == phimax && ay == phimax && az == phimax) ? far
+                                                                                  : jmin(eikonal(ax, ay, az, h), phimax);
+                    v = inside ? -d : d;
+                }
+            }
+            o[m] = v;
+            ty[m] = solid ? SOLID : (v < 0.0f ? LIQUID : AIR);
+        }
         if constexpr (W == 4) {
             *reinterpret_cast<float4*>(out + base) = make_float4(o[0], o[1], o[2], o[3]);
             if (types) *reinterpret_cast<uchar4*>(types + base) = make_uchar4(ty[0], ty[1], ty[2], ty[3]);

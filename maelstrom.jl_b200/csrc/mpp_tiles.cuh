@@ -112,8 +112,9 @@ __host__ __device__ constexpr C rw(int t) {
            ((((t >> 2) & 3) == 1 || ((t >> 2) & 3) == 2) ? (C)0.375f : (C)0.125f) *
            (((t >> 4) == 1 || (t >> 4) == 2) ? (C)0.375f : (C)0.125f);
 }
+template <int W>
 __host__ __device__ constexpr int roff(int t) {
-    return (((t >> 4) * RY + ((t >> 2) & 3)) * 2 + (((t & 3) + ((t >> 2) & 3) + (t >> 4)) & 1)) * R_W + ((t & 3) + 1) / 2;
+    return (((t >> 4) * RY + ((t >> 2) & 3)) * 2 + (((t & 3) + ((t >> 2) & 3) + (t >> 4)) & 1)) * W + ((t & 3) + 1) / 2;
 }
 
 // 16 bytes of elements of type M.
@@ -124,6 +125,84 @@ union Vec16 {
     __device__ Vec16() {}
 };
 
+// A tile's coarse cells from its staged region (rows W elements apart, the region's column 0
+// at sm): b = the weighted sum, and with `start` the level's x started from it.
+template <class Pr, int W, class S>
+__device__ __forceinline__ void restrict_cells(const Lev<typename Pr::M>& L, uint32_t tile, const S* sm, int start) {
+    using C = typename Pr::C;
+    using M = typename Pr::M;
+    const int lh = slot_h(), lj = slot_j(), lk = slot_k();
+    const int th = (int)(tile & 1023u), tj = (int)((tile >> 10) & 1023u), tk = (int)(tile >> 20);
+    const int h = th * TH + lh, J = tj * TY + lj, K = tk * TZ + lk;
+    if (h >= L.H || J >= L.n2 || K >= L.n3) return;
+    const int rb = (K * L.n2 + J) * L.n1;
+#pragma unroll
+    for (int cc = 0; cc < 2; cc++) {
+        const int p = rb + cc * L.H + h;
+        C v = (C)0;
+        if (L.code[p] & SELF) {
+            const S* base = sm + ((2 * lk * RY + 2 * lj) * 2) * W + 2 * lh + ci_of(cc, J, K);
+            C s = (C)0;
+#pragma unroll
+            for (int t = 0; t < 64; t++)  // c outer, a inner: the reference's order
+                s += rw<C>(t) * ld<C>(&base[roff<W>(t)]);
+            v = Pr::scaled ? s : (C)4 * s;
+        }
+        st(L.b + p, v);
+        if (start) {
+            // start_kernel! on the coarse level, fused: x = b / diag on its colour-0
+            // LIQUID cells (b as stored, in the level's element type), 0 elsewhere
+            C xv = (C)0;
+            if (cc == 0 && (L.code[p] & SELF)) {
+                M bm;
+                st(&bm, v);
+                const C bb = ld<C>(&bm), d = ld<C>((Pr::scaled ? L.di : L.dg) + p);
+                if constexpr (Pr::scaled) xv = bb * d;
+                else xv = d > (C)0 ? bb / d : (C)0;
+            }
+            st(L.x + p, xv);
+        }
+    }
+}
+
+// The staged region in 16-byte pieces of the fine level's r: per staged row NCH pieces from
+// the aligned column below hbase (2 TH th - 1), so element (row, hbase + off) sits at
+// row * RWP + CH - 1 + off. A piece lies wholly inside the row [0, H) or wholly outside it.
+template <class M>
+struct RPieces {
+    static constexpr int CH = 16 / (int)sizeof(M), NCH = (R_W + 2 * CH - 2) / CH + 1, RWP = NCH * CH,
+                         NV = R_ROWS * NCH, ELEMS = R_ROWS * RWP;
+};
+// A tile's staging copies (cp.async; pieces outside the level are zero-filled).
+template <class M>
+__device__ __forceinline__ void restrict_issue(const Lev<M>& F, uint32_t tile, M* stage) {
+    using RP = RPieces<M>;
+    const int th = (int)(tile & 1023u), tj = (int)((tile >> 10) & 1023u), tk = (int)(tile >> 20);
+    const int h8 = 2 * TH * th - RP::CH, j0 = 2 * TY * tj - 1, k0 = 2 * TZ * tk - 1;
+#pragma unroll
+    for (int e0 = 0; e0 < RP::NV; e0 += TPB) {
+        const int e = e0 + (int)threadIdx.x;
+        if (e < RP::NV) {
+            const int r = e / RP::NCH, ch = e - r * RP::NCH;
+            const int col = r & 1, jk = r >> 1, j = j0 + jk % RY, k = k0 + jk / RY, h = h8 + ch * RP::CH;
+            const bool in = j >= 0 && j < F.n2 && k >= 0 && k < F.n3 && h >= 0 && h < F.H;
+            cp_async16_zfill(stage + r * RP::RWP + ch * RP::CH, in ? F.r + (k * F.n2 + j) * F.n1 + col * F.H + h : F.r,
+                             in ? 16u : 0u);
+        }
+    }
+}
+
+// Shared memory of k_restrict in bytes: two stages of pieces and, for 16-bit storage, the
+// region widened to the arithmetic type (the 2- and 4-byte forms); or the region in the
+// arithmetic type (the 8-byte form, and levels whose rows are not whole pieces).
+__host__ __device__ constexpr int restrict_smem_bytes(int msize, int csize) {
+    const int region = R_ROWS * R_W * csize;
+    if (msize == 8) return region;
+    const int nch = (R_W + 2 * (16 / msize) - 2) / (16 / msize) + 1;
+    const int piped = 2 * R_ROWS * nch * 16 + (msize != csize ? region : 0);
+    return piped > region ? piped : region;
+}
+
 template <class Pr>
 __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typename Pr::M> L, int start) {
     using C = typename Pr::C;
@@ -131,9 +210,45 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
     C* sm = reinterpret_cast<C*>(smraw);
     using M = typename Pr::M;
     const int n = *L.count;
-    const int lh = slot_h(), lj = slot_j(), lk = slot_k();
     const bool vec = F.H % (16 / (int)sizeof(M)) == 0 && F.n1 % (16 / (int)sizeof(M)) == 0 &&
                      (reinterpret_cast<uintptr_t>(F.r) & 15) == 0;
+    if constexpr (sizeof(M) <= 4) {
+        if (vec) {
+            // Pipelined: a block's copies of its next tile's region go out before it sums
+            // this one (two stages), so the loads stay in flight while it computes.
+            using RP = RPieces<M>;
+            M* raw = reinterpret_cast<M*>(smraw);
+            C* cv = reinterpret_cast<C*>(smraw + 2 * RP::ELEMS * sizeof(M));
+            int t = blockIdx.x;
+            if (t < n) restrict_issue(F, L.tiles[t], raw);
+            cp_async_commit();
+            for (int i = 0; t < n; t += gridDim.x, i++) {
+                const uint32_t tile = L.tiles[t];
+                if (t + (int)gridDim.x < n) restrict_issue(F, L.tiles[t + gridDim.x], raw + ((i + 1) & 1) * RP::ELEMS);
+                cp_async_commit();
+                cp_async_wait<1>();
+                __syncthreads();
+                const M* cur = raw + (i & 1) * RP::ELEMS;
+                if constexpr (std::is_same<M, C>::value) {
+                    restrict_cells<Pr, RP::RWP>(L, tile, cur + (RP::CH - 1), start);
+                } else {
+                    // widened once an element (the sums read each one eight times)
+#pragma unroll
+                    for (int e0 = 0; e0 < R_ROWS * R_W; e0 += TPB) {
+                        const int e = e0 + (int)threadIdx.x;
+                        if (e < R_ROWS * R_W) {
+                            const int r = e / R_W, off = e - r * R_W;
+                            cv[e] = ld<C>(cur + r * RP::RWP + RP::CH - 1 + off);
+                        }
+                    }
+                    __syncthreads();
+                    restrict_cells<Pr, R_W>(L, tile, cv, start);
+                }
+                __syncthreads();  // this stage (and the widened region) free for reuse
+            }
+            return;
+        }
+    }
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
         const uint32_t tile = L.tiles[t];
         const int th = (int)(tile & 1023u), tj = (int)((tile >> 10) & 1023u), tk = (int)(tile >> 20);
@@ -198,43 +313,11 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
         }
         __syncthreads();
         }
-        const int h = th * TH + lh, J = tj * TY + lj, K = tk * TZ + lk;
-        if (h < L.H && J < L.n2 && K < L.n3) {
-            const int rb = (K * L.n2 + J) * L.n1;
-#pragma unroll
-            for (int cc = 0; cc < 2; cc++) {
-                const int p = rb + cc * L.H + h;
-                C v = (C)0;
-                if (L.code[p] & SELF) {
-                    const C* base = sm + ((2 * lk * RY + 2 * lj) * 2) * R_W + 2 * lh + ci_of(cc, J, K);
-                    C s = (C)0;
-#pragma unroll
-                    for (int t = 0; t < 64; t++)  // c outer, a inner: the reference's order
-                        s += rw<C>(t) * base[roff(t)];
-                    v = Pr::scaled ? s : (C)4 * s;
-                }
-                st(L.b + p, v);
-                if (start) {
-                    // start_kernel! on the coarse level, fused: x = b / diag on its colour-0
-                    // LIQUID cells (b as stored, in the level's element type), 0 elsewhere
-                    C xv = (C)0;
-                    if (cc == 0 && (L.code[p] & SELF)) {
-                        M bm;
-                        st(&bm, v);
-                        const C bb = ld<C>(&bm), d = ld<C>((Pr::scaled ? L.di : L.dg) + p);
-                        if constexpr (Pr::scaled) xv = bb * d;
-                        else xv = d > (C)0 ? bb / d : (C)0;
-                    }
-                    st(L.x + p, xv);
-                }
-            }
-        }
+        restrict_cells<Pr, R_W>(L, tile, sm, start);
     }
 }
-// Shared memory of k_restrict (elements of C): the staged rows.
-__host__ __device__ constexpr int restrict_smem_elems(bool) { return R_ROWS * R_W; }
 template <class Pr>
-__global__ void __launch_bounds__(TPB, 4) k_restrict(Lev<typename Pr::M> F, Lev<typename Pr::M> L, int start) {
+__global__ void __launch_bounds__(TPB, 3) k_restrict(Lev<typename Pr::M> F, Lev<typename Pr::M> L, int start) {
     pdl_wait();
     pdl_trigger();
     restrict_body<Pr>(F, L, start);

@@ -21,8 +21,6 @@
 
 namespace mpp {
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
@@ -197,14 +195,6 @@ constexpr int AS_PIECES = 96;  // x pieces a tile needs
 constexpr int AS_STAGE = AS_PIECES * 16 + 2 * 32 * 16;  // + b and 1/diag, a piece a lane
 constexpr int AS_SMEM = (TPB / 32) * AS_STAGES * AS_STAGE;
 
-__device__ __forceinline__ void cp_async16(void* sm, const void* gm) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sm)), "l"(gm) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 // The e-th of a tile's 96 x pieces (slot e of a stage), as (plane kk, row jj, piece pc)
 // around the tile (kk: planes k0-1 .. k0+2, jj: rows j0-1 .. j0+4, pc: pieces -1 .. 4): the
 // tile's own rows (e < 32, e = the lane that owns the piece: 16 (kk-1) + 4 (jj-1) + pc-1),
