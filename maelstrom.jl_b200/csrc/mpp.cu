@@ -241,12 +241,6 @@ int grid_tiles(const mpp_ctx* c, int l) {
     int cap = c->nsm * MAXBLOCKS_PER_SM;
     return g < cap ? (g > 0 ? g : 1) : cap;
 }
-// Block-per-tile kernels (the restriction).
-int grid_tiles1(const mpp_ctx* c, int l) {
-    int g = c->lv[l].ntiles;
-    int cap = c->nsm * MAXBLOCKS_PER_SM;
-    return g < cap ? (g > 0 ? g : 1) : cap;
-}
 
 // Kernel launches: programmatic dependent launch (see pdl_wait in mpp_common.cuh), so a
 // kernel's blocks can be scheduled while the previous kernel drains.
@@ -405,6 +399,24 @@ struct Run {
     bool vec(int l) const { return form(l) != MPP_SMOOTHER_COLUMN && c->lv[l].H % V8 == 0; }
     // a pipelined vector kernel's grid: the blocks resident at once (no second wave), at
     // most one warp per tile
+    // Block-per-tile kernels with dynamic shared memory (the restriction): a block a tile, at
+    // most the blocks resident at once, so each block streams its tiles through its copies.
+    int grid_blk(const void* kern, int l, size_t smem) const {
+        static std::mutex mu;
+        static std::vector<std::pair<const void*, int>> occ;
+        int nb = 0;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            for (auto& e : occ)
+                if (e.first == kern) nb = e.second;
+            if (nb == 0) {
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, TPB, smem) != cudaSuccess || nb < 1) nb = 1;
+                occ.emplace_back(kern, nb);
+            }
+        }
+        const int cap = c->nsm * nb, g = c->lv[l].ntiles;
+        return g < cap ? (g > 0 ? g : 1) : cap;
+    }
     int grid_res(const void* kern, int l) const {
         static std::mutex mu;
         static std::vector<std::pair<const void*, int>> occ;
@@ -576,7 +588,7 @@ struct Run {
             end();
             if (l + 1 < lb) {
                 beg(F_RESTRICT, l + 1);
-                launch(k_restrict<Pr>, grid_tiles1(c, l + 1), TPB, c->restrict_smem, s, view<M>(c, l), view<M>(c, l + 1),
+                launch(k_restrict<Pr>, grid_blk((const void*)k_restrict<Pr>, l + 1, c->restrict_smem), TPB, c->restrict_smem, s, view<M>(c, l), view<M>(c, l + 1),
                        l + 1 < ls ? 1 : 0);
                 end();
             }
@@ -815,7 +827,8 @@ struct GroupRun {
                 launch(k_residual_g<Pr>, g2(grid_tiles(c, l)), TPB, 0, s, lev(l));
             if (l + 1 < lb) {
                 nk++;
-                launch(k_restrict_g<Pr>, g2(grid_tiles1(c, l + 1)), TPB, c->restrict_smem, s, lev2(l, l + 1),
+                launch(k_restrict_g<Pr>, g2(run0.grid_blk((const void*)k_restrict_g<Pr>, l + 1, c->restrict_smem)), TPB,
+                       c->restrict_smem, s, lev2(l, l + 1),
                        l + 1 < ls ? 1 : 0);
             }
         }

@@ -931,29 +931,42 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
         pweights<C>(a.j, b0, wb0, b1, wb1);
         pweights<C>(a.k, k0, wc0, k1, wc1);
         b0 -= J0; b1 -= J0; k0 -= K0; k1 -= K0;
+        // prolongweights of i = 2 (h + q) + ci: coarse columns h + q - 1 + ci and the next,
+        // weights by the parity ci alone. The lane's cells of parity 0 (e0) and 1 (e1) are
+        // summed together, one staged row (B, K) at a time: the row's 10 columns the lane
+        // needs are read once into registers, and each cell takes its 8 terms (w_a w_b) w_c
+        // x in the reference's order (a fastest, then b, then c).
+        C e0[V8], e1[V8];
+#pragma unroll
+        for (int q = 0; q < V8; q++) e0[q] = e1[q] = (C)0;
+        const int lo = a.h - 1 - I0;  // the row's first column the lane reads
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int B = (r & 1) ? b1 : b0, K = (r & 2) ? k1 : k0;
+            const C wbc = ((r & 1) ? wb1 : wb0), wc = ((r & 2) ? wc1 : wc0);
+            // w_a w_b w_c for a = 0, 1 at parity 0 (w_a 1/4, 3/4) and parity 1 (3/4, 1/4)
+            const C wq = (C)0.25f * wbc * wc, w3 = (C)0.75f * wbc * wc;
+            const C* row = &S[K][B][lo];
+            C v[V8 + 2];
+#pragma unroll
+            for (int e = 0; e < V8 + 2; e++) v[e] = row[e];
+#pragma unroll
+            for (int q = 0; q < V8; q++) {
+                e0[q] += wq * v[q];
+                e0[q] += w3 * v[q + 1];
+                e1[q] += w3 * v[q + 1];
+                e1[q] += wq * v[q + 2];
+            }
+        }
 #pragma unroll
         for (int cc = 0; cc < 2; cc++) {
             const int p = a.rb + cc * L.H + a.h;
-            const int ci = ci_of(cc, a.j, a.k);
-            // prolongweights of i = 2 (h + q) + ci: coarse columns h + q - 1 + ci and the next,
-            // weights by the parity ci alone; the 8 products (w_a w_b) w_c are exact dyadic
-            // numbers, formed once for the lane's cells of this colour
-            const C wa0 = ci ? (C)0.75f : (C)0.25f, wa1 = ci ? (C)0.25f : (C)0.75f;
-            C wt[8];
-#pragma unroll
-            for (int m = 0; m < 8; m++)
-                wt[m] = ((m & 1) ? wa1 : wa0) * ((m & 2) ? wb1 : wb0) * ((m & 4) ? wc1 : wc0);
-            const int abase = a.h - 1 + ci - I0;
+            const bool odd = ci_of(cc, a.j, a.k) != 0;
 #pragma unroll
             for (int q = 0; q < V8; q++) {
                 const uint8_t cd = (uint8_t)(((q < 4 ? cdw[cc].x : cdw[cc].y) >> (8 * (q & 3))) & 0xffu);
                 if (!(cd & SELF)) continue;
-                C s = (C)0;
-#pragma unroll
-                for (int m = 0; m < 8; m++) {
-                    const int A = abase + q + (m & 1), B = (m & 2) ? b1 : b0, K = (m & 4) ? k1 : k0;
-                    s += wt[m] * S[K][B][A];
-                }
+                const C s = odd ? e1[q] : e0[q];
                 st(&xv[cc].v[q], addm(xv[cc].v[q], Pr::scaled ? (C)4 * s : s));
             }
             st8(L.x + p, xv[cc]);

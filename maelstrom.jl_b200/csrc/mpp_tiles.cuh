@@ -104,17 +104,12 @@ constexpr int RX = 4 * TH + 2, RY = 2 * TY + 2, RZ = 2 * TZ + 2;
 constexpr int R_W = 2 * TH + 2, R_ROWS = 2 * RY * RZ;  // staged columns per row, rows (x2 colours)
 
 // Term t = 16 c + 4 b + a of a coarse cell: weight w_a w_b w_c (exact dyadic constants,
-// associated as the reference's (w_a w_b) w_c) and its offset from the coarse cell's
-// first staged element.
+// associated as the reference's (w_a w_b) w_c).
 template <class C>
 __host__ __device__ constexpr C rw(int t) {
     return (((t & 3) == 1 || (t & 3) == 2) ? (C)0.375f : (C)0.125f) *
            ((((t >> 2) & 3) == 1 || ((t >> 2) & 3) == 2) ? (C)0.375f : (C)0.125f) *
            (((t >> 4) == 1 || (t >> 4) == 2) ? (C)0.375f : (C)0.125f);
-}
-template <int W>
-__host__ __device__ constexpr int roff(int t) {
-    return (((t >> 4) * RY + ((t >> 2) & 3)) * 2 + (((t & 3) + ((t >> 2) & 3) + (t >> 4)) & 1)) * W + ((t & 3) + 1) / 2;
 }
 
 // 16 bytes of elements of type M.
@@ -126,8 +121,14 @@ union Vec16 {
 };
 
 // A tile's coarse cells from its staged region (rows W elements apart, the region's column 0
-// at sm): b = the weighted sum, and with `start` the level's x started from it.
-template <class Pr, int W, class S>
+// at sm): b = the weighted sum, and with `start` the level's x started from it. A thread's
+// two cells are the natural columns 2h and 2h + 1 (one of each colour); per fine row (b, c)
+// they read three consecutive staged elements of each colour's row (the first cell's
+// a = 0, 2 and the second's a = 0, 2 from one; both cells' a = 1, 3 from the other), so
+// each staged element is read once a thread, and each cell's 64 terms are summed in the
+// reference's order (c outer, a inner). PAIR: rows and sm 8-byte aligned for S, so the
+// pairs are 8-byte loads.
+template <class Pr, int W, bool PAIR, class S>
 __device__ __forceinline__ void restrict_cells(const Lev<typename Pr::M>& L, uint32_t tile, const S* sm, int start) {
     using C = typename Pr::C;
     using M = typename Pr::M;
@@ -136,24 +137,46 @@ __device__ __forceinline__ void restrict_cells(const Lev<typename Pr::M>& L, uin
     const int h = th * TH + lh, J = tj * TY + lj, K = tk * TZ + lk;
     if (h >= L.H || J >= L.n2 || K >= L.n3) return;
     const int rb = (K * L.n2 + J) * L.n1;
+    C s0 = (C)0, s1 = (C)0;  // the cells at natural columns 2h and 2h + 1
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const S* ra = sm + (((2 * lk + c) * RY + 2 * lj + b) * 2 + ((b + c) & 1)) * W + 2 * lh;
+            const S* rq = sm + (((2 * lk + c) * RY + 2 * lj + b) * 2 + ((b + c + 1) & 1)) * W + 2 * lh;
+            C a0, a1, a2, q0, q1, q2;  // ra[0..2], rq[1..3]
+            if constexpr (PAIR) {
+                const auto pa = *reinterpret_cast<const typename std::conditional<sizeof(S) == 4, float2, double2>::type*>(ra);
+                const auto pq = *reinterpret_cast<const typename std::conditional<sizeof(S) == 4, float2, double2>::type*>(rq + 2);
+                a0 = (C)pa.x; a1 = (C)pa.y; a2 = ld<C>(ra + 2);
+                q0 = ld<C>(rq + 1); q1 = (C)pq.x; q2 = (C)pq.y;
+            } else {
+                a0 = ld<C>(ra); a1 = ld<C>(ra + 1); a2 = ld<C>(ra + 2);
+                q0 = ld<C>(rq + 1); q1 = ld<C>(rq + 2); q2 = ld<C>(rq + 3);
+            }
+            const int t = 16 * c + 4 * b;
+            s0 += rw<C>(t) * a0;
+            s0 += rw<C>(t + 1) * q0;
+            s0 += rw<C>(t + 2) * a1;
+            s0 += rw<C>(t + 3) * q1;
+            s1 += rw<C>(t) * a1;
+            s1 += rw<C>(t + 1) * q1;
+            s1 += rw<C>(t + 2) * a2;
+            s1 += rw<C>(t + 3) * q2;
+        }
+    }
 #pragma unroll
     for (int cc = 0; cc < 2; cc++) {
         const int p = rb + cc * L.H + h;
-        C v = (C)0;
-        if (L.code[p] & SELF) {
-            const S* base = sm + ((2 * lk * RY + 2 * lj) * 2) * W + 2 * lh + ci_of(cc, J, K);
-            C s = (C)0;
-#pragma unroll
-            for (int t = 0; t < 64; t++)  // c outer, a inner: the reference's order
-                s += rw<C>(t) * ld<C>(&base[roff<W>(t)]);
-            v = Pr::scaled ? s : (C)4 * s;
-        }
+        const bool liq = (L.code[p] & SELF) != 0;
+        const C sum = ci_of(cc, J, K) ? s1 : s0;
+        const C v = liq ? (Pr::scaled ? sum : (C)4 * sum) : (C)0;
         st(L.b + p, v);
         if (start) {
             // start_kernel! on the coarse level, fused: x = b / diag on its colour-0
             // LIQUID cells (b as stored, in the level's element type), 0 elsewhere
             C xv = (C)0;
-            if (cc == 0 && (L.code[p] & SELF)) {
+            if (cc == 0 && liq) {
                 M bm;
                 st(&bm, v);
                 const C bb = ld<C>(&bm), d = ld<C>((Pr::scaled ? L.di : L.dg) + p);
@@ -179,7 +202,7 @@ __device__ __forceinline__ void restrict_issue(const Lev<M>& F, uint32_t tile, M
     using RP = RPieces<M>;
     const int th = (int)(tile & 1023u), tj = (int)((tile >> 10) & 1023u), tk = (int)(tile >> 20);
     const int h8 = 2 * TH * th - RP::CH, j0 = 2 * TY * tj - 1, k0 = 2 * TZ * tk - 1;
-#pragma unroll
+#pragma unroll 2
     for (int e0 = 0; e0 < RP::NV; e0 += TPB) {
         const int e = e0 + (int)threadIdx.x;
         if (e < RP::NV) {
@@ -230,10 +253,10 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
                 __syncthreads();
                 const M* cur = raw + (i & 1) * RP::ELEMS;
                 if constexpr (std::is_same<M, C>::value) {
-                    restrict_cells<Pr, RP::RWP>(L, tile, cur + (RP::CH - 1), start);
+                    restrict_cells<Pr, RP::RWP, false>(L, tile, cur + (RP::CH - 1), start);
                 } else {
                     // widened once an element (the sums read each one eight times)
-#pragma unroll
+#pragma unroll 4
                     for (int e0 = 0; e0 < R_ROWS * R_W; e0 += TPB) {
                         const int e = e0 + (int)threadIdx.x;
                         if (e < R_ROWS * R_W) {
@@ -242,7 +265,7 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
                         }
                     }
                     __syncthreads();
-                    restrict_cells<Pr, R_W>(L, tile, cv, start);
+                    restrict_cells<Pr, R_W, true>(L, tile, cv, start);
                 }
                 __syncthreads();  // this stage (and the widened region) free for reuse
             }
@@ -256,8 +279,9 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
         __syncthreads();
         // Every non-LIQUID cell's r is zero (the residual pass writes zeros in active tiles
         // and the set-up clears the array each projection), so r is staged unmasked: all of
-        // a thread's loads go out at once, then land in shared memory.
-        if (vec) {
+        // a thread's loads go out at once, then land in shared memory. (The 2- and 4-byte
+        // forms come here only for rows that are not whole pieces.)
+        if (sizeof(M) == 8 && vec) {
             // 16-byte pieces: each staged row's columns from the aligned column below hbase,
             // a piece wholly inside the row [0, H) or wholly outside it (read as zeros)
             constexpr int CH = 16 / (int)sizeof(M), NCH = (R_W + 2 * CH - 2) / CH + 1;
@@ -313,7 +337,7 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
         }
         __syncthreads();
         }
-        restrict_cells<Pr, R_W>(L, tile, sm, start);
+        restrict_cells<Pr, R_W, true>(L, tile, sm, start);
     }
 }
 template <class Pr>
