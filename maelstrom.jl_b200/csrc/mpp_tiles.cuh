@@ -126,18 +126,21 @@ union Vec16 {
 // they read three consecutive staged elements of each colour's row (the first cell's
 // a = 0, 2 and the second's a = 0, 2 from one; both cells' a = 1, 3 from the other), so
 // each staged element is read once a thread, and each cell's 64 terms are summed in the
-// reference's order (c outer, a inner). PAIR: rows and sm 8-byte aligned for S, so the
-// pairs are 8-byte loads.
-template <class Pr, int W, bool PAIR, class S>
+// reference's order (c outer, a inner).
+// P: where the 8-byte-aligned pairs of S lie: 0 none (element loads), 1 from column 0 (sm
+// and W even), 2 from column 1 (sm odd, W even).
+template <class Pr, int W, int P, class S>
 __device__ __forceinline__ void restrict_cells(const Lev<typename Pr::M>& L, uint32_t tile, const S* sm, int start) {
     using C = typename Pr::C;
     using M = typename Pr::M;
+    using S2 = typename std::conditional<sizeof(S) == 4, float2, double2>::type;
     const int lh = slot_h(), lj = slot_j(), lk = slot_k();
     const int th = (int)(tile & 1023u), tj = (int)((tile >> 10) & 1023u), tk = (int)(tile >> 20);
     const int h = th * TH + lh, J = tj * TY + lj, K = tk * TZ + lk;
     if (h >= L.H || J >= L.n2 || K >= L.n3) return;
     const int rb = (K * L.n2 + J) * L.n1;
     C s0 = (C)0, s1 = (C)0;  // the cells at natural columns 2h and 2h + 1
+    auto term = [](C& acc, C w, C x) { acc += w * x; };
 #pragma unroll
     for (int c = 0; c < 4; c++) {
 #pragma unroll
@@ -145,24 +148,27 @@ __device__ __forceinline__ void restrict_cells(const Lev<typename Pr::M>& L, uin
             const S* ra = sm + (((2 * lk + c) * RY + 2 * lj + b) * 2 + ((b + c) & 1)) * W + 2 * lh;
             const S* rq = sm + (((2 * lk + c) * RY + 2 * lj + b) * 2 + ((b + c + 1) & 1)) * W + 2 * lh;
             C a0, a1, a2, q0, q1, q2;  // ra[0..2], rq[1..3]
-            if constexpr (PAIR) {
-                const auto pa = *reinterpret_cast<const typename std::conditional<sizeof(S) == 4, float2, double2>::type*>(ra);
-                const auto pq = *reinterpret_cast<const typename std::conditional<sizeof(S) == 4, float2, double2>::type*>(rq + 2);
+            if constexpr (P == 1) {
+                const S2 pa = *reinterpret_cast<const S2*>(ra), pq = *reinterpret_cast<const S2*>(rq + 2);
                 a0 = (C)pa.x; a1 = (C)pa.y; a2 = ld<C>(ra + 2);
                 q0 = ld<C>(rq + 1); q1 = (C)pq.x; q2 = (C)pq.y;
+            } else if constexpr (P == 2) {
+                const S2 pa = *reinterpret_cast<const S2*>(ra + 1), pq = *reinterpret_cast<const S2*>(rq + 1);
+                a0 = ld<C>(ra); a1 = (C)pa.x; a2 = (C)pa.y;
+                q0 = (C)pq.x; q1 = (C)pq.y; q2 = ld<C>(rq + 3);
             } else {
                 a0 = ld<C>(ra); a1 = ld<C>(ra + 1); a2 = ld<C>(ra + 2);
                 q0 = ld<C>(rq + 1); q1 = ld<C>(rq + 2); q2 = ld<C>(rq + 3);
             }
             const int t = 16 * c + 4 * b;
-            s0 += rw<C>(t) * a0;
-            s0 += rw<C>(t + 1) * q0;
-            s0 += rw<C>(t + 2) * a1;
-            s0 += rw<C>(t + 3) * q1;
-            s1 += rw<C>(t) * a1;
-            s1 += rw<C>(t + 1) * q1;
-            s1 += rw<C>(t + 2) * a2;
-            s1 += rw<C>(t + 3) * q2;
+            term(s0, rw<C>(t), a0);
+            term(s0, rw<C>(t + 1), q0);
+            term(s0, rw<C>(t + 2), a1);
+            term(s0, rw<C>(t + 3), q1);
+            term(s1, rw<C>(t), a1);
+            term(s1, rw<C>(t + 1), q1);
+            term(s1, rw<C>(t + 2), a2);
+            term(s1, rw<C>(t + 3), q2);
         }
     }
 #pragma unroll
@@ -215,14 +221,14 @@ __device__ __forceinline__ void restrict_issue(const Lev<M>& F, uint32_t tile, M
     }
 }
 
-// Shared memory of k_restrict in bytes: two stages of pieces and, for 16-bit storage, the
-// region widened to the arithmetic type (the 2- and 4-byte forms); or the region in the
+// Shared memory of k_restrict in bytes: the 4-byte form's two stages of pieces; the 16-bit
+// forms' one stage and its copy widened to the arithmetic type; the region in the
 // arithmetic type (the 8-byte form, and levels whose rows are not whole pieces).
 __host__ __device__ constexpr int restrict_smem_bytes(int msize, int csize) {
     const int region = R_ROWS * R_W * csize;
     if (msize == 8) return region;
-    const int nch = (R_W + 2 * (16 / msize) - 2) / (16 / msize) + 1;
-    const int piped = 2 * R_ROWS * nch * 16 + (msize != csize ? region : 0);
+    const int stage = R_ROWS * ((R_W + 2 * (16 / msize) - 2) / (16 / msize) + 1) * 16;  // bytes of pieces
+    const int piped = msize == csize ? 2 * stage : stage + stage / msize * csize;
     return piped > region ? piped : region;
 }
 
@@ -238,37 +244,52 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
     if constexpr (sizeof(M) <= 4) {
         if (vec) {
             // Pipelined: a block's copies of its next tile's region go out before it sums
-            // this one (two stages), so the loads stay in flight while it computes.
+            // this one, so the loads stay in flight while it computes.
             using RP = RPieces<M>;
             M* raw = reinterpret_cast<M*>(smraw);
-            C* cv = reinterpret_cast<C*>(smraw + 2 * RP::ELEMS * sizeof(M));
             int t = blockIdx.x;
             if (t < n) restrict_issue(F, L.tiles[t], raw);
             cp_async_commit();
-            for (int i = 0; t < n; t += gridDim.x, i++) {
-                const uint32_t tile = L.tiles[t];
-                if (t + (int)gridDim.x < n) restrict_issue(F, L.tiles[t + gridDim.x], raw + ((i + 1) & 1) * RP::ELEMS);
-                cp_async_commit();
-                cp_async_wait<1>();
-                __syncthreads();
-                const M* cur = raw + (i & 1) * RP::ELEMS;
-                if constexpr (std::is_same<M, C>::value) {
-                    restrict_cells<Pr, RP::RWP, false>(L, tile, cur + (RP::CH - 1), start);
-                } else {
-                    // widened once an element (the sums read each one eight times)
-#pragma unroll 4
-                    for (int e0 = 0; e0 < R_ROWS * R_W; e0 += TPB) {
+            if constexpr (std::is_same<M, C>::value) {
+                // two stages, summed where they land
+                for (int i = 0; t < n; t += gridDim.x, i++) {
+                    const uint32_t tile = L.tiles[t];
+                    if (t + (int)gridDim.x < n) restrict_issue(F, L.tiles[t + gridDim.x], raw + ((i + 1) & 1) * RP::ELEMS);
+                    cp_async_commit();
+                    cp_async_wait<1>();
+                    __syncthreads();
+                    restrict_cells<Pr, RP::RWP, 2>(L, tile, raw + (i & 1) * RP::ELEMS + (RP::CH - 1), start);
+                    __syncthreads();  // this stage free for the copies after next
+                }
+            } else {
+                // one stage, widened into a copy of the same layout (the sums read each
+                // element eight times), after which the next tile's copies reuse the stage
+                C* cv = reinterpret_cast<C*>(smraw + RP::ELEMS * sizeof(M));
+                for (; t < n; t += gridDim.x) {
+                    const uint32_t tile = L.tiles[t];
+                    cp_async_wait<0>();
+                    __syncthreads();
+#pragma unroll 2
+                    for (int e0 = 0; e0 < RP::NV; e0 += TPB) {
                         const int e = e0 + (int)threadIdx.x;
-                        if (e < R_ROWS * R_W) {
-                            const int r = e / R_W, off = e - r * R_W;
-                            cv[e] = ld<C>(cur + r * RP::RWP + RP::CH - 1 + off);
+                        if (e < RP::NV) {
+                            Vec16<M> w;
+                            w.u = *reinterpret_cast<const uint4*>(raw + e * RP::CH);
+                            C v[RP::CH];
+#pragma unroll
+                            for (int q = 0; q < RP::CH; q++) v[q] = ld<C>(&w.m[q]);
+#pragma unroll
+                            for (int q = 0; q < RP::CH; q += 4)
+                                *reinterpret_cast<float4*>(cv + e * RP::CH + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
                         }
                     }
                     __syncthreads();
-                    restrict_cells<Pr, R_W, true>(L, tile, cv, start);
+                    if (t + (int)gridDim.x < n) restrict_issue(F, L.tiles[t + gridDim.x], raw);
+                    cp_async_commit();
+                    restrict_cells<Pr, RP::RWP, 2>(L, tile, cv + (RP::CH - 1), start);
                 }
-                __syncthreads();  // this stage (and the widened region) free for reuse
             }
+            cp_async_wait<0>();
             return;
         }
     }
@@ -337,7 +358,7 @@ __device__ __forceinline__ void restrict_body(Lev<typename Pr::M> F, Lev<typenam
         }
         __syncthreads();
         }
-        restrict_cells<Pr, R_W, true>(L, tile, sm, start);
+        restrict_cells<Pr, R_W, 1>(L, tile, sm, start);
     }
 }
 template <class Pr>
