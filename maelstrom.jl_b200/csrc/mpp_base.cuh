@@ -310,7 +310,7 @@ __device__ __forceinline__ void st_piece(T* p, const T (&v)[N]) {  // N-element 
 // the finer-grained blocks fill more of each SM).
 constexpr int SETUP_V8_TPB = 128, SETUP_W = 4;
 template <class Pr, int W>
-__global__ void __launch_bounds__(SETUP_V8_TPB)
+__global__ void __launch_bounds__(SETUP_V8_TPB, 4)
     k_setup_v8(SetupIn<typename Pr::V> a, Lev<typename Pr::M> L, typename Pr::V* __restrict__ diag,
                typename Pr::V* __restrict__ b, typename Pr::V* __restrict__ r, Scalars* sc, double* partials,
                unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
@@ -326,9 +326,19 @@ __global__ void __launch_bounds__(SETUP_V8_TPB)
     const bool sep_b = (void*)L.b != (void*)r;
     double acc[3] = {0.0, 0.0, 0.0};
     const int nch = nq * n2 * n3;
-    for (int ch = (int)(blockIdx.x * SETUP_V8_TPB + threadIdx.x); ch < nch; ch += (int)(gridDim.x * SETUP_V8_TPB)) {
-        const int q8 = ch % nq, rw = ch / nq, j = rw % n2, k = rw / n2, i0 = W * q8;
-        const int row = rw * n1, idx0 = row + i0;
+    // the chunk's (q8, j, k), stepped by the grid stride's own (dq, dj, dk) with carries
+    // instead of divided out of the chunk index each step
+    const int ch0 = (int)(blockIdx.x * SETUP_V8_TPB + threadIdx.x), step = (int)(gridDim.x * SETUP_V8_TPB);
+    int qi = ch0 % nq, ji = (ch0 / nq) % n2, ki = ch0 / nq / n2;
+    const int dq = step % nq, dj = (step / nq) % n2, dk = step / nq / n2;
+    for (int ch = ch0; ch < nch; ch += step) {
+        const int q8 = qi, j = ji, k = ki, i0 = W * q8;
+        const int row = (j + n2 * k) * n1, idx0 = row + i0;
+        qi += dq;
+        ji += dj;
+        ki += dk;
+        if (qi >= nq) { qi -= nq; ji++; }
+        if (ji >= n2) { ji -= n2; ki++; }
         RowW<uint8_t, W> tc = ld_row<W>(a.types + idx0), tym, typ, tzm, tzp;
 #pragma unroll
         for (int m = 0; m < W; m++) tym.v[m] = typ.v[m] = tzm.v[m] = tzp.v[m] = SOLID;
@@ -362,6 +372,27 @@ __global__ void __launch_bounds__(SETUP_V8_TPB)
                 wlo = ld_row<W>(a.w + idx0);
                 whi = ld_row<W>(a.w + idx0 + sz);
             }
+            // the warm start's rows around the chunk (rows past the grid's are SOLID
+            // neighbours, never read) and the chunk's own level-set values
+            RowW<V, W> pc, pyp, pym, pzp, pzm;
+            V pxl = (V)0, pxr = (V)0;
+            RowW<float, W> phr;
+#pragma unroll
+            for (int m = 0; m < W; m++) {
+                pc.v[m] = pyp.v[m] = pym.v[m] = pzp.v[m] = pzm.v[m] = (V)0;
+                phr.v[m] = 0.f;
+            }
+            if (a.residual) {
+                pc = ld_row<W>(a.P + idx0);
+                if (j + 1 < n2) pyp = ld_row<W>(a.P + idx0 + n1);
+                if (j > 0) pym = ld_row<W>(a.P + idx0 - n1);
+                if (k + 1 < n3) pzp = ld_row<W>(a.P + idx0 + sz);
+                if (k > 0) pzm = ld_row<W>(a.P + idx0 - sz);
+                if (i0 > 0) pxl = a.P[idx0 - 1];
+                if (i0 + W < n1) pxr = a.P[idx0 + W];
+            }
+            if (a.phi) phr = ld_row<W>(a.phi + idx0);
+            bool at_edge = false;
 #pragma unroll
             for (int m = 0; m < W; m++) {
                 if (tc.v[m] != LIQUID) continue;
@@ -371,7 +402,7 @@ __global__ void __launch_bounds__(SETUP_V8_TPB)
                 const int off[6] = {1, -1, n1, -n1, sz, -sz};
                 C dd = (C)0;
                 uint8_t cd = 0;
-                const C phc = a.phi ? (C)a.phi[idx] : (C)0;
+                const C phc = (C)phr.v[m];
 #pragma unroll
                 for (int n = 0; n < 6; n++) {
                     if (tn[n] == LIQUID) {
@@ -398,16 +429,20 @@ __global__ void __launch_bounds__(SETUP_V8_TPB)
                 }
                 bv[m] = bb;
                 if (a.residual) {
+                    const V pn[6] = {m < W - 1 ? pc.v[m < W - 1 ? m + 1 : 0] : pxr, m > 0 ? pc.v[m > 0 ? m - 1 : 0] : pxl,
+                                     pyp.v[m], pym.v[m], pzp.v[m], pzm.v[m]};
                     C s = (C)0;
 #pragma unroll
                     for (int n = 0; n < 6; n++)
-                        if (cd & (1u << n)) s += (C)a.P[idx + off[n]];
-                    rv[m] = bb - (dd * (C)a.P[idx] - s);
+                        if (cd & (1u << n)) s += (C)pn[n];
+                    rv[m] = bb - (dd * (C)pc.v[m] - s);
                 }
-                L.tflag[L.tile_of(i, j, k)] = 1;
-                if (i == 0 || i == n1 - 1 || j == 0 || j == n2 - 1) atomicOr(L.edge, 1);
+                at_edge |= i == 0 || i == n1 - 1 || j == 0 || j == n2 - 1;
                 acc[2] += 1.0;
             }
+            // the chunk's cells share one tile (a tile row is 2 TH cells, W divides it)
+            L.tflag[L.tile_of(i0, j, k)] = 1;
+            if (at_edge) atomicOr(L.edge, 1);
         }
         if (a.clear_P) {
 #pragma unroll
@@ -548,7 +583,7 @@ __device__ __forceinline__ void restrict_bottom_body(Lev<typename Pr::M> F, Lev<
                         const C w = (a3 == 1 || a3 == 2 ? (C)0.375f : (C)0.125f) *
                                     (b3 == 1 || b3 == 2 ? (C)0.375f : (C)0.125f) *
                                     (c3 == 1 || c3 == 2 ? (C)0.375f : (C)0.125f);
-                        s += w * rv;
+                        s = macc<Pr::scaled>(s, w, rv);
                     }
             v = Pr::scaled ? s : (C)4 * s;
         }

@@ -338,8 +338,8 @@ __device__ __forceinline__ void cmg_residual(const CmgSlab& S, int q, int me, in
 // restrict_kernel! value of coarse cell (I, J, K) from fine slab F's r: the 64 terms
 // 16 c + 4 b + a in the reference's order, those outside the grid (zeros) left out. Fine
 // row (jf, kf) holds x = 2I-1+a at its colour (jf+kf)&1 half, position I-1, I, I, I+1 for
-// a = 0..3, alternating halves.
-template <class C, class M>
+// a = 0..3, alternating halves. Each term as macc<FUSE> rounds it.
+template <bool FUSE, class C, class M>
 __device__ __forceinline__ C cmg_restrict_cell(const CmgSlab& F, int I, int J, int K, int me) {
     C s = (C)0;
     const M* r0 = cmg_ptr<M>(F.orr);
@@ -366,7 +366,7 @@ __device__ __forceinline__ C cmg_restrict_cell(const CmgSlab& F, int I, int J, i
             for (int a3 = 0; a3 < 4; a3++) {
                 if (a3 == 0 && I == 0) continue;
                 if (a3 == 3 && I + 1 >= F.H) continue;
-                s += rw<C>(16 * c3 + 4 * b3 + a3) * ld<C>(&t[a3]);
+                s = macc<FUSE>(s, rw<C>(16 * c3 + 4 * b3 + a3), ld<C>(&t[a3]));
             }
         }
     }
@@ -390,7 +390,7 @@ __device__ __forceinline__ void cmg_restrict(const CmgSlab& F, const CmgSlab& Cs
         const int I = 2 * h + ((c + J + K + 1) & 1), e = (kk * Cs.n2 + J) * Cs.n1 + p;
         C v = (C)0;
         if (code[e] & SELF) {
-            const C s = cmg_restrict_cell<C, M>(F, I, J, K, me);
+            const C s = cmg_restrict_cell<Pr::scaled, C, M>(F, I, J, K, me);
             v = Pr::scaled ? s : (C)4 * s;
         }
         st(b + e, v);
@@ -409,7 +409,7 @@ __device__ __forceinline__ void cmg_restrict_bottom(const CmgSlab& F, const Lev<
         C v = (C)0;
         if (B.code[e] & SELF) {
             const int I = e % B.n1, JK = e / B.n1, J = JK % B.n2, K = JK / B.n2;
-            const C s = cmg_restrict_cell<C, M>(F, I, J, K, me);
+            const C s = cmg_restrict_cell<Pr::scaled, C, M>(F, I, J, K, me);
             v = Pr::scaled ? s : (C)4 * s;
         }
         out[e] = v;
@@ -485,7 +485,7 @@ __device__ __forceinline__ void cmg_prolong(const CmgSlab& F, int qf, const CmgS
                 const int A = (m & 1) ? a1 : a0, B = (m & 2) ? b1 : b0, Kc = (m & 4) ? c1 : c0;
                 if (A < 0 || A >= cn1 || B < 0 || B >= cn2 || Kc < 0 || Kc >= cn3) continue;  // a zero term
                 const C wa = (m & 1) ? wa1 : wa0, wb = (m & 2) ? wb1 : wb0, wc = (m & 4) ? wc1 : wc0;
-                s += wa * wb * wc * ld<C>(&cv[u][m]);
+                s = macc<Pr::scaled>(s, wa * wb * wc, ld<C>(&cv[u][m]));
             }
             st(x + e[u], ld<C>(&xv[u]) + (Pr::scaled ? (C)4 * s : s));
         }

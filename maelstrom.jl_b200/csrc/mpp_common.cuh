@@ -79,6 +79,16 @@ __device__ __forceinline__ void st(T* p, C v) {
     else *p = (T)v;
 }
 
+// acc + w x, a term of the V-cycle's transfer sums (restriction, prolongation): FUSE (the
+// 16-bit storage forms) rounds once (a fused multiply-add), otherwise the product and the
+// sum round separately, as in the reference's Float32 arithmetic. A zero term leaves acc
+// unchanged either way, so sums that leave out zero terms agree with ones that add them.
+template <bool FUSE, class C>
+__device__ __forceinline__ C macc(C acc, C w, C x) {
+    if constexpr (FUSE) return fmaf(w, x, acc);
+    else return acc + w * x;
+}
+
 // c + a for a stored value a and an arithmetic value c: for the 16-bit storage forms one
 // mixed-precision add (PTX add.rn.f32.f16 / .bf16: a is widened exactly inside the add,
 // which rounds once), the same bits as widening a first and adding in FP32, in one

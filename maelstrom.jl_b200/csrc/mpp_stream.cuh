@@ -935,7 +935,7 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
         // weights by the parity ci alone. The lane's cells of parity 0 (e0) and 1 (e1) are
         // summed together, one staged row (B, K) at a time: the row's 10 columns the lane
         // needs are read once into registers, and each cell takes its 8 terms (w_a w_b) w_c
-        // x in the reference's order (a fastest, then b, then c).
+        // x in the reference's order (a fastest, then b, then c), each as macc rounds it.
         C e0[V8], e1[V8];
 #pragma unroll
         for (int q = 0; q < V8; q++) e0[q] = e1[q] = (C)0;
@@ -952,10 +952,10 @@ __device__ __forceinline__ void prolong_v8_body(Lev<typename Pr::M> L, Lev<typen
             for (int e = 0; e < V8 + 2; e++) v[e] = row[e];
 #pragma unroll
             for (int q = 0; q < V8; q++) {
-                e0[q] += wq * v[q];
-                e0[q] += w3 * v[q + 1];
-                e1[q] += w3 * v[q + 1];
-                e1[q] += wq * v[q + 2];
+                e0[q] = macc<Pr::scaled>(e0[q], wq, v[q]);
+                e0[q] = macc<Pr::scaled>(e0[q], w3, v[q + 1]);
+                e1[q] = macc<Pr::scaled>(e1[q], w3, v[q + 1]);
+                e1[q] = macc<Pr::scaled>(e1[q], wq, v[q + 2]);
             }
         }
 #pragma unroll

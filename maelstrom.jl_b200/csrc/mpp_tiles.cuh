@@ -126,7 +126,7 @@ union Vec16 {
 // they read three consecutive staged elements of each colour's row (the first cell's
 // a = 0, 2 and the second's a = 0, 2 from one; both cells' a = 1, 3 from the other), so
 // each staged element is read once a thread, and each cell's 64 terms are summed in the
-// reference's order (c outer, a inner).
+// reference's order (c outer, a inner), each term as macc rounds it.
 // P: where the 8-byte-aligned pairs of S lie: 0 none (element loads), 1 from column 0 (sm
 // and W even), 2 from column 1 (sm odd, W even).
 template <class Pr, int W, int P, class S>
@@ -140,7 +140,7 @@ __device__ __forceinline__ void restrict_cells(const Lev<typename Pr::M>& L, uin
     if (h >= L.H || J >= L.n2 || K >= L.n3) return;
     const int rb = (K * L.n2 + J) * L.n1;
     C s0 = (C)0, s1 = (C)0;  // the cells at natural columns 2h and 2h + 1
-    auto term = [](C& acc, C w, C x) { acc += w * x; };
+    auto term = [](C& acc, C w, C x) { acc = macc<Pr::scaled>(acc, w, x); };
 #pragma unroll
     for (int c = 0; c < 4; c++) {
 #pragma unroll
@@ -457,7 +457,7 @@ __device__ __forceinline__ void prolong_body(Lev<typename Pr::M> L, Lev<typename
                         for (int m = 0; m < 8; m++) {
                             const int A = (m & 1) ? a1 : a0, B = (m & 2) ? b1 : b0, Kc = (m & 4) ? k1 : k0;
                             const C wa = (m & 1) ? wa1 : wa0, wb = (m & 2) ? wb1 : wb0, wc = (m & 4) ? wc1 : wc0;
-                            s += wa * wb * wc * sm[sub][Kc][B][A];
+                            s = macc<Pr::scaled>(s, wa * wb * wc, sm[sub][Kc][B][A]);
                         }
                         v[cc][q] = ld<C>(L.x + p) + (Pr::scaled ? (C)4 * s : s);
                     }
@@ -546,7 +546,8 @@ __device__ __forceinline__ void bottom_dev(const typename Pr::C* __restrict__ bi
                     for (int b3 = 0; b3 < 4; b3++)
 #pragma unroll
                         for (int a3 = 0; a3 < 4; a3++)
-                            s += wB<C>(a3) * wB<C>(b3) * wB<C>(c3) * getf(2 * I + a3 - 1, 2 * J + b3 - 1, 2 * K + c3 - 1);
+                            s = macc<Pr::scaled>(s, wB<C>(a3) * wB<C>(b3) * wB<C>(c3),
+                                                 getf(2 * I + a3 - 1, 2 * J + b3 - 1, 2 * K + c3 - 1));
                 v = (T2)(Pr::scaled ? s : (C)4 * s);
             }
             bout[c] = v;
@@ -709,7 +710,7 @@ __device__ __forceinline__ void bottom_dev(const typename Pr::C* __restrict__ bi
                 if (!(ccode[q] & SELF)) continue;
                 const C xc = coarsest ? (C)reinterpret_cast<const CC*>(smraw + Bc.ox)[q]
                                       : reinterpret_cast<const C*>(smraw + Bc.ox)[q];
-                s += wa * wb * wc * xc;
+                s = macc<Pr::scaled>(s, wa * wb * wc, xc);
             }
             x[c] = x[c] + (Pr::scaled ? (C)4 * s : s);
         }
