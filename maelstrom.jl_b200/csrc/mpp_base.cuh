@@ -119,10 +119,19 @@ __global__ void __launch_bounds__(TPB) k_volume(Geo g, const float* __restrict__
     pdl_trigger();
     double acc[1] = {0.0};
     if (g.n[0] % 8 == 0 && (reinterpret_cast<uintptr_t>(phi) & 15) == 0) {  // 8 cells of a row a thread
-        const int nq = g.n[0] / 8, nch = nq * g.n[1] * g.n[2];
-        for (int ch = (int)(blockIdx.x * TPB + threadIdx.x); ch < nch; ch += (int)(gridDim.x * TPB)) {
-            const int q8 = ch % nq, rw = ch / nq, j = rw % g.n[1], k = rw / g.n[1], i0 = 8 * q8;
-            const float4* p4 = reinterpret_cast<const float4*>(phi + (int64_t)rw * g.n[0] + i0);
+        const int nq = g.n[0] / 8, n2 = g.n[1], nch = nq * n2 * g.n[2];
+        // the chunk's (q8, j, k) stepped by the grid stride's own with carries
+        const int ch0 = (int)(blockIdx.x * TPB + threadIdx.x), step = (int)(gridDim.x * TPB);
+        int qi = ch0 % nq, ji = (ch0 / nq) % n2, ki = ch0 / nq / n2;
+        const int dq = step % nq, dj = (step / nq) % n2, dk = step / nq / n2;
+        for (int ch = ch0; ch < nch; ch += step) {
+            const int q8 = qi, j = ji, k = ki, i0 = 8 * q8;
+            qi += dq;
+            ji += dj;
+            ki += dk;
+            if (qi >= nq) { qi -= nq; ji++; }
+            if (ji >= n2) { ji -= n2; ki++; }
+            const float4* p4 = reinterpret_cast<const float4*>(phi + (int64_t)(j + n2 * k) * g.n[0] + i0);
             const float4 a = p4[0], b = p4[1];
             const float ph[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
@@ -678,9 +687,18 @@ __global__ void __launch_bounds__(TPB) k_gradient_v4(int n1, int n2, int n3, flo
     pdl_wait();
     pdl_trigger();
     const int nq = n1 / 4, sz = n1 * n2, nch = nq * n2 * n3;
-    for (int ch = (int)(blockIdx.x * TPB + threadIdx.x); ch < nch; ch += (int)(gridDim.x * TPB)) {
-        const int q4 = ch % nq, rw = ch / nq, j = rw % n2, k = rw / n2, i0 = 4 * q4;
-        const int c = rw * n1 + i0;  // the first cell
+    // the chunk's (q4, j, k) stepped by the grid stride's own with carries
+    const int ch0 = (int)(blockIdx.x * TPB + threadIdx.x), step = (int)(gridDim.x * TPB);
+    int qi = ch0 % nq, ji = (ch0 / nq) % n2, ki = ch0 / nq / n2;
+    const int dq = step % nq, dj = (step / nq) % n2, dk = step / nq / n2;
+    for (int ch = ch0; ch < nch; ch += step) {
+        const int q4 = qi, j = ji, k = ki, i0 = 4 * q4;
+        qi += dq;
+        ji += dj;
+        ki += dk;
+        if (qi >= nq) { qi -= nq; ji++; }
+        if (ji >= n2) { ji -= n2; ki++; }
+        const int c = (j + n2 * k) * n1 + i0;  // the first cell
         const uchar4 tc = *reinterpret_cast<const uchar4*>(types + c);
         const uint8_t t[4] = {tc.x, tc.y, tc.z, tc.w};
         const uint8_t tx = i0 > 0 ? types[c - 1] : (uint8_t)SOLID;
