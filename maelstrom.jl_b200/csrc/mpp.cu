@@ -258,6 +258,17 @@ void launch(void (*kern)(KArgs...), dim3 grid, int block, size_t smem, cudaStrea
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
+// A launch without programmatic dependent launch: the kernel starts after the previous
+// one has completed (for a kernel whose loads before its wait read what that one writes).
+template <typename... KArgs, typename... Args>
+void launch_serial(void (*kern)(KArgs...), dim3 grid, int block, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
 
 // A launch of one thread-block cluster of `cs` CTAs (k_cmg), with programmatic dependent
 // launch like the others.
@@ -560,8 +571,21 @@ struct Run {
         }
     }
 
-    // vcycle! (src/flip.jl:992-1014): z = M^-1 r from zero.
-    void vcycle() {
+    // start_kernel! on the fine level (the first colour's first sweep of a V-cycle). serial:
+    // it follows the tile lists' build (its tile ids load before its wait).
+    void start0(bool serial = false) {
+        beg(F_START, 0);
+        if (vec(0)) {
+            if (serial) launch_serial(k_start_v8<Pr>, grid_res((const void*)k_start_v8<Pr>, 0), TPB, 0, s, view<M>(c, 0));
+            else launch(k_start_v8<Pr>, grid_res((const void*)k_start_v8<Pr>, 0), TPB, 0, s, view<M>(c, 0));
+        } else {
+            launch(k_start<Pr>, grid_tiles(c, 0), TPB, 0, s, view<M>(c, 0));
+        }
+        end();
+    }
+    // vcycle! (src/flip.jl:992-1014): z = M^-1 r from zero. with_start = false: the fine
+    // level's start already ran (the CG loop's: after the set-up, and in the step).
+    void vcycle(bool with_start = true) {
         // sweeps of the fine level and of the coarser ones (the reference's one `sweeps`
         // unless sweeps_coarse is set)
         const int swf = c->opts.sweeps, sw = c->opts.sweeps_coarse > 0 ? c->opts.sweeps_coarse : swf;
@@ -575,13 +599,10 @@ struct Run {
         const int lb = c->lb;
         const int ls = c->cmg_ls > 0 ? c->cmg_ls : lb;  // levels ls .. lb-1 in the cluster
         for (int l = 0; l < ls; l++) {
-            if (l == 0) {  // the coarser levels' starts ride on the restriction into them
-                beg(F_START, l);
-                if (vec(l)) launch(k_start_v8<Pr>, grid_res((const void*)k_start_v8<Pr>, l), TPB, 0, s, view<M>(c, l));
-                else launch(k_start<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
-                end();
-            }
-            smooth(l, l == 0 ? down0 : down, l > 0);
+            if (l == 0 && with_start) start0();  // the coarser levels' starts ride on the restriction
+            // b of the level's first pass waits for the preceding kernel where that kernel wrote
+            // it: the restriction that started a coarse level, the step that started level 0
+            smooth(l, l == 0 ? down0 : down, l > 0 || !with_start);
             beg(F_RESID, l);
             if (vec(l)) launch(k_residual_v8<Pr>, grid_res((const void*)k_residual_v8<Pr>, l), TPB, 0, s, view<M>(c, l));
             else launch(k_residual<Pr>, grid_tiles(c, l), TPB, 0, s, view<M>(c, l));
@@ -635,8 +656,11 @@ struct Run {
 
     // One CG iteration, rotated so a loop of them is pressure!'s loop (src/flip.jl:1095-1108):
     // z = M^-1 r, rho/beta, q = A p and alpha, then the step and the exit test.
+    // The next V-cycle's fine start is part of the step: the vector step writes it (the b
+    // it has just formed, over the stored reciprocal diagonal or diagonal), otherwise the start
+    // kernel follows the step; the set-up is followed by one (record_prologue).
     void body(V* P, cudaGraphConditionalHandle cond, int use_cond) {
-        vcycle();
+        vcycle(false);
         const bool v = vec(0);
         beg(F_DOT, 0);
         if (v)
@@ -658,11 +682,12 @@ struct Run {
         // the vector step moves P in 16-element runs: it needs a 16-byte aligned P
         if (v && (reinterpret_cast<uintptr_t>(P) & 15) == 0)
             launch(k_advance_v8<Pr>, grid_w(0), TPB, 0, s, view<M>(c, 0), (V*)c->d, (const V*)c->q, (V*)c->r, P, c->sc,
-                                                        c->partials, cnt(CNT_ADVANCE), cond, use_cond);
+                                                        c->partials, cnt(CNT_ADVANCE), cond, use_cond, 1);
         else
             launch(k_advance<Pr>, grid_tiles(c, 0), TPB, 0, s, view<M>(c, 0), (V*)c->d, (const V*)c->q, (V*)c->r, P,
                                                             c->sc, c->partials, cnt(CNT_ADVANCE), cond, use_cond);
         end();
+        if (!(v && (reinterpret_cast<uintptr_t>(P) & 15) == 0)) start0();
     }
 
     void true_residual(const V* P) {
@@ -799,7 +824,15 @@ struct GroupRun {
         }
     }
 
-    void vcycle() {
+    void start0() {
+        const mpp_ctx* c = c0();
+        nk++;
+        if (run0.vec(0))
+            launch(k_start_v8_g<Pr>, g2(run0.grid_res((const void*)k_start_v8<Pr>, 0)), TPB, 0, s, lev(0));
+        else
+            launch(k_start_g<Pr>, g2(grid_tiles(c, 0)), TPB, 0, s, lev(0));
+    }
+    void vcycle(bool with_start = true) {
         const mpp_ctx* c = c0();
         const int swf = c->opts.sweeps, sw = c->opts.sweeps_coarse > 0 ? c->opts.sweeps_coarse : swf;
         std::vector<int> down, up, down0, up0;
@@ -812,14 +845,10 @@ struct GroupRun {
         const int lb = c->lb;
         const int ls = c->cmg_ls > 0 ? c->cmg_ls : lb;
         for (int l = 0; l < ls; l++) {
-            if (l == 0) {
-                nk++;
-                if (run0.vec(l))
-                    launch(k_start_v8_g<Pr>, g2(run0.grid_res((const void*)k_start_v8<Pr>, l)), TPB, 0, s, lev(l));
-                else
-                    launch(k_start_g<Pr>, g2(grid_tiles(c, l)), TPB, 0, s, lev(l));
-            }
-            smooth(l, l == 0 ? down0 : down, l > 0);
+            if (l == 0 && with_start) start0();
+            // b of the level's first pass waits for the preceding kernel where that kernel wrote
+            // it: the restriction that started a coarse level, the step that started level 0
+            smooth(l, l == 0 ? down0 : down, l > 0 || !with_start);
             nk++;
             if (run0.vec(l))
                 launch(k_residual_v8_g<Pr>, g2(run0.grid_res((const void*)k_residual_v8<Pr>, l)), TPB, 0, s, lev(l));
@@ -884,7 +913,7 @@ struct GroupRun {
     // Run<Pr>::body for the group, then the group's loop condition.
     void body(cudaGraphConditionalHandle cond) {
         const mpp_ctx* c = c0();
-        vcycle();
+        vcycle(false);
         const bool v = run0.vec(0);
         nk += 4;
         if (v) launch(k_dot_v8_g<Pr>, g2(run0.grid_res((const void*)k_dot_v8<Pr>, 0)), TPB, 0, s, cg_at(CNT_DOT));
@@ -893,8 +922,9 @@ struct GroupRun {
         else launch(k_search_g<Pr>, g2(grid_tiles(c, 0)), TPB, 0, s, cg_at(CNT_SEARCH));
         bool aligned = true;  // the vector step moves P in 16-element runs
         for (V* p : P) aligned = aligned && (reinterpret_cast<uintptr_t>(p) & 15) == 0;
-        if (v && aligned) launch(k_advance_v8_g<Pr>, g2(run0.grid_w(0)), TPB, 0, s, cg_at(CNT_ADVANCE));
+        if (v && aligned) launch(k_advance_v8_g<Pr>, g2(run0.grid_w(0)), TPB, 0, s, cg_at(CNT_ADVANCE), 1);
         else launch(k_advance_g<Pr>, g2(grid_tiles(c, 0)), TPB, 0, s, cg_at(CNT_ADVANCE));
+        if (!(v && aligned)) start0();
         Grp<const int*> d;
         memset(&d, 0, sizeof(d));
         for (int i = 0; i < nb(); i++) d.a[i] = done_of(cs[i]);
@@ -959,6 +989,7 @@ void record_prologue(Run<Pr>& run, const Call& k, cudaGraphConditionalHandle con
     if (k.kind == 1) run.volume(k.phi);
     if (std::is_same<typename Pr::V, double>::value) run.widen(k.P);
     run.setup(setup_in<Pr>(run.c, k), cond, use_cond);
+    run.start0(true);  // the first V-cycle's fine start (the loop's steps write the later ones)
 }
 
 template <class Pr>

@@ -178,9 +178,10 @@ __global__ void __launch_bounds__(TPB) k_search_g(const __grid_constant__ Grp<GC
     search_dev<Pr>(a.L, a.d, a.diag, a.q, a.sc, a.partials, a.counter);
 }
 template <class Pr>
-__global__ void __launch_bounds__(TPB, 3) k_advance_v8_g(const __grid_constant__ Grp<GCg<typename Pr::M, typename Pr::V>> g) {
+__global__ void __launch_bounds__(TPB, 3) k_advance_v8_g(const __grid_constant__ Grp<GCg<typename Pr::M, typename Pr::V>> g,
+                                                           int start) {
     const auto& a = g.a[blockIdx.y];
-    advance_v8_dev<Pr>(a.L, a.d, a.q, a.r, a.P, a.sc, a.partials, a.counter, cudaGraphConditionalHandle{}, 0);
+    advance_v8_dev<Pr>(a.L, a.d, a.q, a.r, a.P, a.sc, a.partials, a.counter, cudaGraphConditionalHandle{}, 0, start);
 }
 template <class Pr>
 __global__ void __launch_bounds__(TPB) k_advance_g(const __grid_constant__ Grp<GCg<typename Pr::M, typename Pr::V>> g) {

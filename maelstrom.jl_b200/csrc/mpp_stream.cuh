@@ -761,7 +761,7 @@ __global__ void __launch_bounds__(TPB, 2) k_search_v8(Lev<typename Pr::M> L, con
 template <class Pr>
 __device__ __forceinline__ void advance_v8_dev(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ qv,
                  typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
-                 unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
+                 unsigned* counter, cudaGraphConditionalHandle cond, int use_cond, int start) {
     using C = typename Pr::C;
     using M = typename Pr::M;
     using V = typename Pr::V;
@@ -821,6 +821,27 @@ __device__ __forceinline__ void advance_v8_dev(Lev<typename Pr::M> L, typename P
             st8(dvec + p, dd);
             st8(r + p, rr);
             if (sep_b) st8(L.b + p, rbv);
+            if (start) {
+                // the next V-cycle's start_kernel! (start_v8_body's arithmetic): x = b / diag
+                // on the first colour's LIQUID cells, b as this step stores it; 0 elsewhere
+                Vec8<M> xs;
+                if (cc == 0) {
+                    const Vec8<M> dv = ld8((Pr::scaled ? L.di : L.dg) + p);
+#pragma unroll
+                    for (int q = 0; q < V8; q++) {
+                        const C bq = sep_b ? ld<C>(&rbv.v[q]) : (C)rr.v[q];
+                        const C d = ld<C>(&dv.v[q]);
+                        C xq;
+                        if constexpr (Pr::scaled) xq = (cd[q] & SELF) ? bq * d : (C)0;
+                        else xq = ((cd[q] & SELF) && d > (C)0) ? bq / d : (C)0;
+                        st(&xs.v[q], xq);
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < V8; q++) st(&xs.v[q], (C)0);
+                }
+                st8(L.x + p, xs);
+            }
         }
         st8(P + pn, P0);
         st8(P + pn + V8, P1);
@@ -830,8 +851,8 @@ __device__ __forceinline__ void advance_v8_dev(Lev<typename Pr::M> L, typename P
 template <class Pr>
 __global__ void __launch_bounds__(TPB, 3) k_advance_v8(Lev<typename Pr::M> L, typename Pr::V* __restrict__ dvec, const typename Pr::V* __restrict__ qv,
                  typename Pr::V* __restrict__ r, typename Pr::V* __restrict__ P, Scalars* sc, double* partials,
-                 unsigned* counter, cudaGraphConditionalHandle cond, int use_cond) {
-    advance_v8_dev<Pr>(L, dvec, qv, r, P, sc, partials, counter, cond, use_cond);
+                 unsigned* counter, cudaGraphConditionalHandle cond, int use_cond, int start) {
+    advance_v8_dev<Pr>(L, dvec, qv, r, P, sc, partials, counter, cond, use_cond, start);
 }
 
 // prolong_kernel! (src/flip.jl:914-929), vector form: one warp per fine tile stages the
