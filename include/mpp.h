@@ -338,6 +338,134 @@ const char* mpp_last_error(void);
 /* Library version string. */
 const char* mpp_version(void);
 
+/* ==== The sparse two-resolution basin (SparseBasin, src/sflip.jl) ====
+ *
+ * Fine 16^3 blocks of cells dx wide where the surface is, over a dense coarse grid of
+ * cells 4 dx wide (nb blocks a side, 4 nb coarse cells), the pressure solved over both at
+ * once: the Losasso-coupled operator (1 between fine cells, 0.4 on each fine sub-face to
+ * a coarse cell, 4 between coarse cells, src/sflip.jl:1059-1074), Galerkin aggregation
+ * multigrid (fine blocks at 16^3 and 8^3 over the coarse grid, then the coarse grid and
+ * its halvings), damped Jacobi smoothing, flexible (Polak-Ribiere) PCG, and with
+ * `fallback` the CG -> FGMRES dispatch of src/fgmres.jl:96-110.
+ *
+ * Arrays are the SparseBasin's own device arrays, in the reference's layout:
+ *   slot:  int32 [nb0 nb1 nb2], the block's 1-based slot in the fine pools (0: coarse only)
+ *          (Topology.slot, src/sflip.jl:78-84)
+ *   where: int32 [3 x nslots], each slot's block (bi, bj, bk), -1s for a free slot
+ *   fine cell pools: [nslots x 4096] (cell i + 16 (j + 16 k) of a slot)
+ *   fine face pools: [nslots x 17*256] a axis (faceindex, src/sflip.jl:106-110)
+ *   coarse cells: column-major (4 nb0, 4 nb1, 4 nb2); coarse faces one longer along
+ *   their axis. Types are SOLID 0, LIQUID 1, AIR 2.
+ * The context owns the workspace for `capacity` slots (the pools' size); a call uses the
+ * first `nslots` of them. Calls on one context must not overlap on the GPU. */
+typedef struct mpp_sparse_ctx mpp_sparse_ctx;
+
+/* SparseGrid (src/sflip.jl:38-44) */
+typedef struct {
+    float lo[3];
+    float dx;
+    int32_t nb[3];
+    float radius;
+    float floor_z;
+} mpp_sparse_grid;
+
+/* The arrays project! reads and writes (Field.fine / Field.coarse pairs). */
+typedef struct {
+    const int32_t* slot;
+    const int32_t* where;
+    int32_t nslots;
+    const uint8_t* types_f;
+    const uint8_t* types_c;
+    const float* phi_f;
+    const float* phi_c;
+    float* P_f;
+    float* P_c;
+    float* u_f;
+    float* u_c;
+    float* v_f;
+    float* v_c;
+    float* w_f;
+    float* w_c;
+    uint8_t* fu_f;
+    uint8_t* fu_c;
+    uint8_t* fv_f;
+    uint8_t* fv_c;
+    uint8_t* fw_f;
+    uint8_t* fw_c;
+} mpp_sparse_basin;
+
+/* pressure!(::SparseBasin; tol, maxiter, sweeps, boost) (src/sflip.jl:1867) and the
+ * fallback dispatch (src/fgmres.jl:96: tol 5e-4, boost 1.5, maxiter 240). */
+typedef struct {
+    float tol;        /* relative residual (default 1e-4) */
+    int32_t maxiter;  /* CG iterations (default 200) */
+    int32_t sweeps;   /* damped Jacobi sweep pairs down and up (default 1) */
+    float boost;      /* coarse corrections' scale (default 1) */
+    int32_t coarse;   /* coarsest solve's sweeps each way (default 40) */
+    int32_t fallback; /* 1: CG capped at 80 iterations, then FGMRES (restart 8) on a missed tol */
+    int32_t graph;    /* 1: the CG loop is one CUDA graph launch with a device-side exit test */
+    int32_t cg_maxiter; /* with fallback: CG iterations before FGMRES (default 80, src/fgmres.jl:99) */
+} mpp_sparse_opts;
+
+typedef struct {
+    int32_t iterations;        /* what pressure! returns (CG + FGMRES iterations) */
+    int32_t fgmres_iterations;
+    int32_t status;            /* MPP_OK, MPP_NOT_CONVERGED, ... */
+    float rel_residual;        /* last residual / |b| */
+    float volume;              /* volume(s) at entry of project! (m^3) */
+    float gamma;               /* the volume-control divergence put into the rhs */
+    int64_t kernel_launches;
+} mpp_sparse_result;
+
+/* Workspace arrays mpp_sparse_read copies out (tests, debugging). */
+enum {
+    MPP_SP_CU_F = 0, MPP_SP_CV_F, MPP_SP_CW_F, /* level 0 fine face couplings */
+    MPP_SP_CU_C, MPP_SP_CV_C, MPP_SP_CW_C,     /* level 0 coarse face couplings */
+    MPP_SP_DD_F, MPP_SP_DD_C,                  /* level 0 Dirichlet diagonals */
+    MPP_SP_ACT_C,                              /* the coarse grid's activity (uint8) */
+    MPP_SP_C1X, MPP_SP_C1Y, MPP_SP_C1Z, MPP_SP_DD1, MPP_SP_ACT1, /* level 1 (8^3 blocks) */
+    MPP_SP_C2X, MPP_SP_C2Y, MPP_SP_C2Z, MPP_SP_DD2,             /* level 2 (the coarse grid) */
+    MPP_SP_NARRAYS
+};
+
+void mpp_sparse_opts_default(mpp_sparse_opts* opts);
+/* The dense levels of the hierarchy (the coarse grid halved while it has more than 1024
+ * cells and even sizes, src/sflip.jl:318-326); -1 if it does not halve to 1024 cells. */
+int32_t mpp_sparse_dense_levels(const int32_t nb[3]);
+/* Create a context with workspace for `capacity` slots (SparseBasin's `blocks`). */
+int mpp_sparse_ctx_create(mpp_sparse_ctx** out, const mpp_sparse_grid* grid, int32_t capacity);
+int mpp_sparse_ctx_destroy(mpp_sparse_ctx* ctx);
+size_t mpp_sparse_ctx_bytes(const mpp_sparse_ctx* ctx);
+/* volume(s) (src/sflip.jl:1990-1996), m^3. */
+int mpp_sparse_volume(mpp_sparse_ctx* ctx, const mpp_sparse_basin* b, double* volume, mpp_stream stream);
+/* coefficients! (src/sflip.jl:1437-1451) and hierarchy! (:1548-1573) into the context,
+ * from the basin's classes and level set: the operator mpp_sparse_apply and
+ * mpp_sparse_vcycle use. */
+int mpp_sparse_operator(mpp_sparse_ctx* ctx, const mpp_sparse_basin* b, mpp_stream stream);
+/* apply! (src/sflip.jl:1849-1855): q = A x with the context's operator. */
+int mpp_sparse_apply(mpp_sparse_ctx* ctx, const mpp_sparse_basin* b, const float* x_f, const float* x_c,
+                     float* q_f, float* q_c, mpp_stream stream);
+/* vcycle!(s, z, r; sweeps, coarse, boost) (src/sflip.jl:1722-1764) with the context's operator. */
+int mpp_sparse_vcycle(mpp_sparse_ctx* ctx, const mpp_sparse_basin* b, const float* r_f, const float* r_c,
+                      float* z_f, float* z_c, int32_t sweeps, int32_t coarse, float boost, mpp_stream stream);
+/* finerhs_kernel! + coarserhs_kernel! (src/sflip.jl:1409-1435) into b_f, b_c. */
+int mpp_sparse_rhs(mpp_sparse_ctx* ctx, const mpp_sparse_basin* b, float gamma, float* b_f, float* b_c,
+                   mpp_stream stream);
+/* pressure!(s) for the right-hand side (b_f, b_c): the operator from the basin's classes
+ * and level set, then the solve from the warm start in P (src/sflip.jl:1867-1904, or the
+ * fallback dispatch, src/fgmres.jl:96-110). Returns the status or an error. */
+int mpp_sparse_pressure(mpp_sparse_ctx* ctx, const mpp_sparse_basin* b, const float* b_f, const float* b_c,
+                        const mpp_sparse_opts* opts, mpp_sparse_result* res, mpp_stream stream);
+/* The velocity update and valid flags from P (projectfine_kernel!, projectcoarse_kernel!,
+ * restrict! of the faces and flags, src/sflip.jl:584-612, 1917-1962, 2010-2016). */
+int mpp_sparse_gradient(mpp_sparse_ctx* ctx, const mpp_sparse_basin* b, mpp_stream stream);
+/* project!(s::SparseBasin, dt; recover) (src/sflip.jl:1998-2018). Returns the status or an error. */
+int mpp_sparse_project(mpp_sparse_ctx* ctx, const mpp_sparse_basin* b, float volume0, double dt, double recover,
+                       const mpp_sparse_opts* opts, mpp_sparse_result* res, mpp_stream stream);
+/* Copy workspace array `which` (MPP_SP_*) of the current operator into dst (host or
+ * device memory, `bytes` at most); the array's size in bytes, or an error. */
+int64_t mpp_sparse_read(mpp_sparse_ctx* ctx, int32_t which, void* dst, size_t bytes, mpp_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,8 +18,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libmpp.so")
-SOURCES = ["mpp.cu"]
-HEADERS = ["mpp_common.cuh", "mpp_base.cuh", "mpp_tiles.cuh", "mpp_stream.cuh", "mpp_tma.cuh", "mpp_fgmres.cuh", "mpp_adjoint.cuh", "mpp_advect.cuh", "mpp_cmg.cuh", "mpp_extrap.cuh", "mpp_levelset.cuh", "mpp_group.cuh"]
+SOURCES = ["mpp.cu", "mpp_sparse.cu"]
+HEADERS = ["mpp_common.cuh", "mpp_base.cuh", "mpp_tiles.cuh", "mpp_stream.cuh", "mpp_tma.cuh", "mpp_fgmres.cuh", "mpp_adjoint.cuh", "mpp_advect.cuh", "mpp_cmg.cuh", "mpp_extrap.cuh", "mpp_levelset.cuh", "mpp_group.cuh", "mpp_sparse.cuh"]
 
 
 def nvcc() -> str:
@@ -31,7 +31,7 @@ def nvcc() -> str:
 
 def flags(verbose: bool = False) -> list:
     f = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
-         "-Xcompiler", "-fPIC,-O2", "-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+         "-Xcompiler", "-fPIC,-O2", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
     if verbose:
         f += ["-Xptxas", "-v"]
     return f
@@ -49,13 +49,26 @@ def build(verbose: bool = False, force: bool = False) -> str:
     if not force and not stale():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
+    # each translation unit compiles in its own nvcc process, in parallel; then one link
+    objs, procs = [], []
+    for src in SOURCES:
+        obj = os.path.join(LIBDIR, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc()] + flags(verbose) + ["-c", "-o", obj, os.path.join(CSRC, src)]
+        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+        objs.append(obj)
+    for cmd, p in procs:
+        out, err = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(f"nvcc failed ({p.returncode}):\n{' '.join(cmd)}\n{out}\n{err}")
+        if verbose:
+            sys.stderr.write(out + err)
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + flags(verbose) + ["-o", tmp] + [os.path.join(CSRC, s) for s in SOURCES]
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp] + objs
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({res.returncode}):\n{' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
-    if verbose:
-        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError(f"nvcc link failed ({res.returncode}):\n{' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+    for o in objs:
+        os.remove(o)
     os.replace(tmp, LIB)
     return LIB
 

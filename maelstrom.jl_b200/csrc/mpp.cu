@@ -1612,6 +1612,9 @@ int32_t mpp_levels_for(const int32_t n[3]) {
     return -1;
 }
 
+// The error text of the other translation units of the library (not exported).
+__attribute__((visibility("hidden"))) void mpp_internal_error(const char* msg) { set_err("%s", msg); }
+
 const char* mpp_last_error(void) { return g_err; }
 const char* mpp_version(void) { return "libmpp 0.1 (sm_100a)"; }
 

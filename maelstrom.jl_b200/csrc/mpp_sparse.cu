@@ -1,0 +1,1407 @@
+// libmpp, the sparse basin: host side. The context (workspace of one SparseBasin), the
+// launch sequences of coefficients!, hierarchy!, vcycle!, the flexible PCG and the FGMRES
+// fallback, and the mpp_sparse_* entry points of include/mpp.h.
+//
+// The CG loop keeps its scalars on the device (SpState): each reduction's last block forms
+// the next scalar and the exit test, so a solve is either a host loop that reads one word
+// per iteration or, with opts.graph, a CUDA graph whose conditional WHILE node runs the
+// rotated iteration (V-cycle, z.r and z.r_old -> beta, d = z + beta d, q = A d and d.q ->
+// alpha, the update and r.r -> exit test) until the update kernel clears the condition.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "mpp.h"
+#include "mpp_sparse.cuh"
+
+using namespace mpp;
+using namespace mpp::sp;
+
+extern "C" void mpp_internal_error(const char* msg);
+
+namespace {
+
+void sp_err(const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    mpp_internal_error(buf);
+}
+
+#define SCK(call)                                                                               \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
+            sp_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return MPP_ERR_CUDA;                                                                \
+        }                                                                                       \
+    } while (0)
+
+constexpr int SP_MAXD = 12;
+constexpr int SP_FGR = 8;  // FGMRES restart (src/fgmres.jl:26)
+enum { SCNT_START, SCNT_INIT, SCNT_DQ, SCNT_UPD, SCNT_DOT2, SCNT_VOL, SCNT_DOT, SCNT_N };
+
+template <typename... KArgs, typename... Args>
+void sp_launch(void (*kern)(KArgs...), dim3 grid, int block, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
+}  // namespace
+
+// ---- the CG kernels (src/sflip.jl:1766-1904) ----
+namespace mpp {
+namespace sp {
+
+// project!'s volume and gamma (src/sflip.jl:1976-2002): the liquid fractions of the fine
+// cells of slots in use and of the uncovered coarse cells, FP64 sums.
+__global__ void __launch_bounds__(SPT) k_sp_volume(Topo t, const float* phif, const float* phic, SpState* st,
+                                                   double* partials, unsigned* counter, int gf) {
+    pdl_wait();
+    pdl_trigger();
+    double acc[2] = {0.0, 0.0};
+    if ((int)blockIdx.x < gf) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS;
+        SP_FINE_LOOP(n, nf, gf) {
+            int sl, i, j, k;
+            pool_cell<16>(n, sl, i, j, k);
+            int w[3];
+            where_of(t, sl, w);
+            if (w[0] < 0) continue;
+            if (!issolid_fine(t, w[0] * BLOCK + i, w[1] * BLOCK + j, w[2] * BLOCK + k)) {
+                const float x = 0.5f - phif[n] / t.dx;
+                acc[0] += (double)(x > 1.0f ? 1.0f : (x < 0.0f ? 0.0f : x));
+            }
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        const float cdx = (float)RATIO * t.dx;
+        SP_COARSE_LOOP(c, nc, gf) {
+            int I, J, K;
+            coarse_cell(t, c, I, J, K);
+            if (covered(t, I, J, K) || issolid_coarse(t, I, J, K)) continue;
+            const float x = 0.5f - phic[c] / cdx;
+            acc[1] += (double)(64.0f * (x > 1.0f ? 1.0f : (x < 0.0f ? 0.0f : x)));
+        }
+    }
+    if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0) {
+        const float vol = ((float)acc[0] + (float)acc[1]) * (t.dx * t.dx * t.dx);
+        st->vol = vol;
+        const float loss = (st->volume0 - vol) / st->volume0;
+        const double lo = -0.01 / st->dt, hi = 0.01 / st->dt, x = (double)loss / st->recover;
+        st->gamma = (float)(x > hi ? hi : (x < lo ? lo : x));
+    }
+}
+
+// finerhs_kernel! + coarserhs_kernel! (src/sflip.jl:1409-1435) with clearfine_kernel! +
+// clearcoarse_kernel! (:1964-1974) on P; gamma from the state (project!) or given.
+__global__ void __launch_bounds__(SPT) k_sp_rhs(Topo t, const uint8_t* tf, const uint8_t* tc, const float* uf,
+                                                const float* vf, const float* wf, const float* uc, const float* vc,
+                                                const float* wc, float* bf, float* bc, float* Pf, float* Pc,
+                                                const SpState* st, float gamma_arg, int gf) {
+    pdl_wait();
+    pdl_trigger();
+    const float gamma = st ? st->gamma : gamma_arg;
+    const float h = t.dx;
+    if ((int)blockIdx.x < gf) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS;
+        SP_FINE_LOOP(n, nf, gf) {
+            int sl, i, j, k;
+            pool_cell<16>(n, sl, i, j, k);
+            if (!slot_used(t, sl)) continue;
+            float v = 0.0f;
+            if (tf[n] == LIQUID) {
+                float div = uf[L16::face(sl, 1, i + 1, j, k) - 1] - uf[L16::face(sl, 1, i, j, k) - 1];
+                div = div + vf[L16::face(sl, 2, i, j + 1, k) - 1];
+                div = div - vf[L16::face(sl, 2, i, j, k) - 1];
+                div = div + wf[L16::face(sl, 3, i, j, k + 1) - 1];
+                div = div - wf[L16::face(sl, 3, i, j, k) - 1];
+                v = (-h) * div + (gamma * h) * h;
+            } else if (Pf) {
+                Pf[n] = 0.0f;
+            }
+            bf[n] = v;
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        const int n1 = t.nc[0], n2 = t.nc[1];
+        SP_COARSE_LOOP(c, nc, gf) {
+            int I, J, K;
+            coarse_cell(t, c, I, J, K);
+            const bool cov = covered(t, I, J, K);
+            float v = 0.0f;
+            if (tc[c] == LIQUID && !cov) {
+                float div = uc[lin3(n1 + 1, n2, I + 1, J, K)] - uc[lin3(n1 + 1, n2, I, J, K)];
+                div = div + vc[lin3(n1, n2 + 1, I, J + 1, K)];
+                div = div - vc[lin3(n1, n2 + 1, I, J, K)];
+                div = div + wc[lin3(n1, n2, I, J, K + 1)];
+                div = div - wc[lin3(n1, n2, I, J, K)];
+                v = ((-16.0f) * h) * div + ((64.0f * gamma) * h) * h;
+            } else if (Pc) {
+                Pc[c] = 0.0f;
+            }
+            bc[c] = v;
+        }
+    }
+}
+
+// r = b - A P (apply! then xpby!(r, b, -1)), |b| and |r| (src/sflip.jl:1870-1877).
+__global__ void __launch_bounds__(SPT) k_sp_start(Topo t, Comp L, const uint8_t* tf, const uint8_t* tc, const float* Pf,
+                                                  const float* Pc, const float* bf, const float* bc, float* rf,
+                                                  float* rc, SpState* st, double* partials, unsigned* counter, int gf,
+                                                  cudaGraphConditionalHandle cond, int use_cond) {
+    pdl_wait();
+    pdl_trigger();
+    double acc[2] = {0.0, 0.0};
+    if ((int)blockIdx.x < gf) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS;
+        SP_FINE_LOOP(n, nf, gf) {
+            bool live;
+            const float q = apply_fine(t, L, tf, Pf, Pc, n, live);
+            if (!live) continue;
+            const float r = bf[n] + (-1.0f) * q;
+            rf[n] = r;
+            if (tf[n] == LIQUID) {
+                acc[0] += (double)bf[n] * (double)bf[n];
+                acc[1] += (double)r * (double)r;
+            }
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            bool cov;
+            const float q = apply_coarse(t, L, Pf, Pc, c, cov);
+            const float r = bc[c] + (-1.0f) * q;
+            rc[c] = r;
+            if (tc[c] == LIQUID && !cov) {
+                acc[0] += (double)bc[c] * (double)bc[c];
+                acc[1] += (double)r * (double)r;
+            }
+        }
+    }
+    if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0) {
+        const float bnorm = sqrtf((float)acc[0]);
+        st->bnorm = bnorm;
+        st->it = 0;
+        st->status = MPP_OK;
+        st->done = 0;
+        if (!isfinite(bnorm)) {
+            st->status = MPP_NONFINITE;
+            st->done = 1;
+        } else if (bnorm == 0.0f) {
+            st->done = 1;
+            st->rnorm = 0.0f;
+        } else {
+            st->target = st->tol * bnorm;
+            st->rnorm = sqrtf((float)acc[1]);
+            if (st->rnorm <= st->target) st->done = 1;
+        }
+        if (use_cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
+    }
+}
+
+// d = z and rho = z.r after the first V-cycle (src/sflip.jl:1879-1883).
+__global__ void __launch_bounds__(SPT) k_sp_dinit(Topo t, const uint8_t* tf, const uint8_t* tc, const float* zf,
+                                                  const float* zc, const float* rf, const float* rc, float* df,
+                                                  float* dc, SpState* st, double* partials, unsigned* counter, int gf,
+                                                  cudaGraphConditionalHandle cond, int use_cond) {
+    pdl_wait();
+    pdl_trigger();
+    if (st->done) return;
+    double acc[1] = {0.0};
+    if ((int)blockIdx.x < gf) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS;
+        SP_FINE_LOOP(n, nf, gf) {
+            if (!slot_used(t, (int)(n >> 12) + 1)) continue;
+            df[n] = zf[n];
+            if (tf[n] == LIQUID) acc[0] += (double)zf[n] * (double)rf[n];
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            dc[c] = zc[c];
+            if (coarse_unknown(t, tc, c)) acc[0] += (double)zc[c] * (double)rc[c];
+        }
+    }
+    if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
+        const float rho = (float)acc[0];
+        st->rho = rho;
+        if (!isfinite(rho)) {
+            st->status = MPP_NONFINITE;
+            st->done = 1;
+        } else if (!(rho > 0.0f)) {
+            st->status = MPP_INDEFINITE;
+            st->done = 1;
+        } else if (st->maxiter <= 0) {
+            st->status = MPP_NOT_CONVERGED;
+            st->done = 1;
+        }
+        if (use_cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
+    }
+}
+
+// q = A d and d.q -> alpha = rho / d.q (src/sflip.jl:1885-1889).
+__global__ void __launch_bounds__(SPT) k_sp_apply_dot(Topo t, Comp L, const uint8_t* tf, const uint8_t* tc,
+                                                      const float* df, const float* dc, float* qf, float* qc,
+                                                      SpState* st, double* partials, unsigned* counter, int gf) {
+    pdl_wait();
+    pdl_trigger();
+    if (st->done) return;
+    double acc[1] = {0.0};
+    if ((int)blockIdx.x < gf) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS;
+        SP_FINE_LOOP(n, nf, gf) {
+            bool live;
+            const float q = apply_fine(t, L, tf, df, dc, n, live);
+            if (!live) continue;
+            qf[n] = q;
+            if (tf[n] == LIQUID) acc[0] += (double)df[n] * (double)q;
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            bool cov;
+            const float q = apply_coarse(t, L, df, dc, c, cov);
+            qc[c] = q;
+            if (tc[c] == LIQUID && !cov) acc[0] += (double)dc[c] * (double)q;
+        }
+    }
+    if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
+        const float den = (float)acc[0];
+        st->den = den;
+        if (!(den > 0.0f)) {
+            st->status = MPP_INDEFINITE;
+            st->done = 1;
+        } else {
+            const float alpha = st->rho / den;
+            st->alpha = alpha;
+            if (!isfinite(alpha)) {
+                st->status = MPP_NONFINITE;
+                st->done = 1;
+            }
+        }
+    }
+}
+
+// P += alpha d; r_old = r; r -= alpha q; |r| and the exit test (src/sflip.jl:1890-1894).
+__global__ void __launch_bounds__(SPT) k_sp_update(Topo t, const uint8_t* tf, const uint8_t* tc, float* Pf, float* Pc,
+                                                   float* rf, float* rc, float* rof, float* roc, const float* df,
+                                                   const float* dc, const float* qf, const float* qc, SpState* st,
+                                                   double* partials, unsigned* counter, int gf,
+                                                   cudaGraphConditionalHandle cond, int use_cond) {
+    pdl_wait();
+    pdl_trigger();
+    if (st->done) {
+        if (use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
+        return;
+    }
+    const float alpha = st->alpha, ma = -alpha;
+    double acc[1] = {0.0};
+    if ((int)blockIdx.x < gf) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS;
+        SP_FINE_LOOP(n, nf, gf) {
+            if (!slot_used(t, (int)(n >> 12) + 1)) continue;
+            Pf[n] += alpha * df[n];
+            const float r0 = rf[n];
+            rof[n] = r0;
+            const float r = r0 + ma * qf[n];
+            rf[n] = r;
+            if (tf[n] == LIQUID) acc[0] += (double)r * (double)r;
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            Pc[c] += alpha * dc[c];
+            const float r0 = rc[c];
+            roc[c] = r0;
+            const float r = r0 + ma * qc[c];
+            rc[c] = r;
+            if (coarse_unknown(t, tc, c)) acc[0] += (double)r * (double)r;
+        }
+    }
+    if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
+        st->it += 1;
+        const float rnorm = sqrtf((float)acc[0]);
+        st->rnorm = rnorm;
+        if (rnorm <= st->target) {
+            st->done = 1;
+        } else if (st->it >= st->maxiter) {
+            st->status = MPP_NOT_CONVERGED;
+            st->done = 1;
+        }
+        if (use_cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
+    }
+}
+
+// rho_new = z.r and z.r_old -> beta = max(0, (rho_new - z.r_old) / rho) (src/sflip.jl:1895-1900).
+__global__ void __launch_bounds__(SPT) k_sp_dot2(Topo t, const uint8_t* tf, const uint8_t* tc, const float* zf,
+                                                 const float* zc, const float* rf, const float* rc, const float* rof,
+                                                 const float* roc, SpState* st, double* partials, unsigned* counter,
+                                                 int gf) {
+    pdl_wait();
+    pdl_trigger();
+    if (st->done) return;
+    double acc[2] = {0.0, 0.0};
+    if ((int)blockIdx.x < gf) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS;
+        SP_FINE_LOOP(n, nf, gf) {
+            if (!fine_unknown(t, tf, n)) continue;
+            acc[0] += (double)zf[n] * (double)rf[n];
+            acc[1] += (double)zf[n] * (double)rof[n];
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            if (!coarse_unknown(t, tc, c)) continue;
+            acc[0] += (double)zc[c] * (double)rc[c];
+            acc[1] += (double)zc[c] * (double)roc[c];
+        }
+    }
+    if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0) {
+        const float rnew = (float)acc[0];
+        if (!(rnew > 0.0f)) {
+            st->status = MPP_INDEFINITE;
+            st->done = 1;
+        } else {
+            float beta = (rnew - (float)acc[1]) / st->rho;
+            beta = beta != beta ? beta : (beta > 0.0f ? beta : 0.0f);  // Julia's max(0f0, x)
+            st->beta = beta;
+            if (!isfinite(beta)) {
+                st->status = MPP_NONFINITE;
+                st->done = 1;
+            }
+            st->rho = rnew;
+        }
+    }
+}
+
+// d = z + beta d (xpby!, src/sflip.jl:1902).
+__global__ void __launch_bounds__(SPT) k_sp_xpby(Topo t, float* df, float* dc, const float* zf, const float* zc,
+                                                 const SpState* st, int gf) {
+    pdl_wait();
+    pdl_trigger();
+    if (st->done) return;
+    const float beta = st->beta;
+    if ((int)blockIdx.x < gf) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS;
+        SP_FINE_LOOP(n, nf, gf) {
+            if (!slot_used(t, (int)(n >> 12) + 1)) continue;
+            df[n] = zf[n] + beta * df[n];
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) { dc[c] = zc[c] + beta * dc[c]; }
+    }
+}
+
+// ---- the FGMRES fallback's vector passes (src/fgmres.jl:26-92) ----
+// q = A x (apply!)
+__global__ void __launch_bounds__(SPT) k_sp_apply(Topo t, Comp L, const uint8_t* tf, const float* xf, const float* xc,
+                                                  float* qf, float* qc, int gf) {
+    pdl_wait();
+    pdl_trigger();
+    if ((int)blockIdx.x < gf) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS;
+        SP_FINE_LOOP(n, nf, gf) {
+            bool live;
+            const float q = apply_fine(t, L, tf, xf, xc, n, live);
+            if (live) qf[n] = q;
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            bool cov;
+            qc[c] = apply_coarse(t, L, xf, xc, c, cov);
+        }
+    }
+}
+// a.b over the unknowns (inner), FP64, into *out
+__global__ void __launch_bounds__(SPT) k_sp_dot(Topo t, const uint8_t* tf, const uint8_t* tc, const float* af,
+                                                const float* ac, const float* bf, const float* bc, double* out,
+                                                double* partials, unsigned* counter, int gf) {
+    pdl_wait();
+    pdl_trigger();
+    double acc[1] = {0.0};
+    if ((int)blockIdx.x < gf) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS;
+        SP_FINE_LOOP(n, nf, gf) {
+            if (fine_unknown(t, tf, n)) acc[0] += (double)af[n] * (double)bf[n];
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            if (coarse_unknown(t, tc, c)) acc[0] += (double)ac[c] * (double)bc[c];
+        }
+    }
+    if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) *out = acc[0];
+}
+// y = (zero ? 0 : y) + a x, or with `copy`, y = x (axpy!, copyfield!)
+__global__ void __launch_bounds__(SPT) k_sp_axpy(Topo t, float* yf, float* yc, float a, const float* xf,
+                                                 const float* xc, int zero, int copy, int gf) {
+    pdl_wait();
+    pdl_trigger();
+    if ((int)blockIdx.x < gf) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS;
+        SP_FINE_LOOP(n, nf, gf) {
+            if (!slot_used(t, (int)(n >> 12) + 1)) continue;
+            yf[n] = copy ? xf[n] : (zero ? 0.0f : yf[n]) + a * xf[n];
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) { yc[c] = copy ? xc[c] : (zero ? 0.0f : yc[c]) + a * xc[c]; }
+    }
+}
+
+// ---- the gradient (src/sflip.jl:1917-1962) and the face restriction (:597-611) ----
+// projectfine_kernel!, the three axes (blockIdx.y)
+__global__ void __launch_bounds__(SPT) k_sp_project_fine(Topo t, float* uf, float* vf, float* wf, uint8_t* fuf,
+                                                         uint8_t* fvf, uint8_t* fwf, const float* Pf, const float* Pc,
+                                                         const uint8_t* tf, const uint8_t* tc, const float* phif,
+                                                         const float* phic) {
+    pdl_wait();
+    pdl_trigger();
+    const int a = (int)blockIdx.y + 1, e0 = a == 1, e1 = a == 2, e2 = a == 3;
+    float* u = a == 1 ? uf : (a == 2 ? vf : wf);
+    uint8_t* fl = a == 1 ? fuf : (a == 2 ? fvf : fwf);
+    const float dx = t.dx;
+    const int64_t nf = (int64_t)t.nslots * BFACES;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += (int64_t)gridDim.x * blockDim.x) {
+        const int sl = (int)(n / BFACES) + 1, f = (int)(n - (int64_t)(sl - 1) * BFACES);
+        int w[3];
+        where_of(t, sl, w);
+        if (w[0] < 0) continue;
+        int i, j, k;
+        if (a == 1) { i = f % 17; const int r = f / 17; j = r & 15; k = r >> 4; }
+        else if (a == 2) { i = f & 15; const int r = f >> 4; j = r % 17; k = r / 17; }
+        else { i = f & 15; j = (f >> 4) & 15; k = f >> 8; }
+        const int I = w[0] * BLOCK + i, J = w[1] * BLOCK + j, K = w[2] * BLOCK + k;
+        bool fp, fm;
+        const uint8_t tp = celltype(t, tf, tc, I, J, K, fp);
+        const uint8_t tm = celltype(t, tf, tc, I - e0, J - e1, K - e2, fm);
+        const bool ok = tp != SOLID && tm != SOLID && (tp == LIQUID || tm == LIQUID);
+        if (ok) {
+            const float d = (fp && fm ? 1.0f : 2.5f) * dx;
+            const float Pp = fine_or_coarse(t, Pf, Pc, I, J, K);
+            const float Pm = fine_or_coarse(t, Pf, Pc, I - e0, J - e1, K - e2);
+            float D;
+            if (tp == LIQUID && tm == LIQUID) D = Pp - Pm;
+            else if (tm == LIQUID)
+                D = -Pm / theta<float>(fine_or_coarse(t, phif, phic, I - e0, J - e1, K - e2),
+                                       fine_or_coarse(t, phif, phic, I, J, K));
+            else
+                D = Pp / theta<float>(fine_or_coarse(t, phif, phic, I, J, K),
+                                      fine_or_coarse(t, phif, phic, I - e0, J - e1, K - e2));
+            u[n] -= D / d;
+        }
+        fl[n] = ok ? 1 : 0;
+    }
+}
+// projectcoarse_kernel! and restrictfaces_kernel! of the velocity and of its flags, the
+// three axes (blockIdx.y): the faces each writes are disjoint (projectcoarse: faces with no
+// fine block on either side; the restriction: faces whose 16 fine faces exist).
+__global__ void __launch_bounds__(SPT) k_sp_project_coarse(Topo t, float* uf, float* vf, float* wf, uint8_t* fuf,
+                                                           uint8_t* fvf, uint8_t* fwf, float* uc, float* vc, float* wc,
+                                                           uint8_t* fuc, uint8_t* fvc, uint8_t* fwc, const float* Pc,
+                                                           const uint8_t* tc, const float* phic) {
+    pdl_wait();
+    pdl_trigger();
+    const int a = (int)blockIdx.y + 1, e0 = a == 1, e1 = a == 2, e2 = a == 3;
+    const float* ufa = a == 1 ? uf : (a == 2 ? vf : wf);
+    const uint8_t* ffa = a == 1 ? fuf : (a == 2 ? fvf : fwf);
+    float* u = a == 1 ? uc : (a == 2 ? vc : wc);
+    uint8_t* fl = a == 1 ? fuc : (a == 2 ? fvc : fwc);
+    const int n1 = t.nc[0], n2 = t.nc[1], n3 = t.nc[2];
+    const int f0 = n1 + e0, f1 = n2 + e1, f2 = n3 + e2;
+    const float cdx = (float)RATIO * t.dx;
+    const int64_t nfc = (int64_t)f0 * f1 * f2;
+    for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < nfc; o += (int64_t)gridDim.x * blockDim.x) {
+        const int I = (int)(o % f0), J = (int)((o / f0) % f1), K = (int)(o / ((int64_t)f0 * f1));
+        const int Im = I - e0, Jm = J - e1, Km = K - e2;
+        const bool inside = 0 <= Im && 0 <= Jm && 0 <= Km && I < n1 && J < n2 && K < n3;
+        if (inside && !covered(t, I, J, K) && !covered(t, Im, Jm, Km)) {
+            const uint8_t tp = tc[lin(t.nc, I, J, K)], tm = tc[lin(t.nc, Im, Jm, Km)];
+            const bool ok = tp != SOLID && tm != SOLID && (tp == LIQUID || tm == LIQUID);
+            if (ok) {
+                const float Pp = Pc[lin(t.nc, I, J, K)], Pm = Pc[lin(t.nc, Im, Jm, Km)];
+                const float pp = phic[lin(t.nc, I, J, K)], pm = phic[lin(t.nc, Im, Jm, Km)];
+                const float D = (tp == LIQUID && tm == LIQUID)
+                                    ? Pp - Pm
+                                    : (tm == LIQUID ? -Pm / theta<float>(pm, pp) : Pp / theta<float>(pp, pm));
+                u[o] -= D / cdx;
+            }
+            fl[o] = ok ? 1 : 0;
+            continue;
+        }
+        if (!inside) fl[o] = 0;
+        float acc = 0.0f, accf = 0.0f;
+        int found = 0;
+        for (int q = 0; q < 4; q++)
+            for (int p = 0; p < 4; p++) {
+                const int FI = RATIO * I + (a == 1 ? 0 : p);
+                const int FJ = RATIO * J + (a == 1 ? p : (a == 2 ? 0 : q));
+                const int FK = RATIO * K + (a == 3 ? 0 : q);
+                const int64_t idx = finefaceat(t, a, FI, FJ, FK);
+                if (idx > 0) {
+                    acc += ufa[idx - 1];
+                    accf += (float)ffa[idx - 1];
+                    found++;
+                }
+            }
+        if (found == 16) {
+            u[o] = acc / 16.0f;
+            fl[o] = accf >= 16.0f - 0.5f ? 1 : 0;
+        }
+    }
+}
+
+}  // namespace sp
+}  // namespace mpp
+
+// ---- the context ----
+struct mpp_sparse_ctx {
+    Topo t;             // grid; slot/where/nslots set per call
+    int capacity;
+    int dev, nsm;
+    int nd;
+    DL D[SP_MAXD];      // D[0]: the coarse grid as level 2
+    int64_t ncc;
+    // level 0 operator
+    float *cf[3], *cc[3], *dDf, *dDc;
+    uint8_t* actc;      // = D[0].act
+    // level 1
+    float *c1[3], *dD1, *x1f, *b1f, *r1f, *t1f, *x1c, *r1c, *t1c;
+    uint8_t* act1;
+    // vectors (fine pool + coarse grid)
+    float *bf, *bc, *rf, *rc, *zf, *zc, *df, *dc, *qf, *qc, *rof, *roc, *tmf, *tmc, *res0f, *res0c;
+    // FGMRES basis (allocated on first use)
+    float *Vf[SP_FGR + 1], *Vc[SP_FGR + 1], *Zf[SP_FGR], *Zc[SP_FGR];
+    bool fg_alloc;
+    SpState* st;
+    SpState* st_host;
+    double* dres;       // dot results (FGMRES)
+    double* dres_host;
+    double* partials;
+    unsigned* counters;
+    std::vector<void*> allocs;
+    size_t bytes;
+    int64_t launches;
+    // a captured CG loop, keyed by the call's arrays and loop settings
+    cudaGraphExec_t gexec;
+    cudaGraph_t graph;
+    const void* gkey[12];
+    int gopt[4];
+    cudaStream_t cap;
+};
+
+namespace {
+
+int sp_alloc(mpp_sparse_ctx* c, void** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        sp_err("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        return MPP_ERR_NOMEM;
+    }
+    e = cudaMemset(*p, 0, bytes);
+    if (e != cudaSuccess) {
+        cudaFree(*p);
+        sp_err("cudaMemset failed: %s", cudaGetErrorString(e));
+        return MPP_ERR_CUDA;
+    }
+    c->allocs.push_back(*p);
+    c->bytes += bytes;
+    return MPP_OK;
+}
+template <class T>
+int sp_alloc_n(mpp_sparse_ctx* c, T** p, int64_t n) {
+    return sp_alloc(c, (void**)p, sizeof(T) * (size_t)n);
+}
+
+int64_t face_count(const int* n, int a) {
+    return (int64_t)(n[0] + (a == 1)) * (n[1] + (a == 2)) * (n[2] + (a == 3));
+}
+
+// grids of a fused fine + coarse launch: blocks for each part, each capped
+int cap_blocks(const mpp_sparse_ctx* c, int64_t n) {
+    const int64_t g = (n + SPT - 1) / SPT, cap = (int64_t)c->nsm * 8;
+    return (int)(g < 1 ? 1 : (g < cap ? g : cap));
+}
+struct Split {
+    int gf, g;
+};
+Split split_for(const mpp_sparse_ctx* c, int64_t nfine) {
+    Split s;
+    s.gf = cap_blocks(c, nfine);
+    s.g = s.gf + cap_blocks(c, c->ncc);
+    return s;
+}
+
+Comp comp0(const mpp_sparse_ctx* c, const uint8_t* tf) {
+    Comp L;
+    L.cfx = c->cf[0]; L.cfy = c->cf[1]; L.cfz = c->cf[2]; L.dDf = c->dDf; L.actf = tf;
+    L.ccx = c->cc[0]; L.ccy = c->cc[1]; L.ccz = c->cc[2]; L.dDc = c->dDc; L.actc = c->actc;
+    return L;
+}
+Comp comp1(const mpp_sparse_ctx* c) {
+    Comp L;
+    L.cfx = c->c1[0]; L.cfy = c->c1[1]; L.cfz = c->c1[2]; L.dDf = c->dD1; L.actf = c->act1;
+    L.ccx = c->cc[0]; L.ccy = c->cc[1]; L.ccz = c->cc[2]; L.dDc = c->dDc; L.actc = c->actc;
+    return L;
+}
+
+int sp_check_basin(mpp_sparse_ctx* c, const mpp_sparse_basin* b) {
+    if (!c || !b || !b->slot || !b->where || !b->types_f || !b->types_c) {
+        sp_err("null context or basin arrays");
+        return MPP_ERR_INVALID;
+    }
+    if (b->nslots < 0 || b->nslots > c->capacity) {
+        sp_err("nslots %d outside the context's capacity %d", b->nslots, c->capacity);
+        return MPP_ERR_INVALID;
+    }
+    c->t.slot = b->slot;
+    c->t.where = b->where;
+    c->t.nslots = b->nslots;
+    return MPP_OK;
+}
+
+// The launch sequences.
+struct SpRun {
+    mpp_sparse_ctx* c;
+    cudaStream_t s;
+    int64_t nk = 0;
+
+    int grid1(int64_t n) const { return cap_blocks(c, n); }
+
+    void operator_(const mpp_sparse_basin* b) {
+        const Topo& t = c->t;
+        const int64_t nff = (int64_t)t.nslots * BFACES;
+        sp_launch(k_sp_finecoef, dim3(grid1(nff), 3), SPT, s, t, c->cf[0], c->cf[1], c->cf[2], b->types_f, b->types_c);
+        int64_t mc = 0;
+        for (int a = 1; a <= 3; a++) mc = std::max(mc, face_count(t.nc, a));
+        sp_launch(k_sp_coarsecoef, dim3(grid1(mc), 3), SPT, s, t, c->cc[0], c->cc[1], c->cc[2], b->types_c);
+        const Split sp = split_for(c, (int64_t)t.nslots * BCELLS);
+        sp_launch(k_sp_dirichlet, dim3(sp.g), SPT, s, t, c->dDf, c->dDc, c->actc, b->types_f, b->types_c, b->phi_f,
+                  b->phi_c, sp.gf);
+        nk += 3;
+        hierarchy(b->types_f);
+    }
+    void hierarchy(const uint8_t* tf) {
+        const Topo& t = c->t;
+        sp_launch(k_sp_coef1, dim3(grid1((int64_t)t.nslots * BFACES1), 3), SPT, s, t, c->c1[0], c->c1[1], c->c1[2],
+                  (const float*)c->cf[0], (const float*)c->cf[1], (const float*)c->cf[2]);
+        sp_launch(k_sp_cells1, dim3(grid1((int64_t)t.nslots * BCELLS1)), SPT, s, t, c->dD1, c->act1,
+                  (const float*)c->dDf, tf);
+        int64_t mc = c->ncc;
+        for (int a = 1; a <= 3; a++) mc = std::max(mc, face_count(t.nc, a));
+        sp_launch(k_sp_level2, dim3(grid1(mc), 4), SPT, s, t, c->D[0].cx, c->D[0].cy, c->D[0].cz,
+                  (const float*)c->cc[0], (const float*)c->cc[1], (const float*)c->cc[2], (const float*)c->c1[0],
+                  (const float*)c->c1[1], (const float*)c->c1[2], c->D[0].dD, c->D[0].act, (const float*)c->dDc,
+                  (const float*)c->dD1, (const uint8_t*)c->act1);
+        nk += 3;
+        for (int l = 1; l < c->nd; l++) {
+            int64_t m = (int64_t)c->D[l].n[0] * c->D[l].n[1] * c->D[l].n[2];
+            for (int a = 1; a <= 3; a++) m = std::max(m, face_count(c->D[l].n, a));
+            sp_launch(k_sp_dense_level, dim3(grid1(m), 4), SPT, s, c->D[l - 1], c->D[l]);
+            nk++;
+        }
+    }
+    // smooth! (src/sflip.jl:1292-1303) after zero!(x): the first sweep from zeros
+    template <int N>
+    void smooth(const Comp& L, float* xf, float* xc, const float* bf, const float* bc, float* tf_, float* tc_,
+                int sweeps, bool from_zero) {
+        const Split sp = split_for(c, (int64_t)c->t.nslots * Lv<N>::CELLS);
+        for (int q = 0; q < sweeps; q++) {
+            if (q == 0 && from_zero)
+                sp_launch(k_sp_jacobi<N, true>, dim3(sp.g), SPT, s, c->t, L, tf_, tc_, (const float*)xf,
+                          (const float*)xc, bf, bc, sp.gf);
+            else
+                sp_launch(k_sp_jacobi<N, false>, dim3(sp.g), SPT, s, c->t, L, tf_, tc_, (const float*)xf,
+                          (const float*)xc, bf, bc, sp.gf);
+            sp_launch(k_sp_jacobi<N, false>, dim3(sp.g), SPT, s, c->t, L, xf, xc, (const float*)tf_, (const float*)tc_,
+                      bf, bc, sp.gf);
+            nk += 2;
+        }
+    }
+    void dense_smooth(int l, int sweeps, bool from_zero) {
+        DL& D = c->D[l];
+        const int g = grid1((int64_t)D.n[0] * D.n[1] * D.n[2]);
+        for (int q = 0; q < sweeps; q++) {
+            if (q == 0 && from_zero) sp_launch(k_sp_djacobi<true>, dim3(g), SPT, s, D, D.t, (const float*)D.x);
+            else sp_launch(k_sp_djacobi<false>, dim3(g), SPT, s, D, D.t, (const float*)D.x);
+            sp_launch(k_sp_djacobi<false>, dim3(g), SPT, s, D, D.x, (const float*)D.t);
+            nk += 2;
+        }
+    }
+    // vcycle! (src/sflip.jl:1722-1764): z = M^-1 r
+    void vcycle(const uint8_t* tf, float* zf, float* zc, const float* rf, const float* rc, int sweeps, int coarse,
+                float boost) {
+        const Topo& t = c->t;
+        const Comp L0 = comp0(c, tf), L1 = comp1(c);
+        const Split s0 = split_for(c, (int64_t)t.nslots * BCELLS), s1 = split_for(c, (int64_t)t.nslots * BCELLS1);
+        smooth<16>(L0, zf, zc, rf, rc, c->tmf, c->tmc, sweeps, true);
+        sp_launch(k_sp_residual<16>, dim3(s0.g), SPT, s, t, L0, c->res0f, c->res0c, (const float*)zf,
+                  (const float*)zc, rf, rc, s0.gf);
+        sp_launch(k_sp_restrict01, dim3(grid1((int64_t)t.nslots * BCELLS1)), SPT, s, t, c->b1f,
+                  (const float*)c->res0f);
+        nk += 2;
+        // level 1's coarse right-hand side is level 0's coarse residual (copyto!, :1730)
+        smooth<8>(L1, c->x1f, c->x1c, c->b1f, c->res0c, c->t1f, c->t1c, sweeps, true);
+        sp_launch(k_sp_residual<8>, dim3(s1.g), SPT, s, t, L1, c->r1f, c->r1c, (const float*)c->x1f,
+                  (const float*)c->x1c, (const float*)c->b1f, (const float*)c->res0c, s1.gf);
+        sp_launch(k_sp_restrict12, dim3(grid1(c->ncc)), SPT, s, t, c->D[0].b, (const float*)c->r1f,
+                  (const float*)c->r1c);
+        nk += 2;
+        for (int l = 0; l + 1 < c->nd; l++) {
+            dense_smooth(l, sweeps, true);
+            const int g = grid1((int64_t)c->D[l].n[0] * c->D[l].n[1] * c->D[l].n[2]);
+            sp_launch(k_sp_dresidual, dim3(g), SPT, s, c->D[l]);
+            sp_launch(k_sp_drestrict, dim3(grid1((int64_t)c->D[l + 1].n[0] * c->D[l + 1].n[1] * c->D[l + 1].n[2])),
+                      SPT, s, c->D[l], c->D[l + 1]);
+            nk += 2;
+        }
+        sp_launch(k_sp_coarsest, dim3(1), 1024, s, c->D[c->nd - 1], coarse);
+        nk++;
+        for (int l = c->nd - 2; l >= 0; l--) {
+            const int g = grid1((int64_t)c->D[l].n[0] * c->D[l].n[1] * c->D[l].n[2]);
+            sp_launch(k_sp_dprolong, dim3(g), SPT, s, c->D[l], c->D[l + 1], boost);
+            nk++;
+            dense_smooth(l, sweeps, false);
+        }
+        sp_launch(k_sp_prolong<8>, dim3(s1.g), SPT, s, t, c->x1f, c->x1c, (const float*)nullptr,
+                  (const float*)c->D[0].x, (const uint8_t*)c->act1, (const uint8_t*)c->actc, boost, s1.gf);
+        nk++;
+        smooth<8>(L1, c->x1f, c->x1c, c->b1f, c->res0c, c->t1f, c->t1c, sweeps, false);
+        sp_launch(k_sp_prolong<16>, dim3(s0.g), SPT, s, t, zf, zc, (const float*)c->x1f, (const float*)c->x1c, tf,
+                  (const uint8_t*)c->actc, boost, s0.gf);
+        nk++;
+        smooth<16>(L0, zf, zc, rf, rc, c->tmf, c->tmc, sweeps, false);
+    }
+    // the CG's prologue up to the loop: r, the norms, the first V-cycle, d and rho, and
+    // the first iteration's q, alpha and update (the rotated loop's body starts with the
+    // V-cycle of the next iteration)
+    void cg_prologue(const mpp_sparse_basin* b, const mpp_sparse_opts* o, cudaGraphConditionalHandle cond,
+                     int use_cond) {
+        const Topo& t = c->t;
+        const Comp L0 = comp0(c, b->types_f);
+        const Split s0 = split_for(c, (int64_t)t.nslots * BCELLS);
+        sp_launch(k_sp_start, dim3(s0.g), SPT, s, t, L0, b->types_f, b->types_c, (const float*)b->P_f,
+                  (const float*)b->P_c, (const float*)c->bf, (const float*)c->bc, c->rf, c->rc, c->st, c->partials,
+                  c->counters + SCNT_START, s0.gf, cond, 0);
+        vcycle(b->types_f, c->zf, c->zc, c->rf, c->rc, o->sweeps, o->coarse, o->boost);
+        sp_launch(k_sp_dinit, dim3(s0.g), SPT, s, t, b->types_f, b->types_c, (const float*)c->zf,
+                  (const float*)c->zc, (const float*)c->rf, (const float*)c->rc, c->df, c->dc, c->st, c->partials,
+                  c->counters + SCNT_INIT, s0.gf, cond, 0);
+        nk += 2;
+        cg_step(b, cond, use_cond);
+    }
+    void cg_step(const mpp_sparse_basin* b, cudaGraphConditionalHandle cond, int use_cond) {
+        const Topo& t = c->t;
+        const Comp L0 = comp0(c, b->types_f);
+        const Split s0 = split_for(c, (int64_t)t.nslots * BCELLS);
+        sp_launch(k_sp_apply_dot, dim3(s0.g), SPT, s, t, L0, b->types_f, b->types_c, (const float*)c->df,
+                  (const float*)c->dc, c->qf, c->qc, c->st, c->partials, c->counters + SCNT_DQ, s0.gf);
+        sp_launch(k_sp_update, dim3(s0.g), SPT, s, t, b->types_f, b->types_c, b->P_f, b->P_c, c->rf, c->rc, c->rof,
+                  c->roc, (const float*)c->df, (const float*)c->dc, (const float*)c->qf, (const float*)c->qc, c->st,
+                  c->partials, c->counters + SCNT_UPD, s0.gf, cond, use_cond);
+        nk += 2;
+    }
+    // the rotated loop body: the V-cycle of the new residual, beta, d, then q, alpha, the update
+    void cg_body(const mpp_sparse_basin* b, const mpp_sparse_opts* o, cudaGraphConditionalHandle cond, int use_cond) {
+        const Topo& t = c->t;
+        const Split s0 = split_for(c, (int64_t)t.nslots * BCELLS);
+        vcycle(b->types_f, c->zf, c->zc, c->rf, c->rc, o->sweeps, o->coarse, o->boost);
+        sp_launch(k_sp_dot2, dim3(s0.g), SPT, s, t, b->types_f, b->types_c, (const float*)c->zf, (const float*)c->zc,
+                  (const float*)c->rf, (const float*)c->rc, (const float*)c->rof, (const float*)c->roc, c->st,
+                  c->partials, c->counters + SCNT_DOT2, s0.gf);
+        sp_launch(k_sp_xpby, dim3(s0.g), SPT, s, t, c->df, c->dc, (const float*)c->zf, (const float*)c->zc,
+                  (const SpState*)c->st, s0.gf);
+        nk += 2;
+        cg_step(b, cond, use_cond);
+    }
+    void gradient(const mpp_sparse_basin* b) {
+        const Topo& t = c->t;
+        sp_launch(k_sp_project_fine, dim3(grid1((int64_t)t.nslots * BFACES), 3), SPT, s, t, b->u_f, b->v_f, b->w_f,
+                  b->fu_f, b->fv_f, b->fw_f, (const float*)b->P_f, (const float*)b->P_c, b->types_f, b->types_c,
+                  b->phi_f, b->phi_c);
+        int64_t mc = 0;
+        for (int a = 1; a <= 3; a++) mc = std::max(mc, face_count(t.nc, a));
+        sp_launch(k_sp_project_coarse, dim3(grid1(mc), 3), SPT, s, t, b->u_f, b->v_f, b->w_f, b->fu_f, b->fv_f,
+                  b->fw_f, b->u_c, b->v_c, b->w_c, b->fu_c, b->fv_c, b->fw_c, (const float*)b->P_c, b->types_c,
+                  b->phi_c);
+        nk += 2;
+    }
+};
+
+int read_state(mpp_sparse_ctx* c, cudaStream_t s) {
+    SCK(cudaMemcpyAsync(c->st_host, c->st, sizeof(SpState), cudaMemcpyDeviceToHost, s));
+    SCK(cudaStreamSynchronize(s));
+    return MPP_OK;
+}
+
+// a dot product over the unknowns, read back (FGMRES)
+int dot_host(mpp_sparse_ctx* c, SpRun& run, const uint8_t* tf, const uint8_t* tc, const float* af, const float* ac,
+             const float* bf, const float* bc, float* out) {
+    const Split s0 = split_for(c, (int64_t)c->t.nslots * BCELLS);
+    sp_launch(k_sp_dot, dim3(s0.g), SPT, run.s, c->t, tf, tc, af, ac, bf, bc, c->dres, c->partials,
+              c->counters + SCNT_DOT, s0.gf);
+    run.nk++;
+    SCK(cudaMemcpyAsync(c->dres_host, c->dres, sizeof(double), cudaMemcpyDeviceToHost, run.s));
+    SCK(cudaStreamSynchronize(run.s));
+    *out = (float)c->dres_host[0];
+    return MPP_OK;
+}
+void axpy(mpp_sparse_ctx* c, SpRun& run, float* yf, float* yc, float a, const float* xf, const float* xc, int zero,
+          int copy) {
+    const Split s0 = split_for(c, (int64_t)c->t.nslots * BCELLS);
+    sp_launch(k_sp_axpy, dim3(s0.g), SPT, run.s, c->t, yf, yc, a, xf, xc, zero, copy, s0.gf);
+    run.nk++;
+}
+void apply_(mpp_sparse_ctx* c, SpRun& run, const uint8_t* tf, const float* xf, const float* xc, float* qf, float* qc) {
+    const Split s0 = split_for(c, (int64_t)c->t.nslots * BCELLS);
+    sp_launch(k_sp_apply, dim3(s0.g), SPT, run.s, c->t, comp0(c, tf), tf, xf, xc, qf, qc, s0.gf);
+    run.nk++;
+}
+
+// |b - A P| with r left in c->rf/rc (the fallback's actual residual)
+int true_residual(mpp_sparse_ctx* c, SpRun& run, const mpp_sparse_basin* b, float* rnorm) {
+    apply_(c, run, b->types_f, b->P_f, b->P_c, c->qf, c->qc);
+    axpy(c, run, c->rf, c->rc, 0.0f, c->bf, c->bc, 0, 1);
+    axpy(c, run, c->rf, c->rc, -1.0f, c->qf, c->qc, 0, 0);
+    float rr;
+    if (int e = dot_host(c, run, b->types_f, b->types_c, c->rf, c->rc, c->rf, c->rc, &rr)) return e;
+    *rnorm = sqrtf(rr);
+    return MPP_OK;
+}
+
+// pressure_fgmres! (src/fgmres.jl:26-92)
+int fgmres(mpp_sparse_ctx* c, SpRun& run, const mpp_sparse_basin* b, const mpp_sparse_opts* o, int* its,
+           int* status, float* rel) {
+    const int64_t nf = (int64_t)c->capacity * BCELLS;
+    if (!c->fg_alloc) {
+        for (int j = 0; j <= SP_FGR; j++) {
+            if (int e = sp_alloc_n(c, &c->Vf[j], nf)) return e;
+            if (int e = sp_alloc_n(c, &c->Vc[j], c->ncc)) return e;
+        }
+        for (int j = 0; j < SP_FGR; j++) {
+            if (int e = sp_alloc_n(c, &c->Zf[j], nf)) return e;
+            if (int e = sp_alloc_n(c, &c->Zc[j], c->ncc)) return e;
+        }
+        c->fg_alloc = true;
+    }
+    const uint8_t *tf = b->types_f, *tc = b->types_c;
+    *its = 0;
+    *status = MPP_OK;
+    *rel = 0.0f;
+    float bb;
+    if (int e = dot_host(c, run, tf, tc, c->bf, c->bc, c->bf, c->bc, &bb)) return e;
+    const float bnorm = sqrtf(bb);
+    if (!std::isfinite(bnorm)) {
+        *status = MPP_NONFINITE;
+        return MPP_OK;
+    }
+    if (bnorm == 0.0f) {
+        axpy(c, run, b->P_f, b->P_c, 0.0f, c->bf, c->bc, 1, 0);  // zero!(s, s.P)
+        return MPP_OK;
+    }
+    const float target = o->tol * bnorm;
+    const int maxiter = o->maxiter;
+    float residual;
+    if (int e = true_residual(c, run, b, &residual)) return e;
+    while (residual > target && *its < maxiter) {
+        if (!std::isfinite(residual)) {
+            *status = MPP_NONFINITE;
+            return MPP_OK;
+        }
+        double H[SP_FGR + 1][SP_FGR] = {}, g[SP_FGR + 1] = {}, cs[SP_FGR] = {}, sn[SP_FGR] = {};
+        g[0] = residual;
+        axpy(c, run, c->Vf[0], c->Vc[0], 1.0f / residual, c->rf, c->rc, 1, 0);
+        int used = 0;
+        const int jmax = std::min(SP_FGR, maxiter - *its);
+        for (int j = 0; j < jmax; j++) {
+            run.vcycle(tf, c->zf, c->zc, c->Vf[j], c->Vc[j], o->sweeps, o->coarse, o->boost);
+            // the diagonal component: one damped Jacobi step from zero (src/fgmres.jl:15-24)
+            const Split s0 = split_for(c, (int64_t)c->t.nslots * BCELLS);
+            sp_launch(k_sp_jacobi<16, true>, dim3(s0.g), SPT, run.s, c->t, comp0(c, tf), c->Zf[j], c->Zc[j],
+                      (const float*)nullptr, (const float*)nullptr, (const float*)c->Vf[j], (const float*)c->Vc[j],
+                      s0.gf);
+            run.nk++;
+            axpy(c, run, c->Zf[j], c->Zc[j], 1.0f, c->zf, c->zc, 0, 0);
+            apply_(c, run, tf, c->Zf[j], c->Zc[j], c->qf, c->qc);
+            for (int pass = 0; pass < 2; pass++)
+                for (int i = 0; i <= j; i++) {
+                    float h;
+                    if (int e = dot_host(c, run, tf, tc, c->qf, c->qc, c->Vf[i], c->Vc[i], &h)) return e;
+                    H[i][j] += (double)h;
+                    axpy(c, run, c->qf, c->qc, -h, c->Vf[i], c->Vc[i], 0, 0);
+                }
+            float hh;
+            if (int e = dot_host(c, run, tf, tc, c->qf, c->qc, c->qf, c->qc, &hh)) return e;
+            const float hnext = sqrtf(hh);
+            if (!std::isfinite(hnext)) {
+                *status = MPP_NONFINITE;
+                return MPP_OK;
+            }
+            H[j + 1][j] = hnext;
+            if (hnext > 0.0f) axpy(c, run, c->Vf[j + 1], c->Vc[j + 1], 1.0f / hnext, c->qf, c->qc, 1, 0);
+            for (int i = 0; i < j; i++) {
+                const double a = H[i][j], bq = H[i + 1][j];
+                H[i][j] = cs[i] * a + sn[i] * bq;
+                H[i + 1][j] = -sn[i] * a + cs[i] * bq;
+            }
+            const double a = H[j][j], bq = H[j + 1][j];
+            const double hyp = std::hypot(a, bq);
+            if (!(hyp > 0)) {
+                *status = MPP_BREAKDOWN;
+                return MPP_OK;
+            }
+            cs[j] = a / hyp;
+            sn[j] = bq / hyp;
+            H[j][j] = hyp;
+            H[j + 1][j] = 0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            used = j + 1;
+            (*its)++;
+            if (std::fabs(g[j + 1]) <= target || hnext == 0.0f) break;
+        }
+        double y[SP_FGR];
+        for (int i = used - 1; i >= 0; i--) {
+            double acc = g[i];
+            for (int q = i + 1; q < used; q++) acc -= H[i][q] * y[q];
+            y[i] = acc / H[i][i];
+        }
+        for (int j = 0; j < used; j++) axpy(c, run, b->P_f, b->P_c, (float)y[j], c->Zf[j], c->Zc[j], 0, 0);
+        if (int e = true_residual(c, run, b, &residual)) return e;
+    }
+    *rel = residual / bnorm;
+    if (!(residual <= target)) *status = MPP_NOT_CONVERGED;
+    return MPP_OK;
+}
+
+int drop_graph(mpp_sparse_ctx* c) {
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->gexec = nullptr;
+    c->graph = nullptr;
+    memset(c->gkey, 0, sizeof(c->gkey));
+    return MPP_OK;
+}
+
+// The CG loop (after the prologue) as a graph: one conditional WHILE node over the rotated body.
+int loop_graph(mpp_sparse_ctx* c, const mpp_sparse_basin* b, const mpp_sparse_opts* o, cudaGraphExec_t* out,
+               int64_t* body_kernels) {
+    const void* key[12] = {b->slot, b->where, b->types_f, b->types_c, b->P_f, b->P_c, b->phi_f, b->phi_c,
+                           (const void*)(intptr_t)b->nslots, nullptr, nullptr, nullptr};
+    const int opt[4] = {o->sweeps, o->coarse, (int)(o->boost * 1024.0f), 0};
+    if (c->gexec && memcmp(key, c->gkey, sizeof(key)) == 0 && memcmp(opt, c->gopt, sizeof(opt)) == 0 &&
+        o->boost == (float)opt[2] / 1024.0f) {
+        *out = c->gexec;
+        *body_kernels = c->gopt[3];
+        return MPP_OK;
+    }
+    drop_graph(c);
+    cudaGraph_t g;
+    SCK(cudaGraphCreate(&g, 0));
+    c->graph = g;
+    cudaGraphConditionalHandle cond;
+    SCK(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    SCK(cudaGraphAddNode(&cnode, g, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    SpRun run{c, c->cap};
+    SCK(cudaStreamBeginCaptureToGraph(c->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    run.cg_body(b, o, cond, 1);
+    const cudaError_t le = cudaGetLastError();
+    SCK(cudaStreamEndCapture(c->cap, &body));
+    SCK(le);
+    SCK(cudaGraphInstantiate(&c->gexec, g, 0));
+    memcpy(c->gkey, key, sizeof(key));
+    memcpy(c->gopt, opt, sizeof(opt));
+    c->gopt[3] = (int)run.nk;
+    *out = c->gexec;
+    *body_kernels = run.nk;
+    return MPP_OK;
+}
+
+// pressure! from the right-hand side in c->bf/bc (the operator already built): the flexible
+// PCG (src/sflip.jl:1867-1904) or the fallback dispatch (src/fgmres.jl:96-110).
+int solve(mpp_sparse_ctx* c, SpRun& run, const mpp_sparse_basin* b, const mpp_sparse_opts* o, mpp_sparse_result* res) {
+    const bool fb = o->fallback != 0;
+    SpState init = {};
+    init.tol = o->tol;
+    init.maxiter = fb ? std::min(o->cg_maxiter, o->maxiter) : o->maxiter;
+    // keep project!'s volume terms already on the device: write only the loop's fields
+    SCK(cudaMemcpyAsync(&c->st->tol, &init.tol, sizeof(float) * 2, cudaMemcpyHostToDevice, run.s));
+    run.cg_prologue(b, o, 0, 0);
+    if (int e = read_state(c, run.s)) return e;
+    if (!c->st_host->done) {
+        if (o->graph) {
+            cudaGraphExec_t ge;
+            int64_t bk;
+            if (int e = loop_graph(c, b, o, &ge, &bk)) return e;
+            SCK(cudaGraphLaunch(ge, run.s));
+            if (int e = read_state(c, run.s)) return e;
+            run.nk += bk * (c->st_host->it - 1);
+        } else {
+            while (!c->st_host->done) {
+                run.cg_body(b, o, 0, 0);
+                if (int e = read_state(c, run.s)) return e;
+            }
+        }
+    }
+    SCK(cudaGetLastError());
+    const SpState& h = *c->st_host;
+    int its = h.it, status = h.status;
+    float rel = h.bnorm > 0.0f ? h.rnorm / h.bnorm : 0.0f;
+    int fg_its = 0;
+    if (fb) {
+        if (status == MPP_NONFINITE || status == MPP_INDEFINITE) its = 0;
+        float rnorm, bb;
+        if (int e = true_residual(c, run, b, &rnorm)) return e;
+        if (int e = dot_host(c, run, b->types_f, b->types_c, c->bf, c->bc, c->bf, c->bc, &bb)) return e;
+        const float bnorm = sqrtf(bb);
+        rel = bnorm > 0.0f ? rnorm / bnorm : 0.0f;
+        status = MPP_OK;
+        if (!(rnorm <= o->tol * bnorm)) {
+            if (!std::isfinite(rnorm) || rnorm > 2.0f * bnorm)
+                axpy(c, run, b->P_f, b->P_c, 0.0f, c->bf, c->bc, 1, 0);  // zero!(s, s.P)
+            if (int e = fgmres(c, run, b, o, &fg_its, &status, &rel)) return e;
+            its += fg_its;
+        }
+    }
+    if (res) {
+        res->iterations = its;
+        res->fgmres_iterations = fg_its;
+        res->status = status;
+        res->rel_residual = rel;
+    }
+    return MPP_OK;
+}
+
+int finish(mpp_sparse_ctx* c, SpRun& run, mpp_sparse_result* res, int status) {
+    SCK(cudaGetLastError());
+    SCK(cudaStreamSynchronize(run.s));
+    c->launches += run.nk;
+    if (res) res->kernel_launches = run.nk;
+    return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+void mpp_sparse_opts_default(mpp_sparse_opts* o) {
+    if (!o) return;
+    o->tol = 1e-4f;
+    o->maxiter = 200;
+    o->sweeps = 1;
+    o->boost = 1.0f;
+    o->coarse = 40;
+    o->fallback = 0;
+    o->graph = 0;
+    o->cg_maxiter = 80;
+}
+
+int32_t mpp_sparse_dense_levels(const int32_t nb[3]) {
+    if (!nb || nb[0] <= 0 || nb[1] <= 0 || nb[2] <= 0) return -1;
+    int m[3] = {4 * nb[0], 4 * nb[1], 4 * nb[2]};
+    for (int nd = 1; nd <= SP_MAXD; nd++) {
+        if ((int64_t)m[0] * m[1] * m[2] <= 1024) return nd;
+        if ((m[0] | m[1] | m[2]) & 1) return -1;
+        m[0] /= 2;
+        m[1] /= 2;
+        m[2] /= 2;
+    }
+    return -1;
+}
+
+int mpp_sparse_ctx_create(mpp_sparse_ctx** out, const mpp_sparse_grid* g, int32_t capacity) {
+    if (!out || !g || capacity <= 0 || !(g->dx > 0.0f)) {
+        sp_err("null output or grid, capacity <= 0 or dx <= 0");
+        return MPP_ERR_INVALID;
+    }
+    *out = nullptr;
+    const int nd = mpp_sparse_dense_levels(g->nb);
+    if (nd < 0) {
+        sp_err("the coarse grid %dx%dx%d does not halve to at most 1024 cells", 4 * g->nb[0], 4 * g->nb[1],
+               4 * g->nb[2]);
+        return MPP_ERR_INVALID;
+    }
+    if ((int64_t)capacity * BFACES > INT32_MAX) {
+        sp_err("capacity %d too large", capacity);
+        return MPP_ERR_INVALID;
+    }
+    mpp_sparse_ctx* c = new mpp_sparse_ctx();
+    memset(&c->t, 0, sizeof(c->t));
+    for (int a = 0; a < 3; a++) {
+        c->t.nb[a] = g->nb[a];
+        c->t.nc[a] = 4 * g->nb[a];
+        c->t.lo[a] = g->lo[a];
+    }
+    c->t.dx = g->dx;
+    c->t.radius = g->radius;
+    c->t.floor_z = g->floor_z;
+    c->capacity = capacity;
+    c->nd = nd;
+    c->ncc = (int64_t)c->t.nc[0] * c->t.nc[1] * c->t.nc[2];
+    auto fail = [&](int e) {
+        mpp_sparse_ctx_destroy(c);
+        return e;
+    };
+    if (cudaGetDevice(&c->dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev) != cudaSuccess) {
+        sp_err("no CUDA device");
+        return fail(MPP_ERR_CUDA);
+    }
+    const int64_t nf = (int64_t)capacity * BCELLS, nff = (int64_t)capacity * BFACES;
+    const int64_t n1 = (int64_t)capacity * BCELLS1, f1 = (int64_t)capacity * BFACES1;
+    int e = 0;
+    for (int a = 0; a < 3 && !e; a++) {
+        e = sp_alloc_n(c, &c->cf[a], nff);
+        if (!e) e = sp_alloc_n(c, &c->cc[a], face_count(c->t.nc, a + 1));
+        if (!e) e = sp_alloc_n(c, &c->c1[a], f1);
+    }
+    float** fine[] = {&c->dDf, &c->bf, &c->rf, &c->zf, &c->df, &c->qf, &c->rof, &c->tmf, &c->res0f};
+    float** coarse[] = {&c->dDc, &c->bc, &c->rc, &c->zc, &c->dc, &c->qc, &c->roc, &c->tmc, &c->res0c,
+                        &c->x1c, &c->r1c, &c->t1c};
+    float** lev1[] = {&c->dD1, &c->x1f, &c->b1f, &c->r1f, &c->t1f};
+    for (auto p : fine)
+        if (!e) e = sp_alloc_n(c, p, nf);
+    for (auto p : coarse)
+        if (!e) e = sp_alloc_n(c, p, c->ncc);
+    for (auto p : lev1)
+        if (!e) e = sp_alloc_n(c, p, n1);
+    if (!e) e = sp_alloc_n(c, &c->act1, n1);
+    int m[3] = {c->t.nc[0], c->t.nc[1], c->t.nc[2]};
+    for (int l = 0; l < nd && !e; l++) {
+        DL& D = c->D[l];
+        memcpy(D.n, m, sizeof(m));
+        const int64_t cells = (int64_t)m[0] * m[1] * m[2];
+        float** arr[] = {&D.x, &D.b, &D.r, &D.t, &D.dD};
+        for (auto p : arr)
+            if (!e) e = sp_alloc_n(c, p, cells);
+        if (!e) e = sp_alloc_n(c, &D.act, cells);
+        if (!e) e = sp_alloc_n(c, &D.cx, face_count(m, 1));
+        if (!e) e = sp_alloc_n(c, &D.cy, face_count(m, 2));
+        if (!e) e = sp_alloc_n(c, &D.cz, face_count(m, 3));
+        m[0] /= 2;
+        m[1] /= 2;
+        m[2] /= 2;
+    }
+    if (e) return fail(e);
+    c->actc = c->D[0].act;
+    if (int e2 = sp_alloc_n(c, &c->st, 1)) return fail(e2);
+    if (int e2 = sp_alloc_n(c, &c->dres, 1)) return fail(e2);
+    if (int e2 = sp_alloc_n(c, &c->partials, (int64_t)c->nsm * 8 * MAXK * 2)) return fail(e2);
+    if (int e2 = sp_alloc_n(c, &c->counters, SCNT_N)) return fail(e2);
+    if (cudaMallocHost((void**)&c->st_host, sizeof(SpState)) != cudaSuccess ||
+        cudaMallocHost((void**)&c->dres_host, sizeof(double)) != cudaSuccess) {
+        sp_err("cudaMallocHost failed");
+        return fail(MPP_ERR_NOMEM);
+    }
+    if (cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking) != cudaSuccess) {
+        sp_err("cudaStreamCreate failed");
+        return fail(MPP_ERR_CUDA);
+    }
+    *out = c;
+    return MPP_OK;
+}
+
+int mpp_sparse_ctx_destroy(mpp_sparse_ctx* c) {
+    if (!c) return MPP_OK;
+    drop_graph(c);
+    for (void* p : c->allocs) cudaFree(p);
+    if (c->st_host) cudaFreeHost(c->st_host);
+    if (c->dres_host) cudaFreeHost(c->dres_host);
+    if (c->cap) cudaStreamDestroy(c->cap);
+    delete c;
+    return MPP_OK;
+}
+
+size_t mpp_sparse_ctx_bytes(const mpp_sparse_ctx* c) { return c ? c->bytes : 0; }
+
+int mpp_sparse_volume(mpp_sparse_ctx* c, const mpp_sparse_basin* b, double* volume, mpp_stream stream) {
+    if (int e = sp_check_basin(c, b)) return e;
+    if (!b->phi_f || !b->phi_c || !volume) {
+        sp_err("null level set or output");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    SpRun run{c, s};
+    SpState init = {};
+    init.volume0 = 1.0f;
+    init.dt = 1.0;
+    init.recover = 1.0;
+    SCK(cudaMemcpyAsync(c->st, &init, sizeof(SpState), cudaMemcpyHostToDevice, s));
+    const Split s0 = split_for(c, (int64_t)b->nslots * BCELLS);
+    sp_launch(k_sp_volume, dim3(s0.g), SPT, s, c->t, b->phi_f, b->phi_c, c->st, c->partials, c->counters + SCNT_VOL,
+              s0.gf);
+    run.nk++;
+    if (int e = read_state(c, s)) return e;
+    *volume = (double)c->st_host->vol;
+    return finish(c, run, nullptr, MPP_OK);
+}
+
+int mpp_sparse_operator(mpp_sparse_ctx* c, const mpp_sparse_basin* b, mpp_stream stream) {
+    if (int e = sp_check_basin(c, b)) return e;
+    if (!b->phi_f || !b->phi_c) {
+        sp_err("null level set");
+        return MPP_ERR_INVALID;
+    }
+    SpRun run{c, (cudaStream_t)stream};
+    run.operator_(b);
+    return finish(c, run, nullptr, MPP_OK);
+}
+
+int mpp_sparse_apply(mpp_sparse_ctx* c, const mpp_sparse_basin* b, const float* xf, const float* xc, float* qf,
+                     float* qc, mpp_stream stream) {
+    if (int e = sp_check_basin(c, b)) return e;
+    SpRun run{c, (cudaStream_t)stream};
+    apply_(c, run, b->types_f, xf, xc, qf, qc);
+    return finish(c, run, nullptr, MPP_OK);
+}
+
+int mpp_sparse_vcycle(mpp_sparse_ctx* c, const mpp_sparse_basin* b, const float* rf, const float* rc, float* zf,
+                      float* zc, int32_t sweeps, int32_t coarse, float boost, mpp_stream stream) {
+    if (int e = sp_check_basin(c, b)) return e;
+    if (sweeps < 1 || coarse < 0) {
+        sp_err("sweeps must be >= 1 and coarse >= 0");
+        return MPP_ERR_INVALID;
+    }
+    SpRun run{c, (cudaStream_t)stream};
+    run.vcycle(b->types_f, zf, zc, rf, rc, sweeps, coarse, boost);
+    return finish(c, run, nullptr, MPP_OK);
+}
+
+int mpp_sparse_rhs(mpp_sparse_ctx* c, const mpp_sparse_basin* b, float gamma, float* bf, float* bc, mpp_stream stream) {
+    if (int e = sp_check_basin(c, b)) return e;
+    SpRun run{c, (cudaStream_t)stream};
+    const Split s0 = split_for(c, (int64_t)b->nslots * BCELLS);
+    sp_launch(k_sp_rhs, dim3(s0.g), SPT, run.s, c->t, b->types_f, b->types_c, (const float*)b->u_f,
+              (const float*)b->v_f, (const float*)b->w_f, (const float*)b->u_c, (const float*)b->v_c,
+              (const float*)b->w_c, bf, bc, (float*)nullptr, (float*)nullptr, (const SpState*)nullptr, gamma, s0.gf);
+    run.nk++;
+    return finish(c, run, nullptr, MPP_OK);
+}
+
+static int check_opts(const mpp_sparse_opts* o) {
+    if (!o || !(o->tol >= 0.0f) || o->maxiter < 0 || o->sweeps < 1 || o->coarse < 0 || o->cg_maxiter < 0) {
+        sp_err("bad options (tol >= 0, maxiter >= 0, sweeps >= 1, coarse >= 0, cg_maxiter >= 0)");
+        return MPP_ERR_INVALID;
+    }
+    return MPP_OK;
+}
+
+int mpp_sparse_pressure(mpp_sparse_ctx* c, const mpp_sparse_basin* b, const float* bf, const float* bc,
+                        const mpp_sparse_opts* o, mpp_sparse_result* res, mpp_stream stream) {
+    if (int e = sp_check_basin(c, b)) return e;
+    if (int e = check_opts(o)) return e;
+    cudaStream_t s = (cudaStream_t)stream;
+    SpRun run{c, s};
+    run.operator_(b);
+    const int64_t nf = (int64_t)b->nslots * BCELLS;
+    SCK(cudaMemcpyAsync(c->bf, bf, sizeof(float) * (size_t)nf, cudaMemcpyDefault, s));
+    SCK(cudaMemcpyAsync(c->bc, bc, sizeof(float) * (size_t)c->ncc, cudaMemcpyDefault, s));
+    mpp_sparse_result r = {};
+    if (int e = solve(c, run, b, o, &r)) return e;
+    if (res) *res = r;
+    return finish(c, run, res, r.status);
+}
+
+int mpp_sparse_gradient(mpp_sparse_ctx* c, const mpp_sparse_basin* b, mpp_stream stream) {
+    if (int e = sp_check_basin(c, b)) return e;
+    SpRun run{c, (cudaStream_t)stream};
+    run.gradient(b);
+    return finish(c, run, nullptr, MPP_OK);
+}
+
+int mpp_sparse_project(mpp_sparse_ctx* c, const mpp_sparse_basin* b, float volume0, double dt, double recover,
+                       const mpp_sparse_opts* o, mpp_sparse_result* res, mpp_stream stream) {
+    if (int e = sp_check_basin(c, b)) return e;
+    if (int e = check_opts(o)) return e;
+    if (!(volume0 > 0.0f) || !(dt > 0.0) || !(recover > 0.0)) {
+        sp_err("volume0, dt and recover must be positive");
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    SpRun run{c, s};
+    SpState init = {};
+    init.volume0 = volume0;
+    init.dt = dt;
+    init.recover = recover;
+    SCK(cudaMemcpyAsync(c->st, &init, sizeof(SpState), cudaMemcpyHostToDevice, s));
+    const Split s0 = split_for(c, (int64_t)b->nslots * BCELLS);
+    sp_launch(k_sp_volume, dim3(s0.g), SPT, s, c->t, b->phi_f, b->phi_c, c->st, c->partials, c->counters + SCNT_VOL,
+              s0.gf);
+    run.operator_(b);
+    sp_launch(k_sp_rhs, dim3(s0.g), SPT, s, c->t, b->types_f, b->types_c, (const float*)b->u_f, (const float*)b->v_f,
+              (const float*)b->w_f, (const float*)b->u_c, (const float*)b->v_c, (const float*)b->w_c, c->bf, c->bc,
+              b->P_f, b->P_c, (const SpState*)c->st, 0.0f, s0.gf);
+    run.nk += 2;
+    mpp_sparse_result r = {};
+    if (int e = solve(c, run, b, o, &r)) return e;
+    run.gradient(b);
+    r.volume = c->st_host->vol;
+    r.gamma = c->st_host->gamma;
+    if (res) *res = r;
+    return finish(c, run, res, r.status);
+}
+
+int64_t mpp_sparse_read(mpp_sparse_ctx* c, int32_t which, void* dst, size_t bytes, mpp_stream stream) {
+    if (!c || !dst) {
+        sp_err("null context or destination");
+        return MPP_ERR_INVALID;
+    }
+    const int64_t nff = (int64_t)c->t.nslots * BFACES, nf = (int64_t)c->t.nslots * BCELLS;
+    const int64_t f1 = (int64_t)c->t.nslots * BFACES1, n1 = (int64_t)c->t.nslots * BCELLS1;
+    const void* src = nullptr;
+    int64_t n = 0;
+    switch (which) {
+        case MPP_SP_CU_F: case MPP_SP_CV_F: case MPP_SP_CW_F:
+            src = c->cf[which - MPP_SP_CU_F]; n = 4 * nff; break;
+        case MPP_SP_CU_C: case MPP_SP_CV_C: case MPP_SP_CW_C:
+            src = c->cc[which - MPP_SP_CU_C]; n = 4 * face_count(c->t.nc, which - MPP_SP_CU_C + 1); break;
+        case MPP_SP_DD_F: src = c->dDf; n = 4 * nf; break;
+        case MPP_SP_DD_C: src = c->dDc; n = 4 * c->ncc; break;
+        case MPP_SP_ACT_C: src = c->actc; n = c->ncc; break;
+        case MPP_SP_C1X: case MPP_SP_C1Y: case MPP_SP_C1Z:
+            src = c->c1[which - MPP_SP_C1X]; n = 4 * f1; break;
+        case MPP_SP_DD1: src = c->dD1; n = 4 * n1; break;
+        case MPP_SP_ACT1: src = c->act1; n = n1; break;
+        case MPP_SP_C2X: src = c->D[0].cx; n = 4 * face_count(c->t.nc, 1); break;
+        case MPP_SP_C2Y: src = c->D[0].cy; n = 4 * face_count(c->t.nc, 2); break;
+        case MPP_SP_C2Z: src = c->D[0].cz; n = 4 * face_count(c->t.nc, 3); break;
+        case MPP_SP_DD2: src = c->D[0].dD; n = 4 * c->ncc; break;
+        default: sp_err("unknown workspace array %d", which); return MPP_ERR_INVALID;
+    }
+    if ((size_t)n > bytes) {
+        sp_err("destination holds %zu bytes, the array %lld", bytes, (long long)n);
+        return MPP_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    SCK(cudaMemcpyAsync(dst, src, (size_t)n, cudaMemcpyDefault, s));
+    SCK(cudaStreamSynchronize(s));
+    return n;
+}
+
+}  // extern "C"

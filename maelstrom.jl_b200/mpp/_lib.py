@@ -60,6 +60,42 @@ class TuneEntry(ctypes.Structure):
 
 SMOOTHERS = {0: "vector", 1: "tma", 2: "column", 3: "async"}
 
+
+class SparseGrid(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_float * 3), ("dx", ctypes.c_float), ("nb", ctypes.c_int32 * 3),
+                ("radius", ctypes.c_float), ("floor_z", ctypes.c_float)]
+
+
+SPARSE_ARRAYS = ("types_f", "types_c", "phi_f", "phi_c", "P_f", "P_c", "u_f", "u_c", "v_f", "v_c", "w_f", "w_c",
+                 "fu_f", "fu_c", "fv_f", "fv_c", "fw_f", "fw_c")
+
+
+class SparseBasinArrays(ctypes.Structure):
+    _fields_ = [("slot", ctypes.c_void_p), ("where", ctypes.c_void_p), ("nslots", ctypes.c_int32)] + [
+        (n, ctypes.c_void_p) for n in SPARSE_ARRAYS]
+
+
+class SparseOpts(ctypes.Structure):
+    _fields_ = [("tol", ctypes.c_float), ("maxiter", ctypes.c_int32), ("sweeps", ctypes.c_int32),
+                ("boost", ctypes.c_float), ("coarse", ctypes.c_int32), ("fallback", ctypes.c_int32),
+                ("graph", ctypes.c_int32), ("cg_maxiter", ctypes.c_int32)]
+
+
+class SparseResult(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("fgmres_iterations", ctypes.c_int32), ("status", ctypes.c_int32),
+                ("rel_residual", ctypes.c_float), ("volume", ctypes.c_float), ("gamma", ctypes.c_float),
+                ("kernel_launches", ctypes.c_int64)]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["status_name"] = STATUS_NAMES.get(self.status, str(self.status))
+        return d
+
+
+# workspace arrays of mpp_sparse_read
+SP_ARRAYS = {n: i for i, n in enumerate(("cu_f", "cv_f", "cw_f", "cu_c", "cv_c", "cw_c", "dD_f", "dD_c", "act_c",
+                                          "c1x", "c1y", "c1z", "dD1", "act1", "c2x", "c2y", "c2z", "dD2"))}
+
 # name -> (restype, argtypes); every symbol include/mpp.h declares.
 P, I32, F32, F64, SZ = ctypes.c_void_p, ctypes.c_int32, ctypes.c_float, ctypes.c_double, ctypes.c_size_t
 _G, _O, _R = ctypes.POINTER(Grid), ctypes.POINTER(Opts), ctypes.POINTER(Result)
@@ -104,6 +140,22 @@ SIGNATURES = {
     "mpp_solution_f64": (ctypes.c_int, [P, P]),
     "mpp_profile_enable": (ctypes.c_int, [P, ctypes.c_int]),
     "mpp_profile_read": (ctypes.c_int, [P, ctypes.c_void_p, ctypes.c_int]),
+    "mpp_sparse_opts_default": (None, [ctypes.POINTER(SparseOpts)]),
+    "mpp_sparse_dense_levels": (I32, [ctypes.POINTER(ctypes.c_int32)]),
+    "mpp_sparse_ctx_create": (ctypes.c_int, [ctypes.POINTER(P), ctypes.POINTER(SparseGrid), I32]),
+    "mpp_sparse_ctx_destroy": (ctypes.c_int, [P]),
+    "mpp_sparse_ctx_bytes": (SZ, [P]),
+    "mpp_sparse_volume": (ctypes.c_int, [P, ctypes.POINTER(SparseBasinArrays), ctypes.POINTER(F64), P]),
+    "mpp_sparse_operator": (ctypes.c_int, [P, ctypes.POINTER(SparseBasinArrays), P]),
+    "mpp_sparse_apply": (ctypes.c_int, [P, ctypes.POINTER(SparseBasinArrays), P, P, P, P, P]),
+    "mpp_sparse_vcycle": (ctypes.c_int, [P, ctypes.POINTER(SparseBasinArrays), P, P, P, P, I32, I32, F32, P]),
+    "mpp_sparse_rhs": (ctypes.c_int, [P, ctypes.POINTER(SparseBasinArrays), F32, P, P, P]),
+    "mpp_sparse_pressure": (ctypes.c_int, [P, ctypes.POINTER(SparseBasinArrays), P, P, ctypes.POINTER(SparseOpts),
+                                           ctypes.POINTER(SparseResult), P]),
+    "mpp_sparse_gradient": (ctypes.c_int, [P, ctypes.POINTER(SparseBasinArrays), P]),
+    "mpp_sparse_project": (ctypes.c_int, [P, ctypes.POINTER(SparseBasinArrays), F32, F64, F64,
+                                          ctypes.POINTER(SparseOpts), ctypes.POINTER(SparseResult), P]),
+    "mpp_sparse_read": (ctypes.c_int64, [P, I32, P, SZ, P]),
     "mpp_last_error": (ctypes.c_char_p, []),
     "mpp_version": (ctypes.c_char_p, []),
 }

@@ -143,6 +143,62 @@ void orc_classify(const orc_grid* g, uint8_t* types, const float* phi);
  * most -2 dx); returns the sweep rounds run. */
 int orc_filltrapped(const orc_grid* g, uint8_t* types, float* phi, int maxrounds);
 
+/* ---- the sparse two-resolution basin (sparse.c; src/sflip.jl:1059-2018, src/fgmres.jl) ----
+ * Fine 16^3 blocks over a dense coarse grid of cells 4 dx wide (nb blocks a side, 4 nb coarse
+ * cells). slot[bi + nb0 (bj + nb1 bk)] is the block's 1-based slot in the fine pools (0: coarse
+ * only); where[3 (s - 1) ..] the slot's block coordinates (-1s: a free slot). Fine cell pools
+ * hold 4096 cells a slot (i + 16 (j + 16 k)); fine face pools 17*256 faces a slot a axis
+ * (faceindex, src/sflip.jl:106-110). Coarse arrays are column-major over the coarse cells,
+ * face arrays one longer along their axis. Float32 throughout, as the reference. */
+typedef struct {
+    float lo[3];
+    float dx;
+    int32_t nb[3];
+    float radius;
+    float floor_z;
+} ors_grid;
+typedef struct {
+    ors_grid g;
+    const int32_t* slot;
+    const int32_t* where;
+    int32_t nslots;
+    const uint8_t *tf, *tc;
+    const float *phif, *phic;
+    float *Pf, *Pc;
+    float *uf, *uc, *vf, *vc, *wf, *wc;
+    uint8_t *fuf, *fuc, *fvf, *fvc, *fwf, *fwc;
+} ors_basin;
+typedef struct {
+    float tol;      /* pressure!(::SparseBasin) default 1e-4; the fallback dispatch's 5e-4 */
+    int32_t maxiter;
+    int32_t sweeps; /* damped Jacobi sweep pairs down and up (default 1) */
+    float boost;    /* coarse corrections' scale (1; the fallback dispatch's 1.5) */
+    int32_t fallback; /* 1: src/fgmres.jl:96-110 (CG capped at cg_maxiter, then FGMRES) */
+    int32_t cg_maxiter; /* the dispatch's CG cap (80 in the reference) */
+} ors_opts;
+enum { ORS_OK = 0, ORS_NOT_CONVERGED = 1, ORS_NONFINITE = 2, ORS_INDEFINITE = 3, ORS_BREAKDOWN = 4 };
+typedef struct {
+    int32_t iterations;        /* what pressure! returns (CG + FGMRES iterations) */
+    int32_t fgmres_iterations;
+    int32_t status;            /* ORS_* */
+    float rel_residual;        /* last residual / |b| */
+    float volume;              /* volume(s) at entry of project! */
+    float gamma;
+} ors_info;
+double ors_volume(const ors_basin* b);
+int ors_levels(const ors_basin* b);
+int ors_coefficients(const ors_basin* b, float* cuf, float* cvf, float* cwf, float* cuc, float* cvc, float* cwc,
+                     float* dDf, float* dDc, uint8_t* actc);
+int ors_apply(const ors_basin* b, const float* xf, const float* xc, float* qf, float* qc);
+int ors_jacobi(const ors_basin* b, const float* xf, const float* xc, const float* bf, const float* bc, float* of,
+               float* oc);
+int ors_vcycle(const ors_basin* b, const float* rf, const float* rc, float* zf, float* zc, int sweeps, int coarse,
+               float boost);
+int ors_rhs(const ors_basin* b, float gamma, float* bf, float* bc);
+int ors_pressure(const ors_basin* b, const float* bf, const float* bc, const ors_opts* o, ors_info* info);
+int ors_gradient(const ors_basin* b);
+int ors_project(const ors_basin* b, float volume0, double dt, double recover, const ors_opts* o, ors_info* info);
+
 #ifdef __cplusplus
 }
 #endif
