@@ -160,27 +160,100 @@ __global__ void __launch_bounds__(SPT) k_sp_rhs(Topo t, const uint8_t* tf, const
     }
 }
 
+// The fine part of the CG's vector passes: a CTA per slot, 16-byte pieces (four cells) of
+// the slot's 4096 cells, four a thread; a free slot's CTA only joins the reduction. The
+// coarse part: the grid's cells four at a time over the remaining CTAs.
+#define SP_SLOT_PIECES(n)                                                                   \
+    for (int m_ = 0; m_ < 4; m_++)                                                          \
+        if (const int64_t n = (int64_t)(sl - 1) * BCELLS + 4 * ((int)threadIdx.x + 256 * m_); true)
+#define SP_COARSE_PIECES(c, nc4, gf)                                                        \
+    for (int64_t c = 4 * ((int64_t)(blockIdx.x - (gf)) * blockDim.x + threadIdx.x); c < 4 * (nc4);   \
+         c += 4 * (int64_t)(gridDim.x - (gf)) * blockDim.x)
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ uchar4 ldm4(const uint8_t* p) { return *reinterpret_cast<const uchar4*>(p); }
+__device__ __forceinline__ double dot4m(float4 a, float4 b, uchar4 m, uint8_t want) {
+    double s = 0.0;
+    if (m.x == want) s += (double)a.x * (double)b.x;
+    if (m.y == want) s += (double)a.y * (double)b.y;
+    if (m.z == want) s += (double)a.z * (double)b.z;
+    if (m.w == want) s += (double)a.w * (double)b.w;
+    return s;
+}
+
+// Level 0's Jacobi sweeps and residual: the fine part a CTA per slot (staged block), the
+// coarse part as jacobicoarse_kernel! / residualcoarse_kernel!.
+template <int OP>
+__global__ void __launch_bounds__(SPT) k_sp_blk(Topo t, Comp L, const uint16_t* code0, const float* dg0, float* outf,
+                                                float* outc, const float* xf, const float* xc, const float* bf,
+                                                const float* bc, int gf) {
+    __shared__ float xs[PCELLS];
+    pdl_wait();
+    pdl_trigger();
+    if ((int)blockIdx.x < gf) {
+        const int sl = (int)blockIdx.x + 1;
+        int w[3];
+        where_of(t, sl, w);
+        if (w[0] < 0) return;
+        if (OP != BOP_JAC_ZS) {
+            stage_block(t, xf, xc, sl, w, xs);
+            __syncthreads();
+        }
+        block_cells<OP>(code0, dg0, bf, xs, sl, [&](int64_t n, const float* v, const float*) {
+            st4(outf + n, make_float4(v[0], v[1], v[2], v[3]));
+        });
+    } else {
+        constexpr bool ZS = OP == BOP_JAC_ZS;
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            int I, J, K;
+            coarse_cell(t, c, I, J, K);
+            float v = 0.0f;
+            if (L.actc[c] != 0 && !covered(t, I, J, K)) {
+                float diag, off;
+                coarserow<16, ZS>(t, L, xf, xc, I, J, K, diag, off);
+                const float x0 = ZS ? 0.0f : xc[c];
+                if (OP == BOP_RES) v = bc[c] - (diag * x0 - off);
+                else v = diag > 0.0f ? x0 + OMEGA * (bc[c] - (diag * x0 - off)) / diag : 0.0f;
+            }
+            outc[c] = v;
+        }
+    }
+}
+
+// q = A x at level 0 for the CG kernels (apply!, src/sflip.jl:1824-1847): the fine part of
+// slot sl through the staged block; `sink(n, q[4], x[4])`.
+template <class Sink>
+__device__ __forceinline__ void apply_block(const Topo& t, const uint16_t* code0, const float* dg0, const float* xf,
+                                            const float* xc, int sl, const int w[3], float* xs, Sink&& sink) {
+    stage_block(t, xf, xc, sl, w, xs);
+    __syncthreads();
+    block_cells<BOP_APPLY>(code0, dg0, nullptr, xs, sl, sink);
+}
+
 // r = b - A P (apply! then xpby!(r, b, -1)), |b| and |r| (src/sflip.jl:1870-1877).
-__global__ void __launch_bounds__(SPT) k_sp_start(Topo t, Comp L, const uint8_t* tf, const uint8_t* tc, const float* Pf,
+__global__ void __launch_bounds__(SPT) k_sp_start(Topo t, Comp L, const uint16_t* code0, const float* dg0,
+                                                  const uint8_t* tf, const uint8_t* cmask, const float* Pf,
                                                   const float* Pc, const float* bf, const float* bc, float* rf,
-                                                  float* rc, SpState* st, double* partials, unsigned* counter, int gf,
-                                                  cudaGraphConditionalHandle cond, int use_cond) {
+                                                  float* rc, SpState* st, double* partials, unsigned* counter, int gf) {
+    __shared__ float xs[PCELLS];
     pdl_wait();
     pdl_trigger();
     double acc[2] = {0.0, 0.0};
     if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * BCELLS;
-        SP_FINE_LOOP(n, nf, gf) {
-            bool live;
-            const float q = apply_fine(t, L, tf, Pf, Pc, n, live);
-            if (!live) continue;
-            const float r = bf[n] + (-1.0f) * q;
-            rf[n] = r;
-            if (tf[n] == LIQUID) {
-                acc[0] += (double)bf[n] * (double)bf[n];
-                acc[1] += (double)r * (double)r;
-            }
-        }
+        const int sl = (int)blockIdx.x + 1;
+        int w[3];
+        where_of(t, sl, w);
+        if (w[0] >= 0)
+            apply_block(t, code0, dg0, Pf, Pc, sl, w, xs, [&](int64_t n, const float* q, const float*) {
+                const float4 b = ld4(bf + n);
+                const float4 r = make_float4(b.x + (-1.0f) * q[0], b.y + (-1.0f) * q[1], b.z + (-1.0f) * q[2],
+                                             b.w + (-1.0f) * q[3]);
+                st4(rf + n, r);
+                const uchar4 m = ldm4(tf + n);
+                acc[0] += dot4m(b, b, m, LIQUID);
+                acc[1] += dot4m(r, r, m, LIQUID);
+            });
     } else {
         const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
         SP_COARSE_LOOP(c, nc, gf) {
@@ -188,7 +261,7 @@ __global__ void __launch_bounds__(SPT) k_sp_start(Topo t, Comp L, const uint8_t*
             const float q = apply_coarse(t, L, Pf, Pc, c, cov);
             const float r = bc[c] + (-1.0f) * q;
             rc[c] = r;
-            if (tc[c] == LIQUID && !cov) {
+            if (cmask[c]) {
                 acc[0] += (double)bc[c] * (double)bc[c];
                 acc[1] += (double)r * (double)r;
             }
@@ -211,31 +284,29 @@ __global__ void __launch_bounds__(SPT) k_sp_start(Topo t, Comp L, const uint8_t*
             st->rnorm = sqrtf((float)acc[1]);
             if (st->rnorm <= st->target) st->done = 1;
         }
-        if (use_cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
     }
 }
 
 // d = z and rho = z.r after the first V-cycle (src/sflip.jl:1879-1883).
-__global__ void __launch_bounds__(SPT) k_sp_dinit(Topo t, const uint8_t* tf, const uint8_t* tc, const float* zf,
+__global__ void __launch_bounds__(SPT) k_sp_dinit(Topo t, const uint8_t* tf, const uint8_t* cmask, const float* zf,
                                                   const float* zc, const float* rf, const float* rc, float* df,
-                                                  float* dc, SpState* st, double* partials, unsigned* counter, int gf,
-                                                  cudaGraphConditionalHandle cond, int use_cond) {
+                                                  float* dc, SpState* st, double* partials, unsigned* counter, int gf) {
     pdl_wait();
     pdl_trigger();
     if (st->done) return;
     double acc[1] = {0.0};
     if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * BCELLS;
-        SP_FINE_LOOP(n, nf, gf) {
-            if (!slot_used(t, (int)(n >> 12) + 1)) continue;
-            df[n] = zf[n];
-            if (tf[n] == LIQUID) acc[0] += (double)zf[n] * (double)rf[n];
-        }
+        const int sl = (int)blockIdx.x + 1;
+        if (slot_used(t, sl)) SP_SLOT_PIECES(n) {
+                const float4 z = ld4(zf + n);
+                st4(df + n, z);
+                acc[0] += dot4m(z, ld4(rf + n), ldm4(tf + n), LIQUID);
+            }
     } else {
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) {
-            dc[c] = zc[c];
-            if (coarse_unknown(t, tc, c)) acc[0] += (double)zc[c] * (double)rc[c];
+        SP_COARSE_PIECES(c, (int64_t)t.nc[0] * t.nc[1] * t.nc[2] / 4, gf) {
+            const float4 z = ld4(zc + c);
+            st4(dc + c, z);
+            acc[0] += dot4m(z, ld4(rc + c), ldm4(cmask + c), 1);
         }
     }
     if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
@@ -251,34 +322,36 @@ __global__ void __launch_bounds__(SPT) k_sp_dinit(Topo t, const uint8_t* tf, con
             st->status = MPP_NOT_CONVERGED;
             st->done = 1;
         }
-        if (use_cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
     }
 }
 
 // q = A d and d.q -> alpha = rho / d.q (src/sflip.jl:1885-1889).
-__global__ void __launch_bounds__(SPT) k_sp_apply_dot(Topo t, Comp L, const uint8_t* tf, const uint8_t* tc,
-                                                      const float* df, const float* dc, float* qf, float* qc,
-                                                      SpState* st, double* partials, unsigned* counter, int gf) {
+__global__ void __launch_bounds__(SPT) k_sp_apply_dot(Topo t, Comp L, const uint16_t* code0, const float* dg0,
+                                                      const uint8_t* tf, const uint8_t* cmask, const float* df,
+                                                      const float* dc, float* qf, float* qc, SpState* st,
+                                                      double* partials, unsigned* counter, int gf) {
+    __shared__ float xs[PCELLS];
     pdl_wait();
     pdl_trigger();
     if (st->done) return;
     double acc[1] = {0.0};
     if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * BCELLS;
-        SP_FINE_LOOP(n, nf, gf) {
-            bool live;
-            const float q = apply_fine(t, L, tf, df, dc, n, live);
-            if (!live) continue;
-            qf[n] = q;
-            if (tf[n] == LIQUID) acc[0] += (double)df[n] * (double)q;
-        }
+        const int sl = (int)blockIdx.x + 1;
+        int w[3];
+        where_of(t, sl, w);
+        if (w[0] >= 0)
+            apply_block(t, code0, dg0, df, dc, sl, w, xs, [&](int64_t n, const float* q, const float* x) {
+                st4(qf + n, make_float4(q[0], q[1], q[2], q[3]));
+                acc[0] += dot4m(make_float4(x[0], x[1], x[2], x[3]), make_float4(q[0], q[1], q[2], q[3]),
+                                ldm4(tf + n), LIQUID);
+            });
     } else {
         const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
         SP_COARSE_LOOP(c, nc, gf) {
             bool cov;
             const float q = apply_coarse(t, L, df, dc, c, cov);
             qc[c] = q;
-            if (tc[c] == LIQUID && !cov) acc[0] += (double)dc[c] * (double)q;
+            if (cmask[c]) acc[0] += (double)dc[c] * (double)q;
         }
     }
     if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
@@ -299,7 +372,16 @@ __global__ void __launch_bounds__(SPT) k_sp_apply_dot(Topo t, Comp L, const uint
 }
 
 // P += alpha d; r_old = r; r -= alpha q; |r| and the exit test (src/sflip.jl:1890-1894).
-__global__ void __launch_bounds__(SPT) k_sp_update(Topo t, const uint8_t* tf, const uint8_t* tc, float* Pf, float* Pc,
+__device__ __forceinline__ float4 upd_piece(float* P, float* r, float* ro, const float* d, const float* q, float a,
+                                            float ma) {
+    const float4 p = ld4(P), dd = ld4(d), r0 = ld4(r), qq = ld4(q);
+    st4(P, make_float4(p.x + a * dd.x, p.y + a * dd.y, p.z + a * dd.z, p.w + a * dd.w));
+    st4(ro, r0);
+    const float4 r1 = make_float4(r0.x + ma * qq.x, r0.y + ma * qq.y, r0.z + ma * qq.z, r0.w + ma * qq.w);
+    st4(r, r1);
+    return r1;
+}
+__global__ void __launch_bounds__(SPT) k_sp_update(Topo t, const uint8_t* tf, const uint8_t* cmask, float* Pf, float* Pc,
                                                    float* rf, float* rc, float* rof, float* roc, const float* df,
                                                    const float* dc, const float* qf, const float* qc, SpState* st,
                                                    double* partials, unsigned* counter, int gf,
@@ -313,25 +395,15 @@ __global__ void __launch_bounds__(SPT) k_sp_update(Topo t, const uint8_t* tf, co
     const float alpha = st->alpha, ma = -alpha;
     double acc[1] = {0.0};
     if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * BCELLS;
-        SP_FINE_LOOP(n, nf, gf) {
-            if (!slot_used(t, (int)(n >> 12) + 1)) continue;
-            Pf[n] += alpha * df[n];
-            const float r0 = rf[n];
-            rof[n] = r0;
-            const float r = r0 + ma * qf[n];
-            rf[n] = r;
-            if (tf[n] == LIQUID) acc[0] += (double)r * (double)r;
-        }
+        const int sl = (int)blockIdx.x + 1;
+        if (slot_used(t, sl)) SP_SLOT_PIECES(n) {
+                const float4 r = upd_piece(Pf + n, rf + n, rof + n, df + n, qf + n, alpha, ma);
+                acc[0] += dot4m(r, r, ldm4(tf + n), LIQUID);
+            }
     } else {
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) {
-            Pc[c] += alpha * dc[c];
-            const float r0 = rc[c];
-            roc[c] = r0;
-            const float r = r0 + ma * qc[c];
-            rc[c] = r;
-            if (coarse_unknown(t, tc, c)) acc[0] += (double)r * (double)r;
+        SP_COARSE_PIECES(c, (int64_t)t.nc[0] * t.nc[1] * t.nc[2] / 4, gf) {
+            const float4 r = upd_piece(Pc + c, rc + c, roc + c, dc + c, qc + c, alpha, ma);
+            acc[0] += dot4m(r, r, ldm4(cmask + c), 1);
         }
     }
     if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
@@ -349,7 +421,7 @@ __global__ void __launch_bounds__(SPT) k_sp_update(Topo t, const uint8_t* tf, co
 }
 
 // rho_new = z.r and z.r_old -> beta = max(0, (rho_new - z.r_old) / rho) (src/sflip.jl:1895-1900).
-__global__ void __launch_bounds__(SPT) k_sp_dot2(Topo t, const uint8_t* tf, const uint8_t* tc, const float* zf,
+__global__ void __launch_bounds__(SPT) k_sp_dot2(Topo t, const uint8_t* tf, const uint8_t* cmask, const float* zf,
                                                  const float* zc, const float* rf, const float* rc, const float* rof,
                                                  const float* roc, SpState* st, double* partials, unsigned* counter,
                                                  int gf) {
@@ -358,18 +430,19 @@ __global__ void __launch_bounds__(SPT) k_sp_dot2(Topo t, const uint8_t* tf, cons
     if (st->done) return;
     double acc[2] = {0.0, 0.0};
     if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * BCELLS;
-        SP_FINE_LOOP(n, nf, gf) {
-            if (!fine_unknown(t, tf, n)) continue;
-            acc[0] += (double)zf[n] * (double)rf[n];
-            acc[1] += (double)zf[n] * (double)rof[n];
-        }
+        const int sl = (int)blockIdx.x + 1;
+        if (slot_used(t, sl)) SP_SLOT_PIECES(n) {
+                const float4 z = ld4(zf + n);
+                const uchar4 m = ldm4(tf + n);
+                acc[0] += dot4m(z, ld4(rf + n), m, LIQUID);
+                acc[1] += dot4m(z, ld4(rof + n), m, LIQUID);
+            }
     } else {
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) {
-            if (!coarse_unknown(t, tc, c)) continue;
-            acc[0] += (double)zc[c] * (double)rc[c];
-            acc[1] += (double)zc[c] * (double)roc[c];
+        SP_COARSE_PIECES(c, (int64_t)t.nc[0] * t.nc[1] * t.nc[2] / 4, gf) {
+            const float4 z = ld4(zc + c);
+            const uchar4 m = ldm4(cmask + c);
+            acc[0] += dot4m(z, ld4(rc + c), m, 1);
+            acc[1] += dot4m(z, ld4(roc + c), m, 1);
         }
     }
     if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0) {
@@ -397,31 +470,33 @@ __global__ void __launch_bounds__(SPT) k_sp_xpby(Topo t, float* df, float* dc, c
     pdl_trigger();
     if (st->done) return;
     const float beta = st->beta;
+    auto piece = [&](float* d, const float* z) {
+        const float4 zz = ld4(z), dd = ld4(d);
+        st4(d, make_float4(zz.x + beta * dd.x, zz.y + beta * dd.y, zz.z + beta * dd.z, zz.w + beta * dd.w));
+    };
     if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * BCELLS;
-        SP_FINE_LOOP(n, nf, gf) {
-            if (!slot_used(t, (int)(n >> 12) + 1)) continue;
-            df[n] = zf[n] + beta * df[n];
-        }
+        const int sl = (int)blockIdx.x + 1;
+        if (slot_used(t, sl)) SP_SLOT_PIECES(n) piece(df + n, zf + n);
     } else {
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) { dc[c] = zc[c] + beta * dc[c]; }
+        SP_COARSE_PIECES(c, (int64_t)t.nc[0] * t.nc[1] * t.nc[2] / 4, gf) piece(dc + c, zc + c);
     }
 }
 
 // ---- the FGMRES fallback's vector passes (src/fgmres.jl:26-92) ----
 // q = A x (apply!)
-__global__ void __launch_bounds__(SPT) k_sp_apply(Topo t, Comp L, const uint8_t* tf, const float* xf, const float* xc,
-                                                  float* qf, float* qc, int gf) {
+__global__ void __launch_bounds__(SPT) k_sp_apply(Topo t, Comp L, const uint16_t* code0, const float* dg0,
+                                                  const float* xf, const float* xc, float* qf, float* qc, int gf) {
+    __shared__ float xs[PCELLS];
     pdl_wait();
     pdl_trigger();
     if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * BCELLS;
-        SP_FINE_LOOP(n, nf, gf) {
-            bool live;
-            const float q = apply_fine(t, L, tf, xf, xc, n, live);
-            if (live) qf[n] = q;
-        }
+        const int sl = (int)blockIdx.x + 1;
+        int w[3];
+        where_of(t, sl, w);
+        if (w[0] < 0) return;
+        apply_block(t, code0, dg0, xf, xc, sl, w, xs, [&](int64_t n, const float* q, const float*) {
+            st4(qf + n, make_float4(q[0], q[1], q[2], q[3]));
+        });
     } else {
         const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
         SP_COARSE_LOOP(c, nc, gf) {
@@ -431,22 +506,18 @@ __global__ void __launch_bounds__(SPT) k_sp_apply(Topo t, Comp L, const uint8_t*
     }
 }
 // a.b over the unknowns (inner), FP64, into *out
-__global__ void __launch_bounds__(SPT) k_sp_dot(Topo t, const uint8_t* tf, const uint8_t* tc, const float* af,
+__global__ void __launch_bounds__(SPT) k_sp_dot(Topo t, const uint8_t* tf, const uint8_t* cmask, const float* af,
                                                 const float* ac, const float* bf, const float* bc, double* out,
                                                 double* partials, unsigned* counter, int gf) {
     pdl_wait();
     pdl_trigger();
     double acc[1] = {0.0};
     if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * BCELLS;
-        SP_FINE_LOOP(n, nf, gf) {
-            if (fine_unknown(t, tf, n)) acc[0] += (double)af[n] * (double)bf[n];
-        }
+        const int sl = (int)blockIdx.x + 1;
+        if (slot_used(t, sl)) SP_SLOT_PIECES(n) acc[0] += dot4m(ld4(af + n), ld4(bf + n), ldm4(tf + n), LIQUID);
     } else {
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) {
-            if (coarse_unknown(t, tc, c)) acc[0] += (double)ac[c] * (double)bc[c];
-        }
+        SP_COARSE_PIECES(c, (int64_t)t.nc[0] * t.nc[1] * t.nc[2] / 4, gf)
+        acc[0] += dot4m(ld4(ac + c), ld4(bc + c), ldm4(cmask + c), 1);
     }
     if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) *out = acc[0];
 }
@@ -455,15 +526,20 @@ __global__ void __launch_bounds__(SPT) k_sp_axpy(Topo t, float* yf, float* yc, f
                                                  const float* xc, int zero, int copy, int gf) {
     pdl_wait();
     pdl_trigger();
-    if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * BCELLS;
-        SP_FINE_LOOP(n, nf, gf) {
-            if (!slot_used(t, (int)(n >> 12) + 1)) continue;
-            yf[n] = copy ? xf[n] : (zero ? 0.0f : yf[n]) + a * xf[n];
+    auto piece = [&](float* y, const float* x) {
+        const float4 xx = ld4(x);
+        if (copy) {
+            st4(y, xx);
+            return;
         }
+        const float4 yy = zero ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4(y);
+        st4(y, make_float4(yy.x + a * xx.x, yy.y + a * xx.y, yy.z + a * xx.z, yy.w + a * xx.w));
+    };
+    if ((int)blockIdx.x < gf) {
+        const int sl = (int)blockIdx.x + 1;
+        if (slot_used(t, sl)) SP_SLOT_PIECES(n) piece(yf + n, xf + n);
     } else {
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) { yc[c] = copy ? xc[c] : (zero ? 0.0f : yc[c]) + a * xc[c]; }
+        SP_COARSE_PIECES(c, (int64_t)t.nc[0] * t.nc[1] * t.nc[2] / 4, gf) piece(yc + c, xc + c);
     }
 }
 
@@ -582,6 +658,9 @@ struct mpp_sparse_ctx {
     int64_t ncc;
     // level 0 operator
     float *cf[3], *cc[3], *dDf, *dDc;
+    uint16_t* code0;    // each fine cell's six couplings, active and LIQUID bits (the block kernels)
+    float* dg0;         // each fine cell's whole diagonal
+    uint8_t* cmask;     // the coarse unknowns (LIQUID, no fine block over them)
     uint8_t* actc;      // = D[0].act
     // level 1
     float *c1[3], *dD1, *x1f, *b1f, *r1f, *t1f, *x1c, *r1c, *t1c;
@@ -651,6 +730,14 @@ Split split_for(const mpp_sparse_ctx* c, int64_t nfine) {
     return s;
 }
 
+// a launch whose fine part is a CTA per slot (the block kernels)
+Split split_blk(const mpp_sparse_ctx* c) {
+    Split s;
+    s.gf = c->t.nslots;
+    s.g = s.gf + cap_blocks(c, c->ncc);
+    return s;
+}
+
 Comp comp0(const mpp_sparse_ctx* c, const uint8_t* tf) {
     Comp L;
     L.cfx = c->cf[0]; L.cfy = c->cf[1]; L.cfz = c->cf[2]; L.dDf = c->dDf; L.actf = tf;
@@ -664,6 +751,8 @@ Comp comp1(const mpp_sparse_ctx* c) {
     return L;
 }
 
+bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
+
 int sp_check_basin(mpp_sparse_ctx* c, const mpp_sparse_basin* b) {
     if (!c || !b || !b->slot || !b->where || !b->types_f || !b->types_c) {
         sp_err("null context or basin arrays");
@@ -671,6 +760,11 @@ int sp_check_basin(mpp_sparse_ctx* c, const mpp_sparse_basin* b) {
     }
     if (b->nslots < 0 || b->nslots > c->capacity) {
         sp_err("nslots %d outside the context's capacity %d", b->nslots, c->capacity);
+        return MPP_ERR_INVALID;
+    }
+    // the vector passes move 16-byte pieces of the pools and the coarse grid
+    if (!aligned(b->P_f, 16) || !aligned(b->P_c, 16) || !aligned(b->types_f, 4)) {
+        sp_err("P_f and P_c must be 16-byte aligned, types_f 4-byte aligned");
         return MPP_ERR_INVALID;
     }
     c->t.slot = b->slot;
@@ -696,7 +790,8 @@ struct SpRun {
         sp_launch(k_sp_coarsecoef, dim3(grid1(mc), 3), SPT, s, t, c->cc[0], c->cc[1], c->cc[2], b->types_c);
         const Split sp = split_for(c, (int64_t)t.nslots * BCELLS);
         sp_launch(k_sp_dirichlet, dim3(sp.g), SPT, s, t, c->dDf, c->dDc, c->actc, b->types_f, b->types_c, b->phi_f,
-                  b->phi_c, sp.gf);
+                  b->phi_c, (const float*)c->cf[0], (const float*)c->cf[1], (const float*)c->cf[2], c->code0, c->dg0,
+                  c->cmask, sp.gf);
         nk += 3;
         hierarchy(b->types_f);
     }
@@ -724,6 +819,21 @@ struct SpRun {
     template <int N>
     void smooth(const Comp& L, float* xf, float* xc, const float* bf, const float* bc, float* tf_, float* tc_,
                 int sweeps, bool from_zero) {
+        if (N == 16) {
+            const Split sp = split_blk(c);
+            for (int q = 0; q < sweeps; q++) {
+                if (q == 0 && from_zero)
+                    sp_launch(k_sp_blk<BOP_JAC_ZS>, dim3(sp.g), SPT, s, c->t, L, (const uint16_t*)c->code0,
+                              (const float*)c->dg0, tf_, tc_, (const float*)xf, (const float*)xc, bf, bc, sp.gf);
+                else
+                    sp_launch(k_sp_blk<BOP_JAC>, dim3(sp.g), SPT, s, c->t, L, (const uint16_t*)c->code0,
+                              (const float*)c->dg0, tf_, tc_, (const float*)xf, (const float*)xc, bf, bc, sp.gf);
+                sp_launch(k_sp_blk<BOP_JAC>, dim3(sp.g), SPT, s, c->t, L, (const uint16_t*)c->code0,
+                          (const float*)c->dg0, xf, xc, (const float*)tf_, (const float*)tc_, bf, bc, sp.gf);
+                nk += 2;
+            }
+            return;
+        }
         const Split sp = split_for(c, (int64_t)c->t.nslots * Lv<N>::CELLS);
         for (int q = 0; q < sweeps; q++) {
             if (q == 0 && from_zero)
@@ -754,8 +864,9 @@ struct SpRun {
         const Comp L0 = comp0(c, tf), L1 = comp1(c);
         const Split s0 = split_for(c, (int64_t)t.nslots * BCELLS), s1 = split_for(c, (int64_t)t.nslots * BCELLS1);
         smooth<16>(L0, zf, zc, rf, rc, c->tmf, c->tmc, sweeps, true);
-        sp_launch(k_sp_residual<16>, dim3(s0.g), SPT, s, t, L0, c->res0f, c->res0c, (const float*)zf,
-                  (const float*)zc, rf, rc, s0.gf);
+        const Split sb = split_blk(c);
+        sp_launch(k_sp_blk<BOP_RES>, dim3(sb.g), SPT, s, t, L0, (const uint16_t*)c->code0, (const float*)c->dg0,
+                  c->res0f, c->res0c, (const float*)zf, (const float*)zc, rf, rc, sb.gf);
         sp_launch(k_sp_restrict01, dim3(grid1((int64_t)t.nslots * BCELLS1)), SPT, s, t, c->b1f,
                   (const float*)c->res0f);
         nk += 2;
@@ -798,24 +909,26 @@ struct SpRun {
                      int use_cond) {
         const Topo& t = c->t;
         const Comp L0 = comp0(c, b->types_f);
-        const Split s0 = split_for(c, (int64_t)t.nslots * BCELLS);
-        sp_launch(k_sp_start, dim3(s0.g), SPT, s, t, L0, b->types_f, b->types_c, (const float*)b->P_f,
-                  (const float*)b->P_c, (const float*)c->bf, (const float*)c->bc, c->rf, c->rc, c->st, c->partials,
-                  c->counters + SCNT_START, s0.gf, cond, 0);
+        const Split s0 = split_blk(c);
+        sp_launch(k_sp_start, dim3(s0.g), SPT, s, t, L0, (const uint16_t*)c->code0, (const float*)c->dg0,
+                  b->types_f, (const uint8_t*)c->cmask, (const float*)b->P_f, (const float*)b->P_c,
+                  (const float*)c->bf, (const float*)c->bc, c->rf, c->rc, c->st, c->partials,
+                  c->counters + SCNT_START, s0.gf);
         vcycle(b->types_f, c->zf, c->zc, c->rf, c->rc, o->sweeps, o->coarse, o->boost);
-        sp_launch(k_sp_dinit, dim3(s0.g), SPT, s, t, b->types_f, b->types_c, (const float*)c->zf,
+        sp_launch(k_sp_dinit, dim3(s0.g), SPT, s, t, b->types_f, (const uint8_t*)c->cmask, (const float*)c->zf,
                   (const float*)c->zc, (const float*)c->rf, (const float*)c->rc, c->df, c->dc, c->st, c->partials,
-                  c->counters + SCNT_INIT, s0.gf, cond, 0);
+                  c->counters + SCNT_INIT, s0.gf);
         nk += 2;
         cg_step(b, cond, use_cond);
     }
     void cg_step(const mpp_sparse_basin* b, cudaGraphConditionalHandle cond, int use_cond) {
         const Topo& t = c->t;
         const Comp L0 = comp0(c, b->types_f);
-        const Split s0 = split_for(c, (int64_t)t.nslots * BCELLS);
-        sp_launch(k_sp_apply_dot, dim3(s0.g), SPT, s, t, L0, b->types_f, b->types_c, (const float*)c->df,
-                  (const float*)c->dc, c->qf, c->qc, c->st, c->partials, c->counters + SCNT_DQ, s0.gf);
-        sp_launch(k_sp_update, dim3(s0.g), SPT, s, t, b->types_f, b->types_c, b->P_f, b->P_c, c->rf, c->rc, c->rof,
+        const Split s0 = split_blk(c);
+        sp_launch(k_sp_apply_dot, dim3(s0.g), SPT, s, t, L0, (const uint16_t*)c->code0, (const float*)c->dg0,
+                  b->types_f, (const uint8_t*)c->cmask, (const float*)c->df, (const float*)c->dc, c->qf, c->qc, c->st,
+                  c->partials, c->counters + SCNT_DQ, s0.gf);
+        sp_launch(k_sp_update, dim3(s0.g), SPT, s, t, b->types_f, (const uint8_t*)c->cmask, b->P_f, b->P_c, c->rf, c->rc, c->rof,
                   c->roc, (const float*)c->df, (const float*)c->dc, (const float*)c->qf, (const float*)c->qc, c->st,
                   c->partials, c->counters + SCNT_UPD, s0.gf, cond, use_cond);
         nk += 2;
@@ -823,9 +936,9 @@ struct SpRun {
     // the rotated loop body: the V-cycle of the new residual, beta, d, then q, alpha, the update
     void cg_body(const mpp_sparse_basin* b, const mpp_sparse_opts* o, cudaGraphConditionalHandle cond, int use_cond) {
         const Topo& t = c->t;
-        const Split s0 = split_for(c, (int64_t)t.nslots * BCELLS);
+        const Split s0 = split_blk(c);
         vcycle(b->types_f, c->zf, c->zc, c->rf, c->rc, o->sweeps, o->coarse, o->boost);
-        sp_launch(k_sp_dot2, dim3(s0.g), SPT, s, t, b->types_f, b->types_c, (const float*)c->zf, (const float*)c->zc,
+        sp_launch(k_sp_dot2, dim3(s0.g), SPT, s, t, b->types_f, (const uint8_t*)c->cmask, (const float*)c->zf, (const float*)c->zc,
                   (const float*)c->rf, (const float*)c->rc, (const float*)c->rof, (const float*)c->roc, c->st,
                   c->partials, c->counters + SCNT_DOT2, s0.gf);
         sp_launch(k_sp_xpby, dim3(s0.g), SPT, s, t, c->df, c->dc, (const float*)c->zf, (const float*)c->zc,
@@ -856,8 +969,9 @@ int read_state(mpp_sparse_ctx* c, cudaStream_t s) {
 // a dot product over the unknowns, read back (FGMRES)
 int dot_host(mpp_sparse_ctx* c, SpRun& run, const uint8_t* tf, const uint8_t* tc, const float* af, const float* ac,
              const float* bf, const float* bc, float* out) {
-    const Split s0 = split_for(c, (int64_t)c->t.nslots * BCELLS);
-    sp_launch(k_sp_dot, dim3(s0.g), SPT, run.s, c->t, tf, tc, af, ac, bf, bc, c->dres, c->partials,
+    const Split s0 = split_blk(c);
+    (void)tc;
+    sp_launch(k_sp_dot, dim3(s0.g), SPT, run.s, c->t, tf, (const uint8_t*)c->cmask, af, ac, bf, bc, c->dres, c->partials,
               c->counters + SCNT_DOT, s0.gf);
     run.nk++;
     SCK(cudaMemcpyAsync(c->dres_host, c->dres, sizeof(double), cudaMemcpyDeviceToHost, run.s));
@@ -867,13 +981,14 @@ int dot_host(mpp_sparse_ctx* c, SpRun& run, const uint8_t* tf, const uint8_t* tc
 }
 void axpy(mpp_sparse_ctx* c, SpRun& run, float* yf, float* yc, float a, const float* xf, const float* xc, int zero,
           int copy) {
-    const Split s0 = split_for(c, (int64_t)c->t.nslots * BCELLS);
+    const Split s0 = split_blk(c);
     sp_launch(k_sp_axpy, dim3(s0.g), SPT, run.s, c->t, yf, yc, a, xf, xc, zero, copy, s0.gf);
     run.nk++;
 }
 void apply_(mpp_sparse_ctx* c, SpRun& run, const uint8_t* tf, const float* xf, const float* xc, float* qf, float* qc) {
-    const Split s0 = split_for(c, (int64_t)c->t.nslots * BCELLS);
-    sp_launch(k_sp_apply, dim3(s0.g), SPT, run.s, c->t, comp0(c, tf), tf, xf, xc, qf, qc, s0.gf);
+    const Split s0 = split_blk(c);
+    sp_launch(k_sp_apply, dim3(s0.g), SPT, run.s, c->t, comp0(c, tf), (const uint16_t*)c->code0, (const float*)c->dg0,
+              xf, xc, qf, qc, s0.gf);
     run.nk++;
 }
 
@@ -935,10 +1050,10 @@ int fgmres(mpp_sparse_ctx* c, SpRun& run, const mpp_sparse_basin* b, const mpp_s
         for (int j = 0; j < jmax; j++) {
             run.vcycle(tf, c->zf, c->zc, c->Vf[j], c->Vc[j], o->sweeps, o->coarse, o->boost);
             // the diagonal component: one damped Jacobi step from zero (src/fgmres.jl:15-24)
-            const Split s0 = split_for(c, (int64_t)c->t.nslots * BCELLS);
-            sp_launch(k_sp_jacobi<16, true>, dim3(s0.g), SPT, run.s, c->t, comp0(c, tf), c->Zf[j], c->Zc[j],
-                      (const float*)nullptr, (const float*)nullptr, (const float*)c->Vf[j], (const float*)c->Vc[j],
-                      s0.gf);
+            const Split s0 = split_blk(c);
+            sp_launch(k_sp_blk<BOP_JAC_ZS>, dim3(s0.g), SPT, run.s, c->t, comp0(c, tf), (const uint16_t*)c->code0,
+                      (const float*)c->dg0, c->Zf[j], c->Zc[j], (const float*)nullptr, (const float*)nullptr,
+                      (const float*)c->Vf[j], (const float*)c->Vc[j], s0.gf);
             run.nk++;
             axpy(c, run, c->Zf[j], c->Zc[j], 1.0f, c->zf, c->zc, 0, 0);
             apply_(c, run, tf, c->Zf[j], c->Zc[j], c->qf, c->qc);
@@ -1192,6 +1307,9 @@ int mpp_sparse_ctx_create(mpp_sparse_ctx** out, const mpp_sparse_grid* g, int32_
     for (auto p : lev1)
         if (!e) e = sp_alloc_n(c, p, n1);
     if (!e) e = sp_alloc_n(c, &c->act1, n1);
+    if (!e) e = sp_alloc_n(c, &c->code0, nf);
+    if (!e) e = sp_alloc_n(c, &c->dg0, nf);
+    if (!e) e = sp_alloc_n(c, &c->cmask, c->ncc);
     int m[3] = {c->t.nc[0], c->t.nc[1], c->t.nc[2]};
     for (int l = 0; l < nd && !e; l++) {
         DL& D = c->D[l];
@@ -1276,6 +1394,10 @@ int mpp_sparse_operator(mpp_sparse_ctx* c, const mpp_sparse_basin* b, mpp_stream
 int mpp_sparse_apply(mpp_sparse_ctx* c, const mpp_sparse_basin* b, const float* xf, const float* xc, float* qf,
                      float* qc, mpp_stream stream) {
     if (int e = sp_check_basin(c, b)) return e;
+    if (!aligned(xf, 16) || !aligned(xc, 16) || !aligned(qf, 16) || !aligned(qc, 16)) {
+        sp_err("x and q must be 16-byte aligned");
+        return MPP_ERR_INVALID;
+    }
     SpRun run{c, (cudaStream_t)stream};
     apply_(c, run, b->types_f, xf, xc, qf, qc);
     return finish(c, run, nullptr, MPP_OK);
@@ -1286,6 +1408,10 @@ int mpp_sparse_vcycle(mpp_sparse_ctx* c, const mpp_sparse_basin* b, const float*
     if (int e = sp_check_basin(c, b)) return e;
     if (sweeps < 1 || coarse < 0) {
         sp_err("sweeps must be >= 1 and coarse >= 0");
+        return MPP_ERR_INVALID;
+    }
+    if (!aligned(rf, 16) || !aligned(rc, 16) || !aligned(zf, 16) || !aligned(zc, 16)) {
+        sp_err("r and z must be 16-byte aligned");
         return MPP_ERR_INVALID;
     }
     SpRun run{c, (cudaStream_t)stream};

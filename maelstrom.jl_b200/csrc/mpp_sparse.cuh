@@ -388,8 +388,17 @@ __global__ void __launch_bounds__(SPT) k_sp_coarsecoef(Topo t, float* cu, float*
 }
 // finedirichlet_kernel! (:1356-1374) + coarsedirichlet_kernel! (:1376-1407) +
 // activecoarse_kernel! (:1315-1319), one launch (fine part first)
+//
+// The fine part also packs each cell's six couplings for the block kernels (code0: 2 bits a
+// face in finerow's order -x, +x, -y, +y, -z, +z: 0 none, 1 FINE_COARSE, 2 FINE_FINE; bit 12
+// active (not SOLID), bit 13 LIQUID) and its whole diagonal dg0 = dD + the positive
+// couplings, added in finerow's order (the same Float32 sums finerow forms every sweep); the
+// coarse part marks the coarse unknowns (LIQUID, no fine block over them) for the dots.
+__device__ __forceinline__ unsigned ccode(float c) { return c == FINE_FINE ? 2u : (c == FINE_COARSE ? 1u : 0u); }
 __global__ void __launch_bounds__(SPT) k_sp_dirichlet(Topo t, float* dDf, float* dDc, uint8_t* actc, const uint8_t* tf,
-                                                      const uint8_t* tc, const float* phif, const float* phic, int gf) {
+                                                      const uint8_t* tc, const float* phif, const float* phic,
+                                                      const float* cfx, const float* cfy, const float* cfz,
+                                                      uint16_t* code0, float* dg0, uint8_t* cmask, int gf) {
     pdl_wait();
     pdl_trigger();
     if ((int)blockIdx.x < gf) {
@@ -414,6 +423,18 @@ __global__ void __launch_bounds__(SPT) k_sp_dirichlet(Topo t, float* dDf, float*
                 }
             }
             dDf[n] = d;
+            const float c6[6] = {cfx[L16::face(sl, 1, i, j, k) - 1], cfx[L16::face(sl, 1, i + 1, j, k) - 1],
+                                 cfy[L16::face(sl, 2, i, j, k) - 1], cfy[L16::face(sl, 2, i, j + 1, k) - 1],
+                                 cfz[L16::face(sl, 3, i, j, k) - 1], cfz[L16::face(sl, 3, i, j, k + 1) - 1]};
+            float dg = d;
+            unsigned code = (tf[n] != SOLID ? 1u << 12 : 0u) | (tf[n] == LIQUID ? 1u << 13 : 0u);
+#pragma unroll
+            for (int m = 0; m < 6; m++) {
+                if (c6[m] > 0.0f) dg += c6[m];
+                code |= ccode(c6[m]) << (2 * m);
+            }
+            code0[n] = (uint16_t)code;
+            dg0[n] = dg;
         }
     } else {
         const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
@@ -447,6 +468,7 @@ __global__ void __launch_bounds__(SPT) k_sp_dirichlet(Topo t, float* dDf, float*
             }
             dDc[c] = d;
             actc[c] = (tc[c] == LIQUID && !cov) ? 1 : 0;
+            cmask[c] = actc[c];
         }
     }
 }
@@ -873,6 +895,123 @@ __device__ __forceinline__ float apply_coarse(const Topo& t, const Comp& L, cons
     float diag, off;
     coarserow<16, false>(t, L, xf, xc, I, J, K, diag, off);
     return diag * xc[c] - off;
+}
+
+
+// ---- level 0's fine part, a CTA per 16^3 block ----
+// The level's stencil passes (Jacobi sweeps, the residual, apply!) run one CTA per slot:
+// the block's x (4096 cells, 16-byte loads) and its one-cell halo (6 x 256 cells: the
+// neighbouring block's boundary plane where that block is fine, else the coarse cell the
+// halo cell lies in, as finerow's neighbourvalue) are staged in shared memory; each thread
+// then takes four consecutive cells of a row four times, reading their codes (code0: the six
+// couplings, 2 bits each, and the active and LIQUID bits), whole diagonals (dg0) and right-
+// hand sides as 8- and 16-byte loads and their neighbours from shared memory. Per cell the
+// arithmetic is finerow's: off sums c x_n over the positive couplings in the order -x, +x,
+// -y, +y, -z, +z, and diag is dg0, the same Float32 sums.
+constexpr int PX = 18, PXY = PX * PX, PCELLS = PXY * PX;  // the staged block with its halo
+__device__ __forceinline__ int pidx(int i, int j, int k) { return (k + 1) * PXY + (j + 1) * PX + (i + 1); }
+__device__ __forceinline__ float cdec(unsigned code, int m) {
+    const unsigned v = (code >> (2 * m)) & 3u;
+    return v == 2u ? FINE_FINE : (v == 1u ? FINE_COARSE : 0.0f);
+}
+
+// Stage slot sl's x and its halo into xs (256 threads).
+__device__ __forceinline__ void stage_block(const Topo& t, const float* __restrict__ x, const float* __restrict__ xc,
+                                            int sl, const int w[3], float* xs) {
+    const int tid = (int)threadIdx.x;
+    const float4* x4 = reinterpret_cast<const float4*>(x + (int64_t)(sl - 1) * BCELLS);
+    float4 v[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) v[m] = x4[tid + 256 * m];
+    const int p = tid & 15, q = tid >> 4;
+    float hv[6];
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        const int ax = f >> 1, sg = (f & 1) ? 1 : -1;
+        const int i = ax == 0 ? (sg < 0 ? -1 : 16) : p;
+        const int j = ax == 1 ? (sg < 0 ? -1 : 16) : (ax == 0 ? p : q);
+        const int k = ax == 2 ? (sg < 0 ? -1 : 16) : q;
+        const int nbi = w[0] + (ax == 0 ? sg : 0), nbj = w[1] + (ax == 1 ? sg : 0), nbk = w[2] + (ax == 2 ? sg : 0);
+        const int s2 = inblocks(t, nbi, nbj, nbk) ? blockslot(t, nbi, nbj, nbk) : 0;
+        if (s2 > 0) {
+            hv[f] = x[(int64_t)(s2 - 1) * BCELLS + (i & 15) + 16 * ((j & 15) + 16 * (k & 15))];
+        } else {
+            const int I = w[0] * BLOCK + i, J = w[1] * BLOCK + j, K = w[2] * BLOCK + k;
+            hv[f] = xc[coarse_clamped(t, I >> 2, J >> 2, K >> 2)];
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const int c = 4 * (tid + 256 * m), i = c & 15, j = (c >> 4) & 15, k = c >> 8;
+        float* d = xs + pidx(i, j, k);
+        d[0] = v[m].x;
+        d[1] = v[m].y;
+        d[2] = v[m].z;
+        d[3] = v[m].w;
+    }
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        const int ax = f >> 1, sg = (f & 1) ? 1 : -1;
+        const int i = ax == 0 ? (sg < 0 ? -1 : 16) : p;
+        const int j = ax == 1 ? (sg < 0 ? -1 : 16) : (ax == 0 ? p : q);
+        const int k = ax == 2 ? (sg < 0 ? -1 : 16) : q;
+        xs[pidx(i, j, k)] = hv[f];
+    }
+}
+
+// off of one cell from the staged block (ZS: x all zeros, off = 0).
+template <bool ZS>
+__device__ __forceinline__ float block_off(const float* xs, int o, unsigned code) {
+    float off = 0.0f;
+    if (ZS) return off;
+    const int nb[6] = {-1, 1, -PX, PX, -PXY, PXY};
+#pragma unroll
+    for (int m = 0; m < 6; m++) {
+        const float c = cdec(code, m);
+        if (c > 0.0f) off += c * xs[o + nb[m]];
+    }
+    return off;
+}
+
+// The block operations: a Jacobi sweep (from x, or from zeros), the residual, and A x.
+enum { BOP_JAC = 0, BOP_JAC_ZS = 1, BOP_RES = 2, BOP_APPLY = 3 };
+
+// One slot's cells through `op`; `sink(n, value, x)` receives each cell's result (pool
+// index, value, the cell's own x). The caller has staged x into xs (not for BOP_JAC_ZS).
+template <int OP, class Sink>
+__device__ __forceinline__ void block_cells(const uint16_t* __restrict__ code0, const float* __restrict__ dg0,
+                                            const float* __restrict__ b, const float* xs, int sl, Sink&& sink) {
+    const int tid = (int)threadIdx.x;
+#pragma unroll 1
+    for (int m = 0; m < 4; m++) {
+        const int q = tid + 256 * m, c = 4 * q, i = c & 15, j = (c >> 4) & 15, k = c >> 8;
+        const int64_t n = (int64_t)(sl - 1) * BCELLS + c;
+        const ushort4 cd = *reinterpret_cast<const ushort4*>(code0 + n);
+        const float4 dg = *reinterpret_cast<const float4*>(dg0 + n);
+        float4 bb = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (OP != BOP_APPLY) bb = *reinterpret_cast<const float4*>(b + n);
+        const unsigned cs[4] = {cd.x, cd.y, cd.z, cd.w};
+        const float ds[4] = {dg.x, dg.y, dg.z, dg.w}, bs[4] = {bb.x, bb.y, bb.z, bb.w};
+        float out[4], xv[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int o = pidx(i + u, j, k);
+            const unsigned code = cs[u];
+            const float x0 = OP == BOP_JAC_ZS ? 0.0f : xs[o];
+            xv[u] = x0;
+            const float diag = ds[u];
+            float v = 0.0f;
+            if (OP == BOP_APPLY) {
+                if (code & (1u << 13)) v = diag * x0 - block_off<false>(xs, o, code);
+            } else if (code & (1u << 12)) {
+                const float off = OP == BOP_JAC_ZS ? block_off<true>(xs, o, code) : block_off<false>(xs, o, code);
+                if (OP == BOP_RES) v = bs[u] - (diag * x0 - off);
+                else v = diag > 0.0f ? x0 + OMEGA * (bs[u] - (diag * x0 - off)) / diag : 0.0f;
+            }
+            out[u] = v;
+        }
+        sink(n, out, xv);
+    }
 }
 
 }  // namespace sp
