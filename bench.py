@@ -445,6 +445,8 @@ def run_mpp(args):
         out["extrapolate"] = bench_extrapolate(max(3, min(args.steps, 10)))
         torch.cuda.empty_cache()
         out["levelset"] = bench_levelset(max(3, min(args.steps, 10)))
+        torch.cuda.empty_cache()
+        out["sparse"] = bench_sparse(max(3, min(args.steps, 10)), cpu=not args.no_cpu)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(basin, max_seconds=args.cpu_seconds)
     if rank == 0:
@@ -754,6 +756,90 @@ def bench_levelset(steps):
             "filltrapped_ms": round(ms_f, 4), "filltrapped_rounds": rounds, "cells_filled": filled,
             "filltrapped_gbs": round(bytes_f / (ms_f / 1e3) / 1e9, 1), "peak_gbs": hbm, "peak_source": src,
             "steps": steps}
+
+
+def bench_sparse(steps, cpu=True):
+    """The sparse two-resolution basin's project! (src/sflip.jl:1998-2018): the seeded
+    whirlpool of mpp.sparse_scene.charybdis, 32 x 32 x 16 blocks of 16^3 cells (a 512 x 512 x
+    256 fine-cell box over a 128 x 128 x 64 coarse grid), 2948 fine blocks along the funnel
+    (12.1 M fine cells, 5.1 M of them water), in the reference's Float32 arithmetic with
+    pressure!'s defaults (tol 1e-4, one sweep pair, boost 1), the CG loop one graph launch.
+    Each call restores P and the velocities outside its CUDA events. Beside it: the level-0
+    stencil pass (apply!: the composite operator over every fine block and the coarse grid,
+    one launch) timed alone, its achieved GB/s on the bytes it must move (a fine cell of the
+    slots in use: x 4, packed couplings 2, diagonal 4, q 4; a coarse cell: activity 1 and q 4,
+    and for an active one x 4, b-side diagonal 4 and six couplings 24), and the CPU oracle's
+    projection of the same basin on the host's threads."""
+    import numpy as np
+    import torch
+
+    from mpp import sparse as msp
+    from mpp import sparse_scene as ss
+
+    sc = ss.charybdis()
+    s = msp.SparseBasin.from_scene(sc, graph=True, tol=1e-4, maxiter=200)
+    saved = {k: getattr(s, k).clone() for k in ("Pf", "Pc", "uf", "uc", "vf", "vc", "wf", "wc")}
+
+    def call():
+        for k, v in saved.items():
+            getattr(s, k).copy_(v)
+        e0, e1 = _events()
+        e0.record()
+        msp.project(s, DT)
+        e1.record()
+        return e0, e1
+
+    for _ in range(3):
+        call()
+    ev = [call() for _ in range(steps)]
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+    its = s.iterations[-1]
+    # the level-0 stencil pass alone
+    used = int((sc.where[:, 0] >= 0).sum())
+    fine_u = (sc.tf == 1) & np.repeat(sc.where[:, 0] >= 0, 4096)
+    ncc = int(np.prod(sc.grid.nc))
+    rng = np.random.default_rng(5)
+    xf = torch.from_numpy(np.where(fine_u, rng.standard_normal(fine_u.size), 0).astype(np.float32)).cuda()
+    xc = torch.from_numpy(np.where(sc.tc == 1, rng.standard_normal(ncc), 0).astype(np.float32)).cuda()
+    qf, qc = torch.empty_like(xf), torch.empty_like(xc)
+    s.operator()
+    cact = int(s.read("act_c").astype(bool).sum())
+    for _ in range(3):
+        s.apply(xf, xc, qf, qc)
+    n_apply = 20
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(n_apply):
+        s.apply(xf, xc, qf, qc)
+    e1.record()
+    torch.cuda.synchronize()
+    apply_ms = e0.elapsed_time(e1) / n_apply
+    nbytes = used * 4096 * 14 + ncc * 5 + cact * 32
+    hbm, src = peaks()
+    out = {"workload": "sparse whirlpool (charybdis): 32x32x16 blocks, 2948 fine blocks, coarse 128x128x64, tol 1e-4",
+           "fine_blocks": used, "fine_cells": used * 4096, "fine_water_cells": int(fine_u.sum()),
+           "coarse_cells": ncc, "ms_per_projection": round(ms, 3), "projections_per_s": round(1e3 / ms, 2),
+           "iterations": its, "rel_residual": s.last.rel_residual, "graph": True,
+           "kernel_launches": int(s.last.kernel_launches),
+           "apply_pass": {"ms": round(apply_ms, 4), "algorithmic_bytes": nbytes,
+                          "achieved_gbs": round(nbytes / (apply_ms / 1e3) / 1e9, 1), "peak_gbs": hbm,
+                          "frac": round(nbytes / (apply_ms / 1e3) / 1e9 / hbm, 4), "peak_source": src},
+           "steps": steps}
+    del s
+    torch.cuda.empty_cache()
+    if cpu:
+        import oracle
+        from oracle import sparse as osp
+
+        vol = osp.volume(sc)
+        t0 = time.perf_counter()
+        info = osp.project(sc.copy(), vol, tol=1e-4, maxiter=200)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_oracle"] = {"ms_per_projection": round(cpu_s * 1e3, 1), "iterations": info["iterations"],
+                             "threads": oracle.num_threads(), "kind": "port",
+                             "sample": "one projection of the same basin by the C/OpenMP oracle"}
+    return out
 
 
 def bench_whirlpool(steps):

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(SPT) k_sp_volume(Topo t, const float* phif, co
     pdl_wait();
     pdl_trigger();
     double acc[2] = {0.0, 0.0};
-    if ((int)blockIdx.x < gf) {
+    if (sp_is_fine(gf)) {
         const int64_t nf = (int64_t)t.nslots * BCELLS;
         SP_FINE_LOOP(n, nf, gf) {
             int sl, i, j, k;
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(SPT) k_sp_rhs(Topo t, const uint8_t* tf, const
     pdl_trigger();
     const float gamma = st ? st->gamma : gamma_arg;
     const float h = t.dx;
-    if ((int)blockIdx.x < gf) {
+    if (sp_is_fine(gf)) {
         const int64_t nf = (int64_t)t.nslots * BCELLS;
         SP_FINE_LOOP(n, nf, gf) {
             int sl, i, j, k;
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(SPT) k_sp_rhs(Topo t, const uint8_t* tf, const
     for (int m_ = 0; m_ < 4; m_++)                                                          \
         if (const int64_t n = (int64_t)(sl - 1) * BCELLS + 4 * ((int)threadIdx.x + 256 * m_); true)
 #define SP_COARSE_PIECES(c, nc4, gf)                                                        \
-    for (int64_t c = 4 * ((int64_t)(blockIdx.x - (gf)) * blockDim.x + threadIdx.x); c < 4 * (nc4);   \
+    for (int64_t c = 4 * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x); c < 4 * (nc4);        \
          c += 4 * (int64_t)(gridDim.x - (gf)) * blockDim.x)
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
@@ -190,8 +190,8 @@ __global__ void __launch_bounds__(SPT) k_sp_blk(Topo t, Comp L, const uint16_t* 
     __shared__ float xs[PCELLS];
     pdl_wait();
     pdl_trigger();
-    if ((int)blockIdx.x < gf) {
-        const int sl = (int)blockIdx.x + 1;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
         int w[3];
         where_of(t, sl, w);
         if (w[0] < 0) return;
@@ -240,8 +240,8 @@ __global__ void __launch_bounds__(SPT) k_sp_start(Topo t, Comp L, const uint16_t
     pdl_wait();
     pdl_trigger();
     double acc[2] = {0.0, 0.0};
-    if ((int)blockIdx.x < gf) {
-        const int sl = (int)blockIdx.x + 1;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
         int w[3];
         where_of(t, sl, w);
         if (w[0] >= 0)
@@ -295,8 +295,8 @@ __global__ void __launch_bounds__(SPT) k_sp_dinit(Topo t, const uint8_t* tf, con
     pdl_trigger();
     if (st->done) return;
     double acc[1] = {0.0};
-    if ((int)blockIdx.x < gf) {
-        const int sl = (int)blockIdx.x + 1;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
         if (slot_used(t, sl)) SP_SLOT_PIECES(n) {
                 const float4 z = ld4(zf + n);
                 st4(df + n, z);
@@ -335,8 +335,8 @@ __global__ void __launch_bounds__(SPT) k_sp_apply_dot(Topo t, Comp L, const uint
     pdl_trigger();
     if (st->done) return;
     double acc[1] = {0.0};
-    if ((int)blockIdx.x < gf) {
-        const int sl = (int)blockIdx.x + 1;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
         int w[3];
         where_of(t, sl, w);
         if (w[0] >= 0)
@@ -394,8 +394,8 @@ __global__ void __launch_bounds__(SPT) k_sp_update(Topo t, const uint8_t* tf, co
     }
     const float alpha = st->alpha, ma = -alpha;
     double acc[1] = {0.0};
-    if ((int)blockIdx.x < gf) {
-        const int sl = (int)blockIdx.x + 1;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
         if (slot_used(t, sl)) SP_SLOT_PIECES(n) {
                 const float4 r = upd_piece(Pf + n, rf + n, rof + n, df + n, qf + n, alpha, ma);
                 acc[0] += dot4m(r, r, ldm4(tf + n), LIQUID);
@@ -429,8 +429,8 @@ __global__ void __launch_bounds__(SPT) k_sp_dot2(Topo t, const uint8_t* tf, cons
     pdl_trigger();
     if (st->done) return;
     double acc[2] = {0.0, 0.0};
-    if ((int)blockIdx.x < gf) {
-        const int sl = (int)blockIdx.x + 1;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
         if (slot_used(t, sl)) SP_SLOT_PIECES(n) {
                 const float4 z = ld4(zf + n);
                 const uchar4 m = ldm4(tf + n);
@@ -474,11 +474,44 @@ __global__ void __launch_bounds__(SPT) k_sp_xpby(Topo t, float* df, float* dc, c
         const float4 zz = ld4(z), dd = ld4(d);
         st4(d, make_float4(zz.x + beta * dd.x, zz.y + beta * dd.y, zz.z + beta * dd.z, zz.w + beta * dd.w));
     };
-    if ((int)blockIdx.x < gf) {
-        const int sl = (int)blockIdx.x + 1;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
         if (slot_used(t, sl)) SP_SLOT_PIECES(n) piece(df + n, zf + n);
     } else {
         SP_COARSE_PIECES(c, (int64_t)t.nc[0] * t.nc[1] * t.nc[2] / 4, gf) piece(dc + c, zc + c);
+    }
+}
+
+// prolong10fine_kernel! + prolongcoarse_kernel! (src/sflip.jl:1695-1705): level 1's correction
+// added to level 0's LIQUID fine cells, each from the level-1 cell it lies in (a piece of four
+// cells of a row reads two), and to the active coarse cells outside fine blocks.
+__global__ void __launch_bounds__(SPT) k_sp_prolong10(Topo t, float* zf, float* zc, const float* x1f, const float* x1c,
+                                                      const uint8_t* tf, const uint8_t* act2, float boost, int gf) {
+    pdl_wait();
+    pdl_trigger();
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
+        if (!slot_used(t, sl)) return;
+        SP_SLOT_PIECES(n) {
+            const int c = (int)(n - (int64_t)(sl - 1) * BCELLS), i0 = c & 15, j = (c >> 4) & 15, k = c >> 8;
+            const int64_t b1 = (int64_t)(sl - 1) * BCELLS1 + (i0 >> 1) + 8 * ((j >> 1) + 8 * (k >> 1));
+            const float xa = x1f[b1], xb = x1f[b1 + 1];
+            const uchar4 m = ldm4(tf + n);
+            float4 z = ld4(zf + n);
+            if (m.x == LIQUID) z.x += boost * xa;
+            if (m.y == LIQUID) z.y += boost * xa;
+            if (m.z == LIQUID) z.z += boost * xb;
+            if (m.w == LIQUID) z.w += boost * xb;
+            st4(zf + n, z);
+        }
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            if (act2[c] == 0) continue;
+            int I, J, K;
+            coarse_cell(t, c, I, J, K);
+            if (!covered(t, I, J, K)) zc[c] += boost * x1c[c];
+        }
     }
 }
 
@@ -489,8 +522,8 @@ __global__ void __launch_bounds__(SPT) k_sp_apply(Topo t, Comp L, const uint16_t
     __shared__ float xs[PCELLS];
     pdl_wait();
     pdl_trigger();
-    if ((int)blockIdx.x < gf) {
-        const int sl = (int)blockIdx.x + 1;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
         int w[3];
         where_of(t, sl, w);
         if (w[0] < 0) return;
@@ -512,8 +545,8 @@ __global__ void __launch_bounds__(SPT) k_sp_dot(Topo t, const uint8_t* tf, const
     pdl_wait();
     pdl_trigger();
     double acc[1] = {0.0};
-    if ((int)blockIdx.x < gf) {
-        const int sl = (int)blockIdx.x + 1;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
         if (slot_used(t, sl)) SP_SLOT_PIECES(n) acc[0] += dot4m(ld4(af + n), ld4(bf + n), ldm4(tf + n), LIQUID);
     } else {
         SP_COARSE_PIECES(c, (int64_t)t.nc[0] * t.nc[1] * t.nc[2] / 4, gf)
@@ -535,8 +568,8 @@ __global__ void __launch_bounds__(SPT) k_sp_axpy(Topo t, float* yf, float* yc, f
         const float4 yy = zero ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4(y);
         st4(y, make_float4(yy.x + a * xx.x, yy.y + a * xx.y, yy.z + a * xx.z, yy.w + a * xx.w));
     };
-    if ((int)blockIdx.x < gf) {
-        const int sl = (int)blockIdx.x + 1;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
         if (slot_used(t, sl)) SP_SLOT_PIECES(n) piece(yf + n, xf + n);
     } else {
         SP_COARSE_PIECES(c, (int64_t)t.nc[0] * t.nc[1] * t.nc[2] / 4, gf) piece(yc + c, xc + c);
@@ -606,7 +639,8 @@ __global__ void __launch_bounds__(SPT) k_sp_project_coarse(Topo t, float* uf, fl
     const float cdx = (float)RATIO * t.dx;
     const int64_t nfc = (int64_t)f0 * f1 * f2;
     for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < nfc; o += (int64_t)gridDim.x * blockDim.x) {
-        const int I = (int)(o % f0), J = (int)((o / f0) % f1), K = (int)(o / ((int64_t)f0 * f1));
+        int I, J, K;
+            split3(o, f0, f1, I, J, K);
         const int Im = I - e0, Jm = J - e1, Km = K - e2;
         const bool inside = 0 <= Im && 0 <= Jm && 0 <= Km && I < n1 && J < n2 && K < n3;
         if (inside && !covered(t, I, J, K) && !covered(t, Im, Jm, Km)) {
@@ -663,7 +697,7 @@ struct mpp_sparse_ctx {
     uint8_t* cmask;     // the coarse unknowns (LIQUID, no fine block over them)
     uint8_t* actc;      // = D[0].act
     // level 1
-    float *c1[3], *dD1, *x1f, *b1f, *r1f, *t1f, *x1c, *r1c, *t1c;
+    float *c1[3], *dD1, *dg1, *x1f, *b1f, *r1f, *t1f, *x1c, *r1c, *t1c;
     uint8_t* act1;
     // vectors (fine pool + coarse grid)
     float *bf, *bc, *rf, *rc, *zf, *zc, *df, *dc, *qf, *qc, *rof, *roc, *tmf, *tmc, *res0f, *res0c;
@@ -800,7 +834,8 @@ struct SpRun {
         sp_launch(k_sp_coef1, dim3(grid1((int64_t)t.nslots * BFACES1), 3), SPT, s, t, c->c1[0], c->c1[1], c->c1[2],
                   (const float*)c->cf[0], (const float*)c->cf[1], (const float*)c->cf[2]);
         sp_launch(k_sp_cells1, dim3(grid1((int64_t)t.nslots * BCELLS1)), SPT, s, t, c->dD1, c->act1,
-                  (const float*)c->dDf, tf);
+                  (const float*)c->dDf, tf, (const float*)c->c1[0], (const float*)c->c1[1], (const float*)c->c1[2],
+                  c->dg1);
         int64_t mc = c->ncc;
         for (int a = 1; a <= 3; a++) mc = std::max(mc, face_count(t.nc, a));
         sp_launch(k_sp_level2, dim3(grid1(mc), 4), SPT, s, t, c->D[0].cx, c->D[0].cy, c->D[0].cz,
@@ -834,16 +869,16 @@ struct SpRun {
             }
             return;
         }
-        const Split sp = split_for(c, (int64_t)c->t.nslots * Lv<N>::CELLS);
+        const Split sp = split_blk(c);
         for (int q = 0; q < sweeps; q++) {
             if (q == 0 && from_zero)
-                sp_launch(k_sp_jacobi<N, true>, dim3(sp.g), SPT, s, c->t, L, tf_, tc_, (const float*)xf,
-                          (const float*)xc, bf, bc, sp.gf);
+                sp_launch(k_sp_blk8<BOP_JAC_ZS>, dim3(sp.g), T8, s, c->t, L, (const float*)c->dg1, tf_, tc_,
+                          (const float*)xf, (const float*)xc, bf, bc, sp.gf);
             else
-                sp_launch(k_sp_jacobi<N, false>, dim3(sp.g), SPT, s, c->t, L, tf_, tc_, (const float*)xf,
-                          (const float*)xc, bf, bc, sp.gf);
-            sp_launch(k_sp_jacobi<N, false>, dim3(sp.g), SPT, s, c->t, L, xf, xc, (const float*)tf_, (const float*)tc_,
-                      bf, bc, sp.gf);
+                sp_launch(k_sp_blk8<BOP_JAC>, dim3(sp.g), T8, s, c->t, L, (const float*)c->dg1, tf_, tc_,
+                          (const float*)xf, (const float*)xc, bf, bc, sp.gf);
+            sp_launch(k_sp_blk8<BOP_JAC>, dim3(sp.g), T8, s, c->t, L, (const float*)c->dg1, xf, xc, (const float*)tf_,
+                      (const float*)tc_, bf, bc, sp.gf);
             nk += 2;
         }
     }
@@ -872,8 +907,8 @@ struct SpRun {
         nk += 2;
         // level 1's coarse right-hand side is level 0's coarse residual (copyto!, :1730)
         smooth<8>(L1, c->x1f, c->x1c, c->b1f, c->res0c, c->t1f, c->t1c, sweeps, true);
-        sp_launch(k_sp_residual<8>, dim3(s1.g), SPT, s, t, L1, c->r1f, c->r1c, (const float*)c->x1f,
-                  (const float*)c->x1c, (const float*)c->b1f, (const float*)c->res0c, s1.gf);
+        sp_launch(k_sp_blk8<BOP_RES>, dim3(sb.g), T8, s, t, L1, (const float*)c->dg1, c->r1f, c->r1c,
+                  (const float*)c->x1f, (const float*)c->x1c, (const float*)c->b1f, (const float*)c->res0c, sb.gf);
         sp_launch(k_sp_restrict12, dim3(grid1(c->ncc)), SPT, s, t, c->D[0].b, (const float*)c->r1f,
                   (const float*)c->r1c);
         nk += 2;
@@ -893,12 +928,12 @@ struct SpRun {
             nk++;
             dense_smooth(l, sweeps, false);
         }
-        sp_launch(k_sp_prolong<8>, dim3(s1.g), SPT, s, t, c->x1f, c->x1c, (const float*)nullptr,
-                  (const float*)c->D[0].x, (const uint8_t*)c->act1, (const uint8_t*)c->actc, boost, s1.gf);
+        sp_launch(k_sp_prolong21, dim3(s1.g), SPT, s, t, c->x1f, c->x1c, (const float*)c->D[0].x,
+                  (const uint8_t*)c->act1, (const uint8_t*)c->actc, boost, s1.gf);
         nk++;
         smooth<8>(L1, c->x1f, c->x1c, c->b1f, c->res0c, c->t1f, c->t1c, sweeps, false);
-        sp_launch(k_sp_prolong<16>, dim3(s0.g), SPT, s, t, zf, zc, (const float*)c->x1f, (const float*)c->x1c, tf,
-                  (const uint8_t*)c->actc, boost, s0.gf);
+        sp_launch(k_sp_prolong10, dim3(sb.g), SPT, s, t, zf, zc, (const float*)c->x1f, (const float*)c->x1c, tf,
+                  (const uint8_t*)c->actc, boost, sb.gf);
         nk++;
         smooth<16>(L0, zf, zc, rf, rc, c->tmf, c->tmc, sweeps, false);
     }
@@ -1299,7 +1334,7 @@ int mpp_sparse_ctx_create(mpp_sparse_ctx** out, const mpp_sparse_grid* g, int32_
     float** fine[] = {&c->dDf, &c->bf, &c->rf, &c->zf, &c->df, &c->qf, &c->rof, &c->tmf, &c->res0f};
     float** coarse[] = {&c->dDc, &c->bc, &c->rc, &c->zc, &c->dc, &c->qc, &c->roc, &c->tmc, &c->res0c,
                         &c->x1c, &c->r1c, &c->t1c};
-    float** lev1[] = {&c->dD1, &c->x1f, &c->b1f, &c->r1f, &c->t1f};
+    float** lev1[] = {&c->dD1, &c->dg1, &c->x1f, &c->b1f, &c->r1f, &c->t1f};
     for (auto p : fine)
         if (!e) e = sp_alloc_n(c, p, nf);
     for (auto p : coarse)
@@ -1330,7 +1365,9 @@ int mpp_sparse_ctx_create(mpp_sparse_ctx** out, const mpp_sparse_grid* g, int32_
     c->actc = c->D[0].act;
     if (int e2 = sp_alloc_n(c, &c->st, 1)) return fail(e2);
     if (int e2 = sp_alloc_n(c, &c->dres, 1)) return fail(e2);
-    if (int e2 = sp_alloc_n(c, &c->partials, (int64_t)c->nsm * 8 * MAXK * 2)) return fail(e2);
+    // a reduction's partial sums: K <= 2 values for every CTA of its launch, which holds a CTA
+    // per slot and at most nsm * 8 for the coarse grid (or nsm * 8 in all)
+    if (int e2 = sp_alloc_n(c, &c->partials, ((int64_t)capacity + (int64_t)c->nsm * 8) * 2)) return fail(e2);
     if (int e2 = sp_alloc_n(c, &c->counters, SCNT_N)) return fail(e2);
     if (cudaMallocHost((void**)&c->st_host, sizeof(SpState)) != cudaSuccess ||
         cudaMallocHost((void**)&c->dres_host, sizeof(double)) != cudaSuccess) {

@@ -10,13 +10,15 @@
 //     slot and axis (faceindex, :106-110); level 1's pools the same at 8^3 (512 cells, 9*64
 //     faces);
 //   * the coarse grid and its halvings: column-major, face arrays one longer along their axis.
-// Kernels run a thread per cell or face, consecutive threads on consecutive pool or grid
-// indices (16 consecutive cells of a fine row, 32 of a coarse row): every array is read and
-// written coalesced; the block table (a few KB) stays in L1/L2. A fine cell's neighbours
-// inside its block are at fixed pool offsets; only the block's boundary cells look the
-// neighbouring block up. The fine and coarse parts of a level pass are one launch (the
-// first `gf` blocks on the fine cells, the rest on the coarse ones): both read the pass's
-// source and write its destination, so they are independent.
+// Kernels: the stencil passes of the two composite levels (Jacobi sweeps, residuals, A x)
+// run a CTA per fine block, the block and a one-cell halo staged in shared memory (level 0's
+// couplings packed in a 16-bit code a cell, level 1's read from its aggregated face arrays,
+// each cell's whole diagonal precomputed once per operator); the CG's vector passes take a
+// slot's cells in 16-byte pieces; the coarse grid, the dense levels and the set-up passes run
+// a thread per cell or face, consecutive threads on consecutive grid indices. The fine and
+// coarse parts of a level pass are one launch (the first `gf` CTAs on the fine blocks, the
+// rest on the coarse cells): both read the pass's source and write its destination, so they
+// are independent.
 //
 // Arithmetic: every value is computed in the reference kernel's Float32 operation order
 // (the library is built with -fmad=false), so the operator, the coefficients, the
@@ -161,37 +163,6 @@ struct Comp {
     const uint8_t* actc;
 };
 
-// finerow (src/sflip.jl:1143-1174): diag and off of (A x) at a level's fine cell. ZS: the
-// source is all zeros (the first sweep after the reference's zero!): no loads of x.
-template <int N, bool ZS>
-__device__ __forceinline__ void finerow(const Topo& t, const Comp& L, const float* x, const float* xc, int sl, int i,
-                                        int j, int k, const int w[3], int64_t n, float& diag, float& off) {
-    using V = Lv<N>;
-    constexpr int sh = V::SH - 2;
-    const int I = w[0] * N + i, J = w[1] * N + j, K = w[2] * N + k;
-    diag = L.dDf[n];
-    off = 0.0f;
-    auto nv = [&](int In, int Jn, int Kn, bool inside, int64_t nn) -> float {
-        if (ZS) return 0.0f;
-        if (inside) return x[nn];  // the same block: cellat gives this pool index
-        const int64_t id = V::cellat(t, In, Jn, Kn);
-        return id > 0 ? x[id - 1] : xc[coarse_clamped(t, In >> sh, Jn >> sh, Kn >> sh)];
-    };
-    float c;
-    c = L.cfx[V::face(sl, 1, i, j, k) - 1];
-    if (c > 0.0f) { diag += c; off += c * nv(I - 1, J, K, i > 0, n - 1); }
-    c = L.cfx[V::face(sl, 1, i + 1, j, k) - 1];
-    if (c > 0.0f) { diag += c; off += c * nv(I + 1, J, K, i < N - 1, n + 1); }
-    c = L.cfy[V::face(sl, 2, i, j, k) - 1];
-    if (c > 0.0f) { diag += c; off += c * nv(I, J - 1, K, j > 0, n - N); }
-    c = L.cfy[V::face(sl, 2, i, j + 1, k) - 1];
-    if (c > 0.0f) { diag += c; off += c * nv(I, J + 1, K, j < N - 1, n + N); }
-    c = L.cfz[V::face(sl, 3, i, j, k) - 1];
-    if (c > 0.0f) { diag += c; off += c * nv(I, J, K - 1, k > 0, n - N * N); }
-    c = L.cfz[V::face(sl, 3, i, j, k + 1) - 1];
-    if (c > 0.0f) { diag += c; off += c * nv(I, J, K + 1, k < N - 1, n + N * N); }
-}
-
 // coarserow (src/sflip.jl:1176-1217): a coarse cell outside fine blocks, its coarse
 // neighbours through coarse faces, a fine block's cells through the block's R^2 sub-faces.
 template <int N, bool ZS>
@@ -212,22 +183,28 @@ __device__ __forceinline__ void coarserow(const Topo& t, const Comp& L, const fl
         for (int sg = -1; sg <= 1; sg += 2) {
             const int In = I + sg * e0, Jn = J + sg * e1, Kn = K + sg * e2;
             if (!(0 <= In && In < n1 && 0 <= Jn && Jn < n2 && 0 <= Kn && Kn < n3)) continue;
-            if (covered(t, In, Jn, Kn)) {
+            // the neighbouring coarse cell's block: covered when it has a slot
+            const int s2 = cellslot(t, In * RATIO, Jn * RATIO, Kn * RATIO);
+            if (s2 != 0) {
+                // Its R^2 cells across the plane lie in block s2; each couples through its own
+                // sub-face, which is in s2 too: the cell's low face (sg > 0), or s2's high plane
+                // (sg < 0; the face's upper cell is this uncovered coarse cell's, faceat takes
+                // the lower block's copy). This is faceat / cellat with the block looked up once.
+#pragma unroll
                 for (int q = 0; q < R; q++)
+#pragma unroll
                     for (int p = 0; p < R; p++) {
                         const int FI = a == 1 ? (sg > 0 ? R * In : R * I - 1) : R * I + p;
                         const int FJ = a == 2 ? (sg > 0 ? R * Jn : R * J - 1) : R * J + (a == 1 ? p : q);
                         const int FK = a == 3 ? (sg > 0 ? R * Kn : R * K - 1) : R * K + q;
-                        const int PI = a == 1 ? (sg > 0 ? FI : FI + 1) : FI;
-                        const int PJ = a == 2 ? (sg > 0 ? FJ : FJ + 1) : FJ;
-                        const int PK = a == 3 ? (sg > 0 ? FK : FK + 1) : FK;
-                        const int64_t fidx = V::faceat(t, a, PI, PJ, PK);
-                        const int64_t cidx = V::cellat(t, FI, FJ, FK);
-                        if (fidx > 0 && cidx > 0) {
-                            const float c = Cf[fidx - 1];
-                            diag += c;
-                            off += c * (ZS ? 0.0f : xf[cidx - 1]);
-                        }
+                        constexpr int M = N - 1;
+                        const int64_t fidx = sg > 0 ? V::face(s2, a, FI & M, FJ & M, FK & M)
+                                                    : V::face(s2, a, a == 1 ? N : (FI & M), a == 2 ? N : (FJ & M),
+                                                              a == 3 ? N : (FK & M));
+                        const int64_t cidx = V::cell(s2, FI & M, FJ & M, FK & M);
+                        const float c = Cf[fidx - 1];
+                        diag += c;
+                        off += c * (ZS ? 0.0f : xf[cidx - 1]);
                     }
             } else {
                 const float c = sg < 0 ? Cc[lin3(f0, f1, I, J, K)] : Cc[lin3(f0, f1, I + e0, J + e1, K + e2)];
@@ -250,98 +227,29 @@ __device__ __forceinline__ void pool_cell(int64_t n, int& sl, int& i, int& j, in
     j = (c >> S) & (N - 1);
     k = c >> (2 * S);
 }
+// (i, j, k) of linear index o over n0 x n1 (x n2): 32-bit arithmetic (the library keeps every
+// grid and face array below 2^31 elements)
+__device__ __forceinline__ void split3(int64_t o, int n0, int n1, int& i, int& j, int& k) {
+    const int v = (int)o, r = v / n0;
+    i = v - r * n0;
+    k = r / n1;
+    j = r - k * n1;
+}
 __device__ __forceinline__ void coarse_cell(const Topo& t, int64_t c, int& I, int& J, int& K) {
-    I = (int)(c % t.nc[0]);
-    const int64_t r = c / t.nc[0];
-    J = (int)(r % t.nc[1]);
-    K = (int)(r / t.nc[1]);
+    split3(c, t.nc[0], t.nc[1], I, J, K);
 }
 
-// Grid-stride loops over a fused launch's fine part (blocks [0, gf)) and coarse part (the rest).
-#define SP_FINE_LOOP(n, total, gf)                                                                 \
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < (total); n += (int64_t)(gf) * blockDim.x)
+// A fused launch's CTAs: the coarse part first (CTAs [0, gridDim - gf), dispatched first, so
+// its slower cells next to fine blocks overlap the fine part instead of trailing it), the
+// fine part the last gf (a CTA per slot in the block kernels, a grid-stride range otherwise).
+__device__ __forceinline__ bool sp_is_fine(int gf) { return (int)blockIdx.x >= (int)gridDim.x - gf; }
+__device__ __forceinline__ int sp_slot(int gf) { return (int)blockIdx.x - ((int)gridDim.x - gf) + 1; }
+#define SP_FINE_LOOP(n, total, gf)                                                                        \
+    for (int64_t n = (int64_t)((int)blockIdx.x - ((int)gridDim.x - (gf))) * blockDim.x + threadIdx.x; n < (total); \
+         n += (int64_t)(gf) * blockDim.x)
 #define SP_COARSE_LOOP(c, total, gf)                                                               \
-    for (int64_t c = (int64_t)(blockIdx.x - (gf)) * blockDim.x + threadIdx.x; c < (total);         \
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < (total);                  \
          c += (int64_t)(gridDim.x - (gf)) * blockDim.x)
-
-// jacobifine_kernel! + jacobicoarse_kernel! (src/sflip.jl:1219-1243): one damped Jacobi
-// sweep of a composite level, out = x + omega (b - A x) / diag on active cells, else 0.
-template <int N, bool ZS>
-__global__ void __launch_bounds__(SPT) k_sp_jacobi(Topo t, Comp L, float* outf, float* outc, const float* xf,
-                                                   const float* xc, const float* bf, const float* bc, int gf) {
-    pdl_wait();
-    pdl_trigger();
-    if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * Lv<N>::CELLS;
-        SP_FINE_LOOP(n, nf, gf) {
-            int sl, i, j, k;
-            pool_cell<N>(n, sl, i, j, k);
-            int w[3];
-            where_of(t, sl, w);
-            if (w[0] < 0) continue;
-            float v = 0.0f;
-            if (L.actf[n] != 0) {
-                float diag, off;
-                finerow<N, ZS>(t, L, xf, xc, sl, i, j, k, w, n, diag, off);
-                const float x0 = ZS ? 0.0f : xf[n];
-                v = diag > 0.0f ? x0 + OMEGA * (bf[n] - (diag * x0 - off)) / diag : 0.0f;
-            }
-            outf[n] = v;
-        }
-    } else {
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) {
-            int I, J, K;
-            coarse_cell(t, c, I, J, K);
-            float v = 0.0f;
-            if (L.actc[c] != 0 && !covered(t, I, J, K)) {
-                float diag, off;
-                coarserow<N, ZS>(t, L, xf, xc, I, J, K, diag, off);
-                const float x0 = ZS ? 0.0f : xc[c];
-                v = diag > 0.0f ? x0 + OMEGA * (bc[c] - (diag * x0 - off)) / diag : 0.0f;
-            }
-            outc[c] = v;
-        }
-    }
-}
-
-// residualfine_kernel! + residualcoarse_kernel! (src/sflip.jl:1245-1270)
-template <int N>
-__global__ void __launch_bounds__(SPT) k_sp_residual(Topo t, Comp L, float* rf, float* rc, const float* xf,
-                                                     const float* xc, const float* bf, const float* bc, int gf) {
-    pdl_wait();
-    pdl_trigger();
-    if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * Lv<N>::CELLS;
-        SP_FINE_LOOP(n, nf, gf) {
-            int sl, i, j, k;
-            pool_cell<N>(n, sl, i, j, k);
-            int w[3];
-            where_of(t, sl, w);
-            if (w[0] < 0) continue;
-            float v = 0.0f;
-            if (L.actf[n] != 0) {
-                float diag, off;
-                finerow<N, false>(t, L, xf, xc, sl, i, j, k, w, n, diag, off);
-                v = bf[n] - (diag * xf[n] - off);
-            }
-            rf[n] = v;
-        }
-    } else {
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) {
-            int I, J, K;
-            coarse_cell(t, c, I, J, K);
-            float v = 0.0f;
-            if (L.actc[c] != 0 && !covered(t, I, J, K)) {
-                float diag, off;
-                coarserow<N, false>(t, L, xf, xc, I, J, K, diag, off);
-                v = bc[c] - (diag * xc[c] - off);
-            }
-            rc[c] = v;
-        }
-    }
-}
 
 // ---- coefficients, level 0 (src/sflip.jl:1315-1451) ----
 // finecoef_kernel! (:1324-1333), the three axes (blockIdx.y)
@@ -353,7 +261,7 @@ __global__ void __launch_bounds__(SPT) k_sp_finecoef(Topo t, float* cu, float* c
     float* c = a == 1 ? cu : (a == 2 ? cv : cw);
     const int64_t nf = (int64_t)t.nslots * BFACES;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += (int64_t)gridDim.x * blockDim.x) {
-        const int sl = (int)(n / BFACES) + 1, f = (int)(n - (int64_t)(sl - 1) * BFACES);
+        const int sl = (int)n / BFACES + 1, f = (int)n - (sl - 1) * BFACES;
         int w[3];
         where_of(t, sl, w);
         if (w[0] < 0) continue;
@@ -377,7 +285,8 @@ __global__ void __launch_bounds__(SPT) k_sp_coarsecoef(Topo t, float* cu, float*
     const int f0 = t.nc[0] + e0, f1 = t.nc[1] + e1, f2 = t.nc[2] + e2;
     const int64_t nfc = (int64_t)f0 * f1 * f2;
     for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < nfc; o += (int64_t)gridDim.x * blockDim.x) {
-        const int I = (int)(o % f0), J = (int)((o / f0) % f1), K = (int)(o / ((int64_t)f0 * f1));
+        int I, J, K;
+            split3(o, f0, f1, I, J, K);
         const int Im = I - e0, Jm = J - e1, Km = K - e2;
         const bool ok = 0 <= Im && 0 <= Jm && 0 <= Km && I < t.nc[0] && J < t.nc[1] && K < t.nc[2];
         c[o] = (ok && !covered(t, I, J, K) && !covered(t, Im, Jm, Km) && tc[lin(t.nc, I, J, K)] == LIQUID &&
@@ -401,7 +310,7 @@ __global__ void __launch_bounds__(SPT) k_sp_dirichlet(Topo t, float* dDf, float*
                                                       uint16_t* code0, float* dg0, uint8_t* cmask, int gf) {
     pdl_wait();
     pdl_trigger();
-    if ((int)blockIdx.x < gf) {
+    if (sp_is_fine(gf)) {
         const int64_t nf = (int64_t)t.nslots * BCELLS;
         SP_FINE_LOOP(n, nf, gf) {
             int sl, i, j, k;
@@ -484,7 +393,7 @@ __global__ void __launch_bounds__(SPT) k_sp_coef1(Topo t, float* c1x, float* c1y
     float* c1 = a == 1 ? c1x : (a == 2 ? c1y : c1z);
     const int64_t nf = (int64_t)t.nslots * BFACES1;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += (int64_t)gridDim.x * blockDim.x) {
-        const int sl = (int)(n / BFACES1) + 1, f = (int)(n - (int64_t)(sl - 1) * BFACES1);
+        const int sl = (int)n / BFACES1 + 1, f = (int)n - (sl - 1) * BFACES1;
         if (!slot_used(t, sl)) continue;
         int i, j, k;
         if (a == 1) { i = f % 9; const int r = f / 9; j = r % 8; k = r / 8; }
@@ -504,8 +413,11 @@ __global__ void __launch_bounds__(SPT) k_sp_coef1(Topo t, float* c1x, float* c1y
     }
 }
 // cells1_kernel! (:1467-1479)
+// and each level-1 cell's whole diagonal dg1 = dD1 + its positive couplings in finerow's
+// order (the block kernels of level 1 read it; the same Float32 sums finerow forms).
 __global__ void __launch_bounds__(SPT) k_sp_cells1(Topo t, float* dD1, uint8_t* act1, const float* dD0,
-                                                   const uint8_t* tf) {
+                                                   const uint8_t* tf, const float* c1x, const float* c1y,
+                                                   const float* c1z, float* dg1) {
     pdl_wait();
     pdl_trigger();
     const int64_t n1 = (int64_t)t.nslots * BCELLS1;
@@ -527,6 +439,13 @@ __global__ void __launch_bounds__(SPT) k_sp_cells1(Topo t, float* dD1, uint8_t* 
                 }
         dD1[n] = d;
         act1[n] = act;
+        const float c6[6] = {c1x[L8::face(sl, 1, i, j, k) - 1], c1x[L8::face(sl, 1, i + 1, j, k) - 1],
+                             c1y[L8::face(sl, 2, i, j, k) - 1], c1y[L8::face(sl, 2, i, j + 1, k) - 1],
+                             c1z[L8::face(sl, 3, i, j, k) - 1], c1z[L8::face(sl, 3, i, j, k + 1) - 1]};
+#pragma unroll
+        for (int m = 0; m < 6; m++)
+            if (c6[m] > 0.0f) d += c6[m];
+        dg1[n] = d;
     }
 }
 // coef2_kernel! (:1485-1507), the three axes, and cells2_kernel! (:1509-1523) as blockIdx.y == 3
@@ -545,7 +464,8 @@ __global__ void __launch_bounds__(SPT) k_sp_level2(Topo t, float* c2x, float* c2
         const int f0 = t.nc[0] + e0, f1 = t.nc[1] + e1, f2 = t.nc[2] + e2;
         const int64_t nfc = (int64_t)f0 * f1 * f2;
         for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < nfc; o += (int64_t)gridDim.x * blockDim.x) {
-            const int I = (int)(o % f0), J = (int)((o / f0) % f1), K = (int)(o / ((int64_t)f0 * f1));
+            int I, J, K;
+            split3(o, f0, f1, I, J, K);
             if (covered(t, I, J, K) || covered(t, I - e0, J - e1, K - e2)) {
                 float acc = 0.0f;
 #pragma unroll
@@ -609,7 +529,8 @@ __global__ void __launch_bounds__(SPT) k_sp_dense_level(DL F, DL C) {
         const int f0 = C.n[0] + e0, f1 = C.n[1] + e1, f2 = C.n[2] + e2;
         const int64_t nfc = (int64_t)f0 * f1 * f2;
         for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < nfc; o += (int64_t)gridDim.x * blockDim.x) {
-            const int I = (int)(o % f0), J = (int)((o / f0) % f1), K = (int)(o / ((int64_t)f0 * f1));
+            int I, J, K;
+            split3(o, f0, f1, I, J, K);
             float acc = 0.0f;
 #pragma unroll
             for (int q = 0; q < 2; q++)
@@ -625,7 +546,8 @@ __global__ void __launch_bounds__(SPT) k_sp_dense_level(DL F, DL C) {
     } else {
         const int64_t nc = (int64_t)C.n[0] * C.n[1] * C.n[2];
         for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < nc; o += (int64_t)gridDim.x * blockDim.x) {
-            const int I = (int)(o % C.n[0]), J = (int)((o / C.n[0]) % C.n[1]), K = (int)(o / ((int64_t)C.n[0] * C.n[1]));
+            int I, J, K;
+            split3(o, C.n[0], C.n[1], I, J, K);
             float d = 0.0f;
             uint8_t act = 0;
 #pragma unroll
@@ -675,7 +597,8 @@ __global__ void __launch_bounds__(SPT) k_sp_djacobi(DL L, float* out, const floa
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
         float v = 0.0f;
         if (L.act[c] != 0) {
-            const int i = (int)(c % L.n[0]), j = (int)((c / L.n[0]) % L.n[1]), k = (int)(c / ((int64_t)L.n[0] * L.n[1]));
+            int i, j, k;
+            split3(c, L.n[0], L.n[1], i, j, k);
             float diag, off;
             denserow<ZS>(L, x, i, j, k, c, diag, off);
             const float x0 = ZS ? 0.0f : x[c];
@@ -693,7 +616,8 @@ __global__ void __launch_bounds__(SPT) k_sp_dresidual(DL L) {
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
         float v = 0.0f;
         if (L.act[c] != 0) {
-            const int i = (int)(c % L.n[0]), j = (int)((c / L.n[0]) % L.n[1]), k = (int)(c / ((int64_t)L.n[0] * L.n[1]));
+            int i, j, k;
+            split3(c, L.n[0], L.n[1], i, j, k);
             float diag, off;
             denserow<false>(L, L.x, i, j, k, c, diag, off);
             v = L.b[c] - (diag * L.x[c] - off);
@@ -706,7 +630,8 @@ __global__ void __launch_bounds__(SPT) k_sp_drestrict(DL F, DL C) {
     pdl_trigger();
     const int64_t nc = (int64_t)C.n[0] * C.n[1] * C.n[2];
     for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < nc; o += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(o % C.n[0]), j = (int)((o / C.n[0]) % C.n[1]), k = (int)(o / ((int64_t)C.n[0] * C.n[1]));
+        int i, j, k;
+            split3(o, C.n[0], C.n[1], i, j, k);
         float acc = 0.0f;
 #pragma unroll
         for (int c = 0; c < 2; c++)
@@ -724,7 +649,8 @@ __global__ void __launch_bounds__(SPT) k_sp_dprolong(DL F, DL C, float boost) {
     const int64_t nc = (int64_t)F.n[0] * F.n[1] * F.n[2];
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
         if (F.act[c] == 0) continue;
-        const int i = (int)(c % F.n[0]), j = (int)((c / F.n[0]) % F.n[1]), k = (int)(c / ((int64_t)F.n[0] * F.n[1]));
+        int i, j, k;
+            split3(c, F.n[0], F.n[1], i, j, k);
         F.x[c] += boost * C.x[lin(C.n, i >> 1, j >> 1, k >> 1)];
     }
 }
@@ -813,36 +739,29 @@ __global__ void __launch_bounds__(SPT) k_sp_restrict12(Topo t, float* b2, const 
         }
     }
 }
-// prolong21fine_kernel! + prolongcoarse_kernel! (:1688-1699) as one launch, and
-// prolong10fine_kernel! + prolongcoarse_kernel! (:1695-1705) with N = 16: the coarser
-// level's correction added to a composite level's active fine cells (each from the cell it
-// lies in) and to its uncovered active coarse cells (their own).
-template <int N>
-__global__ void __launch_bounds__(SPT) k_sp_prolong(Topo t, float* xf, float* xc, const float* from_f,
-                                                    const float* from_c, const uint8_t* actf, const uint8_t* act2,
-                                                    float boost, int gf) {
+// prolong21fine_kernel! + prolongcoarse_kernel! (:1688-1699) as one launch: level 2's
+// correction added to level 1's active fine cells (each from the coarse cell it lies in) and
+// to its active coarse cells outside fine blocks.
+__global__ void __launch_bounds__(SPT) k_sp_prolong21(Topo t, float* xf, float* xc, const float* x2,
+                                                      const uint8_t* act1, const uint8_t* act2, float boost, int gf) {
     pdl_wait();
     pdl_trigger();
-    if ((int)blockIdx.x < gf) {
-        const int64_t nf = (int64_t)t.nslots * Lv<N>::CELLS;
+    if (sp_is_fine(gf)) {
+        const int64_t nf = (int64_t)t.nslots * BCELLS1;
         SP_FINE_LOOP(n, nf, gf) {
             int sl, i, j, k;
-            pool_cell<N>(n, sl, i, j, k);
+            pool_cell<8>(n, sl, i, j, k);
             int w[3];
             where_of(t, sl, w);
-            if (w[0] < 0) continue;
-            if (N == 8) {
-                if (actf[n] != 0) xf[n] += boost * from_c[lin(t.nc, (w[0] * 8 + i) >> 1, (w[1] * 8 + j) >> 1, (w[2] * 8 + k) >> 1)];
-            } else {
-                if (actf[n] == LIQUID) xf[n] += boost * from_f[L8::cell(sl, i >> 1, j >> 1, k >> 1) - 1];
-            }
+            if (w[0] < 0 || act1[n] == 0) continue;
+            xf[n] += boost * x2[lin(t.nc, (w[0] * 8 + i) >> 1, (w[1] * 8 + j) >> 1, (w[2] * 8 + k) >> 1)];
         }
     } else {
         const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
         SP_COARSE_LOOP(c, nc, gf) {
             int I, J, K;
             coarse_cell(t, c, I, J, K);
-            if (act2[c] != 0 && !covered(t, I, J, K)) xc[c] += boost * from_c[c];
+            if (act2[c] != 0 && !covered(t, I, J, K)) xc[c] += boost * x2[c];
         }
     }
 }
@@ -872,20 +791,8 @@ __device__ __forceinline__ bool coarse_unknown(const Topo& t, const uint8_t* tc,
 }
 __device__ __forceinline__ float f32sum(double v) { return (float)v; }
 
-// apply! at level 0 (src/sflip.jl:1824-1847): q = A x on LIQUID fine cells and active
-// uncovered coarse cells, else 0.
-__device__ __forceinline__ float apply_fine(const Topo& t, const Comp& L, const uint8_t* tf, const float* xf,
-                                            const float* xc, int64_t n, bool& live) {
-    int sl, i, j, k;
-    pool_cell<16>(n, sl, i, j, k);
-    int w[3];
-    where_of(t, sl, w);
-    live = w[0] >= 0;
-    if (!live || tf[n] != LIQUID) return 0.0f;
-    float diag, off;
-    finerow<16, false>(t, L, xf, xc, sl, i, j, k, w, n, diag, off);
-    return diag * xf[n] - off;
-}
+// apply! at level 0's coarse part (src/sflip.jl:1837-1847): q = A x on active uncovered
+// coarse cells, else 0.
 __device__ __forceinline__ float apply_coarse(const Topo& t, const Comp& L, const float* xf, const float* xc, int64_t c,
                                               bool& cov) {
     int I, J, K;
@@ -1011,6 +918,124 @@ __device__ __forceinline__ void block_cells(const uint16_t* __restrict__ code0, 
             out[u] = v;
         }
         sink(n, out, xv);
+    }
+}
+
+
+// ---- level 1's fine part, a CTA (128 threads) per 8^3 block ----
+// As level 0's block kernels: the block's x (512 cells) and its halo (6 x 64 cells: the
+// neighbouring block's boundary plane, else the coarse cell the halo cell lies in) staged in
+// shared memory, a thread a piece of four cells of a row. The couplings are level 1's
+// aggregated face arrays (sums of four level-0 faces, read as floats), the diagonal dg1.
+constexpr int T8 = 128, Q = 10, QY = Q * Q, QCELLS = QY * Q;
+__device__ __forceinline__ int qidx(int i, int j, int k) { return (k + 1) * QY + (j + 1) * Q + (i + 1); }
+
+__device__ __forceinline__ void stage_block8(const Topo& t, const float* __restrict__ x, const float* __restrict__ xc,
+                                             int sl, const int w[3], float* xs) {
+    const int tid = (int)threadIdx.x;
+    const float4 v = reinterpret_cast<const float4*>(x + (int64_t)(sl - 1) * BCELLS1)[tid];
+    float hv[3];
+    int hi[3];
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+        const int h = tid + T8 * u, f = h >> 6, pq = h & 63, p = pq & 7, q = pq >> 3;
+        const int ax = f >> 1, sg = (f & 1) ? 1 : -1;
+        const int i = ax == 0 ? (sg < 0 ? -1 : 8) : p;
+        const int j = ax == 1 ? (sg < 0 ? -1 : 8) : (ax == 0 ? p : q);
+        const int k = ax == 2 ? (sg < 0 ? -1 : 8) : q;
+        const int nbi = w[0] + (ax == 0 ? sg : 0), nbj = w[1] + (ax == 1 ? sg : 0), nbk = w[2] + (ax == 2 ? sg : 0);
+        const int s2 = inblocks(t, nbi, nbj, nbk) ? blockslot(t, nbi, nbj, nbk) : 0;
+        if (s2 > 0) {
+            hv[u] = x[(int64_t)(s2 - 1) * BCELLS1 + (i & 7) + 8 * ((j & 7) + 8 * (k & 7))];
+        } else {
+            const int I = w[0] * 8 + i, J = w[1] * 8 + j, K = w[2] * 8 + k;
+            hv[u] = xc[coarse_clamped(t, I >> 1, J >> 1, K >> 1)];
+        }
+        hi[u] = qidx(i, j, k);
+    }
+    const int c = 4 * tid, i = c & 7, j = (c >> 3) & 7, k = c >> 6;
+    float* d = xs + qidx(i, j, k);
+    d[0] = v.x;
+    d[1] = v.y;
+    d[2] = v.z;
+    d[3] = v.w;
+#pragma unroll
+    for (int u = 0; u < 3; u++) xs[hi[u]] = hv[u];
+}
+
+// Level 1's Jacobi sweeps and residual (jacobifine_kernel! / residualfine_kernel! at N = 8,
+// with jacobicoarse_kernel! / residualcoarse_kernel! for the coarse part).
+template <int OP>
+__global__ void __launch_bounds__(T8) k_sp_blk8(Topo t, Comp L, const float* dg1, float* outf, float* outc,
+                                                const float* xf, const float* xc, const float* bf, const float* bc,
+                                                int gf) {
+    __shared__ float xs[QCELLS];
+    pdl_wait();
+    pdl_trigger();
+    constexpr bool ZS = OP == BOP_JAC_ZS;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
+        int w[3];
+        where_of(t, sl, w);
+        if (w[0] < 0) return;
+        const int tid = (int)threadIdx.x, c = 4 * tid, i0 = c & 7, j = (c >> 3) & 7, k = c >> 6;
+        const int64_t n = (int64_t)(sl - 1) * BCELLS1 + c;
+        // this piece's own arrays first: they do not depend on the staging
+        const float4 dg = *reinterpret_cast<const float4*>(dg1 + n);
+        const float4 bb = *reinterpret_cast<const float4*>(bf + n);
+        const uchar4 act = *reinterpret_cast<const uchar4*>(L.actf + n);
+        float cx[5], cy[4][2], cz[4][2];
+#pragma unroll
+        for (int u = 0; u <= 4; u++) cx[u] = L.cfx[L8::face(sl, 1, i0 + u, j, k) - 1];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            cy[u][0] = L.cfy[L8::face(sl, 2, i0 + u, j, k) - 1];
+            cy[u][1] = L.cfy[L8::face(sl, 2, i0 + u, j + 1, k) - 1];
+            cz[u][0] = L.cfz[L8::face(sl, 3, i0 + u, j, k) - 1];
+            cz[u][1] = L.cfz[L8::face(sl, 3, i0 + u, j, k + 1) - 1];
+        }
+        if (!ZS) {
+            stage_block8(t, xf, xc, sl, w, xs);
+            __syncthreads();
+        }
+        const float ds[4] = {dg.x, dg.y, dg.z, dg.w}, bs[4] = {bb.x, bb.y, bb.z, bb.w};
+        const uint8_t as[4] = {act.x, act.y, act.z, act.w};
+        float out[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int o = qidx(i0 + u, j, k);
+            const float c6[6] = {cx[u], cx[u + 1], cy[u][0], cy[u][1], cz[u][0], cz[u][1]};
+            const int nb[6] = {-1, 1, -Q, Q, -QY, QY};
+            float off = 0.0f;
+            if (!ZS) {
+#pragma unroll
+                for (int m = 0; m < 6; m++)
+                    if (c6[m] > 0.0f) off += c6[m] * xs[o + nb[m]];
+            }
+            const float x0 = ZS ? 0.0f : xs[o], diag = ds[u];
+            float v = 0.0f;
+            if (as[u] != 0) {
+                if (OP == BOP_RES) v = bs[u] - (diag * x0 - off);
+                else v = diag > 0.0f ? x0 + OMEGA * (bs[u] - (diag * x0 - off)) / diag : 0.0f;
+            }
+            out[u] = v;
+        }
+        *reinterpret_cast<float4*>(outf + n) = make_float4(out[0], out[1], out[2], out[3]);
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            int I, J, K;
+            coarse_cell(t, c, I, J, K);
+            float v = 0.0f;
+            if (L.actc[c] != 0 && !covered(t, I, J, K)) {
+                float diag, off;
+                coarserow<8, ZS>(t, L, xf, xc, I, J, K, diag, off);
+                const float x0 = ZS ? 0.0f : xc[c];
+                if (OP == BOP_RES) v = bc[c] - (diag * x0 - off);
+                else v = diag > 0.0f ? x0 + OMEGA * (bc[c] - (diag * x0 - off)) / diag : 0.0f;
+            }
+            outc[c] = v;
+        }
     }
 }
 

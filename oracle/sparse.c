@@ -269,6 +269,7 @@ static inline void coarserow(const S* s, const Comp* L, const float* xf, const f
 /* jacobifine_kernel! / jacobicoarse_kernel! (src/sflip.jl:1219-1243). */
 static void jacobi_fine(const S* s, const Comp* L, float* out, const float* x, const float* b, const float* xc) {
     const int N = L->N;
+    #pragma omp parallel for schedule(static)
     for (int64_t sl = 1; sl <= s->nsl; sl++) {
         const int32_t* w = whereof(s, sl);
         if (w[0] < 0) continue;
@@ -303,6 +304,7 @@ static void jacobi_coarse(const S* s, const Comp* L, float* out, const float* x,
 static void residual_comp(const S* s, const Comp* L, float* rf, float* rc, const float* xf, const float* xc,
                           const float* bf, const float* bc) {
     const int N = L->N;
+    #pragma omp parallel for schedule(static)
     for (int64_t sl = 1; sl <= s->nsl; sl++) {
         const int32_t* w = whereof(s, sl);
         if (w[0] < 0) continue;
@@ -318,6 +320,7 @@ static void residual_comp(const S* s, const Comp* L, float* rf, float* rc, const
             }
         }
     }
+    #pragma omp parallel for schedule(static)
     for (int K = 0; K < s->nc[2]; K++)
         for (int J = 0; J < s->nc[1]; J++)
             for (int I = 0; I < s->nc[0]; I++) {
@@ -401,6 +404,7 @@ static void coefs(S* s) {
         int e[3], fm[3];
         unitv(a, e);
         fdims(s->nc, a, fm);
+        #pragma omp parallel for schedule(static)
         for (int64_t sl = 1; sl <= s->nsl; sl++) {
             const int32_t* w = whereof(s, sl);
             if (w[0] < 0) continue;
@@ -416,6 +420,7 @@ static void coefs(S* s) {
             }
         }
         const int n1 = s->nc[0], n2 = s->nc[1], n3 = s->nc[2];
+        #pragma omp parallel for schedule(static)
         for (int K = 0; K < fm[2]; K++)
             for (int J = 0; J < fm[1]; J++)
                 for (int I = 0; I < fm[0]; I++) {
@@ -433,6 +438,7 @@ static const int NB[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0
 /* finedirichlet_kernel! (:1356-1374) and coarsedirichlet_kernel! (:1376-1407) */
 static void dirichlet(S* s) {
     const ors_basin* B = s->B;
+    #pragma omp parallel for schedule(static)
     for (int64_t sl = 1; sl <= s->nsl; sl++) {
         const int32_t* w = whereof(s, sl);
         if (w[0] < 0) continue;
@@ -491,6 +497,7 @@ static void dirichlet(S* s) {
 static void coefficients(S* s) {
     coefs(s);
     dirichlet(s);
+    #pragma omp parallel for schedule(static)
     for (int K = 0; K < s->nc[2]; K++)
         for (int J = 0; J < s->nc[1]; J++)
             for (int I = 0; I < s->nc[0]; I++) {
@@ -505,6 +512,7 @@ static void hierarchy(S* s) {
     for (int a = 1; a <= 3; a++) {
         const float* c0 = a == 1 ? s->cuf : (a == 2 ? s->cvf : s->cwf);
         float* c1 = a == 1 ? s->c1x : (a == 2 ? s->c1y : s->c1z);
+        #pragma omp parallel for schedule(static)
         for (int64_t sl = 1; sl <= s->nsl; sl++) {
             if (whereof(s, sl)[0] < 0) continue;
             for (int f = 0; f < 9 * 64; f++) {
@@ -525,6 +533,7 @@ static void hierarchy(S* s) {
         }
     }
     /* cells1_kernel! (:1467-1479) */
+    #pragma omp parallel for schedule(static)
     for (int64_t sl = 1; sl <= s->nsl; sl++) {
         if (whereof(s, sl)[0] < 0) continue;
         for (int c = 0; c < 512; c++) {
@@ -551,6 +560,7 @@ static void hierarchy(S* s) {
         int e[3], fm[3];
         unitv(a, e);
         fdims(s->nc, a, fm);
+        #pragma omp parallel for schedule(static)
         for (int K = 0; K < fm[2]; K++)
             for (int J = 0; J < fm[1]; J++)
                 for (int I = 0; I < fm[0]; I++) {
@@ -571,6 +581,7 @@ static void hierarchy(S* s) {
                     }
                 }
     }
+    #pragma omp parallel for schedule(static)
     for (int K = 0; K < s->nc[2]; K++)
         for (int J = 0; J < s->nc[1]; J++)
             for (int I = 0; I < s->nc[0]; I++) {
@@ -601,6 +612,7 @@ static void hierarchy(S* s) {
             int fmf[3], fmc[3];
             fdims(F->n, a, fmf);
             fdims(C->n, a, fmc);
+            #pragma omp parallel for schedule(static)
             for (int K = 0; K < fmc[2]; K++)
                 for (int J = 0; J < fmc[1]; J++)
                     for (int I = 0; I < fmc[0]; I++) {
@@ -659,6 +671,7 @@ static inline void denserow(const DLev* L, const float* x, int i, int j, int k, 
 }
 /* jacobidense_kernel! (:1588-1596) */
 static void jacobi_dense(const DLev* L, float* out, const float* x) {
+    #pragma omp parallel for schedule(static)
     for (int k = 0; k < L->n[2]; k++)
         for (int j = 0; j < L->n[1]; j++)
             for (int i = 0; i < L->n[0]; i++) {
@@ -674,6 +687,7 @@ static void jacobi_dense(const DLev* L, float* out, const float* x) {
 }
 /* residualdense_kernel! (:1598-1607) */
 static void residual_dense(DLev* L) {
+    #pragma omp parallel for schedule(static)
     for (int k = 0; k < L->n[2]; k++)
         for (int j = 0; j < L->n[1]; j++)
             for (int i = 0; i < L->n[0]; i++) {
@@ -689,6 +703,7 @@ static void residual_dense(DLev* L) {
 }
 /* restrictdense_kernel! (:1609-1616) */
 static void restrict_dense(const DLev* F, DLev* C) {
+    #pragma omp parallel for schedule(static)
     for (int k = 0; k < C->n[2]; k++)
         for (int j = 0; j < C->n[1]; j++)
             for (int i = 0; i < C->n[0]; i++) {
@@ -701,6 +716,7 @@ static void restrict_dense(const DLev* F, DLev* C) {
 }
 /* prolongdense_kernel! (:1618-1621) */
 static void prolong_dense(DLev* F, const DLev* C, float boost) {
+    #pragma omp parallel for schedule(static)
     for (int k = 0; k < F->n[2]; k++)
         for (int j = 0; j < F->n[1]; j++)
             for (int i = 0; i < F->n[0]; i++) {
@@ -752,6 +768,7 @@ static void vcycle(S* s, float* zf, float* zc, const float* rf, const float* rc,
     smooth_comp(s, &L0, zf, zc, rf, rc, s->tmf, s->tmc, sweeps);
     residual_comp(s, &L0, s->qf, s->qc, zf, zc, rf, rc);
     /* restrict01_kernel! (:1662-1672) */
+    #pragma omp parallel for schedule(static)
     for (int64_t sl = 1; sl <= s->nsl; sl++) {
         if (whereof(s, sl)[0] < 0) continue;
         for (int c = 0; c < 512; c++) {
@@ -770,6 +787,7 @@ static void vcycle(S* s, float* zf, float* zc, const float* rf, const float* rc,
     residual_comp(s, &L1, s->r1f, s->r1c, s->x1f, s->x1c, s->b1f, s->b1c);
     /* restrict12_kernel! (:1674-1686) */
     DLev* D = s->D;
+    #pragma omp parallel for schedule(static)
     for (int K = 0; K < s->nc[2]; K++)
         for (int J = 0; J < s->nc[1]; J++)
             for (int I = 0; I < s->nc[0]; I++) {
@@ -805,6 +823,7 @@ static void vcycle(S* s, float* zf, float* zc, const float* rf, const float* rc,
         }
     }
     /* prolong21fine_kernel! (:1688-1693) and prolongcoarse_kernel! (:1695-1699) */
+    #pragma omp parallel for schedule(static)
     for (int64_t sl = 1; sl <= s->nsl; sl++) {
         const int32_t* w = whereof(s, sl);
         if (w[0] < 0) continue;
@@ -815,6 +834,7 @@ static void vcycle(S* s, float* zf, float* zc, const float* rf, const float* rc,
             s->x1f[n] += boost * D[0].x[LIN(s->nc, (w[0] * 8 + i) >> 1, (w[1] * 8 + j) >> 1, (w[2] * 8 + k) >> 1)];
         }
     }
+    #pragma omp parallel for schedule(static)
     for (int K = 0; K < s->nc[2]; K++)
         for (int J = 0; J < s->nc[1]; J++)
             for (int I = 0; I < s->nc[0]; I++) {
@@ -823,6 +843,7 @@ static void vcycle(S* s, float* zf, float* zc, const float* rf, const float* rc,
             }
     smooth_comp(s, &L1, s->x1f, s->x1c, s->b1f, s->b1c, s->t1f, s->t1c, sweeps);
     /* prolong10fine_kernel! (:1701-1705) and prolongcoarse_kernel! */
+    #pragma omp parallel for schedule(static)
     for (int64_t sl = 1; sl <= s->nsl; sl++) {
         if (whereof(s, sl)[0] < 0) continue;
         for (int c = 0; c < BCELLS; c++) {
@@ -832,6 +853,7 @@ static void vcycle(S* s, float* zf, float* zc, const float* rf, const float* rc,
             zf[n] += boost * s->x1f[cellidx(8, sl, i >> 1, j >> 1, k >> 1) - 1];
         }
     }
+    #pragma omp parallel for schedule(static)
     for (int K = 0; K < s->nc[2]; K++)
         for (int J = 0; J < s->nc[1]; J++)
             for (int I = 0; I < s->nc[0]; I++) {
@@ -850,38 +872,49 @@ static inline float tree256(float* v) { /* groupsum! (src/flip.jl:1020-1031) */
 /* inner (:1794-1805): FP32 partials of 256 consecutive pool cells (LIQUID cells of slots in
    use), summed, plus the coarse grid's (LIQUID cells outside fine blocks). */
 static float inner(const S* s, const float* af, const float* ac, const float* bf, const float* bc) {
-    const int64_t nf = s->nsl * BCELLS;
-    float acc = 0.0f, v[256];
-    for (int64_t g0 = 0; g0 < nf; g0 += 256) {
+    const int64_t nf = s->nsl * BCELLS, gf = (nf + 255) / 256, gc = (s->ncc + 255) / 256;
+    float* part = (float*)malloc(sizeof(float) * (size_t)(gf + gc + 1));
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < gf; g++) {
+        float v[256];
         for (int t = 0; t < 256; t++) {
-            const int64_t i = g0 + t;
+            const int64_t i = g * 256 + t;
             v[t] = 0.0f;
             if (i < nf && s->B->tf[i] == LIQUID && whereof(s, i / BCELLS + 1)[0] >= 0) v[t] = af[i] * bf[i];
         }
-        acc += tree256(v);
+        part[g] = tree256(v);
     }
-    float acc2 = 0.0f;
-    for (int64_t g0 = 0; g0 < s->ncc; g0 += 256) {
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < gc; g++) {
+        float v[256];
         for (int t = 0; t < 256; t++) {
-            const int64_t i = g0 + t;
+            const int64_t i = g * 256 + t;
             v[t] = 0.0f;
             if (i < s->ncc && s->B->tc[i] == LIQUID) {
                 const int I = (int)(i % s->nc[0]), J = (int)((i / s->nc[0]) % s->nc[1]), K = (int)(i / ((int64_t)s->nc[0] * s->nc[1]));
                 if (!covered(s, I, J, K)) v[t] = ac[i] * bc[i];
             }
         }
-        acc2 += tree256(v);
+        part[gf + g] = tree256(v);
     }
+    float acc = 0.0f, acc2 = 0.0f;
+    for (int64_t g = 0; g < gf; g++) acc += part[g];
+    for (int64_t g = 0; g < gc; g++) acc2 += part[gf + g];
+    free(part);
     return acc + acc2;
 }
 static void axpy(const S* s, float* yf, float* yc, float a, const float* xf, const float* xc) {
     const int64_t nf = s->nsl * BCELLS;
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < nf; i++) yf[i] += a * xf[i];
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < s->ncc; i++) yc[i] += a * xc[i];
 }
 static void xpby(const S* s, float* yf, float* yc, const float* xf, const float* xc, float b) {
     const int64_t nf = s->nsl * BCELLS;
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < nf; i++) yf[i] = xf[i] + b * yf[i];
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < s->ncc; i++) yc[i] = xc[i] + b * yc[i];
 }
 static void copyv(const S* s, float* yf, float* yc, const float* xf, const float* xc) {
@@ -905,6 +938,7 @@ static void apply(const S* s, float* qf, float* qc, const float* xf, const float
             }
         }
     }
+    #pragma omp parallel for schedule(static)
     for (int K = 0; K < s->nc[2]; K++)
         for (int J = 0; J < s->nc[1]; J++)
             for (int I = 0; I < s->nc[0]; I++) {
@@ -1164,6 +1198,7 @@ static int pressure_dispatch(S* s, float* Pf, float* Pc, const ors_opts* o, ors_
 static void rhs(S* s, float gamma) {
     const ors_basin* B = s->B;
     const float h = B->g.dx;
+    #pragma omp parallel for schedule(static)
     for (int64_t sl = 1; sl <= s->nsl; sl++) {
         if (whereof(s, sl)[0] < 0) continue;
         for (int c = 0; c < BCELLS; c++) {
@@ -1185,6 +1220,7 @@ static void rhs(S* s, float gamma) {
     fdims(s->nc, 1, fx);
     fdims(s->nc, 2, fy);
     fdims(s->nc, 3, fz);
+    #pragma omp parallel for schedule(static)
     for (int K = 0; K < s->nc[2]; K++)
         for (int J = 0; J < s->nc[1]; J++)
             for (int I = 0; I < s->nc[0]; I++) {
@@ -1204,6 +1240,7 @@ static void rhs(S* s, float gamma) {
 /* clearfine_kernel! / clearcoarse_kernel! (:1964-1974) */
 static void clear(S* s) {
     const ors_basin* B = s->B;
+    #pragma omp parallel for schedule(static)
     for (int64_t sl = 1; sl <= s->nsl; sl++) {
         if (whereof(s, sl)[0] < 0) continue;
         for (int c = 0; c < BCELLS; c++) {
@@ -1211,6 +1248,7 @@ static void clear(S* s) {
             if (B->tf[n] != LIQUID) B->Pf[n] = 0.0f;
         }
     }
+    #pragma omp parallel for schedule(static)
     for (int K = 0; K < s->nc[2]; K++)
         for (int J = 0; J < s->nc[1]; J++)
             for (int I = 0; I < s->nc[0]; I++) {
@@ -1223,6 +1261,7 @@ static float volume(const S* s) {
     const ors_basin* B = s->B;
     const float dx = B->g.dx, cdx = (float)RATIO * dx;
     double sf = 0.0, sc = 0.0;
+    #pragma omp parallel for schedule(static) reduction(+ : sf)
     for (int64_t sl = 1; sl <= s->nsl; sl++) {
         const int32_t* w = whereof(s, sl);
         if (w[0] < 0) continue;
@@ -1231,6 +1270,7 @@ static float volume(const S* s) {
             if (!issolid_fine(&B->g, I, J, K)) sf += (double)clampf(0.5f - B->phif[(sl - 1) * BCELLS + c] / dx, 0.0f, 1.0f);
         }
     }
+    #pragma omp parallel for schedule(static) reduction(+ : sc)
     for (int K = 0; K < s->nc[2]; K++)
         for (int J = 0; J < s->nc[1]; J++)
             for (int I = 0; I < s->nc[0]; I++) {
@@ -1262,6 +1302,7 @@ static void gradient(S* s) {
         int e[3], fm[3];
         unitv(a, e);
         fdims(s->nc, a, fm);
+        #pragma omp parallel for schedule(static)
         for (int64_t sl = 1; sl <= s->nsl; sl++) {
             const int32_t* w = whereof(s, sl);
             if (w[0] < 0) continue;
@@ -1288,6 +1329,7 @@ static void gradient(S* s) {
             }
         }
         const int n1 = s->nc[0], n2 = s->nc[1], n3 = s->nc[2];
+        #pragma omp parallel for schedule(static)
         for (int K = 0; K < fm[2]; K++)
             for (int J = 0; J < fm[1]; J++)
                 for (int I = 0; I < fm[0]; I++) {
@@ -1311,6 +1353,7 @@ static void gradient(S* s) {
                 }
         /* restrict!(s, f, a) then restrict!(s, fl, a): the coarse faces fine blocks hold */
         for (int pass = 0; pass < 2; pass++)
+            #pragma omp parallel for schedule(static)
             for (int K = 0; K < fm[2]; K++)
                 for (int J = 0; J < fm[1]; J++)
                     for (int I = 0; I < fm[0]; I++) {
