@@ -1365,9 +1365,10 @@ int mpp_sparse_ctx_create(mpp_sparse_ctx** out, const mpp_sparse_grid* g, int32_
     c->actc = c->D[0].act;
     if (int e2 = sp_alloc_n(c, &c->st, 1)) return fail(e2);
     if (int e2 = sp_alloc_n(c, &c->dres, 1)) return fail(e2);
-    // a reduction's partial sums: K <= 2 values for every CTA of its launch, which holds a CTA
-    // per slot and at most nsm * 8 for the coarse grid (or nsm * 8 in all)
-    if (int e2 = sp_alloc_n(c, &c->partials, ((int64_t)capacity + (int64_t)c->nsm * 8) * 2)) return fail(e2);
+    // a reduction's partial sums: K <= 2 values for every CTA of its launch, whose fine part
+    // is a CTA per slot or at most nsm * 8 grid-stride CTAs, and its coarse part at most nsm * 8
+    const int64_t cap8 = (int64_t)c->nsm * 8;
+    if (int e2 = sp_alloc_n(c, &c->partials, (std::max((int64_t)capacity, cap8) + cap8) * 2)) return fail(e2);
     if (int e2 = sp_alloc_n(c, &c->counters, SCNT_N)) return fail(e2);
     if (cudaMallocHost((void**)&c->st_host, sizeof(SpState)) != cudaSuccess ||
         cudaMallocHost((void**)&c->dres_host, sizeof(double)) != cudaSuccess) {
