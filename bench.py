@@ -842,6 +842,25 @@ def bench_sparse(steps, cpu=True):
     return out
 
 
+def run_sparse_ncu(steps):
+    """The sparse workload's projections with the CG loop driven from the host (every kernel
+    its own launch, for a profiler's launch list); each starts from the same P and velocities."""
+    import torch
+
+    from mpp import sparse as msp
+    from mpp import sparse_scene as ss
+
+    sc = ss.charybdis()
+    s = msp.SparseBasin.from_scene(sc, graph=False, tol=1e-4, maxiter=200)
+    saved = {k: getattr(s, k).clone() for k in ("Pf", "Pc", "uf", "uc", "vf", "vc", "wf", "wc")}
+    for _ in range(max(1, steps)):
+        for k, v in saved.items():
+            getattr(s, k).copy_(v)
+        msp.project(s, DT)
+    torch.cuda.synchronize()
+    print(json.dumps({"sparse_ncu": True, "iterations": s.iterations, "launches": int(s.last.kernel_launches)}))
+
+
 def bench_whirlpool(steps):
     """384 x 384 x 256 whirlpool, mixed precision with the FGMRES fallback to 1e-6: projections/s,
     the FP64 form's pressure error, and achieved HBM GB/s per kernel family."""
@@ -967,7 +986,12 @@ def main():
                     help="profiling mode: --steps headline projections from the host loop, nothing timed")
     ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "plain64", "box128"],
                     help="--ncu mode: the basin profiled (a smaller one to size a capture)")
+    ap.add_argument("--sparse-ncu", action="store_true",
+                    help="profiling mode: --steps projections of the sparse workload from the host loop, nothing timed")
     args = ap.parse_args()
+    if args.sparse_ncu:
+        run_sparse_ncu(args.steps)
+        return
     if args.warmup < 3 and args.impl == "mpp" and not args.ncu:
         ap.error("--warmup must be at least 3")
     if args.impl == "reference":

@@ -1824,12 +1824,13 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
             B.orr = coarsest ? 0 : take(cs * Nl);
             B.ocode = take(Nl);
             B.odc = take(Nl);
+            B.olist = coarsest ? 0 : take(2 * sizeof(uint16_t) * Nl);
         }
         c->bot_smem = o;
         c->restrict_smem = (size_t)restrict_smem_bytes((int)msize(c->prec), (int)cs);
         int optin = 0;
         CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
-        if (c->bot_smem > (size_t)optin) {
+        if (c->bot_smem + 2 * BOTTOM_MAXLEV * sizeof(int) > (size_t)optin) {  // with the list counts
             set_err("the bottom levels need %zu bytes of shared memory; the device allows %d", c->bot_smem, optin);
             return fail(MPP_ERR_INVALID);
         }
@@ -1838,7 +1839,10 @@ int mpp_ctx_create(mpp_ctx** out, const mpp_grid* g, const mpp_opts* o) {
             // The limit is the function's, shared by every context of the process: raise it
             // to the device's maximum once rather than to this basin's need, which would
             // lower it under a larger basin created earlier.
-            CK(cudaFuncSetAttribute(k_bottom<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            cudaFuncAttributes fb;
+            CK(cudaFuncGetAttributes(&fb, k_bottom<Pr>));  // its static part (the list counts)
+            CK(cudaFuncSetAttribute(k_bottom<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    optin - (int)fb.sharedSizeBytes));
             CK(cudaFuncSetAttribute(k_restrict<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)c->restrict_smem));
             return MPP_OK;
@@ -2040,7 +2044,9 @@ template <class Pr>
 int group_attrs(const mpp_ctx* c) {
     int optin = 0;
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
-    CK(cudaFuncSetAttribute(k_bottom_g<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    cudaFuncAttributes fb;
+    CK(cudaFuncGetAttributes(&fb, k_bottom_g<Pr>));  // its static part (the list counts)
+    CK(cudaFuncSetAttribute(k_bottom_g<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fb.sharedSizeBytes));
     CK(cudaFuncSetAttribute(k_restrict_g<Pr>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->restrict_smem));
     for (auto kern : {k_cmg_g<Pr, 0>, k_cmg_g<Pr, 1>}) {
         cudaFuncAttributes fa;

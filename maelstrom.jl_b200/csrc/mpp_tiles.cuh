@@ -491,6 +491,7 @@ struct BotLev {
     const uint8_t* code;  // stencil codes, natural order, global (k_level)
     const uint8_t* dc;    // non-SOLID neighbour counts, natural order, global (k_level)
     int ox, ob, orr, ocode, odc;  // shared-memory offsets (bytes)
+    int olist;            // the level's LIQUID cells by colour (uint16 indices), levels above the coarsest
 };
 struct BotArgs {
     int nl;  // levels in shared memory, the last one the coarsest
@@ -509,14 +510,26 @@ __device__ __forceinline__ void bottom_dev(const typename Pr::C* __restrict__ bi
     const int T = blockDim.x, tid = threadIdx.x;
     // codes and non-SOLID neighbour counts of every level, and level lb's right-hand side
     // (restricted from the level above by k_restrict_bottom)
+    // per level above the coarsest: its LIQUID cells listed by colour (the red-black passes
+    // walk a colour's list; the order within a list does not matter, a colour's cells being
+    // independent of each other)
+    __shared__ int lcount[BOTTOM_MAXLEV][2];
+    if (tid < 2 * BOTTOM_MAXLEV) lcount[tid >> 1][tid & 1] = 0;
+    __syncthreads();
     for (int l = 0; l < a.nl; l++) {
         const BotLev& B = a.lv[l];
         const int N = B.n1 * B.n2 * B.n3;
         uint8_t* code = smraw + B.ocode;
         uint8_t* dc = smraw + B.odc;
         for (int c = tid; c < N; c += T) {
-            code[c] = B.code[c];
+            const uint8_t cd = B.code[c];
+            code[c] = cd;
             dc[c] = B.dc[c];
+            if (l + 1 < a.nl && (cd & SELF)) {
+                const int i = c % B.n1, j = (c / B.n1) % B.n2, k = c / (B.n1 * B.n2);
+                const int col = (i + j + k + 1) & 1;
+                reinterpret_cast<uint16_t*>(smraw + B.olist)[col * N + atomicAdd(&lcount[l][col], 1)] = (uint16_t)c;
+            }
         }
     }
     {
@@ -561,11 +574,11 @@ __device__ __forceinline__ void bottom_dev(const typename Pr::C* __restrict__ bi
         const uint8_t* dc = smraw + B.odc;
         C* x = reinterpret_cast<C*>(smraw + B.ox);
         const C* b = reinterpret_cast<const C*>(smraw + B.ob);
-        for (int c = tid; c < N; c += T) {
+        const uint16_t* lst = reinterpret_cast<const uint16_t*>(smraw + B.olist) + colour * N;
+        const int nl = lcount[l][colour];
+        for (int e = tid; e < nl; e += T) {
+            const int c = lst[e];
             const uint8_t cd = code[c];
-            if (!(cd & SELF)) continue;
-            const int i = c % B.n1, j = (c / B.n1) % B.n2, k = c / sz;
-            if (((i + j + k + 1) & 1) != colour) continue;
             C s = (C)0;
             if (cd & 1) s += x[c + 1];
             if (cd & 2) s += x[c - 1];
@@ -587,21 +600,27 @@ __device__ __forceinline__ void bottom_dev(const typename Pr::C* __restrict__ bi
         C* x = reinterpret_cast<C*>(smraw + B.ox);
         C* b = reinterpret_cast<C*>(smraw + B.ob);
         C* r = reinterpret_cast<C*>(smraw + B.orr);
-        for (int c = tid; c < N; c += T) {  // start_kernel!
-            C v = (C)0;
-            const int i = c % B.n1, j = (c / B.n1) % B.n2, k = c / sz;
-            if (((i + j + k + 1) & 1) == 0 && (code[c] & SELF)) {
+        // start_kernel!: x = b / diag on colour 0's LIQUID cells, zero elsewhere
+        for (int c = tid; c < N; c += T) x[c] = (C)0;
+        __syncthreads();
+        {
+            const uint16_t* lst = reinterpret_cast<const uint16_t*>(smraw + B.olist);
+            const int nl = lcount[l][0];
+            for (int e = tid; e < nl; e += T) {
+                const int c = lst[e];
                 const C d = (C)dc[c];
-                if (d > (C)0) v = b[c] / d;
+                if (d > (C)0) x[c] = b[c] / d;
             }
-            x[c] = v;
         }
         __syncthreads();
         for (int q = 1; q < 2 * sw; q++) sweep(l, q & 1);  // down: colours 1, 0, 1, ...
-        for (int c = tid; c < N; c += T) {  // residual_kernel!
+        // residual_kernel! on the LIQUID cells (the restriction reads r nowhere else)
+        for (int e = tid; e < lcount[l][0] + lcount[l][1]; e += T) {
+            const int col = e < lcount[l][0] ? 0 : 1;
+            const int c = reinterpret_cast<const uint16_t*>(smraw + B.olist)[col * N + (col ? e - lcount[l][0] : e)];
             const uint8_t cd = code[c];
             C v = (C)0;
-            if (cd & SELF) {
+            {
                 C s = (C)0;
                 if (cd & 1) s += x[c + 1];
                 if (cd & 2) s += x[c - 1];
@@ -692,8 +711,10 @@ __device__ __forceinline__ void bottom_dev(const typename Pr::C* __restrict__ bi
         const uint8_t* ccode = smraw + Bc.ocode;
         C* x = reinterpret_cast<C*>(smraw + B.ox);
         const bool coarsest = l + 2 == a.nl;
-        for (int c = tid; c < N; c += T) {
-            if (!(code[c] & SELF)) continue;
+        (void)code;
+        for (int e = tid; e < lcount[l][0] + lcount[l][1]; e += T) {  // the LIQUID cells
+            const int col = e < lcount[l][0] ? 0 : 1;
+            const int c = reinterpret_cast<const uint16_t*>(smraw + B.olist)[col * N + (col ? e - lcount[l][0] : e)];
             const int i = c % B.n1, j = (c / B.n1) % B.n2, k = c / (B.n1 * B.n2);
             int a0, a1, b0, b1, k0, k1;
             C wa0, wa1, wb0, wb1, wc0, wc1;
