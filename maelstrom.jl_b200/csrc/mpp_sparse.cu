@@ -62,21 +62,6 @@ void sp_launch(void (*kern)(KArgs...), dim3 grid, int block, cudaStream_t st, Ar
     cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
-template <typename... KArgs, typename... Args>
-void sp_launch_sm(void (*kern)(KArgs...), dim3 grid, int block, size_t smem, cudaStream_t st, Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = dim3((unsigned)block);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
-}
-
 }  // namespace
 
 // ---- the CG kernels (src/sflip.jl:1766-1904) ----
@@ -196,127 +181,90 @@ __device__ __forceinline__ double dot4m(float4 a, float4 b, uchar4 m, uint8_t wa
     return s;
 }
 
-// Level 0's Jacobi sweeps and residual (jacobifine_kernel! / residualfine_kernel! and their
-// coarse counterparts, src/sflip.jl:1219-1270): a CTA per slot, then the coarse share.
+// Level 0's Jacobi sweeps and residual: the fine part a CTA per slot (staged block), the
+// coarse part as jacobicoarse_kernel! / residualcoarse_kernel!.
 template <int OP>
-__global__ void __launch_bounds__(SPT, 3) k_sp_blk(Topo t, Comp L, const uint16_t* code0, const float* dg0, float* outf,
-                                                   float* outc, const float* xf, const float* xc, const float* bf,
-                                                   const float* bc) {
+__global__ void __launch_bounds__(SPT) k_sp_blk(Topo t, Comp L, const uint16_t* code0, const float* dg0, float* outf,
+                                                float* outc, const float* xf, const float* xc, const float* bf,
+                                                const float* bc, int gf) {
+    __shared__ float xs[PCELLS];
     pdl_wait();
     pdl_trigger();
-    constexpr bool ZS = OP == BOP_JAC_ZS;
-    block_part<OP, true>(t, code0, dg0, bf, xf, xc,
-                         [&](int64_t n, const float* v, const float*, const unsigned*, const float*) {
-                             st4(outf + n, make_float4(v[0], v[1], v[2], v[3]));
-                         });
-    const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-    SP_COARSE_SHARE(c, nc) {
-        int I, J, K;
-        coarse_cell(t, c, I, J, K);
-        float v = 0.0f;
-        if (L.actc[c] != 0 && !covered(t, I, J, K)) {
-            float diag, off;
-            coarserow<16, ZS>(t, L, xf, xc, I, J, K, diag, off);
-            const float x0 = ZS ? 0.0f : xc[c];
-            if (OP == BOP_RES) v = bc[c] - (diag * x0 - off);
-            else v = diag > 0.0f ? x0 + OMEGA * (bc[c] - (diag * x0 - off)) / diag : 0.0f;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
+        int w[3];
+        where_of(t, sl, w);
+        if (w[0] < 0) return;
+        if (OP != BOP_JAC_ZS) {
+            stage_block(t, xf, xc, sl, w, xs);
+            __syncthreads();
         }
-        outc[c] = v;
+        block_cells<OP>(code0, dg0, bf, xs, sl, [&](int64_t n, const float* v, const float*) {
+            st4(outf + n, make_float4(v[0], v[1], v[2], v[3]));
+        });
+    } else {
+        constexpr bool ZS = OP == BOP_JAC_ZS;
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            int I, J, K;
+            coarse_cell(t, c, I, J, K);
+            float v = 0.0f;
+            if (L.actc[c] != 0 && !covered(t, I, J, K)) {
+                float diag, off;
+                coarserow<16, ZS>(t, L, xf, xc, I, J, K, diag, off);
+                const float x0 = ZS ? 0.0f : xc[c];
+                if (OP == BOP_RES) v = bc[c] - (diag * x0 - off);
+                else v = diag > 0.0f ? x0 + OMEGA * (bc[c] - (diag * x0 - off)) / diag : 0.0f;
+            }
+            outc[c] = v;
+        }
     }
 }
 
-// The CG V-cycle's last level-0 sweep (from its smoothing buffer into z) with the flexible
-// beta folded in: z.r and z.r_old over the unknowns as the new z is written, then in the last
-// CTA rho_new = z.r and beta = max(0, (rho_new - z.r_old) / rho) (src/sflip.jl:1895-1900),
-// so no separate pass reads z, r and r_old again.
-__global__ void __launch_bounds__(SPT, 3) k_sp_jac_dots(Topo t, Comp L, const uint16_t* code0, const float* dg0,
-                                                        float* zf, float* zc, const float* xf, const float* xc,
-                                                        const float* rf, const float* rc, const float* rof,
-                                                        const float* roc, const uint8_t* cmask, SpState* st,
-                                                        double* partials, unsigned* counter) {
-    pdl_wait();
-    pdl_trigger();
-    double acc[2] = {0.0, 0.0};
-    block_part<BOP_JAC, true>(t, code0, dg0, rf, xf, xc,
-                              [&](int64_t n, const float* v, const float*, const unsigned* cs, const float* rs) {
-                                  st4(zf + n, make_float4(v[0], v[1], v[2], v[3]));
-                                  const float4 ro = ld4(rof + n);
-                                  const float ros[4] = {ro.x, ro.y, ro.z, ro.w};
-#pragma unroll
-                                  for (int u = 0; u < 4; u++)
-                                      if (cs[u] & (1u << 13)) {
-                                          acc[0] += (double)v[u] * (double)rs[u];
-                                          acc[1] += (double)v[u] * (double)ros[u];
-                                      }
-                              });
-    const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-    SP_COARSE_SHARE(c, nc) {
-        int I, J, K;
-        coarse_cell(t, c, I, J, K);
-        float v = 0.0f;
-        if (L.actc[c] != 0 && !covered(t, I, J, K)) {
-            float diag, off;
-            coarserow<16, false>(t, L, xf, xc, I, J, K, diag, off);
-            const float x0 = xc[c];
-            v = diag > 0.0f ? x0 + OMEGA * (rc[c] - (diag * x0 - off)) / diag : 0.0f;
-        }
-        zc[c] = v;
-        if (cmask[c]) {
-            acc[0] += (double)v * (double)rc[c];
-            acc[1] += (double)v * (double)roc[c];
-        }
-    }
-    if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0 && !st->done) {
-        const float rnew = (float)acc[0];
-        if (!(rnew > 0.0f)) {
-            st->status = MPP_INDEFINITE;
-            st->done = 1;
-        } else {
-            float beta = (rnew - (float)acc[1]) / st->rho;
-            beta = beta != beta ? beta : (beta > 0.0f ? beta : 0.0f);  // Julia's max(0f0, x)
-            st->beta = beta;
-            if (!isfinite(beta)) {
-                st->status = MPP_NONFINITE;
-                st->done = 1;
-            }
-            st->rho = rnew;
-        }
-    }
+// q = A x at level 0 for the CG kernels (apply!, src/sflip.jl:1824-1847): the fine part of
+// slot sl through the staged block; `sink(n, q[4], x[4])`.
+template <class Sink>
+__device__ __forceinline__ void apply_block(const Topo& t, const uint16_t* code0, const float* dg0, const float* xf,
+                                            const float* xc, int sl, const int w[3], float* xs, Sink&& sink) {
+    stage_block(t, xf, xc, sl, w, xs);
+    __syncthreads();
+    block_cells<BOP_APPLY>(code0, dg0, nullptr, xs, sl, sink);
 }
 
 // r = b - A P (apply! then xpby!(r, b, -1)), |b| and |r| (src/sflip.jl:1870-1877).
-__global__ void __launch_bounds__(SPT, 3) k_sp_start(Topo t, Comp L, const uint16_t* code0, const float* dg0,
-                                                     const uint8_t* cmask, const float* Pf, const float* Pc,
-                                                     const float* bf, const float* bc, float* rf, float* rc,
-                                                     SpState* st, double* partials, unsigned* counter) {
+__global__ void __launch_bounds__(SPT) k_sp_start(Topo t, Comp L, const uint16_t* code0, const float* dg0,
+                                                  const uint8_t* tf, const uint8_t* cmask, const float* Pf,
+                                                  const float* Pc, const float* bf, const float* bc, float* rf,
+                                                  float* rc, SpState* st, double* partials, unsigned* counter, int gf) {
+    __shared__ float xs[PCELLS];
     pdl_wait();
     pdl_trigger();
     double acc[2] = {0.0, 0.0};
-    block_part<BOP_APPLY, false>(t, code0, dg0, nullptr, Pf, Pc,
-                                [&](int64_t n, const float* q, const float*, const unsigned* cs, const float*) {
-                                    // b as given (the prefetch feeds only the Jacobi and residual forms)
-                                    const float4 b4 = ld4(bf + n);
-                                    const float bs[4] = {b4.x, b4.y, b4.z, b4.w};
-                                    float r[4];
-#pragma unroll
-                                    for (int u = 0; u < 4; u++) {
-                                        r[u] = bs[u] + (-1.0f) * q[u];
-                                        if (cs[u] & (1u << 13)) {
-                                            acc[0] += (double)bs[u] * (double)bs[u];
-                                            acc[1] += (double)r[u] * (double)r[u];
-                                        }
-                                    }
-                                    st4(rf + n, make_float4(r[0], r[1], r[2], r[3]));
-                                });
-    const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-    SP_COARSE_SHARE(c, nc) {
-        bool cov;
-        const float q = apply_coarse(t, L, Pf, Pc, c, cov);
-        const float r = bc[c] + (-1.0f) * q;
-        rc[c] = r;
-        if (cmask[c]) {
-            acc[0] += (double)bc[c] * (double)bc[c];
-            acc[1] += (double)r * (double)r;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
+        int w[3];
+        where_of(t, sl, w);
+        if (w[0] >= 0)
+            apply_block(t, code0, dg0, Pf, Pc, sl, w, xs, [&](int64_t n, const float* q, const float*) {
+                const float4 b = ld4(bf + n);
+                const float4 r = make_float4(b.x + (-1.0f) * q[0], b.y + (-1.0f) * q[1], b.z + (-1.0f) * q[2],
+                                             b.w + (-1.0f) * q[3]);
+                st4(rf + n, r);
+                const uchar4 m = ldm4(tf + n);
+                acc[0] += dot4m(b, b, m, LIQUID);
+                acc[1] += dot4m(r, r, m, LIQUID);
+            });
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            bool cov;
+            const float q = apply_coarse(t, L, Pf, Pc, c, cov);
+            const float r = bc[c] + (-1.0f) * q;
+            rc[c] = r;
+            if (cmask[c]) {
+                acc[0] += (double)bc[c] * (double)bc[c];
+                acc[1] += (double)r * (double)r;
+            }
         }
     }
     if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0) {
@@ -378,27 +326,33 @@ __global__ void __launch_bounds__(SPT) k_sp_dinit(Topo t, const uint8_t* tf, con
 }
 
 // q = A d and d.q -> alpha = rho / d.q (src/sflip.jl:1885-1889).
-__global__ void __launch_bounds__(SPT, 3) k_sp_apply_dot(Topo t, Comp L, const uint16_t* code0, const float* dg0,
-                                                         const uint8_t* cmask, const float* df, const float* dc,
-                                                         float* qf, float* qc, SpState* st, double* partials,
-                                                         unsigned* counter) {
+__global__ void __launch_bounds__(SPT) k_sp_apply_dot(Topo t, Comp L, const uint16_t* code0, const float* dg0,
+                                                      const uint8_t* tf, const uint8_t* cmask, const float* df,
+                                                      const float* dc, float* qf, float* qc, SpState* st,
+                                                      double* partials, unsigned* counter, int gf) {
+    __shared__ float xs[PCELLS];
     pdl_wait();
     pdl_trigger();
     if (st->done) return;
     double acc[1] = {0.0};
-    block_part<BOP_APPLY, false>(t, code0, dg0, nullptr, df, dc,
-                                 [&](int64_t n, const float* q, const float* x, const unsigned* cs, const float*) {
-                                     st4(qf + n, make_float4(q[0], q[1], q[2], q[3]));
-#pragma unroll
-                                     for (int u = 0; u < 4; u++)
-                                         if (cs[u] & (1u << 13)) acc[0] += (double)x[u] * (double)q[u];
-                                 });
-    const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-    SP_COARSE_SHARE(c, nc) {
-        bool cov;
-        const float q = apply_coarse(t, L, df, dc, c, cov);
-        qc[c] = q;
-        if (cmask[c]) acc[0] += (double)dc[c] * (double)q;
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
+        int w[3];
+        where_of(t, sl, w);
+        if (w[0] >= 0)
+            apply_block(t, code0, dg0, df, dc, sl, w, xs, [&](int64_t n, const float* q, const float* x) {
+                st4(qf + n, make_float4(q[0], q[1], q[2], q[3]));
+                acc[0] += dot4m(make_float4(x[0], x[1], x[2], x[3]), make_float4(q[0], q[1], q[2], q[3]),
+                                ldm4(tf + n), LIQUID);
+            });
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            bool cov;
+            const float q = apply_coarse(t, L, df, dc, c, cov);
+            qc[c] = q;
+            if (cmask[c]) acc[0] += (double)dc[c] * (double)q;
+        }
     }
     if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
         const float den = (float)acc[0];
@@ -466,6 +420,49 @@ __global__ void __launch_bounds__(SPT) k_sp_update(Topo t, const uint8_t* tf, co
     }
 }
 
+// rho_new = z.r and z.r_old -> beta = max(0, (rho_new - z.r_old) / rho) (src/sflip.jl:1895-1900).
+__global__ void __launch_bounds__(SPT) k_sp_dot2(Topo t, const uint8_t* tf, const uint8_t* cmask, const float* zf,
+                                                 const float* zc, const float* rf, const float* rc, const float* rof,
+                                                 const float* roc, SpState* st, double* partials, unsigned* counter,
+                                                 int gf) {
+    pdl_wait();
+    pdl_trigger();
+    if (st->done) return;
+    double acc[2] = {0.0, 0.0};
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
+        if (slot_used(t, sl)) SP_SLOT_PIECES(n) {
+                const float4 z = ld4(zf + n);
+                const uchar4 m = ldm4(tf + n);
+                acc[0] += dot4m(z, ld4(rf + n), m, LIQUID);
+                acc[1] += dot4m(z, ld4(rof + n), m, LIQUID);
+            }
+    } else {
+        SP_COARSE_PIECES(c, (int64_t)t.nc[0] * t.nc[1] * t.nc[2] / 4, gf) {
+            const float4 z = ld4(zc + c);
+            const uchar4 m = ldm4(cmask + c);
+            acc[0] += dot4m(z, ld4(rc + c), m, 1);
+            acc[1] += dot4m(z, ld4(roc + c), m, 1);
+        }
+    }
+    if (grid_sum<2>(acc, partials, counter) && threadIdx.x == 0) {
+        const float rnew = (float)acc[0];
+        if (!(rnew > 0.0f)) {
+            st->status = MPP_INDEFINITE;
+            st->done = 1;
+        } else {
+            float beta = (rnew - (float)acc[1]) / st->rho;
+            beta = beta != beta ? beta : (beta > 0.0f ? beta : 0.0f);  // Julia's max(0f0, x)
+            st->beta = beta;
+            if (!isfinite(beta)) {
+                st->status = MPP_NONFINITE;
+                st->done = 1;
+            }
+            st->rho = rnew;
+        }
+    }
+}
+
 // d = z + beta d (xpby!, src/sflip.jl:1902).
 __global__ void __launch_bounds__(SPT) k_sp_xpby(Topo t, float* df, float* dc, const float* zf, const float* zc,
                                                  const SpState* st, int gf) {
@@ -520,18 +517,25 @@ __global__ void __launch_bounds__(SPT) k_sp_prolong10(Topo t, float* zf, float* 
 
 // ---- the FGMRES fallback's vector passes (src/fgmres.jl:26-92) ----
 // q = A x (apply!)
-__global__ void __launch_bounds__(SPT, 3) k_sp_apply(Topo t, Comp L, const uint16_t* code0, const float* dg0,
-                                                     const float* xf, const float* xc, float* qf, float* qc) {
+__global__ void __launch_bounds__(SPT) k_sp_apply(Topo t, Comp L, const uint16_t* code0, const float* dg0,
+                                                  const float* xf, const float* xc, float* qf, float* qc, int gf) {
+    __shared__ float xs[PCELLS];
     pdl_wait();
     pdl_trigger();
-    block_part<BOP_APPLY, false>(t, code0, dg0, nullptr, xf, xc,
-                                 [&](int64_t n, const float* q, const float*, const unsigned*, const float*) {
-                                     st4(qf + n, make_float4(q[0], q[1], q[2], q[3]));
-                                 });
-    const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-    SP_COARSE_SHARE(c, nc) {
-        bool cov;
-        qc[c] = apply_coarse(t, L, xf, xc, c, cov);
+    if (sp_is_fine(gf)) {
+        const int sl = sp_slot(gf);
+        int w[3];
+        where_of(t, sl, w);
+        if (w[0] < 0) return;
+        apply_block(t, code0, dg0, xf, xc, sl, w, xs, [&](int64_t n, const float* q, const float*) {
+            st4(qf + n, make_float4(q[0], q[1], q[2], q[3]));
+        });
+    } else {
+        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+        SP_COARSE_LOOP(c, nc, gf) {
+            bool cov;
+            qc[c] = apply_coarse(t, L, xf, xc, c, cov);
+        }
     }
 }
 // a.b over the unknowns (inner), FP64, into *out
@@ -753,28 +757,18 @@ int cap_blocks(const mpp_sparse_ctx* c, int64_t n) {
 struct Split {
     int gf, g;
 };
-// the coarse part of a fused launch: up to two CTAs a SM's eight (its cells next to fine blocks
-// are slow, so more of them in flight)
-int cap_coarse(const mpp_sparse_ctx* c) {
-    const int64_t g = (c->ncc + SPT - 1) / SPT, cap = (int64_t)c->nsm * 16;
-    return (int)(g < 1 ? 1 : (g < cap ? g : cap));
-}
 Split split_for(const mpp_sparse_ctx* c, int64_t nfine) {
     Split s;
     s.gf = cap_blocks(c, nfine);
-    s.g = s.gf + cap_coarse(c);
+    s.g = s.gf + cap_blocks(c, c->ncc);
     return s;
 }
-
-// the level-0 block kernels: a CTA per slot, each then taking a share of the coarse grid
-int grid_blk0(const mpp_sparse_ctx* c) { return std::max(c->t.nslots, cap_coarse(c)); }
-#define LAUNCH_BLK0(kern, st, ...) sp_launch_sm(kern, dim3(grid_blk0(c)), SPT, (size_t)SP_SMEM, st, __VA_ARGS__)
 
 // a launch whose fine part is a CTA per slot (the block kernels)
 Split split_blk(const mpp_sparse_ctx* c) {
     Split s;
     s.gf = c->t.nslots;
-    s.g = s.gf + cap_coarse(c);
+    s.g = s.gf + cap_blocks(c, c->ncc);
     return s;
 }
 
@@ -857,37 +851,20 @@ struct SpRun {
         }
     }
     // smooth! (src/sflip.jl:1292-1303) after zero!(x): the first sweep from zeros
-    // the CG V-cycle's last level-0 sweep folds in the flexible beta's dots (k_sp_jac_dots)
-    const mpp_sparse_basin* dots_for = nullptr;
-
     template <int N>
     void smooth(const Comp& L, float* xf, float* xc, const float* bf, const float* bc, float* tf_, float* tc_,
-                int sweeps, bool from_zero, bool last = false) {
+                int sweeps, bool from_zero) {
         if (N == 16) {
             const Split sp = split_blk(c);
             for (int q = 0; q < sweeps; q++) {
-                if (last && dots_for && q == sweeps - 1) {
-                    if (q == 0 && from_zero)
-                        LAUNCH_BLK0(k_sp_blk<BOP_JAC_ZS>, s, c->t, L, (const uint16_t*)c->code0,
-                                  (const float*)c->dg0, tf_, tc_, (const float*)xf, (const float*)xc, bf, bc);
-                    else
-                        LAUNCH_BLK0(k_sp_blk<BOP_JAC>, s, c->t, L, (const uint16_t*)c->code0,
-                                  (const float*)c->dg0, tf_, tc_, (const float*)xf, (const float*)xc, bf, bc);
-                    LAUNCH_BLK0(k_sp_jac_dots, s, c->t, L, (const uint16_t*)c->code0,
-                              (const float*)c->dg0, xf, xc, (const float*)tf_, (const float*)tc_, bf, bc,
-                              (const float*)c->rof, (const float*)c->roc, (const uint8_t*)c->cmask, c->st, c->partials,
-                              c->counters + SCNT_DOT2);
-                    nk += 2;
-                    continue;
-                }
                 if (q == 0 && from_zero)
-                    LAUNCH_BLK0(k_sp_blk<BOP_JAC_ZS>, s, c->t, L, (const uint16_t*)c->code0,
-                              (const float*)c->dg0, tf_, tc_, (const float*)xf, (const float*)xc, bf, bc);
+                    sp_launch(k_sp_blk<BOP_JAC_ZS>, dim3(sp.g), SPT, s, c->t, L, (const uint16_t*)c->code0,
+                              (const float*)c->dg0, tf_, tc_, (const float*)xf, (const float*)xc, bf, bc, sp.gf);
                 else
-                    LAUNCH_BLK0(k_sp_blk<BOP_JAC>, s, c->t, L, (const uint16_t*)c->code0,
-                              (const float*)c->dg0, tf_, tc_, (const float*)xf, (const float*)xc, bf, bc);
-                LAUNCH_BLK0(k_sp_blk<BOP_JAC>, s, c->t, L, (const uint16_t*)c->code0,
-                          (const float*)c->dg0, xf, xc, (const float*)tf_, (const float*)tc_, bf, bc);
+                    sp_launch(k_sp_blk<BOP_JAC>, dim3(sp.g), SPT, s, c->t, L, (const uint16_t*)c->code0,
+                              (const float*)c->dg0, tf_, tc_, (const float*)xf, (const float*)xc, bf, bc, sp.gf);
+                sp_launch(k_sp_blk<BOP_JAC>, dim3(sp.g), SPT, s, c->t, L, (const uint16_t*)c->code0,
+                          (const float*)c->dg0, xf, xc, (const float*)tf_, (const float*)tc_, bf, bc, sp.gf);
                 nk += 2;
             }
             return;
@@ -923,8 +900,8 @@ struct SpRun {
         const Split s0 = split_for(c, (int64_t)t.nslots * BCELLS), s1 = split_for(c, (int64_t)t.nslots * BCELLS1);
         smooth<16>(L0, zf, zc, rf, rc, c->tmf, c->tmc, sweeps, true);
         const Split sb = split_blk(c);
-        LAUNCH_BLK0(k_sp_blk<BOP_RES>, s, t, L0, (const uint16_t*)c->code0, (const float*)c->dg0,
-                  c->res0f, c->res0c, (const float*)zf, (const float*)zc, rf, rc);
+        sp_launch(k_sp_blk<BOP_RES>, dim3(sb.g), SPT, s, t, L0, (const uint16_t*)c->code0, (const float*)c->dg0,
+                  c->res0f, c->res0c, (const float*)zf, (const float*)zc, rf, rc, sb.gf);
         sp_launch(k_sp_restrict01, dim3(grid1((int64_t)t.nslots * BCELLS1)), SPT, s, t, c->b1f,
                   (const float*)c->res0f);
         nk += 2;
@@ -946,7 +923,7 @@ struct SpRun {
         {
             const DL& Dm = c->D[c->nd - 1];
             const int cells = Dm.n[0] * Dm.n[1] * Dm.n[2];
-            sp_launch(k_sp_coarsest, dim3(1), (cells + 31) / 32 * 32, s, Dm, coarse);
+            sp_launch(k_sp_coarsest, dim3(1), (cells + 31) / 32 * 32, s, Dm, coarse);  // a thread a cell
         }
         nk++;
         for (int l = c->nd - 2; l >= 0; l--) {
@@ -962,7 +939,7 @@ struct SpRun {
         sp_launch(k_sp_prolong10, dim3(sb.g), SPT, s, t, zf, zc, (const float*)c->x1f, (const float*)c->x1c, tf,
                   (const uint8_t*)c->actc, boost, sb.gf);
         nk++;
-        smooth<16>(L0, zf, zc, rf, rc, c->tmf, c->tmc, sweeps, false, true);
+        smooth<16>(L0, zf, zc, rf, rc, c->tmf, c->tmc, sweeps, false);
     }
     // the CG's prologue up to the loop: r, the norms, the first V-cycle, d and rho, and
     // the first iteration's q, alpha and update (the rotated loop's body starts with the
@@ -972,10 +949,10 @@ struct SpRun {
         const Topo& t = c->t;
         const Comp L0 = comp0(c, b->types_f);
         const Split s0 = split_blk(c);
-        LAUNCH_BLK0(k_sp_start, s, t, L0, (const uint16_t*)c->code0, (const float*)c->dg0,
-                  (const uint8_t*)c->cmask, (const float*)b->P_f, (const float*)b->P_c,
+        sp_launch(k_sp_start, dim3(s0.g), SPT, s, t, L0, (const uint16_t*)c->code0, (const float*)c->dg0,
+                  b->types_f, (const uint8_t*)c->cmask, (const float*)b->P_f, (const float*)b->P_c,
                   (const float*)c->bf, (const float*)c->bc, c->rf, c->rc, c->st, c->partials,
-                  c->counters + SCNT_START);
+                  c->counters + SCNT_START, s0.gf);
         vcycle(b->types_f, c->zf, c->zc, c->rf, c->rc, o->sweeps, o->coarse, o->boost);
         sp_launch(k_sp_dinit, dim3(s0.g), SPT, s, t, b->types_f, (const uint8_t*)c->cmask, (const float*)c->zf,
                   (const float*)c->zc, (const float*)c->rf, (const float*)c->rc, c->df, c->dc, c->st, c->partials,
@@ -987,9 +964,9 @@ struct SpRun {
         const Topo& t = c->t;
         const Comp L0 = comp0(c, b->types_f);
         const Split s0 = split_blk(c);
-        LAUNCH_BLK0(k_sp_apply_dot, s, t, L0, (const uint16_t*)c->code0, (const float*)c->dg0,
-                  (const uint8_t*)c->cmask, (const float*)c->df, (const float*)c->dc, c->qf, c->qc, c->st,
-                  c->partials, c->counters + SCNT_DQ);
+        sp_launch(k_sp_apply_dot, dim3(s0.g), SPT, s, t, L0, (const uint16_t*)c->code0, (const float*)c->dg0,
+                  b->types_f, (const uint8_t*)c->cmask, (const float*)c->df, (const float*)c->dc, c->qf, c->qc, c->st,
+                  c->partials, c->counters + SCNT_DQ, s0.gf);
         sp_launch(k_sp_update, dim3(s0.g), SPT, s, t, b->types_f, (const uint8_t*)c->cmask, b->P_f, b->P_c, c->rf, c->rc, c->rof,
                   c->roc, (const float*)c->df, (const float*)c->dc, (const float*)c->qf, (const float*)c->qc, c->st,
                   c->partials, c->counters + SCNT_UPD, s0.gf, cond, use_cond);
@@ -999,12 +976,13 @@ struct SpRun {
     void cg_body(const mpp_sparse_basin* b, const mpp_sparse_opts* o, cudaGraphConditionalHandle cond, int use_cond) {
         const Topo& t = c->t;
         const Split s0 = split_blk(c);
-        dots_for = b;  // the V-cycle's last sweep also forms z.r, z.r_old and beta
         vcycle(b->types_f, c->zf, c->zc, c->rf, c->rc, o->sweeps, o->coarse, o->boost);
-        dots_for = nullptr;
+        sp_launch(k_sp_dot2, dim3(s0.g), SPT, s, t, b->types_f, (const uint8_t*)c->cmask, (const float*)c->zf, (const float*)c->zc,
+                  (const float*)c->rf, (const float*)c->rc, (const float*)c->rof, (const float*)c->roc, c->st,
+                  c->partials, c->counters + SCNT_DOT2, s0.gf);
         sp_launch(k_sp_xpby, dim3(s0.g), SPT, s, t, c->df, c->dc, (const float*)c->zf, (const float*)c->zc,
                   (const SpState*)c->st, s0.gf);
-        nk += 1;
+        nk += 2;
         cg_step(b, cond, use_cond);
     }
     void gradient(const mpp_sparse_basin* b) {
@@ -1048,8 +1026,8 @@ void axpy(mpp_sparse_ctx* c, SpRun& run, float* yf, float* yc, float a, const fl
 }
 void apply_(mpp_sparse_ctx* c, SpRun& run, const uint8_t* tf, const float* xf, const float* xc, float* qf, float* qc) {
     const Split s0 = split_blk(c);
-    LAUNCH_BLK0(k_sp_apply, run.s, c->t, comp0(c, tf), (const uint16_t*)c->code0, (const float*)c->dg0,
-              xf, xc, qf, qc);
+    sp_launch(k_sp_apply, dim3(s0.g), SPT, run.s, c->t, comp0(c, tf), (const uint16_t*)c->code0, (const float*)c->dg0,
+              xf, xc, qf, qc, s0.gf);
     run.nk++;
 }
 
@@ -1112,9 +1090,9 @@ int fgmres(mpp_sparse_ctx* c, SpRun& run, const mpp_sparse_basin* b, const mpp_s
             run.vcycle(tf, c->zf, c->zc, c->Vf[j], c->Vc[j], o->sweeps, o->coarse, o->boost);
             // the diagonal component: one damped Jacobi step from zero (src/fgmres.jl:15-24)
             const Split s0 = split_blk(c);
-            LAUNCH_BLK0(k_sp_blk<BOP_JAC_ZS>, run.s, c->t, comp0(c, tf), (const uint16_t*)c->code0,
+            sp_launch(k_sp_blk<BOP_JAC_ZS>, dim3(s0.g), SPT, run.s, c->t, comp0(c, tf), (const uint16_t*)c->code0,
                       (const float*)c->dg0, c->Zf[j], c->Zc[j], (const float*)nullptr, (const float*)nullptr,
-                      (const float*)c->Vf[j], (const float*)c->Vc[j]);
+                      (const float*)c->Vf[j], (const float*)c->Vc[j], s0.gf);
             run.nk++;
             axpy(c, run, c->Zf[j], c->Zc[j], 1.0f, c->zf, c->zc, 0, 0);
             apply_(c, run, tf, c->Zf[j], c->Zc[j], c->qf, c->qc);
@@ -1392,25 +1370,14 @@ int mpp_sparse_ctx_create(mpp_sparse_ctx** out, const mpp_sparse_grid* g, int32_
     if (int e2 = sp_alloc_n(c, &c->st, 1)) return fail(e2);
     if (int e2 = sp_alloc_n(c, &c->dres, 1)) return fail(e2);
     // a reduction's partial sums: K <= 2 values for every CTA of its launch, whose fine part
-    // is a CTA per slot or at most nsm * 8 grid-stride CTAs, and its coarse part at most nsm * 16
+    // is a CTA per slot or at most nsm * 8 grid-stride CTAs, and its coarse part at most nsm * 8
     const int64_t cap8 = (int64_t)c->nsm * 8;
-    if (int e2 = sp_alloc_n(c, &c->partials, (std::max((int64_t)capacity, cap8) + 2 * cap8) * 2)) return fail(e2);
+    if (int e2 = sp_alloc_n(c, &c->partials, (std::max((int64_t)capacity, cap8) + cap8) * 2)) return fail(e2);
     if (int e2 = sp_alloc_n(c, &c->counters, SCNT_N)) return fail(e2);
     if (cudaMallocHost((void**)&c->st_host, sizeof(SpState)) != cudaSuccess ||
         cudaMallocHost((void**)&c->dres_host, sizeof(double)) != cudaSuccess) {
         sp_err("cudaMallocHost failed");
         return fail(MPP_ERR_NOMEM);
-    }
-    // the level-0 block kernels' shared memory (beyond the 48 KB default)
-    {
-        const void* kerns[] = {(const void*)k_sp_blk<BOP_JAC>, (const void*)k_sp_blk<BOP_JAC_ZS>,
-                               (const void*)k_sp_blk<BOP_RES>, (const void*)k_sp_jac_dots, (const void*)k_sp_start,
-                               (const void*)k_sp_apply_dot, (const void*)k_sp_apply};
-        for (const void* k : kerns)
-            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SP_SMEM) != cudaSuccess) {
-                sp_err("cudaFuncSetAttribute (shared memory) failed");
-                return fail(MPP_ERR_CUDA);
-            }
     }
     if (cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking) != cudaSuccess) {
         sp_err("cudaStreamCreate failed");

@@ -883,60 +883,20 @@ __device__ __forceinline__ float block_off(const float* xs, int o, unsigned code
 // The block operations: a Jacobi sweep (from x, or from zeros), the residual, and A x.
 enum { BOP_JAC = 0, BOP_JAC_ZS = 1, BOP_RES = 2, BOP_APPLY = 3 };
 
-// A block CTA's dynamic shared memory: the staged x with its halo, then the block's codes,
-// diagonals and right-hand side, copied in by cp.async while x is staged, so that every global
-// load of the CTA is in flight at once and the cells are computed from shared memory.
-constexpr int SM_XS = PCELLS * 4, SM_CODE = BCELLS * 2, SM_DG = BCELLS * 4, SM_B = BCELLS * 4;
-constexpr int SP_SMEM = SM_XS + SM_CODE + SM_DG + SM_B;  // 64,288 bytes: three CTAs a SM
-static_assert(SM_XS % 16 == 0, "the copies land on 16-byte boundaries");
-struct BlkSm {
-    float* xs;
-    uint16_t* code;
-    float* dg;
-    float* b;
-};
-__device__ __forceinline__ BlkSm blk_sm() {
-    extern __shared__ __align__(16) unsigned char sp_sm[];
-    BlkSm m;
-    m.xs = reinterpret_cast<float*>(sp_sm);
-    m.code = reinterpret_cast<uint16_t*>(sp_sm + SM_XS);
-    m.dg = reinterpret_cast<float*>(sp_sm + SM_XS + SM_CODE);
-    m.b = reinterpret_cast<float*>(sp_sm + SM_XS + SM_CODE + SM_DG);
-    return m;
-}
-// Slot sl's codes, diagonals and (WITH_B) right-hand side into shared memory, 16-byte pieces.
-template <bool WITH_B>
-__device__ __forceinline__ void prefetch_block(const uint16_t* code0, const float* dg0, const float* b, int sl,
-                                               const BlkSm& m) {
-    const int tid = (int)threadIdx.x;
-    const int64_t base = (int64_t)(sl - 1) * BCELLS;
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-        const int q = tid + 256 * u;
-        cp_async16(m.code + 8 * q, code0 + base + 8 * q);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-        const int q = tid + 256 * u;
-        cp_async16(m.dg + 4 * q, dg0 + base + 4 * q);
-        if (WITH_B) cp_async16(m.b + 4 * q, b + base + 4 * q);
-    }
-    cp_async_commit();
-}
-
-// One slot's cells through `op`, from shared memory; `sink(n, value, x, code)` receives each
-// piece's results (pool index, the four values, the cells' own x and codes).
+// One slot's cells through `op`; `sink(n, value, x)` receives each cell's result (pool
+// index, value, the cell's own x). The caller has staged x into xs (not for BOP_JAC_ZS).
 template <int OP, class Sink>
-__device__ __forceinline__ void block_cells(const BlkSm& m, int sl, Sink&& sink) {
+__device__ __forceinline__ void block_cells(const uint16_t* __restrict__ code0, const float* __restrict__ dg0,
+                                            const float* __restrict__ b, const float* xs, int sl, Sink&& sink) {
     const int tid = (int)threadIdx.x;
 #pragma unroll 1
-    for (int u4 = 0; u4 < 4; u4++) {
-        const int q = tid + 256 * u4, c = 4 * q, i = c & 15, j = (c >> 4) & 15, k = c >> 8;
+    for (int m = 0; m < 4; m++) {
+        const int q = tid + 256 * m, c = 4 * q, i = c & 15, j = (c >> 4) & 15, k = c >> 8;
         const int64_t n = (int64_t)(sl - 1) * BCELLS + c;
-        const ushort4 cd = *reinterpret_cast<const ushort4*>(m.code + c);
-        const float4 dg = *reinterpret_cast<const float4*>(m.dg + c);
+        const ushort4 cd = *reinterpret_cast<const ushort4*>(code0 + n);
+        const float4 dg = *reinterpret_cast<const float4*>(dg0 + n);
         float4 bb = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (OP != BOP_APPLY) bb = *reinterpret_cast<const float4*>(m.b + c);
+        if (OP != BOP_APPLY) bb = *reinterpret_cast<const float4*>(b + n);
         const unsigned cs[4] = {cd.x, cd.y, cd.z, cd.w};
         const float ds[4] = {dg.x, dg.y, dg.z, dg.w}, bs[4] = {bb.x, bb.y, bb.z, bb.w};
         float out[4], xv[4];
@@ -944,44 +904,23 @@ __device__ __forceinline__ void block_cells(const BlkSm& m, int sl, Sink&& sink)
         for (int u = 0; u < 4; u++) {
             const int o = pidx(i + u, j, k);
             const unsigned code = cs[u];
-            const float x0 = OP == BOP_JAC_ZS ? 0.0f : m.xs[o];
+            const float x0 = OP == BOP_JAC_ZS ? 0.0f : xs[o];
             xv[u] = x0;
             const float diag = ds[u];
             float v = 0.0f;
             if (OP == BOP_APPLY) {
-                if (code & (1u << 13)) v = diag * x0 - block_off<false>(m.xs, o, code);
+                if (code & (1u << 13)) v = diag * x0 - block_off<false>(xs, o, code);
             } else if (code & (1u << 12)) {
-                const float off = OP == BOP_JAC_ZS ? block_off<true>(m.xs, o, code) : block_off<false>(m.xs, o, code);
+                const float off = OP == BOP_JAC_ZS ? block_off<true>(xs, o, code) : block_off<false>(xs, o, code);
                 if (OP == BOP_RES) v = bs[u] - (diag * x0 - off);
                 else v = diag > 0.0f ? x0 + OMEGA * (bs[u] - (diag * x0 - off)) / diag : 0.0f;
             }
             out[u] = v;
         }
-        sink(n, out, xv, cs, bs);
+        sink(n, out, xv);
     }
 }
 
-// The block CTA's part of a fused launch: its slot's cells (CTA b takes slot b + 1 while b <
-// nslots), staged and prefetched, then its share of the coarse grid (a grid-stride range
-// over every CTA), so the coarse cells' work trails each CTA's block instead of taking CTAs
-// of its own.
-template <int OP, bool WITH_B, class Sink>
-__device__ __forceinline__ void block_part(const Topo& t, const uint16_t* code0, const float* dg0, const float* b,
-                                           const float* xf, const float* xc, Sink&& sink) {
-    const int sl = (int)blockIdx.x + 1;
-    if (sl > t.nslots) return;
-    int w[3];
-    where_of(t, sl, w);
-    if (w[0] < 0) return;
-    const BlkSm m = blk_sm();
-    prefetch_block<WITH_B>(code0, dg0, b, sl, m);
-    if (OP != BOP_JAC_ZS) stage_block(t, xf, xc, sl, w, m.xs);
-    cp_async_wait<0>();
-    __syncthreads();
-    block_cells<OP>(m, sl, sink);
-}
-#define SP_COARSE_SHARE(c, total)                                                                  \
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < (total); c += (int64_t)gridDim.x * blockDim.x)
 
 // ---- level 1's fine part, a CTA (128 threads) per 8^3 block ----
 // As level 0's block kernels: the block's x (512 cells) and its halo (6 x 64 cells: the
