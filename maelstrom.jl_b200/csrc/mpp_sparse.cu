@@ -204,18 +204,15 @@ __global__ void __launch_bounds__(SPT) k_sp_blk(Topo t, Comp L, const uint16_t* 
         });
     } else {
         constexpr bool ZS = OP == BOP_JAC_ZS;
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) {
+        SP_ACTIVE_LOOP(c, L, gf) {
             int I, J, K;
             coarse_cell(t, c, I, J, K);
-            float v = 0.0f;
-            if (L.actc[c] != 0 && !covered(t, I, J, K)) {
-                float diag, off;
-                coarserow<16, ZS>(t, L, xf, xc, I, J, K, diag, off);
-                const float x0 = ZS ? 0.0f : xc[c];
-                if (OP == BOP_RES) v = bc[c] - (diag * x0 - off);
-                else v = diag > 0.0f ? x0 + OMEGA * (bc[c] - (diag * x0 - off)) / diag : 0.0f;
-            }
+            float diag, off;
+            coarserow<16, ZS>(t, L, xf, xc, I, J, K, diag, off);
+            const float x0 = ZS ? 0.0f : xc[c];
+            float v;
+            if (OP == BOP_RES) v = bc[c] - (diag * x0 - off);
+            else v = diag > 0.0f ? x0 + OMEGA * (bc[c] - (diag * x0 - off)) / diag : 0.0f;
             outc[c] = v;
         }
     }
@@ -346,12 +343,14 @@ __global__ void __launch_bounds__(SPT) k_sp_apply_dot(Topo t, Comp L, const uint
                                 ldm4(tf + n), LIQUID);
             });
     } else {
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) {
-            bool cov;
-            const float q = apply_coarse(t, L, df, dc, c, cov);
+        SP_ACTIVE_LOOP(c, L, gf) {
+            int I, J, K;
+            coarse_cell(t, c, I, J, K);
+            float diag, off;
+            coarserow<16, false>(t, L, df, dc, I, J, K, diag, off);
+            const float q = diag * dc[c] - off;
             qc[c] = q;
-            if (cmask[c]) acc[0] += (double)dc[c] * (double)q;
+            acc[0] += (double)dc[c] * (double)q;
         }
     }
     if (grid_sum<1>(acc, partials, counter) && threadIdx.x == 0) {
@@ -531,10 +530,12 @@ __global__ void __launch_bounds__(SPT) k_sp_apply(Topo t, Comp L, const uint16_t
             st4(qf + n, make_float4(q[0], q[1], q[2], q[3]));
         });
     } else {
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) {
-            bool cov;
-            qc[c] = apply_coarse(t, L, xf, xc, c, cov);
+        SP_ACTIVE_LOOP(c, L, gf) {
+            int I, J, K;
+            coarse_cell(t, c, I, J, K);
+            float diag, off;
+            coarserow<16, false>(t, L, xf, xc, I, J, K, diag, off);
+            qc[c] = diag * xc[c] - off;
         }
     }
 }
@@ -695,6 +696,8 @@ struct mpp_sparse_ctx {
     uint16_t* code0;    // each fine cell's six couplings, active and LIQUID bits (the block kernels)
     float* dg0;         // each fine cell's whole diagonal
     uint8_t* cmask;     // the coarse unknowns (LIQUID, no fine block over them)
+    int* clist;         // and their indices, listed by the operator (nclist of them)
+    int* nclist;
     uint8_t* actc;      // = D[0].act
     // level 1
     float *c1[3], *dD1, *dg1, *x1f, *b1f, *r1f, *t1f, *x1c, *r1c, *t1c;
@@ -776,12 +779,14 @@ Comp comp0(const mpp_sparse_ctx* c, const uint8_t* tf) {
     Comp L;
     L.cfx = c->cf[0]; L.cfy = c->cf[1]; L.cfz = c->cf[2]; L.dDf = c->dDf; L.actf = tf;
     L.ccx = c->cc[0]; L.ccy = c->cc[1]; L.ccz = c->cc[2]; L.dDc = c->dDc; L.actc = c->actc;
+    L.clist = c->clist; L.nclist = c->nclist;
     return L;
 }
 Comp comp1(const mpp_sparse_ctx* c) {
     Comp L;
     L.cfx = c->c1[0]; L.cfy = c->c1[1]; L.cfz = c->c1[2]; L.dDf = c->dD1; L.actf = c->act1;
     L.ccx = c->cc[0]; L.ccy = c->cc[1]; L.ccz = c->cc[2]; L.dDc = c->dDc; L.actc = c->actc;
+    L.clist = c->clist; L.nclist = c->nclist;
     return L;
 }
 
@@ -823,9 +828,13 @@ struct SpRun {
         for (int a = 1; a <= 3; a++) mc = std::max(mc, face_count(t.nc, a));
         sp_launch(k_sp_coarsecoef, dim3(grid1(mc), 3), SPT, s, t, c->cc[0], c->cc[1], c->cc[2], b->types_c);
         const Split sp = split_for(c, (int64_t)t.nslots * BCELLS);
+        cudaMemsetAsync(c->nclist, 0, sizeof(int), s);
+        // the coarse parts the composite passes write only on the listed cells start at zero
+        for (float* a : {c->tmc, c->zc, c->res0c, c->qc, c->t1c, c->x1c, c->r1c})
+            cudaMemsetAsync(a, 0, sizeof(float) * (size_t)c->ncc, s);
         sp_launch(k_sp_dirichlet, dim3(sp.g), SPT, s, t, c->dDf, c->dDc, c->actc, b->types_f, b->types_c, b->phi_f,
                   b->phi_c, (const float*)c->cf[0], (const float*)c->cf[1], (const float*)c->cf[2], c->code0, c->dg0,
-                  c->cmask, sp.gf);
+                  c->cmask, c->clist, c->nclist, sp.gf);
         nk += 3;
         hierarchy(b->types_f);
     }
@@ -1349,6 +1358,8 @@ int mpp_sparse_ctx_create(mpp_sparse_ctx** out, const mpp_sparse_grid* g, int32_
     if (!e) e = sp_alloc_n(c, &c->code0, nf);
     if (!e) e = sp_alloc_n(c, &c->dg0, nf);
     if (!e) e = sp_alloc_n(c, &c->cmask, c->ncc);
+    if (!e) e = sp_alloc_n(c, &c->clist, c->ncc);
+    if (!e) e = sp_alloc_n(c, &c->nclist, 1);
     int m[3] = {c->t.nc[0], c->t.nc[1], c->t.nc[2]};
     for (int l = 0; l < nd && !e; l++) {
         DL& D = c->D[l];
@@ -1441,6 +1452,8 @@ int mpp_sparse_apply(mpp_sparse_ctx* c, const mpp_sparse_basin* b, const float* 
         return MPP_ERR_INVALID;
     }
     SpRun run{c, (cudaStream_t)stream};
+    // the coarse cells outside the operator's list are zero in q (the pass writes only the list)
+    SCK(cudaMemsetAsync(qc, 0, sizeof(float) * (size_t)c->ncc, run.s));
     apply_(c, run, b->types_f, xf, xc, qf, qc);
     return finish(c, run, nullptr, MPP_OK);
 }
@@ -1457,6 +1470,7 @@ int mpp_sparse_vcycle(mpp_sparse_ctx* c, const mpp_sparse_basin* b, const float*
         return MPP_ERR_INVALID;
     }
     SpRun run{c, (cudaStream_t)stream};
+    SCK(cudaMemsetAsync(zc, 0, sizeof(float) * (size_t)c->ncc, run.s));  // as mpp_sparse_apply's q
     run.vcycle(b->types_f, zf, zc, rf, rc, sweeps, coarse, boost);
     return finish(c, run, nullptr, MPP_OK);
 }

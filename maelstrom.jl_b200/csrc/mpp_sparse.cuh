@@ -161,6 +161,11 @@ struct Comp {
     const uint8_t* actf;
     const float *ccx, *ccy, *ccz, *dDc;
     const uint8_t* actc;
+    // the coarse cells the composite passes update (LIQUID, no fine block over them; actc is
+    // set on exactly these outside fine blocks), listed once per operator: the passes walk
+    // the list, and every other coarse cell of their outputs stays at the zero it was cleared to
+    const int* clist;
+    const int* nclist;
 };
 
 // coarserow (src/sflip.jl:1176-1217): a coarse cell outside fine blocks, its coarse
@@ -247,6 +252,12 @@ __device__ __forceinline__ int sp_slot(int gf) { return (int)blockIdx.x - ((int)
 #define SP_FINE_LOOP(n, total, gf)                                                                        \
     for (int64_t n = (int64_t)((int)blockIdx.x - ((int)gridDim.x - (gf))) * blockDim.x + threadIdx.x; n < (total); \
          n += (int64_t)(gf) * blockDim.x)
+// The coarse part's walk over the operator's list of coarse unknowns (the coarse CTAs of a
+// fused launch, [0, gridDim - gf), as SP_COARSE_LOOP).
+#define SP_ACTIVE_LOOP(c, L, gf)                                                                   \
+    for (int64_t e_ = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ne_ = *(L).nclist; e_ < ne_; \
+         e_ += (int64_t)(gridDim.x - (gf)) * blockDim.x)                                           \
+        if (const int64_t c = (L).clist[e_]; true)
 #define SP_COARSE_LOOP(c, total, gf)                                                               \
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < (total);                  \
          c += (int64_t)(gridDim.x - (gf)) * blockDim.x)
@@ -307,7 +318,8 @@ __device__ __forceinline__ unsigned ccode(float c) { return c == FINE_FINE ? 2u 
 __global__ void __launch_bounds__(SPT) k_sp_dirichlet(Topo t, float* dDf, float* dDc, uint8_t* actc, const uint8_t* tf,
                                                       const uint8_t* tc, const float* phif, const float* phic,
                                                       const float* cfx, const float* cfy, const float* cfz,
-                                                      uint16_t* code0, float* dg0, uint8_t* cmask, int gf) {
+                                                      uint16_t* code0, float* dg0, uint8_t* cmask, int* clist,
+                                                      int* nclist, int gf) {
     pdl_wait();
     pdl_trigger();
     if (sp_is_fine(gf)) {
@@ -378,6 +390,7 @@ __global__ void __launch_bounds__(SPT) k_sp_dirichlet(Topo t, float* dDf, float*
             dDc[c] = d;
             actc[c] = (tc[c] == LIQUID && !cov) ? 1 : 0;
             cmask[c] = actc[c];
+            if (actc[c]) clist[atomicAdd(nclist, 1)] = (int)c;
         }
     }
 }
@@ -1022,18 +1035,15 @@ __global__ void __launch_bounds__(T8) k_sp_blk8(Topo t, Comp L, const float* dg1
         }
         *reinterpret_cast<float4*>(outf + n) = make_float4(out[0], out[1], out[2], out[3]);
     } else {
-        const int64_t nc = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
-        SP_COARSE_LOOP(c, nc, gf) {
+        SP_ACTIVE_LOOP(c, L, gf) {
             int I, J, K;
             coarse_cell(t, c, I, J, K);
-            float v = 0.0f;
-            if (L.actc[c] != 0 && !covered(t, I, J, K)) {
-                float diag, off;
-                coarserow<8, ZS>(t, L, xf, xc, I, J, K, diag, off);
-                const float x0 = ZS ? 0.0f : xc[c];
-                if (OP == BOP_RES) v = bc[c] - (diag * x0 - off);
-                else v = diag > 0.0f ? x0 + OMEGA * (bc[c] - (diag * x0 - off)) / diag : 0.0f;
-            }
+            float diag, off;
+            coarserow<8, ZS>(t, L, xf, xc, I, J, K, diag, off);
+            const float x0 = ZS ? 0.0f : xc[c];
+            float v;
+            if (OP == BOP_RES) v = bc[c] - (diag * x0 - off);
+            else v = diag > 0.0f ? x0 + OMEGA * (bc[c] - (diag * x0 - off)) / diag : 0.0f;
             outc[c] = v;
         }
     }
