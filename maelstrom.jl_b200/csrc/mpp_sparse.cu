@@ -184,7 +184,7 @@ __device__ __forceinline__ double dot4m(float4 a, float4 b, uchar4 m, uint8_t wa
 // Level 0's Jacobi sweeps and residual: the fine part a CTA per slot (staged block), the
 // coarse part as jacobicoarse_kernel! / residualcoarse_kernel!.
 template <int OP>
-__global__ void __launch_bounds__(SPT) k_sp_blk(Topo t, Comp L, const uint16_t* code0, const float* dg0, float* outf,
+__global__ void __launch_bounds__(SPT, 6) k_sp_blk(Topo t, Comp L, const uint16_t* code0, const float* dg0, float* outf,
                                                 float* outc, const float* xf, const float* xc, const float* bf,
                                                 const float* bc, int gf) {
     __shared__ float xs[PCELLS];
@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(SPT) k_sp_dinit(Topo t, const uint8_t* tf, con
 }
 
 // q = A d and d.q -> alpha = rho / d.q (src/sflip.jl:1885-1889).
-__global__ void __launch_bounds__(SPT) k_sp_apply_dot(Topo t, Comp L, const uint16_t* code0, const float* dg0,
+__global__ void __launch_bounds__(SPT, 6) k_sp_apply_dot(Topo t, Comp L, const uint16_t* code0, const float* dg0,
                                                       const uint8_t* tf, const uint8_t* cmask, const float* df,
                                                       const float* dc, float* qf, float* qc, SpState* st,
                                                       double* partials, unsigned* counter, int gf) {
