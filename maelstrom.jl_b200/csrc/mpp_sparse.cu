@@ -183,10 +183,12 @@ __device__ __forceinline__ double dot4m(float4 a, float4 b, uchar4 m, uint8_t wa
 
 // Level 0's Jacobi sweeps and residual: the fine part a CTA per slot (staged block), the
 // coarse part as jacobicoarse_kernel! / residualcoarse_kernel!.
-template <int OP>
+// Src (SrcX, SrcZS, SrcPro) is where x comes from: a sweep from SrcZS is the second sweep of a
+// pair from zero, fused with the first; one from SrcPro is the first sweep after the
+// prolongation from level 1, fused with it.
+template <int OP, class Src>
 __global__ void __launch_bounds__(SPT, 6) k_sp_blk(Topo t, Comp L, const uint16_t* code0, const float* dg0, float* outf,
-                                                float* outc, const float* xf, const float* xc, const float* bf,
-                                                const float* bc, int gf) {
+                                                float* outc, Src src, const float* bf, const float* bc, int gf) {
     __shared__ float xs[PCELLS];
     pdl_wait();
     pdl_trigger();
@@ -196,7 +198,7 @@ __global__ void __launch_bounds__(SPT, 6) k_sp_blk(Topo t, Comp L, const uint16_
         where_of(t, sl, w);
         if (w[0] < 0) return;
         if (OP != BOP_JAC_ZS) {
-            stage_block(t, xf, xc, sl, w, xs);
+            stage_block_s(t, src, sl, w, xs);
             __syncthreads();
         }
         block_cells<OP>(code0, dg0, bf, xs, sl, [&](int64_t n, const float* v, const float*) {
@@ -208,13 +210,26 @@ __global__ void __launch_bounds__(SPT, 6) k_sp_blk(Topo t, Comp L, const uint16_
             int I, J, K;
             coarse_cell(t, c, I, J, K);
             float diag, off;
-            coarserow<16, ZS>(t, L, xf, xc, I, J, K, diag, off);
-            const float x0 = ZS ? 0.0f : xc[c];
+            coarserow_s<16, ZS>(t, L, src, I, J, K, diag, off);
+            const float x0 = ZS ? 0.0f : src.coarse(c);
             float v;
             if (OP == BOP_RES) v = bc[c] - (diag * x0 - off);
             else v = diag > 0.0f ? x0 + OMEGA * (bc[c] - (diag * x0 - off)) / diag : 0.0f;
             outc[c] = v;
         }
+    }
+}
+
+// The coarse unknowns' whole diagonals (coarserow's sums), for SrcZS.
+__global__ void __launch_bounds__(SPT) k_sp_dgc(Topo t, Comp L, float* dgc) {
+    pdl_wait();
+    pdl_trigger();
+    SP_ACTIVE_LOOP(c, L, 0) {
+        int I, J, K;
+        coarse_cell(t, c, I, J, K);
+        float diag, off;
+        coarserow<16, true>(t, L, nullptr, nullptr, I, J, K, diag, off);
+        dgc[c] = diag;
     }
 }
 
@@ -696,6 +711,7 @@ struct mpp_sparse_ctx {
     uint16_t* code0;    // each fine cell's six couplings, active and LIQUID bits (the block kernels)
     float* dg0;         // each fine cell's whole diagonal
     uint8_t* cmask;     // the coarse unknowns (LIQUID, no fine block over them)
+    float* dgc;         // and their whole diagonals
     int* clist;         // and their indices, listed by the operator (nclist of them)
     int* nclist;
     uint8_t* actc;      // = D[0].act
@@ -835,7 +851,8 @@ struct SpRun {
         sp_launch(k_sp_dirichlet, dim3(sp.g), SPT, s, t, c->dDf, c->dDc, c->actc, b->types_f, b->types_c, b->phi_f,
                   b->phi_c, (const float*)c->cf[0], (const float*)c->cf[1], (const float*)c->cf[2], c->code0, c->dg0,
                   c->cmask, c->clist, c->nclist, sp.gf);
-        nk += 3;
+        sp_launch(k_sp_dgc, dim3(cap_blocks(c, c->ncc)), SPT, s, t, comp0(c, b->types_f), c->dgc);
+        nk += 4;
         hierarchy(b->types_f);
     }
     void hierarchy(const uint8_t* tf) {
@@ -860,20 +877,32 @@ struct SpRun {
         }
     }
     // smooth! (src/sflip.jl:1292-1303) after zero!(x): the first sweep from zeros
+    // Level 0: from zero, the first pair's two sweeps are one launch (the first sweep formed
+    // on the fly by SrcZS); with `pro` set, the prolongation from level 1 rides in the first
+    // sweep (SrcPro) instead of a pass of its own.
     template <int N>
     void smooth(const Comp& L, float* xf, float* xc, const float* bf, const float* bc, float* tf_, float* tc_,
-                int sweeps, bool from_zero) {
+                int sweeps, bool from_zero, const SrcPro* pro = nullptr) {
         if (N == 16) {
             const Split sp = split_blk(c);
+            const uint16_t* code0 = c->code0;
+            const float* dg0 = c->dg0;
             for (int q = 0; q < sweeps; q++) {
-                if (q == 0 && from_zero)
-                    sp_launch(k_sp_blk<BOP_JAC_ZS>, dim3(sp.g), SPT, s, c->t, L, (const uint16_t*)c->code0,
-                              (const float*)c->dg0, tf_, tc_, (const float*)xf, (const float*)xc, bf, bc, sp.gf);
+                if (q == 0 && from_zero) {
+                    const SrcZS z{code0, dg0, bf, c->cmask, c->dgc, bc};
+                    sp_launch(k_sp_blk<BOP_JAC, SrcZS>, dim3(sp.g), SPT, s, c->t, L, code0, dg0, xf, xc, z, bf, bc,
+                              sp.gf);
+                    nk++;
+                    continue;
+                }
+                if (q == 0 && pro)
+                    sp_launch(k_sp_blk<BOP_JAC, SrcPro>, dim3(sp.g), SPT, s, c->t, L, code0, dg0, tf_, tc_, *pro, bf,
+                              bc, sp.gf);
                 else
-                    sp_launch(k_sp_blk<BOP_JAC>, dim3(sp.g), SPT, s, c->t, L, (const uint16_t*)c->code0,
-                              (const float*)c->dg0, tf_, tc_, (const float*)xf, (const float*)xc, bf, bc, sp.gf);
-                sp_launch(k_sp_blk<BOP_JAC>, dim3(sp.g), SPT, s, c->t, L, (const uint16_t*)c->code0,
-                          (const float*)c->dg0, xf, xc, (const float*)tf_, (const float*)tc_, bf, bc, sp.gf);
+                    sp_launch(k_sp_blk<BOP_JAC, SrcX>, dim3(sp.g), SPT, s, c->t, L, code0, dg0, tf_, tc_,
+                              SrcX{xf, xc}, bf, bc, sp.gf);
+                sp_launch(k_sp_blk<BOP_JAC, SrcX>, dim3(sp.g), SPT, s, c->t, L, code0, dg0, xf, xc,
+                          SrcX{tf_, tc_}, bf, bc, sp.gf);
                 nk += 2;
             }
             return;
@@ -909,8 +938,8 @@ struct SpRun {
         const Split s0 = split_for(c, (int64_t)t.nslots * BCELLS), s1 = split_for(c, (int64_t)t.nslots * BCELLS1);
         smooth<16>(L0, zf, zc, rf, rc, c->tmf, c->tmc, sweeps, true);
         const Split sb = split_blk(c);
-        sp_launch(k_sp_blk<BOP_RES>, dim3(sb.g), SPT, s, t, L0, (const uint16_t*)c->code0, (const float*)c->dg0,
-                  c->res0f, c->res0c, (const float*)zf, (const float*)zc, rf, rc, sb.gf);
+        sp_launch(k_sp_blk<BOP_RES, SrcX>, dim3(sb.g), SPT, s, t, L0, (const uint16_t*)c->code0,
+                  (const float*)c->dg0, c->res0f, c->res0c, SrcX{zf, zc}, rf, rc, sb.gf);
         sp_launch(k_sp_restrict01, dim3(grid1((int64_t)t.nslots * BCELLS1)), SPT, s, t, c->b1f,
                   (const float*)c->res0f);
         nk += 2;
@@ -945,10 +974,9 @@ struct SpRun {
                   (const uint8_t*)c->act1, (const uint8_t*)c->actc, boost, s1.gf);
         nk++;
         smooth<8>(L1, c->x1f, c->x1c, c->b1f, c->res0c, c->t1f, c->t1c, sweeps, false);
-        sp_launch(k_sp_prolong10, dim3(sb.g), SPT, s, t, zf, zc, (const float*)c->x1f, (const float*)c->x1c, tf,
-                  (const uint8_t*)c->actc, boost, sb.gf);
-        nk++;
-        smooth<16>(L0, zf, zc, rf, rc, c->tmf, c->tmc, sweeps, false);
+        // prolong10 rides in level 0's first up sweep
+        const SrcPro pro{zf, zc, c->code0, c->x1f, c->x1c, c->cmask, boost};
+        smooth<16>(L0, zf, zc, rf, rc, c->tmf, c->tmc, sweeps, false, &pro);
     }
     // the CG's prologue up to the loop: r, the norms, the first V-cycle, d and rho, and
     // the first iteration's q, alpha and update (the rotated loop's body starts with the
@@ -1099,9 +1127,9 @@ int fgmres(mpp_sparse_ctx* c, SpRun& run, const mpp_sparse_basin* b, const mpp_s
             run.vcycle(tf, c->zf, c->zc, c->Vf[j], c->Vc[j], o->sweeps, o->coarse, o->boost);
             // the diagonal component: one damped Jacobi step from zero (src/fgmres.jl:15-24)
             const Split s0 = split_blk(c);
-            sp_launch(k_sp_blk<BOP_JAC_ZS>, dim3(s0.g), SPT, run.s, c->t, comp0(c, tf), (const uint16_t*)c->code0,
-                      (const float*)c->dg0, c->Zf[j], c->Zc[j], (const float*)nullptr, (const float*)nullptr,
-                      (const float*)c->Vf[j], (const float*)c->Vc[j], s0.gf);
+            sp_launch(k_sp_blk<BOP_JAC_ZS, SrcX>, dim3(s0.g), SPT, run.s, c->t, comp0(c, tf),
+                      (const uint16_t*)c->code0, (const float*)c->dg0, c->Zf[j], c->Zc[j],
+                      SrcX{nullptr, nullptr}, (const float*)c->Vf[j], (const float*)c->Vc[j], s0.gf);
             run.nk++;
             axpy(c, run, c->Zf[j], c->Zc[j], 1.0f, c->zf, c->zc, 0, 0);
             apply_(c, run, tf, c->Zf[j], c->Zc[j], c->qf, c->qc);
@@ -1346,7 +1374,7 @@ int mpp_sparse_ctx_create(mpp_sparse_ctx** out, const mpp_sparse_grid* g, int32_
     }
     float** fine[] = {&c->dDf, &c->bf, &c->rf, &c->zf, &c->df, &c->qf, &c->rof, &c->tmf, &c->res0f};
     float** coarse[] = {&c->dDc, &c->bc, &c->rc, &c->zc, &c->dc, &c->qc, &c->roc, &c->tmc, &c->res0c,
-                        &c->x1c, &c->r1c, &c->t1c};
+                        &c->x1c, &c->r1c, &c->t1c, &c->dgc};
     float** lev1[] = {&c->dD1, &c->dg1, &c->x1f, &c->b1f, &c->r1f, &c->t1f};
     for (auto p : fine)
         if (!e) e = sp_alloc_n(c, p, nf);

@@ -168,11 +168,79 @@ struct Comp {
     const int* nclist;
 };
 
+// Where a level-0 pass reads x: the stored values (SrcX), or values formed on the fly, with
+// the same Float32 operations, from what a pass that the fused one replaces would have
+// stored. SrcZS: the first sweep of smooth! from zeros, elementwise (x = 0 makes off = 0).
+// SrcPro: z after prolong10fine_kernel! / prolongcoarse_kernel! (z plus boost times the
+// level-1 cell's value, on LIQUID fine cells and on the coarse unknowns).
+struct SrcX {
+    const float* xf;
+    const float* xc;
+    __device__ __forceinline__ float4 fine4(int64_t n) const { return *reinterpret_cast<const float4*>(xf + n); }
+    __device__ __forceinline__ float fine(int64_t n) const { return xf[n]; }
+    __device__ __forceinline__ float coarse(int64_t c) const { return xc[c]; }
+};
+struct SrcZS {
+    const uint16_t* code0;
+    const float* dg0;
+    const float* bf;
+    const uint8_t* cmask;  // the coarse unknowns: the cells the coarse part of a sweep writes
+    const float* dgc;      // their whole diagonals, coarserow's sums
+    const float* bc;
+    __device__ __forceinline__ static float sweep0(bool act, float diag, float b) {
+        const float x0 = 0.0f, off = 0.0f;
+        return act && diag > 0.0f ? x0 + OMEGA * (b - (diag * x0 - off)) / diag : 0.0f;
+    }
+    __device__ __forceinline__ float4 fine4(int64_t n) const {
+        const ushort4 cd = *reinterpret_cast<const ushort4*>(code0 + n);
+        const float4 d = *reinterpret_cast<const float4*>(dg0 + n), b = *reinterpret_cast<const float4*>(bf + n);
+        return make_float4(sweep0(cd.x & 0x1000u, d.x, b.x), sweep0(cd.y & 0x1000u, d.y, b.y),
+                           sweep0(cd.z & 0x1000u, d.z, b.z), sweep0(cd.w & 0x1000u, d.w, b.w));
+    }
+    __device__ __forceinline__ float fine(int64_t n) const { return sweep0(code0[n] & 0x1000u, dg0[n], bf[n]); }
+    __device__ __forceinline__ float coarse(int64_t c) const { return sweep0(cmask[c] != 0, dgc[c], bc[c]); }
+};
+struct SrcPro {
+    const float* zf;
+    const float* zc;
+    const uint16_t* code0;
+    const float* x1f;
+    const float* x1c;
+    const uint8_t* cmask;
+    float boost;
+    // the level-1 cell of fine pool cell n
+    __device__ __forceinline__ static int64_t parent(int64_t n) {
+        const int c = (int)(n & (BCELLS - 1)), i = c & 15, j = (c >> 4) & 15, k = c >> 8;
+        return (n >> 12) * BCELLS1 + (i >> 1) + 8 * ((j >> 1) + 8 * (k >> 1));
+    }
+    __device__ __forceinline__ float4 fine4(int64_t n) const {
+        float4 z = *reinterpret_cast<const float4*>(zf + n);
+        const ushort4 cd = *reinterpret_cast<const ushort4*>(code0 + n);
+        const int64_t b1 = parent(n);
+        const float xa = x1f[b1], xb = x1f[b1 + 1];
+        if (cd.x & 0x2000u) z.x += boost * xa;
+        if (cd.y & 0x2000u) z.y += boost * xa;
+        if (cd.z & 0x2000u) z.z += boost * xb;
+        if (cd.w & 0x2000u) z.w += boost * xb;
+        return z;
+    }
+    __device__ __forceinline__ float fine(int64_t n) const {
+        float v = zf[n];
+        if (code0[n] & 0x2000u) v += boost * x1f[parent(n)];
+        return v;
+    }
+    __device__ __forceinline__ float coarse(int64_t c) const {
+        float v = zc[c];
+        if (cmask[c] != 0) v += boost * x1c[c];
+        return v;
+    }
+};
+
 // coarserow (src/sflip.jl:1176-1217): a coarse cell outside fine blocks, its coarse
 // neighbours through coarse faces, a fine block's cells through the block's R^2 sub-faces.
-template <int N, bool ZS>
-__device__ __forceinline__ void coarserow(const Topo& t, const Comp& L, const float* xf, const float* xc, int I,
-                                          int J, int K, float& diag, float& off) {
+template <int N, bool ZS, class Src>
+__device__ __forceinline__ void coarserow_s(const Topo& t, const Comp& L, const Src& src, int I, int J, int K,
+                                            float& diag, float& off) {
     using V = Lv<N>;
     constexpr int R = N / 4;
     const int n1 = t.nc[0], n2 = t.nc[1], n3 = t.nc[2];
@@ -209,17 +277,23 @@ __device__ __forceinline__ void coarserow(const Topo& t, const Comp& L, const fl
                         const int64_t cidx = V::cell(s2, FI & M, FJ & M, FK & M);
                         const float c = Cf[fidx - 1];
                         diag += c;
-                        off += c * (ZS ? 0.0f : xf[cidx - 1]);
+                        off += c * (ZS ? 0.0f : src.fine(cidx - 1));
                     }
             } else {
                 const float c = sg < 0 ? Cc[lin3(f0, f1, I, J, K)] : Cc[lin3(f0, f1, I + e0, J + e1, K + e2)];
                 if (c > 0.0f) {
                     diag += c;
-                    off += c * (ZS ? 0.0f : xc[lin(t.nc, In, Jn, Kn)]);
+                    off += c * (ZS ? 0.0f : src.coarse(lin(t.nc, In, Jn, Kn)));
                 }
             }
         }
     }
+}
+
+template <int N, bool ZS>
+__device__ __forceinline__ void coarserow(const Topo& t, const Comp& L, const float* xf, const float* xc, int I,
+                                          int J, int K, float& diag, float& off) {
+    coarserow_s<N, ZS>(t, L, SrcX{xf, xc}, I, J, K, diag, off);
 }
 
 // The fine pool cell of thread index n: slot (1-based), local (i, j, k).
@@ -836,13 +910,13 @@ __device__ __forceinline__ float cdec(unsigned code, int m) {
 }
 
 // Stage slot sl's x and its halo into xs (256 threads).
-__device__ __forceinline__ void stage_block(const Topo& t, const float* __restrict__ x, const float* __restrict__ xc,
-                                            int sl, const int w[3], float* xs) {
+template <class Src>
+__device__ __forceinline__ void stage_block_s(const Topo& t, const Src& src, int sl, const int w[3], float* xs) {
     const int tid = (int)threadIdx.x;
-    const float4* x4 = reinterpret_cast<const float4*>(x + (int64_t)(sl - 1) * BCELLS);
+    const int64_t base = (int64_t)(sl - 1) * BCELLS;
     float4 v[4];
 #pragma unroll
-    for (int m = 0; m < 4; m++) v[m] = x4[tid + 256 * m];
+    for (int m = 0; m < 4; m++) v[m] = src.fine4(base + 4 * (tid + 256 * m));
     const int p = tid & 15, q = tid >> 4;
     float hv[6];
 #pragma unroll
@@ -854,10 +928,10 @@ __device__ __forceinline__ void stage_block(const Topo& t, const float* __restri
         const int nbi = w[0] + (ax == 0 ? sg : 0), nbj = w[1] + (ax == 1 ? sg : 0), nbk = w[2] + (ax == 2 ? sg : 0);
         const int s2 = inblocks(t, nbi, nbj, nbk) ? blockslot(t, nbi, nbj, nbk) : 0;
         if (s2 > 0) {
-            hv[f] = x[(int64_t)(s2 - 1) * BCELLS + (i & 15) + 16 * ((j & 15) + 16 * (k & 15))];
+            hv[f] = src.fine((int64_t)(s2 - 1) * BCELLS + (i & 15) + 16 * ((j & 15) + 16 * (k & 15)));
         } else {
             const int I = w[0] * BLOCK + i, J = w[1] * BLOCK + j, K = w[2] * BLOCK + k;
-            hv[f] = xc[coarse_clamped(t, I >> 2, J >> 2, K >> 2)];
+            hv[f] = src.coarse(coarse_clamped(t, I >> 2, J >> 2, K >> 2));
         }
     }
 #pragma unroll
@@ -877,6 +951,11 @@ __device__ __forceinline__ void stage_block(const Topo& t, const float* __restri
         const int k = ax == 2 ? (sg < 0 ? -1 : 16) : q;
         xs[pidx(i, j, k)] = hv[f];
     }
+}
+
+__device__ __forceinline__ void stage_block(const Topo& t, const float* __restrict__ x, const float* __restrict__ xc,
+                                            int sl, const int w[3], float* xs) {
+    stage_block_s(t, SrcX{x, xc}, sl, w, xs);
 }
 
 // off of one cell from the staged block (ZS: x all zeros, off = 0).
