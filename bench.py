@@ -778,7 +778,7 @@ def bench_sparse(steps, cpu=True):
 
     sc = ss.charybdis()
     # the CG loop driven from the host, one state read an iteration: faster here than the
-    # graph's conditional loop (11.8 against 12.1 ms measured)
+    # graph's conditional loop (10.8 against 11.3 ms measured)
     s = msp.SparseBasin.from_scene(sc, graph=False, tol=1e-4, maxiter=200)
     saved = {k: getattr(s, k).clone() for k in ("Pf", "Pc", "uf", "uc", "vf", "vc", "wf", "wc")}
 
