@@ -166,6 +166,8 @@ __global__ void __launch_bounds__(SPT) k_sp_rhs(Topo t, const uint8_t* tf, const
 #define SP_SLOT_PIECES(n)                                                                   \
     for (int m_ = 0; m_ < 4; m_++)                                                          \
         if (const int64_t n = (int64_t)(sl - 1) * BCELLS + 4 * ((int)threadIdx.x + 256 * m_); true)
+// the slots of a fine part of gf CTAs, each CTA every gf-th from its own
+#define SP_SLOTS(sl, gf) for (int sl = sp_slot(gf); sl <= t.nslots; sl += (gf))
 #define SP_COARSE_PIECES(c, nc4, gf)                                                        \
     for (int64_t c = 4 * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x); c < 4 * (nc4);        \
          c += 4 * (int64_t)(gridDim.x - (gf)) * blockDim.x)
@@ -409,8 +411,7 @@ __global__ void __launch_bounds__(SPT) k_sp_update(Topo t, const uint8_t* tf, co
     const float alpha = st->alpha, ma = -alpha;
     double acc[1] = {0.0};
     if (sp_is_fine(gf)) {
-        const int sl = sp_slot(gf);
-        if (slot_used(t, sl)) SP_SLOT_PIECES(n) {
+        SP_SLOTS(sl, gf) if (slot_used(t, sl)) SP_SLOT_PIECES(n) {
                 const float4 r = upd_piece(Pf + n, rf + n, rof + n, df + n, qf + n, alpha, ma);
                 acc[0] += dot4m(r, r, ldm4(tf + n), LIQUID);
             }
@@ -444,8 +445,7 @@ __global__ void __launch_bounds__(SPT) k_sp_dot2(Topo t, const uint8_t* tf, cons
     if (st->done) return;
     double acc[2] = {0.0, 0.0};
     if (sp_is_fine(gf)) {
-        const int sl = sp_slot(gf);
-        if (slot_used(t, sl)) SP_SLOT_PIECES(n) {
+        SP_SLOTS(sl, gf) if (slot_used(t, sl)) SP_SLOT_PIECES(n) {
                 const float4 z = ld4(zf + n);
                 const uchar4 m = ldm4(tf + n);
                 acc[0] += dot4m(z, ld4(rf + n), m, LIQUID);
@@ -489,8 +489,7 @@ __global__ void __launch_bounds__(SPT) k_sp_xpby(Topo t, float* df, float* dc, c
         st4(d, make_float4(zz.x + beta * dd.x, zz.y + beta * dd.y, zz.z + beta * dd.z, zz.w + beta * dd.w));
     };
     if (sp_is_fine(gf)) {
-        const int sl = sp_slot(gf);
-        if (slot_used(t, sl)) SP_SLOT_PIECES(n) piece(df + n, zf + n);
+        SP_SLOTS(sl, gf) if (slot_used(t, sl)) SP_SLOT_PIECES(n) piece(df + n, zf + n);
     } else {
         SP_COARSE_PIECES(c, (int64_t)t.nc[0] * t.nc[1] * t.nc[2] / 4, gf) piece(dc + c, zc + c);
     }
@@ -791,6 +790,17 @@ Split split_blk(const mpp_sparse_ctx* c) {
     return s;
 }
 
+// the CG's vector passes: a fine part of at most SP_VEC_CTAS CTAs a SM striding over the slots
+#ifndef SP_VEC_CTAS
+#define SP_VEC_CTAS 8
+#endif
+Split split_vec(const mpp_sparse_ctx* c) {
+    Split s;
+    s.gf = std::max(1, std::min(c->t.nslots, c->nsm * SP_VEC_CTAS));
+    s.g = s.gf + cap_blocks(c, c->ncc);
+    return s;
+}
+
 Comp comp0(const mpp_sparse_ctx* c, const uint8_t* tf) {
     Comp L;
     L.cfx = c->cf[0]; L.cfy = c->cf[1]; L.cfz = c->cf[2]; L.dDf = c->dDf; L.actf = tf;
@@ -1004,21 +1014,22 @@ struct SpRun {
         sp_launch(k_sp_apply_dot, dim3(s0.g), SPT, s, t, L0, (const uint16_t*)c->code0, (const float*)c->dg0,
                   b->types_f, (const uint8_t*)c->cmask, (const float*)c->df, (const float*)c->dc, c->qf, c->qc, c->st,
                   c->partials, c->counters + SCNT_DQ, s0.gf);
-        sp_launch(k_sp_update, dim3(s0.g), SPT, s, t, b->types_f, (const uint8_t*)c->cmask, b->P_f, b->P_c, c->rf, c->rc, c->rof,
+        const Split sv = split_vec(c);
+        sp_launch(k_sp_update, dim3(sv.g), SPT, s, t, b->types_f, (const uint8_t*)c->cmask, b->P_f, b->P_c, c->rf, c->rc, c->rof,
                   c->roc, (const float*)c->df, (const float*)c->dc, (const float*)c->qf, (const float*)c->qc, c->st,
-                  c->partials, c->counters + SCNT_UPD, s0.gf, cond, use_cond);
+                  c->partials, c->counters + SCNT_UPD, sv.gf, cond, use_cond);
         nk += 2;
     }
     // the rotated loop body: the V-cycle of the new residual, beta, d, then q, alpha, the update
     void cg_body(const mpp_sparse_basin* b, const mpp_sparse_opts* o, cudaGraphConditionalHandle cond, int use_cond) {
         const Topo& t = c->t;
-        const Split s0 = split_blk(c);
+        const Split sv = split_vec(c);
         vcycle(b->types_f, c->zf, c->zc, c->rf, c->rc, o->sweeps, o->coarse, o->boost);
-        sp_launch(k_sp_dot2, dim3(s0.g), SPT, s, t, b->types_f, (const uint8_t*)c->cmask, (const float*)c->zf, (const float*)c->zc,
+        sp_launch(k_sp_dot2, dim3(sv.g), SPT, s, t, b->types_f, (const uint8_t*)c->cmask, (const float*)c->zf, (const float*)c->zc,
                   (const float*)c->rf, (const float*)c->rc, (const float*)c->rof, (const float*)c->roc, c->st,
-                  c->partials, c->counters + SCNT_DOT2, s0.gf);
-        sp_launch(k_sp_xpby, dim3(s0.g), SPT, s, t, c->df, c->dc, (const float*)c->zf, (const float*)c->zc,
-                  (const SpState*)c->st, s0.gf);
+                  c->partials, c->counters + SCNT_DOT2, sv.gf);
+        sp_launch(k_sp_xpby, dim3(sv.g), SPT, s, t, c->df, c->dc, (const float*)c->zf, (const float*)c->zc,
+                  (const SpState*)c->st, sv.gf);
         nk += 2;
         cg_step(b, cond, use_cond);
     }
